@@ -1,0 +1,1021 @@
+/*
+ * gcr_oracle.c -- CPU restatement of the gliding-collective-rotation step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity checker for the CUDA
+ * path and the CPU baseline timed beside it.  Nothing in the product package
+ * links, loads or calls it.
+ *
+ * It restates, loop for loop, the reference's Numba hot path:
+ *   SRK_jit                    SRK.py:13-484   (SRK2 branch only)
+ *   thread_wait                SRK.py:487-495  (-> OpenMP barrier)
+ *   WCA                        forces.py:13-15
+ *   inbounds_diff              forces.py:44-55
+ *   central_pair_force         forces.py:57-145 (WCA rule, no active sliding)
+ *   self_propel                forces.py:206-224
+ *   calc_chain_spring_forces   forces.py:285-403 (Hookean branch)
+ *   update_grid_list_mini      updates.py:502-522
+ *   update_grid_list           updates.py:525-583 (overwrite / append modes)
+ *   update_nbor_list           updates.py:586-669
+ *   update_nbor_list_few       updates.py:672-734
+ *   chunk_chain                updates.py:323-344
+ *   calc_avg_phi_chain         output_methods.py:492-510
+ *   polar_orderparameter       analysis.py:315-328
+ *   nematic_orderparameter     analysis.py:294-313
+ * and the random streams the reference consumes:
+ *   MT19937 (Matsumoto & Nishimura 1998) with the 53-bit double and the
+ *   Marsaglia polar Gaussian with one cached deviate -- the stream that
+ *   Numba's np.random.standard_normal and numpy's RandomState produce.
+ * plus the counter-based Philox4x32-10 stream (Salmon et al., SC'11) that the
+ * CUDA path draws, keyed exactly as the CUDA path keys it.
+ *
+ * Arithmetic is IEEE double without contraction (built with
+ * -ffp-contract=off); integer power follows Numba's exponentiation by
+ * squaring.  Arrays use the reference's numpy layouts: float64 [N,dim],
+ * int64 chain ids, grid_list int64 [n,n,nz,1+depth], nbor_list int64
+ * [N,1+depth].
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <omp.h>
+
+#define GCRO_EXPORT __attribute__((visibility("default")))
+
+/* ------------------------------------------------------------------ */
+/* Random streams                                                      */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    uint32_t mt[624];
+    int idx;
+    int has_gauss;
+    double gauss;
+} gcro_mt;
+
+GCRO_EXPORT void gcro_mt_seed(gcro_mt *s, uint32_t seed)
+{
+    /* init_genrand of the 1998 MT19937 reference implementation */
+    s->mt[0] = seed;
+    for (int i = 1; i < 624; i++)
+        s->mt[i] = 1812433253u * (s->mt[i - 1] ^ (s->mt[i - 1] >> 30)) + (uint32_t)i;
+    s->idx = 624;
+    s->has_gauss = 0;
+    s->gauss = 0.0;
+}
+
+static uint32_t mt_next(gcro_mt *s)
+{
+    if (s->idx >= 624) {
+        for (int i = 0; i < 624; i++) {
+            uint32_t y = (s->mt[i] & 0x80000000u) | (s->mt[(i + 1) % 624] & 0x7fffffffu);
+            uint32_t v = s->mt[(i + 397) % 624] ^ (y >> 1);
+            if (y & 1u) v ^= 0x9908b0dfu;
+            s->mt[i] = v;
+        }
+        s->idx = 0;
+    }
+    uint32_t y = s->mt[s->idx++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
+}
+
+static double mt_double(gcro_mt *s)
+{
+    /* 53-bit resolution double in [0,1) from two 32-bit draws */
+    uint32_t a = mt_next(s) >> 5, b = mt_next(s) >> 6;
+    return ((double)a * 67108864.0 + (double)b) / 9007199254740992.0;
+}
+
+GCRO_EXPORT double gcro_mt_normal(gcro_mt *s)
+{
+    /* Marsaglia polar method, second deviate cached */
+    if (s->has_gauss) {
+        s->has_gauss = 0;
+        return s->gauss;
+    }
+    double x1, x2, r2;
+    do {
+        x1 = 2.0 * mt_double(s) - 1.0;
+        x2 = 2.0 * mt_double(s) - 1.0;
+        r2 = x1 * x1 + x2 * x2;
+    } while (r2 >= 1.0 || r2 == 0.0);
+    double f = sqrt(-2.0 * log(r2) / r2);
+    s->gauss = f * x1;
+    s->has_gauss = 1;
+    return f * x2;
+}
+
+GCRO_EXPORT void gcro_mt_normals(uint32_t seed, int64_t n, double *out)
+{
+    gcro_mt s;
+    gcro_mt_seed(&s, seed);
+    for (int64_t i = 0; i < n; i++) out[i] = gcro_mt_normal(&s);
+}
+
+/* Philox4x32-10: round function and key schedule from Salmon, Moraes, Dror
+ * and Shaw, "Parallel random numbers: as easy as 1, 2, 3" (SC'11). */
+static void philox4x32_10(const uint32_t ctr_in[4], const uint32_t key_in[2], uint32_t out[4])
+{
+    uint32_t c0 = ctr_in[0], c1 = ctr_in[1], c2 = ctr_in[2], c3 = ctr_in[3];
+    uint32_t k0 = key_in[0], k1 = key_in[1];
+    for (int r = 0; r < 10; r++) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0;
+        uint32_t hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n1 = lo1;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        uint32_t n3 = lo0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* Two standard normals from one Philox block, as the CUDA path draws them:
+ * counter = (bead, step lo, step hi, stream), key = (seed lo, seed hi);
+ * u1 in (0,1] and u2 in [0,1) with 53 bits each; Box-Muller. */
+GCRO_EXPORT void gcro_philox_pair(uint64_t seed, uint32_t bead, int64_t step, uint32_t stream,
+                                  double out[2])
+{
+    uint32_t ctr[4] = {bead, (uint32_t)((uint64_t)step & 0xffffffffu),
+                       (uint32_t)((uint64_t)step >> 32), stream};
+    uint32_t key[2] = {(uint32_t)(seed & 0xffffffffu), (uint32_t)(seed >> 32)};
+    uint32_t r[4];
+    philox4x32_10(ctr, key, r);
+    const double two_m53 = 1.1102230246251565e-16; /* 2^-53 */
+    uint64_t a = ((uint64_t)r[0] << 21) ^ (uint64_t)(r[1] >> 11);
+    uint64_t b = ((uint64_t)r[2] << 21) ^ (uint64_t)(r[3] >> 11);
+    a &= ((uint64_t)1 << 53) - 1;
+    b &= ((uint64_t)1 << 53) - 1;
+    double u1 = ((double)a + 1.0) * two_m53;  /* (0,1] */
+    double u2 = (double)b * two_m53;          /* [0,1) */
+    double rad = sqrt(-2.0 * log(u1));
+    double ang = 6.283185307179586 * u2;
+    out[0] = rad * cos(ang);
+    out[1] = rad * sin(ang);
+}
+
+/* Fill noise_vec [N, 2*dim] for one step from the Philox stream.
+ * Translational components use streams 0..; rotational ones 2... */
+GCRO_EXPORT void gcro_philox_noise(uint64_t seed, int64_t step, int dim, int64_t n,
+                                   int do_trans, int do_rot, double *noise)
+{
+    for (int64_t b = 0; b < n; b++) {
+        double z[4];
+        double *row = noise + b * 2 * dim;
+        if (do_trans) {
+            gcro_philox_pair(seed, (uint32_t)b, step, 0u, z);
+            if (dim == 3) gcro_philox_pair(seed, (uint32_t)b, step, 1u, z + 2);
+            for (int i = 0; i < dim; i++) row[i] = z[i];
+        }
+        if (do_rot) {
+            gcro_philox_pair(seed, (uint32_t)b, step, 2u, z);
+            if (dim == 3) gcro_philox_pair(seed, (uint32_t)b, step, 3u, z + 2);
+            for (int i = 0; i < dim; i++) row[dim + i] = z[i];
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* Small arithmetic helpers with the reference's semantics             */
+/* ------------------------------------------------------------------ */
+
+/* Python float modulo (floor-mod, result has the sign of the divisor). */
+static inline double py_mod(double x, double m)
+{
+    double r = fmod(x, m);
+    if (r != 0.0) {
+        if ((m < 0) != (r < 0)) r += m;
+    } else {
+        r = copysign(0.0, m);
+    }
+    return r;
+}
+
+/* Python float floor division (CPython float_floor_div / divmod). */
+static inline double py_floordiv(double x, double m)
+{
+    double mod = fmod(x, m);
+    double div = (x - mod) / m;
+    if (mod != 0.0) {
+        if ((m < 0) != (mod < 0)) div -= 1.0;
+    }
+    double fd;
+    if (div != 0.0) {
+        fd = floor(div);
+        if (div - fd > 0.5) fd += 1.0;
+    } else {
+        fd = copysign(0.0, x / m);
+    }
+    return fd;
+}
+
+/* x ** (-n) by squaring, as Numba lowers integer powers. */
+static inline double ipow_neg(double x, int n)
+{
+    double r = 1.0, a = x;
+    int e = n;
+    while (e) {
+        if (e & 1) r *= a;
+        e >>= 1;
+        a *= a;
+    }
+    return 1.0 / r;
+}
+
+/* forces.inbounds_diff (forces.py:44-55) */
+static inline double inbounds_diff(const double *a, const double *b, double hb, double L,
+                                   double *out, int dim)
+{
+    double ds = 0.0;
+    for (int i = 0; i < dim; i++) {
+        out[i] = a[i] - b[i];
+        if (out[i] < -hb)
+            out[i] += L;
+        else if (out[i] >= hb)
+            out[i] -= L;
+        ds += out[i] * out[i];
+    }
+    return ds;
+}
+
+/* ------------------------------------------------------------------ */
+/* Parameters and state                                                */
+/* ------------------------------------------------------------------ */
+
+typedef struct {
+    int32_t dim;
+    int32_t n_threads;
+    double L;
+    int64_t n_beads;
+    int64_t n_chains;
+    /* force switches derived as SRK.py:58-97 derives them */
+    int32_t calc_springs;
+    int32_t calc_wca;
+    int32_t self_propel;
+    int32_t noise_mode;     /* 0 = MT19937 (reference RNG), 1 = injected, 2 = Philox */
+    double spring[6];       /* populations.py:345-353 */
+    double wca[4];          /* populations.py:48-58 */
+    double active[3];       /* populations.py:355-358 */
+    double D, Dr, radius;
+    double rigid_rod;       /* must be 0: rigid-rod projection is not restated */
+    int64_t n_nearby;
+    int64_t longest_chain_length;
+    double grid_factor;
+    /* time_vals, updates.py:144-146 */
+    double dt, dtmax, max_dist_per_step, rk_cheat, max_dt_usable;
+    int64_t steps_until_update, n_steps_update, max_steps;
+    /* Philox key and the global step index of the first step of this call */
+    uint64_t seed;
+    int64_t step0;
+} gcro_params;
+
+typedef struct {
+    double *pos, *pos1, *noise, *tangent, *forces;
+    int64_t *where_active;
+    int64_t *where_is_bead;   /* [N,3] */
+    const int64_t *chain_id;  /* [N]   */
+    const double *rest_lengths; /* [n_chains] */
+    int64_t *grid_list;       /* [n, n, nz, depth1] */
+    int64_t n_grid, n_grid_z, grid_depth1;
+    int64_t *nbor_list;       /* [N, depth1] */
+    int64_t nbor_depth1;
+    /* injected noise: [n_steps][N][2*dim] snapshots of noise_vec */
+    const double *noise_inject;
+    int64_t noise_inject_steps;
+    /* MT19937 state per thread (n_threads entries) */
+    gcro_mt *mt;
+} gcro_state;
+
+/* shared_arr row layout, SRK.py: 0 dt, 1 elapsed, 2 steps, 3 max force,
+ * 4 barrier counter, 5 list-overflow flag */
+typedef struct {
+    double dt, dt_used_total, steps, max_forces_strength, counter, flag;
+} gcro_result;
+
+/* ------------------------------------------------------------------ */
+/* Forces                                                              */
+/* ------------------------------------------------------------------ */
+
+/* forces.calc_chain_spring_forces (forces.py:285-403), Hookean branch.
+ * Operates on a chain-aligned chunk [0,n) of the arrays. */
+static void spring_forces(const double *pos, double *tangent_list, const int64_t *chain_id,
+                          double *forces, int64_t n, double L, const double *sp,
+                          const double *rest_lengths, int dim)
+{
+    double half_L = L / 2.0;
+    int b_calc_f_bend = (sp[1] != 0.0);
+    int64_t max_b1 = n - 1;
+    int b_get_orientations = (sp[4] != 0.0);
+    double tangents[2][3] = {{0}};
+    int new_chain = 1;
+    int ti = 0, tj = 1;
+    int64_t ci = 0;
+    double chain_a = 0.0;
+
+    for (int64_t b1 = 0; b1 < n; b1++) {
+        if (new_chain) {
+            ti = 0;
+            tj = 1;
+            ci = chain_id[b1];
+            chain_a = rest_lengths[ci];
+        }
+        int end_of_chain;
+        if (b1 == max_b1)
+            end_of_chain = 1;
+        else if (chain_id[b1 + 1] != ci)
+            end_of_chain = 1;
+        else
+            end_of_chain = 0;
+        if (!end_of_chain) {
+            double dist_sq = inbounds_diff(pos + b1 * dim, pos + (b1 + 1) * dim, half_L, L,
+                                           tangents[ti], dim);
+            if (dist_sq != 0.0) {
+                double inv_dist = 1.0 / sqrt(dist_sq);
+                double f_spring_mag = sp[0] * (chain_a * inv_dist - 1.0);
+                for (int i = 0; i < dim; i++) {
+                    double f = tangents[ti][i] * f_spring_mag;
+                    forces[b1 * dim + i] += f;
+                    forces[(b1 + 1) * dim + i] -= f;
+                    tangents[ti][i] *= inv_dist;
+                }
+            }
+        }
+        if (b_get_orientations || b_calc_f_bend) {
+            if (new_chain) {
+                if (b_get_orientations)
+                    for (int i = 0; i < dim; i++) tangent_list[b1 * dim + i] = tangents[ti][i];
+            } else if (end_of_chain) {
+                if (b_get_orientations)
+                    for (int i = 0; i < dim; i++) tangent_list[b1 * dim + i] = tangents[tj][i];
+            } else {
+                double c = 0.0;
+                for (int i = 0; i < dim; i++) c += tangents[ti][i] * tangents[tj][i];
+                if (-1.0 < c && c < 1.0) {
+                    if (b_calc_f_bend) {
+                        double phi = acos(c);
+                        if (sp[2] != 0.0) {
+                            double cr = -tangents[ti][0] * tangents[tj][1] +
+                                        tangents[ti][1] * tangents[tj][0];
+                            double sg = (cr > 0) - (cr < 0);
+                            phi += sp[2] * sg;
+                        }
+                        phi *= sp[1] / sqrt(1.0 - c * c);
+                        for (int i = 0; i < dim; i++) {
+                            double fwd = phi * (c * tangents[tj][i] - tangents[ti][i]);
+                            double bwd = phi * (tangents[tj][i] - c * tangents[ti][i]);
+                            forces[b1 * dim + i] += fwd + bwd;
+                            forces[(b1 - 1) * dim + i] -= fwd;
+                            forces[(b1 + 1) * dim + i] -= bwd;
+                        }
+                    }
+                    if (b_get_orientations) {
+                        double coeff = 1.0 / sqrt(2.0 * (1.0 + c));
+                        for (int i = 0; i < dim; i++)
+                            tangent_list[b1 * dim + i] = coeff * (tangents[ti][i] + tangents[tj][i]);
+                    }
+                } else {
+                    if (b_get_orientations)
+                        for (int i = 0; i < dim; i++) tangent_list[b1 * dim + i] = tangents[ti][i];
+                }
+            }
+        }
+        tj = ti;
+        ti = 1 - ti;
+        new_chain = end_of_chain;
+    }
+}
+
+/* forces.central_pair_force (forces.py:57-145) with force_rule = forces.WCA
+ * (forces.py:13-15), same population, thread chunk [start, start+n). */
+static void pair_forces(int64_t start, const double *pos_chunk, const int64_t *nbor, int64_t nbd1,
+                        double *forces_chunk, int64_t n, double L, const double *pos2,
+                        const double *wp, double pbc_w, int dim)
+{
+    double half_L = L / 2.0;
+    double rc_sq = wp[3] * wp[3];
+    double pbc_wR = L - pbc_w;
+    int64_t end = start + n;
+    double seps[3];
+    for (int64_t b1 = 0; b1 < n; b1++) {
+        int flags[3];
+        for (int i = 0; i < dim; i++) {
+            double x = pos_chunk[b1 * dim + i];
+            flags[i] = !(pbc_w <= x && x < pbc_wR);
+        }
+        int64_t true_b1 = b1 + start;
+        const int64_t *row = nbor + b1 * nbd1;
+        for (int64_t j = 0; j < row[0]; j++) {
+            int64_t b2 = row[1 + j];
+            if (true_b1 <= b2 && b2 < end) continue;
+            int same_thread = (true_b1 > b2 && b2 >= start);
+            double ds = 0.0;
+            for (int i = 0; i < dim; i++) {
+                double sep = pos2[b2 * dim + i] - pos_chunk[b1 * dim + i];
+                if (flags[i]) {
+                    if (sep < -half_L)
+                        sep += L;
+                    else if (sep >= half_L)
+                        sep -= L;
+                }
+                seps[i] = sep;
+                ds += sep * sep;
+            }
+            if (0.0 < ds && ds <= rc_sq) {
+                if (wp[2] != 0.0) {
+                    double mag = sqrt(ds);
+                    double nm = mag + wp[2];
+                    if (nm < 0.0) nm = 0.0;
+                    double rescale = nm / mag;
+                    for (int i = 0; i < dim; i++) seps[i] *= rescale;
+                    ds = nm * nm;
+                }
+                double coeff = ipow_neg(ds, 4) * (wp[0] - wp[1] * ipow_neg(ds, 3));
+                if (same_thread) {
+                    int64_t b2l = b2 - start;
+                    for (int i = 0; i < dim; i++) {
+                        double f = seps[i] * coeff;
+                        forces_chunk[b1 * dim + i] += f;
+                        forces_chunk[b2l * dim + i] -= f;
+                    }
+                } else {
+                    for (int i = 0; i < dim; i++) forces_chunk[b1 * dim + i] += seps[i] * coeff;
+                }
+            }
+        }
+    }
+}
+
+/* forces.self_propel (forces.py:206-224) */
+static void self_propel(double *forces, const double *tangent, int64_t n, const double *ap, int dim)
+{
+    double v0 = ap[0], ang = ap[2];
+    if (ang == 0.0 || dim != 2) {
+        for (int64_t b = 0; b < n; b++)
+            for (int i = 0; i < dim; i++) forces[b * dim + i] += v0 * tangent[b * dim + i];
+    } else {
+        double sn = sin(ang), cs = cos(ang);
+        for (int64_t b = 0; b < n; b++) {
+            double tx = tangent[b * dim], ty = tangent[b * dim + 1];
+            forces[b * dim] += v0 * (cs * tx - sn * ty);
+            forces[b * dim + 1] += v0 * (sn * tx + cs * ty);
+        }
+    }
+}
+
+/* Public single-call wrappers for unit tests (whole array = one chunk). */
+GCRO_EXPORT void gcro_spring_forces(const double *pos, double *tangent_list, const int64_t *chain_id,
+                                    double *forces, int64_t n, double L, const double *spring_params,
+                                    const double *rest_lengths, int dim)
+{
+    spring_forces(pos, tangent_list, chain_id, forces, n, L, spring_params, rest_lengths, dim);
+}
+
+GCRO_EXPORT void gcro_pair_forces(const double *pos, const int64_t *nbor, int64_t nbd1, double *forces,
+                                  int64_t n, double L, const double *wca_params, double pbc_w, int dim)
+{
+    pair_forces(0, pos, nbor, nbd1, forces, n, L, pos, wca_params, pbc_w, dim);
+}
+
+GCRO_EXPORT void gcro_self_propel(double *forces, const double *tangent, int64_t n,
+                                  const double *active_params, int dim)
+{
+    self_propel(forces, tangent, n, active_params, dim);
+}
+
+/* ------------------------------------------------------------------ */
+/* Cell and neighbour lists                                            */
+/* ------------------------------------------------------------------ */
+
+#define GL(g, gx, gy, gz, k) \
+    (g)->grid_list[((((gx) * (g)->n_grid + (gy)) * (g)->n_grid_z + (gz)) * (g)->grid_depth1) + (k)]
+
+/* updates.update_grid_list_mini (updates.py:502-522) over all beads of the
+ * population for the x-slab [start_gx, end_gx).  Returns 1 on success. */
+static int grid_list_mini(gcro_state *g, int64_t n_beads, int64_t start_gx, int64_t end_gx)
+{
+    int64_t depth_less_one = g->grid_depth1 - 2;
+    for (int64_t gx = start_gx; gx < end_gx; gx++)
+        for (int64_t gy = 0; gy < g->n_grid; gy++)
+            for (int64_t gz = 0; gz < g->n_grid_z; gz++) GL(g, gx, gy, gz, 0) = 0;
+    for (int64_t bi = 0; bi < n_beads; bi++) {
+        const int64_t *w = g->where_is_bead + bi * 3;
+        /* A bead at exactly x == L (floor-mod of a tiny negative number)
+         * has cell index n_grid; the reference then writes outside its
+         * array.  Such a bead is left out of every cell here. */
+        if (start_gx <= w[0] && w[0] < end_gx && w[1] >= 0 && w[1] < g->n_grid && w[2] >= 0 &&
+            w[2] < g->n_grid_z) {
+            int64_t *cell = &GL(g, w[0], w[1], w[2], 0);
+            cell[0] += 1;
+            if (cell[0] < depth_less_one)
+                cell[cell[0]] = bi;
+            else
+                return 0;
+        }
+    }
+    return 1;
+}
+
+/* updates.update_grid_list (updates.py:525-583), as populations.py:104-112
+ * calls it (overwrite / append modes and the incremental mode). */
+GCRO_EXPORT int gcro_update_grid_list(gcro_state *g, const double *pos, int64_t n, double L, int dim,
+                                      int append_mode, int overwrite, int64_t start)
+{
+    int64_t ng = g->n_grid, ngz = g->n_grid_z;
+    double spacing = L / (double)ng;
+    for (int64_t bi = 0; bi < n; bi++) {
+        for (int i = 0; i < dim; i++)
+            g->where_is_bead[bi * 3 + i] = (int64_t)py_floordiv(pos[bi * dim + i], spacing);
+        if (dim == 2) g->where_is_bead[bi * 3 + 2] = 0;
+    }
+    if (append_mode || overwrite) {
+        for (int64_t bi = 0; bi < n; bi++) g->where_is_bead[bi * 3] = -g->where_is_bead[bi * 3] - 1;
+        if (overwrite)
+            for (int64_t c = 0; c < ng * ng * ngz; c++) g->grid_list[c * g->grid_depth1] = 0;
+    } else {
+        start = 0;
+        for (int64_t gx = 0; gx < ng; gx++)
+            for (int64_t gy = 0; gy < ng; gy++)
+                for (int64_t gz = 0; gz < ngz; gz++) {
+                    int64_t *cell = &GL(g, gx, gy, gz, 0);
+                    int64_t gxyz[3] = {gx, gy, gz};
+                    int64_t num_here_now = 0;
+                    int64_t cnt = cell[0];
+                    for (int64_t k = 0; k < cnt; k++) {
+                        int64_t bi = cell[1 + k];
+                        int moved = 0;
+                        for (int i = 0; i < dim; i++)
+                            if (g->where_is_bead[bi * 3 + i] != gxyz[i]) {
+                                moved = 1;
+                                break;
+                            }
+                        if (moved) {
+                            cell[1 + num_here_now] = bi;
+                            num_here_now++;
+                        } else {
+                            g->where_is_bead[bi * 3] = -g->where_is_bead[bi * 3] - 1;
+                        }
+                    }
+                    cell[0] = num_here_now;
+                }
+    }
+    int64_t depth = g->grid_depth1;
+    for (int64_t bi = 0; bi < n; bi++) {
+        int64_t *w = g->where_is_bead + bi * 3;
+        if (w[0] < 0) {
+            w[0] = -w[0] - 1;
+            if (w[0] >= ng || w[1] < 0 || w[1] >= ng || w[2] < 0 || w[2] >= ngz) continue;
+            int64_t *cell = &GL(g, w[0], w[1], w[2], 0);
+            if (cell[0] < depth - 2)
+                cell[1 + cell[0]] = start + bi;
+            else
+                return 0;
+            cell[0] += 1;
+        }
+    }
+    return 1;
+}
+
+/* updates.update_nbor_list (updates.py:586-669) for a chunk starting at
+ * `start` (same population).  Returns 1 on success, 0 on overflow. */
+static int nbor_list_cells(int64_t start, const double *pos1, const int64_t *wib1, int64_t *nb,
+                           int64_t nbd1, int64_t n, const int64_t *chain_id, const double *pos2,
+                           const gcro_state *g, int64_t n_nearby, double L, int64_t gw, int dim)
+{
+    int b3d = (dim == 3);
+    int64_t ng = g->n_grid;
+    double hgrid = (double)gw * L / (double)ng;
+    double max_dist_sq = hgrid * hgrid;
+    double half_L = L / 2.0;
+    for (int64_t b1 = 0; b1 < n; b1++) nb[b1 * nbd1] = 0;
+    int64_t dg_start = -(gw < ng / 2 ? gw : ng / 2);
+    int64_t dg_end = (1 + gw < ng + dg_start) ? 1 + gw : ng + dg_start;
+    for (int64_t b1 = 0; b1 < n; b1++) {
+        int64_t b1u = b1 + start;
+        int flags[3];
+        for (int i = 0; i < dim; i++) {
+            int64_t w = wib1[b1 * 3 + i];
+            flags[i] = (w < gw + 1) || (w >= ng - (gw + 1));
+        }
+        int64_t gy0 = dg_start + wib1[b1 * 3 + 1], gy1 = wib1[b1 * 3 + 1] + dg_end;
+        int64_t gz0, gz1;
+        if (b3d) {
+            gz0 = dg_start + wib1[b1 * 3 + 2];
+            gz1 = wib1[b1 * 3 + 2] + dg_end;
+        } else {
+            gz0 = 0;
+            gz1 = 1;
+        }
+        for (int64_t gx2r = dg_start + wib1[b1 * 3]; gx2r < wib1[b1 * 3] + dg_end; gx2r++) {
+            int64_t gx2 = gx2r;
+            if (flags[0]) gx2 = ((gx2 % ng) + ng) % ng;
+            for (int64_t gy2r = gy0; gy2r < gy1; gy2r++) {
+                int64_t gy2 = gy2r;
+                if (flags[1]) gy2 = ((gy2 % ng) + ng) % ng;
+                for (int64_t gz2r = gz0; gz2r < gz1; gz2r++) {
+                    int64_t gz2 = gz2r;
+                    if (b3d && flags[2]) gz2 = ((gz2 % ng) + ng) % ng;
+                    const int64_t *cell = &g->grid_list[(((gx2 * ng + gy2) * g->n_grid_z + gz2) * g->grid_depth1)];
+                    int64_t cnt = cell[0];
+                    for (int64_t k = 0; k < cnt; k++) {
+                        int64_t b2 = cell[1 + k];
+                        if (chain_id[b1u] == chain_id[b2]) {
+                            if (n_nearby < 0) continue;
+                            int64_t d = b1u - b2;
+                            if (d < 0) d = -d;
+                            if (d <= n_nearby) continue;
+                        }
+                        double dist_sq = 0.0;
+                        for (int i = 0; i < dim; i++) {
+                            double sep = pos2[b2 * dim + i] - pos1[b1 * dim + i];
+                            if (flags[i]) {
+                                if (sep < -half_L)
+                                    sep += L;
+                                else if (sep >= half_L)
+                                    sep -= L;
+                            }
+                            dist_sq += sep * sep;
+                        }
+                        if (dist_sq <= max_dist_sq) {
+                            int64_t *row = nb + b1 * nbd1;
+                            if (row[0] + 1 >= nbd1) {
+                                row[0] = -1;
+                                return 0;
+                            }
+                            row[0] += 1;
+                            row[row[0]] = b2;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    return 1;
+}
+
+/* updates.update_nbor_list_few (updates.py:672-734) */
+static int nbor_list_few(int64_t start, const double *pos1, const int64_t *wib1, int64_t *nb,
+                         int64_t nbd1, int64_t n, const int64_t *chain_id, const double *pos2,
+                         const int64_t *wib2, int64_t n2, int64_t n_nearby, double L, int64_t ng,
+                         int64_t gw, int dim)
+{
+    double hgrid = (double)gw * L / (double)ng;
+    double max_dist_sq = hgrid * hgrid;
+    double half_L = L / 2.0;
+    double half_ng = (double)ng / 2.0;
+    for (int64_t b1 = 0; b1 < n; b1++) nb[b1 * nbd1] = 0;
+    for (int64_t b1 = 0; b1 < n; b1++) {
+        for (int64_t b2 = 0; b2 < n2; b2++) {
+            int use = 1;
+            for (int i = 0; i < dim; i++) {
+                double dg = (double)(wib2[b2 * 3 + i] - wib1[b1 * 3 + i]);
+                if (dg < -half_ng)
+                    dg += (double)ng;
+                else if (dg >= half_ng)
+                    dg -= (double)ng;
+                if (fabs(dg) > (double)gw) {
+                    use = 0;
+                    break;
+                }
+            }
+            if (!use) continue;
+            int64_t b1u = b1 + start;
+            if (chain_id[b1u] == chain_id[b2]) {
+                if (n_nearby < 0) continue;
+                int64_t d = b1u - b2;
+                if (d < 0) d = -d;
+                if (d <= n_nearby) continue;
+            }
+            double dist_sq = 0.0;
+            for (int i = 0; i < dim; i++) {
+                double sep = pos2[b2 * dim + i] - pos1[b1 * dim + i];
+                if (sep < -half_L)
+                    sep += L;
+                else if (sep >= half_L)
+                    sep -= L;
+                dist_sq += sep * sep;
+            }
+            if (dist_sq <= max_dist_sq) {
+                int64_t *row = nb + b1 * nbd1;
+                if (row[0] + 1 >= nbd1) {
+                    row[0] = -1;
+                    return 0;
+                }
+                row[0] += 1;
+                row[row[0]] = b2;
+            }
+        }
+    }
+    return 1;
+}
+
+/* populations.update_nbor_list_with_pop2 core (populations.py:156-180) for
+ * the whole population: one updates.update_nbor_list call.  Returns 1 on
+ * success; on overflow the caller doubles the depth and calls again. */
+GCRO_EXPORT int gcro_update_nbor_list(gcro_state *g, const double *pos, int64_t n, double L,
+                                      int64_t n_nearby, int64_t gw, int dim)
+{
+    return nbor_list_cells(0, pos, g->where_is_bead, g->nbor_list, g->nbor_depth1, n, g->chain_id, pos,
+                           g, n_nearby, L, gw, dim);
+}
+
+GCRO_EXPORT int gcro_update_nbor_list_few(gcro_state *g, const double *pos, int64_t n, double L,
+                                          int64_t n_nearby, int64_t gw, int dim)
+{
+    return nbor_list_few(0, pos, g->where_is_bead, g->nbor_list, g->nbor_depth1, n, g->chain_id, pos,
+                         g->where_is_bead, n, n_nearby, L, g->n_grid, gw, dim);
+}
+
+/* ------------------------------------------------------------------ */
+/* updates.chunk_chain (updates.py:323-344)                            */
+/* ------------------------------------------------------------------ */
+
+GCRO_EXPORT int gcro_chunk_chain(int64_t n_threads, int64_t total, const int64_t *chain_id,
+                                 int64_t *split /* [n_threads-1] */)
+{
+    int64_t chunklen = (total + n_threads - 1) / n_threads;
+    int64_t first = 0;
+    int64_t sii = 0;
+    while (first < total && sii < n_threads - 1) {
+        if (first > 0) {
+            split[sii] = first;
+            sii++;
+        }
+        int64_t test = (sii + 1) * chunklen - 1;
+        if (test < first) test = first;
+        if (test > total - 1) test = total - 1;
+        int64_t last_ci = chain_id[test];
+        while (test < total) {
+            if (chain_id[test] != last_ci) break;
+            test++;
+        }
+        first = test;
+    }
+    return (int)sii; /* entries of split that were set */
+}
+
+/* ------------------------------------------------------------------ */
+/* SRK.SRK_jit (SRK.py:13-484), SRK2, one population                   */
+/* ------------------------------------------------------------------ */
+
+static double draw_normal(gcro_state *st, int tid)
+{
+    return gcro_mt_normal(&st->mt[tid]);
+}
+
+GCRO_EXPORT int gcro_srk2_run(const gcro_params *p, gcro_state *st, gcro_result *out)
+{
+    const int dim = p->dim;
+    const int64_t N = p->n_beads;
+    const double L = p->L;
+    int T = p->n_threads > 0 ? p->n_threads : 1;
+    if (p->rigid_rod != 0.0 && p->longest_chain_length > 2) return -1;
+
+    /* chunk boundaries: chain-aligned (updates.py:192-199, 323-344) */
+    int64_t *bounds = (int64_t *)malloc(sizeof(int64_t) * (T + 1));
+    {
+        bounds[0] = 0;
+        if (T > 1) {
+            int64_t *split = (int64_t *)calloc((size_t)(T - 1), sizeof(int64_t));
+            gcro_chunk_chain(T, N, st->chain_id, split);
+            /* numpy.array_split with these indices (unset entries are the
+             * uninitialised tail of np.empty in the reference; here they
+             * are left at the array end) */
+            for (int t = 0; t < T - 1; t++) bounds[t + 1] = split[t] > 0 ? split[t] : N;
+            free(split);
+        }
+        bounds[T] = N;
+        for (int t = 1; t <= T; t++)
+            if (bounds[t] < bounds[t - 1]) bounds[t] = bounds[t - 1];
+    }
+    double (*shared)[6] = calloc((size_t)T, sizeof(double[6]));
+    for (int t = 0; t < T; t++) shared[t][0] = p->dt;
+
+    int64_t ng = st->n_grid;
+    double grid_spacing = L / (double)ng;
+    double nbor_length_scale = p->calc_wca ? p->wca[3] : 0.0;
+    int64_t grid_window = (int64_t)ceil(p->grid_factor * nbor_length_scale / grid_spacing);
+    if (grid_window < 1) grid_window = 1;
+    double pbc_width = (double)grid_window * L / (double)ng;
+    int64_t n_pow = 1;
+    for (int i = 0; i < dim; i++) n_pow *= ng;
+    int use_few = (N < n_pow);
+    int b_get_orientations = p->calc_springs ? (p->spring[4] != 0.0) : 0;
+    int64_t inject_step = 0;
+    int rc = 0;
+
+#pragma omp parallel num_threads(T)
+    {
+        int t = omp_get_thread_num();
+        int64_t s0 = bounds[t], s1 = bounds[t + 1], n = s1 - s0;
+        double *pos = st->pos + s0 * dim, *pos1 = st->pos1 + s0 * dim;
+        double *noise = st->noise + s0 * 2 * dim, *tan = st->tangent + s0 * dim;
+        double *F = st->forces + s0 * dim;
+        int64_t *nb = st->nbor_list + s0 * st->nbor_depth1;
+        int64_t *wib = st->where_is_bead + s0 * 3;
+        int64_t gchunk = (ng + T - 1) / T;
+        int64_t start_gx = t * gchunk;
+        int64_t end_gx = (t + 1) * gchunk < ng ? (t + 1) * gchunk : ng;
+        double dt = p->dt;
+        double dt_for_update = dt;
+        int64_t steps_until = p->steps_until_update;
+        shared[t][4] = 0;
+
+        while ((shared[t][2] < (double)p->max_steps || p->max_steps < 0) &&
+               (shared[t][1] < p->max_dt_usable || p->max_dt_usable < 0) && shared[t][5] >= 0) {
+            int64_t local_step = (int64_t)shared[t][2];
+            for (int64_t b = 0; b < n; b++) st->where_active[s0 + b] = -1;
+            /* noise: SRK.py:134-142 */
+            if (p->noise_mode == 0) {
+                if (p->D > 0)
+                    for (int64_t b = 0; b < n; b++)
+                        for (int i = 0; i < dim; i++) noise[b * 2 * dim + i] = draw_normal(st, t);
+                if (p->Dr > 0)
+                    for (int64_t b = 0; b < n; b++)
+                        for (int i = dim; i < 2 * dim; i++) noise[b * 2 * dim + i] = draw_normal(st, t);
+            } else if (p->noise_mode == 1) {
+                int64_t k = local_step < st->noise_inject_steps ? local_step : st->noise_inject_steps - 1;
+                const double *src = st->noise_inject + (k * N + s0) * 2 * dim;
+                for (int64_t b = 0; b < n * 2 * dim; b++) noise[b] = src[b];
+            } else {
+                for (int64_t b = 0; b < n; b++) {
+                    double z[4];
+                    double *row = noise + b * 2 * dim;
+                    int64_t gs = p->step0 + local_step;
+                    if (p->D > 0) {
+                        gcro_philox_pair(p->seed, (uint32_t)(s0 + b), gs, 0u, z);
+                        if (dim == 3) gcro_philox_pair(p->seed, (uint32_t)(s0 + b), gs, 1u, z + 2);
+                        for (int i = 0; i < dim; i++) row[i] = z[i];
+                    }
+                    if (p->Dr > 0) {
+                        gcro_philox_pair(p->seed, (uint32_t)(s0 + b), gs, 2u, z);
+                        if (dim == 3) gcro_philox_pair(p->seed, (uint32_t)(s0 + b), gs, 3u, z + 2);
+                        for (int i = 0; i < dim; i++) row[dim + i] = z[i];
+                    }
+                }
+            }
+            for (int64_t b = 0; b < n * dim; b++) F[b] = 0.0;
+            shared[t][5] = 0;
+
+            for (int stage = 0; stage < 2; stage++) {
+                double *X = stage == 0 ? pos : pos1;
+                double *Xfull = stage == 0 ? st->pos : st->pos1;
+                double *W = stage == 0 ? pos1 : pos;
+                double pref = stage == 0 ? 1.0 : 0.5;
+#pragma omp barrier
+                if (p->calc_springs)
+                    spring_forces(X, tan, st->chain_id + s0, F, n, L, p->spring, st->rest_lengths, dim);
+#pragma omp barrier
+                if (p->calc_wca)
+                    pair_forces(s0, X, nb, st->nbor_depth1, F, n, L, Xfull, p->wca, pbc_width, dim);
+                if (p->self_propel) self_propel(F, tan, n, p->active, dim);
+                if (stage == 1) {
+                    shared[t][3] = sqrt(2.0 * p->D);
+                    if (n > 0) {
+                        double m = -1.0;
+                        for (int64_t b = 0; b < n; b++) {
+                            double s = 0.0;
+                            for (int i = 0; i < dim; i++) s += F[b * dim + i] * F[b * dim + i];
+                            if (s > m) m = s;
+                        }
+                        shared[t][3] += pref * sqrt(m) / p->radius;
+                    }
+                    shared[t][2] += 1;
+                }
+#pragma omp barrier
+                if (stage == 1) {
+                    double mfs = shared[0][3];
+                    for (int u = 1; u < T; u++)
+                        if (shared[u][3] > mfs) mfs = shared[u][3];
+                    if (mfs == 0.0)
+                        dt = p->dtmax;
+                    else {
+                        double c = p->max_dist_per_step / mfs;
+                        dt = p->dtmax < c ? p->dtmax : c;
+                    }
+                    double dt_used = p->rk_cheat * dt;
+                    if (p->max_dt_usable > 0) {
+                        double lim = p->max_dt_usable - shared[t][1];
+                        if (lim < dt_used) dt_used = lim;
+                    }
+                    shared[t][0] = dt;
+                    shared[t][1] += dt_used;
+                    dt_for_update = dt_used;
+                } else {
+                    dt_for_update = dt;
+                }
+                double dt_eff = dt_for_update * pref;
+                double s2 = sqrt(2.0 * dt_for_update * p->D);
+                if (n > 0) {
+                    dt_eff /= p->radius;
+                    for (int64_t b = 0; b < n; b++)
+                        for (int i = 0; i < dim; i++) {
+                            double tmp = pos[b * dim + i] + dt_eff * F[b * dim + i];
+                            if (s2 != 0.0) tmp += s2 * noise[b * 2 * dim + i];
+                            W[b * dim + i] = py_mod(tmp, L);
+                        }
+                }
+            }
+            /* rotational diffusion: SRK.py:399-423 */
+            if (p->Dr > 0 && !b_get_orientations) {
+                double sq = sqrt(2.0 * dt_for_update * p->Dr) * 3.141592653589793;
+                for (int64_t b = 0; b < n; b++) {
+                    double *xr = noise + b * 2 * dim + dim;
+                    double *tb = tan + b * dim;
+                    double proj = 0.0;
+                    for (int i = 0; i < dim; i++) proj += xr[i] * tb[i];
+                    for (int i = 0; i < dim; i++) xr[i] -= proj * tb[i];
+                    double mag = 0.0;
+                    for (int i = 0; i < dim; i++) {
+                        double v = tb[i] + sq * xr[i];
+                        mag += v * v;
+                        tb[i] = v;
+                    }
+                    mag = sqrt(mag);
+                    for (int i = 0; i < dim; i++) tb[i] /= mag;
+                }
+            }
+            /* periodic rebuild: SRK.py:428-484 */
+            if (shared[t][2] >= (double)steps_until) {
+                for (int64_t b = 0; b < n; b++)
+                    for (int i = 0; i < dim; i++)
+                        wib[b * 3 + i] = (int64_t)py_floordiv(pos[b * dim + i], grid_spacing);
+#pragma omp barrier
+                for (int ii = 0; ii < 2; ii++) {
+                    int success = 1;
+                    if (ii == 0) {
+                        success = grid_list_mini(st, N, start_gx, end_gx);
+                    } else if (n > 0) {
+                        if (use_few)
+                            success = nbor_list_few(s0, pos, wib, nb, st->nbor_depth1, n, st->chain_id,
+                                                    st->pos, st->where_is_bead, N, p->n_nearby, L, ng,
+                                                    grid_window, dim);
+                        else
+                            success = nbor_list_cells(s0, pos, wib, nb, st->nbor_depth1, n, st->chain_id,
+                                                      st->pos, st, p->n_nearby, L, grid_window, dim);
+                    }
+                    if (!success) shared[t][5] = -ii;
+#pragma omp barrier
+                    for (int u = 0; u < T; u++)
+                        if (shared[u][5] < 0) shared[t][5] = shared[u][5];
+#pragma omp barrier
+                }
+                steps_until += p->n_steps_update;
+            }
+            (void)inject_step;
+        }
+    }
+    out->dt = shared[0][0];
+    out->dt_used_total = shared[0][1];
+    out->steps = shared[0][2];
+    out->max_forces_strength = shared[0][3];
+    out->counter = shared[0][4];
+    out->flag = shared[0][5];
+    free(shared);
+    free(bounds);
+    return rc;
+}
+
+/* ------------------------------------------------------------------ */
+/* Observables                                                         */
+/* ------------------------------------------------------------------ */
+
+/* output_methods.calc_avg_phi_chain (492-510) + analysis.polar_orderparameter
+ * (315-328) + analysis.nematic_orderparameter (294-313).  Chains are given
+ * as contiguous bead ranges [chain_start[c], chain_start[c+1]).
+ * out = [P, S, director_angle]. */
+GCRO_EXPORT void gcro_order_params(const double *tangent, const int64_t *chain_start, int64_t n_chains,
+                                   int dim, double *out)
+{
+    double ex_sum = 0.0, ey_sum = 0.0, q11 = 0.0, q12 = 0.0;
+    for (int64_t c = 0; c < n_chains; c++) {
+        double sx = 0.0, sy = 0.0;
+        for (int64_t b = chain_start[c]; b < chain_start[c + 1]; b++) {
+            sx += tangent[b * dim];
+            sy += tangent[b * dim + 1];
+        }
+        double phi = atan2(sy, sx);
+        double ex = cos(phi), ey = sin(phi);
+        ex_sum += ex;
+        ey_sum += ey;
+        q11 += 2.0 * ex * ex - 1.0;
+        q12 += 2.0 * ex * ey;
+    }
+    double P = sqrt(ex_sum * ex_sum + ey_sum * ey_sum) / (double)n_chains;
+    double Sfull = sqrt(q11 * q11 + q12 * q12);
+    double ang = atan((Sfull - q11) / q12);
+    out[0] = P;
+    out[1] = Sfull / (double)n_chains;
+    out[2] = ang;
+}
+
+GCRO_EXPORT int gcro_sizeof_params(void) { return (int)sizeof(gcro_params); }
+GCRO_EXPORT int gcro_sizeof_state(void) { return (int)sizeof(gcro_state); }
+GCRO_EXPORT int gcro_sizeof_mt(void) { return (int)sizeof(gcro_mt); }
