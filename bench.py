@@ -1,0 +1,431 @@
+#!/usr/bin/env python3
+"""Benchmark of the gliding-collective-rotation SRK2 step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gcr|reference]
+                    [--workload sweep|large|config1|config5] [--precision mixed|fp64]
+
+Default workload: the batched sweep -- 256 independent 2D systems (chains of
+5-40 beads, 50-4000 chains per system, area fraction 0.1-0.4, chirality and
+bending drawn per system, FP32 forces / FP64 positions, Philox seeds 0..255),
+advanced together by one captured graph of persistent kernels.  One step is
+one SRK2 step of every system.  Metric: bead-steps/s (beads x SRK2 steps per
+second, one bead-step = two force evaluations).
+
+Printed as one JSON line by rank 0.  Under torchrun every rank runs its own
+256 systems (weak scaling, no collective in the data path); the timed region
+is bracketed by barriers and its length is the max over ranks.
+
+``--impl reference`` times the reference's algorithm on the host cores: the
+CPU restatement of the reference's Numba step (oracle/), all host threads,
+chain-aligned chunks, Verlet lists rebuilt every 40 steps, on a bounded
+sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        d["source"] = "measured"
+        return d
+    return dict(PEAKS_FALLBACK)
+
+
+# --------------------------------------------------------------------------
+# workloads
+# --------------------------------------------------------------------------
+
+def make_workload(name, rank=0, scale=1.0):
+    from gliding_collective_rotation_b200 import workloads as W
+    if name == "sweep":
+        specs = W.config3(n_systems=256, param_seed=12345 + rank)
+        desc = ("batched sweep: 256 independent 2D systems, 50-4000 chains of 5-40 beads, area fraction "
+                "0.1-0.4, chirality -0.5..0.5, bending 1..50, WCA r_c=1, T=0.01, dt=1e-3, SRK2")
+    elif name == "large":
+        specs = [W.config2(seed=rank, scale=scale)]
+        desc = "large single system: 2D L=1000, 20,000 chains x 25 beads, LJ r_c=2.5 sigma eps 0.5, chiral 0.2, SRK2"
+    elif name == "config1":
+        specs = [W.config1(seed=rank)]
+        desc = "small single system: 2D L=60, 200 chains x 10 beads, WCA, SRK2"
+    elif name == "config5":
+        specs = [W.config5(seed=rank, scale=scale)]
+        desc = "3D precision stress: L=200, 40,000 chains x 25 beads, LJ eps 1, Dr 0.1, SRK2"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    return specs, desc
+
+
+# --------------------------------------------------------------------------
+# algorithmic bytes per kernel launch (HBM roofline)
+# --------------------------------------------------------------------------
+
+def algorithmic_bytes(dim, precision, n_beads, n_cells, get_orient, rot_diff):
+    """Minimum DRAM bytes of one launch of each step kernel: every input read
+    once and every output written once (neighbour records counted once)."""
+    P = 8                                   # FP64 position component
+    F = 8 if precision == "fp64" else 4     # force / tangent component
+    R = 32 if precision == "fp64" else 16   # packed record per bead
+    tan = dim * F if get_orient else 0
+    pack = n_beads * (dim * P + R + 4) + n_cells * 8
+    stage0 = n_beads * (dim * P + R + 5 + dim * F + dim * P + tan + 8)
+    stage1 = n_beads * (dim * P + R + 5 + dim * F + dim * F + tan)
+    update = n_beads * (dim * P + dim * F + dim * P + 8 + (2 * dim * F if rot_diff else 0))
+    return {"pack_pos": pack, "stage0": stage0, "pack_pos1": pack, "stage1": stage1, "update": update}
+
+
+KERNELS = ["pack_pos", "stage0", "pack_pos1", "stage1", "update"]
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index=0):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as fh:
+            for line in fh:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# --------------------------------------------------------------------------
+# CPU arm: the reference's algorithm (oracle) on a bounded sample
+# --------------------------------------------------------------------------
+
+def cpu_sample_rate(specs, states_host, steps, threads, max_systems=4, budget_s=20.0):
+    """bead-steps/s of the oracle (the reference's Numba step restated in C,
+    OpenMP threads over chain-aligned chunks) on the first systems of the
+    workload, each run for `steps` steps after an untimed list build."""
+    from oracle import oracle as O
+    total_bs, total_t, used = 0, 0.0, []
+    for spec, (pos, tan) in list(zip(specs, states_host))[:max_systems]:
+        p = spec.params
+        ng = max(1, int(p.L / (2.0 * max(2 * spec.rest_lengths.max(), p.wca_params[3]))))
+        sysm = O.OracleSystem(pos, tan, spec.chain_id, spec.rest_lengths, p.L, p.spring_params, p.wca_params,
+                              p.active_params, p.D, p.Dr, p.radius, p.n_nearby, ng, nbor_depth=32)
+        sysm.build_lists(grid_window=1)
+        sysm.seed_mt(int(p.seed), threads)
+        t0 = time.perf_counter()
+        res = sysm.run(steps, dt=spec.dt, n_threads=threads)
+        dt = time.perf_counter() - t0
+        total_bs += spec.n * res["steps"]
+        total_t += dt
+        used.append(f"{spec.name}({spec.n} beads)")
+        if total_t > budget_s:
+            break
+    return total_bs / total_t, used, total_t
+
+
+def relax_on_cpu(spec, max_steps=600):
+    """Untimed adaptive-dt warm-up with the oracle (the reference's own
+    adaptive step), used by the reference arm."""
+    from oracle import oracle as O
+    p = spec.params
+    ng = max(1, int(p.L / (2.0 * max(2 * spec.rest_lengths.max(), p.wca_params[3]))))
+    sysm = O.OracleSystem(spec.pos, spec.tangent, spec.chain_id, spec.rest_lengths, p.L, p.spring_params,
+                          p.wca_params, p.active_params, p.D, p.Dr, p.radius, p.n_nearby, ng, nbor_depth=32)
+    sysm.build_lists(grid_window=1)
+    sysm.seed_mt(7, os.cpu_count() or 1)
+    done = 0
+    dt = spec.dt * 1e-4
+    while done < max_steps:
+        res = sysm.run(100, dt=dt, dtmax=spec.dt, max_dist_per_step=spec.relax_mdps, n_threads=os.cpu_count() or 1)
+        done += res["steps"]
+        dt = res["dt"]
+        if res["flag"] < 0:
+            sysm.build_lists(grid_window=1)
+        if dt >= spec.dt * (1 - 1e-12):
+            break
+    return sysm.pos.copy(), sysm.tangent_list.copy()
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    specs, desc = make_workload(args.workload)
+    threads = os.cpu_count() or 1
+    # a bounded sample: the first systems, relaxed untimed with the reference's adaptive dt
+    sample = specs[:args.cpu_systems]
+    states = [relax_on_cpu(s) for s in sample]
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_sample_rate(sample, states, 2, threads, max_systems=1)
+    rates = []
+    for _ in range(args.steps):
+        r, used, secs = cpu_sample_rate(sample, states, args.cpu_steps, threads, max_systems=len(sample),
+                                        budget_s=args.cpu_budget / max(args.steps, 1))
+        rates.append(r)
+    value = float(np.median(rates))
+    line = {
+        "impl": "reference", "metric": "bead-steps/s", "value": value, "unit": "bead-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "sample": ", ".join(used)},
+        "cpu_baseline": {"value": value, "unit": "bead-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"{len(used)} systems x {args.cpu_steps} steps per timed step: {', '.join(used)}"},
+        "e2e": {"value": value, "unit": "bead-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+    from gliding_collective_rotation_b200.batch import Batch, PlainRunner
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+
+    specs, desc = make_workload(args.workload, rank=rank, scale=args.scale)
+    batch = Batch(specs, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph)
+    eng = batch.engine
+    n_beads = batch.n_beads
+    relax_steps = batch.relax(max_steps=args.relax_steps)
+    # warm-up at the fixed dt
+    batch.begin(args.warmup)
+    batch.run(args.warmup)
+    eng.synchronize()
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-timed batched steps -------------------------------------
+    batch.begin(args.steps)
+    clocks = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(eng.stream)
+    batch.run(args.steps)
+    ev1.record(eng.stream)
+    ev1.synchronize()
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    st = batch.statuses()
+    steps_done = min(s["steps_done"] for s in st)
+    flags = sorted({s["flags"] for s in st})
+    value = world * n_beads * args.steps / (ms / 1e3)
+
+    # ---- per-kernel profile (roofline) ----------------------------------
+    batch.begin(args.profile_steps)
+    kms = eng.profile_steps(args.profile_steps) / args.profile_steps
+    cfg = eng.cfg
+    from gliding_collective_rotation_b200.engine import footprint
+    n_cells = sum(footprint(cfg, s.params, s.n, len(s.rest_lengths))[0] for s in specs)
+    get_orient = bool(specs[0].params.spring_params[4])
+    rot_diff = (not get_orient) and specs[0].params.Dr > 0
+    alg = algorithmic_bytes(batch.dim, args.precision, n_beads, n_cells, get_orient, rot_diff)
+    dom = int(np.argmax(kms))
+    pk = peaks()
+    achieved = alg[KERNELS[dom]] / (kms[dom] / 1e3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        with open(tpath) as fh:
+            tr = json.load(fh).get(args.workload, {}).get(args.precision, {})
+        if KERNELS[dom] in tr:
+            traffic = tr[KERNELS[dom]] * n_beads
+    roofline = {"bound": "hbm", "kernel": KERNELS[dom], "achieved": achieved, "peak": pk["hbm_gbs"],
+                "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
+                "algorithmic_bytes": alg[KERNELS[dom]], "peak_source": pk["source"],
+                "kernel_ms": {k: float(v) for k, v in zip(KERNELS, kms)},
+                "step_alg_bytes_per_bead": sum(alg.values()) / n_beads,
+                "step_frac": (sum(alg.values()) / (kms.sum() / 1e3) / 1e9) / pk["hbm_gbs"]}
+
+    # ---- plain path: one system per launch sequence ---------------------
+    plain = None
+    if args.plain and len(specs) > 1:
+        pr = PlainRunner(specs, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph)
+        pr.copy_state_from(batch)
+        pr.begin(args.plain_steps)
+        pr.run(min(args.plain_steps, 10))
+        pr.synchronize()
+        pr.begin(args.plain_steps)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(pr.stream)
+        pr.run(args.plain_steps)
+        e1.record(pr.stream)
+        e1.synchronize()
+        pms = e0.elapsed_time(e1)
+        plain = {"value": pr.n_beads * args.plain_steps / (pms / 1e3), "unit": "bead-steps/s",
+                 "steps": args.plain_steps, "ms_per_step": pms / args.plain_steps}
+        pr.close()
+
+    # ---- end to end through the public API with host buffers ------------
+    big = batch.big
+    h_pos = torch.empty(big["pos"].shape, dtype=big["pos"].dtype, pin_memory=True)
+    h_tan = torch.empty(big["tangent"].shape, dtype=big["tangent"].dtype, pin_memory=True)
+    h_pos.copy_(big["pos"])
+    h_tan.copy_(big["tangent"])
+    torch.cuda.synchronize()
+    spc = args.e2e_steps_per_call
+    n_calls = max(1, args.steps // spc)
+    e2e_bytes_in = h_pos.numel() * h_pos.element_size() + h_tan.numel() * h_tan.element_size()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n_calls):
+        big["pos"].copy_(h_pos, non_blocking=True)
+        big["tangent"].copy_(h_tan, non_blocking=True)
+        batch.begin(spc)
+        batch.run(spc)
+        eng.synchronize()
+        h_pos.copy_(big["pos"], non_blocking=True)
+        h_tan.copy_(big["tangent"], non_blocking=True)
+        torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    if world > 1:
+        t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * n_beads * spc * n_calls / e2e_s, "unit": "bead-steps/s",
+           "h2d_bytes_per_step": e2e_bytes_in / spc, "d2h_bytes_per_step": e2e_bytes_in / spc,
+           "steps_per_call": spc, "calls": n_calls,
+           "api": "Batch.begin/run (gcr_call_begin_batch, gcr_run) with pinned host buffers"}
+
+    # ---- CPU baseline (rank 0, N = 1) ------------------------------------
+    cpu = None
+    if world == 1 and args.cpu_baseline:
+        host_states = [(s.pos.cpu().numpy(), s.tangent.double().cpu().numpy()) for s in batch.states]
+        threads = os.cpu_count() or 1
+        r, used, secs = cpu_sample_rate(specs, host_states, args.cpu_steps, threads, max_systems=args.cpu_systems,
+                                        budget_s=args.cpu_budget)
+        cpu = {"value": r, "unit": "bead-steps/s", "cores": threads, "kind": "port",
+               "sample": f"{args.cpu_steps} steps of {', '.join(used)} ({secs:.1f} s)"}
+
+    working_set = sum(v.numel() * v.element_size() for v in big.values()) + eng.cfg.cell_capacity * (
+        8 + eng.cfg.cell_depth * (4 + (32 if args.precision == "fp64" else 16)))
+    line = {
+        "metric": "bead-steps/s", "value": value, "unit": "bead-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": desc, "systems_per_gpu": len(specs), "beads_per_gpu": n_beads,
+                   "precision": ("FP32 forces and SRK arithmetic, FP64 positions" if args.precision == "mixed"
+                                 else "FP64"),
+                   "parallelism": f"{world} GPU(s), independent systems per GPU",
+                   "l2": f"inputs larger than L2: working set {working_set / 1e6:.0f} MB per GPU > 126 MB",
+                   "relax_steps": relax_steps, "steps_done": steps_done, "flags": flags,
+                   "steps_per_graph": args.steps_per_graph},
+        "e2e": e2e, "roofline": roofline, "clocks": clk,
+        "gpu_launches": 5 * args.steps + 1,
+    }
+    if plain is not None:
+        line["plain"] = plain
+        line["batched_over_plain"] = value / world / plain["value"]
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="gcr", choices=["gcr", "reference"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "large", "config1", "config5"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--steps-per-graph", type=int, default=10)
+    ap.add_argument("--relax-steps", type=int, default=2000)
+    ap.add_argument("--profile-steps", type=int, default=10)
+    ap.add_argument("--plain", type=int, default=1)
+    ap.add_argument("--plain-steps", type=int, default=50)
+    ap.add_argument("--e2e-steps-per-call", type=int, default=100)
+    ap.add_argument("--cpu-baseline", type=int, default=1)
+    ap.add_argument("--cpu-steps", type=int, default=20)
+    ap.add_argument("--cpu-systems", type=int, default=4)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,157 @@
+"""Many independent systems of different sizes advanced together.
+
+All systems of a ``Batch`` share one ``Engine`` (one ``libgcr`` context), so
+one captured CUDA graph of persistent kernels steps every system: the
+kernels walk a per-system tile table in device memory, each system keeps its
+own parameters, adaptive dt, step counter and Philox seed.  The bead state of
+all systems lives in a few large device tensors (per-system views), so the
+host <-> device copies of a call are single bulk transfers.
+
+The plain path (``PlainRunner``) advances the same systems one system per
+launch sequence, as the drop-in does; it is the baseline the batched path is
+measured against.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from .engine import Engine, SystemState, footprint, default_config
+
+
+def _views(specs, precision, device):
+    ft = torch.float64 if precision == "fp64" else torch.float32
+    dim = specs[0].dim
+    n_tot = sum(s.n for s in specs)
+    c_tot = sum(len(s.rest_lengths) for s in specs)
+    big = {
+        "pos": torch.empty((n_tot, dim), dtype=torch.float64, device=device),
+        "pos1": torch.zeros((n_tot, dim), dtype=torch.float64, device=device),
+        "tangent": torch.empty((n_tot, dim), dtype=ft, device=device),
+        "forces": torch.zeros((n_tot, dim), dtype=ft, device=device),
+        "chain_id": torch.empty(n_tot, dtype=torch.int32, device=device),
+        "rest": torch.empty(c_tot, dtype=torch.float64, device=device),
+    }
+    h_pos = np.concatenate([s.pos for s in specs])
+    h_tan = np.concatenate([s.tangent for s in specs])
+    h_chain = np.concatenate([s.chain_id for s in specs]).astype(np.int32)
+    h_rest = np.concatenate([s.rest_lengths for s in specs])
+    big["pos"].copy_(torch.from_numpy(h_pos))
+    big["tangent"].copy_(torch.from_numpy(h_tan))
+    big["chain_id"].copy_(torch.from_numpy(h_chain))
+    big["rest"].copy_(torch.from_numpy(h_rest))
+    states, bo, co = [], 0, 0
+    for s in specs:
+        n, nc = s.n, len(s.rest_lengths)
+        states.append(SystemState(pos=big["pos"][bo:bo + n], pos1=big["pos1"][bo:bo + n],
+                                  tangent=big["tangent"][bo:bo + n], forces=big["forces"][bo:bo + n],
+                                  chain_id=big["chain_id"][bo:bo + n], rest_lengths=big["rest"][co:co + nc],
+                                  params=s.params))
+        bo += n
+        co += nc
+    return big, states
+
+
+class Batch:
+    """Systems of one dimension and precision resident in one context."""
+
+    def __init__(self, specs, precision="mixed", device=None, steps_per_graph=10, cell_depth=None,
+                 block_beads=256, block_cells=256, stream=None):
+        if not specs:
+            raise ValueError("empty batch")
+        dims = {s.dim for s in specs}
+        if len(dims) != 1:
+            raise ValueError("a batch holds systems of one dimension")
+        self.dim = dims.pop()
+        self.specs = specs
+        self.precision = precision
+        self.device = torch.device(device or "cuda")
+        cfg = default_config(self.dim, precision, cell_depth=cell_depth)
+        cells = sum(footprint(cfg, s.params, s.n, len(s.rest_lengths))[0] for s in specs)
+        self.n_beads = sum(s.n for s in specs)
+        self.engine = Engine(self.dim, precision, device=self.device, bead_capacity=self.n_beads,
+                             system_capacity=len(specs), cell_capacity=max(cells, 1), cell_depth=cell_depth,
+                             block_beads=block_beads, block_cells=block_cells, steps_per_graph=steps_per_graph,
+                             stream=stream)
+        self.big, self.states = _views(specs, precision, self.device)
+        torch.cuda.synchronize(self.device)
+        for st in self.states:
+            self.engine.admit(st)
+
+    # -- calls -------------------------------------------------------------------
+    def begin(self, max_steps, dt=None, max_dist_per_step=None, max_dt_usable=-1.0):
+        """Arm every system for the next run (one SRK2_force_calc call each)."""
+        for st in self.states:
+            if max_dist_per_step is not None and st.params.max_dist_per_step != max_dist_per_step:
+                st.params.max_dist_per_step = max_dist_per_step
+                self.engine.update_params(st)
+        dts = [spec.dt if dt is None else dt for spec in self.specs]
+        self.engine.call_begin_many([st.slot for st in self.states], max_steps, dts, max_dt_usable)
+
+    def run(self, max_steps, sync_every=0):
+        self.engine.run(max_steps, sync_every)
+
+    def relax(self, max_steps=2000, chunk=200):
+        """Untimed warm-up under the reference's adaptive dt (dtmax = the
+        system's dt, max_dist_per_step from grid_list_setup) until every
+        system takes full steps; removes the overlaps of random placement."""
+        done = 0
+        while done < max_steps:
+            for st, spec in zip(self.states, self.specs):
+                if st.params.max_dist_per_step != spec.relax_mdps:
+                    st.params.max_dist_per_step = spec.relax_mdps
+                    self.engine.update_params(st)
+            self.engine.call_begin_many([st.slot for st in self.states], chunk, [s.dt for s in self.specs])
+            self.engine.run(chunk)
+            done += chunk
+            dts = [self.engine.status(st.slot)["dt"] for st in self.states]
+            if all(d >= spec.dt * (1 - 1e-12) for d, spec in zip(dts, self.specs)):
+                break
+        for st in self.states:
+            st.params.max_dist_per_step = math.inf
+            self.engine.update_params(st)
+        return done
+
+    def statuses(self):
+        return [self.engine.status(st.slot) for st in self.states]
+
+    def order_params(self):
+        return np.array([self.engine.order_params(st.slot) for st in self.states])
+
+    def close(self):
+        self.engine.close()
+
+
+class PlainRunner:
+    """The same systems, one context and one launch sequence per system."""
+
+    def __init__(self, specs, precision="mixed", device=None, steps_per_graph=10, cell_depth=None):
+        # one stream for every context: launches of different systems do not overlap
+        self.stream = torch.cuda.Stream(device=device)
+        self.batches = [Batch([s], precision, device, steps_per_graph, cell_depth, stream=self.stream)
+                        for s in specs]
+        self.n_beads = sum(s.n for s in specs)
+
+    def copy_state_from(self, batch):
+        for b, st in zip(self.batches, batch.states):
+            b.states[0].pos.copy_(st.pos)
+            b.states[0].tangent.copy_(st.tangent)
+        torch.cuda.synchronize()
+
+    def begin(self, max_steps):
+        for b in self.batches:
+            b.begin(max_steps)
+
+    def run(self, max_steps):
+        for b in self.batches:
+            b.run(max_steps)
+
+    def synchronize(self):
+        for b in self.batches:
+            b.engine.synchronize()
+
+    def close(self):
+        for b in self.batches:
+            b.close()

@@ -1,0 +1,766 @@
+// gcr_abi.cu -- the C ABI of libgcr.so (declared in include/gcr.h).
+//
+// A context owns the scratch of many resident systems and one CUDA graph of
+// `steps_per_graph` SRK2 steps.  The graph's kernels are persistent and read
+// the system descriptors and tile tables from device memory, so admitting or
+// evicting a system (continuous batching) never re-captures the graph.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/gcr.h"
+#include "gcr_device.cuh"
+#include "gcr_kernels.h"
+
+using namespace gcr;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+#define GCR_CUDA(call)                                                                             \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            return fail(e_ == cudaErrorMemoryAllocation ? GCR_ERR_OOM : GCR_ERR_CUDA,              \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                       \
+    } while (0)
+
+// first-fit allocator of integer ranges [0, capacity)
+struct RangeAlloc {
+    int64_t capacity = 0;
+    std::map<int64_t, int64_t> free_;  // offset -> length
+    void init(int64_t cap)
+    {
+        capacity = cap;
+        free_.clear();
+        if (cap > 0) free_[0] = cap;
+    }
+    int64_t alloc(int64_t n)
+    {
+        if (n <= 0) return 0;
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= n) {
+                int64_t off = it->first, len = it->second;
+                free_.erase(it);
+                if (len > n) free_[off + n] = len - n;
+                return off;
+            }
+        }
+        return -1;
+    }
+    void release(int64_t off, int64_t n)
+    {
+        if (n <= 0) return;
+        auto it = free_.emplace(off, n).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+};
+
+struct Slot {
+    bool used = false;
+    gcr_system_desc desc{};
+    gcr_system_buffers buf{};
+    int64_t bead_off = 0, cell_off = 0, chain_off = 0;
+    int64_t n_cells = 0;
+};
+
+int ilog2(int v)
+{
+    int l = 0;
+    while ((1 << l) < v) l++;
+    return l;
+}
+
+}  // namespace
+
+struct gcr_ctx {
+    gcr_config cfg{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    int sm_count = 0;
+    KernelSet ks{};
+    // device arrays
+    SysP *dP = nullptr;
+    SysS *dS = nullptr;
+    Tile *d_bead_tiles = nullptr;
+    Tile *d_cell_tiles = nullptr;
+    int *d_ntiles = nullptr;  // [0] bead tiles, [1] cell tiles
+    uint8_t *topo = nullptr;
+    int *cnt0 = nullptr;
+    int *cnt1 = nullptr;
+    int *items = nullptr;
+    void *rec = nullptr;
+    int32_t *chain_starts = nullptr;
+    int *d_err = nullptr;
+    double *d_out = nullptr;
+    size_t rec_bytes = 0;
+    int64_t max_bead_tiles = 0, max_cell_tiles = 0;
+    // host mirrors
+    std::vector<Slot> slots;
+    std::vector<SysP> hP;
+    std::vector<SysS> hS;
+    std::vector<Tile> h_bead_tiles, h_cell_tiles;
+    RangeAlloc beads, cells, chains;
+    BatchArgs args{};
+    int grid_beads = 1, grid_cells = 1;
+    cudaGraphExec_t graph = nullptr;
+    bool tiles_dirty = true;
+};
+
+namespace {
+
+int kernel_grid(const gcr_ctx *c, void *fn, int block, int64_t max_tiles)
+{
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, 0) != cudaSuccess || occ < 1) occ = 1;
+    if (c->cfg.ctas_per_sm > 0) occ = std::min(occ, c->cfg.ctas_per_sm);
+    int64_t g = (int64_t)c->sm_count * occ;
+    g = std::min<int64_t>(g, std::max<int64_t>(max_tiles, 1));
+    return (int)std::max<int64_t>(g, 1);
+}
+
+int rebuild_tiles(gcr_ctx *c)
+{
+    c->h_bead_tiles.clear();
+    c->h_cell_tiles.clear();
+    const int tb = c->cfg.block_beads, tcl = c->cfg.block_cells;
+    for (int s = 0; s < (int)c->slots.size(); s++) {
+        const Slot &sl = c->slots[s];
+        if (!sl.used) continue;
+        for (int64_t b = 0; b < sl.desc.n_beads; b += tb) c->h_bead_tiles.push_back(Tile{s, (int32_t)b});
+        if (sl.desc.calc_wca)
+            for (int64_t q = 0; q < sl.n_cells; q += tcl) c->h_cell_tiles.push_back(Tile{s, (int32_t)q});
+    }
+    if ((int64_t)c->h_bead_tiles.size() > c->max_bead_tiles || (int64_t)c->h_cell_tiles.size() > c->max_cell_tiles)
+        return fail(GCR_ERR_CAPACITY, "tile table capacity exceeded");
+    int nt[2] = {(int)c->h_bead_tiles.size(), (int)c->h_cell_tiles.size()};
+    if (nt[0]) GCR_CUDA(cudaMemcpyAsync(c->d_bead_tiles, c->h_bead_tiles.data(), nt[0] * sizeof(Tile),
+                                        cudaMemcpyHostToDevice, c->stream));
+    if (nt[1]) GCR_CUDA(cudaMemcpyAsync(c->d_cell_tiles, c->h_cell_tiles.data(), nt[1] * sizeof(Tile),
+                                        cudaMemcpyHostToDevice, c->stream));
+    GCR_CUDA(cudaMemcpyAsync(c->d_ntiles, nt, sizeof(nt), cudaMemcpyHostToDevice, c->stream));
+    // the host arrays must outlive the asynchronous copies
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    c->tiles_dirty = false;
+    return GCR_OK;
+}
+
+int validate_desc(const gcr_config &cfg, const gcr_system_desc *d, int64_t *nc_out)
+{
+    if (!d) return fail(GCR_ERR_BAD_ARG, "null descriptor");
+    if (d->n_beads <= 0 || d->n_beads > (int64_t)INT32_MAX / 2) return fail(GCR_ERR_BAD_ARG, "n_beads out of range");
+    if (d->n_chains <= 0 || d->n_chains > d->n_beads) return fail(GCR_ERR_BAD_ARG, "n_chains out of range");
+    if (!(d->L > 0.0) || !std::isfinite(d->L)) return fail(GCR_ERR_BAD_ARG, "box side L must be positive");
+    if (!(d->radius > 0.0)) return fail(GCR_ERR_BAD_ARG, "radius must be positive");
+    if (d->spring_params[3] != 0.0) return fail(GCR_ERR_BAD_ARG, "FENE springs are not supported");
+    if (d->active_params[1] > 0.0) return fail(GCR_ERR_BAD_ARG, "active sliding is not supported");
+    int64_t nc = 1;
+    if (d->calc_wca) {
+        double rc = d->wca_params[3];
+        double cf = d->cell_factor >= 1.0 ? d->cell_factor : 1.0;
+        if (!(rc > 0.0)) return fail(GCR_ERR_BAD_ARG, "pair cutoff must be positive");
+        nc = (int64_t)std::floor(d->L / (rc * cf));
+        if (nc < 3)
+            return fail(GCR_ERR_BAD_ARG, "box side must be at least 3 pair cutoffs for the GPU cell grid");
+        // h = L/nc must not fall below the cutoff through rounding
+        while (nc > 3 && d->L / (double)nc < rc) nc--;
+        int64_t cells = 1;
+        for (int i = 0; i < cfg.dim; i++) cells *= nc;
+        if (cells > (int64_t)INT32_MAX / 2) return fail(GCR_ERR_BAD_ARG, "too many GPU cells");
+    }
+    *nc_out = nc;
+    return GCR_OK;
+}
+
+void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, SysP &p)
+{
+    const gcr_system_desc &d = sl.desc;
+    std::memset(&p, 0, sizeof(p));
+    p.pos = sl.buf.pos;
+    p.pos1 = sl.buf.pos1;
+    p.tan = sl.buf.tangent;
+    p.frc = sl.buf.forces;
+    p.chain = sl.buf.chain_id;
+    p.rest = sl.buf.rest_lengths;
+    p.bead_off = sl.bead_off;
+    p.cell_off = sl.cell_off;
+    p.n = (int32_t)d.n_beads;
+    p.n_chains = (int32_t)d.n_chains;
+    p.nc = (int32_t)nc;
+    p.n_cells = (int32_t)sl.n_cells;
+    p.n_bead_tiles = (int32_t)((d.n_beads + c->cfg.block_beads - 1) / c->cfg.block_beads);
+    p.n_cell_tiles = (int32_t)((sl.n_cells + c->cfg.block_cells - 1) / c->cfg.block_cells);
+    p.L = d.L;
+    p.half_L = d.L / 2.0;
+    p.h = d.L / (double)nc;
+    p.inv_h = (double)nc / d.L;
+    p.hf = (float)p.h;
+    p.k = d.spring_params[0];
+    p.kappa = d.spring_params[1];
+    p.theta0 = d.spring_params[2];
+    p.calc_springs = d.calc_springs ? 1 : 0;
+    p.get_orient = (d.calc_springs && d.spring_params[4] != 0.0) ? 1 : 0;
+    p.calc_bend = (d.calc_springs && d.spring_params[1] != 0.0) ? 1 : 0;
+    p.calc_wca = d.calc_wca ? 1 : 0;
+    p.p0 = d.wca_params[0];
+    p.p1 = d.wca_params[1];
+    p.shift = d.wca_params[2];
+    p.rc2 = d.wca_params[3] * d.wca_params[3];
+    p.n_nearby = d.n_nearby;
+    p.self_propel = d.self_propel ? 1 : 0;
+    p.v0 = d.active_params[0];
+    double ang = d.active_params[2];
+    p.rotate_prop = (ang != 0.0 && c->cfg.dim == 2) ? 1 : 0;
+    p.cos_a = std::cos(ang);
+    p.sin_a = std::sin(ang);
+    p.D = d.D;
+    p.Dr = d.Dr;
+    p.radius = d.radius;
+    p.sqrt2D = std::sqrt(2.0 * d.D);
+    p.dtmax = d.dtmax;
+    p.mdps = d.max_dist_per_step;
+    p.rk = d.rk_cheat;
+    p.seed = d.seed;
+}
+
+int launch(gcr_ctx *c, void *fn, int grid, int block)
+{
+    void *a[] = {&c->args};
+    GCR_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(block), a, 0, c->stream));
+    return GCR_OK;
+}
+
+int enqueue_step(gcr_ctx *c)
+{
+    int rc;
+    const int bb = c->cfg.block_beads, bc = c->cfg.block_cells;
+    if ((rc = launch(c, c->ks.pack0, c->grid_cells, bc))) return rc;
+    if ((rc = launch(c, c->ks.stage0, c->grid_beads, bb))) return rc;
+    if ((rc = launch(c, c->ks.pack1, c->grid_cells, bc))) return rc;
+    if ((rc = launch(c, c->ks.stage1, c->grid_beads, bb))) return rc;
+    if ((rc = launch(c, c->ks.update, c->grid_beads, bb))) return rc;
+    return GCR_OK;
+}
+
+int build_graph(gcr_ctx *c)
+{
+    if (c->graph) return GCR_OK;
+    cudaGraph_t g = nullptr;
+    GCR_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int rc = GCR_OK;
+    for (int s = 0; s < c->cfg.steps_per_graph && rc == GCR_OK; s++) rc = enqueue_step(c);
+    cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+    if (rc != GCR_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (e != cudaSuccess) return fail(GCR_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(GCR_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return GCR_OK;
+}
+
+bool valid_slot(const gcr_ctx *c, int32_t slot)
+{
+    return c && slot >= 0 && slot < (int32_t)c->slots.size() && c->slots[slot].used;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *gcr_last_error(void) { return g_last_error.c_str(); }
+
+int gcr_version(void) { return 1; }
+
+int gcr_footprint(const gcr_config *cfg, const gcr_system_desc *desc, int64_t *cells_out, int64_t *bytes_out)
+{
+    if (!cfg) return fail(GCR_ERR_BAD_ARG, "null config");
+    int64_t nc = 1;
+    int rc = validate_desc(*cfg, desc, &nc);
+    if (rc) return rc;
+    int64_t cells = 0;
+    if (desc->calc_wca) {
+        cells = 1;
+        for (int i = 0; i < cfg->dim; i++) cells *= nc;
+    }
+    const int64_t n = desc->n_beads, d = cfg->dim;
+    const int64_t ft = cfg->precision == GCR_FP64 ? 8 : 4;
+    const int64_t recb = cfg->precision == GCR_FP64 ? 32 : 16;
+    int64_t bytes = n * d * (8 + 8 + ft + ft) + n * 4 + desc->n_chains * 8  // caller-owned state
+                    + n + 4 * (desc->n_chains + 1)                            // topo, chain starts
+                    + cells * (8 + (int64_t)cfg->cell_depth * (4 + recb));    // cell table
+    if (cells_out) *cells_out = cells;
+    if (bytes_out) *bytes_out = bytes;
+    return GCR_OK;
+}
+
+int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
+{
+    if (!cfg_in || !out) return fail(GCR_ERR_BAD_ARG, "null argument");
+    gcr_config cfg = *cfg_in;
+    if (cfg.dim != 2 && cfg.dim != 3) return fail(GCR_ERR_BAD_ARG, "dim must be 2 or 3");
+    if (cfg.precision != GCR_FP64 && cfg.precision != GCR_MIXED) return fail(GCR_ERR_BAD_ARG, "bad precision");
+    if (cfg.cell_depth != 8 && cfg.cell_depth != 16 && cfg.cell_depth != 32 && cfg.cell_depth != 64)
+        return fail(GCR_ERR_BAD_ARG, "cell_depth must be 8, 16, 32 or 64");
+    if (cfg.block_beads < 64 || cfg.block_beads > 512 || cfg.block_beads % 32)
+        return fail(GCR_ERR_BAD_ARG, "block_beads must be a multiple of 32 in [64, 512]");
+    if (cfg.block_cells < 64 || cfg.block_cells > 512 || cfg.block_cells % 32)
+        return fail(GCR_ERR_BAD_ARG, "block_cells must be a multiple of 32 in [64, 512]");
+    if (cfg.steps_per_graph < 1 || cfg.steps_per_graph > 64)
+        return fail(GCR_ERR_BAD_ARG, "steps_per_graph must be in [1, 64]");
+    if (cfg.bead_capacity <= 0 || cfg.system_capacity <= 0 || cfg.cell_capacity < 0)
+        return fail(GCR_ERR_BAD_ARG, "capacities must be positive");
+
+    gcr_ctx *c = new (std::nothrow) gcr_ctx();
+    if (!c) return fail(GCR_ERR_OOM, "host allocation");
+    c->cfg = cfg;
+    auto cleanup = [&](int code) {
+        gcr_destroy(c);
+        return code;
+    };
+    if (cudaGetDevice(&c->device) != cudaSuccess) return cleanup(fail(GCR_ERR_CUDA, "no CUDA device"));
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, c->device);
+    if (cuda_stream) {
+        c->stream = (cudaStream_t)cuda_stream;
+    } else {
+        if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+            return cleanup(fail(GCR_ERR_CUDA, "stream creation"));
+        c->own_stream = true;
+    }
+    c->ks = kernel_set(cfg.dim, cfg.precision);
+    const int64_t S = cfg.system_capacity;
+    c->max_bead_tiles = cfg.bead_capacity / cfg.block_beads + S;
+    c->max_cell_tiles = cfg.cell_capacity / cfg.block_cells + S;
+    const int64_t slots_total = cfg.cell_capacity * (int64_t)cfg.cell_depth;
+    c->rec_bytes = (size_t)slots_total * (cfg.precision == GCR_FP64 ? 32 : 16);
+    cudaError_t e = cudaSuccess;
+    e = e ? e : cudaMalloc(&c->dP, sizeof(SysP) * S);
+    e = e ? e : cudaMalloc(&c->dS, sizeof(SysS) * S);
+    e = e ? e : cudaMalloc(&c->d_bead_tiles, sizeof(Tile) * c->max_bead_tiles);
+    e = e ? e : cudaMalloc(&c->d_cell_tiles, sizeof(Tile) * c->max_cell_tiles);
+    e = e ? e : cudaMalloc(&c->d_ntiles, sizeof(int) * 2);
+    e = e ? e : cudaMalloc(&c->topo, (size_t)cfg.bead_capacity);
+    e = e ? e : cudaMalloc(&c->cnt0, sizeof(int) * std::max<int64_t>(cfg.cell_capacity, 1));
+    e = e ? e : cudaMalloc(&c->cnt1, sizeof(int) * std::max<int64_t>(cfg.cell_capacity, 1));
+    e = e ? e : cudaMalloc(&c->items, sizeof(int) * std::max<int64_t>(slots_total, 1));
+    e = e ? e : cudaMalloc(&c->rec, std::max<size_t>(c->rec_bytes, 32));
+    e = e ? e : cudaMalloc(&c->chain_starts, sizeof(int32_t) * (cfg.bead_capacity + S));
+    e = e ? e : cudaMalloc(&c->d_err, sizeof(int));
+    e = e ? e : cudaMalloc(&c->d_out, sizeof(double) * 8);
+    if (e != cudaSuccess)
+        return cleanup(fail(e == cudaErrorMemoryAllocation ? GCR_ERR_OOM : GCR_ERR_CUDA,
+                            std::string("device allocation: ") + cudaGetErrorString(e)));
+    cudaMemsetAsync(c->dS, 0, sizeof(SysS) * S, c->stream);
+    cudaMemsetAsync(c->d_ntiles, 0, sizeof(int) * 2, c->stream);
+    cudaMemsetAsync(c->cnt0, 0, sizeof(int) * std::max<int64_t>(cfg.cell_capacity, 1), c->stream);
+    cudaMemsetAsync(c->cnt1, 0, sizeof(int) * std::max<int64_t>(cfg.cell_capacity, 1), c->stream);
+    c->slots.assign(S, Slot());
+    c->hP.assign(S, SysP());
+    c->hS.assign(S, SysS());
+    c->beads.init(cfg.bead_capacity);
+    c->cells.init(cfg.cell_capacity);
+    c->chains.init(cfg.bead_capacity + S);
+    BatchArgs &a = c->args;
+    a.P = c->dP;
+    a.S = c->dS;
+    a.bead_tiles = c->d_bead_tiles;
+    a.n_bead_tiles = c->d_ntiles;
+    a.cell_tiles = c->d_cell_tiles;
+    a.n_cell_tiles = c->d_ntiles + 1;
+    a.topo = c->topo;
+    a.cnt0 = c->cnt0;
+    a.cnt1 = c->cnt1;
+    a.items = c->items;
+    a.rec = c->rec;
+    a.depth = cfg.cell_depth;
+    a.log_depth = ilog2(cfg.cell_depth);
+    a.tile_beads = cfg.block_beads;
+    a.tile_cells = cfg.block_cells;
+    int gb = kernel_grid(c, c->ks.stage0, cfg.block_beads, c->max_bead_tiles);
+    gb = std::min(gb, kernel_grid(c, c->ks.stage1, cfg.block_beads, c->max_bead_tiles));
+    gb = std::min(gb, kernel_grid(c, c->ks.update, cfg.block_beads, c->max_bead_tiles));
+    c->grid_beads = gb;
+    c->grid_cells = kernel_grid(c, c->ks.pack0, cfg.block_cells, c->max_cell_tiles);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return cleanup(fail(GCR_ERR_CUDA, "initialisation"));
+    *out = c;
+    return GCR_OK;
+}
+
+int gcr_destroy(gcr_ctx *c)
+{
+    if (!c) return GCR_OK;
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->topo, c->cnt0, c->cnt1,
+                    c->items, c->rec, c->chain_starts, c->d_err, c->d_out};
+    for (void *p : ptrs)
+        if (p) cudaFree(p);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return GCR_OK;
+}
+
+int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers *buf, int32_t *slot_out)
+{
+    if (!c || !desc || !buf || !slot_out) return fail(GCR_ERR_BAD_ARG, "null argument");
+    if (!buf->pos || !buf->pos1 || !buf->tangent || !buf->forces || !buf->chain_id || !buf->rest_lengths)
+        return fail(GCR_ERR_BAD_ARG, "all state buffers must be bound");
+    int64_t nc = 1;
+    int rc = validate_desc(c->cfg, desc, &nc);
+    if (rc) return rc;
+    int slot = -1;
+    for (int s = 0; s < (int)c->slots.size(); s++)
+        if (!c->slots[s].used) {
+            slot = s;
+            break;
+        }
+    if (slot < 0) return fail(GCR_ERR_CAPACITY, "no free system slot");
+    int64_t n_cells = 0;
+    if (desc->calc_wca) {
+        n_cells = 1;
+        for (int i = 0; i < c->cfg.dim; i++) n_cells *= nc;
+    }
+    int64_t boff = c->beads.alloc(desc->n_beads);
+    if (boff < 0) return fail(GCR_ERR_CAPACITY, "bead capacity exhausted");
+    int64_t coff = n_cells ? c->cells.alloc(n_cells) : 0;
+    if (coff < 0) {
+        c->beads.release(boff, desc->n_beads);
+        return fail(GCR_ERR_CAPACITY, "cell capacity exhausted");
+    }
+    int64_t choff = c->chains.alloc(desc->n_chains + 1);
+    if (choff < 0) {
+        c->beads.release(boff, desc->n_beads);
+        if (n_cells) c->cells.release(coff, n_cells);
+        return fail(GCR_ERR_CAPACITY, "chain capacity exhausted");
+    }
+    Slot &sl = c->slots[slot];
+    sl.used = true;
+    sl.desc = *desc;
+    sl.buf = *buf;
+    sl.bead_off = boff;
+    sl.cell_off = coff;
+    sl.chain_off = choff;
+    sl.n_cells = n_cells;
+    fill_sysp(c, sl, nc, c->hP[slot]);
+    SysS &s = c->hS[slot];
+    std::memset(&s, 0, sizeof(s));
+    s.dt = desc->dtmax;
+    s.step = desc->step;
+    s.max_steps = 0;
+    s.max_dt_usable = -1.0;
+    GCR_CUDA(cudaMemcpyAsync(c->dP + slot, &c->hP[slot], sizeof(SysP), cudaMemcpyHostToDevice, c->stream));
+    GCR_CUDA(cudaMemcpyAsync(c->dS + slot, &s, sizeof(SysS), cudaMemcpyHostToDevice, c->stream));
+    int n = (int)desc->n_beads;
+    void *targs[] = {(void *)&buf->chain_id, &n, nullptr};
+    uint8_t *tp = c->topo + boff;
+    targs[2] = &tp;
+    GCR_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    GCR_CUDA(cudaLaunchKernel(c->ks.topo, dim3((n + 255) / 256), dim3(256), targs, 0, c->stream));
+    GCR_CUDA(launch_chain_starts(buf->chain_id, n, (int)desc->n_chains, c->chain_starts + choff, c->d_err,
+                                 c->stream));
+    int err = 0;
+    GCR_CUDA(cudaMemcpyAsync(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    if (err) {
+        c->beads.release(boff, desc->n_beads);
+        if (n_cells) c->cells.release(coff, n_cells);
+        c->chains.release(choff, desc->n_chains + 1);
+        sl = Slot();
+        return fail(GCR_ERR_BAD_ARG, "chain ids must be non-decreasing and in [0, n_chains)");
+    }
+    rc = rebuild_tiles(c);
+    if (rc) return rc;
+    *slot_out = slot;
+    return GCR_OK;
+}
+
+int gcr_evict(gcr_ctx *c, int32_t slot)
+{
+    if (!valid_slot(c, slot)) return fail(GCR_ERR_BAD_ARG, "invalid slot");
+    Slot &sl = c->slots[slot];
+    // make sure no queued work still uses the slot's scratch
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    c->beads.release(sl.bead_off, sl.desc.n_beads);
+    if (sl.n_cells) c->cells.release(sl.cell_off, sl.n_cells);
+    c->chains.release(sl.chain_off, sl.desc.n_chains + 1);
+    sl = Slot();
+    SysS &s = c->hS[slot];
+    std::memset(&s, 0, sizeof(s));
+    GCR_CUDA(cudaMemcpyAsync(c->dS + slot, &s, sizeof(SysS), cudaMemcpyHostToDevice, c->stream));
+    return rebuild_tiles(c);
+}
+
+int gcr_update_desc(gcr_ctx *c, int32_t slot, const gcr_system_desc *desc)
+{
+    if (!valid_slot(c, slot)) return fail(GCR_ERR_BAD_ARG, "invalid slot");
+    Slot &sl = c->slots[slot];
+    if (desc->n_beads != sl.desc.n_beads || desc->n_chains != sl.desc.n_chains)
+        return fail(GCR_ERR_BAD_ARG, "bead and chain counts of a resident system cannot change");
+    int64_t nc = 1;
+    int rc = validate_desc(c->cfg, desc, &nc);
+    if (rc) return rc;
+    int64_t n_cells = 0;
+    if (desc->calc_wca) {
+        n_cells = 1;
+        for (int i = 0; i < c->cfg.dim; i++) n_cells *= nc;
+    }
+    if (n_cells != sl.n_cells) return fail(GCR_ERR_BAD_ARG, "the GPU cell grid of a resident system cannot change");
+    sl.desc = *desc;
+    fill_sysp(c, sl, nc, c->hP[slot]);
+    GCR_CUDA(cudaMemcpyAsync(c->dP + slot, &c->hP[slot], sizeof(SysP), cudaMemcpyHostToDevice, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    return GCR_OK;
+}
+
+namespace {
+int check_call(const gcr_call *call)
+{
+    if (!call) return fail(GCR_ERR_BAD_ARG, "null call");
+    if (call->noise && call->noise_steps <= 0) return fail(GCR_ERR_BAD_ARG, "injected noise without steps");
+    if (call->noise && call->max_steps < 0) return fail(GCR_ERR_BAD_ARG, "injected noise needs a step limit");
+    if (call->noise && call->max_steps > call->noise_steps)
+        return fail(GCR_ERR_BAD_ARG, "fewer injected noise steps than the step limit");
+    return GCR_OK;
+}
+
+void arm(SysS &s, const gcr_call *call)
+{
+    s.dt = call->dt;
+    s.dt_next = call->dt;
+    s.dt_used = 0.0;
+    s.elapsed = 0.0;
+    s.max_f2 = 0ull;
+    s.steps_done = 0;
+    s.max_steps = call->max_steps;
+    s.max_dt_usable = call->max_dt_usable;
+    s.noise = call->noise;
+    s.noise_steps = call->noise_steps;
+    s.flags = 0;
+    s.tile_ctr[0] = s.tile_ctr[1] = 0u;
+    s.active = ((0 < s.max_steps || s.max_steps < 0) && (0.0 < s.max_dt_usable || s.max_dt_usable < 0.0)) ? 1 : 0;
+}
+}  // namespace
+
+int gcr_call_begin_batch(gcr_ctx *c, int32_t n, const int32_t *slots, const gcr_call *calls)
+{
+    if (!c || n < 0 || (n > 0 && (!slots || !calls))) return fail(GCR_ERR_BAD_ARG, "bad argument");
+    for (int i = 0; i < n; i++) {
+        if (!valid_slot(c, slots[i])) return fail(GCR_ERR_BAD_ARG, "invalid slot");
+        int rc = check_call(calls + i);
+        if (rc) return rc;
+    }
+    const int S = (int)c->slots.size();
+    // the device table holds the step counters: fetch it, arm, write it back
+    GCR_CUDA(cudaMemcpyAsync(c->hS.data(), c->dS, sizeof(SysS) * S, cudaMemcpyDeviceToHost, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < n; i++) arm(c->hS[slots[i]], calls + i);
+    GCR_CUDA(cudaMemcpyAsync(c->dS, c->hS.data(), sizeof(SysS) * S, cudaMemcpyHostToDevice, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    return GCR_OK;
+}
+
+int gcr_call_begin(gcr_ctx *c, int32_t slot, const gcr_call *call)
+{
+    if (!valid_slot(c, slot) || !call) return fail(GCR_ERR_BAD_ARG, "invalid slot or call");
+    int rc = check_call(call);
+    if (rc) return rc;
+    SysS &s = c->hS[slot];
+    // the device copy holds the current step counter: fetch it first
+    GCR_CUDA(cudaMemcpyAsync(&s, c->dS + slot, sizeof(SysS), cudaMemcpyDeviceToHost, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    arm(s, call);
+    GCR_CUDA(cudaMemcpyAsync(c->dS + slot, &s, sizeof(SysS), cudaMemcpyHostToDevice, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    return GCR_OK;
+}
+
+int gcr_run(gcr_ctx *c, int64_t max_steps, int32_t sync_every)
+{
+    if (!c) return fail(GCR_ERR_BAD_ARG, "null context");
+    if (max_steps <= 0) return GCR_OK;
+    if (c->tiles_dirty) {
+        int rc = rebuild_tiles(c);
+        if (rc) return rc;
+    }
+    int rc = build_graph(c);
+    if (rc) return rc;
+    const size_t cb = sizeof(int) * std::max<int64_t>(c->cfg.cell_capacity, 1);
+    GCR_CUDA(cudaMemsetAsync(c->cnt0, 0, cb, c->stream));
+    GCR_CUDA(cudaMemsetAsync(c->cnt1, 0, cb, c->stream));
+    rc = launch(c, c->ks.insert, c->grid_beads, c->cfg.block_beads);
+    if (rc) return rc;
+    const int64_t spg = c->cfg.steps_per_graph;
+    const int64_t graphs = (max_steps + spg - 1) / spg;
+    for (int64_t g = 0; g < graphs; g++) {
+        GCR_CUDA(cudaGraphLaunch(c->graph, c->stream));
+        if (sync_every > 0 && (g + 1) % sync_every == 0 && g + 1 < graphs) {
+            int32_t n = 0;
+            rc = gcr_count_active(c, &n);
+            if (rc) return rc;
+            if (n == 0) break;
+        }
+    }
+    GCR_CUDA(cudaGetLastError());
+    return GCR_OK;
+}
+
+int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
+{
+    if (!c || !ms_out || n_steps <= 0) return fail(GCR_ERR_BAD_ARG, "bad argument");
+    if (c->tiles_dirty) {
+        int rc = rebuild_tiles(c);
+        if (rc) return rc;
+    }
+    const size_t cb = sizeof(int) * std::max<int64_t>(c->cfg.cell_capacity, 1);
+    GCR_CUDA(cudaMemsetAsync(c->cnt0, 0, cb, c->stream));
+    GCR_CUDA(cudaMemsetAsync(c->cnt1, 0, cb, c->stream));
+    int rc = launch(c, c->ks.insert, c->grid_beads, c->cfg.block_beads);
+    if (rc) return rc;
+    void *fns[5] = {c->ks.pack0, c->ks.stage0, c->ks.pack1, c->ks.stage1, c->ks.update};
+    const bool cellk[5] = {true, false, true, false, false};
+    std::vector<cudaEvent_t> ev((size_t)n_steps * 10, nullptr);
+    for (auto &e : ev) GCR_CUDA(cudaEventCreate(&e));
+    for (int s = 0; s < n_steps; s++)
+        for (int k = 0; k < 5; k++) {
+            GCR_CUDA(cudaEventRecord(ev[(size_t)s * 10 + 2 * k], c->stream));
+            rc = launch(c, fns[k], cellk[k] ? c->grid_cells : c->grid_beads,
+                        cellk[k] ? c->cfg.block_cells : c->cfg.block_beads);
+            if (rc) return rc;
+            GCR_CUDA(cudaEventRecord(ev[(size_t)s * 10 + 2 * k + 1], c->stream));
+        }
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 5; k++) ms_out[k] = 0.f;
+    for (int s = 0; s < n_steps; s++)
+        for (int k = 0; k < 5; k++) {
+            float ms = 0.f;
+            GCR_CUDA(cudaEventElapsedTime(&ms, ev[(size_t)s * 10 + 2 * k], ev[(size_t)s * 10 + 2 * k + 1]));
+            ms_out[k] += ms;
+        }
+    for (auto &e : ev) cudaEventDestroy(e);
+    return GCR_OK;
+}
+
+int gcr_synchronize(gcr_ctx *c)
+{
+    if (!c) return fail(GCR_ERR_BAD_ARG, "null context");
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    return GCR_OK;
+}
+
+int gcr_count_active(gcr_ctx *c, int32_t *n_out)
+{
+    if (!c || !n_out) return fail(GCR_ERR_BAD_ARG, "null argument");
+    const int S = (int)c->slots.size();
+    GCR_CUDA(cudaMemcpyAsync(c->hS.data(), c->dS, sizeof(SysS) * S, cudaMemcpyDeviceToHost, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    int n = 0;
+    for (int s = 0; s < S; s++)
+        if (c->slots[s].used && c->hS[s].active) n++;
+    *n_out = n;
+    return GCR_OK;
+}
+
+int gcr_get_status(gcr_ctx *c, int32_t slot, gcr_status *out)
+{
+    if (!valid_slot(c, slot) || !out) return fail(GCR_ERR_BAD_ARG, "invalid slot or output");
+    SysS &s = c->hS[slot];
+    GCR_CUDA(cudaMemcpyAsync(&s, c->dS + slot, sizeof(SysS), cudaMemcpyDeviceToHost, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    out->dt = s.dt;
+    out->dt_used = s.elapsed;
+    out->max_forces_strength = s.mfs;
+    out->steps_done = s.steps_done;
+    out->step = s.step;
+    out->flags = s.flags;
+    out->active = s.active;
+    return GCR_OK;
+}
+
+int gcr_order_params(gcr_ctx *c, int32_t slot, double out[3])
+{
+    if (!valid_slot(c, slot) || !out) return fail(GCR_ERR_BAD_ARG, "invalid slot or output");
+    if (c->cfg.dim != 2) return fail(GCR_ERR_BAD_ARG, "order parameters are defined for 2D systems");
+    const Slot &sl = c->slots[slot];
+    GCR_CUDA(launch_order_params(c->cfg.dim, c->cfg.precision, c->hP[slot], c->chain_starts + sl.chain_off,
+                                 c->d_out, c->stream));
+    GCR_CUDA(cudaMemcpyAsync(out, c->d_out, sizeof(double) * 3, cudaMemcpyDeviceToHost, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    return GCR_OK;
+}
+
+int gcr_reference_lists(gcr_ctx *c, int32_t slot, int64_t n_grid, int64_t grid_window, int64_t *where_is_bead,
+                        int64_t *grid_list, int64_t grid_depth1, int64_t *nbor_list, int64_t nbor_depth1,
+                        int32_t mode)
+{
+    if (!valid_slot(c, slot) || !where_is_bead) return fail(GCR_ERR_BAD_ARG, "invalid slot or output");
+    if (n_grid < 1 || grid_window < 1) return fail(GCR_ERR_BAD_ARG, "bad grid");
+    if (grid_list && grid_depth1 < 3) return fail(GCR_ERR_BAD_ARG, "grid depth too small");
+    if (nbor_list && nbor_depth1 < 2) return fail(GCR_ERR_BAD_ARG, "neighbour depth too small");
+    if (mode == 1 && !grid_list) return fail(GCR_ERR_BAD_ARG, "the cell-window neighbour list needs grid_list");
+    GCR_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    SysP p = c->hP[slot];
+    // mode 0: the rule of SRK.py:450 (all-pairs when N < n_grid^dim),
+    // 1: cell window (populations.update_nbor_list_with_pop2), 2: all pairs
+    int64_t n_pow = 1;
+    for (int i = 0; i < c->cfg.dim; i++) n_pow *= n_grid;
+    bool few = (mode == 2) || (mode == 0 && p.n < n_pow) || !grid_list;
+    if (few && nbor_list && p.n > 200000)
+        return fail(GCR_ERR_BAD_ARG, "the all-pairs neighbour builder is limited to 200000 beads");
+    GCR_CUDA(launch_reference_lists(c->cfg.dim, p, n_grid, grid_window, where_is_bead, grid_list, grid_depth1,
+                                    few ? nullptr : nbor_list, nbor_depth1, c->d_err, c->stream));
+    if (few && nbor_list)
+        GCR_CUDA(launch_reference_lists(c->cfg.dim, p, n_grid, grid_window, where_is_bead, nullptr, grid_depth1,
+                                        nbor_list, nbor_depth1, c->d_err, c->stream));
+    int err = 0;
+    GCR_CUDA(cudaMemcpyAsync(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    if (err) return fail(GCR_ERR_OVERFLOW, err & 1 ? "grid_list depth too small" : "nbor_list depth too small");
+    return GCR_OK;
+}
+
+int gcr_cell_assignment(gcr_ctx *c, int32_t slot, int32_t *cell_of_bead, int32_t *n_cells_side)
+{
+    if (!valid_slot(c, slot) || !cell_of_bead) return fail(GCR_ERR_BAD_ARG, "invalid slot or output");
+    GCR_CUDA(launch_cell_assignment(c->cfg.dim, c->hP[slot], cell_of_bead, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    if (n_cells_side) *n_cells_side = c->hP[slot].nc;
+    return GCR_OK;
+}
+
+int gcr_philox_noise(int32_t dim, uint64_t seed, int64_t step, int64_t n, int32_t do_trans, int32_t do_rot,
+                     double *out, void *cuda_stream)
+{
+    if ((dim != 2 && dim != 3) || n < 0 || !out) return fail(GCR_ERR_BAD_ARG, "bad argument");
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    GCR_CUDA(launch_philox_noise(dim, seed, step, n, do_trans, do_rot, out, st));
+    GCR_CUDA(cudaStreamSynchronize(st));
+    return GCR_OK;
+}
+
+}  // extern "C"

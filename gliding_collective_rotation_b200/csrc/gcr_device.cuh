@@ -1,0 +1,195 @@
+// gcr_device.cuh -- device-side types and helpers of the B200 SRK2 hot path.
+//
+// Data layout in HBM (one context, many systems):
+//   * per system, caller-owned: pos/pos1 FP64 [n,d] (AoS), tangent/forces FT
+//     [n,d], chain_id int32 [n], rest_lengths FP64 [n_chains];
+//   * library scratch, per system at a bead / cell offset:
+//       topo      uint8 [bead]       chain-neighbour bits of each bead
+//       cnt[2]    int32 [cell]       beads binned per GPU cell (ping-pong)
+//       items     int32 [cell*depth] bead ids per cell slot (unsorted)
+//       rec       float4|double4 [cell*depth] packed positions per slot,
+//                 sorted by bead id inside a cell
+//   * SysP (read-only during a step) and SysS (device-updated) per slot.
+// The GPU cell table has a fixed depth per cell, the same shape as the
+// reference's grid_list (updates.py:502-522): a count and `depth` slots.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gcr {
+
+constexpr int kMaxDim = 3;
+
+// topology bits of a bead (same chain as b-1, b-2, b+1, b+2)
+constexpr uint8_t kHasPrev = 1, kHasPrev2 = 2, kHasNext = 4, kHasNext2 = 8;
+
+// device status flags (mirror GCR_FLAG_* in gcr.h)
+constexpr int kFlagCellOverflow = 1;
+constexpr int kFlagNonFinite = 2;
+constexpr int kFlagNextOverflow = 4;
+
+struct SysP {
+    // caller-owned state
+    double *pos;
+    double *pos1;
+    void *tan;
+    void *frc;
+    const int32_t *chain;
+    const double *rest;
+    // scratch placement
+    int64_t bead_off;  // into topo
+    int64_t cell_off;  // into cnt / items / rec
+    int32_t n;
+    int32_t n_chains;
+    int32_t nc;        // GPU cells per side
+    int32_t n_cells;   // nc^d
+    int32_t n_bead_tiles;
+    int32_t n_cell_tiles;
+    double L, half_L, h, inv_h;
+    float hf;          // h rounded to FP32 (mixed records)
+    // bonded
+    double k, kappa, theta0;
+    int32_t calc_springs, get_orient, calc_bend, calc_wca;
+    // pair (WCA / LJ: coeff = ds^-4 (p0 - p1 ds^-3))
+    double p0, p1, shift, rc2;
+    int32_t n_nearby;
+    int32_t self_propel;
+    int32_t rotate_prop;  // 2D and v_tan_angle != 0
+    int32_t pad0;
+    double v0, cos_a, sin_a;
+    // noise / SRK
+    double D, Dr, radius, sqrt2D;
+    double dtmax, mdps, rk;
+    uint64_t seed;
+};
+
+struct SysS {
+    double dt;          // predictor dt of the coming step (status.dt)
+    double dt_next;     // dt chosen by the max-force rule this step
+    double dt_used;     // corrector dt of this step
+    double elapsed;     // time elapsed in the call (shared_arr[:,1])
+    double mfs;         // max_forces_strength of the last step
+    double max_dt_usable;
+    unsigned long long max_f2;  // bit pattern of max |F|^2 (non-negative double)
+    int64_t step;       // global step index (Philox counter)
+    int64_t steps_done; // steps completed in the call
+    int64_t max_steps;
+    const double *noise;  // injected noise_vec snapshots or nullptr
+    int64_t noise_steps;
+    int32_t active;
+    int32_t flags;
+    uint32_t tile_ctr[2];
+};
+
+struct Tile {
+    int32_t sys;
+    int32_t begin;
+};
+
+// ---------------------------------------------------------------------
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as
+// easy as 1, 2, 3", SC'11) and the Box-Muller pair drawn from one block.
+// counter = (bead, step lo, step hi, stream), key = (seed lo, seed hi).
+// ---------------------------------------------------------------------
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1)
+{
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        uint32_t lo0 = c.x * 0xD2511F53u, hi0 = __umulhi(c.x, 0xD2511F53u);
+        uint32_t lo1 = c.z * 0xCD9E8D57u, hi1 = __umulhi(c.z, 0xCD9E8D57u);
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+__device__ __forceinline__ void normal_pair(uint64_t seed, uint32_t bead, int64_t step,
+                                            uint32_t stream, double &z0, double &z1)
+{
+    uint4 r = philox4x32_10(make_uint4(bead, (uint32_t)((uint64_t)step & 0xffffffffu),
+                                       (uint32_t)((uint64_t)step >> 32), stream),
+                            (uint32_t)(seed & 0xffffffffu), (uint32_t)(seed >> 32));
+    const double two_m53 = 1.1102230246251565e-16;
+    uint64_t a = (((uint64_t)r.x << 21) ^ (uint64_t)(r.y >> 11)) & ((1ull << 53) - 1);
+    uint64_t b = (((uint64_t)r.z << 21) ^ (uint64_t)(r.w >> 11)) & ((1ull << 53) - 1);
+    double u1 = ((double)a + 1.0) * two_m53;
+    double u2 = (double)b * two_m53;
+    double rad = sqrt(-2.0 * log(u1));
+    double s, c;
+    sincos(6.283185307179586 * u2, &s, &c);
+    z0 = rad * c;
+    z1 = rad * s;
+}
+
+// translational (stream 0,1) or rotational (stream 2,3) deviates of one bead
+template <int D>
+__device__ __forceinline__ void philox_normals(uint64_t seed, uint32_t bead, int64_t step, bool rot,
+                                               double out[D])
+{
+    double z0, z1;
+    uint32_t s0 = rot ? 2u : 0u;
+    normal_pair(seed, bead, step, s0, z0, z1);
+    out[0] = z0;
+    out[1] = z1;
+    if (D == 3) {
+        double z2, z3;
+        normal_pair(seed, bead, step, s0 + 1u, z2, z3);
+        out[D - 1] = z2;
+    }
+}
+
+// Python float modulo: result in [0, m) with the sign of m, the wrap the
+// reference applies after every update (SRK.py:387).
+__device__ __forceinline__ double py_mod(double x, double m)
+{
+    if (x >= 0.0 && x < m) return x == 0.0 ? 0.0 : x;
+    if (x < 0.0 && x >= -m) return x + m;
+    if (x >= m && x < 2.0 * m) return x - m;
+    double r = fmod(x, m);
+    if (r != 0.0) {
+        if ((m < 0.0) != (r < 0.0)) r += m;
+    } else {
+        r = copysign(0.0, m);
+    }
+    return r;
+}
+
+// CPython float floor division (float_divmod), as Numba lowers `x // h`.
+__device__ __forceinline__ double py_floordiv(double x, double m)
+{
+    double mod = fmod(x, m);
+    double div = __ddiv_rn(__dsub_rn(x, mod), m);
+    if (mod != 0.0) {
+        if ((m < 0.0) != (mod < 0.0)) div = __dsub_rn(div, 1.0);
+    }
+    double fd;
+    if (div != 0.0) {
+        fd = floor(div);
+        if (__dsub_rn(div, fd) > 0.5) fd = __dadd_rn(fd, 1.0);
+    } else {
+        fd = copysign(0.0, x / m);
+    }
+    return fd;
+}
+
+// minimum image of a - b along one axis, forces.inbounds_diff (forces.py:44-55)
+__device__ __forceinline__ double inbounds(double a, double b, double half_L, double L)
+{
+    double o = a - b;
+    if (o < -half_L)
+        o += L;
+    else if (o >= half_L)
+        o -= L;
+    return o;
+}
+
+// GPU cell coordinate of a position (clamped; non-finite -> 0)
+__device__ __forceinline__ int cell_coord(double x, double inv_h, int nc)
+{
+    double f = floor(x * inv_h);
+    int c = (f >= 0.0 && f < (double)nc) ? (int)f : (f >= (double)nc ? nc - 1 : 0);
+    return c;
+}
+
+}  // namespace gcr

@@ -1,0 +1,54 @@
+// gcr_kernels.h -- kernel arguments and entry points shared by the host
+// library (gcr_abi.cu) and the kernel translation units.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "gcr_device.cuh"
+
+namespace gcr {
+
+// Everything a step kernel reads: device pointers of one context.
+struct BatchArgs {
+    const SysP *P;
+    SysS *S;
+    const Tile *bead_tiles;
+    const int *n_bead_tiles;
+    const Tile *cell_tiles;
+    const int *n_cell_tiles;
+    const uint8_t *topo;
+    int *cnt0;
+    int *cnt1;
+    int *items;
+    void *rec;
+    int depth;
+    int log_depth;
+    int tile_beads;
+    int tile_cells;
+};
+
+struct KernelSet {
+    void *insert;
+    void *pack0;
+    void *pack1;
+    void *stage0;
+    void *stage1;
+    void *update;
+    void *topo;
+};
+
+KernelSet kernel_set(int dim, int precision);
+
+// gcr_lists.cu
+cudaError_t launch_reference_lists(int dim, const SysP &p, int64_t n_grid, int64_t grid_window,
+                                   int64_t *where_is_bead, int64_t *grid_list, int64_t grid_depth1,
+                                   int64_t *nbor_list, int64_t nbor_depth1, int *d_err, cudaStream_t st);
+cudaError_t launch_order_params(int dim, int precision, const SysP &p, const int32_t *chain_start,
+                                double *d_out, cudaStream_t st);
+cudaError_t launch_chain_starts(const int32_t *chain, int n, int n_chains, int32_t *chain_start, int *d_err,
+                                cudaStream_t st);
+cudaError_t launch_cell_assignment(int dim, const SysP &p, int32_t *cell_of_bead, cudaStream_t st);
+cudaError_t launch_philox_noise(int dim, uint64_t seed, int64_t step, int64_t n, int do_trans,
+                                int do_rot, double *out, cudaStream_t st);
+
+}  // namespace gcr

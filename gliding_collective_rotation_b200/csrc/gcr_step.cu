@@ -1,0 +1,700 @@
+// gcr_step.cu -- the SRK2 step kernels (sm_100a).
+//
+// One step of every resident system is five persistent, grid-stride launches
+// over per-system tile tables:
+//
+//   pack<A>    per GPU cell: sort the slot contents by bead id, write packed
+//              records of pos, clear the B counters
+//   stage<0>   per bead: pair forces over the 3^d neighbour cells + bond,
+//              bend and tangent + self-propulsion + predictor update
+//              pos1 = (pos + dt/r F0 + sqrt(2 D dt) xi) mod L; bins pos1 into B
+//   pack<B>    as pack<A> for pos1, clears the A counters
+//   stage<1>   per bead: the same forces at pos1 accumulated onto F0; block
+//              max of |F0+F1|^2; the last tile of each system picks dt
+//              (SRK.py:323-353)
+//   update     per bead: corrector pos = (pos + dt_used/(2r) (F0+F1)
+//              + sqrt(2 D dt_used) xi) mod L, rotational diffusion
+//              (SRK.py:398-423), bins pos into A; the last tile advances the
+//              system's step bookkeeping
+//
+// The same xi is used by predictor and corrector (SRK.py:134-142, 385): it is
+// drawn twice from the counter-based Philox stream keyed by (seed, bead,
+// global step, stream), or read from an injected noise_vec snapshot.
+//
+// Reference functions restated per bead: forces.calc_chain_spring_forces
+// (forces.py:285-403), forces.central_pair_force with forces.WCA
+// (forces.py:57-145, 13-15), forces.self_propel (forces.py:206-224), the
+// SRK2 stage updates (SRK.py:166-184, 355-396).
+#include "gcr_device.cuh"
+#include "gcr_kernels.h"
+
+namespace gcr {
+
+template <typename FT>
+struct Rec;
+template <>
+struct Rec<float> {
+    using type = float4;
+};
+struct alignas(32) Dbl4 {
+    double x, y, z, w;
+};
+template <>
+struct Rec<double> {
+    using type = Dbl4;
+};
+
+// ------------------------------------------------------------------------
+// bonded forces (forces.py:285-403) for one bead, gathered from bonds
+// b-2 .. b+1; accumulation order follows the reference's sequential loop
+// ------------------------------------------------------------------------
+template <int D, typename FT>
+struct Bond {
+    FT d[D];
+    FT t[D];
+    FT fmag;
+    bool valid;
+};
+
+template <int D, typename FT>
+__device__ __forceinline__ void make_bond(const SysP &p, const double *__restrict__ X, int j, FT a,
+                                          FT k, Bond<D, FT> &bd)
+{
+    FT r2 = FT(0);
+#pragma unroll
+    for (int i = 0; i < D; i++) {
+        double o = inbounds(__ldg(X + (size_t)j * D + i), __ldg(X + (size_t)(j + 1) * D + i), p.half_L, p.L);
+        bd.d[i] = (FT)o;
+        r2 += bd.d[i] * bd.d[i];
+    }
+    bd.valid = (r2 != FT(0));
+    if (bd.valid) {
+        FT inv = FT(1) / sqrt(r2);
+        bd.fmag = k * (a * inv - FT(1));
+#pragma unroll
+        for (int i = 0; i < D; i++) bd.t[i] = bd.d[i] * inv;
+    } else {
+        bd.fmag = FT(0);
+#pragma unroll
+        for (int i = 0; i < D; i++) bd.t[i] = bd.d[i];
+    }
+}
+
+// bend at a bead with forward tangent ti (its own bond) and backward tangent
+// tj (the previous bond); returns false when the tangents are aligned
+template <int D, typename FT>
+__device__ __forceinline__ bool bend(const FT *ti, const FT *tj, FT theta0, FT kappa, bool want_force,
+                                     FT *fwd, FT *bwd, FT &c)
+{
+    c = FT(0);
+#pragma unroll
+    for (int i = 0; i < D; i++) c += ti[i] * tj[i];
+    if (!(FT(-1) < c && c < FT(1))) return false;
+    if (want_force) {
+        FT phi = acos(c);
+        if (theta0 != FT(0)) {
+            FT cr = -ti[0] * tj[1] + ti[1] * tj[0];
+            FT sg = (FT)((cr > FT(0)) - (cr < FT(0)));
+            phi += theta0 * sg;
+        }
+        phi *= kappa / sqrt(FT(1) - c * c);
+#pragma unroll
+        for (int i = 0; i < D; i++) {
+            fwd[i] = phi * (c * tj[i] - ti[i]);
+            bwd[i] = phi * (tj[i] - c * ti[i]);
+        }
+    }
+    return true;
+}
+
+template <int D, typename FT>
+__device__ __forceinline__ void bonded(const SysP &p, const uint8_t tp, const double *__restrict__ X, int b,
+                                       FT *F, FT *tang, bool &tang_set)
+{
+    const FT a = (FT)__ldg(p.rest + __ldg(p.chain + b));
+    const FT k = (FT)p.k;
+    const FT kappa = (FT)p.kappa, theta0 = (FT)p.theta0;
+    const bool cb = p.calc_bend;
+    Bond<D, FT> bm2, bm1, b0, bp1;
+    if (tp & kHasPrev2) make_bond<D, FT>(p, X, b - 2, a, k, bm2);
+    if (tp & kHasPrev) make_bond<D, FT>(p, X, b - 1, a, k, bm1);
+    if (tp & kHasNext) make_bond<D, FT>(p, X, b, a, k, b0);
+    if (tp & kHasNext2) make_bond<D, FT>(p, X, b + 1, a, k, bp1);
+    FT fwd[D], bwd[D], c;
+    // iteration b-1 of the reference loop: spring of bond b-1, bend at b-1
+    if (tp & kHasPrev) {
+        if (bm1.valid) {
+#pragma unroll
+            for (int i = 0; i < D; i++) F[i] -= bm1.d[i] * bm1.fmag;
+        }
+        if ((tp & kHasPrev2) && cb) {
+            if (bend<D, FT>(bm1.t, bm2.t, theta0, kappa, true, fwd, bwd, c)) {
+#pragma unroll
+                for (int i = 0; i < D; i++) F[i] -= bwd[i];
+            }
+        }
+    }
+    // iteration b: spring of bond b, bend at b, tangent of b
+    if (tp & kHasNext) {
+        if (b0.valid) {
+#pragma unroll
+            for (int i = 0; i < D; i++) F[i] += b0.d[i] * b0.fmag;
+        }
+    }
+    if (p.get_orient || cb) {
+        if ((tp & kHasPrev) && (tp & kHasNext)) {
+            if (bend<D, FT>(b0.t, bm1.t, theta0, kappa, cb, fwd, bwd, c)) {
+                if (cb) {
+#pragma unroll
+                    for (int i = 0; i < D; i++) F[i] += fwd[i] + bwd[i];
+                }
+                if (p.get_orient) {
+                    FT coeff = FT(1) / sqrt(FT(2) * (FT(1) + c));
+#pragma unroll
+                    for (int i = 0; i < D; i++) tang[i] = coeff * (b0.t[i] + bm1.t[i]);
+                    tang_set = true;
+                }
+            } else if (p.get_orient) {
+#pragma unroll
+                for (int i = 0; i < D; i++) tang[i] = b0.t[i];
+                tang_set = true;
+            }
+        } else if (p.get_orient && (tp & kHasNext)) {  // head bead
+#pragma unroll
+            for (int i = 0; i < D; i++) tang[i] = b0.t[i];
+            tang_set = true;
+        } else if (p.get_orient && (tp & kHasPrev)) {  // tail bead
+#pragma unroll
+            for (int i = 0; i < D; i++) tang[i] = bm1.t[i];
+            tang_set = true;
+        }
+    }
+    // iteration b+1: bend at b+1 pushes on b
+    if ((tp & kHasNext2) && cb) {
+        if (bend<D, FT>(bp1.t, b0.t, theta0, kappa, true, fwd, bwd, c)) {
+#pragma unroll
+            for (int i = 0; i < D; i++) F[i] -= fwd[i];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------
+// pair forces (forces.py:57-145, rule forces.WCA) over the 3^d GPU cells
+// around the bead; records are packed per cell, sorted by bead id
+// ------------------------------------------------------------------------
+template <typename FT>
+__device__ __forceinline__ FT wca_coeff(FT ds, FT p0, FT p1)
+{
+    // ds**-4 * (p0 - p1 * ds**-3), integer powers by squaring as Numba does
+    FT d2 = ds * ds;
+    FT i4 = FT(1) / (d2 * d2);
+    FT i3 = FT(1) / (ds * d2);
+    return i4 * (p0 - p1 * i3);
+}
+
+template <int D, typename FT>
+__device__ __forceinline__ void pair_forces(const SysP &p, const BatchArgs &A, const int *__restrict__ cnt,
+                                            int b, const double *xb, FT *F)
+{
+    using R = typename Rec<FT>::type;
+    const R *__restrict__ rec = reinterpret_cast<const R *>(A.rec);
+    const int nc = p.nc;
+    int ci[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < D; i++) ci[i] = cell_coord(xb[i], p.inv_h, nc);
+    FT own[3] = {FT(0), FT(0), FT(0)};
+    if constexpr (sizeof(FT) == 4) {
+#pragma unroll
+        for (int i = 0; i < D; i++) own[i] = (FT)(xb[i] - ((double)ci[i] + 0.5) * p.h);
+    }
+    const FT rc2 = (FT)p.rc2, p0 = (FT)p.p0, p1 = (FT)p.p1, shift = (FT)p.shift;
+    const FT hf = (FT)p.hf;
+    const int nn = p.n_nearby;
+    const int my_chain = __ldg(p.chain + b);
+    const int zlo = (D == 3) ? -1 : 0, zhi = (D == 3) ? 1 : 0;
+    for (int dz = zlo; dz <= zhi; dz++) {
+        int cz = 0;
+        if (D == 3) {
+            cz = ci[2] + dz;
+            cz += (cz < 0) ? nc : 0;
+            cz -= (cz >= nc) ? nc : 0;
+        }
+        for (int dy = -1; dy <= 1; dy++) {
+            int cy = ci[1] + dy;
+            cy += (cy < 0) ? nc : 0;
+            cy -= (cy >= nc) ? nc : 0;
+            const int64_t rowbase = p.cell_off + ((int64_t)cz * nc + cy) * nc;
+#pragma unroll
+            for (int dx = -1; dx <= 1; dx++) {
+                int cx = ci[0] + dx;
+                cx += (cx < 0) ? nc : 0;
+                cx -= (cx >= nc) ? nc : 0;
+                const int64_t gc = rowbase + cx;
+                int m = __ldg(cnt + gc);
+                m = m < A.depth ? m : A.depth;
+                const R *__restrict__ cr = rec + (gc << A.log_depth);
+                FT off[3];
+                off[0] = (FT)dx * hf;
+                off[1] = (FT)dy * hf;
+                off[2] = (FT)dz * hf;
+                for (int j = 0; j < m; j++) {
+                    R r;
+                    int bj;
+                    FT sep[3];
+                    if constexpr (sizeof(FT) == 4) {
+                        r = __ldg(cr + j);
+                        sep[0] = (r.x - own[0]) + off[0];
+                        sep[1] = (r.y - own[1]) + off[1];
+                        if (D == 3) sep[2] = (r.z - own[2]) + off[2];
+                        bj = __float_as_int(r.w);
+                    } else {
+                        const double *q = reinterpret_cast<const double *>(cr + j);
+                        sep[0] = inbounds(__ldg(q + 0), xb[0], p.half_L, p.L);
+                        sep[1] = inbounds(__ldg(q + 1), xb[1], p.half_L, p.L);
+                        if (D == 3) sep[2] = inbounds(__ldg(q + 2), xb[2], p.half_L, p.L);
+                        bj = (int)__ldg(q + 3);
+                    }
+                    FT ds = FT(0);
+#pragma unroll
+                    for (int i = 0; i < D; i++) ds += sep[i] * sep[i];
+                    if (FT(0) < ds && ds <= rc2) {
+                        int db = b - bj;
+                        db = db < 0 ? -db : db;
+                        if ((nn < 0 || db <= nn) && __ldg(p.chain + bj) == my_chain) continue;
+                        if (shift != FT(0)) {
+                            FT mag = sqrt(ds);
+                            FT nm = mag + shift;
+                            nm = nm < FT(0) ? FT(0) : nm;
+                            FT rs = nm / mag;
+#pragma unroll
+                            for (int i = 0; i < D; i++) sep[i] *= rs;
+                            ds = nm * nm;
+                        }
+                        FT coeff = wca_coeff<FT>(ds, p0, p1);
+#pragma unroll
+                        for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
+                    }
+                }
+            }
+        }
+    }
+}
+
+template <int D>
+__device__ __forceinline__ bool bin_bead(const SysP &p, const BatchArgs &A, int *cnt, const double *x, int b)
+{
+    int c[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < D; i++) c[i] = cell_coord(x[i], p.inv_h, p.nc);
+    int64_t gc = p.cell_off + ((int64_t)c[2] * p.nc + c[1]) * p.nc + c[0];
+    int slot = atomicAdd(cnt + gc, 1);
+    if (slot < A.depth) {
+        A.items[(gc << A.log_depth) + slot] = b;
+        return true;
+    }
+    return false;
+}
+
+template <int D, typename FT>
+__device__ __forceinline__ void noise_trans(const SysP &p, const SysS &s, int b, FT *xi)
+{
+    if (s.noise) {
+        const double *q = s.noise + ((size_t)s.steps_done * p.n + b) * 2 * D;
+#pragma unroll
+        for (int i = 0; i < D; i++) xi[i] = (FT)q[i];
+    } else {
+        double z[D];
+        philox_normals<D>(p.seed, (uint32_t)b, s.step, false, z);
+#pragma unroll
+        for (int i = 0; i < D; i++) xi[i] = (FT)z[i];
+    }
+}
+
+template <int D, typename FT>
+__device__ __forceinline__ void noise_rot(const SysP &p, const SysS &s, int b, FT *xi)
+{
+    if (s.noise) {
+        const double *q = s.noise + ((size_t)s.steps_done * p.n + b) * 2 * D + D;
+#pragma unroll
+        for (int i = 0; i < D; i++) xi[i] = (FT)q[i];
+    } else {
+        double z[D];
+        philox_normals<D>(p.seed, (uint32_t)b, s.step, true, z);
+#pragma unroll
+        for (int i = 0; i < D; i++) xi[i] = (FT)z[i];
+    }
+}
+
+// pos + dt_eff F + s2 xi, wrapped; FP64 in the reference's operation order,
+// mixed: the increment in FP32 and the accumulation in FP64
+template <typename FT>
+__device__ __forceinline__ double srk_update(double x, double dt_eff, double s2, FT f, FT xi, double L)
+{
+    double tmp;
+    if constexpr (sizeof(FT) == 8) {
+        tmp = x + dt_eff * f;
+        if (s2 != 0.0) tmp += s2 * xi;
+    } else {
+        float inc = (float)dt_eff * f + (float)s2 * xi;
+        tmp = x + (double)inc;
+    }
+    return py_mod(tmp, L);
+}
+
+// ------------------------------------------------------------------------
+// kernels
+// ------------------------------------------------------------------------
+template <int D>
+__global__ void __launch_bounds__(512) k_insert(BatchArgs A)
+{
+    const int nt = *A.n_bead_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.bead_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        SysS &s = A.S[tl.sys];
+        if (!s.active || !p.calc_wca) continue;
+        int b = tl.begin + threadIdx.x;
+        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
+        double x[3];
+#pragma unroll
+        for (int i = 0; i < D; i++) x[i] = p.pos[(size_t)b * D + i];
+        if (!bin_bead<D>(p, A, A.cnt0, x, b)) atomicOr(&s.flags, kFlagCellOverflow);
+    }
+}
+
+template <int D, typename FT, int WHICH>
+__global__ void __launch_bounds__(512) k_pack(BatchArgs A)
+{
+    using R = typename Rec<FT>::type;
+    R *rec = reinterpret_cast<R *>(A.rec);
+    const int nt = *A.n_cell_tiles;
+    int *cnt = WHICH == 0 ? A.cnt0 : A.cnt1;
+    int *other = WHICH == 0 ? A.cnt1 : A.cnt0;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.cell_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        const SysS &s = A.S[tl.sys];
+        bool run = s.active && p.calc_wca && (WHICH == 0 || !(s.flags & kFlagCellOverflow));
+        if (!run) continue;
+        int c = tl.begin + threadIdx.x;
+        if (c >= p.n_cells || threadIdx.x >= A.tile_cells) continue;
+        const int64_t gc = p.cell_off + c;
+        int n = cnt[gc];
+        n = n < A.depth ? n : A.depth;
+        other[gc] = 0;
+        int *it = A.items + (gc << A.log_depth);
+        const double *X = WHICH == 0 ? p.pos : p.pos1;
+        int cc[3];
+        cc[0] = c % p.nc;
+        cc[1] = (c / p.nc) % p.nc;
+        cc[2] = (D == 3) ? c / (p.nc * p.nc) : 0;
+        double ctr[3];
+#pragma unroll
+        for (int i = 0; i < 3; i++) ctr[i] = ((double)cc[i] + 0.5) * p.h;
+        R *out = rec + (gc << A.log_depth);
+        auto emit = [&](int j, int b) {
+            double x[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int i = 0; i < D; i++) x[i] = X[(size_t)b * D + i];
+            R r;
+            if constexpr (sizeof(FT) == 4) {
+                r.x = (float)(x[0] - ctr[0]);
+                r.y = (float)(x[1] - ctr[1]);
+                r.z = (D == 3) ? (float)(x[2] - ctr[2]) : 0.f;
+                r.w = __int_as_float(b);
+            } else {
+                r.x = x[0];
+                r.y = x[1];
+                r.z = x[2];
+                r.w = (double)b;
+            }
+            out[j] = r;
+        };
+        if (n <= 8) {
+            int v[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) v[j] = j < n ? it[j] : 0x7fffffff;
+            // Batcher odd-even merge sort network for 8 keys (19 comparators)
+#define GCR_CX(a, b)                 \
+    {                                \
+        int lo = min(v[a], v[b]);    \
+        int hi = max(v[a], v[b]);    \
+        v[a] = lo;                   \
+        v[b] = hi;                   \
+    }
+            GCR_CX(0, 1) GCR_CX(2, 3) GCR_CX(4, 5) GCR_CX(6, 7)
+            GCR_CX(0, 2) GCR_CX(1, 3) GCR_CX(4, 6) GCR_CX(5, 7)
+            GCR_CX(1, 2) GCR_CX(5, 6)
+            GCR_CX(0, 4) GCR_CX(1, 5) GCR_CX(2, 6) GCR_CX(3, 7)
+            GCR_CX(2, 4) GCR_CX(3, 5)
+            GCR_CX(1, 2) GCR_CX(3, 4) GCR_CX(5, 6)
+#undef GCR_CX
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+                if (j < n) emit(j, v[j]);
+        } else {
+            // insertion sort in place (cells this dense are rare)
+            for (int j = 1; j < n; j++) {
+                int key = it[j];
+                int q = j - 1;
+                while (q >= 0 && it[q] > key) {
+                    it[q + 1] = it[q];
+                    q--;
+                }
+                it[q + 1] = key;
+            }
+            for (int j = 0; j < n; j++) emit(j, it[j]);
+        }
+    }
+}
+
+template <int D, typename FT, int STAGE>
+__global__ void __launch_bounds__(512) k_stage(BatchArgs A)
+{
+    __shared__ unsigned long long sh_bits[32];
+    const int nt = *A.n_bead_tiles;
+    const int *cnt = STAGE == 0 ? A.cnt0 : A.cnt1;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.bead_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        SysS &s = A.S[tl.sys];
+        bool run = s.active && (STAGE == 0 || !(s.flags & kFlagCellOverflow));
+        if (!run) continue;
+        const int b = tl.begin + threadIdx.x;
+        double mf2 = 0.0;
+        if (b < p.n && threadIdx.x < A.tile_beads) {
+            const double *__restrict__ X = STAGE == 0 ? p.pos : p.pos1;
+            FT *frc = reinterpret_cast<FT *>(p.frc);
+            FT *tan = reinterpret_cast<FT *>(p.tan);
+            double xb[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int i = 0; i < D; i++) xb[i] = __ldg(X + (size_t)b * D + i);
+            FT F[3], tg[3];
+#pragma unroll
+            for (int i = 0; i < D; i++) {
+                F[i] = STAGE == 0 ? FT(0) : frc[(size_t)b * D + i];
+                tg[i] = tan[(size_t)b * D + i];
+            }
+            bool tang_set = false;
+            if (p.calc_springs) bonded<D, FT>(p, A.topo[p.bead_off + b], X, b, F, tg, tang_set);
+            if (p.calc_wca) pair_forces<D, FT>(p, A, cnt, b, xb, F);
+            if (p.self_propel) {
+                const FT v0 = (FT)p.v0;
+                if (p.rotate_prop) {
+                    const FT cs = (FT)p.cos_a, sn = (FT)p.sin_a;
+                    FT fx = v0 * (cs * tg[0] - sn * tg[1]);
+                    FT fy = v0 * (sn * tg[0] + cs * tg[1]);
+                    F[0] += fx;
+                    F[1] += fy;
+                } else {
+#pragma unroll
+                    for (int i = 0; i < D; i++) F[i] += v0 * tg[i];
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < D; i++) frc[(size_t)b * D + i] = F[i];
+            if (tang_set) {
+#pragma unroll
+                for (int i = 0; i < D; i++) tan[(size_t)b * D + i] = tg[i];
+            }
+            if (STAGE == 0) {
+                // predictor: pos1 = (pos + dt/r F0 + sqrt(2 D dt) xi) mod L
+                FT xi[3] = {FT(0), FT(0), FT(0)};
+                if (p.D > 0.0) noise_trans<D, FT>(p, s, b, xi);
+                const double dt = s.dt;
+                const double dt_eff = dt * 1.0 / p.radius;
+                const double s2 = sqrt(2.0 * dt * p.D);
+                double x1[3] = {0.0, 0.0, 0.0};
+                bool finite = true;
+#pragma unroll
+                for (int i = 0; i < D; i++) {
+                    x1[i] = srk_update<FT>(xb[i], dt_eff, s2, F[i], xi[i], p.L);
+                    finite &= isfinite(x1[i]);
+                    p.pos1[(size_t)b * D + i] = x1[i];
+                }
+                if (!finite) atomicOr(&s.flags, kFlagNonFinite);
+                if (p.calc_wca && !bin_bead<D>(p, A, A.cnt1, x1, b))
+                    atomicOr(&s.flags, kFlagCellOverflow);
+            } else {
+                // |F0+F1|^2 in FP64 for the dt rule (SRK.py:328)
+                double acc = 0.0;
+#pragma unroll
+                for (int i = 0; i < D; i++) acc += (double)F[i] * (double)F[i];
+                mf2 = acc;
+            }
+        }
+        if (STAGE == 1) {
+            // warp / block max over non-negative doubles via their bit patterns
+            unsigned long long bits = (unsigned long long)__double_as_longlong(mf2);
+            for (int o = 16; o > 0; o >>= 1) {
+                unsigned long long other = __shfl_xor_sync(0xffffffffu, bits, o);
+                bits = other > bits ? other : bits;
+            }
+            if ((threadIdx.x & 31) == 0) sh_bits[threadIdx.x >> 5] = bits;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                unsigned long long m = 0;
+                for (int w = 0; w < (blockDim.x + 31) / 32; w++) m = sh_bits[w] > m ? sh_bits[w] : m;
+                atomicMax(&s.max_f2, m);
+                __threadfence();
+                unsigned prev = atomicAdd(&s.tile_ctr[0], 1u);
+                if (prev == (unsigned)p.n_bead_tiles - 1u) {
+                    __threadfence();
+                    // last tile of this system: dt rule (SRK.py:323-353)
+                    double mf2s = __longlong_as_double(atomicAdd(&s.max_f2, 0ull));
+                    double S = p.sqrt2D + 0.5 * sqrt(mf2s) / p.radius;
+                    double dt;
+                    if (S == 0.0)
+                        dt = p.dtmax;
+                    else {
+                        double q = p.mdps / S;
+                        dt = (q < p.dtmax) ? q : p.dtmax;
+                    }
+                    double dt_used = p.rk * dt;
+                    if (s.max_dt_usable > 0.0) {
+                        double lim = s.max_dt_usable - s.elapsed;
+                        dt_used = (lim < dt_used) ? lim : dt_used;
+                    }
+                    s.dt_next = dt;
+                    s.dt_used = dt_used;
+                    s.mfs = S;
+                    s.tile_ctr[0] = 0u;
+                    __threadfence();
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <int D, typename FT>
+__global__ void __launch_bounds__(512) k_update(BatchArgs A)
+{
+    const int nt = *A.n_bead_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.bead_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        SysS &s = A.S[tl.sys];
+        bool run = s.active && !(s.flags & kFlagCellOverflow);
+        if (!run) continue;
+        const int b = tl.begin + threadIdx.x;
+        if (b < p.n && threadIdx.x < A.tile_beads) {
+            const FT *frc = reinterpret_cast<const FT *>(p.frc);
+            const double dtu = s.dt_used;
+            const double dt_eff = dtu * 0.5 / p.radius;
+            const double s2 = sqrt(2.0 * dtu * p.D);
+            FT xi[3] = {FT(0), FT(0), FT(0)};
+            if (p.D > 0.0) noise_trans<D, FT>(p, s, b, xi);
+            double x[3] = {0.0, 0.0, 0.0};
+            bool finite = true;
+#pragma unroll
+            for (int i = 0; i < D; i++) {
+                x[i] = srk_update<FT>(p.pos[(size_t)b * D + i], dt_eff, s2, frc[(size_t)b * D + i], xi[i], p.L);
+                finite &= isfinite(x[i]);
+                p.pos[(size_t)b * D + i] = x[i];
+            }
+            if (!finite) atomicOr(&s.flags, kFlagNonFinite);
+            if (p.Dr > 0.0 && !p.get_orient) {
+                // rotational diffusion, SRK.py:399-423 (note the factor pi)
+                FT xr[3] = {FT(0), FT(0), FT(0)};
+                noise_rot<D, FT>(p, s, b, xr);
+                FT *tan = reinterpret_cast<FT *>(p.tan);
+                FT tb[3];
+#pragma unroll
+                for (int i = 0; i < D; i++) tb[i] = tan[(size_t)b * D + i];
+                const FT sq = (FT)(sqrt(2.0 * dtu * p.Dr) * 3.141592653589793);
+                FT proj = FT(0);
+#pragma unroll
+                for (int i = 0; i < D; i++) proj += xr[i] * tb[i];
+#pragma unroll
+                for (int i = 0; i < D; i++) xr[i] -= proj * tb[i];
+                FT mag = FT(0);
+#pragma unroll
+                for (int i = 0; i < D; i++) {
+                    FT v = tb[i] + sq * xr[i];
+                    mag += v * v;
+                    tb[i] = v;
+                }
+                mag = sqrt(mag);
+#pragma unroll
+                for (int i = 0; i < D; i++) tan[(size_t)b * D + i] = tb[i] / mag;
+            }
+            if (p.calc_wca && !bin_bead<D>(p, A, A.cnt0, x, b)) atomicOr(&s.flags, kFlagNextOverflow);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            unsigned prev = atomicAdd(&s.tile_ctr[1], 1u);
+            if (prev == (unsigned)p.n_bead_tiles - 1u) {
+                __threadfence();
+                // last tile: step bookkeeping (SRK.py:330, 348-349, 128-130)
+                s.dt = s.dt_next;
+                s.elapsed += s.dt_used;
+                s.step += 1;
+                s.steps_done += 1;
+                s.max_f2 = 0ull;
+                int fl = atomicOr(&s.flags, 0);
+                bool more = (s.steps_done < s.max_steps || s.max_steps < 0) &&
+                            (s.elapsed < s.max_dt_usable || s.max_dt_usable < 0.0) &&
+                            !(fl & (kFlagCellOverflow | kFlagNextOverflow));
+                s.active = more ? 1 : 0;
+                s.tile_ctr[1] = 0u;
+                __threadfence();
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// chain-neighbour bits of every bead of one system
+__global__ void k_topo(const int32_t *__restrict__ chain, int n, uint8_t *topo)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    int c = chain[b];
+    uint8_t t = 0;
+    if (b >= 1 && chain[b - 1] == c) t |= kHasPrev;
+    if (b >= 2 && chain[b - 2] == c) t |= kHasPrev2;
+    if (b + 1 < n && chain[b + 1] == c) t |= kHasNext;
+    if (b + 2 < n && chain[b + 2] == c) t |= kHasNext2;
+    topo[b] = t;
+}
+
+// ------------------------------------------------------------------------
+// launchers
+// ------------------------------------------------------------------------
+template <int D, typename FT>
+struct StepKernels {
+    static void *insert() { return (void *)k_insert<D>; }
+    static void *pack0() { return (void *)k_pack<D, FT, 0>; }
+    static void *pack1() { return (void *)k_pack<D, FT, 1>; }
+    static void *stage0() { return (void *)k_stage<D, FT, 0>; }
+    static void *stage1() { return (void *)k_stage<D, FT, 1>; }
+    static void *update() { return (void *)k_update<D, FT>; }
+};
+
+KernelSet kernel_set(int dim, int precision)
+{
+    KernelSet k{};
+#define GCR_FILL(D_, FT_)                           \
+    k.insert = StepKernels<D_, FT_>::insert();      \
+    k.pack0 = StepKernels<D_, FT_>::pack0();        \
+    k.pack1 = StepKernels<D_, FT_>::pack1();        \
+    k.stage0 = StepKernels<D_, FT_>::stage0();      \
+    k.stage1 = StepKernels<D_, FT_>::stage1();      \
+    k.update = StepKernels<D_, FT_>::update();
+    if (dim == 2 && precision == 0) {
+        GCR_FILL(2, double)
+    } else if (dim == 2) {
+        GCR_FILL(2, float)
+    } else if (precision == 0) {
+        GCR_FILL(3, double)
+    } else {
+        GCR_FILL(3, float)
+    }
+#undef GCR_FILL
+    k.topo = (void *)k_topo;
+    return k;
+}
+
+}  // namespace gcr

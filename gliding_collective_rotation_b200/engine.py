@@ -1,0 +1,297 @@
+"""Torch-facing wrapper of one ``libgcr`` context.
+
+State of every system lives in torch CUDA tensors that the context binds by
+device pointer (``gcr_admit``); the context owns only its scratch.  An
+``Engine`` can hold one system (the drop-in ``SRK2_force_calc`` path) or many
+systems of different sizes (batched sweeps, serving).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import Call, Config, GcrError, Status, SystemBuffers, SystemDesc, check
+
+PRECISIONS = {"fp64": _lib.GCR_FP64, "mixed": _lib.GCR_MIXED}
+
+
+@dataclass
+class SystemParams:
+    """One system's parameters, packed the way the reference packs them.
+
+    ``spring_params`` = Chain_Collection.spring_params() (populations.py:345-353),
+    ``wca_params`` = make_WCA_params(...) (populations.py:48-58),
+    ``active_params`` = Chain_Collection.active_params() (populations.py:355-358).
+    """
+    L: float
+    spring_params: np.ndarray
+    wca_params: np.ndarray
+    active_params: np.ndarray
+    D: float
+    Dr: float
+    radius: float
+    n_nearby: int
+    calc_springs: bool = True
+    calc_wca: bool = True
+    self_propel: bool = True
+    dtmax: float = 1e-3
+    max_dist_per_step: float = math.inf
+    rk_cheat: float = 1.0
+    seed: int = 0
+    step: int = 0
+    cell_factor: float = 1.0
+
+    def desc(self, n_beads, n_chains):
+        d = SystemDesc()
+        d.n_beads, d.n_chains, d.L = int(n_beads), int(n_chains), float(self.L)
+        for i in range(6):
+            d.spring_params[i] = float(self.spring_params[i])
+        for i in range(4):
+            d.wca_params[i] = float(self.wca_params[i])
+        for i in range(3):
+            d.active_params[i] = float(self.active_params[i])
+        d.calc_springs, d.calc_wca = int(bool(self.calc_springs)), int(bool(self.calc_wca))
+        d.self_propel, d.n_nearby = int(bool(self.self_propel)), int(self.n_nearby)
+        d.D, d.Dr, d.radius = float(self.D), float(self.Dr), float(self.radius)
+        d.dtmax, d.max_dist_per_step, d.rk_cheat = float(self.dtmax), float(self.max_dist_per_step), \
+            float(self.rk_cheat)
+        d.seed, d.step, d.cell_factor = int(self.seed) & (2 ** 64 - 1), int(self.step), float(self.cell_factor)
+        return d
+
+
+@dataclass
+class SystemState:
+    """Device state of one system (bead order, chains contiguous)."""
+    pos: torch.Tensor            # float64 [n, d]
+    pos1: torch.Tensor           # float64 [n, d]
+    tangent: torch.Tensor        # float64 | float32 [n, d]
+    forces: torch.Tensor         # float64 | float32 [n, d]
+    chain_id: torch.Tensor       # int32 [n]
+    rest_lengths: torch.Tensor   # float64 [n_chains]
+    params: SystemParams
+    slot: int = -1
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def n(self):
+        return self.pos.shape[0]
+
+    @property
+    def n_chains(self):
+        return self.rest_lengths.shape[0]
+
+    @staticmethod
+    def from_host(pos, tangent, chain_id, rest_lengths, params, precision="fp64", device="cuda"):
+        ft = torch.float64 if precision == "fp64" else torch.float32
+        pos_t = torch.as_tensor(np.ascontiguousarray(pos), dtype=torch.float64, device=device)
+        chain = np.asarray(chain_id)
+        if np.any(np.diff(chain) < 0):
+            raise ValueError("chains must be contiguous, increasing ranges of beads")
+        return SystemState(
+            pos=pos_t.clone(),
+            pos1=torch.zeros_like(pos_t),
+            tangent=torch.as_tensor(np.ascontiguousarray(tangent), dtype=ft, device=device).clone(),
+            forces=torch.zeros(pos_t.shape, dtype=ft, device=device),
+            chain_id=torch.as_tensor(chain.astype(np.int32), device=device),
+            rest_lengths=torch.as_tensor(np.asarray(rest_lengths, dtype=np.float64), device=device).clone(),
+            params=params)
+
+    def buffers(self):
+        b = SystemBuffers()
+        b.pos, b.pos1 = self.pos.data_ptr(), self.pos1.data_ptr()
+        b.tangent, b.forces = self.tangent.data_ptr(), self.forces.data_ptr()
+        b.chain_id, b.rest_lengths = self.chain_id.data_ptr(), self.rest_lengths.data_ptr()
+        return b
+
+
+def default_config(dim, precision="fp64", bead_capacity=1 << 20, system_capacity=1,
+                   cell_capacity=None, cell_depth=None, block_beads=256, block_cells=256,
+                   steps_per_graph=10, ctas_per_sm=0):
+    cfg = Config()
+    cfg.dim = dim
+    cfg.precision = PRECISIONS[precision]
+    cfg.bead_capacity = int(bead_capacity)
+    cfg.system_capacity = int(system_capacity)
+    cfg.cell_capacity = int(cell_capacity if cell_capacity is not None else 4 * bead_capacity)
+    cfg.cell_depth = int(cell_depth if cell_depth is not None else (16 if dim == 2 else 32))
+    cfg.block_beads, cfg.block_cells = int(block_beads), int(block_cells)
+    cfg.steps_per_graph, cfg.ctas_per_sm = int(steps_per_graph), int(ctas_per_sm)
+    return cfg
+
+
+def footprint(cfg, params, n_beads, n_chains):
+    cells, byts = C.c_int64(), C.c_int64()
+    check(_lib.load().gcr_footprint(C.byref(cfg), C.byref(params.desc(n_beads, n_chains)), C.byref(cells),
+                                    C.byref(byts)))
+    return cells.value, byts.value
+
+
+class Engine:
+    """A ``gcr_ctx``: scratch for up to ``system_capacity`` resident systems."""
+
+    def __init__(self, dim, precision="fp64", device=None, stream=None, **cfg_kwargs):
+        if not torch.cuda.is_available():
+            raise GcrError(-2, "no CUDA device: the gcr hot path runs on the GPU only")
+        self.lib = _lib.load()
+        self.dim = dim
+        self.precision = precision
+        self.device = torch.device(device or "cuda")
+        self.cfg = default_config(dim, precision, **cfg_kwargs)
+        self.stream = stream or torch.cuda.Stream(device=self.device)
+        self._ctx = C.c_void_p()
+        with torch.cuda.device(self.device):
+            check(self.lib.gcr_create(C.byref(self.cfg), C.c_void_p(self.stream.cuda_stream),
+                                      C.byref(self._ctx)))
+        self.systems = {}
+
+    # -- lifecycle ---------------------------------------------------------
+    def close(self):
+        if self._ctx:
+            self.lib.gcr_destroy(self._ctx)
+            self._ctx = C.c_void_p()
+            self.systems.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- systems -------------------------------------------------------------
+    def admit(self, st: SystemState):
+        torch.cuda.current_stream(self.device).synchronize()
+        slot = C.c_int32()
+        check(self.lib.gcr_admit(self._ctx, C.byref(st.params.desc(st.n, st.n_chains)), C.byref(st.buffers()),
+                                 C.byref(slot)))
+        st.slot = slot.value
+        self.systems[st.slot] = st
+        return st.slot
+
+    def try_admit(self, st: SystemState):
+        try:
+            return self.admit(st)
+        except GcrError as e:
+            if e.code == -6:
+                return None
+            raise
+
+    def evict(self, slot):
+        check(self.lib.gcr_evict(self._ctx, int(slot)))
+        st = self.systems.pop(int(slot), None)
+        if st is not None:
+            st.slot = -1
+
+    def update_params(self, st: SystemState):
+        check(self.lib.gcr_update_desc(self._ctx, st.slot, C.byref(st.params.desc(st.n, st.n_chains))))
+
+    def call_begin(self, slot, max_steps, dt, max_dt_usable=-1.0, noise=None):
+        """Arm one system for the next ``run``: the arguments of one
+        ``SRK2_force_calc`` call (updates.py:138-146)."""
+        c = Call()
+        c.max_steps, c.max_dt_usable, c.dt = int(max_steps), float(max_dt_usable), float(dt)
+        if noise is not None:
+            assert noise.dtype == torch.float64 and noise.is_cuda and noise.is_contiguous()
+            c.noise, c.noise_steps = noise.data_ptr(), noise.shape[0]
+            self.systems[slot].extra["noise_ref"] = noise  # keep alive while in use
+        else:
+            c.noise, c.noise_steps = None, 0
+        torch.cuda.current_stream(self.device).synchronize()
+        check(self.lib.gcr_call_begin(self._ctx, int(slot), C.byref(c)))
+
+    def call_begin_many(self, slots, max_steps, dts, max_dt_usable=-1.0):
+        """Arm many systems with one copy of the state table each way."""
+        n = len(slots)
+        calls = (Call * n)()
+        arr = (C.c_int32 * n)(*[int(s) for s in slots])
+        for i in range(n):
+            calls[i].max_steps = int(max_steps[i] if np.ndim(max_steps) else max_steps)
+            calls[i].max_dt_usable = float(max_dt_usable[i] if np.ndim(max_dt_usable) else max_dt_usable)
+            calls[i].dt = float(dts[i] if np.ndim(dts) else dts)
+            calls[i].noise, calls[i].noise_steps = None, 0
+        torch.cuda.current_stream(self.device).synchronize()
+        check(self.lib.gcr_call_begin_batch(self._ctx, n, arr, calls))
+
+    # -- stepping ------------------------------------------------------------
+    def run(self, max_steps, sync_every=0):
+        check(self.lib.gcr_run(self._ctx, int(max_steps), int(sync_every)))
+
+    def synchronize(self):
+        check(self.lib.gcr_synchronize(self._ctx))
+
+    def profile_steps(self, n_steps):
+        """Milliseconds per kernel type over ``n_steps`` individually launched
+        steps: [pack(pos), stage 0, pack(pos1), stage 1, update]."""
+        out = (C.c_float * 5)()
+        check(self.lib.gcr_profile_steps(self._ctx, int(n_steps), out))
+        return np.array(out[:], dtype=np.float64)
+
+    def count_active(self):
+        n = C.c_int32()
+        check(self.lib.gcr_count_active(self._ctx, C.byref(n)))
+        return n.value
+
+    def status(self, slot):
+        s = Status()
+        check(self.lib.gcr_get_status(self._ctx, int(slot), C.byref(s)))
+        return {"dt": s.dt, "dt_used": s.dt_used, "max_forces_strength": s.max_forces_strength,
+                "steps_done": s.steps_done, "step": s.step, "flags": s.flags, "active": bool(s.active)}
+
+    # -- observables and exports --------------------------------------------
+    def order_params(self, slot):
+        out = (C.c_double * 3)()
+        check(self.lib.gcr_order_params(self._ctx, int(slot), out))
+        return np.array(out[:])
+
+    def reference_lists(self, slot, n_grid, grid_window, grid_depth1=None, nbor_depth1=9, mode=1):
+        """The reference's where_is_bead / grid_list / nbor_list, built on the
+        device; depths double on overflow as populations.py:104-112, 176-180 do."""
+        st = self.systems[slot]
+        n = st.n
+        nz = 1 if self.dim == 2 else n_grid
+        if grid_depth1 is None:
+            grid_depth1 = 1 + max(1, int(8 * n / n_grid ** self.dim))
+        dev = st.pos.device
+        while True:
+            wib = torch.zeros((n, 3), dtype=torch.int64, device=dev)
+            grid = torch.zeros((n_grid, n_grid, nz, grid_depth1), dtype=torch.int64, device=dev)
+            nb = torch.zeros((n, nbor_depth1), dtype=torch.int64, device=dev)
+            torch.cuda.current_stream(dev).synchronize()
+            rc = self.lib.gcr_reference_lists(self._ctx, int(slot), int(n_grid), int(grid_window),
+                                              wib.data_ptr(), grid.data_ptr(), grid_depth1, nb.data_ptr(),
+                                              nbor_depth1, int(mode))
+            if rc == 0:
+                return wib, grid, nb
+            msg = self.lib.gcr_last_error().decode()
+            if rc != -8:
+                raise GcrError(rc, msg)
+            if "grid" in msg:
+                grid_depth1 = 2 * grid_depth1
+            else:
+                nbor_depth1 = 2 * nbor_depth1
+
+    def cell_assignment(self, slot):
+        st = self.systems[slot]
+        out = torch.empty(st.n, dtype=torch.int32, device=st.pos.device)
+        ncs = C.c_int32()
+        torch.cuda.current_stream(st.pos.device).synchronize()
+        check(self.lib.gcr_cell_assignment(self._ctx, int(slot), out.data_ptr(), C.byref(ncs)))
+        return out, ncs.value
+
+
+def philox_noise(dim, seed, step, n, do_trans=True, do_rot=True, device="cuda"):
+    out = torch.zeros((n, 2 * dim), dtype=torch.float64, device=device)
+    torch.cuda.current_stream().synchronize()
+    check(_lib.load().gcr_philox_noise(dim, int(seed) & (2 ** 64 - 1), int(step), int(n), int(do_trans),
+                                       int(do_rot), out.data_ptr(), None))
+    return out

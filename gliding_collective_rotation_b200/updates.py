@@ -1,0 +1,233 @@
+"""``SRK2_force_calc(pops, status, sim)`` on the B200: the drop-in step.
+
+Same signature, inputs, outputs and bookkeeping as the reference's
+``updates.SRK2_force_calc`` (updates.py:132-267):
+
+* runs up to ``status.next_output_step - status.stepnum`` SRK2 steps, stops
+  early when the elapsed time reaches ``status.next_save_time - status.t``
+  (if saving) -- SRK.py:128-130, 345-346;
+* writes back ``status.dt`` (last dt), ``status.dt_used`` (time elapsed in the
+  call), ``status.stepnum``, ``status.t``, ``status.max_forces_strength`` and
+  ``status.update_grid_list_counter`` -- updates.py:249-256;
+* leaves the population's ``pos``, ``pos1``, ``tangent_list`` and ``forces``
+  as the reference leaves them (F0 + F1 of the last step, tangents at pos1);
+* raises no exception for numerical trouble: a GPU cell overflow makes the
+  next call use deeper cells (the reference regrows its lists the same way,
+  updates.py:257-267) and non-finite values are reported in
+  ``status.gpu_flags``.
+
+The bead state stays on the device between calls; each call uploads the
+host arrays (the caller may have changed them) and downloads the result.
+Features outside the GPU path (walls, motors, rigid rods, FENE, active
+sliding, E-field, SRK4, several populations) raise ``NotImplementedError``.
+
+``install(updates_module, config_module)`` rebinds a reference checkout's
+``updates.SRK2_force_calc`` to this function and makes it read that
+checkout's ``config`` module.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import torch
+
+from . import config as _default_config
+from .engine import Engine, SystemParams, SystemState
+
+_config = _default_config
+_pair_rule_check = None
+
+
+def install(updates_module, config_module, force_rules_module=None, forces_module=None):
+    """Use this step inside a reference checkout: ``updates.SRK2_force_calc``
+    becomes the GPU step and reads the checkout's ``config`` globals."""
+    global _config, _pair_rule_check
+    _config = config_module
+    if force_rules_module is not None and forces_module is not None:
+        _pair_rule_check = (force_rules_module, forces_module)
+    updates_module.SRK2_force_calc = SRK2_force_calc
+    return SRK2_force_calc
+
+
+def _force_list(pop):
+    """interpop_forces(pop, pop) (updates.py:274-312) as a dict of name -> params."""
+    if pop.name in getattr(pop, "special_interactions", {}):
+        forces_list = pop.special_interactions[pop.name]
+    else:
+        forces_list = pop.self_interactions()
+    out = {}
+    for name, params in forces_list:
+        out[name] = np.array(params, dtype=np.float64)
+    if getattr(pop, "b_init_growing", False):
+        for name in ("WCA", "active_sliding_and_WCA"):
+            if name in out and out[name][0] != 0:
+                out[name][3] = (out[name][1] / out[name][0]) ** (1 / 6)
+    return out
+
+
+_SUPPORTED = {"springs", "WCA", "self-propulsion"}
+
+
+class _GpuPop:
+    """Device copy of one population and the context that steps it."""
+
+    def __init__(self, pop, sim, dim, precision, params, cell_depth):
+        self.key = (pop.total_pop, len(pop.rest_lengths), dim, precision, float(params.L),
+                    float(params.wca_params[3]), float(params.cell_factor), cell_depth, bool(params.calc_wca))
+        n = pop.total_pop
+        spg = int(sim.get('gpu_steps_per_graph', 10))
+        self.engine = Engine(dim, precision, bead_capacity=max(n, 1), system_capacity=1,
+                             cell_capacity=self._cells(params, dim), cell_depth=cell_depth,
+                             steps_per_graph=spg)
+        self.state = SystemState.from_host(pop.pos, pop.tangent_list, pop.chain_id, pop.rest_lengths, params,
+                                           precision=precision, device=self.engine.device)
+        self.engine.admit(self.state)
+        ft = torch.float64 if precision == "fp64" else torch.float32
+        self.h_pos = torch.empty((n, dim), dtype=torch.float64, pin_memory=True)
+        self.h_tan = torch.empty((n, dim), dtype=ft, pin_memory=True)
+        self.h_frc = torch.empty((n, dim), dtype=ft, pin_memory=True)
+        self.h_pos1 = torch.empty((n, dim), dtype=torch.float64, pin_memory=True)
+        self.rng = None
+
+    @staticmethod
+    def _cells(params, dim):
+        if not params.calc_wca:
+            return 1
+        nc = int(math.floor(params.L / (params.wca_params[3] * max(1.0, params.cell_factor))))
+        return max(nc, 3) ** dim
+
+
+def _gpu_state(pop, sim, dim, precision, params):
+    depth = getattr(pop, "_gcr_cell_depth", 16 if dim == 2 else 32)
+    g = getattr(pop, "_gcr", None)
+    key = (pop.total_pop, len(pop.rest_lengths), dim, precision, float(params.L), float(params.wca_params[3]),
+           float(params.cell_factor), depth, bool(params.calc_wca))
+    if g is None or g.key != key:
+        if g is not None:
+            g.engine.close()
+        g = _GpuPop(pop, sim, dim, precision, params, depth)
+        pop._gcr = g
+    return g
+
+
+def SRK2_force_calc(pops, status, sim):
+    """Stochastic Runge-Kutta 2nd-order update (Branka and Heyes, PRE 60:2381,
+    1999) of one bead-spring-chain population on the GPU."""
+    cfg = _config
+    if getattr(cfg, "SRK_order", 2) != 2:
+        raise NotImplementedError("the GPU step implements SRK_order = 2")
+    if np.any(getattr(cfg, "walls", np.zeros(3, dtype=bool))):
+        raise NotImplementedError("walls are not part of the GPU step")
+    movers = [p for p in pops if not p.fixed]
+    if len(pops) != 1 or len(movers) != 1:
+        raise NotImplementedError("the GPU step advances exactly one population")
+    if _pair_rule_check is not None:
+        fr, fm = _pair_rule_check
+        if fr.central_pair_force_rule is not fm.WCA:
+            raise NotImplementedError("the GPU step implements the forces.WCA pair rule")
+    pop = pops[0]
+    forces = _force_list(pop)
+    extra = set(forces) - _SUPPORTED
+    if extra:
+        raise NotImplementedError(f"forces not on the GPU step: {sorted(extra)}")
+    longest = int(pop.longest_chain_length)
+    if getattr(pop, "rigid_rod_projection_factor", 0) != 0 and longest > 2:
+        raise NotImplementedError("rigid-rod projection is not part of the GPU step")
+    dim = int(cfg.dim)
+    precision = sim.get('gpu_precision', 'fp64')
+    calc_springs = "springs" in forces and longest > 1
+    spring = forces.get("springs", np.zeros(6))
+    if calc_springs and spring[3] != 0:
+        raise NotImplementedError("FENE springs are not part of the GPU step")
+    calc_wca = "WCA" in forces
+    wca = forces.get("WCA", np.zeros(4))
+    self_propel = "self-propulsion" in forces and bool(status.b_calc_active_forces)
+    active = forces.get("self-propulsion", np.zeros(3))
+
+    # time_vals, updates.py:138-146
+    max_dt_usable = (status.next_save_time - status.t) if sim.get('save_state_every', -1) > 0 else -1.0
+    max_steps = status.next_output_step - status.stepnum
+    seed = int(sim.get('seed', 0))
+    params = SystemParams(
+        L=float(cfg.Lx), spring_params=spring, wca_params=wca, active_params=active, D=float(pop.D),
+        Dr=float(pop.Dr), radius=float(pop.repel_d_max), n_nearby=int(pop.n_nearby_beads_dont_repel),
+        calc_springs=calc_springs, calc_wca=calc_wca, self_propel=self_propel, dtmax=float(status.dtmax),
+        max_dist_per_step=float(cfg.max_dist_per_step), rk_cheat=float(cfg.RK_cheat_factor), seed=seed,
+        step=int(status.stepnum), cell_factor=float(sim.get('gpu_cell_factor', 1.0)))
+    g = _gpu_state(pop, sim, dim, precision, params)
+    st, eng = g.state, g.engine
+
+    # upload the host state (the caller may have changed it between calls)
+    g.h_pos.numpy()[:] = pop.pos
+    g.h_tan.numpy()[:] = pop.tangent_list
+    st.pos.copy_(g.h_pos, non_blocking=True)
+    st.tangent.copy_(g.h_tan, non_blocking=True)
+    st.rest_lengths.copy_(torch.from_numpy(np.asarray(pop.rest_lengths, dtype=np.float64)))
+    st.params = params
+    eng.update_params(st)
+
+    noise = None
+    n_noise = 0
+    mode = sim.get('gpu_noise', 'philox')
+    if mode == 'mt':
+        # the reference's MT19937 stream, drawn on the host in SRK.py:134-142 order
+        if g.rng is None:
+            g.rng = np.random.RandomState(seed)
+        if max_steps < 0:
+            raise NotImplementedError("injected noise needs a bounded step count per call")
+        per = st.n * dim * (int(pop.D > 0) + int(pop.Dr > 0))
+        rng_state = g.rng.get_state()
+        flat = g.rng.standard_normal(per * max_steps)
+        snaps = np.zeros((max_steps, st.n, 2 * dim))
+        k = 0
+        for s in range(max_steps):
+            if pop.D > 0:
+                snaps[s, :, :dim] = flat[k:k + st.n * dim].reshape(st.n, dim)
+                k += st.n * dim
+            if pop.Dr > 0:
+                snaps[s, :, dim:] = flat[k:k + st.n * dim].reshape(st.n, dim)
+                k += st.n * dim
+        noise = torch.from_numpy(snaps).to(eng.device)
+        n_noise = max_steps
+    elif mode != 'philox':
+        raise ValueError(f"unknown gpu_noise {mode!r}")
+
+    eng.call_begin(st.slot, max_steps=max_steps, dt=float(status.dt), max_dt_usable=max_dt_usable, noise=noise)
+    if max_steps >= 0 and max_dt_usable < 0:
+        eng.run(max_steps, sync_every=0)
+    else:
+        # time-limited: check between graphs whether the system is done
+        budget = max_steps if max_steps >= 0 else (1 << 62)
+        eng.run(budget, sync_every=1)
+    res = eng.status(st.slot)
+    steps_done = int(res['steps_done'])
+    if mode == 'mt' and steps_done < n_noise:
+        # give back the deviates of steps that did not run
+        g.rng.set_state(rng_state)
+        g.rng.standard_normal(per * steps_done)
+
+    # download into the population's arrays
+    g.h_pos.copy_(st.pos, non_blocking=True)
+    g.h_pos1.copy_(st.pos1, non_blocking=True)
+    g.h_tan.copy_(st.tangent, non_blocking=True)
+    g.h_frc.copy_(st.forces, non_blocking=True)
+    torch.cuda.synchronize(eng.device)
+    pop.pos[:] = g.h_pos.numpy()
+    pop.pos1[:] = g.h_pos1.numpy()
+    pop.tangent_list[:] = g.h_tan.numpy()
+    pop.forces[:] = g.h_frc.numpy()
+
+    # write-back, updates.py:249-256
+    status.dt = res['dt']
+    status.dt_used = res['dt_used']
+    status.stepnum += steps_done
+    status.t += status.dt_used
+    status.max_forces_strength = res['max_forces_strength']
+    status.update_grid_list_counter = max(
+        1, (steps_done + status.update_grid_list_counter) % cfg.n_steps_update_grid_list)
+    status.gpu_flags = res['flags']
+    if res['flags'] & 5:
+        # cell overflow: deeper cells for the next call (updates.py:257-267)
+        pop._gcr_cell_depth = min(64, 2 * getattr(pop, "_gcr_cell_depth", 16 if dim == 2 else 32))
+    return None

@@ -1,0 +1,145 @@
+"""Synthetic workloads with the shapes of the five benchmark configurations.
+
+Initial states follow the reference's placement rule
+(``Chain_Collection.random_initialization``, populations.py:530-557): chain
+heads uniform in the box, chain angles uniform, beads laid straight behind
+the head at the rest length.  Overlapping placements are relaxed before any
+timed step by the step itself under the reference's adaptive dt
+(``relax``).  All randomness is seeded.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from .engine import SystemParams
+from .populations import make_WCA_params
+
+LJ_CUTOFF = 2.5 / 2 ** (1 / 6)  # 2.5 sigma in units of r_WCA = 2^(1/6) sigma
+
+
+@dataclass
+class SystemSpec:
+    name: str
+    dim: int
+    pos: np.ndarray
+    tangent: np.ndarray
+    chain_id: np.ndarray
+    rest_lengths: np.ndarray
+    params: SystemParams
+    dt: float
+    relax_mdps: float
+
+    @property
+    def n(self):
+        return self.pos.shape[0]
+
+
+def lay_chains(rs, n_chains, chain_length, L, a, dim):
+    """Head uniform in [0, L)^dim, direction uniform (on the circle / sphere),
+    beads at head - j a t (populations.py:530-557 with a_init_factor = 1)."""
+    heads = rs.uniform(0.0, L, size=(n_chains, dim))
+    if dim == 2:
+        ang = rs.uniform(0.0, 2 * np.pi, size=n_chains)
+        t = np.stack([np.cos(ang), np.sin(ang)], axis=1)
+    else:
+        phi = rs.uniform(0.0, 2 * np.pi, size=n_chains)
+        ct = rs.uniform(-1.0, 1.0, size=n_chains)
+        st = np.sqrt(1 - ct * ct)
+        t = np.stack([st * np.cos(phi), st * np.sin(phi), ct], axis=1)
+    j = np.arange(chain_length, dtype=np.float64)
+    pos = heads[:, None, :] - a * j[None, :, None] * t[:, None, :]
+    pos = np.mod(pos.reshape(-1, dim), L)
+    tan = np.repeat(t, chain_length, axis=0)
+    chain = np.repeat(np.arange(n_chains), chain_length)
+    return pos, tan, chain
+
+
+def _relax_mdps(a, rc, grid_factor=2.0, n_update=40):
+    # config.grid_list_setup: 0.5 (grid_factor - 1) min_dist / n_steps_update
+    return 0.5 * (grid_factor - 1) * max(2 * a, rc) / n_update
+
+
+def make_system(name, dim, n_chains, chain_length, L, seed, *, a=0.5, k=100.0, kappa=20.0, eps=1.0,
+                cutoff=1.0, v0=1.0, v_tan_angle=0.0, T=0.01, Dr=None, tangent_locked=True, dt=1e-3,
+                noise_seed=None, cell_factor=1.0):
+    rs = np.random.RandomState(seed)
+    pos, tan, chain = lay_chains(rs, n_chains, chain_length, L, a, dim)
+    radius = 1.0
+    D = T / radius
+    if Dr is None:
+        Dr = 3 * D / (4 * radius ** 2)
+    get_orient = tangent_locked and chain_length > 1
+    wca = make_WCA_params(radius, eps, 0.0, cutoff)
+    params = SystemParams(
+        L=L, spring_params=np.array([k, kappa, 0.0, 0.0, float(get_orient), 0.1]), wca_params=wca,
+        active_params=np.array([v0, 0.0, v_tan_angle]), D=D, Dr=Dr, radius=radius, n_nearby=4,
+        calc_springs=chain_length > 1, calc_wca=True, self_propel=True, dtmax=dt, max_dist_per_step=math.inf,
+        rk_cheat=1.0, seed=seed if noise_seed is None else noise_seed, step=0, cell_factor=cell_factor)
+    return SystemSpec(name, dim, pos, tan, chain, np.full(n_chains, a), params, dt, _relax_mdps(a, wca[3]))
+
+
+def config1(seed=0):
+    """2D, Lx=60, 200 x 10 beads, WCA, v0 = 1 tangent-locked, T = 0.01, dt = 1e-3."""
+    return make_system("config1", 2, 200, 10, 60.0, seed)
+
+
+def config2(seed=0, scale=1.0):
+    """2D, Lx=1000, 20,000 x 25 beads, LJ (2.5 sigma, eps 0.5), chiral 0.2."""
+    n_chains = int(round(20000 * scale))
+    L = 1000.0 * math.sqrt(scale)
+    return make_system("config2", 2, n_chains, 25, L, seed, eps=0.5, cutoff=LJ_CUTOFF, v_tan_angle=0.2)
+
+
+def config3(n_systems=256, param_seed=12345, first=0):
+    """Batched sweep: per system n_chains log-uniform [50, 4000], chain length
+    uniform integer [5, 40], area fraction uniform [0.1, 0.4], chirality
+    uniform [-0.5, 0.5], bending uniform [1, 50]; otherwise config 1; the
+    Philox seed of system i is i."""
+    rng = np.random.default_rng(param_seed)
+    nch = np.exp(rng.uniform(np.log(50), np.log(4000), size=n_systems)).astype(int)
+    clen = rng.integers(5, 41, size=n_systems)
+    phi = rng.uniform(0.1, 0.4, size=n_systems)
+    ang = rng.uniform(-0.5, 0.5, size=n_systems)
+    kap = rng.uniform(1.0, 50.0, size=n_systems)
+    out = []
+    for i in range(first, n_systems):
+        a = 0.5
+        # excluded area of a chain r (a (L-1) + r) with r = 1 (config.py:81-82)
+        L = math.sqrt(nch[i] * (a * (clen[i] - 1) + 1.0) / phi[i])
+        out.append(make_system(f"sweep{i}", 2, int(nch[i]), int(clen[i]), L, seed=1000 + i, kappa=float(kap[i]),
+                               v_tan_angle=float(ang[i]), noise_seed=i))
+    return out
+
+
+def config5(seed=0, scale=1.0):
+    """3D, L=200, 40,000 x 25 beads, LJ eps 1 (2.5 sigma), kappa 10,
+    rotationally diffusing propulsion (Dr 0.1), T 0.05, dt 5e-4."""
+    n_chains = int(round(40000 * scale))
+    L = 200.0 * scale ** (1 / 3)
+    return make_system("config5", 3, n_chains, 25, L, seed, kappa=10.0, eps=1.0, cutoff=LJ_CUTOFF, T=0.05,
+                       Dr=0.1, tangent_locked=False, dt=5e-4)
+
+
+def serve_trace(n_requests, rate=20.0, seed=7, min_beads=1000, max_beads=1_000_000, min_steps=1000,
+                max_steps=20000):
+    """Poisson arrivals at `rate`/s of config-3-style systems with bead count
+    log-uniform in [min_beads, max_beads] and a step count uniform in
+    [min_steps, max_steps]."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, size=n_requests))
+    beads = np.exp(rng.uniform(np.log(min_beads), np.log(max_beads), size=n_requests))
+    steps = rng.integers(min_steps, max_steps + 1, size=n_requests)
+    clen = rng.integers(5, 41, size=n_requests)
+    phi = rng.uniform(0.1, 0.4, size=n_requests)
+    ang = rng.uniform(-0.5, 0.5, size=n_requests)
+    kap = rng.uniform(1.0, 50.0, size=n_requests)
+    reqs = []
+    for i in range(n_requests):
+        nch = max(1, int(round(beads[i] / clen[i])))
+        L = math.sqrt(nch * (0.5 * (clen[i] - 1) + 1.0) / phi[i])
+        reqs.append(dict(id=i, arrival=float(t[i]), n_chains=nch, chain_length=int(clen[i]), L=L,
+                         steps=int(steps[i]), kappa=float(kap[i]), v_tan_angle=float(ang[i]), seed=i))
+    return reqs

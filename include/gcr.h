@@ -1,0 +1,197 @@
+/*
+ * gcr.h -- C ABI of libgcr.so, the B200 (sm_100a) hot path of the
+ * gliding-collective-rotation Brownian-dynamics step.
+ *
+ * One context (gcr_ctx) owns the device scratch for up to `system_capacity`
+ * independent bead-spring-chain systems with `bead_capacity` beads in total.
+ * Bead state (positions, tangents, forces, chain ids, rest lengths) lives in
+ * caller-owned device buffers that are bound to a slot at admission; the
+ * library never frees them.  A context is bound to one CUDA stream and is not
+ * thread-safe; separate contexts may be used concurrently.
+ *
+ * Every function returns GCR_OK (0) or a negative GCR_ERR_* code; no C++
+ * exception crosses this boundary.  gcr_last_error() gives a message for the
+ * last failure on the calling thread.
+ *
+ * Reference interfaces replaced (paths inside the reference project):
+ *   gcr_run / gcr_call_begin  <- updates.SRK2_force_calc   updates.py:132-267
+ *                                (the SRK.SRK_jit loop      SRK.py:13-484)
+ *   pair rule                 <- force_rules.central_pair_force_rule = forces.WCA
+ *                                                           force_rules.py:3, forces.py:13-15
+ *   gcr_system_desc packing   <- populations.make_WCA_params populations.py:48-58,
+ *                                Chain_Collection.spring_params populations.py:345-353,
+ *                                Chain_Collection.active_params populations.py:355-358,
+ *                                SRK2_force_calc time_vals / pop_consts updates.py:138-162
+ *   gcr_reference_lists       <- updates.update_grid_list_mini updates.py:502-522 and
+ *                                updates.update_nbor_list   updates.py:586-669
+ *   gcr_order_params          <- output_methods.calc_avg_phi_chain output_methods.py:492-510,
+ *                                analysis.polar_orderparameter analysis.py:315-328,
+ *                                analysis.nematic_orderparameter analysis.py:294-313
+ */
+#ifndef GCR_H
+#define GCR_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GCR_API __attribute__((visibility("default")))
+#else
+#define GCR_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GCR_OK 0
+#define GCR_ERR_BAD_ARG (-1)
+#define GCR_ERR_CUDA (-2)
+#define GCR_ERR_OOM (-3)
+#define GCR_ERR_NONFINITE (-4)
+#define GCR_ERR_TIMEOUT (-5)
+#define GCR_ERR_CAPACITY (-6)
+#define GCR_ERR_STATE (-7)
+#define GCR_ERR_OVERFLOW (-8)
+
+/* precision of forces, tangents and SRK arithmetic (positions are FP64) */
+#define GCR_FP64 0
+#define GCR_MIXED 1
+
+/* per-system device status flags */
+#define GCR_FLAG_CELL_OVERFLOW 1   /* more beads in a cell than cell_depth */
+#define GCR_FLAG_NONFINITE 2       /* a non-finite force or position */
+#define GCR_FLAG_NEXT_OVERFLOW 4   /* overflow while binning for the next step */
+
+typedef struct gcr_ctx gcr_ctx;
+
+typedef struct {
+    int32_t dim;              /* 2 or 3 (every system of a context has it) */
+    int32_t precision;        /* GCR_FP64 or GCR_MIXED */
+    int64_t bead_capacity;    /* beads over all resident systems */
+    int32_t system_capacity;  /* resident systems */
+    int64_t cell_capacity;    /* GPU cells over all resident systems */
+    int32_t cell_depth;       /* bead slots per GPU cell: 8, 16, 32 or 64 */
+    int32_t block_beads;      /* threads per CTA of bead kernels (64..512) */
+    int32_t block_cells;      /* threads per CTA of the cell kernel (64..512) */
+    int32_t steps_per_graph;  /* SRK2 steps per captured CUDA graph (1..64) */
+    int32_t ctas_per_sm;      /* persistent CTAs per SM (0 = from occupancy) */
+} gcr_config;
+
+/* One system.  The packed arrays follow the reference's packing exactly. */
+typedef struct {
+    int64_t n_beads;
+    int64_t n_chains;
+    double L;                   /* periodic box side */
+    double spring_params[6];    /* [k, kappa, theta0, FENE(=0), get_orientations, FENE_tol] */
+    double wca_params[4];       /* [12 eps r^6, 12 eps r^12, shift, r_cut] */
+    double active_params[3];    /* [v0, sliding_partner_maxdist(=0), v_tan_angle] */
+    int32_t calc_springs;       /* "springs" force present and chains longer than 1 */
+    int32_t calc_wca;           /* "WCA" force present */
+    int32_t self_propel;        /* "self-propulsion" present and b_calc_active_forces */
+    int32_t n_nearby;           /* n_nearby_beads_dont_repel (<0: whole chain) */
+    double D, Dr, radius;       /* pop_consts [D, Dr, repel_d_max] */
+    double dtmax, max_dist_per_step, rk_cheat;
+    uint64_t seed;              /* Philox key */
+    int64_t step;               /* global index of the next step (Philox counter) */
+    double cell_factor;         /* GPU cell side >= r_cut * cell_factor (>= 1) */
+} gcr_system_desc;
+
+/* Caller-owned device buffers of one system (bound, not copied). */
+typedef struct {
+    double *pos;                /* [n, dim] FP64 */
+    double *pos1;               /* [n, dim] FP64 predictor positions */
+    void *tangent;              /* [n, dim] FP64 or FP32 (precision) */
+    void *forces;               /* [n, dim] FP64 or FP32 (precision) */
+    const int32_t *chain_id;    /* [n] chain index; chains are contiguous ranges */
+    const double *rest_lengths; /* [n_chains] */
+} gcr_system_buffers;
+
+/* Limits and inputs of one SRK2_force_calc call for one system. */
+typedef struct {
+    int64_t max_steps;          /* next_output_step - stepnum (<0: unlimited) */
+    double max_dt_usable;       /* next_save_time - t; negative: unlimited (SRK.py:128-129) */
+    double dt;                  /* status.dt: predictor dt of the first step */
+    const double *noise;        /* injected noise_vec snapshots [noise_steps][n][2*dim],
+                                   device memory, or NULL for the Philox stream */
+    int64_t noise_steps;
+} gcr_call;
+
+/* What SRK2_force_calc writes back (shared_arr[0], updates.py:249-256). */
+typedef struct {
+    double dt;                  /* most recent dt */
+    double dt_used;             /* time elapsed in the call */
+    double max_forces_strength; /* sqrt(2D) + max|F0+F1| / (2 r) of the last step */
+    int64_t steps_done;         /* steps completed in the call */
+    int64_t step;               /* global index of the next step */
+    int32_t flags;              /* GCR_FLAG_* */
+    int32_t active;             /* still running (limits not reached) */
+} gcr_status;
+
+/* ---- context ---------------------------------------------------------- */
+GCR_API int gcr_create(const gcr_config *cfg, void *cuda_stream, gcr_ctx **out);
+GCR_API int gcr_destroy(gcr_ctx *ctx);
+GCR_API const char *gcr_last_error(void);
+GCR_API int gcr_version(void);
+
+/* ---- systems ---------------------------------------------------------- */
+/* Admit a system: reserves scratch, derives the GPU cell grid, uploads its
+ * descriptor.  Fails with GCR_ERR_CAPACITY when beads, cells or slots do not
+ * fit (the caller queues it). */
+GCR_API int gcr_admit(gcr_ctx *ctx, const gcr_system_desc *desc, const gcr_system_buffers *buf,
+              int32_t *slot_out);
+GCR_API int gcr_evict(gcr_ctx *ctx, int32_t slot);
+/* Replace the parameters of a resident system (same bead and chain counts). */
+GCR_API int gcr_update_desc(gcr_ctx *ctx, int32_t slot, const gcr_system_desc *desc);
+/* Arm a resident system for the next gcr_run (one SRK2_force_calc call). */
+GCR_API int gcr_call_begin(gcr_ctx *ctx, int32_t slot, const gcr_call *call);
+/* Arm `n` resident systems at once (one copy of the state table each way). */
+GCR_API int gcr_call_begin_batch(gcr_ctx *ctx, int32_t n, const int32_t *slots, const gcr_call *calls);
+/* Cells and bytes a system of this description would occupy. */
+GCR_API int gcr_footprint(const gcr_config *cfg, const gcr_system_desc *desc, int64_t *cells_out,
+                  int64_t *bytes_out);
+
+/* ---- stepping --------------------------------------------------------- */
+/* Advance every armed system until its limits are reached or `max_steps`
+ * steps have been launched, through captured CUDA graphs of
+ * steps_per_graph steps.  `sync_every` graphs between checks of whether any
+ * system is still running (0: never check; run exactly ceil(max_steps /
+ * steps_per_graph) graphs).  Asynchronous on the context stream unless a
+ * check is made. */
+GCR_API int gcr_run(gcr_ctx *ctx, int64_t max_steps, int32_t sync_every);
+/* Copy the status of a system to the host (synchronises the stream). */
+GCR_API int gcr_get_status(gcr_ctx *ctx, int32_t slot, gcr_status *out);
+/* Number of armed systems still running (synchronises the stream). */
+GCR_API int gcr_count_active(gcr_ctx *ctx, int32_t *n_out);
+GCR_API int gcr_synchronize(gcr_ctx *ctx);
+/* Run `n_steps` steps launching the five step kernels one by one (not
+ * through the graph) with CUDA events around each on the context stream;
+ * ms_out[0..4] receive the total milliseconds of pack(pos), stage 0,
+ * pack(pos1), stage 1 and update.  For profiling; results equal gcr_run's. */
+GCR_API int gcr_profile_steps(gcr_ctx *ctx, int32_t n_steps, float *ms_out);
+
+/* ---- observables and exports ------------------------------------------ */
+/* [P, S, director_angle] of one system from its tangents, FP64 (host out). */
+GCR_API int gcr_order_params(gcr_ctx *ctx, int32_t slot, double out[3]);
+/* The reference's cell and neighbour lists of one system, built on the
+ * device from its current positions: where_is_bead int64 [n,3], grid_list
+ * int64 [n_grid, n_grid, nz, grid_depth1], nbor_list int64 [n, nbor_depth1]
+ * (device buffers).  Returns GCR_ERR_OVERFLOW when a depth is too small
+ * (the reference then doubles it).  mode 0 picks the neighbour builder as
+ * SRK.py:450 does (all pairs when n < n_grid^dim), 1 the cell-window builder
+ * (updates.update_nbor_list, as populations.py:164 calls it), 2 all pairs
+ * (updates.update_nbor_list_few). */
+GCR_API int gcr_reference_lists(gcr_ctx *ctx, int32_t slot, int64_t n_grid, int64_t grid_window,
+                        int64_t *where_is_bead, int64_t *grid_list, int64_t grid_depth1,
+                        int64_t *nbor_list, int64_t nbor_depth1, int32_t mode);
+/* The GPU cell table of one system after binning its current positions:
+ * cell index per bead (int32 [n], device) and the grid side (host). */
+GCR_API int gcr_cell_assignment(gcr_ctx *ctx, int32_t slot, int32_t *cell_of_bead, int32_t *n_cells_side);
+/* Standard normals of the Philox stream the step draws: [n][2*dim] noise_vec
+ * layout for one step (device out). */
+GCR_API int gcr_philox_noise(int32_t dim, uint64_t seed, int64_t step, int64_t n, int32_t do_trans,
+                     int32_t do_rot, double *out, void *cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GCR_H */
