@@ -53,11 +53,11 @@ def peaks():
 # workloads
 # --------------------------------------------------------------------------
 
-def make_workload(name, rank=0, scale=1.0):
+def make_workload(name, rank=0, scale=1.0, systems=256):
     from gliding_collective_rotation_b200 import workloads as W
     if name == "sweep":
-        specs = W.config3(n_systems=256, param_seed=12345 + rank)
-        desc = ("batched sweep: 256 independent 2D systems, 50-4000 chains of 5-40 beads, area fraction "
+        specs = W.config3(n_systems=256, param_seed=12345 + rank)[:systems]
+        desc = (f"batched sweep: {len(specs)} independent 2D systems, 50-4000 chains of 5-40 beads, area fraction "
                 "0.1-0.4, chirality -0.5..0.5, bending 1..50, WCA r_c=1, T=0.01, dt=1e-3, SRK2")
     elif name == "large":
         specs = [W.config2(seed=rank, scale=scale)]
@@ -152,7 +152,7 @@ def cpu_sample_rate(specs, states_host, steps, threads, max_systems=4, budget_s=
     OpenMP threads over chain-aligned chunks) on the first systems of the
     workload, each run for `steps` steps after an untimed list build."""
     from oracle import oracle as O
-    total_bs, total_t, used = 0, 0.0, []
+    systems = []
     for spec, (pos, tan) in list(zip(specs, states_host))[:max_systems]:
         p = spec.params
         ng = max(1, int(p.L / (2.0 * max(2 * spec.rest_lengths.max(), p.wca_params[3]))))
@@ -160,14 +160,21 @@ def cpu_sample_rate(specs, states_host, steps, threads, max_systems=4, budget_s=
                               p.active_params, p.D, p.Dr, p.radius, p.n_nearby, ng, nbor_depth=32)
         sysm.build_lists(grid_window=1)
         sysm.seed_mt(int(p.seed), threads)
-        t0 = time.perf_counter()
-        res = sysm.run(steps, dt=spec.dt, n_threads=threads)
-        dt = time.perf_counter() - t0
-        total_bs += spec.n * res["steps"]
-        total_t += dt
-        used.append(f"{spec.name}({spec.n} beads)")
-        if total_t > budget_s:
-            break
+        systems.append((spec, sysm))
+    # rounds of `steps` steps over the sample until the time budget is used
+    total_bs, total_t, used = 0, 0.0, []
+    rounds = 0
+    while total_t < budget_s and rounds < 1000:
+        for spec, sysm in systems:
+            t0 = time.perf_counter()
+            res = sysm.run(steps, dt=spec.dt, n_threads=threads)
+            total_t += time.perf_counter() - t0
+            total_bs += spec.n * res["steps"]
+            if res["flag"] < 0:
+                sysm.build_lists(grid_window=1)
+        rounds += 1
+    used = [f"{spec.name}({spec.n} beads)" for spec, _ in systems]
+    used.append(f"{rounds} rounds of {steps} steps")
     return total_bs / total_t, used, total_t
 
 
@@ -198,7 +205,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    specs, desc = make_workload(args.workload)
+    specs, desc = make_workload(args.workload, systems=args.systems)
     threads = os.cpu_count() or 1
     # a bounded sample: the first systems, relaxed untimed with the reference's adaptive dt
     sample = specs[:args.cpu_systems]
@@ -244,7 +251,7 @@ def run_gpu(args):
         torch.cuda.set_device(0)
     dev = torch.device("cuda", torch.cuda.current_device())
 
-    specs, desc = make_workload(args.workload, rank=rank, scale=args.scale)
+    specs, desc = make_workload(args.workload, rank=rank, scale=args.scale, systems=args.systems)
     batch = Batch(specs, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph)
     eng = batch.engine
     n_beads = batch.n_beads
@@ -266,9 +273,11 @@ def run_gpu(args):
     clocks.start()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")
     ev0.record(eng.stream)
     batch.run(args.steps)
     ev1.record(eng.stream)
+    torch.cuda.nvtx.range_pop()
     ev1.synchronize()
     clk = clocks.stop()
     torch.cuda.synchronize()
@@ -408,6 +417,7 @@ def main():
     ap.add_argument("--workload", default="sweep", choices=["sweep", "large", "config1", "config5"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--systems", type=int, default=256, help="systems of the sweep workload")
     ap.add_argument("--steps-per-graph", type=int, default=10)
     ap.add_argument("--relax-steps", type=int, default=2000)
     ap.add_argument("--profile-steps", type=int, default=10)
@@ -417,7 +427,7 @@ def main():
     ap.add_argument("--cpu-baseline", type=int, default=1)
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--cpu-systems", type=int, default=4)
-    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

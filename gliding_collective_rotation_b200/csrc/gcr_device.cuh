@@ -27,6 +27,8 @@ constexpr uint8_t kHasPrev = 1, kHasPrev2 = 2, kHasNext = 4, kHasNext2 = 8;
 constexpr int kFlagCellOverflow = 1;
 constexpr int kFlagNonFinite = 2;
 constexpr int kFlagNextOverflow = 4;
+// a system with one of these stops: every kernel skips it until re-armed
+constexpr int kFlagFatal = kFlagCellOverflow | kFlagNonFinite;
 
 struct SysP {
     // caller-owned state

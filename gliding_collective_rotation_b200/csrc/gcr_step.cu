@@ -185,6 +185,17 @@ __device__ __forceinline__ void bonded(const SysP &p, const uint8_t tp, const do
 template <typename FT>
 __device__ __forceinline__ FT wca_coeff(FT ds, FT p0, FT p1)
 {
+    if constexpr (sizeof(FT) == 4) {
+        // r < 0.01: ds^-7 leaves the FP32 range (overlaps of a random
+        // placement); evaluate in FP64 and clamp.  The adaptive dt rule turns
+        // any huge force into a step of max_dist_per_step, as in FP64.
+        if (ds < 1e-4f) {
+            double d = ds, d2 = d * d;
+            double c = (1.0 / (d2 * d2)) * ((double)p0 - (double)p1 * (1.0 / (d * d2)));
+            c = fmin(fmax(c, -1e30), 1e30);
+            return (float)c;
+        }
+    }
     // ds**-4 * (p0 - p1 * ds**-3), integer powers by squaring as Numba does
     FT d2 = ds * ds;
     FT i4 = FT(1) / (d2 * d2);
@@ -352,7 +363,7 @@ __global__ void __launch_bounds__(512) k_insert(BatchArgs A)
         const Tile tl = A.bead_tiles[t];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
-        if (!s.active || !p.calc_wca) continue;
+        if (!s.active || (s.flags & kFlagFatal) || !p.calc_wca) continue;
         int b = tl.begin + threadIdx.x;
         if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
         double x[3];
@@ -374,7 +385,7 @@ __global__ void __launch_bounds__(512) k_pack(BatchArgs A)
         const Tile tl = A.cell_tiles[t];
         const SysP &p = A.P[tl.sys];
         const SysS &s = A.S[tl.sys];
-        bool run = s.active && p.calc_wca && (WHICH == 0 || !(s.flags & kFlagCellOverflow));
+        bool run = s.active && p.calc_wca && !(s.flags & kFlagFatal);
         if (!run) continue;
         int c = tl.begin + threadIdx.x;
         if (c >= p.n_cells || threadIdx.x >= A.tile_cells) continue;
@@ -458,7 +469,7 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
         const Tile tl = A.bead_tiles[t];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
-        bool run = s.active && (STAGE == 0 || !(s.flags & kFlagCellOverflow));
+        bool run = s.active && !(s.flags & kFlagFatal);
         if (!run) continue;
         const int b = tl.begin + threadIdx.x;
         double mf2 = 0.0;
@@ -512,8 +523,9 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
                     finite &= isfinite(x1[i]);
                     p.pos1[(size_t)b * D + i] = x1[i];
                 }
-                if (!finite) atomicOr(&s.flags, kFlagNonFinite);
-                if (p.calc_wca && !bin_bead<D>(p, A, A.cnt1, x1, b))
+                if (!finite)
+                    atomicOr(&s.flags, kFlagNonFinite);
+                else if (p.calc_wca && !bin_bead<D>(p, A, A.cnt1, x1, b))
                     atomicOr(&s.flags, kFlagCellOverflow);
             } else {
                 // |F0+F1|^2 in FP64 for the dt rule (SRK.py:328)
@@ -575,7 +587,7 @@ __global__ void __launch_bounds__(512) k_update(BatchArgs A)
         const Tile tl = A.bead_tiles[t];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
-        bool run = s.active && !(s.flags & kFlagCellOverflow);
+        bool run = s.active && !(s.flags & kFlagFatal);
         if (!run) continue;
         const int b = tl.begin + threadIdx.x;
         if (b < p.n && threadIdx.x < A.tile_beads) {
@@ -619,7 +631,7 @@ __global__ void __launch_bounds__(512) k_update(BatchArgs A)
 #pragma unroll
                 for (int i = 0; i < D; i++) tan[(size_t)b * D + i] = tb[i] / mag;
             }
-            if (p.calc_wca && !bin_bead<D>(p, A, A.cnt0, x, b)) atomicOr(&s.flags, kFlagNextOverflow);
+            if (finite && p.calc_wca && !bin_bead<D>(p, A, A.cnt0, x, b)) atomicOr(&s.flags, kFlagNextOverflow);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -636,7 +648,7 @@ __global__ void __launch_bounds__(512) k_update(BatchArgs A)
                 int fl = atomicOr(&s.flags, 0);
                 bool more = (s.steps_done < s.max_steps || s.max_steps < 0) &&
                             (s.elapsed < s.max_dt_usable || s.max_dt_usable < 0.0) &&
-                            !(fl & (kFlagCellOverflow | kFlagNextOverflow));
+                            !(fl & (kFlagFatal | kFlagNextOverflow));
                 s.active = more ? 1 : 0;
                 s.tile_ctr[1] = 0u;
                 __threadfence();
