@@ -252,6 +252,8 @@ def run_gpu(args):
     dev = torch.device("cuda", torch.cuda.current_device())
 
     specs, desc = make_workload(args.workload, rank=rank, scale=args.scale, systems=args.systems)
+    for sp in specs:
+        sp.params.cell_factor = args.cell_factor
     batch = Batch(specs, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph)
     eng = batch.engine
     n_beads = batch.n_beads
@@ -392,6 +394,7 @@ def run_gpu(args):
                    "parallelism": f"{world} GPU(s), independent systems per GPU",
                    "l2": f"inputs larger than L2: working set {working_set / 1e6:.0f} MB per GPU > 126 MB",
                    "relax_steps": relax_steps, "steps_done": steps_done, "flags": flags,
+                   "cell_factor": args.cell_factor,
                    "steps_per_graph": args.steps_per_graph},
         "e2e": e2e, "roofline": roofline, "clocks": clk,
         "gpu_launches": 5 * args.steps + 1,
@@ -418,6 +421,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--systems", type=int, default=256, help="systems of the sweep workload")
+    ap.add_argument("--cell-factor", type=float, default=1.0, help="GPU cell side / pair cutoff")
     ap.add_argument("--steps-per-graph", type=int, default=10)
     ap.add_argument("--relax-steps", type=int, default=2000)
     ap.add_argument("--profile-steps", type=int, default=10)

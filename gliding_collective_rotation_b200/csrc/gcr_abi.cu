@@ -114,6 +114,8 @@ struct gcr_ctx {
     int *cnt1 = nullptr;
     int *items = nullptr;
     void *rec = nullptr;
+    void *xi = nullptr;
+    size_t stage_smem = 0;
     int32_t *chain_starts = nullptr;
     int *d_err = nullptr;
     double *d_out = nullptr;
@@ -133,10 +135,10 @@ struct gcr_ctx {
 
 namespace {
 
-int kernel_grid(const gcr_ctx *c, void *fn, int block, int64_t max_tiles)
+int kernel_grid(const gcr_ctx *c, void *fn, int block, int64_t max_tiles, size_t smem = 0)
 {
     int occ = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, 0) != cudaSuccess || occ < 1) occ = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, smem) != cudaSuccess || occ < 1) occ = 1;
     if (c->cfg.ctas_per_sm > 0) occ = std::min(occ, c->cfg.ctas_per_sm);
     int64_t g = (int64_t)c->sm_count * occ;
     g = std::min<int64_t>(g, std::max<int64_t>(max_tiles, 1));
@@ -247,10 +249,10 @@ void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, SysP &p)
     p.seed = d.seed;
 }
 
-int launch(gcr_ctx *c, void *fn, int grid, int block)
+int launch(gcr_ctx *c, void *fn, int grid, int block, size_t smem = 0)
 {
     void *a[] = {&c->args};
-    GCR_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(block), a, 0, c->stream));
+    GCR_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(block), a, smem, c->stream));
     return GCR_OK;
 }
 
@@ -259,9 +261,9 @@ int enqueue_step(gcr_ctx *c)
     int rc;
     const int bb = c->cfg.block_beads, bc = c->cfg.block_cells;
     if ((rc = launch(c, c->ks.pack0, c->grid_cells, bc))) return rc;
-    if ((rc = launch(c, c->ks.stage0, c->grid_beads, bb))) return rc;
+    if ((rc = launch(c, c->ks.stage0, c->grid_beads, bb, c->stage_smem))) return rc;
     if ((rc = launch(c, c->ks.pack1, c->grid_cells, bc))) return rc;
-    if ((rc = launch(c, c->ks.stage1, c->grid_beads, bb))) return rc;
+    if ((rc = launch(c, c->ks.stage1, c->grid_beads, bb, c->stage_smem))) return rc;
     if ((rc = launch(c, c->ks.update, c->grid_beads, bb))) return rc;
     return GCR_OK;
 }
@@ -370,6 +372,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     e = e ? e : cudaMalloc(&c->cnt1, sizeof(int) * std::max<int64_t>(cfg.cell_capacity, 1));
     e = e ? e : cudaMalloc(&c->items, sizeof(int) * std::max<int64_t>(slots_total, 1));
     e = e ? e : cudaMalloc(&c->rec, std::max<size_t>(c->rec_bytes, 32));
+    e = e ? e : cudaMalloc(&c->xi, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
     e = e ? e : cudaMalloc(&c->chain_starts, sizeof(int32_t) * (cfg.bead_capacity + S));
     e = e ? e : cudaMalloc(&c->d_err, sizeof(int));
     e = e ? e : cudaMalloc(&c->d_out, sizeof(double) * 8);
@@ -398,12 +401,18 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     a.cnt1 = c->cnt1;
     a.items = c->items;
     a.rec = c->rec;
+    a.xi = c->xi;
     a.depth = cfg.cell_depth;
     a.log_depth = ilog2(cfg.cell_depth);
     a.tile_beads = cfg.block_beads;
     a.tile_cells = cfg.block_cells;
-    int gb = kernel_grid(c, c->ks.stage0, cfg.block_beads, c->max_bead_tiles);
-    gb = std::min(gb, kernel_grid(c, c->ks.stage1, cfg.block_beads, c->max_bead_tiles));
+    c->stage_smem = c->ks.stage_smem(cfg.block_beads);
+    if (c->stage_smem > 48 * 1024) {
+        cudaFuncSetAttribute(c->ks.stage0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->stage_smem);
+        cudaFuncSetAttribute(c->ks.stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->stage_smem);
+    }
+    int gb = kernel_grid(c, c->ks.stage0, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
+    gb = std::min(gb, kernel_grid(c, c->ks.stage1, cfg.block_beads, c->max_bead_tiles, c->stage_smem));
     gb = std::min(gb, kernel_grid(c, c->ks.update, cfg.block_beads, c->max_bead_tiles));
     c->grid_beads = gb;
     c->grid_cells = kernel_grid(c, c->ks.pack0, cfg.block_cells, c->max_cell_tiles);
@@ -418,7 +427,7 @@ int gcr_destroy(gcr_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->topo, c->cnt0, c->cnt1,
-                    c->items, c->rec, c->chain_starts, c->d_err, c->d_out};
+                    c->items, c->rec, c->xi, c->chain_starts, c->d_err, c->d_out};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -650,7 +659,7 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
         for (int k = 0; k < 5; k++) {
             GCR_CUDA(cudaEventRecord(ev[(size_t)s * 10 + 2 * k], c->stream));
             rc = launch(c, fns[k], cellk[k] ? c->grid_cells : c->grid_beads,
-                        cellk[k] ? c->cfg.block_cells : c->cfg.block_beads);
+                        cellk[k] ? c->cfg.block_cells : c->cfg.block_beads, (k == 1 || k == 3) ? c->stage_smem : 0);
             if (rc) return rc;
             GCR_CUDA(cudaEventRecord(ev[(size_t)s * 10 + 2 * k + 1], c->stream));
         }

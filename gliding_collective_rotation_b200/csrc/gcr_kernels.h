@@ -21,6 +21,7 @@ struct BatchArgs {
     int *cnt1;
     int *items;
     void *rec;
+    void *xi;  // translational noise of the current step per bead, FT [bead][dim]
     int depth;
     int log_depth;
     int tile_beads;
@@ -35,6 +36,7 @@ struct KernelSet {
     void *stage1;
     void *update;
     void *topo;
+    size_t (*stage_smem)(int block_beads);  // dynamic shared memory of the stage kernels
 };
 
 KernelSet kernel_set(int dim, int precision);

@@ -45,137 +45,63 @@ struct Rec<double> {
 };
 
 // ------------------------------------------------------------------------
-// bonded forces (forces.py:285-403) for one bead, gathered from bonds
-// b-2 .. b+1; accumulation order follows the reference's sequential loop
+// bonded forces (forces.py:285-403).  A tile of TB beads stages the
+// positions of beads begin-2 .. begin+TB+1 in shared memory, computes every
+// bond (j, j+1) once and every bend once, then each bead gathers
+//   F -= s_{b-1} d_{b-1}; F -= bwd_{b-1}; F += s_b d_b; F += fwd_b + bwd_b;
+//   F -= fwd_{b+1}
+// which is the order in which the reference's sequential loop adds them.
 // ------------------------------------------------------------------------
 template <int D, typename FT>
-struct Bond {
-    FT d[D];
-    FT t[D];
-    FT fmag;
-    bool valid;
+struct StageSmem {
+    double *x;     // [TB+4][D] positions, index k <-> bead begin-2+k
+    uint8_t *tp;   // [TB+4]    topology bits
+    FT *bd;        // [TB+3][D] bond vector d_j = min_image(x_j - x_{j+1}), k <-> bond begin-2+k
+    FT *bt;        // [TB+3][D] unit tangent of the bond (d itself when |d| = 0)
+    FT *bf;        // [TB+3]    spring magnitude k (a/|d| - 1), 0 when |d| = 0
+    FT *fw;        // [TB+2][D] bend "forward" term at bead begin-1+k
+    FT *bw;        // [TB+2][D] bend "backward" term
+    __device__ void carve(unsigned char *base, int TB)
+    {
+        x = reinterpret_cast<double *>(base);
+        bd = reinterpret_cast<FT *>(x + (size_t)(TB + 4) * D);
+        bt = bd + (size_t)(TB + 3) * D;
+        bf = bt + (size_t)(TB + 3) * D;
+        fw = bf + (TB + 3);
+        bw = fw + (size_t)(TB + 2) * D;
+        tp = reinterpret_cast<uint8_t *>(bw + (size_t)(TB + 2) * D);
+    }
 };
 
 template <int D, typename FT>
-__device__ __forceinline__ void make_bond(const SysP &p, const double *__restrict__ X, int j, FT a,
-                                          FT k, Bond<D, FT> &bd)
+size_t stage_smem_bytes(int TB)
 {
-    FT r2 = FT(0);
-#pragma unroll
-    for (int i = 0; i < D; i++) {
-        double o = inbounds(__ldg(X + (size_t)j * D + i), __ldg(X + (size_t)(j + 1) * D + i), p.half_L, p.L);
-        bd.d[i] = (FT)o;
-        r2 += bd.d[i] * bd.d[i];
-    }
-    bd.valid = (r2 != FT(0));
-    if (bd.valid) {
-        FT inv = FT(1) / sqrt(r2);
-        bd.fmag = k * (a * inv - FT(1));
-#pragma unroll
-        for (int i = 0; i < D; i++) bd.t[i] = bd.d[i] * inv;
-    } else {
-        bd.fmag = FT(0);
-#pragma unroll
-        for (int i = 0; i < D; i++) bd.t[i] = bd.d[i];
-    }
+    return (size_t)(TB + 4) * D * sizeof(double) + (size_t)(TB + 3) * (2 * D + 1) * sizeof(FT) +
+           (size_t)(TB + 2) * 2 * D * sizeof(FT) + (size_t)(TB + 4) + 16;
 }
 
 // bend at a bead with forward tangent ti (its own bond) and backward tangent
-// tj (the previous bond); returns false when the tangents are aligned
+// tj (the previous bond); false when the tangents are aligned
 template <int D, typename FT>
-__device__ __forceinline__ bool bend(const FT *ti, const FT *tj, FT theta0, FT kappa, bool want_force,
-                                     FT *fwd, FT *bwd, FT &c)
+__device__ __forceinline__ bool bend(const FT *ti, const FT *tj, FT theta0, FT kappa, FT *fwd, FT *bwd)
 {
-    c = FT(0);
+    FT c = FT(0);
 #pragma unroll
     for (int i = 0; i < D; i++) c += ti[i] * tj[i];
     if (!(FT(-1) < c && c < FT(1))) return false;
-    if (want_force) {
-        FT phi = acos(c);
-        if (theta0 != FT(0)) {
-            FT cr = -ti[0] * tj[1] + ti[1] * tj[0];
-            FT sg = (FT)((cr > FT(0)) - (cr < FT(0)));
-            phi += theta0 * sg;
-        }
-        phi *= kappa / sqrt(FT(1) - c * c);
+    FT phi = acos(c);
+    if (theta0 != FT(0)) {
+        FT cr = -ti[0] * tj[1] + ti[1] * tj[0];
+        FT sg = (FT)((cr > FT(0)) - (cr < FT(0)));
+        phi += theta0 * sg;
+    }
+    phi *= kappa / sqrt(FT(1) - c * c);
 #pragma unroll
-        for (int i = 0; i < D; i++) {
-            fwd[i] = phi * (c * tj[i] - ti[i]);
-            bwd[i] = phi * (tj[i] - c * ti[i]);
-        }
+    for (int i = 0; i < D; i++) {
+        fwd[i] = phi * (c * tj[i] - ti[i]);
+        bwd[i] = phi * (tj[i] - c * ti[i]);
     }
     return true;
-}
-
-template <int D, typename FT>
-__device__ __forceinline__ void bonded(const SysP &p, const uint8_t tp, const double *__restrict__ X, int b,
-                                       FT *F, FT *tang, bool &tang_set)
-{
-    const FT a = (FT)__ldg(p.rest + __ldg(p.chain + b));
-    const FT k = (FT)p.k;
-    const FT kappa = (FT)p.kappa, theta0 = (FT)p.theta0;
-    const bool cb = p.calc_bend;
-    Bond<D, FT> bm2, bm1, b0, bp1;
-    if (tp & kHasPrev2) make_bond<D, FT>(p, X, b - 2, a, k, bm2);
-    if (tp & kHasPrev) make_bond<D, FT>(p, X, b - 1, a, k, bm1);
-    if (tp & kHasNext) make_bond<D, FT>(p, X, b, a, k, b0);
-    if (tp & kHasNext2) make_bond<D, FT>(p, X, b + 1, a, k, bp1);
-    FT fwd[D], bwd[D], c;
-    // iteration b-1 of the reference loop: spring of bond b-1, bend at b-1
-    if (tp & kHasPrev) {
-        if (bm1.valid) {
-#pragma unroll
-            for (int i = 0; i < D; i++) F[i] -= bm1.d[i] * bm1.fmag;
-        }
-        if ((tp & kHasPrev2) && cb) {
-            if (bend<D, FT>(bm1.t, bm2.t, theta0, kappa, true, fwd, bwd, c)) {
-#pragma unroll
-                for (int i = 0; i < D; i++) F[i] -= bwd[i];
-            }
-        }
-    }
-    // iteration b: spring of bond b, bend at b, tangent of b
-    if (tp & kHasNext) {
-        if (b0.valid) {
-#pragma unroll
-            for (int i = 0; i < D; i++) F[i] += b0.d[i] * b0.fmag;
-        }
-    }
-    if (p.get_orient || cb) {
-        if ((tp & kHasPrev) && (tp & kHasNext)) {
-            if (bend<D, FT>(b0.t, bm1.t, theta0, kappa, cb, fwd, bwd, c)) {
-                if (cb) {
-#pragma unroll
-                    for (int i = 0; i < D; i++) F[i] += fwd[i] + bwd[i];
-                }
-                if (p.get_orient) {
-                    FT coeff = FT(1) / sqrt(FT(2) * (FT(1) + c));
-#pragma unroll
-                    for (int i = 0; i < D; i++) tang[i] = coeff * (b0.t[i] + bm1.t[i]);
-                    tang_set = true;
-                }
-            } else if (p.get_orient) {
-#pragma unroll
-                for (int i = 0; i < D; i++) tang[i] = b0.t[i];
-                tang_set = true;
-            }
-        } else if (p.get_orient && (tp & kHasNext)) {  // head bead
-#pragma unroll
-            for (int i = 0; i < D; i++) tang[i] = b0.t[i];
-            tang_set = true;
-        } else if (p.get_orient && (tp & kHasPrev)) {  // tail bead
-#pragma unroll
-            for (int i = 0; i < D; i++) tang[i] = bm1.t[i];
-            tang_set = true;
-        }
-    }
-    // iteration b+1: bend at b+1 pushes on b
-    if ((tp & kHasNext2) && cb) {
-        if (bend<D, FT>(bp1.t, b0.t, theta0, kappa, true, fwd, bwd, c)) {
-#pragma unroll
-            for (int i = 0; i < D; i++) F[i] -= fwd[i];
-        }
-    }
 }
 
 // ------------------------------------------------------------------------
@@ -190,17 +116,19 @@ __device__ __forceinline__ FT wca_coeff(FT ds, FT p0, FT p1)
         // placement); evaluate in FP64 and clamp.  The adaptive dt rule turns
         // any huge force into a step of max_dist_per_step, as in FP64.
         if (ds < 1e-4f) {
-            double d = ds, d2 = d * d;
-            double c = (1.0 / (d2 * d2)) * ((double)p0 - (double)p1 * (1.0 / (d * d2)));
+            double d = ds, inv = 1.0 / d, i2 = inv * inv;
+            double c = (i2 * i2) * ((double)p0 - (double)p1 * (i2 * inv));
             c = fmin(fmax(c, -1e30), 1e30);
             return (float)c;
         }
+        // ds**-4 (p0 - p1 ds**-3) from one correctly rounded reciprocal
+        float inv = __frcp_rn(ds);
+        float i2 = inv * inv;
+        return (i2 * i2) * (p0 - p1 * (i2 * inv));
+    } else {
+        double inv = 1.0 / ds, i2 = inv * inv;
+        return (i2 * i2) * (p0 - p1 * (i2 * inv));
     }
-    // ds**-4 * (p0 - p1 * ds**-3), integer powers by squaring as Numba does
-    FT d2 = ds * ds;
-    FT i4 = FT(1) / (d2 * d2);
-    FT i3 = FT(1) / (ds * d2);
-    return i4 * (p0 - p1 * i3);
 }
 
 template <int D, typename FT>
@@ -208,8 +136,10 @@ __device__ __forceinline__ void pair_forces(const SysP &p, const BatchArgs &A, c
                                             int b, const double *xb, FT *F)
 {
     using R = typename Rec<FT>::type;
-    const R *__restrict__ rec = reinterpret_cast<const R *>(A.rec);
     const int nc = p.nc;
+    const int depth = A.depth, ld = A.log_depth;
+    const R *__restrict__ rec = reinterpret_cast<const R *>(A.rec) + ((size_t)p.cell_off << ld);
+    const int *__restrict__ cn = cnt + p.cell_off;
     int ci[3] = {0, 0, 0};
 #pragma unroll
     for (int i = 0; i < D; i++) ci[i] = cell_coord(xb[i], p.inv_h, nc);
@@ -220,54 +150,61 @@ __device__ __forceinline__ void pair_forces(const SysP &p, const BatchArgs &A, c
     }
     const FT rc2 = (FT)p.rc2, p0 = (FT)p.p0, p1 = (FT)p.p1, shift = (FT)p.shift;
     const FT hf = (FT)p.hf;
+    const double L = p.L, half_L = p.half_L;
     const int nn = p.n_nearby;
     const int my_chain = __ldg(p.chain + b);
+    // neighbour column indices (wrapped), shared by all rows
+    int cx[3];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        int v = ci[0] + d - 1;
+        cx[d] = v < 0 ? v + nc : (v >= nc ? v - nc : v);
+    }
     const int zlo = (D == 3) ? -1 : 0, zhi = (D == 3) ? 1 : 0;
     for (int dz = zlo; dz <= zhi; dz++) {
         int cz = 0;
         if (D == 3) {
             cz = ci[2] + dz;
-            cz += (cz < 0) ? nc : 0;
-            cz -= (cz >= nc) ? nc : 0;
+            cz = cz < 0 ? cz + nc : (cz >= nc ? cz - nc : cz);
         }
+#pragma unroll
         for (int dy = -1; dy <= 1; dy++) {
             int cy = ci[1] + dy;
-            cy += (cy < 0) ? nc : 0;
-            cy -= (cy >= nc) ? nc : 0;
-            const int64_t rowbase = p.cell_off + ((int64_t)cz * nc + cy) * nc;
+            cy = cy < 0 ? cy + nc : (cy >= nc ? cy - nc : cy);
+            const int rowbase = (cz * nc + cy) * nc;
+            int lc[3], m[3];
 #pragma unroll
-            for (int dx = -1; dx <= 1; dx++) {
-                int cx = ci[0] + dx;
-                cx += (cx < 0) ? nc : 0;
-                cx -= (cx >= nc) ? nc : 0;
-                const int64_t gc = rowbase + cx;
-                int m = __ldg(cnt + gc);
-                m = m < A.depth ? m : A.depth;
-                const R *__restrict__ cr = rec + (gc << A.log_depth);
+            for (int d = 0; d < 3; d++) {
+                lc[d] = rowbase + cx[d];
+                int q = __ldg(cn + lc[d]);
+                m[d] = q < depth ? q : depth;
+            }
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const R *__restrict__ cr = rec + ((unsigned)lc[d] << ld);
                 FT off[3];
-                off[0] = (FT)dx * hf;
+                off[0] = (FT)(d - 1) * hf;
                 off[1] = (FT)dy * hf;
                 off[2] = (FT)dz * hf;
-                for (int j = 0; j < m; j++) {
-                    R r;
+                for (int j = 0; j < m[d]; j++) {
                     int bj;
                     FT sep[3];
                     if constexpr (sizeof(FT) == 4) {
-                        r = __ldg(cr + j);
+                        float4 r = __ldg(cr + j);
                         sep[0] = (r.x - own[0]) + off[0];
                         sep[1] = (r.y - own[1]) + off[1];
                         if (D == 3) sep[2] = (r.z - own[2]) + off[2];
                         bj = __float_as_int(r.w);
                     } else {
-                        const double *q = reinterpret_cast<const double *>(cr + j);
-                        sep[0] = inbounds(__ldg(q + 0), xb[0], p.half_L, p.L);
-                        sep[1] = inbounds(__ldg(q + 1), xb[1], p.half_L, p.L);
-                        if (D == 3) sep[2] = inbounds(__ldg(q + 2), xb[2], p.half_L, p.L);
-                        bj = (int)__ldg(q + 3);
+                        const double2 *q = reinterpret_cast<const double2 *>(cr + j);
+                        double2 r0 = __ldg(q), r1 = __ldg(q + 1);
+                        sep[0] = inbounds(r0.x, xb[0], half_L, L);
+                        sep[1] = inbounds(r0.y, xb[1], half_L, L);
+                        if (D == 3) sep[2] = inbounds(r1.x, xb[2], half_L, L);
+                        bj = (int)r1.y;
                     }
-                    FT ds = FT(0);
-#pragma unroll
-                    for (int i = 0; i < D; i++) ds += sep[i] * sep[i];
+                    FT ds = sep[0] * sep[0] + sep[1] * sep[1];
+                    if (D == 3) ds += sep[2] * sep[2];
                     if (FT(0) < ds && ds <= rc2) {
                         int db = b - bj;
                         db = db < 0 ? -db : db;
@@ -462,24 +399,106 @@ __global__ void __launch_bounds__(512) k_pack(BatchArgs A)
 template <int D, typename FT, int STAGE>
 __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
 {
-    __shared__ unsigned long long sh_bits[32];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ unsigned long long sh_bits[16];
+    __shared__ int sh_run;
+    const int TB = blockDim.x;
+    StageSmem<D, FT> sm;
+    sm.carve(smem_raw, TB);
     const int nt = *A.n_bead_tiles;
     const int *cnt = STAGE == 0 ? A.cnt0 : A.cnt1;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        __syncthreads();  // the previous tile is done with shared memory
         const Tile tl = A.bead_tiles[t];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
-        bool run = s.active && !(s.flags & kFlagFatal);
-        if (!run) continue;
-        const int b = tl.begin + threadIdx.x;
+        // one decision per CTA: other CTAs may raise the system's flags while
+        // this one runs, and every thread must reach the same barriers
+        if (threadIdx.x == 0) sh_run = s.active && !(atomicOr(&s.flags, 0) & kFlagFatal);
+        __syncthreads();
+        if (!sh_run) continue;
+        const int n = p.n;
+        const int base = tl.begin - 2;
+        const double *__restrict__ X = STAGE == 0 ? p.pos : p.pos1;
+        // 1. positions and topology of beads begin-2 .. begin+TB+1
+        for (int k = threadIdx.x; k < TB + 4; k += TB) {
+            int m = base + k;
+            if (m >= 0 && m < n) {
+#pragma unroll
+                for (int i = 0; i < D; i++) sm.x[k * D + i] = __ldg(X + (size_t)m * D + i);
+                sm.tp[k] = A.topo[p.bead_off + m];
+            } else {
+                sm.tp[k] = 0;
+            }
+        }
+        __syncthreads();
+        const bool springs = p.calc_springs, cb = p.calc_bend;
+        if (springs) {
+            // 2. every bond (j, j+1) of the tile once
+            const FT kspring = (FT)p.k;
+            for (int k = threadIdx.x; k < TB + 3; k += TB) {
+                FT d[D], tt[D], f = FT(0);
+#pragma unroll
+                for (int i = 0; i < D; i++) d[i] = tt[i] = FT(0);
+                if (sm.tp[k] & kHasNext) {
+                    FT r2 = FT(0);
+#pragma unroll
+                    for (int i = 0; i < D; i++) {
+                        d[i] = (FT)inbounds(sm.x[k * D + i], sm.x[(k + 1) * D + i], p.half_L, p.L);
+                        r2 += d[i] * d[i];
+                    }
+                    if (r2 != FT(0)) {
+                        const FT a = (FT)__ldg(p.rest + __ldg(p.chain + base + k));
+                        FT inv = FT(1) / sqrt(r2);
+                        f = kspring * (a * inv - FT(1));
+#pragma unroll
+                        for (int i = 0; i < D; i++) tt[i] = d[i] * inv;
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < D; i++) tt[i] = d[i];
+                    }
+                }
+#pragma unroll
+                for (int i = 0; i < D; i++) {
+                    sm.bd[k * D + i] = d[i];
+                    sm.bt[k * D + i] = tt[i];
+                }
+                sm.bf[k] = f;
+            }
+            __syncthreads();
+            // 3. every bend once: bead begin-1+k uses bonds k+1 (own) and k
+            if (cb) {
+                const FT kappa = (FT)p.kappa, theta0 = (FT)p.theta0;
+                for (int k = threadIdx.x; k < TB + 2; k += TB) {
+                    FT fw[D], bw[D];
+#pragma unroll
+                    for (int i = 0; i < D; i++) fw[i] = bw[i] = FT(0);
+                    const uint8_t tp = sm.tp[k + 1];
+                    if ((tp & kHasPrev) && (tp & kHasNext)) {
+                        if (!bend<D, FT>(sm.bt + (k + 1) * D, sm.bt + k * D, theta0, kappa, fw, bw)) {
+#pragma unroll
+                            for (int i = 0; i < D; i++) fw[i] = bw[i] = FT(0);
+                        }
+                    }
+#pragma unroll
+                    for (int i = 0; i < D; i++) {
+                        sm.fw[k * D + i] = fw[i];
+                        sm.bw[k * D + i] = bw[i];
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        // 4. per bead: gather bonded terms, pair forces, propulsion, update
+        const int tid = threadIdx.x;
+        const int b = tl.begin + tid;
         double mf2 = 0.0;
-        if (b < p.n && threadIdx.x < A.tile_beads) {
-            const double *__restrict__ X = STAGE == 0 ? p.pos : p.pos1;
+        if (b < n) {
             FT *frc = reinterpret_cast<FT *>(p.frc);
             FT *tan = reinterpret_cast<FT *>(p.tan);
             double xb[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-            for (int i = 0; i < D; i++) xb[i] = __ldg(X + (size_t)b * D + i);
+            for (int i = 0; i < D; i++) xb[i] = sm.x[(tid + 2) * D + i];
             FT F[3], tg[3];
 #pragma unroll
             for (int i = 0; i < D; i++) {
@@ -487,7 +506,55 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
                 tg[i] = tan[(size_t)b * D + i];
             }
             bool tang_set = false;
-            if (p.calc_springs) bonded<D, FT>(p, A.topo[p.bead_off + b], X, b, F, tg, tang_set);
+            if (springs) {
+                const uint8_t tp = sm.tp[tid + 2];
+                const bool prev = tp & kHasPrev, next = tp & kHasNext;
+                if (prev) {
+                    const FT f = sm.bf[tid + 1];
+#pragma unroll
+                    for (int i = 0; i < D; i++) F[i] -= sm.bd[(tid + 1) * D + i] * f;
+                    if ((tp & kHasPrev2) && cb) {
+#pragma unroll
+                        for (int i = 0; i < D; i++) F[i] -= sm.bw[tid * D + i];
+                    }
+                }
+                if (next) {
+                    const FT f = sm.bf[tid + 2];
+#pragma unroll
+                    for (int i = 0; i < D; i++) F[i] += sm.bd[(tid + 2) * D + i] * f;
+                }
+                if (prev && next && cb) {
+#pragma unroll
+                    for (int i = 0; i < D; i++) F[i] += sm.fw[(tid + 1) * D + i] + sm.bw[(tid + 1) * D + i];
+                }
+                if ((tp & kHasNext2) && cb) {
+#pragma unroll
+                    for (int i = 0; i < D; i++) F[i] -= sm.fw[(tid + 2) * D + i];
+                }
+                if (p.get_orient && (prev || next)) {
+                    const FT *ti = sm.bt + (tid + 2) * D, *tj = sm.bt + (tid + 1) * D;
+                    if (prev && next) {
+                        FT c = FT(0);
+#pragma unroll
+                        for (int i = 0; i < D; i++) c += ti[i] * tj[i];
+                        if (FT(-1) < c && c < FT(1)) {
+                            FT coeff = FT(1) / sqrt(FT(2) * (FT(1) + c));
+#pragma unroll
+                            for (int i = 0; i < D; i++) tg[i] = coeff * (ti[i] + tj[i]);
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < D; i++) tg[i] = ti[i];
+                        }
+                    } else if (next) {  // head bead
+#pragma unroll
+                        for (int i = 0; i < D; i++) tg[i] = ti[i];
+                    } else {  // tail bead
+#pragma unroll
+                        for (int i = 0; i < D; i++) tg[i] = tj[i];
+                    }
+                    tang_set = true;
+                }
+            }
             if (p.calc_wca) pair_forces<D, FT>(p, A, cnt, b, xb, F);
             if (p.self_propel) {
                 const FT v0 = (FT)p.v0;
@@ -509,9 +576,15 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
                 for (int i = 0; i < D; i++) tan[(size_t)b * D + i] = tg[i];
             }
             if (STAGE == 0) {
-                // predictor: pos1 = (pos + dt/r F0 + sqrt(2 D dt) xi) mod L
+                // the step's translational noise, drawn once and kept for the corrector
                 FT xi[3] = {FT(0), FT(0), FT(0)};
-                if (p.D > 0.0) noise_trans<D, FT>(p, s, b, xi);
+                if (p.D > 0.0) {
+                    noise_trans<D, FT>(p, s, b, xi);
+                    FT *xs = reinterpret_cast<FT *>(A.xi) + (size_t)(p.bead_off + b) * D;
+#pragma unroll
+                    for (int i = 0; i < D; i++) xs[i] = xi[i];
+                }
+                // predictor: pos1 = (pos + dt/r F0 + sqrt(2 D dt) xi) mod L
                 const double dt = s.dt;
                 const double dt_eff = dt * 1.0 / p.radius;
                 const double s2 = sqrt(2.0 * dt * p.D);
@@ -545,9 +618,9 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
             if ((threadIdx.x & 31) == 0) sh_bits[threadIdx.x >> 5] = bits;
             __syncthreads();
             if (threadIdx.x == 0) {
-                unsigned long long m = 0;
-                for (int w = 0; w < (blockDim.x + 31) / 32; w++) m = sh_bits[w] > m ? sh_bits[w] : m;
-                atomicMax(&s.max_f2, m);
+                unsigned long long mx = 0;
+                for (int w = 0; w < (TB + 31) / 32; w++) mx = sh_bits[w] > mx ? sh_bits[w] : mx;
+                atomicMax(&s.max_f2, mx);
                 __threadfence();
                 unsigned prev = atomicAdd(&s.tile_ctr[0], 1u);
                 if (prev == (unsigned)p.n_bead_tiles - 1u) {
@@ -574,7 +647,6 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
                     __threadfence();
                 }
             }
-            __syncthreads();
         }
     }
 }
@@ -582,13 +654,17 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
 template <int D, typename FT>
 __global__ void __launch_bounds__(512) k_update(BatchArgs A)
 {
+    __shared__ int sh_run;
     const int nt = *A.n_bead_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const Tile tl = A.bead_tiles[t];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
-        bool run = s.active && !(s.flags & kFlagFatal);
-        if (!run) continue;
+        // one decision per CTA (flags may change under other CTAs)
+        __syncthreads();
+        if (threadIdx.x == 0) sh_run = s.active && !(atomicOr(&s.flags, 0) & kFlagFatal);
+        __syncthreads();
+        if (!sh_run) continue;
         const int b = tl.begin + threadIdx.x;
         if (b < p.n && threadIdx.x < A.tile_beads) {
             const FT *frc = reinterpret_cast<const FT *>(p.frc);
@@ -596,7 +672,11 @@ __global__ void __launch_bounds__(512) k_update(BatchArgs A)
             const double dt_eff = dtu * 0.5 / p.radius;
             const double s2 = sqrt(2.0 * dtu * p.D);
             FT xi[3] = {FT(0), FT(0), FT(0)};
-            if (p.D > 0.0) noise_trans<D, FT>(p, s, b, xi);
+            if (p.D > 0.0) {
+                const FT *xs = reinterpret_cast<const FT *>(A.xi) + (size_t)(p.bead_off + b) * D;
+#pragma unroll
+                for (int i = 0; i < D; i++) xi[i] = xs[i];
+            }
             double x[3] = {0.0, 0.0, 0.0};
             bool finite = true;
 #pragma unroll
@@ -688,6 +768,10 @@ struct StepKernels {
 KernelSet kernel_set(int dim, int precision)
 {
     KernelSet k{};
+    if (dim == 2)
+        k.stage_smem = precision == 0 ? stage_smem_bytes<2, double> : stage_smem_bytes<2, float>;
+    else
+        k.stage_smem = precision == 0 ? stage_smem_bytes<3, double> : stage_smem_bytes<3, float>;
 #define GCR_FILL(D_, FT_)                           \
     k.insert = StepKernels<D_, FT_>::insert();      \
     k.pack0 = StepKernels<D_, FT_>::pack0();        \
