@@ -258,9 +258,9 @@ def run_gpu(args):
     eng = batch.engine
     n_beads = batch.n_beads
     relax_steps = batch.relax(max_steps=args.relax_steps)
-    # warm-up at the fixed dt
-    batch.begin(args.warmup)
-    batch.run(args.warmup)
+    # warm-up at the fixed dt (regrows the cells if a system overflowed them)
+    batch.run_checked(args.warmup)
+    eng = batch.engine
     eng.synchronize()
 
     def barrier():
@@ -395,7 +395,7 @@ def run_gpu(args):
                    "l2": f"inputs larger than L2: working set {working_set / 1e6:.0f} MB per GPU > 126 MB",
                    "relax_steps": relax_steps, "steps_done": steps_done, "flags": flags,
                    "cell_factor": args.cell_factor,
-                   "steps_per_graph": args.steps_per_graph},
+                   "steps_per_graph": args.steps_per_graph, "cell_depth": batch.cell_depth},
         "e2e": e2e, "roofline": roofline, "clocks": clk,
         "gpu_launches": 5 * args.steps + 1,
     }

@@ -18,7 +18,22 @@ import math
 import numpy as np
 import torch
 
+from ._lib import FLAG_CELL_OVERFLOW, FLAG_NEXT_OVERFLOW
 from .engine import Engine, SystemState, footprint, default_config
+
+OVERFLOW = FLAG_CELL_OVERFLOW | FLAG_NEXT_OVERFLOW
+MAX_DEPTH = 128
+
+
+def default_depth(dim, cell_factor):
+    """Slots per GPU cell: 16 (2D) / 32 (3D) at the cutoff, scaled with the
+    cell volume and rounded up to a power of two."""
+    base = 16 if dim == 2 else 32
+    want = base * max(1.0, cell_factor) ** dim
+    d = 8
+    while d < want and d < MAX_DEPTH:
+        d *= 2
+    return d
 
 
 def _views(specs, precision, device):
@@ -68,17 +83,41 @@ class Batch:
         self.specs = specs
         self.precision = precision
         self.device = torch.device(device or "cuda")
-        cfg = default_config(self.dim, precision, cell_depth=cell_depth)
-        cells = sum(footprint(cfg, s.params, s.n, len(s.rest_lengths))[0] for s in specs)
+        if cell_depth is None:
+            cell_depth = default_depth(self.dim, max(s.params.cell_factor for s in specs))
+        self.cell_depth = cell_depth
+        self._engine_kw = dict(block_beads=block_beads, block_cells=block_cells, steps_per_graph=steps_per_graph,
+                               stream=stream)
         self.n_beads = sum(s.n for s in specs)
-        self.engine = Engine(self.dim, precision, device=self.device, bead_capacity=self.n_beads,
-                             system_capacity=len(specs), cell_capacity=max(cells, 1), cell_depth=cell_depth,
-                             block_beads=block_beads, block_cells=block_cells, steps_per_graph=steps_per_graph,
-                             stream=stream)
         self.big, self.states = _views(specs, precision, self.device)
         torch.cuda.synchronize(self.device)
+        self.engine = None
+        self._make_engine()
+
+    def _make_engine(self):
+        cfg = default_config(self.dim, self.precision, cell_depth=self.cell_depth)
+        cells = sum(footprint(cfg, s.params, s.n, len(s.rest_lengths))[0] for s in self.specs)
+        self.engine = Engine(self.dim, self.precision, device=self.device, bead_capacity=self.n_beads,
+                             system_capacity=len(self.specs), cell_capacity=max(cells, 1),
+                             cell_depth=self.cell_depth, **self._engine_kw)
         for st in self.states:
             self.engine.admit(st)
+
+    def overflowed(self, statuses=None):
+        statuses = statuses if statuses is not None else self.statuses()
+        return any(s["flags"] & OVERFLOW for s in statuses)
+
+    def regrow(self):
+        """Double the slots per GPU cell after an overflow (the reference
+        doubles its list depth the same way, updates.py:257-267) and re-admit
+        every system; step counters carry over, so the noise stream goes on."""
+        if self.cell_depth >= MAX_DEPTH:
+            raise RuntimeError("GPU cell depth limit reached")
+        for st, s in zip(self.states, self.statuses()):
+            st.params.step = s["step"]
+        self.engine.close()
+        self.cell_depth *= 2
+        self._make_engine()
 
     # -- calls -------------------------------------------------------------------
     def begin(self, max_steps, dt=None, max_dist_per_step=None, max_dt_usable=-1.0):
@@ -106,8 +145,11 @@ class Batch:
             self.engine.call_begin_many([st.slot for st in self.states], chunk, [s.dt for s in self.specs])
             self.engine.run(chunk)
             done += chunk
-            dts = [self.engine.status(st.slot)["dt"] for st in self.states]
-            if all(d >= spec.dt * (1 - 1e-12) for d, spec in zip(dts, self.specs)):
+            sts = self.statuses()
+            if self.overflowed(sts):
+                self.regrow()
+                continue
+            if all(s["dt"] >= spec.dt * (1 - 1e-12) for s, spec in zip(sts, self.specs)):
                 break
         for st in self.states:
             st.params.max_dist_per_step = math.inf
@@ -116,6 +158,22 @@ class Batch:
 
     def statuses(self):
         return [self.engine.status(st.slot) for st in self.states]
+
+    def run_checked(self, steps, max_regrow=3):
+        """Run `steps` steps of every system; after a cell overflow regrow the
+        cells and run the remaining steps of the systems that stopped."""
+        self.begin(steps)
+        self.run(steps)
+        for _ in range(max_regrow):
+            sts = self.statuses()
+            if not self.overflowed(sts):
+                return sts
+            left = [steps - s["steps_done"] for s in sts]
+            self.regrow()
+            slots = [st.slot for st in self.states]
+            self.engine.call_begin_many(slots, left, [s["dt"] for s in sts])
+            self.run(max(left))
+        return self.statuses()
 
     def order_params(self):
         return np.array([self.engine.order_params(st.slot) for st in self.states])

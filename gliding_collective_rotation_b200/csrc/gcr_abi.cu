@@ -128,7 +128,7 @@ struct gcr_ctx {
     std::vector<Tile> h_bead_tiles, h_cell_tiles;
     RangeAlloc beads, cells, chains;
     BatchArgs args{};
-    int grid_beads = 1, grid_cells = 1;
+    int grid_beads = 1, grid_cells = 1, grid_update = 1, grid_pack = 1, grid_sys = 1;
     cudaGraphExec_t graph = nullptr;
     bool tiles_dirty = true;
 };
@@ -256,15 +256,25 @@ int launch(gcr_ctx *c, void *fn, int grid, int block, size_t smem = 0)
     return GCR_OK;
 }
 
+int launch_sys(gcr_ctx *c, void *fn)
+{
+    int n = (int)c->slots.size();
+    void *a[] = {&c->args, &n};
+    GCR_CUDA(cudaLaunchKernel(fn, dim3(c->grid_sys), dim3(128), a, 0, c->stream));
+    return GCR_OK;
+}
+
 int enqueue_step(gcr_ctx *c)
 {
     int rc;
     const int bb = c->cfg.block_beads, bc = c->cfg.block_cells;
-    if ((rc = launch(c, c->ks.pack0, c->grid_cells, bc))) return rc;
+    if ((rc = launch(c, c->ks.pack0, c->grid_pack, bc))) return rc;
     if ((rc = launch(c, c->ks.stage0, c->grid_beads, bb, c->stage_smem))) return rc;
-    if ((rc = launch(c, c->ks.pack1, c->grid_cells, bc))) return rc;
+    if ((rc = launch(c, c->ks.pack1, c->grid_pack, bc))) return rc;
     if ((rc = launch(c, c->ks.stage1, c->grid_beads, bb, c->stage_smem))) return rc;
-    if ((rc = launch(c, c->ks.update, c->grid_beads, bb))) return rc;
+    if ((rc = launch_sys(c, c->ks.sys_dt))) return rc;
+    if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
+    if ((rc = launch_sys(c, c->ks.sys_end))) return rc;
     return GCR_OK;
 }
 
@@ -328,8 +338,9 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     gcr_config cfg = *cfg_in;
     if (cfg.dim != 2 && cfg.dim != 3) return fail(GCR_ERR_BAD_ARG, "dim must be 2 or 3");
     if (cfg.precision != GCR_FP64 && cfg.precision != GCR_MIXED) return fail(GCR_ERR_BAD_ARG, "bad precision");
-    if (cfg.cell_depth != 8 && cfg.cell_depth != 16 && cfg.cell_depth != 32 && cfg.cell_depth != 64)
-        return fail(GCR_ERR_BAD_ARG, "cell_depth must be 8, 16, 32 or 64");
+    if (cfg.cell_depth != 8 && cfg.cell_depth != 16 && cfg.cell_depth != 32 && cfg.cell_depth != 64 &&
+        cfg.cell_depth != 128)
+        return fail(GCR_ERR_BAD_ARG, "cell_depth must be 8, 16, 32, 64 or 128");
     if (cfg.block_beads < 64 || cfg.block_beads > 512 || cfg.block_beads % 32)
         return fail(GCR_ERR_BAD_ARG, "block_beads must be a multiple of 32 in [64, 512]");
     if (cfg.block_cells < 64 || cfg.block_cells > 512 || cfg.block_cells % 32)
@@ -413,9 +424,11 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     }
     int gb = kernel_grid(c, c->ks.stage0, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
     gb = std::min(gb, kernel_grid(c, c->ks.stage1, cfg.block_beads, c->max_bead_tiles, c->stage_smem));
-    gb = std::min(gb, kernel_grid(c, c->ks.update, cfg.block_beads, c->max_bead_tiles));
     c->grid_beads = gb;
-    c->grid_cells = kernel_grid(c, c->ks.pack0, cfg.block_cells, c->max_cell_tiles);
+    c->grid_update = kernel_grid(c, c->ks.update, cfg.block_beads, c->max_bead_tiles);
+    c->grid_pack = kernel_grid(c, c->ks.pack0, cfg.block_cells, c->max_cell_tiles);
+    c->grid_cells = c->grid_pack;
+    c->grid_sys = (int)((S + 127) / 128);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return cleanup(fail(GCR_ERR_CUDA, "initialisation"));
     *out = c;
     return GCR_OK;
@@ -571,7 +584,6 @@ void arm(SysS &s, const gcr_call *call)
     s.noise = call->noise;
     s.noise_steps = call->noise_steps;
     s.flags = 0;
-    s.tile_ctr[0] = s.tile_ctr[1] = 0u;
     s.active = ((0 < s.max_steps || s.max_steps < 0) && (0.0 < s.max_dt_usable || s.max_dt_usable < 0.0)) ? 1 : 0;
 }
 }  // namespace
@@ -622,7 +634,7 @@ int gcr_run(gcr_ctx *c, int64_t max_steps, int32_t sync_every)
     const size_t cb = sizeof(int) * std::max<int64_t>(c->cfg.cell_capacity, 1);
     GCR_CUDA(cudaMemsetAsync(c->cnt0, 0, cb, c->stream));
     GCR_CUDA(cudaMemsetAsync(c->cnt1, 0, cb, c->stream));
-    rc = launch(c, c->ks.insert, c->grid_beads, c->cfg.block_beads);
+    rc = launch(c, c->ks.insert, c->grid_update, c->cfg.block_beads);
     if (rc) return rc;
     const int64_t spg = c->cfg.steps_per_graph;
     const int64_t graphs = (max_steps + spg - 1) / spg;
@@ -649,20 +661,32 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
     const size_t cb = sizeof(int) * std::max<int64_t>(c->cfg.cell_capacity, 1);
     GCR_CUDA(cudaMemsetAsync(c->cnt0, 0, cb, c->stream));
     GCR_CUDA(cudaMemsetAsync(c->cnt1, 0, cb, c->stream));
-    int rc = launch(c, c->ks.insert, c->grid_beads, c->cfg.block_beads);
+    int rc = launch(c, c->ks.insert, c->grid_update, c->cfg.block_beads);
     if (rc) return rc;
-    void *fns[5] = {c->ks.pack0, c->ks.stage0, c->ks.pack1, c->ks.stage1, c->ks.update};
-    const bool cellk[5] = {true, false, true, false, false};
+    // pack(pos), stage 0, pack(pos1), stage 1 + dt rule, update + bookkeeping
     std::vector<cudaEvent_t> ev((size_t)n_steps * 10, nullptr);
     for (auto &e : ev) GCR_CUDA(cudaEventCreate(&e));
-    for (int s = 0; s < n_steps; s++)
-        for (int k = 0; k < 5; k++) {
-            GCR_CUDA(cudaEventRecord(ev[(size_t)s * 10 + 2 * k], c->stream));
-            rc = launch(c, fns[k], cellk[k] ? c->grid_cells : c->grid_beads,
-                        cellk[k] ? c->cfg.block_cells : c->cfg.block_beads, (k == 1 || k == 3) ? c->stage_smem : 0);
-            if (rc) return rc;
-            GCR_CUDA(cudaEventRecord(ev[(size_t)s * 10 + 2 * k + 1], c->stream));
-        }
+    const int bb = c->cfg.block_beads, bc = c->cfg.block_cells;
+    for (int s = 0; s < n_steps && rc == GCR_OK; s++) {
+        cudaEvent_t *e = ev.data() + (size_t)s * 10;
+        GCR_CUDA(cudaEventRecord(e[0], c->stream));
+        rc = launch(c, c->ks.pack0, c->grid_pack, bc);
+        GCR_CUDA(cudaEventRecord(e[1], c->stream));
+        GCR_CUDA(cudaEventRecord(e[2], c->stream));
+        if (!rc) rc = launch(c, c->ks.stage0, c->grid_beads, bb, c->stage_smem);
+        GCR_CUDA(cudaEventRecord(e[3], c->stream));
+        GCR_CUDA(cudaEventRecord(e[4], c->stream));
+        if (!rc) rc = launch(c, c->ks.pack1, c->grid_pack, bc);
+        GCR_CUDA(cudaEventRecord(e[5], c->stream));
+        GCR_CUDA(cudaEventRecord(e[6], c->stream));
+        if (!rc) rc = launch(c, c->ks.stage1, c->grid_beads, bb, c->stage_smem);
+        if (!rc) rc = launch_sys(c, c->ks.sys_dt);
+        GCR_CUDA(cudaEventRecord(e[7], c->stream));
+        GCR_CUDA(cudaEventRecord(e[8], c->stream));
+        if (!rc) rc = launch(c, c->ks.update, c->grid_update, bb);
+        if (!rc) rc = launch_sys(c, c->ks.sys_end);
+        GCR_CUDA(cudaEventRecord(e[9], c->stream));
+    }
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     for (int k = 0; k < 5; k++) ms_out[k] = 0.f;
     for (int s = 0; s < n_steps; s++)
@@ -672,7 +696,7 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
             ms_out[k] += ms;
         }
     for (auto &e : ev) cudaEventDestroy(e);
-    return GCR_OK;
+    return rc;
 }
 
 int gcr_synchronize(gcr_ctx *c)

@@ -80,7 +80,7 @@ struct SysS {
     int64_t noise_steps;
     int32_t active;
     int32_t flags;
-    uint32_t tile_ctr[2];
+    uint32_t pad[2];
 };
 
 struct Tile {
@@ -185,6 +185,9 @@ __device__ __forceinline__ double inbounds(double a, double b, double half_L, do
         o -= L;
     return o;
 }
+
+// read of a word that other CTAs may change during the kernel
+__device__ __forceinline__ int ld_volatile(const int *p) { return *(const volatile int *)p; }
 
 // GPU cell coordinate of a position (clamped; non-finite -> 0)
 __device__ __forceinline__ int cell_coord(double x, double inv_h, int nc)

@@ -36,6 +36,8 @@ struct KernelSet {
     void *stage1;
     void *update;
     void *topo;
+    void *sys_dt;
+    void *sys_end;
     size_t (*stage_smem)(int block_beads);  // dynamic shared memory of the stage kernels
 };
 

@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(512) k_insert(BatchArgs A)
         const Tile tl = A.bead_tiles[t];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
-        if (!s.active || (s.flags & kFlagFatal) || !p.calc_wca) continue;
+        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal) || !p.calc_wca) continue;
         int b = tl.begin + threadIdx.x;
         if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
         double x[3];
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(512) k_pack(BatchArgs A)
         const Tile tl = A.cell_tiles[t];
         const SysP &p = A.P[tl.sys];
         const SysS &s = A.S[tl.sys];
-        bool run = s.active && p.calc_wca && !(s.flags & kFlagFatal);
+        bool run = s.active && p.calc_wca && !(ld_volatile(&s.flags) & kFlagFatal);
         if (!run) continue;
         int c = tl.begin + threadIdx.x;
         if (c >= p.n_cells || threadIdx.x >= A.tile_cells) continue;
@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
         SysS &s = A.S[tl.sys];
         // one decision per CTA: other CTAs may raise the system's flags while
         // this one runs, and every thread must reach the same barriers
-        if (threadIdx.x == 0) sh_run = s.active && !(atomicOr(&s.flags, 0) & kFlagFatal);
+        if (threadIdx.x == 0) sh_run = ld_volatile(&s.active) && !(ld_volatile(&s.flags) & kFlagFatal);
         __syncthreads();
         if (!sh_run) continue;
         const int n = p.n;
@@ -620,32 +620,7 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
             if (threadIdx.x == 0) {
                 unsigned long long mx = 0;
                 for (int w = 0; w < (TB + 31) / 32; w++) mx = sh_bits[w] > mx ? sh_bits[w] : mx;
-                atomicMax(&s.max_f2, mx);
-                __threadfence();
-                unsigned prev = atomicAdd(&s.tile_ctr[0], 1u);
-                if (prev == (unsigned)p.n_bead_tiles - 1u) {
-                    __threadfence();
-                    // last tile of this system: dt rule (SRK.py:323-353)
-                    double mf2s = __longlong_as_double(atomicAdd(&s.max_f2, 0ull));
-                    double S = p.sqrt2D + 0.5 * sqrt(mf2s) / p.radius;
-                    double dt;
-                    if (S == 0.0)
-                        dt = p.dtmax;
-                    else {
-                        double q = p.mdps / S;
-                        dt = (q < p.dtmax) ? q : p.dtmax;
-                    }
-                    double dt_used = p.rk * dt;
-                    if (s.max_dt_usable > 0.0) {
-                        double lim = s.max_dt_usable - s.elapsed;
-                        dt_used = (lim < dt_used) ? lim : dt_used;
-                    }
-                    s.dt_next = dt;
-                    s.dt_used = dt_used;
-                    s.mfs = S;
-                    s.tile_ctr[0] = 0u;
-                    __threadfence();
-                }
+                if (mx) atomicMax(&s.max_f2, mx);
             }
         }
     }
@@ -654,88 +629,106 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
 template <int D, typename FT>
 __global__ void __launch_bounds__(512) k_update(BatchArgs A)
 {
-    __shared__ int sh_run;
     const int nt = *A.n_bead_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const Tile tl = A.bead_tiles[t];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
-        // one decision per CTA (flags may change under other CTAs)
-        __syncthreads();
-        if (threadIdx.x == 0) sh_run = s.active && !(atomicOr(&s.flags, 0) & kFlagFatal);
-        __syncthreads();
-        if (!sh_run) continue;
+        // no barriers in this kernel: a per-thread decision is safe
+        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal)) continue;
         const int b = tl.begin + threadIdx.x;
-        if (b < p.n && threadIdx.x < A.tile_beads) {
-            const FT *frc = reinterpret_cast<const FT *>(p.frc);
-            const double dtu = s.dt_used;
-            const double dt_eff = dtu * 0.5 / p.radius;
-            const double s2 = sqrt(2.0 * dtu * p.D);
-            FT xi[3] = {FT(0), FT(0), FT(0)};
-            if (p.D > 0.0) {
-                const FT *xs = reinterpret_cast<const FT *>(A.xi) + (size_t)(p.bead_off + b) * D;
+        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
+        const FT *frc = reinterpret_cast<const FT *>(p.frc);
+        const double dtu = s.dt_used;
+        const double dt_eff = dtu * 0.5 / p.radius;
+        const double s2 = sqrt(2.0 * dtu * p.D);
+        FT xi[3] = {FT(0), FT(0), FT(0)};
+        if (p.D > 0.0) {
+            const FT *xs = reinterpret_cast<const FT *>(A.xi) + (size_t)(p.bead_off + b) * D;
 #pragma unroll
-                for (int i = 0; i < D; i++) xi[i] = xs[i];
-            }
-            double x[3] = {0.0, 0.0, 0.0};
-            bool finite = true;
+            for (int i = 0; i < D; i++) xi[i] = xs[i];
+        }
+        double x[3] = {0.0, 0.0, 0.0};
+        bool finite = true;
+#pragma unroll
+        for (int i = 0; i < D; i++) {
+            x[i] = srk_update<FT>(p.pos[(size_t)b * D + i], dt_eff, s2, frc[(size_t)b * D + i], xi[i], p.L);
+            finite &= isfinite(x[i]);
+            p.pos[(size_t)b * D + i] = x[i];
+        }
+        if (!finite) atomicOr(&s.flags, kFlagNonFinite);
+        if (p.Dr > 0.0 && !p.get_orient) {
+            // rotational diffusion, SRK.py:399-423 (note the factor pi)
+            FT xr[3] = {FT(0), FT(0), FT(0)};
+            noise_rot<D, FT>(p, s, b, xr);
+            FT *tan = reinterpret_cast<FT *>(p.tan);
+            FT tb[3];
+#pragma unroll
+            for (int i = 0; i < D; i++) tb[i] = tan[(size_t)b * D + i];
+            const FT sq = (FT)(sqrt(2.0 * dtu * p.Dr) * 3.141592653589793);
+            FT proj = FT(0);
+#pragma unroll
+            for (int i = 0; i < D; i++) proj += xr[i] * tb[i];
+#pragma unroll
+            for (int i = 0; i < D; i++) xr[i] -= proj * tb[i];
+            FT mag = FT(0);
 #pragma unroll
             for (int i = 0; i < D; i++) {
-                x[i] = srk_update<FT>(p.pos[(size_t)b * D + i], dt_eff, s2, frc[(size_t)b * D + i], xi[i], p.L);
-                finite &= isfinite(x[i]);
-                p.pos[(size_t)b * D + i] = x[i];
+                FT v = tb[i] + sq * xr[i];
+                mag += v * v;
+                tb[i] = v;
             }
-            if (!finite) atomicOr(&s.flags, kFlagNonFinite);
-            if (p.Dr > 0.0 && !p.get_orient) {
-                // rotational diffusion, SRK.py:399-423 (note the factor pi)
-                FT xr[3] = {FT(0), FT(0), FT(0)};
-                noise_rot<D, FT>(p, s, b, xr);
-                FT *tan = reinterpret_cast<FT *>(p.tan);
-                FT tb[3];
+            mag = sqrt(mag);
 #pragma unroll
-                for (int i = 0; i < D; i++) tb[i] = tan[(size_t)b * D + i];
-                const FT sq = (FT)(sqrt(2.0 * dtu * p.Dr) * 3.141592653589793);
-                FT proj = FT(0);
-#pragma unroll
-                for (int i = 0; i < D; i++) proj += xr[i] * tb[i];
-#pragma unroll
-                for (int i = 0; i < D; i++) xr[i] -= proj * tb[i];
-                FT mag = FT(0);
-#pragma unroll
-                for (int i = 0; i < D; i++) {
-                    FT v = tb[i] + sq * xr[i];
-                    mag += v * v;
-                    tb[i] = v;
-                }
-                mag = sqrt(mag);
-#pragma unroll
-                for (int i = 0; i < D; i++) tan[(size_t)b * D + i] = tb[i] / mag;
-            }
-            if (finite && p.calc_wca && !bin_bead<D>(p, A, A.cnt0, x, b)) atomicOr(&s.flags, kFlagNextOverflow);
+            for (int i = 0; i < D; i++) tan[(size_t)b * D + i] = tb[i] / mag;
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            unsigned prev = atomicAdd(&s.tile_ctr[1], 1u);
-            if (prev == (unsigned)p.n_bead_tiles - 1u) {
-                __threadfence();
-                // last tile: step bookkeeping (SRK.py:330, 348-349, 128-130)
-                s.dt = s.dt_next;
-                s.elapsed += s.dt_used;
-                s.step += 1;
-                s.steps_done += 1;
-                s.max_f2 = 0ull;
-                int fl = atomicOr(&s.flags, 0);
-                bool more = (s.steps_done < s.max_steps || s.max_steps < 0) &&
-                            (s.elapsed < s.max_dt_usable || s.max_dt_usable < 0.0) &&
-                            !(fl & (kFlagFatal | kFlagNextOverflow));
-                s.active = more ? 1 : 0;
-                s.tile_ctr[1] = 0u;
-                __threadfence();
-            }
-        }
-        __syncthreads();
+        if (finite && p.calc_wca && !bin_bead<D>(p, A, A.cnt0, x, b)) atomicOr(&s.flags, kFlagNextOverflow);
     }
+}
+
+// per-system dt rule after stage 1 (SRK.py:323-353): one thread per slot
+__global__ void k_sys_dt(BatchArgs A, int n_slots)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_slots) return;
+    const SysP &p = A.P[i];
+    SysS &s = A.S[i];
+    if (!s.active || (s.flags & kFlagFatal)) return;
+    double mf2s = __longlong_as_double((long long)s.max_f2);
+    double S = p.sqrt2D + 0.5 * sqrt(mf2s) / p.radius;
+    double dt;
+    if (S == 0.0)
+        dt = p.dtmax;
+    else {
+        double q = p.mdps / S;
+        dt = (q < p.dtmax) ? q : p.dtmax;
+    }
+    double dt_used = p.rk * dt;
+    if (s.max_dt_usable > 0.0) {
+        double lim = s.max_dt_usable - s.elapsed;
+        dt_used = (lim < dt_used) ? lim : dt_used;
+    }
+    s.dt_next = dt;
+    s.dt_used = dt_used;
+    s.mfs = S;
+}
+
+// per-system step bookkeeping after the corrector (SRK.py:330, 348-349,
+// 128-130): one thread per slot; a step aborted by a fatal flag is not counted
+__global__ void k_sys_end(BatchArgs A, int n_slots)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_slots) return;
+    SysS &s = A.S[i];
+    if (!s.active || (s.flags & kFlagFatal)) return;
+    s.dt = s.dt_next;
+    s.elapsed += s.dt_used;
+    s.step += 1;
+    s.steps_done += 1;
+    s.max_f2 = 0ull;
+    bool more = (s.steps_done < s.max_steps || s.max_steps < 0) &&
+                (s.elapsed < s.max_dt_usable || s.max_dt_usable < 0.0) && !(s.flags & kFlagNextOverflow);
+    s.active = more ? 1 : 0;
 }
 
 // chain-neighbour bits of every bead of one system
@@ -790,6 +783,8 @@ KernelSet kernel_set(int dim, int precision)
     }
 #undef GCR_FILL
     k.topo = (void *)k_topo;
+    k.sys_dt = (void *)k_sys_dt;
+    k.sys_end = (void *)k_sys_end;
     return k;
 }
 

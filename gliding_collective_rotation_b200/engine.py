@@ -119,6 +119,8 @@ def default_config(dim, precision="fp64", bead_capacity=1 << 20, system_capacity
     cfg.system_capacity = int(system_capacity)
     cfg.cell_capacity = int(cell_capacity if cell_capacity is not None else 4 * bead_capacity)
     cfg.cell_depth = int(cell_depth if cell_depth is not None else (16 if dim == 2 else 32))
+    if cfg.cell_depth not in (8, 16, 32, 64, 128):
+        raise ValueError("cell_depth must be 8, 16, 32, 64 or 128")
     cfg.block_beads, cfg.block_cells = int(block_beads), int(block_cells)
     cfg.steps_per_graph, cfg.ctas_per_sm = int(steps_per_graph), int(ctas_per_sm)
     return cfg

@@ -70,7 +70,7 @@ typedef struct {
     int64_t bead_capacity;    /* beads over all resident systems */
     int32_t system_capacity;  /* resident systems */
     int64_t cell_capacity;    /* GPU cells over all resident systems */
-    int32_t cell_depth;       /* bead slots per GPU cell: 8, 16, 32 or 64 */
+    int32_t cell_depth;       /* bead slots per GPU cell: 8, 16, 32, 64 or 128 */
     int32_t block_beads;      /* threads per CTA of bead kernels (64..512) */
     int32_t block_cells;      /* threads per CTA of the cell kernel (64..512) */
     int32_t steps_per_graph;  /* SRK2 steps per captured CUDA graph (1..64) */
@@ -166,7 +166,8 @@ GCR_API int gcr_synchronize(gcr_ctx *ctx);
 /* Run `n_steps` steps launching the five step kernels one by one (not
  * through the graph) with CUDA events around each on the context stream;
  * ms_out[0..4] receive the total milliseconds of pack(pos), stage 0,
- * pack(pos1), stage 1 and update.  For profiling; results equal gcr_run's. */
+ * pack(pos1), stage 1 with the dt rule, and update with the step
+ * bookkeeping.  For profiling; results equal gcr_run's. */
 GCR_API int gcr_profile_steps(gcr_ctx *ctx, int32_t n_steps, float *ms_out);
 
 /* ---- observables and exports ------------------------------------------ */
