@@ -78,20 +78,22 @@ def make_workload(name, rank=0, scale=1.0, systems=256):
 # --------------------------------------------------------------------------
 
 def algorithmic_bytes(dim, precision, n_beads, n_cells, get_orient, rot_diff):
-    """Minimum DRAM bytes of one launch of each step kernel: every input read
+    """Minimum DRAM bytes of one launch of each kernel group: every input read
     once and every output written once (neighbour records counted once)."""
     P = 8                                   # FP64 position component
-    F = 8 if precision == "fp64" else 4     # force / tangent component
+    F = 8 if precision == "fp64" else 4     # force / tangent / noise component
     R = 32 if precision == "fp64" else 16   # packed record per bead
     tan = dim * F if get_orient else 0
-    pack = n_beads * (dim * P + R + 4) + n_cells * 8
-    stage0 = n_beads * (dim * P + R + 5 + dim * F + dim * P + tan + 8)
-    stage1 = n_beads * (dim * P + R + 5 + dim * F + dim * F + tan)
-    update = n_beads * (dim * P + dim * F + dim * P + 8 + (2 * dim * F if rot_diff else 0))
-    return {"pack_pos": pack, "stage0": stage0, "pack_pos1": pack, "stage1": stage1, "update": update}
+    cells = n_beads * (dim * P + 4 + R + 4) + n_cells * 20
+    pair = n_beads * (R + 4 + R + 4 + dim * F)
+    stage0 = n_beads * (dim * P + 1 + dim * F + dim * F + dim * P + tan + dim * F + 8)
+    stage1 = n_beads * (dim * P + 1 + dim * F + dim * F + dim * F + tan)
+    update = n_beads * (dim * P + dim * F + dim * F + dim * P + 8 + (2 * dim * F if rot_diff else 0))
+    return {"cells_pos": cells, "pair_pos": pair, "stage0": stage0, "cells_pos1": cells, "pair_pos1": pair,
+            "stage1": stage1, "update": update}
 
 
-KERNELS = ["pack_pos", "stage0", "pack_pos1", "stage1", "update"]
+KERNELS = ["cells_pos", "pair_pos", "stage0", "cells_pos1", "pair_pos1", "stage1", "update"]
 
 
 # --------------------------------------------------------------------------
@@ -397,7 +399,7 @@ def run_gpu(args):
                    "cell_factor": args.cell_factor,
                    "steps_per_graph": args.steps_per_graph, "cell_depth": batch.cell_depth},
         "e2e": e2e, "roofline": roofline, "clocks": clk,
-        "gpu_launches": 5 * args.steps + 1,
+        "gpu_launches": 13 * args.steps + 1,
     }
     if plain is not None:
         line["plain"] = plain

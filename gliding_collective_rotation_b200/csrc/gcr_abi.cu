@@ -115,6 +115,11 @@ struct gcr_ctx {
     int *items = nullptr;
     void *rec = nullptr;
     void *xi = nullptr;
+    void *fp = nullptr;
+    int *cstart = nullptr;
+    int *rcell = nullptr;
+    int *tsum = nullptr;
+    int *toff = nullptr;
     size_t stage_smem = 0;
     int32_t *chain_starts = nullptr;
     int *d_err = nullptr;
@@ -128,7 +133,7 @@ struct gcr_ctx {
     std::vector<Tile> h_bead_tiles, h_cell_tiles;
     RangeAlloc beads, cells, chains;
     BatchArgs args{};
-    int grid_beads = 1, grid_cells = 1, grid_update = 1, grid_pack = 1, grid_sys = 1;
+    int grid_beads = 1, grid_cells = 1, grid_update = 1, grid_pack = 1, grid_sys = 1, grid_pair = 1, grid_scan = 1;
     cudaGraphExec_t graph = nullptr;
     bool tiles_dirty = true;
 };
@@ -154,9 +159,12 @@ int rebuild_tiles(gcr_ctx *c)
         const Slot &sl = c->slots[s];
         if (!sl.used) continue;
         for (int64_t b = 0; b < sl.desc.n_beads; b += tb) c->h_bead_tiles.push_back(Tile{s, (int32_t)b});
+        c->hP[s].cell_tile0 = (int32_t)c->h_cell_tiles.size();
         if (sl.desc.calc_wca)
             for (int64_t q = 0; q < sl.n_cells; q += tcl) c->h_cell_tiles.push_back(Tile{s, (int32_t)q});
     }
+    GCR_CUDA(cudaMemcpyAsync(c->dP, c->hP.data(), sizeof(SysP) * c->hP.size(), cudaMemcpyHostToDevice,
+                             c->stream));
     if ((int64_t)c->h_bead_tiles.size() > c->max_bead_tiles || (int64_t)c->h_cell_tiles.size() > c->max_cell_tiles)
         return fail(GCR_ERR_CAPACITY, "tile table capacity exceeded");
     int nt[2] = {(int)c->h_bead_tiles.size(), (int)c->h_cell_tiles.size()};
@@ -264,13 +272,33 @@ int launch_sys(gcr_ctx *c, void *fn)
     return GCR_OK;
 }
 
+int launch_scan_tiles(gcr_ctx *c)
+{
+    int n = (int)c->slots.size();
+    void *a[] = {&c->args, &n};
+    GCR_CUDA(cudaLaunchKernel(c->ks.scan_tiles, dim3(n), dim3(256), a, 0, c->stream));
+    return GCR_OK;
+}
+
+// one stage's cell list: block scans, per-system tile scan, compact pack
+int enqueue_cells(gcr_ctx *c, int which)
+{
+    int rc;
+    const int bc = c->cfg.block_cells;
+    if ((rc = launch(c, which ? c->ks.scan_local1 : c->ks.scan_local0, c->grid_scan, bc))) return rc;
+    if ((rc = launch_scan_tiles(c))) return rc;
+    return launch(c, which ? c->ks.pack1 : c->ks.pack0, c->grid_pack, bc);
+}
+
 int enqueue_step(gcr_ctx *c)
 {
     int rc;
-    const int bb = c->cfg.block_beads, bc = c->cfg.block_cells;
-    if ((rc = launch(c, c->ks.pack0, c->grid_pack, bc))) return rc;
+    const int bb = c->cfg.block_beads;
+    if ((rc = enqueue_cells(c, 0))) return rc;
+    if ((rc = launch(c, c->ks.pair, c->grid_pair, bb))) return rc;
     if ((rc = launch(c, c->ks.stage0, c->grid_beads, bb, c->stage_smem))) return rc;
-    if ((rc = launch(c, c->ks.pack1, c->grid_pack, bc))) return rc;
+    if ((rc = enqueue_cells(c, 1))) return rc;
+    if ((rc = launch(c, c->ks.pair, c->grid_pair, bb))) return rc;
     if ((rc = launch(c, c->ks.stage1, c->grid_beads, bb, c->stage_smem))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_dt))) return rc;
     if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
@@ -320,13 +348,14 @@ int gcr_footprint(const gcr_config *cfg, const gcr_system_desc *desc, int64_t *c
     if (desc->calc_wca) {
         cells = 1;
         for (int i = 0; i < cfg->dim; i++) cells *= nc;
+        cells += 1;  // end sentinel of the compact cell list
     }
     const int64_t n = desc->n_beads, d = cfg->dim;
     const int64_t ft = cfg->precision == GCR_FP64 ? 8 : 4;
     const int64_t recb = cfg->precision == GCR_FP64 ? 32 : 16;
-    int64_t bytes = n * d * (8 + 8 + ft + ft) + n * 4 + desc->n_chains * 8  // caller-owned state
-                    + n + 4 * (desc->n_chains + 1)                            // topo, chain starts
-                    + cells * (8 + (int64_t)cfg->cell_depth * (4 + recb));    // cell table
+    int64_t bytes = n * d * (8 + 8 + ft + ft) + n * 4 + desc->n_chains * 8     // caller-owned state
+                    + n * (1 + recb + 4 + 2 * d * ft) + 4 * (desc->n_chains + 1)  // topo, list, fp, xi
+                    + cells * (12 + (int64_t)cfg->cell_depth * 4);               // counts, starts, slots
     if (cells_out) *cells_out = cells;
     if (bytes_out) *bytes_out = bytes;
     return GCR_OK;
@@ -371,7 +400,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     c->max_bead_tiles = cfg.bead_capacity / cfg.block_beads + S;
     c->max_cell_tiles = cfg.cell_capacity / cfg.block_cells + S;
     const int64_t slots_total = cfg.cell_capacity * (int64_t)cfg.cell_depth;
-    c->rec_bytes = (size_t)slots_total * (cfg.precision == GCR_FP64 ? 32 : 16);
+    c->rec_bytes = (size_t)cfg.bead_capacity * (cfg.precision == GCR_FP64 ? 32 : 16);
     cudaError_t e = cudaSuccess;
     e = e ? e : cudaMalloc(&c->dP, sizeof(SysP) * S);
     e = e ? e : cudaMalloc(&c->dS, sizeof(SysS) * S);
@@ -384,6 +413,11 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     e = e ? e : cudaMalloc(&c->items, sizeof(int) * std::max<int64_t>(slots_total, 1));
     e = e ? e : cudaMalloc(&c->rec, std::max<size_t>(c->rec_bytes, 32));
     e = e ? e : cudaMalloc(&c->xi, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
+    e = e ? e : cudaMalloc(&c->fp, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
+    e = e ? e : cudaMalloc(&c->cstart, sizeof(int) * std::max<int64_t>(cfg.cell_capacity, 1));
+    e = e ? e : cudaMalloc(&c->rcell, sizeof(int) * cfg.bead_capacity);
+    e = e ? e : cudaMalloc(&c->tsum, sizeof(int) * c->max_cell_tiles);
+    e = e ? e : cudaMalloc(&c->toff, sizeof(int) * c->max_cell_tiles);
     e = e ? e : cudaMalloc(&c->chain_starts, sizeof(int32_t) * (cfg.bead_capacity + S));
     e = e ? e : cudaMalloc(&c->d_err, sizeof(int));
     e = e ? e : cudaMalloc(&c->d_out, sizeof(double) * 8);
@@ -413,6 +447,11 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     a.items = c->items;
     a.rec = c->rec;
     a.xi = c->xi;
+    a.fp = c->fp;
+    a.cstart = c->cstart;
+    a.rcell = c->rcell;
+    a.tsum = c->tsum;
+    a.toff = c->toff;
     a.depth = cfg.cell_depth;
     a.log_depth = ilog2(cfg.cell_depth);
     a.tile_beads = cfg.block_beads;
@@ -427,6 +466,8 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     c->grid_beads = gb;
     c->grid_update = kernel_grid(c, c->ks.update, cfg.block_beads, c->max_bead_tiles);
     c->grid_pack = kernel_grid(c, c->ks.pack0, cfg.block_cells, c->max_cell_tiles);
+    c->grid_scan = kernel_grid(c, c->ks.scan_local0, cfg.block_cells, c->max_cell_tiles);
+    c->grid_pair = kernel_grid(c, c->ks.pair, cfg.block_beads, c->max_bead_tiles);
     c->grid_cells = c->grid_pack;
     c->grid_sys = (int)((S + 127) / 128);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return cleanup(fail(GCR_ERR_CUDA, "initialisation"));
@@ -440,7 +481,8 @@ int gcr_destroy(gcr_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->topo, c->cnt0, c->cnt1,
-                    c->items, c->rec, c->xi, c->chain_starts, c->d_err, c->d_out};
+                    c->items, c->rec, c->xi, c->fp, c->cstart, c->rcell, c->tsum, c->toff, c->chain_starts,
+                    c->d_err, c->d_out};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -470,7 +512,7 @@ int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers 
     }
     int64_t boff = c->beads.alloc(desc->n_beads);
     if (boff < 0) return fail(GCR_ERR_CAPACITY, "bead capacity exhausted");
-    int64_t coff = n_cells ? c->cells.alloc(n_cells) : 0;
+    int64_t coff = n_cells ? c->cells.alloc(n_cells + 1) : 0;
     if (coff < 0) {
         c->beads.release(boff, desc->n_beads);
         return fail(GCR_ERR_CAPACITY, "cell capacity exhausted");
@@ -478,7 +520,7 @@ int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers 
     int64_t choff = c->chains.alloc(desc->n_chains + 1);
     if (choff < 0) {
         c->beads.release(boff, desc->n_beads);
-        if (n_cells) c->cells.release(coff, n_cells);
+        if (n_cells) c->cells.release(coff, n_cells + 1);
         return fail(GCR_ERR_CAPACITY, "chain capacity exhausted");
     }
     Slot &sl = c->slots[slot];
@@ -511,7 +553,7 @@ int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers 
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     if (err) {
         c->beads.release(boff, desc->n_beads);
-        if (n_cells) c->cells.release(coff, n_cells);
+        if (n_cells) c->cells.release(coff, n_cells + 1);
         c->chains.release(choff, desc->n_chains + 1);
         sl = Slot();
         return fail(GCR_ERR_BAD_ARG, "chain ids must be non-decreasing and in [0, n_chains)");
@@ -529,7 +571,7 @@ int gcr_evict(gcr_ctx *c, int32_t slot)
     // make sure no queued work still uses the slot's scratch
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     c->beads.release(sl.bead_off, sl.desc.n_beads);
-    if (sl.n_cells) c->cells.release(sl.cell_off, sl.n_cells);
+    if (sl.n_cells) c->cells.release(sl.cell_off, sl.n_cells + 1);
     c->chains.release(sl.chain_off, sl.desc.n_chains + 1);
     sl = Slot();
     SysS &s = c->hS[slot];
@@ -663,36 +705,38 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
     GCR_CUDA(cudaMemsetAsync(c->cnt1, 0, cb, c->stream));
     int rc = launch(c, c->ks.insert, c->grid_update, c->cfg.block_beads);
     if (rc) return rc;
-    // pack(pos), stage 0, pack(pos1), stage 1 + dt rule, update + bookkeeping
-    std::vector<cudaEvent_t> ev((size_t)n_steps * 10, nullptr);
+    // groups: cells(pos), pair(pos), stage 0, cells(pos1), pair(pos1),
+    // stage 1 + dt rule, update + bookkeeping
+    const int G = 7;
+    std::vector<cudaEvent_t> ev((size_t)n_steps * (G + 1), nullptr);
     for (auto &e : ev) GCR_CUDA(cudaEventCreate(&e));
-    const int bb = c->cfg.block_beads, bc = c->cfg.block_cells;
+    const int bb = c->cfg.block_beads;
     for (int s = 0; s < n_steps && rc == GCR_OK; s++) {
-        cudaEvent_t *e = ev.data() + (size_t)s * 10;
+        cudaEvent_t *e = ev.data() + (size_t)s * (G + 1);
         GCR_CUDA(cudaEventRecord(e[0], c->stream));
-        rc = launch(c, c->ks.pack0, c->grid_pack, bc);
+        rc = enqueue_cells(c, 0);
         GCR_CUDA(cudaEventRecord(e[1], c->stream));
+        if (!rc) rc = launch(c, c->ks.pair, c->grid_pair, bb);
         GCR_CUDA(cudaEventRecord(e[2], c->stream));
         if (!rc) rc = launch(c, c->ks.stage0, c->grid_beads, bb, c->stage_smem);
         GCR_CUDA(cudaEventRecord(e[3], c->stream));
+        if (!rc) rc = enqueue_cells(c, 1);
         GCR_CUDA(cudaEventRecord(e[4], c->stream));
-        if (!rc) rc = launch(c, c->ks.pack1, c->grid_pack, bc);
+        if (!rc) rc = launch(c, c->ks.pair, c->grid_pair, bb);
         GCR_CUDA(cudaEventRecord(e[5], c->stream));
-        GCR_CUDA(cudaEventRecord(e[6], c->stream));
         if (!rc) rc = launch(c, c->ks.stage1, c->grid_beads, bb, c->stage_smem);
         if (!rc) rc = launch_sys(c, c->ks.sys_dt);
-        GCR_CUDA(cudaEventRecord(e[7], c->stream));
-        GCR_CUDA(cudaEventRecord(e[8], c->stream));
+        GCR_CUDA(cudaEventRecord(e[6], c->stream));
         if (!rc) rc = launch(c, c->ks.update, c->grid_update, bb);
         if (!rc) rc = launch_sys(c, c->ks.sys_end);
-        GCR_CUDA(cudaEventRecord(e[9], c->stream));
+        GCR_CUDA(cudaEventRecord(e[7], c->stream));
     }
     GCR_CUDA(cudaStreamSynchronize(c->stream));
-    for (int k = 0; k < 5; k++) ms_out[k] = 0.f;
+    for (int k = 0; k < G; k++) ms_out[k] = 0.f;
     for (int s = 0; s < n_steps; s++)
-        for (int k = 0; k < 5; k++) {
+        for (int k = 0; k < G; k++) {
             float ms = 0.f;
-            GCR_CUDA(cudaEventElapsedTime(&ms, ev[(size_t)s * 10 + 2 * k], ev[(size_t)s * 10 + 2 * k + 1]));
+            GCR_CUDA(cudaEventElapsedTime(&ms, ev[(size_t)s * (G + 1) + k], ev[(size_t)s * (G + 1) + k + 1]));
             ms_out[k] += ms;
         }
     for (auto &e : ev) cudaEventDestroy(e);

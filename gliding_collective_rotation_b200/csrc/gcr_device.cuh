@@ -6,12 +6,16 @@
 //   * library scratch, per system at a bead / cell offset:
 //       topo      uint8 [bead]       chain-neighbour bits of each bead
 //       cnt[2]    int32 [cell]       beads binned per GPU cell (ping-pong)
-//       items     int32 [cell*depth] bead ids per cell slot (unsorted)
-//       rec       float4|double4 [cell*depth] packed positions per slot,
-//                 sorted by bead id inside a cell
+//       items     int32 [cell*depth] bead ids per cell slot (unsorted staging)
+//       cstart    int32 [cell+1]     start of each cell in the compact list
+//       rec       float4|double4 [bead] compact cell list: packed positions
+//                 in cell order, sorted by bead id inside a cell
+//       rcell     int32 [bead]       cell of each record
+//       fp, xi    FT [bead][d]       pair force and step noise per bead
 //   * SysP (read-only during a step) and SysS (device-updated) per slot.
-// The GPU cell table has a fixed depth per cell, the same shape as the
-// reference's grid_list (updates.py:502-522): a count and `depth` slots.
+// Binning writes a fixed-depth table (a count and `depth` slots per cell, the
+// shape of the reference's grid_list, updates.py:502-522); a per-system
+// counting sort turns it into the compact cell list the pair kernel reads.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -47,6 +51,8 @@ struct SysP {
     int32_t n_cells;   // nc^d
     int32_t n_bead_tiles;
     int32_t n_cell_tiles;
+    int32_t cell_tile0;  // index of the system's first cell tile
+    int32_t pad1;
     double L, half_L, h, inv_h;
     float hf;          // h rounded to FP32 (mixed records)
     // bonded

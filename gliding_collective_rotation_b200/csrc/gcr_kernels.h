@@ -21,7 +21,12 @@ struct BatchArgs {
     int *cnt1;
     int *items;
     void *rec;
-    void *xi;  // translational noise of the current step per bead, FT [bead][dim]
+    void *xi;      // translational noise of the current step per bead, FT [bead][dim]
+    void *fp;      // pair force per bead (bead order), FT [bead][dim]
+    int *cstart;   // start of each cell in the compact list (+ end sentinel per system)
+    int *rcell;    // cell of each compact-list record
+    int *tsum;     // cell count of each cell tile
+    int *toff;     // start of each cell tile within its system
     int depth;
     int log_depth;
     int tile_beads;
@@ -38,6 +43,10 @@ struct KernelSet {
     void *topo;
     void *sys_dt;
     void *sys_end;
+    void *pair;
+    void *scan_local0;
+    void *scan_local1;
+    void *scan_tiles;
     size_t (*stage_smem)(int block_beads);  // dynamic shared memory of the stage kernels
 };
 

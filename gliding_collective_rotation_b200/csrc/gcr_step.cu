@@ -131,29 +131,46 @@ __device__ __forceinline__ FT wca_coeff(FT ds, FT p0, FT p1)
     }
 }
 
+// One bead's pair force, the bead taken in cell order: record k of the
+// system's compact cell list.  All lanes of a warp sit in the same or
+// neighbouring cells, so they walk the same candidate records (uniform trip
+// counts, broadcast loads).  Candidates of cell c are records
+// [cstart[c], cstart[c+1]), sorted by bead id.
 template <int D, typename FT>
-__device__ __forceinline__ void pair_forces(const SysP &p, const BatchArgs &A, const int *__restrict__ cnt,
-                                            int b, const double *xb, FT *F)
+__device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs &A, int k, int &b_out, FT *F)
 {
     using R = typename Rec<FT>::type;
     const int nc = p.nc;
-    const int depth = A.depth, ld = A.log_depth;
-    const R *__restrict__ rec = reinterpret_cast<const R *>(A.rec) + ((size_t)p.cell_off << ld);
-    const int *__restrict__ cn = cnt + p.cell_off;
-    int ci[3] = {0, 0, 0};
-#pragma unroll
-    for (int i = 0; i < D; i++) ci[i] = cell_coord(xb[i], p.inv_h, nc);
+    const R *__restrict__ rec = reinterpret_cast<const R *>(A.rec) + p.bead_off;
+    const int *__restrict__ cs = A.cstart + p.cell_off;
+    const int c = __ldg(A.rcell + p.bead_off + k);
+    int ci[3];
+    ci[0] = c % nc;
+    ci[1] = (c / nc) % nc;
+    ci[2] = (D == 3) ? c / (nc * nc) : 0;
     FT own[3] = {FT(0), FT(0), FT(0)};
+    double xb[3] = {0.0, 0.0, 0.0};
+    int b;
     if constexpr (sizeof(FT) == 4) {
-#pragma unroll
-        for (int i = 0; i < D; i++) own[i] = (FT)(xb[i] - ((double)ci[i] + 0.5) * p.h);
+        float4 r = __ldg(rec + k);
+        own[0] = r.x;
+        own[1] = r.y;
+        own[2] = r.z;
+        b = __float_as_int(r.w);
+    } else {
+        const double2 *q = reinterpret_cast<const double2 *>(rec + k);
+        double2 r0 = __ldg(q), r1 = __ldg(q + 1);
+        xb[0] = r0.x;
+        xb[1] = r0.y;
+        xb[2] = r1.x;
+        b = (int)r1.y;
     }
+    b_out = b;
     const FT rc2 = (FT)p.rc2, p0 = (FT)p.p0, p1 = (FT)p.p1, shift = (FT)p.shift;
     const FT hf = (FT)p.hf;
     const double L = p.L, half_L = p.half_L;
     const int nn = p.n_nearby;
     const int my_chain = __ldg(p.chain + b);
-    // neighbour column indices (wrapped), shared by all rows
     int cx[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -172,31 +189,29 @@ __device__ __forceinline__ void pair_forces(const SysP &p, const BatchArgs &A, c
             int cy = ci[1] + dy;
             cy = cy < 0 ? cy + nc : (cy >= nc ? cy - nc : cy);
             const int rowbase = (cz * nc + cy) * nc;
-            int lc[3], m[3];
+            int lo[3], hi[3];
 #pragma unroll
             for (int d = 0; d < 3; d++) {
-                lc[d] = rowbase + cx[d];
-                int q = __ldg(cn + lc[d]);
-                m[d] = q < depth ? q : depth;
+                lo[d] = __ldg(cs + rowbase + cx[d]);
+                hi[d] = __ldg(cs + rowbase + cx[d] + 1);
             }
 #pragma unroll
             for (int d = 0; d < 3; d++) {
-                const R *__restrict__ cr = rec + ((unsigned)lc[d] << ld);
                 FT off[3];
                 off[0] = (FT)(d - 1) * hf;
                 off[1] = (FT)dy * hf;
                 off[2] = (FT)dz * hf;
-                for (int j = 0; j < m[d]; j++) {
+                for (int j = lo[d]; j < hi[d]; j++) {
                     int bj;
                     FT sep[3];
                     if constexpr (sizeof(FT) == 4) {
-                        float4 r = __ldg(cr + j);
+                        float4 r = __ldg(rec + j);
                         sep[0] = (r.x - own[0]) + off[0];
                         sep[1] = (r.y - own[1]) + off[1];
                         if (D == 3) sep[2] = (r.z - own[2]) + off[2];
                         bj = __float_as_int(r.w);
                     } else {
-                        const double2 *q = reinterpret_cast<const double2 *>(cr + j);
+                        const double2 *q = reinterpret_cast<const double2 *>(rec + j);
                         double2 r0 = __ldg(q), r1 = __ldg(q + 1);
                         sep[0] = inbounds(r0.x, xb[0], half_L, L);
                         sep[1] = inbounds(r0.y, xb[1], half_L, L);
@@ -310,26 +325,129 @@ __global__ void __launch_bounds__(512) k_insert(BatchArgs A)
     }
 }
 
+// exclusive scan of the binned counts of one tile of cells (block scan),
+// clearing the other count buffer for the next binning
+template <int WHICH>
+__global__ void __launch_bounds__(512) k_scan_local(BatchArgs A)
+{
+    __shared__ int sh_w[16];
+    __shared__ int sh_run;
+    const int nt = *A.n_cell_tiles;
+    const int *cnt = WHICH == 0 ? A.cnt0 : A.cnt1;
+    int *other = WHICH == 0 ? A.cnt1 : A.cnt0;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        __syncthreads();
+        const Tile tl = A.cell_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        SysS &s = A.S[tl.sys];
+        if (threadIdx.x == 0)
+            sh_run = ld_volatile(&s.active) && p.calc_wca && !(ld_volatile(&s.flags) & kFlagFatal);
+        __syncthreads();
+        if (!sh_run) continue;
+        const int c = tl.begin + threadIdx.x;
+        const bool in = c < p.n_cells && threadIdx.x < A.tile_cells;
+        const int64_t gc = p.cell_off + c;
+        int v = 0;
+        if (in) {
+            v = cnt[gc];
+            v = v < A.depth ? v : A.depth;
+            other[gc] = 0;
+        }
+        // block exclusive scan
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) sh_w[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int nw = (blockDim.x + 31) >> 5;
+            int y = lane < nw ? sh_w[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int z = __shfl_up_sync(0xffffffffu, y, o);
+                if (lane >= o) y += z;
+            }
+            if (lane < nw) sh_w[lane] = y;  // inclusive prefix of warp totals
+        }
+        __syncthreads();
+        int ex = x - v + (w > 0 ? sh_w[w - 1] : 0);
+        if (in) A.cstart[gc] = ex;
+        if (threadIdx.x == blockDim.x - 1) A.tsum[t] = ex + v;
+    }
+}
+
+// exclusive scan of the tile totals of each system (one CTA per system);
+// writes the end sentinel cstart[n_cells]
+__global__ void __launch_bounds__(256) k_scan_tiles(BatchArgs A, int n_slots)
+{
+    __shared__ int sh_w[8];
+    __shared__ int sh_carry;
+    const int sys = blockIdx.x;
+    if (sys >= n_slots) return;
+    const SysP &p = A.P[sys];
+    SysS &s = A.S[sys];
+    if (!(s.active && p.calc_wca && !(s.flags & kFlagFatal)) || p.n_cell_tiles == 0) return;
+    if (threadIdx.x == 0) sh_carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int base = 0; base < p.n_cell_tiles; base += blockDim.x) {
+        const int t = base + threadIdx.x;
+        const int v = t < p.n_cell_tiles ? A.tsum[p.cell_tile0 + t] : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) sh_w[w] = x;
+        __syncthreads();
+        if (w == 0) {
+            int nw = blockDim.x >> 5;
+            int y = lane < nw ? sh_w[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int z = __shfl_up_sync(0xffffffffu, y, o);
+                if (lane >= o) y += z;
+            }
+            if (lane < nw) sh_w[lane] = y;
+        }
+        __syncthreads();
+        const int carry = sh_carry;
+        const int ex = x - v + (w > 0 ? sh_w[w - 1] : 0) + carry;
+        if (t < p.n_cell_tiles) A.toff[p.cell_tile0 + t] = ex;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) sh_carry = ex + v;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) A.cstart[p.cell_off + p.n_cells] = sh_carry;
+}
+
+// per GPU cell: final start, the slot contents sorted by bead id, packed
+// records of the build's positions written to the compact list
 template <int D, typename FT, int WHICH>
 __global__ void __launch_bounds__(512) k_pack(BatchArgs A)
 {
     using R = typename Rec<FT>::type;
-    R *rec = reinterpret_cast<R *>(A.rec);
     const int nt = *A.n_cell_tiles;
-    int *cnt = WHICH == 0 ? A.cnt0 : A.cnt1;
-    int *other = WHICH == 0 ? A.cnt1 : A.cnt0;
+    const int *cnt = WHICH == 0 ? A.cnt0 : A.cnt1;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const Tile tl = A.cell_tiles[t];
         const SysP &p = A.P[tl.sys];
         const SysS &s = A.S[tl.sys];
-        bool run = s.active && p.calc_wca && !(ld_volatile(&s.flags) & kFlagFatal);
+        bool run = ld_volatile(&s.active) && p.calc_wca && !(ld_volatile(&s.flags) & kFlagFatal);
         if (!run) continue;
         int c = tl.begin + threadIdx.x;
         if (c >= p.n_cells || threadIdx.x >= A.tile_cells) continue;
         const int64_t gc = p.cell_off + c;
         int n = cnt[gc];
         n = n < A.depth ? n : A.depth;
-        other[gc] = 0;
+        const int start = A.toff[t] + A.cstart[gc];
+        A.cstart[gc] = start;
+        if (n == 0) continue;
         int *it = A.items + (gc << A.log_depth);
         const double *X = WHICH == 0 ? p.pos : p.pos1;
         int cc[3];
@@ -339,7 +457,8 @@ __global__ void __launch_bounds__(512) k_pack(BatchArgs A)
         double ctr[3];
 #pragma unroll
         for (int i = 0; i < 3; i++) ctr[i] = ((double)cc[i] + 0.5) * p.h;
-        R *out = rec + (gc << A.log_depth);
+        R *out = reinterpret_cast<R *>(A.rec) + p.bead_off + start;
+        int *ocell = A.rcell + p.bead_off + start;
         auto emit = [&](int j, int b) {
             double x[3] = {0.0, 0.0, 0.0};
 #pragma unroll
@@ -357,6 +476,7 @@ __global__ void __launch_bounds__(512) k_pack(BatchArgs A)
                 r.w = (double)b;
             }
             out[j] = r;
+            ocell[j] = c;
         };
         if (n <= 8) {
             int v[8];
@@ -396,6 +516,28 @@ __global__ void __launch_bounds__(512) k_pack(BatchArgs A)
     }
 }
 
+// pair forces in cell order (forces.py:57-145, rule forces.WCA); writes the
+// pair force of every bead to fp[bead]
+template <int D, typename FT>
+__global__ void __launch_bounds__(512) k_pair(BatchArgs A)
+{
+    const int nt = *A.n_bead_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.bead_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        const SysS &s = A.S[tl.sys];
+        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal) || !p.calc_wca) continue;
+        const int k = tl.begin + threadIdx.x;
+        if (k >= p.n || threadIdx.x >= A.tile_beads) continue;
+        FT F[3] = {FT(0), FT(0), FT(0)};
+        int b;
+        pair_force_sorted<D, FT>(p, A, k, b, F);
+        FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
+#pragma unroll
+        for (int i = 0; i < D; i++) fp[i] = F[i];
+    }
+}
+
 template <int D, typename FT, int STAGE>
 __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
 {
@@ -406,7 +548,6 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
     StageSmem<D, FT> sm;
     sm.carve(smem_raw, TB);
     const int nt = *A.n_bead_tiles;
-    const int *cnt = STAGE == 0 ? A.cnt0 : A.cnt1;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         __syncthreads();  // the previous tile is done with shared memory
         const Tile tl = A.bead_tiles[t];
@@ -555,7 +696,11 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
                     tang_set = true;
                 }
             }
-            if (p.calc_wca) pair_forces<D, FT>(p, A, cnt, b, xb, F);
+            if (p.calc_wca) {
+                const FT *fp = reinterpret_cast<const FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
+#pragma unroll
+                for (int i = 0; i < D; i++) F[i] += fp[i];
+            }
             if (p.self_propel) {
                 const FT v0 = (FT)p.v0;
                 if (p.rotate_prop) {
@@ -750,6 +895,7 @@ __global__ void k_topo(const int32_t *__restrict__ chain, int n, uint8_t *topo)
 // ------------------------------------------------------------------------
 template <int D, typename FT>
 struct StepKernels {
+    static void *pair() { return (void *)k_pair<D, FT>; }
     static void *insert() { return (void *)k_insert<D>; }
     static void *pack0() { return (void *)k_pack<D, FT, 0>; }
     static void *pack1() { return (void *)k_pack<D, FT, 1>; }
@@ -766,6 +912,7 @@ KernelSet kernel_set(int dim, int precision)
     else
         k.stage_smem = precision == 0 ? stage_smem_bytes<3, double> : stage_smem_bytes<3, float>;
 #define GCR_FILL(D_, FT_)                           \
+    k.pair = StepKernels<D_, FT_>::pair();          \
     k.insert = StepKernels<D_, FT_>::insert();      \
     k.pack0 = StepKernels<D_, FT_>::pack0();        \
     k.pack1 = StepKernels<D_, FT_>::pack1();        \
@@ -784,6 +931,9 @@ KernelSet kernel_set(int dim, int precision)
 #undef GCR_FILL
     k.topo = (void *)k_topo;
     k.sys_dt = (void *)k_sys_dt;
+    k.scan_local0 = (void *)k_scan_local<0>;
+    k.scan_local1 = (void *)k_scan_local<1>;
+    k.scan_tiles = (void *)k_scan_tiles;
     k.sys_end = (void *)k_sys_end;
     return k;
 }

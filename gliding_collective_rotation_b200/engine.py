@@ -231,10 +231,12 @@ class Engine:
     def synchronize(self):
         check(self.lib.gcr_synchronize(self._ctx))
 
+    PROFILE_GROUPS = ["cells_pos", "pair_pos", "stage0", "cells_pos1", "pair_pos1", "stage1", "update"]
+
     def profile_steps(self, n_steps):
-        """Milliseconds per kernel type over ``n_steps`` individually launched
-        steps: [pack(pos), stage 0, pack(pos1), stage 1, update]."""
-        out = (C.c_float * 5)()
+        """Milliseconds per kernel group over ``n_steps`` individually
+        launched steps, in the order of ``PROFILE_GROUPS``."""
+        out = (C.c_float * 7)()
         check(self.lib.gcr_profile_steps(self._ctx, int(n_steps), out))
         return np.array(out[:], dtype=np.float64)
 

@@ -33,7 +33,7 @@ import numpy as np
 import torch
 
 from . import config as _default_config
-from .engine import Engine, SystemParams, SystemState
+from .engine import Engine, SystemParams, SystemState, default_config, footprint
 
 _config = _default_config
 _pair_rule_check = None
@@ -77,9 +77,10 @@ class _GpuPop:
                     float(params.wca_params[3]), float(params.cell_factor), cell_depth, bool(params.calc_wca))
         n = pop.total_pop
         spg = int(sim.get('gpu_steps_per_graph', 10))
+        cfg = default_config(dim, precision, cell_depth=cell_depth)
+        cells = footprint(cfg, params, n, len(pop.rest_lengths))[0]
         self.engine = Engine(dim, precision, bead_capacity=max(n, 1), system_capacity=1,
-                             cell_capacity=self._cells(params, dim), cell_depth=cell_depth,
-                             steps_per_graph=spg)
+                             cell_capacity=max(cells, 1), cell_depth=cell_depth, steps_per_graph=spg)
         self.state = SystemState.from_host(pop.pos, pop.tangent_list, pop.chain_id, pop.rest_lengths, params,
                                            precision=precision, device=self.engine.device)
         self.engine.admit(self.state)
@@ -89,13 +90,6 @@ class _GpuPop:
         self.h_frc = torch.empty((n, dim), dtype=ft, pin_memory=True)
         self.h_pos1 = torch.empty((n, dim), dtype=torch.float64, pin_memory=True)
         self.rng = None
-
-    @staticmethod
-    def _cells(params, dim):
-        if not params.calc_wca:
-            return 1
-        nc = int(math.floor(params.L / (params.wca_params[3] * max(1.0, params.cell_factor))))
-        return max(nc, 3) ** dim
 
 
 def _gpu_state(pop, sim, dim, precision, params):

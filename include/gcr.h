@@ -163,11 +163,12 @@ GCR_API int gcr_get_status(gcr_ctx *ctx, int32_t slot, gcr_status *out);
 /* Number of armed systems still running (synchronises the stream). */
 GCR_API int gcr_count_active(gcr_ctx *ctx, int32_t *n_out);
 GCR_API int gcr_synchronize(gcr_ctx *ctx);
-/* Run `n_steps` steps launching the five step kernels one by one (not
- * through the graph) with CUDA events around each on the context stream;
- * ms_out[0..4] receive the total milliseconds of pack(pos), stage 0,
- * pack(pos1), stage 1 with the dt rule, and update with the step
- * bookkeeping.  For profiling; results equal gcr_run's. */
+/* Run `n_steps` steps launching the step kernels one by one (not through
+ * the graph) with CUDA events between groups on the context stream;
+ * ms_out[0..6] receive the total milliseconds of: cell list of pos (scans and
+ * pack), pair forces at pos, stage 0, cell list of pos1, pair forces at
+ * pos1, stage 1 with the dt rule, update with the step bookkeeping.  For
+ * profiling; the results equal gcr_run's. */
 GCR_API int gcr_profile_steps(gcr_ctx *ctx, int32_t n_steps, float *ms_out);
 
 /* ---- observables and exports ------------------------------------------ */
