@@ -596,7 +596,10 @@ int gcr_update_desc(gcr_ctx *c, int32_t slot, const gcr_system_desc *desc)
     }
     if (n_cells != sl.n_cells) return fail(GCR_ERR_BAD_ARG, "the GPU cell grid of a resident system cannot change");
     sl.desc = *desc;
+    // the tile placement of a resident system does not change with its parameters
+    const int32_t tile0 = c->hP[slot].cell_tile0;
     fill_sysp(c, sl, nc, c->hP[slot]);
+    c->hP[slot].cell_tile0 = tile0;
     GCR_CUDA(cudaMemcpyAsync(c->dP + slot, &c->hP[slot], sizeof(SysP), cudaMemcpyHostToDevice, c->stream));
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     return GCR_OK;

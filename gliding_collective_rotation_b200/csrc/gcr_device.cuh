@@ -31,8 +31,9 @@ constexpr uint8_t kHasPrev = 1, kHasPrev2 = 2, kHasNext = 4, kHasNext2 = 8;
 constexpr int kFlagCellOverflow = 1;
 constexpr int kFlagNonFinite = 2;
 constexpr int kFlagNextOverflow = 4;
+constexpr int kFlagListCorrupt = 8;  // an inconsistent cell list was detected and not used
 // a system with one of these stops: every kernel skips it until re-armed
-constexpr int kFlagFatal = kFlagCellOverflow | kFlagNonFinite;
+constexpr int kFlagFatal = kFlagCellOverflow | kFlagNonFinite | kFlagListCorrupt;
 
 struct SysP {
     // caller-owned state

@@ -143,7 +143,8 @@ __device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs
     const int nc = p.nc;
     const R *__restrict__ rec = reinterpret_cast<const R *>(A.rec) + p.bead_off;
     const int *__restrict__ cs = A.cstart + p.cell_off;
-    const int c = __ldg(A.rcell + p.bead_off + k);
+    int c = __ldg(A.rcell + p.bead_off + k);
+    c = (c < 0 || c >= p.n_cells) ? 0 : c;
     int ci[3];
     ci[0] = c % nc;
     ci[1] = (c / nc) % nc;
@@ -166,6 +167,7 @@ __device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs
         b = (int)r1.y;
     }
     b_out = b;
+    if ((unsigned)b >= (unsigned)p.n) return;  // inconsistent list: the caller flags it
     const FT rc2 = (FT)p.rc2, p0 = (FT)p.p0, p1 = (FT)p.p1, shift = (FT)p.shift;
     const FT hf = (FT)p.hf;
     const double L = p.L, half_L = p.half_L;
@@ -192,8 +194,15 @@ __device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs
             int lo[3], hi[3];
 #pragma unroll
             for (int d = 0; d < 3; d++) {
-                lo[d] = __ldg(cs + rowbase + cx[d]);
-                hi[d] = __ldg(cs + rowbase + cx[d] + 1);
+                int l = __ldg(cs + rowbase + cx[d]);
+                int h = __ldg(cs + rowbase + cx[d] + 1);
+                // a cell holds at most `depth` records inside [0, n): clamp, so
+                // that an inconsistent list can never send a loop out of range
+                l = l < 0 ? 0 : (l > p.n ? p.n : l);
+                h = h < l ? l : (h > p.n ? p.n : h);
+                h = h - l > A.depth ? l + A.depth : h;
+                lo[d] = l;
+                hi[d] = h;
             }
 #pragma unroll
             for (int d = 0; d < 3; d++) {
@@ -221,6 +230,7 @@ __device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs
                     FT ds = sep[0] * sep[0] + sep[1] * sep[1];
                     if (D == 3) ds += sep[2] * sep[2];
                     if (FT(0) < ds && ds <= rc2) {
+                        if ((unsigned)bj >= (unsigned)p.n) continue;  // never index outside the system
                         int db = b - bj;
                         db = db < 0 ? -db : db;
                         if ((nn < 0 || db <= nn) && __ldg(p.chain + bj) == my_chain) continue;
@@ -391,6 +401,10 @@ __global__ void __launch_bounds__(256) k_scan_tiles(BatchArgs A, int n_slots)
     const SysP &p = A.P[sys];
     SysS &s = A.S[sys];
     if (!(s.active && p.calc_wca && !(s.flags & kFlagFatal)) || p.n_cell_tiles == 0) return;
+    if (p.cell_tile0 < 0 || p.cell_tile0 + p.n_cell_tiles > *A.n_cell_tiles) {
+        if (threadIdx.x == 0) atomicOr(&s.flags, kFlagListCorrupt);
+        return;
+    }
     if (threadIdx.x == 0) sh_carry = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -448,6 +462,11 @@ __global__ void __launch_bounds__(512) k_pack(BatchArgs A)
         const int start = A.toff[t] + A.cstart[gc];
         A.cstart[gc] = start;
         if (n == 0) continue;
+        if (start < 0 || start + n > p.n) {
+            // never write outside the system's part of the list
+            atomicOr((int *)&s.flags, kFlagListCorrupt);
+            continue;
+        }
         int *it = A.items + (gc << A.log_depth);
         const double *X = WHICH == 0 ? p.pos : p.pos1;
         int cc[3];
@@ -532,6 +551,10 @@ __global__ void __launch_bounds__(512) k_pair(BatchArgs A)
         FT F[3] = {FT(0), FT(0), FT(0)};
         int b;
         pair_force_sorted<D, FT>(p, A, k, b, F);
+        if (b < 0 || b >= p.n) {
+            atomicOr((int *)&s.flags, kFlagListCorrupt);
+            continue;
+        }
         FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
 #pragma unroll
         for (int i = 0; i < D; i++) fp[i] = F[i];

@@ -61,6 +61,7 @@ extern "C" {
 #define GCR_FLAG_CELL_OVERFLOW 1   /* more beads in a cell than cell_depth */
 #define GCR_FLAG_NONFINITE 2       /* a non-finite force or position */
 #define GCR_FLAG_NEXT_OVERFLOW 4   /* overflow while binning for the next step */
+#define GCR_FLAG_LIST_CORRUPT 8    /* an inconsistent cell list was detected and not used */
 
 typedef struct gcr_ctx gcr_ctx;
 

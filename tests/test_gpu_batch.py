@@ -58,6 +58,33 @@ def test_batched_equals_alone_bitwise(precision):
         return b
 
     mix = fresh(list(range(len(specs))))
+    # a parameter update of every resident system (as relax() makes) must not
+    # disturb the batch: run on and compare with a fresh batch started from
+    # the same state
+    for st in mix.states:
+        mix.engine.update_params(st)
+    snap_pos = [st.pos.clone() for st in mix.states]
+    snap_tan = [st.tangent.clone() for st in mix.states]
+    snap_step = [s["step"] for s in mix.statuses()]
+    mix.begin(steps)
+    mix.run(steps)
+    mix.engine.synchronize()
+    for i in range(len(specs)):
+        specs[i].params.step = snap_step[i]
+    again = Batch(specs, precision=precision)
+    for j in range(len(specs)):
+        again.states[j].pos.copy_(snap_pos[j])
+        again.states[j].tangent.copy_(snap_tan[j])
+    torch.cuda.synchronize()
+    again.begin(steps)
+    again.run(steps)
+    again.engine.synchronize()
+    for j in range(len(specs)):
+        assert torch.equal(again.states[j].pos, mix.states[j].pos), j
+    assert not any(s["flags"] for s in mix.statuses())
+    again.close()
+    mix.close()
+    mix = fresh(list(range(len(specs))))
     for i in range(len(specs)):
         alone = fresh([i])
         assert torch.equal(alone.states[0].pos, mix.states[i].pos), i
