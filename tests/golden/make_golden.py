@@ -161,8 +161,18 @@ def run_case(name, spec, mods):
     pops = [populations.Equal_Size_Chain_Collection(sim)]
     status = config.status_class(sim)
     control.configure_start(sim, pops, status)
-    t0 = time.time()
     pop = pops[0]
+    # the reference's placement and derived settings, before any step
+    init = dict(init_pos=pop.pos.copy(), init_tangent=pop.tangent_list.copy(),
+                init_wca_params=pop.WCA_params.copy(), init_spring_params=pop.spring_params(),
+                init_active_params=pop.active_params())
+    init_scal = dict(n_chains=int(sim["n_chains"]), n_beads=int(sim["n_beads"]), n_grid_setup=int(sim["n_grid"]),
+                     grid_spacing=float(sim["grid_spacing"]),
+                     n_steps_update_grid_list=int(sim["n_steps_update_grid_list"]),
+                     max_dist_per_step_setup=float(sim["max_dist_per_step"]), grid_window_setup=int(sim["grid_window"]),
+                     D_init=float(pop.D), Dr_init=float(pop.Dr), b_init_growing=bool(sim["b_init_growing"]),
+                     sim_overrides=spec["sim"], dt_override=spec["dt"])
+    t0 = time.time()
     if spec.get("init_grow", True):
         control.sim_loop(pops, sim, status)        # init-grow until t > 0
         control.early_time_procedures(pops, status, sim)  # ends init-grow
@@ -175,7 +185,7 @@ def run_case(name, spec, mods):
     grow_s = time.time() - t0
 
     # relaxed state and the parameters the hot path sees
-    out = {}
+    out = dict(init)
     out["pos0"] = pop.pos.copy()
     out["tangent0"] = pop.tangent_list.copy()
     out["chain_id"] = pop.chain_id.astype(np.int64)
@@ -190,7 +200,7 @@ def run_case(name, spec, mods):
                 longest_chain_length=pop.longest_chain_length,
                 b_get_orientations=bool(pop.b_get_orientations), noise_seed=spec["noise_seed"],
                 fixed_dt=spec["fixed_dt"], save_every=spec["save_every"],
-                init_grow_steps=int(status.stepnum), init_grow_seconds=grow_s)
+                init_grow_steps=int(status.stepnum), init_grow_seconds=grow_s, **init_scal)
 
     # single-kernel goldens on the relaxed state
     dim = config.dim
