@@ -96,6 +96,10 @@ int ilog2(int v)
 
 }  // namespace
 
+namespace gcr {
+void set_last_error(const char *msg) { g_last_error = msg ? msg : ""; }
+}  // namespace gcr
+
 struct gcr_ctx {
     gcr_config cfg{};
     cudaStream_t stream = nullptr;

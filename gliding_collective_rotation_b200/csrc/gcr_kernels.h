@@ -52,6 +52,9 @@ struct KernelSet {
 
 KernelSet kernel_set(int dim, int precision);
 
+// message returned by gcr_last_error() on the calling thread (gcr_abi.cu)
+void set_last_error(const char *msg);
+
 // gcr_lists.cu
 cudaError_t launch_reference_lists(int dim, const SysP &p, int64_t n_grid, int64_t grid_window,
                                    int64_t *where_is_bead, int64_t *grid_list, int64_t grid_depth1,

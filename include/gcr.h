@@ -194,6 +194,26 @@ GCR_API int gcr_cell_assignment(gcr_ctx *ctx, int32_t slot, int32_t *cell_of_bea
 GCR_API int gcr_philox_noise(int32_t dim, uint64_t seed, int64_t step, int64_t n, int32_t do_trans,
                      int32_t do_rot, double *out, void *cuda_stream);
 
+/* ---- without device allocation ---------------------------------------- */
+/* No counterpart in the reference.  The order parameters of one 2D system
+ * (what gcr_order_params computes) from caller-owned device arrays --
+ * tangents [n_beads][2] (FP64 for GCR_FP64, FP32 for GCR_MIXED) and chain
+ * ids [n_beads] running 0..n_chains-1 in contiguous ranges -- without a
+ * context and without allocating device memory: for callers that must not
+ * call cudaMalloc/cudaFree (an analysis hook running while steps are queued,
+ * since cudaFree synchronises the device; code inside a global-mode stream
+ * capture; an application that owns all device memory through its own
+ * pool).  Its scratch is a static device array of about 1 MiB held by every
+ * GPU that loads the library, sized for at most GCR_NOALLOC_MAX_CHAINS
+ * chains; more chains return GCR_ERR_CAPACITY.  The first call on a device
+ * looks up that array's device address (cudaGetSymbolAddress) and must come
+ * before any stream capture.  Calls that overlap on the GPU race on the
+ * shared scratch.  Synchronises `cuda_stream`; out = [P, S, director]. */
+#define GCR_NOALLOC_MAX_CHAINS 262144
+GCR_API int gcr_order_params_noalloc(int32_t dim, int32_t precision, const void *tangent,
+                                     const int32_t *chain_id, int64_t n_beads, int64_t n_chains,
+                                     double out[3], void *cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
