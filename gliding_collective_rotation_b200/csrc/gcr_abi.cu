@@ -138,6 +138,7 @@ struct gcr_ctx {
     RangeAlloc beads, cells, chains;
     BatchArgs args{};
     int grid_beads = 1, grid_cells = 1, grid_update = 1, grid_pack = 1, grid_sys = 1, grid_pair = 1, grid_scan = 1;
+    int grid_stage0 = 1, grid_stage1 = 1;
     cudaGraphExec_t graph = nullptr;
     bool tiles_dirty = true;
 };
@@ -300,10 +301,10 @@ int enqueue_step(gcr_ctx *c)
     const int bb = c->cfg.block_beads;
     if ((rc = enqueue_cells(c, 0))) return rc;
     if ((rc = launch(c, c->ks.pair, c->grid_pair, bb))) return rc;
-    if ((rc = launch(c, c->ks.stage0, c->grid_beads, bb, c->stage_smem))) return rc;
+    if ((rc = launch(c, c->ks.stage0, c->grid_stage0, bb, c->stage_smem))) return rc;
     if ((rc = enqueue_cells(c, 1))) return rc;
     if ((rc = launch(c, c->ks.pair, c->grid_pair, bb))) return rc;
-    if ((rc = launch(c, c->ks.stage1, c->grid_beads, bb, c->stage_smem))) return rc;
+    if ((rc = launch(c, c->ks.stage1, c->grid_stage1, bb, c->stage_smem))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_dt))) return rc;
     if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_end))) return rc;
@@ -465,9 +466,9 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
         cudaFuncSetAttribute(c->ks.stage0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->stage_smem);
         cudaFuncSetAttribute(c->ks.stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->stage_smem);
     }
-    int gb = kernel_grid(c, c->ks.stage0, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
-    gb = std::min(gb, kernel_grid(c, c->ks.stage1, cfg.block_beads, c->max_bead_tiles, c->stage_smem));
-    c->grid_beads = gb;
+    c->grid_stage0 = kernel_grid(c, c->ks.stage0, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
+    c->grid_stage1 = kernel_grid(c, c->ks.stage1, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
+    c->grid_beads = std::min(c->grid_stage0, c->grid_stage1);
     c->grid_update = kernel_grid(c, c->ks.update, cfg.block_beads, c->max_bead_tiles);
     c->grid_pack = kernel_grid(c, c->ks.pack0, cfg.block_cells, c->max_cell_tiles);
     c->grid_scan = kernel_grid(c, c->ks.scan_local0, cfg.block_cells, c->max_cell_tiles);
@@ -725,13 +726,13 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
         GCR_CUDA(cudaEventRecord(e[1], c->stream));
         if (!rc) rc = launch(c, c->ks.pair, c->grid_pair, bb);
         GCR_CUDA(cudaEventRecord(e[2], c->stream));
-        if (!rc) rc = launch(c, c->ks.stage0, c->grid_beads, bb, c->stage_smem);
+        if (!rc) rc = launch(c, c->ks.stage0, c->grid_stage0, bb, c->stage_smem);
         GCR_CUDA(cudaEventRecord(e[3], c->stream));
         if (!rc) rc = enqueue_cells(c, 1);
         GCR_CUDA(cudaEventRecord(e[4], c->stream));
         if (!rc) rc = launch(c, c->ks.pair, c->grid_pair, bb);
         GCR_CUDA(cudaEventRecord(e[5], c->stream));
-        if (!rc) rc = launch(c, c->ks.stage1, c->grid_beads, bb, c->stage_smem);
+        if (!rc) rc = launch(c, c->ks.stage1, c->grid_stage1, bb, c->stage_smem);
         if (!rc) rc = launch_sys(c, c->ks.sys_dt);
         GCR_CUDA(cudaEventRecord(e[6], c->stream));
         if (!rc) rc = launch(c, c->ks.update, c->grid_update, bb);

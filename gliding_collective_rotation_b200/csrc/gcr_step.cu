@@ -140,6 +140,7 @@ template <int D, typename FT>
 __device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs &A, int k, int &b_out, FT *F)
 {
     using R = typename Rec<FT>::type;
+    constexpr int kPairBuf = 24;  // in-range pairs kept before their forces are summed
     const int nc = p.nc;
     const R *__restrict__ rec = reinterpret_cast<const R *>(A.rec) + p.bead_off;
     const int *__restrict__ cs = A.cstart + p.cell_off;
@@ -173,6 +174,38 @@ __device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs
     const double L = p.L, half_L = p.half_L;
     const int nn = p.n_nearby;
     const int my_chain = __ldg(p.chain + b);
+    // In-range candidates are buffered and their forces summed in a second,
+    // nearly uniform loop: a force evaluation inside the distance loop would
+    // be executed by the whole warp for almost every candidate.  The buffer
+    // keeps discovery order, so the sum order (and the result) is the same
+    // as one loop would give.
+    FT buf_sep[kPairBuf][3];
+    FT buf_ds[kPairBuf];
+    int buf_id[kPairBuf];
+    int nbuf = 0;
+    auto flush = [&]() {
+        for (int q = 0; q < nbuf; q++) {
+            const int bj = buf_id[q];
+            if ((unsigned)bj >= (unsigned)p.n) continue;  // never index outside the system
+            int db = b - bj;
+            db = db < 0 ? -db : db;
+            if ((nn < 0 || db <= nn) && __ldg(p.chain + bj) == my_chain) continue;
+            FT sep[3] = {buf_sep[q][0], buf_sep[q][1], D == 3 ? buf_sep[q][2] : FT(0)};
+            FT ds = buf_ds[q];
+            if (shift != FT(0)) {
+                FT mag = sqrt(ds);
+                FT nm = mag + shift;
+                nm = nm < FT(0) ? FT(0) : nm;
+                FT rs = nm / mag;
+#pragma unroll
+                for (int i = 0; i < D; i++) sep[i] *= rs;
+                ds = nm * nm;
+            }
+            FT coeff = wca_coeff<FT>(ds, p0, p1);
+#pragma unroll
+            for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
+        }
+    };
     int cx[3];
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -210,6 +243,8 @@ __device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs
                 off[0] = (FT)(d - 1) * hf;
                 off[1] = (FT)dy * hf;
                 off[2] = (FT)dz * hf;
+                // phase 1: distance filter only; in-range candidates go to
+                // the buffer in discovery order
                 for (int j = lo[d]; j < hi[d]; j++) {
                     int bj;
                     FT sep[3];
@@ -230,27 +265,22 @@ __device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs
                     FT ds = sep[0] * sep[0] + sep[1] * sep[1];
                     if (D == 3) ds += sep[2] * sep[2];
                     if (FT(0) < ds && ds <= rc2) {
-                        if ((unsigned)bj >= (unsigned)p.n) continue;  // never index outside the system
-                        int db = b - bj;
-                        db = db < 0 ? -db : db;
-                        if ((nn < 0 || db <= nn) && __ldg(p.chain + bj) == my_chain) continue;
-                        if (shift != FT(0)) {
-                            FT mag = sqrt(ds);
-                            FT nm = mag + shift;
-                            nm = nm < FT(0) ? FT(0) : nm;
-                            FT rs = nm / mag;
-#pragma unroll
-                            for (int i = 0; i < D; i++) sep[i] *= rs;
-                            ds = nm * nm;
+                        if (nbuf == kPairBuf) {
+                            flush();
+                            nbuf = 0;
                         }
-                        FT coeff = wca_coeff<FT>(ds, p0, p1);
 #pragma unroll
-                        for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
+                        for (int i = 0; i < D; i++) buf_sep[nbuf][i] = sep[i];
+                        buf_ds[nbuf] = ds;
+                        buf_id[nbuf] = bj;
+                        nbuf++;
                     }
                 }
             }
         }
     }
+    // phase 2: forces of the in-range pairs
+    flush();
 }
 
 template <int D>
