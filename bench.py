@@ -256,7 +256,8 @@ def run_gpu(args):
     specs, desc = make_workload(args.workload, rank=rank, scale=args.scale, systems=args.systems)
     for sp in specs:
         sp.params.cell_factor = args.cell_factor
-    batch = Batch(specs, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph)
+    batch = Batch(specs, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph,
+                  ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads)
     eng = batch.engine
     n_beads = batch.n_beads
     relax_steps = batch.relax(max_steps=args.relax_steps)
@@ -425,6 +426,9 @@ def main():
     ap.add_argument("--systems", type=int, default=256, help="systems of the sweep workload")
     ap.add_argument("--cell-factor", type=float, default=1.0, help="GPU cell side / pair cutoff")
     ap.add_argument("--steps-per-graph", type=int, default=10)
+    ap.add_argument("--ctas-per-sm", type=int, default=0,
+                    help="CTAs per SM of the tile kernels (0: from occupancy, <0: one CTA per tile)")
+    ap.add_argument("--block-beads", type=int, default=256)
     ap.add_argument("--relax-steps", type=int, default=2000)
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--plain", type=int, default=1)

@@ -73,7 +73,7 @@ class Batch:
     """Systems of one dimension and precision resident in one context."""
 
     def __init__(self, specs, precision="mixed", device=None, steps_per_graph=10, cell_depth=None,
-                 block_beads=256, block_cells=256, stream=None):
+                 block_beads=256, block_cells=256, stream=None, ctas_per_sm=0):
         if not specs:
             raise ValueError("empty batch")
         dims = {s.dim for s in specs}
@@ -87,7 +87,7 @@ class Batch:
             cell_depth = default_depth(self.dim, max(s.params.cell_factor for s in specs))
         self.cell_depth = cell_depth
         self._engine_kw = dict(block_beads=block_beads, block_cells=block_cells, steps_per_graph=steps_per_graph,
-                               stream=stream)
+                               stream=stream, ctas_per_sm=ctas_per_sm)
         self.n_beads = sum(s.n for s in specs)
         self.big, self.states = _views(specs, precision, self.device)
         torch.cuda.synchronize(self.device)

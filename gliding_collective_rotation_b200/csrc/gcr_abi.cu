@@ -147,6 +147,9 @@ namespace {
 
 int kernel_grid(const gcr_ctx *c, void *fn, int block, int64_t max_tiles, size_t smem = 0)
 {
+    // ctas_per_sm < 0: one CTA per tile (the hardware scheduler streams the
+    // tiles; CTAs past the live tile count exit at once)
+    if (c->cfg.ctas_per_sm < 0) return (int)std::max<int64_t>(max_tiles, 1);
     int occ = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, block, smem) != cudaSuccess || occ < 1) occ = 1;
     if (c->cfg.ctas_per_sm > 0) occ = std::min(occ, c->cfg.ctas_per_sm);

@@ -136,29 +136,36 @@ __device__ __forceinline__ FT wca_coeff(FT ds, FT p0, FT p1)
 // neighbouring cells, so they walk the same candidate records (uniform trip
 // counts, broadcast loads).  Candidates of cell c are records
 // [cstart[c], cstart[c+1]), sorted by bead id.
+// Pair force of the bead at record k of its system's compact cell list
+// (forces.py:57-145).  Threads of a warp hold beads of the same or of
+// neighbouring cells, so they walk the same candidate records (broadcast
+// loads, similar trip counts).  The three cells cx-1, cx, cx+1 of one row are
+// one contiguous range of records; a row that wraps around the box is two
+// ranges.  Candidates of cell c are records [cstart[c], cstart[c+1]), sorted
+// by bead id, so the sum is taken in a fixed order.
 template <int D, typename FT>
 __device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs &A, int k, int &b_out, FT *F)
 {
     using R = typename Rec<FT>::type;
-    constexpr int kPairBuf = 24;  // in-range pairs kept before their forces are summed
     const int nc = p.nc;
+    const int n = p.n;
     const R *__restrict__ rec = reinterpret_cast<const R *>(A.rec) + p.bead_off;
     const int *__restrict__ cs = A.cstart + p.cell_off;
     int c = __ldg(A.rcell + p.bead_off + k);
     c = (c < 0 || c >= p.n_cells) ? 0 : c;
-    int ci[3];
-    ci[0] = c % nc;
-    ci[1] = (c / nc) % nc;
-    ci[2] = (D == 3) ? c / (nc * nc) : 0;
+    const int cx = c % nc;
+    const int cy0 = (c / nc) % nc;
+    const int cz0 = (D == 3) ? c / (nc * nc) : 0;
     FT own[3] = {FT(0), FT(0), FT(0)};
     double xb[3] = {0.0, 0.0, 0.0};
-    int b;
+    int b, my_chain = 0;
     if constexpr (sizeof(FT) == 4) {
         float4 r = __ldg(rec + k);
         own[0] = r.x;
         own[1] = r.y;
         own[2] = r.z;
         b = __float_as_int(r.w);
+        if (D == 2) my_chain = __float_as_int(r.z);
     } else {
         const double2 *q = reinterpret_cast<const double2 *>(rec + k);
         double2 r0 = __ldg(q), r1 = __ldg(q + 1);
@@ -166,93 +173,66 @@ __device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs
         xb[1] = r0.y;
         xb[2] = r1.x;
         b = (int)r1.y;
+        if (D == 2) my_chain = (int)r1.x;
     }
     b_out = b;
-    if ((unsigned)b >= (unsigned)p.n) return;  // inconsistent list: the caller flags it
+    if ((unsigned)b >= (unsigned)n) return;  // inconsistent list: the caller flags it
+    if (D == 3) my_chain = __ldg(p.chain + b);
     const FT rc2 = (FT)p.rc2, p0 = (FT)p.p0, p1 = (FT)p.p1, shift = (FT)p.shift;
     const FT hf = (FT)p.hf;
     const double L = p.L, half_L = p.half_L;
     const int nn = p.n_nearby;
-    const int my_chain = __ldg(p.chain + b);
-    // In-range candidates are buffered and their forces summed in a second,
-    // nearly uniform loop: a force evaluation inside the distance loop would
-    // be executed by the whole warp for almost every candidate.  The buffer
-    // keeps discovery order, so the sum order (and the result) is the same
-    // as one loop would give.
-    FT buf_sep[kPairBuf][3];
-    FT buf_ds[kPairBuf];
-    int buf_id[kPairBuf];
-    int nbuf = 0;
-    auto flush = [&]() {
-        for (int q = 0; q < nbuf; q++) {
-            const int bj = buf_id[q];
-            if ((unsigned)bj >= (unsigned)p.n) continue;  // never index outside the system
-            int db = b - bj;
-            db = db < 0 ? -db : db;
-            if ((nn < 0 || db <= nn) && __ldg(p.chain + bj) == my_chain) continue;
-            FT sep[3] = {buf_sep[q][0], buf_sep[q][1], D == 3 ? buf_sep[q][2] : FT(0)};
-            FT ds = buf_ds[q];
-            if (shift != FT(0)) {
-                FT mag = sqrt(ds);
-                FT nm = mag + shift;
-                nm = nm < FT(0) ? FT(0) : nm;
-                FT rs = nm / mag;
-#pragma unroll
-                for (int i = 0; i < D; i++) sep[i] *= rs;
-                ds = nm * nm;
-            }
-            FT coeff = wca_coeff<FT>(ds, p0, p1);
-#pragma unroll
-            for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
-        }
-    };
-    int cx[3];
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-        int v = ci[0] + d - 1;
-        cx[d] = v < 0 ? v + nc : (v >= nc ? v - nc : v);
-    }
+    const int span = 3 * A.depth;
+    // the row's ranges: [lo, hi) with the x offset -1/0/+1 cells changing at m1, m2
+    const bool wrap_lo = cx == 0, wrap_hi = cx == nc - 1;
+    const int x_first = wrap_lo ? 0 : cx - 1;          // first cell of the contiguous part
+    const int x_last = wrap_hi ? nc - 1 : cx + 1;      // last cell of the contiguous part
+    const int d_first = wrap_lo ? 0 : -1;              // its x offset in cells
+    const int x_extra = wrap_lo ? nc - 1 : 0;          // the wrapped cell, if any
+    const int d_extra = wrap_lo ? -1 : 1;
+    const int n_seg = (wrap_lo || wrap_hi) ? 2 : 1;
     const int zlo = (D == 3) ? -1 : 0, zhi = (D == 3) ? 1 : 0;
     for (int dz = zlo; dz <= zhi; dz++) {
         int cz = 0;
         if (D == 3) {
-            cz = ci[2] + dz;
+            cz = cz0 + dz;
             cz = cz < 0 ? cz + nc : (cz >= nc ? cz - nc : cz);
         }
 #pragma unroll
         for (int dy = -1; dy <= 1; dy++) {
-            int cy = ci[1] + dy;
+            int cy = cy0 + dy;
             cy = cy < 0 ? cy + nc : (cy >= nc ? cy - nc : cy);
-            const int rowbase = (cz * nc + cy) * nc;
-            int lo[3], hi[3];
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-                int l = __ldg(cs + rowbase + cx[d]);
-                int h = __ldg(cs + rowbase + cx[d] + 1);
-                // a cell holds at most `depth` records inside [0, n): clamp, so
-                // that an inconsistent list can never send a loop out of range
-                l = l < 0 ? 0 : (l > p.n ? p.n : l);
-                h = h < l ? l : (h > p.n ? p.n : h);
-                h = h - l > A.depth ? l + A.depth : h;
-                lo[d] = l;
-                hi[d] = h;
-            }
-#pragma unroll
-            for (int d = 0; d < 3; d++) {
-                FT off[3];
-                off[0] = (FT)(d - 1) * hf;
-                off[1] = (FT)dy * hf;
-                off[2] = (FT)dz * hf;
-                // phase 1: distance filter only; in-range candidates go to
-                // the buffer in discovery order
-                for (int j = lo[d]; j < hi[d]; j++) {
-                    int bj;
+            const int row = (cz * nc + cy) * nc;
+            for (int seg = 0; seg < n_seg; seg++) {
+                int lo, hi, m1, m2, d0;
+                if (seg == 0) {
+                    lo = __ldg(cs + row + x_first);
+                    m1 = __ldg(cs + row + x_first + 1);
+                    m2 = __ldg(cs + row + x_first + 2);
+                    hi = __ldg(cs + row + x_last + 1);
+                    d0 = d_first;
+                } else {
+                    lo = __ldg(cs + row + x_extra);
+                    hi = __ldg(cs + row + x_extra + 1);
+                    m1 = m2 = 0x7fffffff;
+                    d0 = d_extra;
+                }
+                // clamps keep every record index inside [0, n), whatever the list holds
+                lo = lo < 0 ? 0 : (lo > n ? n : lo);
+                hi = hi < lo ? lo : (hi > n ? n : hi);
+                hi = hi - lo > span ? lo + span : hi;
+                const FT o0 = (FT)d0 * hf, o1 = (FT)(d0 + 1) * hf, o2 = (FT)(d0 + 2) * hf;
+                const FT oy = (FT)dy * hf, oz = (FT)dz * hf;
+                for (int j = lo; j < hi; j++) {
+                    int bj, cj = 0;
                     FT sep[3];
                     if constexpr (sizeof(FT) == 4) {
                         float4 r = __ldg(rec + j);
-                        sep[0] = (r.x - own[0]) + off[0];
-                        sep[1] = (r.y - own[1]) + off[1];
-                        if (D == 3) sep[2] = (r.z - own[2]) + off[2];
+                        const FT ox = j < m1 ? o0 : (j < m2 ? o1 : o2);
+                        sep[0] = (r.x - own[0]) + ox;
+                        sep[1] = (r.y - own[1]) + oy;
+                        if (D == 3) sep[2] = (r.z - own[2]) + oz;
+                        else cj = __float_as_int(r.z);
                         bj = __float_as_int(r.w);
                     } else {
                         const double2 *q = reinterpret_cast<const double2 *>(rec + j);
@@ -260,27 +240,35 @@ __device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs
                         sep[0] = inbounds(r0.x, xb[0], half_L, L);
                         sep[1] = inbounds(r0.y, xb[1], half_L, L);
                         if (D == 3) sep[2] = inbounds(r1.x, xb[2], half_L, L);
+                        else cj = (int)r1.x;
                         bj = (int)r1.y;
                     }
                     FT ds = sep[0] * sep[0] + sep[1] * sep[1];
                     if (D == 3) ds += sep[2] * sep[2];
-                    if (FT(0) < ds && ds <= rc2) {
-                        if (nbuf == kPairBuf) {
-                            flush();
-                            nbuf = 0;
-                        }
-#pragma unroll
-                        for (int i = 0; i < D; i++) buf_sep[nbuf][i] = sep[i];
-                        buf_ds[nbuf] = ds;
-                        buf_id[nbuf] = bj;
-                        nbuf++;
+                    if (!(FT(0) < ds && ds <= rc2)) continue;
+                    if ((unsigned)bj >= (unsigned)n) continue;  // never index outside the system
+                    int db = b - bj;
+                    db = db < 0 ? -db : db;
+                    if (nn < 0 || db <= nn) {
+                        if (D == 3) cj = __ldg(p.chain + bj);
+                        if (cj == my_chain) continue;
                     }
+                    if (shift != FT(0)) {
+                        FT mag = sqrt(ds);
+                        FT nm = mag + shift;
+                        nm = nm < FT(0) ? FT(0) : nm;
+                        FT rs = nm / mag;
+#pragma unroll
+                        for (int i = 0; i < D; i++) sep[i] *= rs;
+                        ds = nm * nm;
+                    }
+                    FT coeff = wca_coeff<FT>(ds, p0, p1);
+#pragma unroll
+                    for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
                 }
             }
         }
     }
-    // phase 2: forces of the in-range pairs
-    flush();
 }
 
 template <int D>
@@ -513,15 +501,17 @@ __global__ void __launch_bounds__(512) k_pack(BatchArgs A)
 #pragma unroll
             for (int i = 0; i < D; i++) x[i] = X[(size_t)b * D + i];
             R r;
+            // 2D records carry the bead's chain id in the spare z slot, so the
+            // pair loop's exclusion test needs no second load
             if constexpr (sizeof(FT) == 4) {
                 r.x = (float)(x[0] - ctr[0]);
                 r.y = (float)(x[1] - ctr[1]);
-                r.z = (D == 3) ? (float)(x[2] - ctr[2]) : 0.f;
+                r.z = (D == 3) ? (float)(x[2] - ctr[2]) : __int_as_float(__ldg(p.chain + b));
                 r.w = __int_as_float(b);
             } else {
                 r.x = x[0];
                 r.y = x[1];
-                r.z = x[2];
+                r.z = (D == 3) ? x[2] : (double)__ldg(p.chain + b);
                 r.w = (double)b;
             }
             out[j] = r;
@@ -574,7 +564,7 @@ __global__ void __launch_bounds__(512) k_pair(BatchArgs A)
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const Tile tl = A.bead_tiles[t];
         const SysP &p = A.P[tl.sys];
-        const SysS &s = A.S[tl.sys];
+        SysS &s = A.S[tl.sys];
         if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal) || !p.calc_wca) continue;
         const int k = tl.begin + threadIdx.x;
         if (k >= p.n || threadIdx.x >= A.tile_beads) continue;
@@ -582,7 +572,7 @@ __global__ void __launch_bounds__(512) k_pair(BatchArgs A)
         int b;
         pair_force_sorted<D, FT>(p, A, k, b, F);
         if (b < 0 || b >= p.n) {
-            atomicOr((int *)&s.flags, kFlagListCorrupt);
+            atomicOr(&s.flags, kFlagListCorrupt);
             continue;
         }
         FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;

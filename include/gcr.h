@@ -75,7 +75,7 @@ typedef struct {
     int32_t block_beads;      /* threads per CTA of bead kernels (64..512) */
     int32_t block_cells;      /* threads per CTA of the cell kernel (64..512) */
     int32_t steps_per_graph;  /* SRK2 steps per captured CUDA graph (1..64) */
-    int32_t ctas_per_sm;      /* persistent CTAs per SM (0 = from occupancy) */
+    int32_t ctas_per_sm;      /* persistent CTAs per SM (0 = from occupancy, <0 = one CTA per tile) */
 } gcr_config;
 
 /* One system.  The packed arrays follow the reference's packing exactly. */
