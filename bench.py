@@ -414,13 +414,46 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+# --------------------------------------------------------------------------
+# serving: a Poisson trace through the continuous-batching server
+# --------------------------------------------------------------------------
+
+def run_serve(args):
+    import torch
+    from gliding_collective_rotation_b200 import serve as S
+    from gliding_collective_rotation_b200 import workloads as W
+
+    torch.cuda.set_device(0)
+    tr = W.serve_trace(args.requests, rate=args.rate, seed=7, max_beads=args.max_beads, min_steps=args.min_steps,
+                       max_steps=args.max_steps)
+    reqs = [S.request_from_trace(e, relax=True, obs_every=args.obs_every) for e in tr]
+    srv = S.Server(2, args.precision, hbm_budget=int(args.hbm_budget_gb * (1 << 30)), chunk=args.chunk)
+    clocks = ClockSampler(0)
+    clocks.start()
+    res = srv.serve(reqs, timeout=args.serve_timeout)
+    clk = clocks.stop()
+    srv.close()
+    s = S.summarize(res)
+    line = {
+        "metric": "bead-steps/s", "value": s["bead_steps_per_s"], "unit": "bead-steps/s", "n_gpus": 1,
+        "steps": None, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": f"served trace: {args.requests} requests, Poisson {args.rate}/s, beads log-uniform "
+                               f"[1e3, {args.max_beads:.0e}], steps uniform [{args.min_steps}, {args.max_steps}], "
+                               f"relaxed on arrival, P/S/angle every {args.obs_every} steps",
+                   "chunk": args.chunk, "hbm_budget_gb": args.hbm_budget_gb, **s},
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="gcr", choices=["gcr", "reference"])
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "large", "config1", "config5"])
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "large", "config1", "config5", "serve"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--systems", type=int, default=256, help="systems of the sweep workload")
@@ -438,7 +471,19 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--cpu-systems", type=int, default=4)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--requests", type=int, default=64, help="serve: requests in the trace")
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate per second")
+    ap.add_argument("--max-beads", type=float, default=2e5, help="serve: largest request")
+    ap.add_argument("--min-steps", type=int, default=1000)
+    ap.add_argument("--max-steps", type=int, default=5000)
+    ap.add_argument("--obs-every", type=int, default=100)
+    ap.add_argument("--chunk", type=int, default=200)
+    ap.add_argument("--hbm-budget-gb", type=float, default=16.0)
+    ap.add_argument("--serve-timeout", type=float, default=600.0)
     args = ap.parse_args()
+    if args.workload == "serve" and args.impl == "gcr":
+        run_serve(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

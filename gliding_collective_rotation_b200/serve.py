@@ -1,0 +1,293 @@
+"""Continuous batching of simulation requests on one GPU.
+
+A request is one independent system (a ``SystemSpec``) to be advanced a
+given number of SRK2 steps, with the order parameters P, S and the director
+angle (``output_methods.calc_avg_phi_chain`` + ``analysis.polar_orderparameter``
++ ``analysis.nematic_orderparameter``, output_methods.py:492-510,
+analysis.py:294-328) sampled every ``obs_every`` steps.  The server keeps
+every resident system in one ``Engine`` context, so one captured graph of
+persistent kernels advances all of them at once.  Requests are admitted as
+soon as the context's bead, cell and slot ranges have room (the library's
+allocator is the memory budget); a finished request is evicted at once and
+its ranges go to the next one.  Admission is first come first served, and a
+later request that fits may go ahead of a head request that does not
+(backfill) unless the head has waited longer than ``max_head_wait`` seconds.
+
+Fresh chains laid straight at random overlap, so by default a request first
+relaxes under the reference's adaptive dt (``max_dist_per_step`` of
+``config.grid_list_setup``, config.py:189) until the step takes the full dt,
+then runs its requested steps at the fixed dt.  Relaxation steps are
+reported apart from the requested ones.
+
+Calls are chunked: every system is armed for at most ``chunk`` steps (and
+never past its next observation step), the graph runs, statuses come back in
+one copy, finished requests leave.  With a fixed dt a system's trajectory
+does not depend on how its steps are split into calls (the Philox noise is
+keyed by bead and step, and the pair sums are taken in a fixed order), so a
+request served in a busy mix ends bit-for-bit where it ends alone.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from .batch import MAX_DEPTH, OVERFLOW, default_depth
+from .engine import Engine, SystemState
+from .workloads import SystemSpec, make_system
+
+# resident bytes per bead of the state tensors (FP64 pos/pos1, FT tangent/forces, chain id)
+_STATE_BYTES = {"mixed": 2 * 16 + 2 * 8 + 4, "fp64": 2 * 16 + 2 * 16 + 4}
+
+
+@dataclass
+class Request:
+    id: int
+    spec: SystemSpec
+    steps: int
+    arrival: float = 0.0
+    obs_every: int = 0
+    relax: bool = True
+
+
+@dataclass
+class Result:
+    id: int
+    n_beads: int
+    steps: int
+    arrival: float
+    admitted: float
+    finished: float
+    relax_steps: int
+    pos: np.ndarray
+    tangent: np.ndarray
+    series: np.ndarray          # rows (step, P, S, angle)
+    flags: int
+
+    @property
+    def latency(self):
+        return self.finished - self.arrival
+
+
+@dataclass
+class _Live:
+    req: Request
+    state: SystemState
+    admitted: float
+    relaxing: bool
+    relax_steps: int = 0
+    done: int = 0
+    series: list = field(default_factory=list)
+
+
+def request_from_trace(entry, relax=True, obs_every=0):
+    """A ``Request`` from one entry of ``workloads.serve_trace``."""
+    spec = make_system(f"req{entry['id']}", 2, entry["n_chains"], entry["chain_length"], entry["L"],
+                       seed=10_000 + entry["id"], kappa=entry["kappa"], v_tan_angle=entry["v_tan_angle"],
+                       noise_seed=entry["seed"])
+    return Request(entry["id"], spec, entry["steps"], entry["arrival"], obs_every, relax)
+
+
+class Server:
+    """One GPU, one context, many resident requests."""
+
+    def __init__(self, dim=2, precision="mixed", hbm_budget=8 << 30, cells_per_bead=4.0, max_systems=256,
+                 chunk=200, device=None, cell_depth=None, relax_max_steps=4000, max_head_wait=5.0,
+                 steps_per_graph=10):
+        self.dim, self.precision = dim, precision
+        self.device = torch.device(device or "cuda")
+        self.chunk = int(chunk)
+        self.relax_max_steps = int(relax_max_steps)
+        self.max_head_wait = float(max_head_wait)
+        self.cell_depth = cell_depth or default_depth(dim, 1.0)
+        self.max_systems = int(max_systems)
+        self.cells_per_bead = float(cells_per_bead)
+        self.steps_per_graph = int(steps_per_graph)
+        self.hbm_budget = int(hbm_budget)
+        self._size_context()
+        self.engine = self._make_engine()
+        self.live: dict[int, _Live] = {}
+        self.queue: list[Request] = []
+        self.results: list[Result] = []
+        self.t0 = None
+
+    # -- memory ----------------------------------------------------------------
+    def _per_bead_bytes(self):
+        ft = 4 if self.precision == "mixed" else 8
+        rec = 16 if self.precision == "mixed" else 32
+        scratch = rec + 4 + 2 * self.dim * ft + 1          # records, record cells, pair force, noise, topology
+        per_cell = 4 * (self.cell_depth + 3)               # slots, two counts, start
+        return _STATE_BYTES[self.precision] + scratch + self.cells_per_bead * per_cell
+
+    def _size_context(self):
+        self.bead_capacity = max(1024, int(self.hbm_budget / self._per_bead_bytes()))
+        self.cell_capacity = int(self.cells_per_bead * self.bead_capacity)
+
+    def _make_engine(self):
+        return Engine(self.dim, self.precision, device=self.device, bead_capacity=self.bead_capacity,
+                      system_capacity=self.max_systems, cell_capacity=self.cell_capacity,
+                      cell_depth=self.cell_depth, steps_per_graph=self.steps_per_graph)
+
+    def fits_ever(self, req: Request):
+        return req.spec.n <= self.bead_capacity
+
+    # -- clock -----------------------------------------------------------------
+    def now(self):
+        return time.perf_counter() - self.t0
+
+    # -- admission -------------------------------------------------------------
+    def _admit_one(self, req: Request):
+        sp = req.spec
+        p = sp.params
+        if req.relax:
+            p.max_dist_per_step = sp.relax_mdps
+        st = SystemState.from_host(sp.pos, sp.tangent, sp.chain_id, sp.rest_lengths, p, precision=self.precision,
+                                   device=self.device)
+        slot = self.engine.try_admit(st)
+        if slot is None:
+            del st
+            return False
+        self.live[slot] = _Live(req, st, self.now(), relaxing=req.relax)
+        return True
+
+    def _admit(self):
+        now = self.now()
+        arrived = [r for r in self.queue if r.arrival <= now]
+        if not arrived:
+            return
+        blocked = None  # the first arrived request that did not fit
+        for r in arrived:
+            if len(self.live) >= self.max_systems:
+                break
+            if blocked is not None and now - blocked.arrival > self.max_head_wait:
+                break  # no backfill past a head that has waited too long
+            if self._admit_one(r):
+                self.queue.remove(r)
+            elif blocked is None:
+                blocked = r
+
+    # -- overflow --------------------------------------------------------------
+    def _regrow(self, statuses):
+        if self.cell_depth >= MAX_DEPTH:
+            raise RuntimeError("GPU cell depth limit reached")
+        for slot, lv in self.live.items():
+            lv.state.params.step = statuses[slot]["step"]
+        old = list(self.live.values())
+        self.engine.close()
+        self.cell_depth *= 2
+        self._size_context()
+        self.engine = self._make_engine()
+        self.live = {}
+        for lv in old:
+            slot = self.engine.admit(lv.state)
+            self.live[slot] = lv
+
+    # -- one round of calls ----------------------------------------------------
+    def _plan(self, lv: _Live):
+        if lv.relaxing:
+            return min(self.chunk, self.relax_max_steps - lv.relax_steps)
+        left = lv.req.steps - lv.done
+        k = min(self.chunk, left)
+        if lv.req.obs_every > 0:
+            k = min(k, lv.req.obs_every - lv.done % lv.req.obs_every)
+        return k
+
+    def _round(self):
+        slots = sorted(self.live)
+        plan = [self._plan(self.live[s]) for s in slots]
+        dts = [self.live[s].req.spec.dt for s in slots]
+        self.engine.call_begin_many(slots, plan, dts)
+        self.engine.run(max(plan))
+        statuses = {s: self.engine.status(s) for s in slots}
+        finished, overflow = [], False
+        for s, k in zip(slots, plan):
+            lv, st = self.live[s], statuses[s]
+            # steps completed before a stop are valid; an overflowed system
+            # resumes from there once the cells have grown
+            n_done = st["steps_done"]
+            if st["flags"] & OVERFLOW:
+                overflow = True
+                if lv.relaxing:
+                    lv.relax_steps += n_done
+                else:
+                    lv.done += n_done
+                continue
+            if lv.relaxing:
+                lv.relax_steps += n_done
+                full = st["dt"] >= lv.req.spec.dt * (1 - 1e-12)
+                if full or lv.relax_steps >= self.relax_max_steps:
+                    lv.relaxing = False
+                    lv.state.params.max_dist_per_step = math.inf
+                    self.engine.update_params(lv.state)
+                continue
+            lv.done += n_done
+            if st["flags"] or n_done < k:
+                finished.append(s)  # a failed system leaves with its flags
+                continue
+            if lv.req.obs_every > 0 and lv.done % lv.req.obs_every == 0:
+                lv.series.append((lv.done, *self.engine.order_params(s)))
+            if lv.done >= lv.req.steps:
+                finished.append(s)
+        for s in finished:
+            self._finish(s, statuses[s]["flags"])
+        if overflow:
+            self._regrow({s: statuses[s] for s in self.live})
+
+    def _finish(self, slot, flags):
+        lv = self.live.pop(slot)
+        st = lv.state
+        self.engine.synchronize()
+        res = Result(lv.req.id, st.n, lv.done, lv.req.arrival, lv.admitted, self.now(), lv.relax_steps,
+                     st.pos.cpu().numpy(), st.tangent.double().cpu().numpy(),
+                     np.array(lv.series, dtype=np.float64).reshape(-1, 4), int(flags))
+        self.engine.evict(slot)
+        self.results.append(res)
+
+    # -- driver ----------------------------------------------------------------
+    def serve(self, requests, timeout=None):
+        """Serve ``requests`` (arrival times in seconds from the start) until
+        all are done; returns the results in completion order."""
+        for r in requests:
+            if not self.fits_ever(r):
+                raise ValueError(f"request {r.id}: {r.spec.n} beads exceed the context ({self.bead_capacity})")
+        self.queue = sorted(requests, key=lambda r: (r.arrival, r.id))
+        self.t0 = time.perf_counter()
+        while self.queue or self.live:
+            if timeout is not None and self.now() > timeout:
+                raise TimeoutError(f"serving did not finish in {timeout} s")
+            self._admit()
+            if not self.live:
+                if self.queue:
+                    wait = self.queue[0].arrival - self.now()
+                    if wait > 0:
+                        time.sleep(min(wait, 0.05))
+                    elif not self._admit_one_blocking():
+                        raise RuntimeError("a request does not fit an empty context")
+                continue
+            self._round()
+        return self.results
+
+    def _admit_one_blocking(self):
+        head = self.queue[0]
+        if self._admit_one(head):
+            self.queue.remove(head)
+            return True
+        return False
+
+    def close(self):
+        self.engine.close()
+
+
+def summarize(results, makespan=None):
+    """Latency percentiles and throughput of a served trace."""
+    lat = np.array([r.latency for r in results])
+    bead_steps = float(sum(r.n_beads * r.steps for r in results))
+    relax = float(sum(r.n_beads * r.relax_steps for r in results))
+    span = makespan if makespan is not None else max(r.finished for r in results)
+    return {"requests": len(results), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+            "bead_steps": bead_steps, "relax_bead_steps": relax, "makespan_s": span,
+            "bead_steps_per_s": bead_steps / span if span > 0 else float("nan"),
+            "failed": sum(1 for r in results if r.flags)}
