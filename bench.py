@@ -77,23 +77,27 @@ def make_workload(name, rank=0, scale=1.0, systems=256):
 # algorithmic bytes per kernel launch (HBM roofline)
 # --------------------------------------------------------------------------
 
-def algorithmic_bytes(dim, precision, n_beads, n_cells, get_orient, rot_diff):
+def algorithmic_bytes(dim, precision, n_beads, n_cells, get_orient, rot_diff, list_mean, builds_per_stage):
     """Minimum DRAM bytes of one launch of each kernel group: every input read
-    once and every output written once (neighbour records counted once)."""
+    once and every output written once.  A list build (bin + sort + build)
+    reads the positions, writes and reads one cell slot per bead, writes the
+    list and the build positions; it runs for a fraction `builds_per_stage`
+    of the beads per stage (measured), and that fraction of its bytes is
+    charged to each list launch."""
     P = 8                                   # FP64 position component
     F = 8 if precision == "fp64" else 4     # force / tangent / noise component
-    R = 32 if precision == "fp64" else 16   # packed record per bead
     tan = dim * F if get_orient else 0
-    cells = n_beads * (dim * P + 4 + R + 4) + n_cells * 20
-    pair = n_beads * (R + 4 + R + 4 + dim * F)
-    stage0 = n_beads * (dim * P + 1 + dim * F + dim * F + dim * P + tan + dim * F + 8)
+    build = n_beads * (dim * P + 4 + 4 + 4 * list_mean + 4 + dim * P) + n_cells * 8
+    lists = builds_per_stage * build
+    pair = n_beads * (dim * P + 4 + 4 * list_mean + dim * F)
+    stage0 = n_beads * (dim * P + 1 + dim * F + dim * F + dim * P + tan + dim * F + dim * P + 8)
     stage1 = n_beads * (dim * P + 1 + dim * F + dim * F + dim * F + tan)
-    update = n_beads * (dim * P + dim * F + dim * F + dim * P + 8 + (2 * dim * F if rot_diff else 0))
-    return {"cells_pos": cells, "pair_pos": pair, "stage0": stage0, "cells_pos1": cells, "pair_pos1": pair,
+    update = n_beads * (dim * P + dim * F + dim * F + dim * P + dim * P + 8 + (2 * dim * F if rot_diff else 0))
+    return {"lists_pos": lists, "pair_pos": pair, "stage0": stage0, "lists_pos1": lists, "pair_pos1": pair,
             "stage1": stage1, "update": update}
 
 
-KERNELS = ["cells_pos", "pair_pos", "stage0", "cells_pos1", "pair_pos1", "stage1", "update"]
+KERNELS = ["lists_pos", "pair_pos", "stage0", "lists_pos1", "pair_pos1", "stage1", "update"]
 
 
 # --------------------------------------------------------------------------
@@ -256,8 +260,9 @@ def run_gpu(args):
     specs, desc = make_workload(args.workload, rank=rank, scale=args.scale, systems=args.systems)
     for sp in specs:
         sp.params.cell_factor = args.cell_factor
+        sp.params.skin = args.skin
     batch = Batch(specs, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph,
-                  ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads)
+                  ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads, list_depth=args.list_depth or None)
     eng = batch.engine
     n_beads = batch.n_beads
     relax_steps = batch.relax(max_steps=args.relax_steps)
@@ -271,6 +276,7 @@ def run_gpu(args):
             dist.barrier()
 
     # ---- device-timed batched steps -------------------------------------
+    builds0 = [s["list_builds"] for s in batch.statuses()]
     batch.begin(args.steps)
     clocks = ClockSampler(local)
     barrier()
@@ -296,6 +302,11 @@ def run_gpu(args):
     steps_done = min(s["steps_done"] for s in st)
     flags = sorted({s["flags"] for s in st})
     value = world * n_beads * args.steps / (ms / 1e3)
+    # neighbour lists: mean length, and bead-builds per stage in the timed region
+    list_entries = sum(eng.neighbour_list(x.slot, partners=False)[3] for x in batch.states)
+    list_mean = list_entries / n_beads
+    bead_builds = sum((s["list_builds"] - b0) * x.n for s, b0, x in zip(st, builds0, batch.states))
+    builds_per_stage = bead_builds / (2.0 * args.steps * n_beads)
 
     # ---- per-kernel profile (roofline) ----------------------------------
     batch.begin(args.profile_steps)
@@ -305,7 +316,8 @@ def run_gpu(args):
     n_cells = sum(footprint(cfg, s.params, s.n, len(s.rest_lengths))[0] for s in specs)
     get_orient = bool(specs[0].params.spring_params[4])
     rot_diff = (not get_orient) and specs[0].params.Dr > 0
-    alg = algorithmic_bytes(batch.dim, args.precision, n_beads, n_cells, get_orient, rot_diff)
+    alg = algorithmic_bytes(batch.dim, args.precision, n_beads, n_cells, get_orient, rot_diff, list_mean,
+                            builds_per_stage)
     dom = int(np.argmax(kms))
     pk = peaks()
     achieved = alg[KERNELS[dom]] / (kms[dom] / 1e3) / 1e9
@@ -386,7 +398,7 @@ def run_gpu(args):
                "sample": f"{args.cpu_steps} steps of {', '.join(used)} ({secs:.1f} s)"}
 
     working_set = sum(v.numel() * v.element_size() for v in big.values()) + eng.cfg.cell_capacity * (
-        8 + eng.cfg.cell_depth * (4 + (32 if args.precision == "fp64" else 16)))
+        8 + eng.cfg.cell_depth * 4) + n_beads * (4 * list_mean + 4 + 8 * batch.dim)
     line = {
         "metric": "bead-steps/s", "value": value, "unit": "bead-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -397,8 +409,10 @@ def run_gpu(args):
                    "parallelism": f"{world} GPU(s), independent systems per GPU",
                    "l2": f"inputs larger than L2: working set {working_set / 1e6:.0f} MB per GPU > 126 MB",
                    "relax_steps": relax_steps, "steps_done": steps_done, "flags": flags,
-                   "cell_factor": args.cell_factor,
-                   "steps_per_graph": args.steps_per_graph, "cell_depth": batch.cell_depth},
+                   "cell_factor": args.cell_factor, "skin": args.skin,
+                   "steps_per_graph": args.steps_per_graph, "cell_depth": batch.cell_depth,
+                   "list_depth": batch.list_depth, "list_mean": list_mean,
+                   "list_builds_per_stage": builds_per_stage},
         "e2e": e2e, "roofline": roofline, "clocks": clk,
         "gpu_launches": 13 * args.steps + 1,
     }
@@ -462,6 +476,8 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0,
                     help="CTAs per SM of the tile kernels (0: from occupancy, <0: one CTA per tile)")
     ap.add_argument("--block-beads", type=int, default=256)
+    ap.add_argument("--skin", type=float, default=0.3, help="Verlet skin of the neighbour lists")
+    ap.add_argument("--list-depth", type=int, default=0, help="neighbour slots per bead (0: default)")
     ap.add_argument("--relax-steps", type=int, default=2000)
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--plain", type=int, default=1)

@@ -16,7 +16,7 @@ GCR_OK = 0
 ERRORS = {-1: "BAD_ARG", -2: "CUDA", -3: "OOM", -4: "NONFINITE", -5: "TIMEOUT", -6: "CAPACITY",
           -7: "STATE", -8: "OVERFLOW"}
 GCR_FP64, GCR_MIXED = 0, 1
-FLAG_CELL_OVERFLOW, FLAG_NONFINITE, FLAG_NEXT_OVERFLOW = 1, 2, 4
+FLAG_CELL_OVERFLOW, FLAG_NONFINITE, FLAG_NEXT_OVERFLOW, FLAG_LIST_CORRUPT, FLAG_LIST_OVERFLOW = 1, 2, 4, 8, 16
 
 
 class GcrError(RuntimeError):
@@ -29,7 +29,7 @@ class Config(C.Structure):
     _fields_ = [("dim", C.c_int32), ("precision", C.c_int32), ("bead_capacity", C.c_int64),
                 ("system_capacity", C.c_int32), ("cell_capacity", C.c_int64), ("cell_depth", C.c_int32),
                 ("block_beads", C.c_int32), ("block_cells", C.c_int32), ("steps_per_graph", C.c_int32),
-                ("ctas_per_sm", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("list_depth", C.c_int32)]
 
 
 class SystemDesc(C.Structure):
@@ -39,7 +39,7 @@ class SystemDesc(C.Structure):
                 ("self_propel", C.c_int32), ("n_nearby", C.c_int32), ("D", C.c_double), ("Dr", C.c_double),
                 ("radius", C.c_double), ("dtmax", C.c_double), ("max_dist_per_step", C.c_double),
                 ("rk_cheat", C.c_double), ("seed", C.c_uint64), ("step", C.c_int64),
-                ("cell_factor", C.c_double)]
+                ("cell_factor", C.c_double), ("skin", C.c_double)]
 
 
 class SystemBuffers(C.Structure):
@@ -54,7 +54,8 @@ class Call(C.Structure):
 
 class Status(C.Structure):
     _fields_ = [("dt", C.c_double), ("dt_used", C.c_double), ("max_forces_strength", C.c_double),
-                ("steps_done", C.c_int64), ("step", C.c_int64), ("flags", C.c_int32), ("active", C.c_int32)]
+                ("steps_done", C.c_int64), ("step", C.c_int64), ("flags", C.c_int32), ("active", C.c_int32),
+                ("list_builds", C.c_int64)]
 
 
 # exported symbols and their signatures (every declaration of include/gcr.h)
@@ -80,6 +81,8 @@ SIGNATURES = {
     "gcr_reference_lists": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
                                       C.c_int64, C.c_void_p, C.c_int64, C.c_int32]),
     "gcr_cell_assignment": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_int32)]),
+    "gcr_neighbour_list": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
+                                     C.POINTER(C.c_int64)]),
     "gcr_philox_noise": (C.c_int, [C.c_int32, C.c_uint64, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
                                    C.c_void_p, C.c_void_p]),
     "gcr_order_params_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64,

@@ -18,22 +18,33 @@ import math
 import numpy as np
 import torch
 
-from ._lib import FLAG_CELL_OVERFLOW, FLAG_NEXT_OVERFLOW
+from ._lib import FLAG_CELL_OVERFLOW, FLAG_LIST_OVERFLOW, FLAG_NEXT_OVERFLOW
 from .engine import Engine, SystemState, footprint, default_config
 
-OVERFLOW = FLAG_CELL_OVERFLOW | FLAG_NEXT_OVERFLOW
+OVERFLOW = FLAG_CELL_OVERFLOW | FLAG_NEXT_OVERFLOW | FLAG_LIST_OVERFLOW
 MAX_DEPTH = 128
+MAX_LIST_DEPTH = 1024
 
 
 def default_depth(dim, cell_factor):
-    """Slots per GPU cell: 16 (2D) / 32 (3D) at the cutoff, scaled with the
-    cell volume and rounded up to a power of two."""
+    """Slots per GPU cell: 16 (2D) / 32 (3D) for a cell of side r_cut, scaled
+    with the cell volume and rounded up to a power of two."""
     base = 16 if dim == 2 else 32
     want = base * max(1.0, cell_factor) ** dim
     d = 8
     while d < want and d < MAX_DEPTH:
         d *= 2
     return d
+
+
+def cell_scale(params):
+    """GPU cell side over the pair cutoff: (r_cut + skin) * cell_factor / r_cut."""
+    rc = float(params.wca_params[3])
+    return max(1.0, params.cell_factor) * (rc + max(0.0, params.skin)) / rc
+
+
+def default_list_depth(dim):
+    return 32 if dim == 2 else 96
 
 
 def _views(specs, precision, device):
@@ -73,7 +84,7 @@ class Batch:
     """Systems of one dimension and precision resident in one context."""
 
     def __init__(self, specs, precision="mixed", device=None, steps_per_graph=10, cell_depth=None,
-                 block_beads=256, block_cells=256, stream=None, ctas_per_sm=0):
+                 block_beads=256, block_cells=256, stream=None, ctas_per_sm=0, list_depth=None):
         if not specs:
             raise ValueError("empty batch")
         dims = {s.dim for s in specs}
@@ -84,8 +95,9 @@ class Batch:
         self.precision = precision
         self.device = torch.device(device or "cuda")
         if cell_depth is None:
-            cell_depth = default_depth(self.dim, max(s.params.cell_factor for s in specs))
+            cell_depth = default_depth(self.dim, max(cell_scale(s.params) for s in specs))
         self.cell_depth = cell_depth
+        self.list_depth = list_depth or default_list_depth(self.dim)
         self._engine_kw = dict(block_beads=block_beads, block_cells=block_cells, steps_per_graph=steps_per_graph,
                                stream=stream, ctas_per_sm=ctas_per_sm)
         self.n_beads = sum(s.n for s in specs)
@@ -95,11 +107,11 @@ class Batch:
         self._make_engine()
 
     def _make_engine(self):
-        cfg = default_config(self.dim, self.precision, cell_depth=self.cell_depth)
+        cfg = default_config(self.dim, self.precision, cell_depth=self.cell_depth, list_depth=self.list_depth)
         cells = sum(footprint(cfg, s.params, s.n, len(s.rest_lengths))[0] for s in self.specs)
         self.engine = Engine(self.dim, self.precision, device=self.device, bead_capacity=self.n_beads,
                              system_capacity=len(self.specs), cell_capacity=max(cells, 1),
-                             cell_depth=self.cell_depth, **self._engine_kw)
+                             cell_depth=self.cell_depth, list_depth=self.list_depth, **self._engine_kw)
         for st in self.states:
             self.engine.admit(st)
 
@@ -108,15 +120,24 @@ class Batch:
         return any(s["flags"] & OVERFLOW for s in statuses)
 
     def regrow(self):
-        """Double the slots per GPU cell after an overflow (the reference
-        doubles its list depth the same way, updates.py:257-267) and re-admit
-        every system; step counters carry over, so the noise stream goes on."""
-        if self.cell_depth >= MAX_DEPTH:
-            raise RuntimeError("GPU cell depth limit reached")
-        for st, s in zip(self.states, self.statuses()):
+        """Double the slots per GPU cell or per neighbour list after an
+        overflow (the reference doubles its list depths the same way,
+        updates.py:257-267) and re-admit every system; step counters carry
+        over, so the noise stream goes on."""
+        sts = self.statuses()
+        flags = 0
+        for st, s in zip(self.states, sts):
             st.params.step = s["step"]
+            flags |= s["flags"]
+        cell = bool(flags & FLAG_CELL_OVERFLOW)
+        lst = bool(flags & FLAG_LIST_OVERFLOW) or not cell
+        if (cell and self.cell_depth >= MAX_DEPTH) or (lst and self.list_depth >= MAX_LIST_DEPTH):
+            raise RuntimeError("GPU cell or list depth limit reached")
         self.engine.close()
-        self.cell_depth *= 2
+        if cell:
+            self.cell_depth *= 2
+        if lst:
+            self.list_depth *= 2
         self._make_engine()
 
     # -- calls -------------------------------------------------------------------

@@ -114,21 +114,18 @@ struct gcr_ctx {
     Tile *d_cell_tiles = nullptr;
     int *d_ntiles = nullptr;  // [0] bead tiles, [1] cell tiles
     uint8_t *topo = nullptr;
-    int *cnt0 = nullptr;
-    int *cnt1 = nullptr;
+    int *cnt = nullptr;
+    int *ncell = nullptr;
     int *items = nullptr;
-    void *rec = nullptr;
+    int *nbr = nullptr;
+    int *ncount = nullptr;
+    double *xref = nullptr;
     void *xi = nullptr;
     void *fp = nullptr;
-    int *cstart = nullptr;
-    int *rcell = nullptr;
-    int *tsum = nullptr;
-    int *toff = nullptr;
     size_t stage_smem = 0;
     int32_t *chain_starts = nullptr;
     int *d_err = nullptr;
     double *d_out = nullptr;
-    size_t rec_bytes = 0;
     int64_t max_bead_tiles = 0, max_cell_tiles = 0;
     // host mirrors
     std::vector<Slot> slots;
@@ -137,7 +134,7 @@ struct gcr_ctx {
     std::vector<Tile> h_bead_tiles, h_cell_tiles;
     RangeAlloc beads, cells, chains;
     BatchArgs args{};
-    int grid_beads = 1, grid_cells = 1, grid_update = 1, grid_pack = 1, grid_sys = 1, grid_pair = 1, grid_scan = 1;
+    int grid_update = 1, grid_sys = 1, grid_pair = 1, grid_bin = 1, grid_sort = 1, grid_build = 1;
     int grid_stage0 = 1, grid_stage1 = 1;
     cudaGraphExec_t graph = nullptr;
     bool tiles_dirty = true;
@@ -167,7 +164,6 @@ int rebuild_tiles(gcr_ctx *c)
         const Slot &sl = c->slots[s];
         if (!sl.used) continue;
         for (int64_t b = 0; b < sl.desc.n_beads; b += tb) c->h_bead_tiles.push_back(Tile{s, (int32_t)b});
-        c->hP[s].cell_tile0 = (int32_t)c->h_cell_tiles.size();
         if (sl.desc.calc_wca)
             for (int64_t q = 0; q < sl.n_cells; q += tcl) c->h_cell_tiles.push_back(Tile{s, (int32_t)q});
     }
@@ -187,7 +183,9 @@ int rebuild_tiles(gcr_ctx *c)
     return GCR_OK;
 }
 
-int validate_desc(const gcr_config &cfg, const gcr_system_desc *d, int64_t *nc_out)
+// checks a descriptor; derives the GPU cell grid (cells of side >= (r_cut +
+// skin) * cell_factor, at least 3 per side) and the skin actually used
+int validate_desc(const gcr_config &cfg, const gcr_system_desc *d, int64_t *nc_out, double *skin_out = nullptr)
 {
     if (!d) return fail(GCR_ERR_BAD_ARG, "null descriptor");
     if (d->n_beads <= 0 || d->n_beads > (int64_t)INT32_MAX / 2) return fail(GCR_ERR_BAD_ARG, "n_beads out of range");
@@ -196,25 +194,35 @@ int validate_desc(const gcr_config &cfg, const gcr_system_desc *d, int64_t *nc_o
     if (!(d->radius > 0.0)) return fail(GCR_ERR_BAD_ARG, "radius must be positive");
     if (d->spring_params[3] != 0.0) return fail(GCR_ERR_BAD_ARG, "FENE springs are not supported");
     if (d->active_params[1] > 0.0) return fail(GCR_ERR_BAD_ARG, "active sliding is not supported");
+    if (!(d->skin >= 0.0) || !std::isfinite(d->skin)) return fail(GCR_ERR_BAD_ARG, "skin must be >= 0");
     int64_t nc = 1;
+    double skin = d->skin;
     if (d->calc_wca) {
         double rc = d->wca_params[3];
         double cf = d->cell_factor >= 1.0 ? d->cell_factor : 1.0;
         if (!(rc > 0.0)) return fail(GCR_ERR_BAD_ARG, "pair cutoff must be positive");
-        nc = (int64_t)std::floor(d->L / (rc * cf));
-        if (nc < 3)
+        if (d->L < 3.0 * rc * cf)
             return fail(GCR_ERR_BAD_ARG, "box side must be at least 3 pair cutoffs for the GPU cell grid");
-        // h = L/nc must not fall below the cutoff through rounding
-        while (nc > 3 && d->L / (double)nc < rc) nc--;
+        // a box too small for the skin keeps 3 cells per side with a smaller skin
+        if ((rc + skin) * cf * 3.0 > d->L) skin = d->L / (3.0 * cf) - rc;
+        skin = skin > 0.0 ? skin : 0.0;
+        const double side = (rc + skin) * cf;
+        nc = (int64_t)std::floor(d->L / side);
+        nc = nc < 3 ? 3 : nc;
+        // h = L/nc must not fall below the list radius through rounding
+        while (nc > 3 && d->L / (double)nc < rc + skin) nc--;
+        if (d->L / (double)nc < rc + skin) skin = d->L / (double)nc - rc;
+        skin = skin > 0.0 ? skin : 0.0;
         int64_t cells = 1;
         for (int i = 0; i < cfg.dim; i++) cells *= nc;
         if (cells > (int64_t)INT32_MAX / 2) return fail(GCR_ERR_BAD_ARG, "too many GPU cells");
     }
     *nc_out = nc;
+    if (skin_out) *skin_out = skin;
     return GCR_OK;
 }
 
-void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, SysP &p)
+void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, double skin, SysP &p)
 {
     const gcr_system_desc &d = sl.desc;
     std::memset(&p, 0, sizeof(p));
@@ -224,6 +232,7 @@ void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, SysP &p)
     p.frc = sl.buf.forces;
     p.chain = sl.buf.chain_id;
     p.rest = sl.buf.rest_lengths;
+    p.chain_start = c->chain_starts + sl.chain_off;
     p.bead_off = sl.bead_off;
     p.cell_off = sl.cell_off;
     p.n = (int32_t)d.n_beads;
@@ -236,7 +245,6 @@ void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, SysP &p)
     p.half_L = d.L / 2.0;
     p.h = d.L / (double)nc;
     p.inv_h = (double)nc / d.L;
-    p.hf = (float)p.h;
     p.k = d.spring_params[0];
     p.kappa = d.spring_params[1];
     p.theta0 = d.spring_params[2];
@@ -248,6 +256,8 @@ void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, SysP &p)
     p.p1 = d.wca_params[1];
     p.shift = d.wca_params[2];
     p.rc2 = d.wca_params[3] * d.wca_params[3];
+    p.rl2 = (d.wca_params[3] + skin) * (d.wca_params[3] + skin);
+    p.half_skin2 = 0.25 * skin * skin;
     p.n_nearby = d.n_nearby;
     p.self_propel = d.self_propel ? 1 : 0;
     p.v0 = d.active_params[0];
@@ -280,38 +290,37 @@ int launch_sys(gcr_ctx *c, void *fn)
     return GCR_OK;
 }
 
-int launch_scan_tiles(gcr_ctx *c)
-{
-    int n = (int)c->slots.size();
-    void *a[] = {&c->args, &n};
-    GCR_CUDA(cudaLaunchKernel(c->ks.scan_tiles, dim3(n), dim3(256), a, 0, c->stream));
-    return GCR_OK;
-}
-
-// one stage's cell list: block scans, per-system tile scan, compact pack
-int enqueue_cells(gcr_ctx *c, int which)
+// one stage's neighbour lists (flagged systems only): bin, per-cell sort, build
+int enqueue_lists(gcr_ctx *c, int which)
 {
     int rc;
-    const int bc = c->cfg.block_cells;
-    if ((rc = launch(c, which ? c->ks.scan_local1 : c->ks.scan_local0, c->grid_scan, bc))) return rc;
-    if ((rc = launch_scan_tiles(c))) return rc;
-    return launch(c, which ? c->ks.pack1 : c->ks.pack0, c->grid_pack, bc);
+    const int bb = c->cfg.block_beads, bc = c->cfg.block_cells;
+    if ((rc = launch(c, which ? c->ks.bin1 : c->ks.bin0, c->grid_bin, bb))) return rc;
+    if ((rc = launch(c, c->ks.sort, c->grid_sort, bc))) return rc;
+    return launch(c, which ? c->ks.build1 : c->ks.build0, c->grid_build, bb);
 }
 
 int enqueue_step(gcr_ctx *c)
 {
     int rc;
     const int bb = c->cfg.block_beads;
-    if ((rc = enqueue_cells(c, 0))) return rc;
-    if ((rc = launch(c, c->ks.pair, c->grid_pair, bb))) return rc;
+    if ((rc = enqueue_lists(c, 0))) return rc;
+    if ((rc = launch(c, c->ks.pair0, c->grid_pair, bb))) return rc;
     if ((rc = launch(c, c->ks.stage0, c->grid_stage0, bb, c->stage_smem))) return rc;
-    if ((rc = enqueue_cells(c, 1))) return rc;
-    if ((rc = launch(c, c->ks.pair, c->grid_pair, bb))) return rc;
+    if ((rc = enqueue_lists(c, 1))) return rc;
+    if ((rc = launch(c, c->ks.pair1, c->grid_pair, bb))) return rc;
     if ((rc = launch(c, c->ks.stage1, c->grid_stage1, bb, c->stage_smem))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_dt))) return rc;
     if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_end))) return rc;
     return GCR_OK;
+}
+
+// start of a run: zero the cell counts, flag every system for a list build
+int enqueue_run_start(gcr_ctx *c)
+{
+    GCR_CUDA(cudaMemsetAsync(c->cnt, 0, sizeof(int) * std::max<int64_t>(c->cfg.cell_capacity, 1), c->stream));
+    return launch_sys(c, c->ks.sys_mark);
 }
 
 int build_graph(gcr_ctx *c)
@@ -356,14 +365,14 @@ int gcr_footprint(const gcr_config *cfg, const gcr_system_desc *desc, int64_t *c
     if (desc->calc_wca) {
         cells = 1;
         for (int i = 0; i < cfg->dim; i++) cells *= nc;
-        cells += 1;  // end sentinel of the compact cell list
     }
     const int64_t n = desc->n_beads, d = cfg->dim;
     const int64_t ft = cfg->precision == GCR_FP64 ? 8 : 4;
-    const int64_t recb = cfg->precision == GCR_FP64 ? 32 : 16;
+    const int64_t ld = cfg->list_depth > 0 ? cfg->list_depth : (cfg->dim == 2 ? 32 : 96);
     int64_t bytes = n * d * (8 + 8 + ft + ft) + n * 4 + desc->n_chains * 8     // caller-owned state
-                    + n * (1 + recb + 4 + 2 * d * ft) + 4 * (desc->n_chains + 1)  // topo, list, fp, xi
-                    + cells * (12 + (int64_t)cfg->cell_depth * 4);               // counts, starts, slots
+                    + n * (1 + 2 * d * ft) + 4 * (desc->n_chains + 1)          // topo, fp, xi, chain starts
+                    + n * (4 * ld + 4 + 8 * d)                                 // neighbour list, xref
+                    + cells * (8 + (int64_t)cfg->cell_depth * 4);              // counts, slots
     if (cells_out) *cells_out = cells;
     if (bytes_out) *bytes_out = bytes;
     return GCR_OK;
@@ -386,6 +395,8 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
         return fail(GCR_ERR_BAD_ARG, "steps_per_graph must be in [1, 64]");
     if (cfg.bead_capacity <= 0 || cfg.system_capacity <= 0 || cfg.cell_capacity < 0)
         return fail(GCR_ERR_BAD_ARG, "capacities must be positive");
+    if (cfg.list_depth == 0) cfg.list_depth = cfg.dim == 2 ? 32 : 96;
+    if (cfg.list_depth < 4 || cfg.list_depth > 1024) return fail(GCR_ERR_BAD_ARG, "list_depth must be in [4, 1024]");
 
     gcr_ctx *c = new (std::nothrow) gcr_ctx();
     if (!c) return fail(GCR_ERR_OOM, "host allocation");
@@ -408,7 +419,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     c->max_bead_tiles = cfg.bead_capacity / cfg.block_beads + S;
     c->max_cell_tiles = cfg.cell_capacity / cfg.block_cells + S;
     const int64_t slots_total = cfg.cell_capacity * (int64_t)cfg.cell_depth;
-    c->rec_bytes = (size_t)cfg.bead_capacity * (cfg.precision == GCR_FP64 ? 32 : 16);
+    const size_t cells_alloc = (size_t)std::max<int64_t>(cfg.cell_capacity, 1);
     cudaError_t e = cudaSuccess;
     e = e ? e : cudaMalloc(&c->dP, sizeof(SysP) * S);
     e = e ? e : cudaMalloc(&c->dS, sizeof(SysS) * S);
@@ -416,16 +427,14 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     e = e ? e : cudaMalloc(&c->d_cell_tiles, sizeof(Tile) * c->max_cell_tiles);
     e = e ? e : cudaMalloc(&c->d_ntiles, sizeof(int) * 2);
     e = e ? e : cudaMalloc(&c->topo, (size_t)cfg.bead_capacity);
-    e = e ? e : cudaMalloc(&c->cnt0, sizeof(int) * std::max<int64_t>(cfg.cell_capacity, 1));
-    e = e ? e : cudaMalloc(&c->cnt1, sizeof(int) * std::max<int64_t>(cfg.cell_capacity, 1));
+    e = e ? e : cudaMalloc(&c->cnt, sizeof(int) * cells_alloc);
+    e = e ? e : cudaMalloc(&c->ncell, sizeof(int) * cells_alloc);
     e = e ? e : cudaMalloc(&c->items, sizeof(int) * std::max<int64_t>(slots_total, 1));
-    e = e ? e : cudaMalloc(&c->rec, std::max<size_t>(c->rec_bytes, 32));
+    e = e ? e : cudaMalloc(&c->nbr, sizeof(int) * (size_t)cfg.bead_capacity * (size_t)cfg.list_depth);
+    e = e ? e : cudaMalloc(&c->ncount, sizeof(int) * (size_t)cfg.bead_capacity);
+    e = e ? e : cudaMalloc(&c->xref, sizeof(double) * (size_t)cfg.bead_capacity * cfg.dim);
     e = e ? e : cudaMalloc(&c->xi, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
     e = e ? e : cudaMalloc(&c->fp, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
-    e = e ? e : cudaMalloc(&c->cstart, sizeof(int) * std::max<int64_t>(cfg.cell_capacity, 1));
-    e = e ? e : cudaMalloc(&c->rcell, sizeof(int) * cfg.bead_capacity);
-    e = e ? e : cudaMalloc(&c->tsum, sizeof(int) * c->max_cell_tiles);
-    e = e ? e : cudaMalloc(&c->toff, sizeof(int) * c->max_cell_tiles);
     e = e ? e : cudaMalloc(&c->chain_starts, sizeof(int32_t) * (cfg.bead_capacity + S));
     e = e ? e : cudaMalloc(&c->d_err, sizeof(int));
     e = e ? e : cudaMalloc(&c->d_out, sizeof(double) * 8);
@@ -434,8 +443,9 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
                             std::string("device allocation: ") + cudaGetErrorString(e)));
     cudaMemsetAsync(c->dS, 0, sizeof(SysS) * S, c->stream);
     cudaMemsetAsync(c->d_ntiles, 0, sizeof(int) * 2, c->stream);
-    cudaMemsetAsync(c->cnt0, 0, sizeof(int) * std::max<int64_t>(cfg.cell_capacity, 1), c->stream);
-    cudaMemsetAsync(c->cnt1, 0, sizeof(int) * std::max<int64_t>(cfg.cell_capacity, 1), c->stream);
+    cudaMemsetAsync(c->cnt, 0, sizeof(int) * cells_alloc, c->stream);
+    cudaMemsetAsync(c->ncell, 0, sizeof(int) * cells_alloc, c->stream);
+    cudaMemsetAsync(c->ncount, 0, sizeof(int) * (size_t)cfg.bead_capacity, c->stream);
     c->slots.assign(S, Slot());
     c->hP.assign(S, SysP());
     c->hS.assign(S, SysS());
@@ -450,16 +460,16 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     a.cell_tiles = c->d_cell_tiles;
     a.n_cell_tiles = c->d_ntiles + 1;
     a.topo = c->topo;
-    a.cnt0 = c->cnt0;
-    a.cnt1 = c->cnt1;
+    a.cnt = c->cnt;
+    a.ncell = c->ncell;
     a.items = c->items;
-    a.rec = c->rec;
+    a.nbr = c->nbr;
+    a.ncount = c->ncount;
+    a.xref = c->xref;
     a.xi = c->xi;
     a.fp = c->fp;
-    a.cstart = c->cstart;
-    a.rcell = c->rcell;
-    a.tsum = c->tsum;
-    a.toff = c->toff;
+    a.list_stride = cfg.bead_capacity;
+    a.list_depth = cfg.list_depth;
     a.depth = cfg.cell_depth;
     a.log_depth = ilog2(cfg.cell_depth);
     a.tile_beads = cfg.block_beads;
@@ -471,12 +481,11 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     }
     c->grid_stage0 = kernel_grid(c, c->ks.stage0, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
     c->grid_stage1 = kernel_grid(c, c->ks.stage1, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
-    c->grid_beads = std::min(c->grid_stage0, c->grid_stage1);
     c->grid_update = kernel_grid(c, c->ks.update, cfg.block_beads, c->max_bead_tiles);
-    c->grid_pack = kernel_grid(c, c->ks.pack0, cfg.block_cells, c->max_cell_tiles);
-    c->grid_scan = kernel_grid(c, c->ks.scan_local0, cfg.block_cells, c->max_cell_tiles);
-    c->grid_pair = kernel_grid(c, c->ks.pair, cfg.block_beads, c->max_bead_tiles);
-    c->grid_cells = c->grid_pack;
+    c->grid_pair = kernel_grid(c, c->ks.pair0, cfg.block_beads, c->max_bead_tiles);
+    c->grid_bin = kernel_grid(c, c->ks.bin0, cfg.block_beads, c->max_bead_tiles);
+    c->grid_sort = kernel_grid(c, c->ks.sort, cfg.block_cells, c->max_cell_tiles);
+    c->grid_build = kernel_grid(c, c->ks.build0, cfg.block_beads, c->max_bead_tiles);
     c->grid_sys = (int)((S + 127) / 128);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return cleanup(fail(GCR_ERR_CUDA, "initialisation"));
     *out = c;
@@ -488,9 +497,8 @@ int gcr_destroy(gcr_ctx *c)
     if (!c) return GCR_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
-    void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->topo, c->cnt0, c->cnt1,
-                    c->items, c->rec, c->xi, c->fp, c->cstart, c->rcell, c->tsum, c->toff, c->chain_starts,
-                    c->d_err, c->d_out};
+    void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->topo, c->cnt, c->ncell,
+                    c->items, c->nbr, c->ncount, c->xref, c->xi, c->fp, c->chain_starts, c->d_err, c->d_out};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -504,7 +512,8 @@ int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers 
     if (!buf->pos || !buf->pos1 || !buf->tangent || !buf->forces || !buf->chain_id || !buf->rest_lengths)
         return fail(GCR_ERR_BAD_ARG, "all state buffers must be bound");
     int64_t nc = 1;
-    int rc = validate_desc(c->cfg, desc, &nc);
+    double skin = 0.0;
+    int rc = validate_desc(c->cfg, desc, &nc, &skin);
     if (rc) return rc;
     int slot = -1;
     for (int s = 0; s < (int)c->slots.size(); s++)
@@ -520,7 +529,7 @@ int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers 
     }
     int64_t boff = c->beads.alloc(desc->n_beads);
     if (boff < 0) return fail(GCR_ERR_CAPACITY, "bead capacity exhausted");
-    int64_t coff = n_cells ? c->cells.alloc(n_cells + 1) : 0;
+    int64_t coff = n_cells ? c->cells.alloc(n_cells) : 0;
     if (coff < 0) {
         c->beads.release(boff, desc->n_beads);
         return fail(GCR_ERR_CAPACITY, "cell capacity exhausted");
@@ -528,7 +537,7 @@ int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers 
     int64_t choff = c->chains.alloc(desc->n_chains + 1);
     if (choff < 0) {
         c->beads.release(boff, desc->n_beads);
-        if (n_cells) c->cells.release(coff, n_cells + 1);
+        if (n_cells) c->cells.release(coff, n_cells);
         return fail(GCR_ERR_CAPACITY, "chain capacity exhausted");
     }
     Slot &sl = c->slots[slot];
@@ -539,7 +548,7 @@ int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers 
     sl.cell_off = coff;
     sl.chain_off = choff;
     sl.n_cells = n_cells;
-    fill_sysp(c, sl, nc, c->hP[slot]);
+    fill_sysp(c, sl, nc, skin, c->hP[slot]);
     SysS &s = c->hS[slot];
     std::memset(&s, 0, sizeof(s));
     s.dt = desc->dtmax;
@@ -561,7 +570,7 @@ int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers 
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     if (err) {
         c->beads.release(boff, desc->n_beads);
-        if (n_cells) c->cells.release(coff, n_cells + 1);
+        if (n_cells) c->cells.release(coff, n_cells);
         c->chains.release(choff, desc->n_chains + 1);
         sl = Slot();
         return fail(GCR_ERR_BAD_ARG, "chain ids must be non-decreasing and in [0, n_chains)");
@@ -579,7 +588,7 @@ int gcr_evict(gcr_ctx *c, int32_t slot)
     // make sure no queued work still uses the slot's scratch
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     c->beads.release(sl.bead_off, sl.desc.n_beads);
-    if (sl.n_cells) c->cells.release(sl.cell_off, sl.n_cells + 1);
+    if (sl.n_cells) c->cells.release(sl.cell_off, sl.n_cells);
     c->chains.release(sl.chain_off, sl.desc.n_chains + 1);
     sl = Slot();
     SysS &s = c->hS[slot];
@@ -595,7 +604,8 @@ int gcr_update_desc(gcr_ctx *c, int32_t slot, const gcr_system_desc *desc)
     if (desc->n_beads != sl.desc.n_beads || desc->n_chains != sl.desc.n_chains)
         return fail(GCR_ERR_BAD_ARG, "bead and chain counts of a resident system cannot change");
     int64_t nc = 1;
-    int rc = validate_desc(c->cfg, desc, &nc);
+    double skin = 0.0;
+    int rc = validate_desc(c->cfg, desc, &nc, &skin);
     if (rc) return rc;
     int64_t n_cells = 0;
     if (desc->calc_wca) {
@@ -604,10 +614,7 @@ int gcr_update_desc(gcr_ctx *c, int32_t slot, const gcr_system_desc *desc)
     }
     if (n_cells != sl.n_cells) return fail(GCR_ERR_BAD_ARG, "the GPU cell grid of a resident system cannot change");
     sl.desc = *desc;
-    // the tile placement of a resident system does not change with its parameters
-    const int32_t tile0 = c->hP[slot].cell_tile0;
-    fill_sysp(c, sl, nc, c->hP[slot]);
-    c->hP[slot].cell_tile0 = tile0;
+    fill_sysp(c, sl, nc, skin, c->hP[slot]);
     GCR_CUDA(cudaMemcpyAsync(c->dP + slot, &c->hP[slot], sizeof(SysP), cudaMemcpyHostToDevice, c->stream));
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     return GCR_OK;
@@ -684,10 +691,7 @@ int gcr_run(gcr_ctx *c, int64_t max_steps, int32_t sync_every)
     }
     int rc = build_graph(c);
     if (rc) return rc;
-    const size_t cb = sizeof(int) * std::max<int64_t>(c->cfg.cell_capacity, 1);
-    GCR_CUDA(cudaMemsetAsync(c->cnt0, 0, cb, c->stream));
-    GCR_CUDA(cudaMemsetAsync(c->cnt1, 0, cb, c->stream));
-    rc = launch(c, c->ks.insert, c->grid_update, c->cfg.block_beads);
+    rc = enqueue_run_start(c);
     if (rc) return rc;
     const int64_t spg = c->cfg.steps_per_graph;
     const int64_t graphs = (max_steps + spg - 1) / spg;
@@ -711,12 +715,9 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
         int rc = rebuild_tiles(c);
         if (rc) return rc;
     }
-    const size_t cb = sizeof(int) * std::max<int64_t>(c->cfg.cell_capacity, 1);
-    GCR_CUDA(cudaMemsetAsync(c->cnt0, 0, cb, c->stream));
-    GCR_CUDA(cudaMemsetAsync(c->cnt1, 0, cb, c->stream));
-    int rc = launch(c, c->ks.insert, c->grid_update, c->cfg.block_beads);
+    int rc = enqueue_run_start(c);
     if (rc) return rc;
-    // groups: cells(pos), pair(pos), stage 0, cells(pos1), pair(pos1),
+    // groups: lists(pos), pair(pos), stage 0, lists(pos1), pair(pos1),
     // stage 1 + dt rule, update + bookkeeping
     const int G = 7;
     std::vector<cudaEvent_t> ev((size_t)n_steps * (G + 1), nullptr);
@@ -725,15 +726,15 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
     for (int s = 0; s < n_steps && rc == GCR_OK; s++) {
         cudaEvent_t *e = ev.data() + (size_t)s * (G + 1);
         GCR_CUDA(cudaEventRecord(e[0], c->stream));
-        rc = enqueue_cells(c, 0);
+        rc = enqueue_lists(c, 0);
         GCR_CUDA(cudaEventRecord(e[1], c->stream));
-        if (!rc) rc = launch(c, c->ks.pair, c->grid_pair, bb);
+        if (!rc) rc = launch(c, c->ks.pair0, c->grid_pair, bb);
         GCR_CUDA(cudaEventRecord(e[2], c->stream));
         if (!rc) rc = launch(c, c->ks.stage0, c->grid_stage0, bb, c->stage_smem);
         GCR_CUDA(cudaEventRecord(e[3], c->stream));
-        if (!rc) rc = enqueue_cells(c, 1);
+        if (!rc) rc = enqueue_lists(c, 1);
         GCR_CUDA(cudaEventRecord(e[4], c->stream));
-        if (!rc) rc = launch(c, c->ks.pair, c->grid_pair, bb);
+        if (!rc) rc = launch(c, c->ks.pair1, c->grid_pair, bb);
         GCR_CUDA(cudaEventRecord(e[5], c->stream));
         if (!rc) rc = launch(c, c->ks.stage1, c->grid_stage1, bb, c->stage_smem);
         if (!rc) rc = launch_sys(c, c->ks.sys_dt);
@@ -787,6 +788,7 @@ int gcr_get_status(gcr_ctx *c, int32_t slot, gcr_status *out)
     out->step = s.step;
     out->flags = s.flags;
     out->active = s.active;
+    out->list_builds = s.list_builds;
     return GCR_OK;
 }
 
@@ -838,6 +840,29 @@ int gcr_cell_assignment(gcr_ctx *c, int32_t slot, int32_t *cell_of_bead, int32_t
     GCR_CUDA(launch_cell_assignment(c->cfg.dim, c->hP[slot], cell_of_bead, c->stream));
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     if (n_cells_side) *n_cells_side = c->hP[slot].nc;
+    return GCR_OK;
+}
+
+int gcr_neighbour_list(gcr_ctx *c, int32_t slot, int32_t *counts, int32_t *partners, int32_t partners_depth,
+                       double *build_pos, int64_t *entries)
+{
+    if (!valid_slot(c, slot)) return fail(GCR_ERR_BAD_ARG, "invalid slot");
+    if (partners && partners_depth < c->cfg.list_depth)
+        return fail(GCR_ERR_BAD_ARG, "partners_depth is smaller than the context's list_depth");
+    const Slot &sl = c->slots[slot];
+    unsigned long long *total = reinterpret_cast<unsigned long long *>(c->d_out);
+    GCR_CUDA(cudaMemsetAsync(total, 0, sizeof(unsigned long long), c->stream));
+    GCR_CUDA(launch_export_list(c->nbr + sl.bead_off, c->ncount + sl.bead_off, c->cfg.bead_capacity,
+                                c->cfg.list_depth, (int)sl.desc.n_beads, counts, partners, partners_depth, total,
+                                c->stream));
+    if (build_pos)
+        GCR_CUDA(cudaMemcpyAsync(build_pos, c->xref + (size_t)sl.bead_off * c->cfg.dim,
+                                 sizeof(double) * (size_t)sl.desc.n_beads * c->cfg.dim, cudaMemcpyDeviceToDevice,
+                                 c->stream));
+    unsigned long long h = 0;
+    GCR_CUDA(cudaMemcpyAsync(&h, total, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    if (entries) *entries = (int64_t)h;
     return GCR_OK;
 }
 

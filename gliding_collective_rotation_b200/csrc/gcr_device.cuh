@@ -4,18 +4,21 @@
 //   * per system, caller-owned: pos/pos1 FP64 [n,d] (AoS), tangent/forces FT
 //     [n,d], chain_id int32 [n], rest_lengths FP64 [n_chains];
 //   * library scratch, per system at a bead / cell offset:
-//       topo      uint8 [bead]       chain-neighbour bits of each bead
-//       cnt[2]    int32 [cell]       beads binned per GPU cell (ping-pong)
-//       items     int32 [cell*depth] bead ids per cell slot (unsorted staging)
-//       cstart    int32 [cell+1]     start of each cell in the compact list
-//       rec       float4|double4 [bead] compact cell list: packed positions
-//                 in cell order, sorted by bead id inside a cell
-//       rcell     int32 [bead]       cell of each record
-//       fp, xi    FT [bead][d]       pair force and step noise per bead
+//       topo      uint8 [bead]        chain-neighbour bits of each bead
+//       cnt       int32 [cell]        beads binned per GPU cell (zeroed by the sort)
+//       ncell     int32 [cell]        beads of each cell at the last list build
+//       items     int32 [cell*depth]  bead ids per cell, sorted by id
+//       nbr       int32 [slot][bead]  neighbour list, slot-major (coalesced
+//                                     across the beads of a warp)
+//       ncount    int32 [bead]        neighbours of each bead
+//       xref      FP64 [bead][d]      positions at the last list build
+//       fp, xi    FT [bead][d]        pair force and step noise per bead
 //   * SysP (read-only during a step) and SysS (device-updated) per slot.
 // Binning writes a fixed-depth table (a count and `depth` slots per cell, the
-// shape of the reference's grid_list, updates.py:502-522); a per-system
-// counting sort turns it into the compact cell list the pair kernel reads.
+// shape of the reference's grid_list, updates.py:502-522); a per-cell sort
+// makes the slot order deterministic; the list build walks the 3^d cells
+// around each bead (the reference's update_nbor_list, updates.py:586-669,
+// with a skin added to the cutoff).
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -31,9 +34,10 @@ constexpr uint8_t kHasPrev = 1, kHasPrev2 = 2, kHasNext = 4, kHasNext2 = 8;
 constexpr int kFlagCellOverflow = 1;
 constexpr int kFlagNonFinite = 2;
 constexpr int kFlagNextOverflow = 4;
-constexpr int kFlagListCorrupt = 8;  // an inconsistent cell list was detected and not used
+constexpr int kFlagListCorrupt = 8;  // an inconsistent cell or neighbour list was detected and not used
+constexpr int kFlagListOverflow = 16;  // more list partners of a bead than the list depth
 // a system with one of these stops: every kernel skips it until re-armed
-constexpr int kFlagFatal = kFlagCellOverflow | kFlagNonFinite | kFlagListCorrupt;
+constexpr int kFlagFatal = kFlagCellOverflow | kFlagNonFinite | kFlagListCorrupt | kFlagListOverflow;
 
 struct SysP {
     // caller-owned state
@@ -43,6 +47,7 @@ struct SysP {
     void *frc;
     const int32_t *chain;
     const double *rest;
+    const int32_t *chain_start;  // first bead of each chain (+ end), library scratch
     // scratch placement
     int64_t bead_off;  // into topo
     int64_t cell_off;  // into cnt / items / rec
@@ -52,15 +57,14 @@ struct SysP {
     int32_t n_cells;   // nc^d
     int32_t n_bead_tiles;
     int32_t n_cell_tiles;
-    int32_t cell_tile0;  // index of the system's first cell tile
-    int32_t pad1;
     double L, half_L, h, inv_h;
-    float hf;          // h rounded to FP32 (mixed records)
     // bonded
     double k, kappa, theta0;
     int32_t calc_springs, get_orient, calc_bend, calc_wca;
     // pair (WCA / LJ: coeff = ds^-4 (p0 - p1 ds^-3))
     double p0, p1, shift, rc2;
+    double rl2;         // (r_cut + skin)^2: radius of the neighbour list
+    double half_skin2;  // (skin / 2)^2: a bead that moved farther forces a rebuild
     int32_t n_nearby;
     int32_t self_propel;
     int32_t rotate_prop;  // 2D and v_tan_angle != 0
@@ -87,7 +91,9 @@ struct SysS {
     int64_t noise_steps;
     int32_t active;
     int32_t flags;
-    uint32_t pad[2];
+    int32_t rebuild;      // the neighbour list must be rebuilt before the next pair kernel
+    int32_t pad0;
+    int64_t list_builds;  // neighbour-list builds since admission
 };
 
 struct Tile {

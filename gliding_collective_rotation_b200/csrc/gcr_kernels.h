@@ -17,16 +17,16 @@ struct BatchArgs {
     const Tile *cell_tiles;
     const int *n_cell_tiles;
     const uint8_t *topo;
-    int *cnt0;
-    int *cnt1;
-    int *items;
-    void *rec;
+    int *cnt;      // beads binned per cell (the sort reads and zeroes it)
+    int *ncell;    // beads per cell at the last list build
+    int *items;    // bead ids per cell, `depth` slots per cell
+    int *nbr;      // neighbour list: slot k of bead g at nbr[k * list_stride + g]
+    int *ncount;   // neighbours per bead
+    double *xref;  // positions at the last list build, FP64 [bead][dim]
     void *xi;      // translational noise of the current step per bead, FT [bead][dim]
     void *fp;      // pair force per bead (bead order), FT [bead][dim]
-    int *cstart;   // start of each cell in the compact list (+ end sentinel per system)
-    int *rcell;    // cell of each compact-list record
-    int *tsum;     // cell count of each cell tile
-    int *toff;     // start of each cell tile within its system
+    int64_t list_stride;
+    int list_depth;
     int depth;
     int log_depth;
     int tile_beads;
@@ -34,19 +34,20 @@ struct BatchArgs {
 };
 
 struct KernelSet {
-    void *insert;
-    void *pack0;
-    void *pack1;
+    void *bin0;     // cell binning of pos / pos1 for a list build
+    void *bin1;
+    void *sort;     // per-cell sort of the binned ids (zeroes the counts)
+    void *build0;   // neighbour lists from pos / pos1
+    void *build1;
+    void *pair0;    // pair forces at pos / pos1
+    void *pair1;
     void *stage0;
     void *stage1;
     void *update;
     void *topo;
     void *sys_dt;
     void *sys_end;
-    void *pair;
-    void *scan_local0;
-    void *scan_local1;
-    void *scan_tiles;
+    void *sys_mark;  // flag every resident system for a list build
     size_t (*stage_smem)(int block_beads);  // dynamic shared memory of the stage kernels
 };
 
@@ -64,6 +65,9 @@ cudaError_t launch_order_params(int dim, int precision, const SysP &p, const int
 cudaError_t launch_chain_starts(const int32_t *chain, int n, int n_chains, int32_t *chain_start, int *d_err,
                                 cudaStream_t st);
 cudaError_t launch_cell_assignment(int dim, const SysP &p, int32_t *cell_of_bead, cudaStream_t st);
+cudaError_t launch_export_list(const int *nbr, const int *ncount, int64_t stride, int list_depth, int n,
+                               int32_t *counts, int32_t *partners, int partners_depth, unsigned long long *total,
+                               cudaStream_t st);
 cudaError_t launch_philox_noise(int dim, uint64_t seed, int64_t step, int64_t n, int do_trans,
                                 int do_rot, double *out, cudaStream_t st);
 

@@ -343,4 +343,28 @@ cudaError_t launch_philox_noise(int dim, uint64_t seed, int64_t step, int64_t n,
     return cudaGetLastError();
 }
 
+// the neighbour list of one system, slot-major -> bead-major, and its total
+__global__ void k_export_list(const int *__restrict__ nbr, const int *__restrict__ ncount, int64_t stride,
+                              int list_depth, int n, int32_t *counts, int32_t *partners, int partners_depth,
+                              unsigned long long *total)
+{
+    int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= n) return;
+    int c = ncount[b];
+    c = c < 0 ? 0 : (c > list_depth ? list_depth : c);
+    if (counts) counts[b] = c;
+    if (partners)
+        for (int k = 0; k < c; k++) partners[(size_t)b * partners_depth + k] = nbr[(size_t)k * stride + b];
+    atomicAdd(total, (unsigned long long)c);
+}
+
+cudaError_t launch_export_list(const int *nbr, const int *ncount, int64_t stride, int list_depth, int n,
+                               int32_t *counts, int32_t *partners, int partners_depth, unsigned long long *total,
+                               cudaStream_t st)
+{
+    k_export_list<<<(n + 255) / 256, 256, 0, st>>>(nbr, ncount, stride, list_depth, n, counts, partners,
+                                                   partners_depth, total);
+    return cudaGetLastError();
+}
+
 }  // namespace gcr

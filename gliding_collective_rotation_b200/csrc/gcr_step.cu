@@ -1,48 +1,41 @@
 // gcr_step.cu -- the SRK2 step kernels (sm_100a).
 //
-// One step of every resident system is five persistent, grid-stride launches
-// over per-system tile tables:
+// One step of every resident system is a fixed sequence of persistent,
+// grid-stride launches over per-system tile tables (one captured graph
+// serves any mix of systems):
 //
-//   pack<A>    per GPU cell: sort the slot contents by bead id, write packed
-//              records of pos, clear the B counters
-//   stage<0>   per bead: pair forces over the 3^d neighbour cells + bond,
-//              bend and tangent + self-propulsion + predictor update
-//              pos1 = (pos + dt/r F0 + sqrt(2 D dt) xi) mod L; bins pos1 into B
-//   pack<B>    as pack<A> for pos1, clears the A counters
-//   stage<1>   per bead: the same forces at pos1 accumulated onto F0; block
-//              max of |F0+F1|^2; the last tile of each system picks dt
-//              (SRK.py:323-353)
-//   update     per bead: corrector pos = (pos + dt_used/(2r) (F0+F1)
-//              + sqrt(2 D dt_used) xi) mod L, rotational diffusion
-//              (SRK.py:398-423), bins pos into A; the last tile advances the
-//              system's step bookkeeping
+//   bin<A>, sort, build<A>   neighbour lists from pos, for the systems whose
+//                            rebuild flag is set (the others skip at once)
+//   pair<A>                  per bead: pair forces over its neighbour list
+//   stage<0>                 per bead: bond, bend and tangent + pair force +
+//                            self-propulsion + predictor update
+//                            pos1 = (pos + dt/r F0 + sqrt(2 D dt) xi) mod L;
+//                            flags a rebuild if a bead left its skin
+//   bin<B>, sort, build<B>   as above, from pos1
+//   pair<B>, stage<1>        the same forces at pos1 accumulated onto F0;
+//                            block max of |F0+F1|^2
+//   sys_dt                   per system: dt rule (SRK.py:323-353)
+//   update                   per bead: corrector pos = (pos + dt_used/(2r)
+//                            (F0+F1) + sqrt(2 D dt_used) xi) mod L, rotational
+//                            diffusion (SRK.py:398-423); flags a rebuild if a
+//                            bead left its skin
+//   sys_end                  per system: step bookkeeping
 //
 // The same xi is used by predictor and corrector (SRK.py:134-142, 385): it is
-// drawn twice from the counter-based Philox stream keyed by (seed, bead,
-// global step, stream), or read from an injected noise_vec snapshot.
+// drawn once from the counter-based Philox stream keyed by (seed, bead,
+// global step, stream), or read from an injected noise_vec snapshot, and kept
+// for the corrector.
 //
 // Reference functions restated per bead: forces.calc_chain_spring_forces
 // (forces.py:285-403), forces.central_pair_force with forces.WCA
 // (forces.py:57-145, 13-15), forces.self_propel (forces.py:206-224), the
-// SRK2 stage updates (SRK.py:166-184, 355-396).
+// SRK2 stage updates (SRK.py:166-184, 355-396), the cell and neighbour lists
+// (updates.update_grid_list_mini, updates.update_nbor_list,
+// updates.py:502-522, 586-669).
 #include "gcr_device.cuh"
 #include "gcr_kernels.h"
 
 namespace gcr {
-
-template <typename FT>
-struct Rec;
-template <>
-struct Rec<float> {
-    using type = float4;
-};
-struct alignas(32) Dbl4 {
-    double x, y, z, w;
-};
-template <>
-struct Rec<double> {
-    using type = Dbl4;
-};
 
 // ------------------------------------------------------------------------
 // bonded forces (forces.py:285-403).  A tile of TB beads stages the
@@ -105,8 +98,7 @@ __device__ __forceinline__ bool bend(const FT *ti, const FT *tj, FT theta0, FT k
 }
 
 // ------------------------------------------------------------------------
-// pair forces (forces.py:57-145, rule forces.WCA) over the 3^d GPU cells
-// around the bead; records are packed per cell, sorted by bead id
+// the pair rule forces.WCA (forces.py:13-15): coeff = ds^-4 (p0 - p1 ds^-3)
 // ------------------------------------------------------------------------
 template <typename FT>
 __device__ __forceinline__ FT wca_coeff(FT ds, FT p0, FT p1)
@@ -131,159 +123,272 @@ __device__ __forceinline__ FT wca_coeff(FT ds, FT p0, FT p1)
     }
 }
 
-// One bead's pair force, the bead taken in cell order: record k of the
-// system's compact cell list.  All lanes of a warp sit in the same or
-// neighbouring cells, so they walk the same candidate records (uniform trip
-// counts, broadcast loads).  Candidates of cell c are records
-// [cstart[c], cstart[c+1]), sorted by bead id.
-// Pair force of the bead at record k of its system's compact cell list
-// (forces.py:57-145).  Threads of a warp hold beads of the same or of
-// neighbouring cells, so they walk the same candidate records (broadcast
-// loads, similar trip counts).  The three cells cx-1, cx, cx+1 of one row are
-// one contiguous range of records; a row that wraps around the box is two
-// ranges.  Candidates of cell c are records [cstart[c], cstart[c+1]), sorted
-// by bead id, so the sum is taken in a fixed order.
-template <int D, typename FT>
-__device__ __forceinline__ void pair_force_sorted(const SysP &p, const BatchArgs &A, int k, int &b_out, FT *F)
+// ------------------------------------------------------------------------
+// Verlet neighbour lists.  A system's list holds, per bead, every other bead
+// within r_l = r_cut + skin that the pair rule does not exclude (same chain
+// and |b1 - b2| <= n_nearby, forces.py:57-145), found through a cell grid of
+// side >= r_l.  It is rebuilt only when some bead has moved more than skin/2
+// since the last build, so no pair can come within r_cut without being on
+// the list: the producers of positions (stage 0 for pos1, the update for
+// pos) test every bead against the positions of the last build and raise the
+// system's rebuild flag; the bin, sort and build kernels run for flagged
+// systems and skip the others; the pair kernel clears the flag.  Each list
+// is in cell order (z, y, x of the 3^d cells, bead ids ascending inside a
+// cell), so its sums are taken in a fixed order whatever the batch holds.
+// ------------------------------------------------------------------------
+
+// the system takes part in a list build now
+__device__ __forceinline__ bool builds(const SysP &p, const SysS &s)
 {
-    using R = typename Rec<FT>::type;
-    const int nc = p.nc;
-    const int n = p.n;
-    const R *__restrict__ rec = reinterpret_cast<const R *>(A.rec) + p.bead_off;
-    const int *__restrict__ cs = A.cstart + p.cell_off;
-    int c = __ldg(A.rcell + p.bead_off + k);
-    c = (c < 0 || c >= p.n_cells) ? 0 : c;
-    const int cx = c % nc;
-    const int cy0 = (c / nc) % nc;
-    const int cz0 = (D == 3) ? c / (nc * nc) : 0;
-    FT own[3] = {FT(0), FT(0), FT(0)};
-    double xb[3] = {0.0, 0.0, 0.0};
-    int b, my_chain = 0;
-    if constexpr (sizeof(FT) == 4) {
-        float4 r = __ldg(rec + k);
-        own[0] = r.x;
-        own[1] = r.y;
-        own[2] = r.z;
-        b = __float_as_int(r.w);
-        if (D == 2) my_chain = __float_as_int(r.z);
-    } else {
-        const double2 *q = reinterpret_cast<const double2 *>(rec + k);
-        double2 r0 = __ldg(q), r1 = __ldg(q + 1);
-        xb[0] = r0.x;
-        xb[1] = r0.y;
-        xb[2] = r1.x;
-        b = (int)r1.y;
-        if (D == 2) my_chain = (int)r1.x;
+    return p.calc_wca && ld_volatile(&s.active) && s.rebuild && !(ld_volatile(&s.flags) & kFlagFatal);
+}
+
+template <int D>
+__device__ __forceinline__ void cell_of(const SysP &p, const double *x, int *ci)
+{
+    ci[0] = ci[1] = ci[2] = 0;
+#pragma unroll
+    for (int i = 0; i < D; i++) ci[i] = cell_coord(x[i], p.inv_h, p.nc);
+}
+
+// a bead moved farther than skin/2 from where the list was built
+template <int D>
+__device__ __forceinline__ bool left_skin(const SysP &p, const BatchArgs &A, int b, const double *x)
+{
+    const double *r = A.xref + (size_t)(p.bead_off + b) * D;
+    double dd = 0.0;
+#pragma unroll
+    for (int i = 0; i < D; i++) {
+        double d = inbounds(x[i], r[i], p.half_L, p.L);
+        dd += d * d;
     }
-    b_out = b;
-    if ((unsigned)b >= (unsigned)n) return;  // inconsistent list: the caller flags it
-    if (D == 3) my_chain = __ldg(p.chain + b);
-    const FT rc2 = (FT)p.rc2, p0 = (FT)p.p0, p1 = (FT)p.p1, shift = (FT)p.shift;
-    const FT hf = (FT)p.hf;
-    const double L = p.L, half_L = p.half_L;
-    const int nn = p.n_nearby;
-    const int span = 3 * A.depth;
-    // the row's ranges: [lo, hi) with the x offset -1/0/+1 cells changing at m1, m2
-    const bool wrap_lo = cx == 0, wrap_hi = cx == nc - 1;
-    const int x_first = wrap_lo ? 0 : cx - 1;          // first cell of the contiguous part
-    const int x_last = wrap_hi ? nc - 1 : cx + 1;      // last cell of the contiguous part
-    const int d_first = wrap_lo ? 0 : -1;              // its x offset in cells
-    const int x_extra = wrap_lo ? nc - 1 : 0;          // the wrapped cell, if any
-    const int d_extra = wrap_lo ? -1 : 1;
-    const int n_seg = (wrap_lo || wrap_hi) ? 2 : 1;
-    const int zlo = (D == 3) ? -1 : 0, zhi = (D == 3) ? 1 : 0;
-    for (int dz = zlo; dz <= zhi; dz++) {
-        int cz = 0;
-        if (D == 3) {
-            cz = cz0 + dz;
-            cz = cz < 0 ? cz + nc : (cz >= nc ? cz - nc : cz);
-        }
+    return !(dd <= p.half_skin2);
+}
+
+// bin every bead of a flagged system into its cell (fixed-depth slots)
+template <int D, int WHICH>
+__global__ void __launch_bounds__(512) k_bin(BatchArgs A)
+{
+    const int nt = *A.n_bead_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.bead_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        SysS &s = A.S[tl.sys];
+        if (!builds(p, s)) continue;
+        const int b = tl.begin + threadIdx.x;
+        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
+        const double *X = WHICH == 0 ? p.pos : p.pos1;
+        double x[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-        for (int dy = -1; dy <= 1; dy++) {
-            int cy = cy0 + dy;
-            cy = cy < 0 ? cy + nc : (cy >= nc ? cy - nc : cy);
-            const int row = (cz * nc + cy) * nc;
-            for (int seg = 0; seg < n_seg; seg++) {
-                int lo, hi, m1, m2, d0;
-                if (seg == 0) {
-                    lo = __ldg(cs + row + x_first);
-                    m1 = __ldg(cs + row + x_first + 1);
-                    m2 = __ldg(cs + row + x_first + 2);
-                    hi = __ldg(cs + row + x_last + 1);
-                    d0 = d_first;
-                } else {
-                    lo = __ldg(cs + row + x_extra);
-                    hi = __ldg(cs + row + x_extra + 1);
-                    m1 = m2 = 0x7fffffff;
-                    d0 = d_extra;
+        for (int i = 0; i < D; i++) x[i] = X[(size_t)b * D + i];
+        int ci[3];
+        cell_of<D>(p, x, ci);
+        const int64_t gc = p.cell_off + ((int64_t)ci[2] * p.nc + ci[1]) * p.nc + ci[0];
+        const int slot = atomicAdd(A.cnt + gc, 1);
+        if (slot < A.depth)
+            A.items[(gc << A.log_depth) + slot] = b;
+        else
+            atomicOr(&s.flags, kFlagCellOverflow);
+    }
+}
+
+// per cell of a flagged system: take the count (and zero it for the next
+// binning), sort the slot contents by bead id
+__global__ void __launch_bounds__(512) k_sort(BatchArgs A)
+{
+    const int nt = *A.n_cell_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.cell_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        SysS &s = A.S[tl.sys];
+        if (!builds(p, s)) continue;
+        const int c = tl.begin + threadIdx.x;
+        if (c >= p.n_cells || threadIdx.x >= A.tile_cells) continue;
+        const int64_t gc = p.cell_off + c;
+        int n = A.cnt[gc];
+        A.cnt[gc] = 0;
+        n = n < 0 ? 0 : (n < A.depth ? n : A.depth);
+        A.ncell[gc] = n;
+        if (n < 2) continue;
+        int *it = A.items + (gc << A.log_depth);
+        if (n <= 8) {
+            int v[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) v[j] = j < n ? it[j] : 0x7fffffff;
+            // Batcher odd-even merge sort network for 8 keys (19 comparators)
+#define GCR_CX(a, b)                 \
+    {                                \
+        int lo = min(v[a], v[b]);    \
+        int hi = max(v[a], v[b]);    \
+        v[a] = lo;                   \
+        v[b] = hi;                   \
+    }
+            GCR_CX(0, 1) GCR_CX(2, 3) GCR_CX(4, 5) GCR_CX(6, 7)
+            GCR_CX(0, 2) GCR_CX(1, 3) GCR_CX(4, 6) GCR_CX(5, 7)
+            GCR_CX(1, 2) GCR_CX(5, 6)
+            GCR_CX(0, 4) GCR_CX(1, 5) GCR_CX(2, 6) GCR_CX(3, 7)
+            GCR_CX(2, 4) GCR_CX(3, 5)
+            GCR_CX(1, 2) GCR_CX(3, 4) GCR_CX(5, 6)
+#undef GCR_CX
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+                if (j < n) it[j] = v[j];
+        } else {
+            // insertion sort in place (cells this dense are rare)
+            for (int j = 1; j < n; j++) {
+                int key = it[j];
+                int q = j - 1;
+                while (q >= 0 && it[q] > key) {
+                    it[q + 1] = it[q];
+                    q--;
                 }
-                // clamps keep every record index inside [0, n), whatever the list holds
-                lo = lo < 0 ? 0 : (lo > n ? n : lo);
-                hi = hi < lo ? lo : (hi > n ? n : hi);
-                hi = hi - lo > span ? lo + span : hi;
-                const FT o0 = (FT)d0 * hf, o1 = (FT)(d0 + 1) * hf, o2 = (FT)(d0 + 2) * hf;
-                const FT oy = (FT)dy * hf, oz = (FT)dz * hf;
-                for (int j = lo; j < hi; j++) {
-                    int bj, cj = 0;
-                    FT sep[3];
-                    if constexpr (sizeof(FT) == 4) {
-                        float4 r = __ldg(rec + j);
-                        const FT ox = j < m1 ? o0 : (j < m2 ? o1 : o2);
-                        sep[0] = (r.x - own[0]) + ox;
-                        sep[1] = (r.y - own[1]) + oy;
-                        if (D == 3) sep[2] = (r.z - own[2]) + oz;
-                        else cj = __float_as_int(r.z);
-                        bj = __float_as_int(r.w);
-                    } else {
-                        const double2 *q = reinterpret_cast<const double2 *>(rec + j);
-                        double2 r0 = __ldg(q), r1 = __ldg(q + 1);
-                        sep[0] = inbounds(r0.x, xb[0], half_L, L);
-                        sep[1] = inbounds(r0.y, xb[1], half_L, L);
-                        if (D == 3) sep[2] = inbounds(r1.x, xb[2], half_L, L);
-                        else cj = (int)r1.x;
-                        bj = (int)r1.y;
-                    }
-                    FT ds = sep[0] * sep[0] + sep[1] * sep[1];
-                    if (D == 3) ds += sep[2] * sep[2];
-                    if (!(FT(0) < ds && ds <= rc2)) continue;
-                    if ((unsigned)bj >= (unsigned)n) continue;  // never index outside the system
-                    int db = b - bj;
-                    db = db < 0 ? -db : db;
-                    if (nn < 0 || db <= nn) {
-                        if (D == 3) cj = __ldg(p.chain + bj);
-                        if (cj == my_chain) continue;
-                    }
-                    if (shift != FT(0)) {
-                        FT mag = sqrt(ds);
-                        FT nm = mag + shift;
-                        nm = nm < FT(0) ? FT(0) : nm;
-                        FT rs = nm / mag;
-#pragma unroll
-                        for (int i = 0; i < D; i++) sep[i] *= rs;
-                        ds = nm * nm;
-                    }
-                    FT coeff = wca_coeff<FT>(ds, p0, p1);
-#pragma unroll
-                    for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
-                }
+                it[q + 1] = key;
             }
         }
     }
 }
 
-template <int D>
-__device__ __forceinline__ bool bin_bead(const SysP &p, const BatchArgs &A, int *cnt, const double *x, int b)
+// per bead of a flagged system: every non-excluded bead within r_l in the
+// 3^d cells around it, in cell order; records the positions of the build
+template <int D, int WHICH>
+__global__ void __launch_bounds__(512) k_build(BatchArgs A)
 {
-    int c[3] = {0, 0, 0};
+    const int nt = *A.n_bead_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.bead_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        SysS &s = A.S[tl.sys];
+        if (!builds(p, s)) continue;
+        if (tl.begin == 0 && threadIdx.x == 0) s.list_builds += 1;  // one thread per system and build
+        const int b = tl.begin + threadIdx.x;
+        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
+        const int n = p.n, nc = p.nc;
+        const double *X = WHICH == 0 ? p.pos : p.pos1;
+        double x[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-    for (int i = 0; i < D; i++) c[i] = cell_coord(x[i], p.inv_h, p.nc);
-    int64_t gc = p.cell_off + ((int64_t)c[2] * p.nc + c[1]) * p.nc + c[0];
-    int slot = atomicAdd(cnt + gc, 1);
-    if (slot < A.depth) {
-        A.items[(gc << A.log_depth) + slot] = b;
-        return true;
+        for (int i = 0; i < D; i++) x[i] = X[(size_t)b * D + i];
+        int ci[3];
+        cell_of<D>(p, x, ci);
+        // excluded partners: the beads of b's chain within n_nearby of b (all
+        // of them when n_nearby < 0); chains are contiguous bead ranges
+        int ch = p.chain[b];
+        ch = ch < 0 ? 0 : (ch >= p.n_chains ? p.n_chains - 1 : ch);
+        const int c_lo = p.chain_start[ch], c_hi = p.chain_start[ch + 1] - 1;
+        const int nn = p.n_nearby;
+        const int ex_lo = nn < 0 ? c_lo : max(c_lo, b - nn);
+        const int ex_hi = nn < 0 ? c_hi : min(c_hi, b + nn);
+        int *out = A.nbr + p.bead_off + b;
+        const int64_t stride = A.list_stride;
+        const int cap = A.list_depth;
+        int cnt = 0;
+        bool bad = false;
+        const int zlo = (D == 3) ? -1 : 0, zhi = (D == 3) ? 1 : 0;
+        for (int dz = zlo; dz <= zhi; dz++) {
+            int cz = 0;
+            if (D == 3) {
+                cz = ci[2] + dz;
+                cz = cz < 0 ? cz + nc : (cz >= nc ? cz - nc : cz);
+            }
+            for (int dy = -1; dy <= 1; dy++) {
+                int cy = ci[1] + dy;
+                cy = cy < 0 ? cy + nc : (cy >= nc ? cy - nc : cy);
+                for (int dx = -1; dx <= 1; dx++) {
+                    int cx = ci[0] + dx;
+                    cx = cx < 0 ? cx + nc : (cx >= nc ? cx - nc : cx);
+                    const int64_t gc = p.cell_off + ((int64_t)cz * nc + cy) * nc + cx;
+                    int m = A.ncell[gc];
+                    m = m < 0 ? 0 : (m < A.depth ? m : A.depth);
+                    const int *it = A.items + (gc << A.log_depth);
+                    for (int q = 0; q < m; q++) {
+                        const int j = it[q];
+                        if ((unsigned)j >= (unsigned)n) {
+                            bad = true;  // never index outside the system
+                            continue;
+                        }
+                        if (j >= ex_lo && j <= ex_hi) continue;  // b itself is in this range
+                        double ds = 0.0;
+#pragma unroll
+                        for (int i = 0; i < D; i++) {
+                            double d = inbounds(X[(size_t)j * D + i], x[i], p.half_L, p.L);
+                            ds += d * d;
+                        }
+                        if (ds <= p.rl2) {
+                            if (cnt < cap) out[(size_t)cnt * stride] = j;
+                            cnt++;
+                        }
+                    }
+                }
+            }
+        }
+        A.ncount[p.bead_off + b] = cnt < cap ? cnt : cap;
+        double *r = A.xref + (size_t)(p.bead_off + b) * D;
+#pragma unroll
+        for (int i = 0; i < D; i++) r[i] = x[i];
+        if (cnt > cap) atomicOr(&s.flags, kFlagListOverflow);
+        if (bad) atomicOr(&s.flags, kFlagListCorrupt);
     }
-    return false;
+}
+
+// pair forces over the neighbour list (forces.py:57-145, rule forces.WCA):
+// min-image separation of the FP64 positions, rounded to FT, then the rule
+// in FT; writes the pair force of every bead to fp[bead]
+template <int D, typename FT, int WHICH>
+__global__ void __launch_bounds__(512) k_pair(BatchArgs A)
+{
+    const int nt = *A.n_bead_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.bead_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        SysS &s = A.S[tl.sys];
+        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal) || !p.calc_wca) continue;
+        // the list is current for this stage: the next build needs a new flag
+        if (threadIdx.x == 0 && s.rebuild) s.rebuild = 0;
+        const int b = tl.begin + threadIdx.x;
+        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
+        const int n = p.n;
+        const double *X = WHICH == 0 ? p.pos : p.pos1;
+        double xb[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < D; i++) xb[i] = X[(size_t)b * D + i];
+        int cnt = A.ncount[p.bead_off + b];
+        cnt = cnt < 0 ? 0 : (cnt < A.list_depth ? cnt : A.list_depth);
+        const int *nb = A.nbr + p.bead_off + b;
+        const int64_t stride = A.list_stride;
+        const FT rc2 = (FT)p.rc2, p0 = (FT)p.p0, p1 = (FT)p.p1, shift = (FT)p.shift;
+        FT F[3] = {FT(0), FT(0), FT(0)};
+        bool bad = false;
+        for (int k = 0; k < cnt; k++) {
+            const int j = nb[(size_t)k * stride];
+            if ((unsigned)j >= (unsigned)n) {
+                bad = true;
+                continue;
+            }
+            FT sep[3];
+            FT ds = FT(0);
+#pragma unroll
+            for (int i = 0; i < D; i++) {
+                sep[i] = (FT)inbounds(X[(size_t)j * D + i], xb[i], p.half_L, p.L);
+                ds += sep[i] * sep[i];
+            }
+            if (!(FT(0) < ds && ds <= rc2)) continue;
+            if (shift != FT(0)) {
+                FT mag = sqrt(ds);
+                FT nm = mag + shift;
+                nm = nm < FT(0) ? FT(0) : nm;
+                FT rs = nm / mag;
+#pragma unroll
+                for (int i = 0; i < D; i++) sep[i] *= rs;
+                ds = nm * nm;
+            }
+            FT coeff = wca_coeff<FT>(ds, p0, p1);
+#pragma unroll
+            for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
+        }
+        if (bad) atomicOr(&s.flags, kFlagListCorrupt);
+        FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
+#pragma unroll
+        for (int i = 0; i < D; i++) fp[i] = F[i];
+    }
 }
 
 template <int D, typename FT>
@@ -332,255 +437,10 @@ __device__ __forceinline__ double srk_update(double x, double dt_eff, double s2,
     return py_mod(tmp, L);
 }
 
+
 // ------------------------------------------------------------------------
-// kernels
+// stage and update kernels
 // ------------------------------------------------------------------------
-template <int D>
-__global__ void __launch_bounds__(512) k_insert(BatchArgs A)
-{
-    const int nt = *A.n_bead_tiles;
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const Tile tl = A.bead_tiles[t];
-        const SysP &p = A.P[tl.sys];
-        SysS &s = A.S[tl.sys];
-        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal) || !p.calc_wca) continue;
-        int b = tl.begin + threadIdx.x;
-        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
-        double x[3];
-#pragma unroll
-        for (int i = 0; i < D; i++) x[i] = p.pos[(size_t)b * D + i];
-        if (!bin_bead<D>(p, A, A.cnt0, x, b)) atomicOr(&s.flags, kFlagCellOverflow);
-    }
-}
-
-// exclusive scan of the binned counts of one tile of cells (block scan),
-// clearing the other count buffer for the next binning
-template <int WHICH>
-__global__ void __launch_bounds__(512) k_scan_local(BatchArgs A)
-{
-    __shared__ int sh_w[16];
-    __shared__ int sh_run;
-    const int nt = *A.n_cell_tiles;
-    const int *cnt = WHICH == 0 ? A.cnt0 : A.cnt1;
-    int *other = WHICH == 0 ? A.cnt1 : A.cnt0;
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        __syncthreads();
-        const Tile tl = A.cell_tiles[t];
-        const SysP &p = A.P[tl.sys];
-        SysS &s = A.S[tl.sys];
-        if (threadIdx.x == 0)
-            sh_run = ld_volatile(&s.active) && p.calc_wca && !(ld_volatile(&s.flags) & kFlagFatal);
-        __syncthreads();
-        if (!sh_run) continue;
-        const int c = tl.begin + threadIdx.x;
-        const bool in = c < p.n_cells && threadIdx.x < A.tile_cells;
-        const int64_t gc = p.cell_off + c;
-        int v = 0;
-        if (in) {
-            v = cnt[gc];
-            v = v < A.depth ? v : A.depth;
-            other[gc] = 0;
-        }
-        // block exclusive scan
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        int x = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) sh_w[w] = x;
-        __syncthreads();
-        if (w == 0) {
-            int nw = (blockDim.x + 31) >> 5;
-            int y = lane < nw ? sh_w[lane] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int z = __shfl_up_sync(0xffffffffu, y, o);
-                if (lane >= o) y += z;
-            }
-            if (lane < nw) sh_w[lane] = y;  // inclusive prefix of warp totals
-        }
-        __syncthreads();
-        int ex = x - v + (w > 0 ? sh_w[w - 1] : 0);
-        if (in) A.cstart[gc] = ex;
-        if (threadIdx.x == blockDim.x - 1) A.tsum[t] = ex + v;
-    }
-}
-
-// exclusive scan of the tile totals of each system (one CTA per system);
-// writes the end sentinel cstart[n_cells]
-__global__ void __launch_bounds__(256) k_scan_tiles(BatchArgs A, int n_slots)
-{
-    __shared__ int sh_w[8];
-    __shared__ int sh_carry;
-    const int sys = blockIdx.x;
-    if (sys >= n_slots) return;
-    const SysP &p = A.P[sys];
-    SysS &s = A.S[sys];
-    if (!(s.active && p.calc_wca && !(s.flags & kFlagFatal)) || p.n_cell_tiles == 0) return;
-    if (p.cell_tile0 < 0 || p.cell_tile0 + p.n_cell_tiles > *A.n_cell_tiles) {
-        if (threadIdx.x == 0) atomicOr(&s.flags, kFlagListCorrupt);
-        return;
-    }
-    if (threadIdx.x == 0) sh_carry = 0;
-    __syncthreads();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    for (int base = 0; base < p.n_cell_tiles; base += blockDim.x) {
-        const int t = base + threadIdx.x;
-        const int v = t < p.n_cell_tiles ? A.tsum[p.cell_tile0 + t] : 0;
-        int x = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, x, o);
-            if (lane >= o) x += y;
-        }
-        if (lane == 31) sh_w[w] = x;
-        __syncthreads();
-        if (w == 0) {
-            int nw = blockDim.x >> 5;
-            int y = lane < nw ? sh_w[lane] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int z = __shfl_up_sync(0xffffffffu, y, o);
-                if (lane >= o) y += z;
-            }
-            if (lane < nw) sh_w[lane] = y;
-        }
-        __syncthreads();
-        const int carry = sh_carry;
-        const int ex = x - v + (w > 0 ? sh_w[w - 1] : 0) + carry;
-        if (t < p.n_cell_tiles) A.toff[p.cell_tile0 + t] = ex;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) sh_carry = ex + v;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) A.cstart[p.cell_off + p.n_cells] = sh_carry;
-}
-
-// per GPU cell: final start, the slot contents sorted by bead id, packed
-// records of the build's positions written to the compact list
-template <int D, typename FT, int WHICH>
-__global__ void __launch_bounds__(512) k_pack(BatchArgs A)
-{
-    using R = typename Rec<FT>::type;
-    const int nt = *A.n_cell_tiles;
-    const int *cnt = WHICH == 0 ? A.cnt0 : A.cnt1;
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const Tile tl = A.cell_tiles[t];
-        const SysP &p = A.P[tl.sys];
-        const SysS &s = A.S[tl.sys];
-        bool run = ld_volatile(&s.active) && p.calc_wca && !(ld_volatile(&s.flags) & kFlagFatal);
-        if (!run) continue;
-        int c = tl.begin + threadIdx.x;
-        if (c >= p.n_cells || threadIdx.x >= A.tile_cells) continue;
-        const int64_t gc = p.cell_off + c;
-        int n = cnt[gc];
-        n = n < A.depth ? n : A.depth;
-        const int start = A.toff[t] + A.cstart[gc];
-        A.cstart[gc] = start;
-        if (n == 0) continue;
-        if (start < 0 || start + n > p.n) {
-            // never write outside the system's part of the list
-            atomicOr((int *)&s.flags, kFlagListCorrupt);
-            continue;
-        }
-        int *it = A.items + (gc << A.log_depth);
-        const double *X = WHICH == 0 ? p.pos : p.pos1;
-        int cc[3];
-        cc[0] = c % p.nc;
-        cc[1] = (c / p.nc) % p.nc;
-        cc[2] = (D == 3) ? c / (p.nc * p.nc) : 0;
-        double ctr[3];
-#pragma unroll
-        for (int i = 0; i < 3; i++) ctr[i] = ((double)cc[i] + 0.5) * p.h;
-        R *out = reinterpret_cast<R *>(A.rec) + p.bead_off + start;
-        int *ocell = A.rcell + p.bead_off + start;
-        auto emit = [&](int j, int b) {
-            double x[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-            for (int i = 0; i < D; i++) x[i] = X[(size_t)b * D + i];
-            R r;
-            // 2D records carry the bead's chain id in the spare z slot, so the
-            // pair loop's exclusion test needs no second load
-            if constexpr (sizeof(FT) == 4) {
-                r.x = (float)(x[0] - ctr[0]);
-                r.y = (float)(x[1] - ctr[1]);
-                r.z = (D == 3) ? (float)(x[2] - ctr[2]) : __int_as_float(__ldg(p.chain + b));
-                r.w = __int_as_float(b);
-            } else {
-                r.x = x[0];
-                r.y = x[1];
-                r.z = (D == 3) ? x[2] : (double)__ldg(p.chain + b);
-                r.w = (double)b;
-            }
-            out[j] = r;
-            ocell[j] = c;
-        };
-        if (n <= 8) {
-            int v[8];
-#pragma unroll
-            for (int j = 0; j < 8; j++) v[j] = j < n ? it[j] : 0x7fffffff;
-            // Batcher odd-even merge sort network for 8 keys (19 comparators)
-#define GCR_CX(a, b)                 \
-    {                                \
-        int lo = min(v[a], v[b]);    \
-        int hi = max(v[a], v[b]);    \
-        v[a] = lo;                   \
-        v[b] = hi;                   \
-    }
-            GCR_CX(0, 1) GCR_CX(2, 3) GCR_CX(4, 5) GCR_CX(6, 7)
-            GCR_CX(0, 2) GCR_CX(1, 3) GCR_CX(4, 6) GCR_CX(5, 7)
-            GCR_CX(1, 2) GCR_CX(5, 6)
-            GCR_CX(0, 4) GCR_CX(1, 5) GCR_CX(2, 6) GCR_CX(3, 7)
-            GCR_CX(2, 4) GCR_CX(3, 5)
-            GCR_CX(1, 2) GCR_CX(3, 4) GCR_CX(5, 6)
-#undef GCR_CX
-#pragma unroll
-            for (int j = 0; j < 8; j++)
-                if (j < n) emit(j, v[j]);
-        } else {
-            // insertion sort in place (cells this dense are rare)
-            for (int j = 1; j < n; j++) {
-                int key = it[j];
-                int q = j - 1;
-                while (q >= 0 && it[q] > key) {
-                    it[q + 1] = it[q];
-                    q--;
-                }
-                it[q + 1] = key;
-            }
-            for (int j = 0; j < n; j++) emit(j, it[j]);
-        }
-    }
-}
-
-// pair forces in cell order (forces.py:57-145, rule forces.WCA); writes the
-// pair force of every bead to fp[bead]
-template <int D, typename FT>
-__global__ void __launch_bounds__(512) k_pair(BatchArgs A)
-{
-    const int nt = *A.n_bead_tiles;
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const Tile tl = A.bead_tiles[t];
-        const SysP &p = A.P[tl.sys];
-        SysS &s = A.S[tl.sys];
-        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal) || !p.calc_wca) continue;
-        const int k = tl.begin + threadIdx.x;
-        if (k >= p.n || threadIdx.x >= A.tile_beads) continue;
-        FT F[3] = {FT(0), FT(0), FT(0)};
-        int b;
-        pair_force_sorted<D, FT>(p, A, k, b, F);
-        if (b < 0 || b >= p.n) {
-            atomicOr(&s.flags, kFlagListCorrupt);
-            continue;
-        }
-        FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
-#pragma unroll
-        for (int i = 0; i < D; i++) fp[i] = F[i];
-    }
-}
-
 template <int D, typename FT, int STAGE>
 __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
 {
@@ -786,8 +646,8 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
                 }
                 if (!finite)
                     atomicOr(&s.flags, kFlagNonFinite);
-                else if (p.calc_wca && !bin_bead<D>(p, A, A.cnt1, x1, b))
-                    atomicOr(&s.flags, kFlagCellOverflow);
+                else if (p.calc_wca && left_skin<D>(p, A, b, x1))
+                    s.rebuild = 1;  // the list of pos no longer covers pos1
             } else {
                 // |F0+F1|^2 in FP64 for the dt rule (SRK.py:328)
                 double acc = 0.0;
@@ -870,7 +730,7 @@ __global__ void __launch_bounds__(512) k_update(BatchArgs A)
 #pragma unroll
             for (int i = 0; i < D; i++) tan[(size_t)b * D + i] = tb[i] / mag;
         }
-        if (finite && p.calc_wca && !bin_bead<D>(p, A, A.cnt0, x, b)) atomicOr(&s.flags, kFlagNextOverflow);
+        if (finite && p.calc_wca && left_skin<D>(p, A, b, x)) s.rebuild = 1;  // rebuild before the next step
     }
 }
 
@@ -915,7 +775,7 @@ __global__ void k_sys_end(BatchArgs A, int n_slots)
     s.steps_done += 1;
     s.max_f2 = 0ull;
     bool more = (s.steps_done < s.max_steps || s.max_steps < 0) &&
-                (s.elapsed < s.max_dt_usable || s.max_dt_usable < 0.0) && !(s.flags & kFlagNextOverflow);
+                (s.elapsed < s.max_dt_usable || s.max_dt_usable < 0.0);
     s.active = more ? 1 : 0;
 }
 
@@ -933,15 +793,23 @@ __global__ void k_topo(const int32_t *__restrict__ chain, int n, uint8_t *topo)
     topo[b] = t;
 }
 
+
+// flag every resident system for a list build (the start of a run: the host
+// may have changed positions since the last list)
+__global__ void k_sys_mark(BatchArgs A, int n_slots)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_slots) return;
+    A.S[i].rebuild = 1;
+}
+
 // ------------------------------------------------------------------------
 // launchers
 // ------------------------------------------------------------------------
 template <int D, typename FT>
 struct StepKernels {
-    static void *pair() { return (void *)k_pair<D, FT>; }
-    static void *insert() { return (void *)k_insert<D>; }
-    static void *pack0() { return (void *)k_pack<D, FT, 0>; }
-    static void *pack1() { return (void *)k_pack<D, FT, 1>; }
+    static void *pair0() { return (void *)k_pair<D, FT, 0>; }
+    static void *pair1() { return (void *)k_pair<D, FT, 1>; }
     static void *stage0() { return (void *)k_stage<D, FT, 0>; }
     static void *stage1() { return (void *)k_stage<D, FT, 1>; }
     static void *update() { return (void *)k_update<D, FT>; }
@@ -954,13 +822,11 @@ KernelSet kernel_set(int dim, int precision)
         k.stage_smem = precision == 0 ? stage_smem_bytes<2, double> : stage_smem_bytes<2, float>;
     else
         k.stage_smem = precision == 0 ? stage_smem_bytes<3, double> : stage_smem_bytes<3, float>;
-#define GCR_FILL(D_, FT_)                           \
-    k.pair = StepKernels<D_, FT_>::pair();          \
-    k.insert = StepKernels<D_, FT_>::insert();      \
-    k.pack0 = StepKernels<D_, FT_>::pack0();        \
-    k.pack1 = StepKernels<D_, FT_>::pack1();        \
-    k.stage0 = StepKernels<D_, FT_>::stage0();      \
-    k.stage1 = StepKernels<D_, FT_>::stage1();      \
+#define GCR_FILL(D_, FT_)                       \
+    k.pair0 = StepKernels<D_, FT_>::pair0();    \
+    k.pair1 = StepKernels<D_, FT_>::pair1();    \
+    k.stage0 = StepKernels<D_, FT_>::stage0();  \
+    k.stage1 = StepKernels<D_, FT_>::stage1();  \
     k.update = StepKernels<D_, FT_>::update();
     if (dim == 2 && precision == 0) {
         GCR_FILL(2, double)
@@ -972,12 +838,22 @@ KernelSet kernel_set(int dim, int precision)
         GCR_FILL(3, float)
     }
 #undef GCR_FILL
+    if (dim == 2) {
+        k.bin0 = (void *)k_bin<2, 0>;
+        k.bin1 = (void *)k_bin<2, 1>;
+        k.build0 = (void *)k_build<2, 0>;
+        k.build1 = (void *)k_build<2, 1>;
+    } else {
+        k.bin0 = (void *)k_bin<3, 0>;
+        k.bin1 = (void *)k_bin<3, 1>;
+        k.build0 = (void *)k_build<3, 0>;
+        k.build1 = (void *)k_build<3, 1>;
+    }
+    k.sort = (void *)k_sort;
     k.topo = (void *)k_topo;
     k.sys_dt = (void *)k_sys_dt;
-    k.scan_local0 = (void *)k_scan_local<0>;
-    k.scan_local1 = (void *)k_scan_local<1>;
-    k.scan_tiles = (void *)k_scan_tiles;
     k.sys_end = (void *)k_sys_end;
+    k.sys_mark = (void *)k_sys_mark;
     return k;
 }
 

@@ -45,6 +45,7 @@ class SystemParams:
     seed: int = 0
     step: int = 0
     cell_factor: float = 1.0
+    skin: float = 0.3            # Verlet skin of the neighbour list (length units of the box)
 
     def desc(self, n_beads, n_chains):
         d = SystemDesc()
@@ -61,6 +62,7 @@ class SystemParams:
         d.dtmax, d.max_dist_per_step, d.rk_cheat = float(self.dtmax), float(self.max_dist_per_step), \
             float(self.rk_cheat)
         d.seed, d.step, d.cell_factor = int(self.seed) & (2 ** 64 - 1), int(self.step), float(self.cell_factor)
+        d.skin = float(self.skin)
         return d
 
 
@@ -111,7 +113,7 @@ class SystemState:
 
 def default_config(dim, precision="fp64", bead_capacity=1 << 20, system_capacity=1,
                    cell_capacity=None, cell_depth=None, block_beads=256, block_cells=256,
-                   steps_per_graph=10, ctas_per_sm=0):
+                   steps_per_graph=10, ctas_per_sm=0, list_depth=0):
     cfg = Config()
     cfg.dim = dim
     cfg.precision = PRECISIONS[precision]
@@ -123,6 +125,7 @@ def default_config(dim, precision="fp64", bead_capacity=1 << 20, system_capacity
         raise ValueError("cell_depth must be 8, 16, 32, 64 or 128")
     cfg.block_beads, cfg.block_cells = int(block_beads), int(block_cells)
     cfg.steps_per_graph, cfg.ctas_per_sm = int(steps_per_graph), int(ctas_per_sm)
+    cfg.list_depth = int(list_depth)
     return cfg
 
 
@@ -231,7 +234,7 @@ class Engine:
     def synchronize(self):
         check(self.lib.gcr_synchronize(self._ctx))
 
-    PROFILE_GROUPS = ["cells_pos", "pair_pos", "stage0", "cells_pos1", "pair_pos1", "stage1", "update"]
+    PROFILE_GROUPS = ["lists_pos", "pair_pos", "stage0", "lists_pos1", "pair_pos1", "stage1", "update"]
 
     def profile_steps(self, n_steps):
         """Milliseconds per kernel group over ``n_steps`` individually
@@ -249,7 +252,8 @@ class Engine:
         s = Status()
         check(self.lib.gcr_get_status(self._ctx, int(slot), C.byref(s)))
         return {"dt": s.dt, "dt_used": s.dt_used, "max_forces_strength": s.max_forces_strength,
-                "steps_done": s.steps_done, "step": s.step, "flags": s.flags, "active": bool(s.active)}
+                "steps_done": s.steps_done, "step": s.step, "flags": s.flags, "active": bool(s.active),
+                "list_builds": s.list_builds}
 
     # -- observables and exports --------------------------------------------
     def order_params(self, slot):
@@ -283,6 +287,22 @@ class Engine:
                 grid_depth1 = 2 * grid_depth1
             else:
                 nbor_depth1 = 2 * nbor_depth1
+
+    def neighbour_list(self, slot, partners=True):
+        """Counts [n], partners [n, list_depth] (bead ids in summation order,
+        -1 past the count), the FP64 positions of the build [n, d] and the
+        total entries of a system's list as of its last build."""
+        st = self.systems[slot]
+        dev = st.pos.device
+        counts = torch.zeros(st.n, dtype=torch.int32, device=dev)
+        part = torch.full((st.n, self.cfg.list_depth), -1, dtype=torch.int32, device=dev) if partners else None
+        xb = torch.zeros((st.n, self.dim), dtype=torch.float64, device=dev)
+        total = C.c_int64()
+        torch.cuda.current_stream(dev).synchronize()
+        check(self.lib.gcr_neighbour_list(self._ctx, int(slot), C.c_void_p(counts.data_ptr()),
+                                          C.c_void_p(part.data_ptr()) if part is not None else None,
+                                          self.cfg.list_depth, C.c_void_p(xb.data_ptr()), C.byref(total)))
+        return counts, part, xb, total.value
 
     def cell_assignment(self, slot):
         st = self.systems[slot]

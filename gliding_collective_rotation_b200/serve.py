@@ -35,7 +35,8 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from .batch import MAX_DEPTH, OVERFLOW, default_depth
+from ._lib import FLAG_CELL_OVERFLOW, FLAG_LIST_OVERFLOW
+from .batch import MAX_DEPTH, MAX_LIST_DEPTH, OVERFLOW, default_depth, default_list_depth
 from .engine import Engine, SystemState
 from .workloads import SystemSpec, make_system
 
@@ -102,7 +103,8 @@ class Server:
         self.chunk = int(chunk)
         self.relax_max_steps = int(relax_max_steps)
         self.max_head_wait = float(max_head_wait)
-        self.cell_depth = cell_depth or default_depth(dim, 1.0)
+        self.cell_depth = cell_depth or default_depth(dim, 1.3)  # cells of side r_cut + skin
+        self.list_depth = default_list_depth(dim)
         self.max_systems = int(max_systems)
         self.cells_per_bead = float(cells_per_bead)
         self.steps_per_graph = int(steps_per_graph)
@@ -117,9 +119,8 @@ class Server:
     # -- memory ----------------------------------------------------------------
     def _per_bead_bytes(self):
         ft = 4 if self.precision == "mixed" else 8
-        rec = 16 if self.precision == "mixed" else 32
-        scratch = rec + 4 + 2 * self.dim * ft + 1          # records, record cells, pair force, noise, topology
-        per_cell = 4 * (self.cell_depth + 3)               # slots, two counts, start
+        scratch = 2 * self.dim * ft + 1 + 4 * self.list_depth + 4 + 8 * self.dim  # fp, xi, topo, list, xref
+        per_cell = 4 * (self.cell_depth + 2)               # slots, count, count at the build
         return _STATE_BYTES[self.precision] + scratch + self.cells_per_bead * per_cell
 
     def _size_context(self):
@@ -129,7 +130,7 @@ class Server:
     def _make_engine(self):
         return Engine(self.dim, self.precision, device=self.device, bead_capacity=self.bead_capacity,
                       system_capacity=self.max_systems, cell_capacity=self.cell_capacity,
-                      cell_depth=self.cell_depth, steps_per_graph=self.steps_per_graph)
+                      cell_depth=self.cell_depth, list_depth=self.list_depth, steps_per_graph=self.steps_per_graph)
 
     def fits_ever(self, req: Request):
         return req.spec.n <= self.bead_capacity
@@ -171,13 +172,20 @@ class Server:
 
     # -- overflow --------------------------------------------------------------
     def _regrow(self, statuses):
-        if self.cell_depth >= MAX_DEPTH:
-            raise RuntimeError("GPU cell depth limit reached")
+        flags = 0
         for slot, lv in self.live.items():
             lv.state.params.step = statuses[slot]["step"]
+            flags |= statuses[slot]["flags"]
+        cell = bool(flags & FLAG_CELL_OVERFLOW)
+        lst = bool(flags & FLAG_LIST_OVERFLOW) or not cell
+        if (cell and self.cell_depth >= MAX_DEPTH) or (lst and self.list_depth >= MAX_LIST_DEPTH):
+            raise RuntimeError("GPU cell or list depth limit reached")
         old = list(self.live.values())
         self.engine.close()
-        self.cell_depth *= 2
+        if cell:
+            self.cell_depth *= 2
+        if lst:
+            self.list_depth *= 2
         self._size_context()
         self.engine = self._make_engine()
         self.live = {}

@@ -11,10 +11,10 @@ Same signature, inputs, outputs and bookkeeping as the reference's
   ``status.update_grid_list_counter`` -- updates.py:249-256;
 * leaves the population's ``pos``, ``pos1``, ``tangent_list`` and ``forces``
   as the reference leaves them (F0 + F1 of the last step, tangents at pos1);
-* raises no exception for numerical trouble: a GPU cell overflow makes the
-  next call use deeper cells (the reference regrows its lists the same way,
-  updates.py:257-267) and non-finite values are reported in
-  ``status.gpu_flags``.
+* raises no exception for numerical trouble: a GPU cell or neighbour-list
+  overflow makes the next call use deeper cells or lists (the reference
+  regrows its lists the same way, updates.py:257-267) and non-finite values
+  are reported in ``status.gpu_flags``.
 
 The bead state stays on the device between calls; each call uploads the
 host arrays (the caller may have changed them) and downloads the result.
@@ -33,6 +33,8 @@ import numpy as np
 import torch
 
 from . import config as _default_config
+from ._lib import FLAG_CELL_OVERFLOW, FLAG_LIST_OVERFLOW
+from .batch import MAX_DEPTH, MAX_LIST_DEPTH, cell_scale, default_depth, default_list_depth
 from .engine import Engine, SystemParams, SystemState, default_config, footprint
 
 _config = _default_config
@@ -72,15 +74,15 @@ _SUPPORTED = {"springs", "WCA", "self-propulsion"}
 class _GpuPop:
     """Device copy of one population and the context that steps it."""
 
-    def __init__(self, pop, sim, dim, precision, params, cell_depth):
-        self.key = (pop.total_pop, len(pop.rest_lengths), dim, precision, float(params.L),
-                    float(params.wca_params[3]), float(params.cell_factor), cell_depth, bool(params.calc_wca))
+    def __init__(self, pop, sim, dim, precision, params, cell_depth, list_depth, key):
+        self.key = key
         n = pop.total_pop
         spg = int(sim.get('gpu_steps_per_graph', 10))
-        cfg = default_config(dim, precision, cell_depth=cell_depth)
+        cfg = default_config(dim, precision, cell_depth=cell_depth, list_depth=list_depth)
         cells = footprint(cfg, params, n, len(pop.rest_lengths))[0]
         self.engine = Engine(dim, precision, bead_capacity=max(n, 1), system_capacity=1,
-                             cell_capacity=max(cells, 1), cell_depth=cell_depth, steps_per_graph=spg)
+                             cell_capacity=max(cells, 1), cell_depth=cell_depth, list_depth=list_depth,
+                             steps_per_graph=spg)
         self.state = SystemState.from_host(pop.pos, pop.tangent_list, pop.chain_id, pop.rest_lengths, params,
                                            precision=precision, device=self.engine.device)
         self.engine.admit(self.state)
@@ -93,14 +95,15 @@ class _GpuPop:
 
 
 def _gpu_state(pop, sim, dim, precision, params):
-    depth = getattr(pop, "_gcr_cell_depth", 16 if dim == 2 else 32)
+    depth = getattr(pop, "_gcr_cell_depth", default_depth(dim, cell_scale(params)))
+    ldepth = getattr(pop, "_gcr_list_depth", default_list_depth(dim))
     g = getattr(pop, "_gcr", None)
     key = (pop.total_pop, len(pop.rest_lengths), dim, precision, float(params.L), float(params.wca_params[3]),
-           float(params.cell_factor), depth, bool(params.calc_wca))
+           float(params.cell_factor), float(params.skin), depth, ldepth, bool(params.calc_wca))
     if g is None or g.key != key:
         if g is not None:
             g.engine.close()
-        g = _GpuPop(pop, sim, dim, precision, params, depth)
+        g = _GpuPop(pop, sim, dim, precision, params, depth, ldepth, key)
         pop._gcr = g
     return g
 
@@ -148,7 +151,8 @@ def SRK2_force_calc(pops, status, sim):
         Dr=float(pop.Dr), radius=float(pop.repel_d_max), n_nearby=int(pop.n_nearby_beads_dont_repel),
         calc_springs=calc_springs, calc_wca=calc_wca, self_propel=self_propel, dtmax=float(status.dtmax),
         max_dist_per_step=float(cfg.max_dist_per_step), rk_cheat=float(cfg.RK_cheat_factor), seed=seed,
-        step=int(status.stepnum), cell_factor=float(sim.get('gpu_cell_factor', 1.0)))
+        step=int(status.stepnum), cell_factor=float(sim.get('gpu_cell_factor', 1.0)),
+        skin=float(sim.get('gpu_skin', 0.3)))
     g = _gpu_state(pop, sim, dim, precision, params)
     st, eng = g.state, g.engine
 
@@ -221,7 +225,9 @@ def SRK2_force_calc(pops, status, sim):
     status.update_grid_list_counter = max(
         1, (steps_done + status.update_grid_list_counter) % cfg.n_steps_update_grid_list)
     status.gpu_flags = res['flags']
-    if res['flags'] & 5:
+    if res['flags'] & FLAG_CELL_OVERFLOW:
         # cell overflow: deeper cells for the next call (updates.py:257-267)
-        pop._gcr_cell_depth = min(64, 2 * getattr(pop, "_gcr_cell_depth", 16 if dim == 2 else 32))
+        pop._gcr_cell_depth = min(MAX_DEPTH, 2 * g.engine.cfg.cell_depth)
+    if res['flags'] & FLAG_LIST_OVERFLOW:
+        pop._gcr_list_depth = min(MAX_LIST_DEPTH, 2 * g.engine.cfg.list_depth)
     return None

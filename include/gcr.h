@@ -60,8 +60,9 @@ extern "C" {
 /* per-system device status flags */
 #define GCR_FLAG_CELL_OVERFLOW 1   /* more beads in a cell than cell_depth */
 #define GCR_FLAG_NONFINITE 2       /* a non-finite force or position */
-#define GCR_FLAG_NEXT_OVERFLOW 4   /* overflow while binning for the next step */
-#define GCR_FLAG_LIST_CORRUPT 8    /* an inconsistent cell list was detected and not used */
+#define GCR_FLAG_NEXT_OVERFLOW 4   /* reserved (no longer raised) */
+#define GCR_FLAG_LIST_CORRUPT 8    /* an inconsistent cell or neighbour list was detected and not used */
+#define GCR_FLAG_LIST_OVERFLOW 16  /* more list partners of a bead than list_depth */
 
 typedef struct gcr_ctx gcr_ctx;
 
@@ -76,6 +77,7 @@ typedef struct {
     int32_t block_cells;      /* threads per CTA of the cell kernel (64..512) */
     int32_t steps_per_graph;  /* SRK2 steps per captured CUDA graph (1..64) */
     int32_t ctas_per_sm;      /* persistent CTAs per SM (0 = from occupancy, <0 = one CTA per tile) */
+    int32_t list_depth;       /* neighbour-list slots per bead, 4..1024 (0 = 32 in 2D, 96 in 3D) */
 } gcr_config;
 
 /* One system.  The packed arrays follow the reference's packing exactly. */
@@ -94,7 +96,10 @@ typedef struct {
     double dtmax, max_dist_per_step, rk_cheat;
     uint64_t seed;              /* Philox key */
     int64_t step;               /* global index of the next step (Philox counter) */
-    double cell_factor;         /* GPU cell side >= r_cut * cell_factor (>= 1) */
+    double cell_factor;         /* GPU cell side >= (r_cut + skin) * cell_factor (>= 1) */
+    double skin;                /* Verlet skin (>= 0): the neighbour list holds the pairs within
+                                   r_cut + skin and is rebuilt once a bead has moved skin / 2;
+                                   reduced to L/3 - r_cut when the box is too small for it */
 } gcr_system_desc;
 
 /* Caller-owned device buffers of one system (bound, not copied). */
@@ -126,6 +131,7 @@ typedef struct {
     int64_t step;               /* global index of the next step */
     int32_t flags;              /* GCR_FLAG_* */
     int32_t active;             /* still running (limits not reached) */
+    int64_t list_builds;        /* neighbour-list builds since admission */
 } gcr_status;
 
 /* ---- context ---------------------------------------------------------- */
@@ -189,6 +195,14 @@ GCR_API int gcr_reference_lists(gcr_ctx *ctx, int32_t slot, int64_t n_grid, int6
 /* The GPU cell table of one system after binning its current positions:
  * cell index per bead (int32 [n], device) and the grid side (host). */
 GCR_API int gcr_cell_assignment(gcr_ctx *ctx, int32_t slot, int32_t *cell_of_bead, int32_t *n_cells_side);
+/* The neighbour list of a resident system as of its last build (no
+ * counterpart in the reference, whose nbor_list gcr_reference_lists gives):
+ * counts[n] (device, or NULL) partners per bead; partners[n][partners_depth]
+ * (device, or NULL; partners_depth >= the context's list_depth) their bead
+ * ids in summation order; build_pos[n][dim] (device, or NULL) the FP64
+ * positions the list was built from; *entries (host, or NULL) the total. */
+GCR_API int gcr_neighbour_list(gcr_ctx *ctx, int32_t slot, int32_t *counts, int32_t *partners,
+                               int32_t partners_depth, double *build_pos, int64_t *entries);
 /* Standard normals of the Philox stream the step draws: [n][2*dim] noise_vec
  * layout for one step (device out). */
 GCR_API int gcr_philox_noise(int32_t dim, uint64_t seed, int64_t step, int64_t n, int32_t do_trans,
