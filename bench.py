@@ -265,7 +265,9 @@ def run_gpu(args):
                   ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads, list_depth=args.list_depth or None)
     eng = batch.engine
     n_beads = batch.n_beads
-    relax_steps = batch.relax(max_steps=args.relax_steps)
+    # untimed warm-up; every step after it, timed or not, follows the
+    # reference's default adaptive dt rule (dtmax = the configured dt)
+    relax_steps = batch.relax(max_steps=args.relax_steps, adaptive_after=True)
     # warm-up at the fixed dt (regrows the cells if a system overflowed them)
     batch.run_checked(args.warmup)
     eng = batch.engine
@@ -302,6 +304,8 @@ def run_gpu(args):
     steps_done = min(s["steps_done"] for s in st)
     flags = sorted({s["flags"] for s in st})
     value = world * n_beads * args.steps / (ms / 1e3)
+    # the dt the adaptive rule took: bead-weighted mean over the timed steps
+    dt_mean = sum(s["dt_used"] * x.n for s, x in zip(st, batch.states)) / (args.steps * n_beads)
     # neighbour lists: mean length, and bead-builds per stage in the timed region
     list_entries = sum(eng.neighbour_list(x.slot, partners=False)[3] for x in batch.states)
     list_mean = list_entries / n_beads
@@ -409,6 +413,8 @@ def run_gpu(args):
                    "parallelism": f"{world} GPU(s), independent systems per GPU",
                    "l2": f"inputs larger than L2: working set {working_set / 1e6:.0f} MB per GPU > 126 MB",
                    "relax_steps": relax_steps, "steps_done": steps_done, "flags": flags,
+                   "dt_rule": "adaptive (SRK.py:323-353): dtmax = configured dt, max_dist_per_step of "
+                              "config.grid_list_setup", "dt_mean": dt_mean,
                    "cell_factor": args.cell_factor, "skin": args.skin,
                    "steps_per_graph": args.steps_per_graph, "cell_depth": batch.cell_depth,
                    "list_depth": batch.list_depth, "list_mean": list_mean,
@@ -440,7 +446,7 @@ def run_serve(args):
     torch.cuda.set_device(0)
     tr = W.serve_trace(args.requests, rate=args.rate, seed=7, max_beads=args.max_beads, min_steps=args.min_steps,
                        max_steps=args.max_steps)
-    reqs = [S.request_from_trace(e, relax=True, obs_every=args.obs_every) for e in tr]
+    reqs = [S.request_from_trace(e, obs_every=args.obs_every) for e in tr]
     srv = S.Server(2, args.precision, hbm_budget=int(args.hbm_budget_gb * (1 << 30)), chunk=args.chunk)
     clocks = ClockSampler(0)
     clocks.start()
@@ -454,7 +460,7 @@ def run_serve(args):
         "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": f"served trace: {args.requests} requests, Poisson {args.rate}/s, beads log-uniform "
                                f"[1e3, {args.max_beads:.0e}], steps uniform [{args.min_steps}, {args.max_steps}], "
-                               f"relaxed on arrival, P/S/angle every {args.obs_every} steps",
+                               f"adaptive dt (dtmax 1e-3), P/S/angle every {args.obs_every} steps",
                    "chunk": args.chunk, "hbm_budget_gb": args.hbm_budget_gb, **s},
         "clocks": clk,
     }

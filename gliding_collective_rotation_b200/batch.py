@@ -104,6 +104,7 @@ class Batch:
         self.big, self.states = _views(specs, precision, self.device)
         torch.cuda.synchronize(self.device)
         self.engine = None
+        self._carry_dt = None  # dts to hand to the next call after a regrow
         self._make_engine()
 
     def _make_engine(self):
@@ -129,6 +130,8 @@ class Batch:
         for st, s in zip(self.states, sts):
             st.params.step = s["step"]
             flags |= s["flags"]
+        # a re-admitted system starts from dtmax: its dt is handed over by the next call
+        self._carry_dt = [s["dt"] for s in sts]
         cell = bool(flags & FLAG_CELL_OVERFLOW)
         lst = bool(flags & FLAG_LIST_OVERFLOW) or not cell
         if (cell and self.cell_depth >= MAX_DEPTH) or (lst and self.list_depth >= MAX_LIST_DEPTH):
@@ -142,28 +145,49 @@ class Batch:
 
     # -- calls -------------------------------------------------------------------
     def begin(self, max_steps, dt=None, max_dist_per_step=None, max_dt_usable=-1.0):
-        """Arm every system for the next run (one SRK2_force_calc call each)."""
+        """Arm every system for the next run (one SRK2_force_calc call each).
+        Without `dt` each system keeps the dt its last step chose, as the
+        reference's status.dt carries from call to call."""
         for st in self.states:
             if max_dist_per_step is not None and st.params.max_dist_per_step != max_dist_per_step:
                 st.params.max_dist_per_step = max_dist_per_step
                 self.engine.update_params(st)
-        dts = [spec.dt if dt is None else dt for spec in self.specs]
-        self.engine.call_begin_many([st.slot for st in self.states], max_steps, dts, max_dt_usable)
+        self.engine.call_begin_many([st.slot for st in self.states], max_steps, self._dts(dt), max_dt_usable)
+
+    def _dts(self, dt=None):
+        """Per-system dt of the next call: `dt`, else the dts carried over a
+        regrow, else 0 (each system keeps its own)."""
+        if dt is not None:
+            return [dt] * len(self.states)
+        carry, self._carry_dt = self._carry_dt, None
+        return carry if carry is not None else [0.0] * len(self.states)
+
+    def set_adaptive(self, on=True):
+        """The reference's adaptive dt (dtmax = the system's dt,
+        max_dist_per_step of config.grid_list_setup, SRK.py:323-353) or a
+        fixed dt (max_dist_per_step = inf) for every system."""
+        for st, spec in zip(self.states, self.specs):
+            want = spec.relax_mdps if on else math.inf
+            if st.params.max_dist_per_step != want:
+                st.params.max_dist_per_step = want
+                self.engine.update_params(st)
 
     def run(self, max_steps, sync_every=0):
         self.engine.run(max_steps, sync_every)
 
-    def relax(self, max_steps=2000, chunk=200):
+    def relax(self, max_steps=2000, chunk=200, adaptive_after=False):
         """Untimed warm-up under the reference's adaptive dt (dtmax = the
         system's dt, max_dist_per_step from grid_list_setup) until every
-        system takes full steps; removes the overlaps of random placement."""
+        system takes full steps or `max_steps` have run; removes the overlaps
+        of random placement.  Afterwards the systems keep the adaptive rule
+        (`adaptive_after`) or take a fixed dt."""
         done = 0
+        first = True
         while done < max_steps:
-            for st, spec in zip(self.states, self.specs):
-                if st.params.max_dist_per_step != spec.relax_mdps:
-                    st.params.max_dist_per_step = spec.relax_mdps
-                    self.engine.update_params(st)
-            self.engine.call_begin_many([st.slot for st in self.states], chunk, [s.dt for s in self.specs])
+            self.set_adaptive(True)
+            dts = [s.dt for s in self.specs] if first else self._dts()
+            first = False
+            self.engine.call_begin_many([st.slot for st in self.states], chunk, dts)
             self.engine.run(chunk)
             done += chunk
             sts = self.statuses()
@@ -172,29 +196,34 @@ class Batch:
                 continue
             if all(s["dt"] >= spec.dt * (1 - 1e-12) for s, spec in zip(sts, self.specs)):
                 break
-        for st in self.states:
-            st.params.max_dist_per_step = math.inf
-            self.engine.update_params(st)
+        self.set_adaptive(adaptive_after)
         return done
 
     def statuses(self):
         return [self.engine.status(st.slot) for st in self.states]
 
-    def run_checked(self, steps, max_regrow=3):
-        """Run `steps` steps of every system; after a cell overflow regrow the
-        cells and run the remaining steps of the systems that stopped."""
+    def run_checked(self, steps, max_regrow=6):
+        """Run `steps` steps of every system; after a cell or list overflow
+        regrow and run the remaining steps of the systems that stopped.  The
+        returned statuses count in ``steps_done`` the steps of all calls."""
         self.begin(steps)
         self.run(steps)
-        for _ in range(max_regrow):
+        done = [0] * len(self.states)
+        regrows = 0
+        while True:
             sts = self.statuses()
-            if not self.overflowed(sts):
-                return sts
-            left = [steps - s["steps_done"] for s in sts]
+            done = [d + s["steps_done"] for d, s in zip(done, sts)]
+            if not self.overflowed(sts) or regrows >= max_regrow:
+                break
+            left = [steps - d for d in done]
             self.regrow()
+            regrows += 1
             slots = [st.slot for st in self.states]
-            self.engine.call_begin_many(slots, left, [s["dt"] for s in sts])
+            self.engine.call_begin_many(slots, left, self._dts())
             self.run(max(left))
-        return self.statuses()
+        for s, d in zip(sts, done):
+            s["steps_done"] = d
+        return sts
 
     def order_params(self):
         return np.array([self.engine.order_params(st.slot) for st in self.states])

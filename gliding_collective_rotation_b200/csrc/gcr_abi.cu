@@ -633,8 +633,10 @@ int check_call(const gcr_call *call)
 
 void arm(SysS &s, const gcr_call *call)
 {
-    s.dt = call->dt;
-    s.dt_next = call->dt;
+    // dt <= 0: the system keeps the dt its last step chose (status.dt of the
+    // reference, which carries from call to call)
+    if (call->dt > 0.0) s.dt = call->dt;
+    s.dt_next = s.dt;
     s.dt_used = 0.0;
     s.elapsed = 0.0;
     s.max_f2 = 0ull;

@@ -13,11 +13,13 @@ its ranges go to the next one.  Admission is first come first served, and a
 later request that fits may go ahead of a head request that does not
 (backfill) unless the head has waited longer than ``max_head_wait`` seconds.
 
-Fresh chains laid straight at random overlap, so by default a request first
-relaxes under the reference's adaptive dt (``max_dist_per_step`` of
-``config.grid_list_setup``, config.py:189) until the step takes the full dt,
-then runs its requested steps at the fixed dt.  Relaxation steps are
-reported apart from the requested ones.
+Steps follow the reference's adaptive dt by default (dtmax = the request's
+dt, ``max_dist_per_step`` of ``config.grid_list_setup``, config.py:189), which
+also takes fresh chains laid straight at random through their overlaps; a
+request may instead ask for a fixed dt, and then for an untimed relaxation
+under the adaptive rule first (until the step takes the full dt), reported
+apart from the requested steps.  Each system's dt carries from call to call,
+as the reference's ``status.dt`` does.
 
 Calls are chunked: every system is armed for at most ``chunk`` steps (and
 never past its next observation step), the graph runs, statuses come back in
@@ -51,7 +53,8 @@ class Request:
     steps: int
     arrival: float = 0.0
     obs_every: int = 0
-    relax: bool = True
+    relax: bool = False
+    adaptive: bool = True
 
 
 @dataclass
@@ -81,15 +84,16 @@ class _Live:
     relaxing: bool
     relax_steps: int = 0
     done: int = 0
+    dt: float | None = None
     series: list = field(default_factory=list)
 
 
-def request_from_trace(entry, relax=True, obs_every=0):
+def request_from_trace(entry, relax=False, obs_every=0, adaptive=True):
     """A ``Request`` from one entry of ``workloads.serve_trace``."""
     spec = make_system(f"req{entry['id']}", 2, entry["n_chains"], entry["chain_length"], entry["L"],
                        seed=10_000 + entry["id"], kappa=entry["kappa"], v_tan_angle=entry["v_tan_angle"],
                        noise_seed=entry["seed"])
-    return Request(entry["id"], spec, entry["steps"], entry["arrival"], obs_every, relax)
+    return Request(entry["id"], spec, entry["steps"], entry["arrival"], obs_every, relax, adaptive)
 
 
 class Server:
@@ -143,7 +147,7 @@ class Server:
     def _admit_one(self, req: Request):
         sp = req.spec
         p = sp.params
-        if req.relax:
+        if req.relax or req.adaptive:
             p.max_dist_per_step = sp.relax_mdps
         st = SystemState.from_host(sp.pos, sp.tangent, sp.chain_id, sp.rest_lengths, p, precision=self.precision,
                                    device=self.device)
@@ -206,7 +210,8 @@ class Server:
     def _round(self):
         slots = sorted(self.live)
         plan = [self._plan(self.live[s]) for s in slots]
-        dts = [self.live[s].req.spec.dt for s in slots]
+        # each system's dt carries from call to call (the reference's status.dt)
+        dts = [self.live[s].dt if self.live[s].dt is not None else self.live[s].req.spec.dt for s in slots]
         self.engine.call_begin_many(slots, plan, dts)
         self.engine.run(max(plan))
         statuses = {s: self.engine.status(s) for s in slots}
@@ -216,6 +221,7 @@ class Server:
             # steps completed before a stop are valid; an overflowed system
             # resumes from there once the cells have grown
             n_done = st["steps_done"]
+            lv.dt = st["dt"]
             if st["flags"] & OVERFLOW:
                 overflow = True
                 if lv.relaxing:
@@ -228,8 +234,9 @@ class Server:
                 full = st["dt"] >= lv.req.spec.dt * (1 - 1e-12)
                 if full or lv.relax_steps >= self.relax_max_steps:
                     lv.relaxing = False
-                    lv.state.params.max_dist_per_step = math.inf
-                    self.engine.update_params(lv.state)
+                    if not lv.req.adaptive:
+                        lv.state.params.max_dist_per_step = math.inf
+                        self.engine.update_params(lv.state)
                 continue
             lv.done += n_done
             if st["flags"] or n_done < k:

@@ -76,16 +76,14 @@ class _GpuPop:
 
     def __init__(self, pop, sim, dim, precision, params, cell_depth, list_depth, key):
         self.key = key
-        n = pop.total_pop
-        spg = int(sim.get('gpu_steps_per_graph', 10))
-        cfg = default_config(dim, precision, cell_depth=cell_depth, list_depth=list_depth)
-        cells = footprint(cfg, params, n, len(pop.rest_lengths))[0]
-        self.engine = Engine(dim, precision, bead_capacity=max(n, 1), system_capacity=1,
-                             cell_capacity=max(cells, 1), cell_depth=cell_depth, list_depth=list_depth,
-                             steps_per_graph=spg)
+        self.dim, self.precision = dim, precision
+        self.n, self.n_chains = pop.total_pop, len(pop.rest_lengths)
+        self.spg = int(sim.get('gpu_steps_per_graph', 10))
         self.state = SystemState.from_host(pop.pos, pop.tangent_list, pop.chain_id, pop.rest_lengths, params,
-                                           precision=precision, device=self.engine.device)
-        self.engine.admit(self.state)
+                                           precision=precision, device=torch.device("cuda"))
+        self.engine = None
+        self.make_engine(params, cell_depth, list_depth)
+        n = self.n
         ft = torch.float64 if precision == "fp64" else torch.float32
         self.h_pos = torch.empty((n, dim), dtype=torch.float64, pin_memory=True)
         self.h_tan = torch.empty((n, dim), dtype=ft, pin_memory=True)
@@ -93,13 +91,29 @@ class _GpuPop:
         self.h_pos1 = torch.empty((n, dim), dtype=torch.float64, pin_memory=True)
         self.rng = None
 
+    def make_engine(self, params, cell_depth, list_depth):
+        """(Re)create the context and bind the device state to it; the state
+        tensors, and so the bead state, carry over."""
+        if self.engine is not None:
+            self.engine.close()
+        cfg = default_config(self.dim, self.precision, cell_depth=cell_depth, list_depth=list_depth)
+        cells = footprint(cfg, params, self.n, self.n_chains)[0]
+        self.engine = Engine(self.dim, self.precision, bead_capacity=max(self.n, 1), system_capacity=1,
+                             cell_capacity=max(cells, 1), cell_depth=cell_depth, list_depth=list_depth,
+                             steps_per_graph=self.spg, device=self.state.pos.device)
+        self.engine.admit(self.state)
+
+
+def _key(pop, dim, precision, params, depth, ldepth):
+    return (pop.total_pop, len(pop.rest_lengths), dim, precision, float(params.L), float(params.wca_params[3]),
+            float(params.cell_factor), float(params.skin), depth, ldepth, bool(params.calc_wca))
+
 
 def _gpu_state(pop, sim, dim, precision, params):
     depth = getattr(pop, "_gcr_cell_depth", default_depth(dim, cell_scale(params)))
     ldepth = getattr(pop, "_gcr_list_depth", default_list_depth(dim))
     g = getattr(pop, "_gcr", None)
-    key = (pop.total_pop, len(pop.rest_lengths), dim, precision, float(params.L), float(params.wca_params[3]),
-           float(params.cell_factor), float(params.skin), depth, ldepth, bool(params.calc_wca))
+    key = _key(pop, dim, precision, params, depth, ldepth)
     if g is None or g.key != key:
         if g is not None:
             g.engine.close()
@@ -191,15 +205,36 @@ def SRK2_force_calc(pops, status, sim):
     elif mode != 'philox':
         raise ValueError(f"unknown gpu_noise {mode!r}")
 
-    eng.call_begin(st.slot, max_steps=max_steps, dt=float(status.dt), max_dt_usable=max_dt_usable, noise=noise)
-    if max_steps >= 0 and max_dt_usable < 0:
-        eng.run(max_steps, sync_every=0)
-    else:
-        # time-limited: check between graphs whether the system is done
-        budget = max_steps if max_steps >= 0 else (1 << 62)
-        eng.run(budget, sync_every=1)
-    res = eng.status(st.slot)
-    steps_done = int(res['steps_done'])
+    # An overflow of the GPU cells or lists is the library's capacity, not the
+    # model's: grow them in place and finish the call (steps already taken
+    # stand; the step counter, and so the noise stream, carries on).
+    done, elapsed, dt = 0, 0.0, float(status.dt)
+    while True:
+        left = max_steps - done if max_steps >= 0 else -1
+        lim = max_dt_usable - elapsed if max_dt_usable >= 0 else -1.0
+        eng.call_begin(st.slot, max_steps=left, dt=dt, max_dt_usable=lim,
+                       noise=noise[done:] if noise is not None else None)
+        if left >= 0 and max_dt_usable < 0:
+            eng.run(left, sync_every=0)
+        else:
+            # time-limited: check between graphs whether the system is done
+            eng.run(left if left >= 0 else (1 << 62), sync_every=1)
+        res = eng.status(st.slot)
+        done += int(res['steps_done'])
+        elapsed += res['dt_used']
+        dt = res['dt']
+        grow_cells = bool(res['flags'] & FLAG_CELL_OVERFLOW) and eng.cfg.cell_depth < MAX_DEPTH
+        grow_lists = bool(res['flags'] & FLAG_LIST_OVERFLOW) and eng.cfg.list_depth < MAX_LIST_DEPTH
+        if not (grow_cells or grow_lists) or done == max_steps or (max_dt_usable >= 0 and elapsed >= max_dt_usable):
+            break
+        depth = min(MAX_DEPTH, 2 * eng.cfg.cell_depth) if grow_cells else eng.cfg.cell_depth
+        ldepth = min(MAX_LIST_DEPTH, 2 * eng.cfg.list_depth) if grow_lists else eng.cfg.list_depth
+        pop._gcr_cell_depth, pop._gcr_list_depth = depth, ldepth
+        st.params.step = int(res['step'])
+        g.make_engine(st.params, depth, ldepth)
+        g.key = _key(pop, dim, precision, params, depth, ldepth)
+        eng = g.engine
+    steps_done = done
     if mode == 'mt' and steps_done < n_noise:
         # give back the deviates of steps that did not run
         g.rng.set_state(rng_state)
@@ -217,17 +252,12 @@ def SRK2_force_calc(pops, status, sim):
     pop.forces[:] = g.h_frc.numpy()
 
     # write-back, updates.py:249-256
-    status.dt = res['dt']
-    status.dt_used = res['dt_used']
+    status.dt = dt
+    status.dt_used = elapsed
     status.stepnum += steps_done
     status.t += status.dt_used
     status.max_forces_strength = res['max_forces_strength']
     status.update_grid_list_counter = max(
         1, (steps_done + status.update_grid_list_counter) % cfg.n_steps_update_grid_list)
     status.gpu_flags = res['flags']
-    if res['flags'] & FLAG_CELL_OVERFLOW:
-        # cell overflow: deeper cells for the next call (updates.py:257-267)
-        pop._gcr_cell_depth = min(MAX_DEPTH, 2 * g.engine.cfg.cell_depth)
-    if res['flags'] & FLAG_LIST_OVERFLOW:
-        pop._gcr_list_depth = min(MAX_LIST_DEPTH, 2 * g.engine.cfg.list_depth)
     return None

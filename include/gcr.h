@@ -116,7 +116,8 @@ typedef struct {
 typedef struct {
     int64_t max_steps;          /* next_output_step - stepnum (<0: unlimited) */
     double max_dt_usable;       /* next_save_time - t; negative: unlimited (SRK.py:128-129) */
-    double dt;                  /* status.dt: predictor dt of the first step */
+    double dt;                  /* status.dt: predictor dt of the first step (<= 0: keep the
+                                   system's current dt, i.e. carry it over from its last call) */
     const double *noise;        /* injected noise_vec snapshots [noise_steps][n][2*dim],
                                    device memory, or NULL for the Philox stream */
     int64_t noise_steps;

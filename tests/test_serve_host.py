@@ -60,11 +60,12 @@ class FakeEngine:
             v["done"] = d
             v["step"] += d
             relaxing = math.isfinite(v["st"].params.max_dist_per_step)
+            dtmax = v["st"].params.dtmax
             if relaxing:
                 v["relaxed"] += d
-                v["dt"] = v["dt_call"] if v["relaxed"] >= self.relax_needed else 0.1 * v["dt_call"]
+                v["dt"] = dtmax if v["relaxed"] >= self.relax_needed else 0.1 * dtmax
             else:
-                v["dt"] = v["dt_call"]
+                v["dt"] = dtmax
             v["armed"] = 0
 
     def status(self, slot):
@@ -95,12 +96,12 @@ class FakeServer(S.Server):
         return eng
 
 
-def _requests(n, steps, relax=False, obs_every=0, sizes=None):
+def _requests(n, steps, relax=False, obs_every=0, sizes=None, adaptive=True):
     out = []
     for i in range(n):
         nch = (sizes[i] if sizes else 20)
         spec = W.make_system(f"r{i}", 2, nch, 10, 40.0, seed=i)
-        out.append(S.Request(i, spec, steps[i] if np.ndim(steps) else steps, 0.0, obs_every, relax))
+        out.append(S.Request(i, spec, steps[i] if np.ndim(steps) else steps, 0.0, obs_every, relax, adaptive))
     return out
 
 
@@ -120,13 +121,22 @@ def test_every_request_runs_exactly_its_steps_with_observations():
 
 def test_relaxation_comes_first_and_is_counted_apart():
     srv = FakeServer(hbm_budget=1 << 26, chunk=100, relax_needed=250)
-    reqs = _requests(2, 120, relax=True)
+    reqs = _requests(2, 120, relax=True, adaptive=False)
     res = srv.serve(reqs, timeout=30)
     for r in res:
         assert r.relax_steps == 300  # three chunks of 100 until the dt is full
         assert r.steps == 120
     for rq in reqs:
-        assert math.isinf(rq.spec.params.max_dist_per_step)  # handed back to the fixed dt
+        assert math.isinf(rq.spec.params.max_dist_per_step)  # handed over to the fixed dt
+
+
+def test_adaptive_requests_keep_the_adaptive_rule_and_carry_dt():
+    srv = FakeServer(hbm_budget=1 << 26, chunk=50)
+    reqs = _requests(2, 120)
+    res = srv.serve(reqs, timeout=30)
+    assert all(r.steps == 120 and r.relax_steps == 0 for r in res)
+    for rq in reqs:
+        assert rq.spec.params.max_dist_per_step == rq.spec.relax_mdps
 
 
 def test_admission_waits_for_room_and_backfills():
