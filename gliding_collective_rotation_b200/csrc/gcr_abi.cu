@@ -256,7 +256,9 @@ void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, double skin, SysP &
     p.p1 = d.wca_params[1];
     p.shift = d.wca_params[2];
     p.rc2 = d.wca_params[3] * d.wca_params[3];
-    p.rl2 = (d.wca_params[3] + skin) * (d.wca_params[3] + skin);
+    // list radius with a relative margin of 1e-6 in r^2, above the rounding of
+    // the FP32 pair test, so that every pair that test accepts is listed
+    p.rl2 = (d.wca_params[3] + skin) * (d.wca_params[3] + skin) * (1.0 + 1e-6);
     p.half_skin2 = 0.25 * skin * skin;
     p.n_nearby = d.n_nearby;
     p.self_propel = d.self_propel ? 1 : 0;

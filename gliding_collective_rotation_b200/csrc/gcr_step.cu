@@ -133,8 +133,9 @@ __device__ __forceinline__ FT wca_coeff(FT ds, FT p0, FT p1)
 // pos) test every bead against the positions of the last build and raise the
 // system's rebuild flag; the bin, sort and build kernels run for flagged
 // systems and skip the others; the pair kernel clears the flag.  Each list
-// is in cell order (z, y, x of the 3^d cells, bead ids ascending inside a
-// cell), so its sums are taken in a fixed order whatever the batch holds.
+// is kept in ascending bead id, so a bead's pair force is summed over the
+// partners within r_cut in id order: a function of the positions alone,
+// whatever the batch, the skin, the cell grid or the rebuild history.
 // ------------------------------------------------------------------------
 
 // the system takes part in a list build now
@@ -249,7 +250,7 @@ __global__ void __launch_bounds__(512) k_sort(BatchArgs A)
 }
 
 // per bead of a flagged system: every non-excluded bead within r_l in the
-// 3^d cells around it, in cell order; records the positions of the build
+// 3^d cells around it, in ascending id; records the positions of the build
 template <int D, int WHICH>
 __global__ void __launch_bounds__(512) k_build(BatchArgs A)
 {
@@ -313,7 +314,19 @@ __global__ void __launch_bounds__(512) k_build(BatchArgs A)
                             ds += d * d;
                         }
                         if (ds <= p.rl2) {
-                            if (cnt < cap) out[(size_t)cnt * stride] = j;
+                            if (cnt < cap) {
+                                // insert in ascending bead id: the pair sum then
+                                // depends on the positions only, not on when
+                                // or on which cell grid the list was built
+                                int q2 = cnt;
+                                while (q2 > 0) {
+                                    const int prev = out[(size_t)(q2 - 1) * stride];
+                                    if (prev < j) break;
+                                    out[(size_t)q2 * stride] = prev;
+                                    q2--;
+                                }
+                                out[(size_t)q2 * stride] = j;
+                            }
                             cnt++;
                         }
                     }

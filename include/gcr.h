@@ -200,7 +200,7 @@ GCR_API int gcr_cell_assignment(gcr_ctx *ctx, int32_t slot, int32_t *cell_of_bea
  * counterpart in the reference, whose nbor_list gcr_reference_lists gives):
  * counts[n] (device, or NULL) partners per bead; partners[n][partners_depth]
  * (device, or NULL; partners_depth >= the context's list_depth) their bead
- * ids in summation order; build_pos[n][dim] (device, or NULL) the FP64
+ * ids in ascending order (the summation order); build_pos[n][dim] (device, or NULL) the FP64
  * positions the list was built from; *entries (host, or NULL) the total. */
 GCR_API int gcr_neighbour_list(gcr_ctx *ctx, int32_t slot, int32_t *counts, int32_t *partners,
                                int32_t partners_depth, double *build_pos, int64_t *entries);

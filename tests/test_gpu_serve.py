@@ -1,6 +1,7 @@
 """The serving loop on the GPU: a request served in a mix of others, split
-into chunks at other requests' pace, ends bit-for-bit where it ends when run
-alone in one call; its order-parameter series ends at the alone value."""
+into chunks at other requests' pace (its adaptive dt carried from chunk to
+chunk), ends bit-for-bit where it ends when run alone in one call; its
+order-parameter series ends at the alone value."""
 import copy
 
 import numpy as np
@@ -16,10 +17,11 @@ from gliding_collective_rotation_b200.batch import Batch  # noqa: E402
 
 
 def _relaxed(n):
-    """n small sweep systems, relaxed once under the adaptive dt."""
+    """n small sweep systems, relaxed once under the adaptive dt, which
+    they keep (the rule a request's steps follow)."""
     specs = sorted(W.config3(n_systems=64, param_seed=5), key=lambda s: s.n)[:n]
     b = Batch(specs, "mixed")
-    b.relax(max_steps=2000)
+    b.relax(max_steps=2000, adaptive_after=True)
     out = []
     for sp, st, status in zip(specs, b.states, b.statuses()):
         sp = copy.deepcopy(sp)
