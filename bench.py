@@ -244,6 +244,7 @@ def run_gpu(args):
     import torch
     import torch.distributed as dist
     from gliding_collective_rotation_b200.batch import Batch, PlainRunner
+    from gliding_collective_rotation_b200.engine import default_skin
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -260,7 +261,7 @@ def run_gpu(args):
     specs, desc = make_workload(args.workload, rank=rank, scale=args.scale, systems=args.systems)
     for sp in specs:
         sp.params.cell_factor = args.cell_factor
-        sp.params.skin = args.skin
+        sp.params.skin = args.skin if args.skin >= 0 else None
     batch = Batch(specs, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph,
                   ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads, list_depth=args.list_depth or None)
     eng = batch.engine
@@ -415,12 +416,14 @@ def run_gpu(args):
                    "relax_steps": relax_steps, "steps_done": steps_done, "flags": flags,
                    "dt_rule": "adaptive (SRK.py:323-353): dtmax = configured dt, max_dist_per_step of "
                               "config.grid_list_setup", "dt_mean": dt_mean,
-                   "cell_factor": args.cell_factor, "skin": args.skin,
+                   "cell_factor": args.cell_factor,
+                   "skin": specs[0].params.skin if specs[0].params.skin is not None
+                   else default_skin(specs[0].params.wca_params[3]),
                    "steps_per_graph": args.steps_per_graph, "cell_depth": batch.cell_depth,
                    "list_depth": batch.list_depth, "list_mean": list_mean,
                    "list_builds_per_stage": builds_per_stage},
         "e2e": e2e, "roofline": roofline, "clocks": clk,
-        "gpu_launches": 13 * args.steps + 1,
+        "gpu_launches": 15 * args.steps + 1,
     }
     if plain is not None:
         line["plain"] = plain
@@ -482,7 +485,8 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0,
                     help="CTAs per SM of the tile kernels (0: from occupancy, <0: one CTA per tile)")
     ap.add_argument("--block-beads", type=int, default=256)
-    ap.add_argument("--skin", type=float, default=0.3, help="Verlet skin of the neighbour lists")
+    ap.add_argument("--skin", type=float, default=-1.0,
+                    help="Verlet skin of the neighbour lists (<0: 0.2 r_cut + 0.1, within [0.2, 1])")
     ap.add_argument("--list-depth", type=int, default=0, help="neighbour slots per bead (0: default)")
     ap.add_argument("--relax-steps", type=int, default=2000)
     ap.add_argument("--profile-steps", type=int, default=10)

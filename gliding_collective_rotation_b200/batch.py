@@ -19,7 +19,7 @@ import numpy as np
 import torch
 
 from ._lib import FLAG_CELL_OVERFLOW, FLAG_LIST_OVERFLOW, FLAG_NEXT_OVERFLOW
-from .engine import Engine, SystemState, footprint, default_config
+from .engine import Engine, SystemState, default_config, default_skin, footprint
 
 OVERFLOW = FLAG_CELL_OVERFLOW | FLAG_NEXT_OVERFLOW | FLAG_LIST_OVERFLOW
 MAX_DEPTH = 128
@@ -40,7 +40,8 @@ def default_depth(dim, cell_factor):
 def cell_scale(params):
     """GPU cell side over the pair cutoff: (r_cut + skin) * cell_factor / r_cut."""
     rc = float(params.wca_params[3])
-    return max(1.0, params.cell_factor) * (rc + max(0.0, params.skin)) / rc
+    skin = params.skin if params.skin is not None else default_skin(rc)
+    return max(1.0, params.cell_factor) * (rc + max(0.0, skin)) / rc
 
 
 def default_list_depth(dim):

@@ -120,6 +120,7 @@ struct gcr_ctx {
     int *nbr = nullptr;
     int *ncount = nullptr;
     double *xref = nullptr;
+    int *work = nullptr;
     void *xi = nullptr;
     void *fp = nullptr;
     size_t stage_smem = 0;
@@ -292,11 +293,13 @@ int launch_sys(gcr_ctx *c, void *fn)
     return GCR_OK;
 }
 
-// one stage's neighbour lists (flagged systems only): bin, per-cell sort, build
+// one stage's neighbour lists (flagged systems only): plan, bin, per-cell
+// sort, build
 int enqueue_lists(gcr_ctx *c, int which)
 {
     int rc;
     const int bb = c->cfg.block_beads, bc = c->cfg.block_cells;
+    if ((rc = launch(c, c->ks.lists_plan, 1, 1024))) return rc;
     if ((rc = launch(c, which ? c->ks.bin1 : c->ks.bin0, c->grid_bin, bb))) return rc;
     if ((rc = launch(c, c->ks.sort, c->grid_sort, bc))) return rc;
     return launch(c, which ? c->ks.build1 : c->ks.build0, c->grid_build, bb);
@@ -435,6 +438,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     e = e ? e : cudaMalloc(&c->nbr, sizeof(int) * (size_t)cfg.bead_capacity * (size_t)cfg.list_depth);
     e = e ? e : cudaMalloc(&c->ncount, sizeof(int) * (size_t)cfg.bead_capacity);
     e = e ? e : cudaMalloc(&c->xref, sizeof(double) * (size_t)cfg.bead_capacity * cfg.dim);
+    e = e ? e : cudaMalloc(&c->work, sizeof(int) * (size_t)(3 + 3 * (S + 1)));
     e = e ? e : cudaMalloc(&c->xi, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
     e = e ? e : cudaMalloc(&c->fp, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
     e = e ? e : cudaMalloc(&c->chain_starts, sizeof(int32_t) * (cfg.bead_capacity + S));
@@ -448,6 +452,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     cudaMemsetAsync(c->cnt, 0, sizeof(int) * cells_alloc, c->stream);
     cudaMemsetAsync(c->ncell, 0, sizeof(int) * cells_alloc, c->stream);
     cudaMemsetAsync(c->ncount, 0, sizeof(int) * (size_t)cfg.bead_capacity, c->stream);
+    cudaMemsetAsync(c->work, 0, sizeof(int) * (size_t)(3 + 3 * (S + 1)), c->stream);
     c->slots.assign(S, Slot());
     c->hP.assign(S, SysP());
     c->hS.assign(S, SysS());
@@ -470,6 +475,8 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     a.xref = c->xref;
     a.xi = c->xi;
     a.fp = c->fp;
+    a.work = c->work;
+    a.n_slots = (int)S;
     a.list_stride = cfg.bead_capacity;
     a.list_depth = cfg.list_depth;
     a.depth = cfg.cell_depth;
@@ -500,7 +507,8 @@ int gcr_destroy(gcr_ctx *c)
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->topo, c->cnt, c->ncell,
-                    c->items, c->nbr, c->ncount, c->xref, c->xi, c->fp, c->chain_starts, c->d_err, c->d_out};
+                    c->items, c->nbr, c->ncount, c->xref, c->work, c->xi, c->fp, c->chain_starts, c->d_err,
+                    c->d_out};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);

@@ -137,6 +137,42 @@ __device__ __forceinline__ void normal_pair(uint64_t seed, uint32_t bead, int64_
     z1 = rad * s;
 }
 
+// The same Philox block turned into two FP32 deviates (mixed precision):
+// 24-bit uniforms from the top bits of the words the FP64 pair uses, and the
+// Box-Muller transform in FP32.  Normals agree with the FP64 pair to about
+// 1e-6 relative; the largest |z| is sqrt(2 ln 2^24) = 5.77.
+__device__ __forceinline__ void normal_pair_f(uint64_t seed, uint32_t bead, int64_t step, uint32_t stream,
+                                              float &z0, float &z1)
+{
+    uint4 r = philox4x32_10(make_uint4(bead, (uint32_t)((uint64_t)step & 0xffffffffu),
+                                       (uint32_t)((uint64_t)step >> 32), stream),
+                            (uint32_t)(seed & 0xffffffffu), (uint32_t)(seed >> 32));
+    const float two_m24 = 5.9604644775390625e-08f;
+    float u1 = ((float)(r.x >> 8) + 1.0f) * two_m24;
+    float u2 = (float)(r.z >> 8) * two_m24;
+    float rad = sqrtf(-2.0f * logf(u1));
+    float s, c;
+    sincospif(2.0f * u2, &s, &c);
+    z0 = rad * c;
+    z1 = rad * s;
+}
+
+template <int D>
+__device__ __forceinline__ void philox_normals_f(uint64_t seed, uint32_t bead, int64_t step, bool rot,
+                                                 float out[D])
+{
+    float z0, z1;
+    uint32_t s0 = rot ? 2u : 0u;
+    normal_pair_f(seed, bead, step, s0, z0, z1);
+    out[0] = z0;
+    out[1] = z1;
+    if (D == 3) {
+        float z2, z3;
+        normal_pair_f(seed, bead, step, s0 + 1u, z2, z3);
+        out[D - 1] = z2;
+    }
+}
+
 // translational (stream 0,1) or rotational (stream 2,3) deviates of one bead
 template <int D>
 __device__ __forceinline__ void philox_normals(uint64_t seed, uint32_t bead, int64_t step, bool rot,

@@ -25,6 +25,8 @@ struct BatchArgs {
     double *xref;  // positions at the last list build, FP64 [bead][dim]
     void *xi;      // translational noise of the current step per bead, FT [bead][dim]
     void *fp;      // pair force per bead (bead order), FT [bead][dim]
+    int *work;     // flagged systems of the coming list build (k_lists_plan)
+    int n_slots;
     int64_t list_stride;
     int list_depth;
     int depth;
@@ -48,6 +50,7 @@ struct KernelSet {
     void *sys_dt;
     void *sys_end;
     void *sys_mark;  // flag every resident system for a list build
+    void *lists_plan;  // compact the systems that take part in a list build
     size_t (*stage_smem)(int block_beads);  // dynamic shared memory of the stage kernels
 };
 

@@ -97,6 +97,15 @@ __device__ __forceinline__ bool bend(const FT *ti, const FT *tj, FT theta0, FT k
     return true;
 }
 
+// CTAs of 512 threads per SM that the bead kernels are compiled for: the 2D
+// mixed-precision kernels fit in 42 registers a thread (6 CTAs of 256 per
+// SM); the FP64 and 3D kernels keep the registers they need
+template <int D, typename FT>
+constexpr int min_blocks()
+{
+    return (D == 2 && sizeof(FT) == 4) ? 3 : 1;
+}
+
 // ------------------------------------------------------------------------
 // the pair rule forces.WCA (forces.py:13-15): coeff = ds^-4 (p0 - p1 ds^-3)
 // ------------------------------------------------------------------------
@@ -166,17 +175,127 @@ __device__ __forceinline__ bool left_skin(const SysP &p, const BatchArgs &A, int
     return !(dd <= p.half_skin2);
 }
 
+// Work list of a list build: the flagged systems, compacted, with the
+// running sum of their bead tiles and cell tiles.  Layout of A.work:
+//   [0] flagged systems m, [1] their bead tiles, [2] their cell tiles,
+//   then sys[S], bead_prefix[S+1], cell_prefix[S+1] (S = slot count).
+// Built by one CTA before each stage's list kernels, which then visit the
+// tiles of flagged systems only, and leave at once when there are none.
+struct Work {
+    int m, n_bead, n_cell;
+    const int *sys, *bead0, *cell0;
+};
+
+__device__ __forceinline__ Work work_list(const BatchArgs &A)
+{
+    Work w;
+    const int *q = A.work;
+    w.m = q[0];
+    w.n_bead = q[1];
+    w.n_cell = q[2];
+    w.sys = q + 3;
+    w.bead0 = w.sys + A.n_slots;
+    w.cell0 = w.bead0 + A.n_slots + 1;
+    return w;
+}
+
+// the flagged system holding work item i of a prefix (largest k: pre[k] <= i)
+__device__ __forceinline__ int work_owner(const int *pre, int m, int i)
+{
+    int lo = 0, hi = m - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= i)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+// one CTA: compact the systems that take part in a list build now
+__global__ void __launch_bounds__(1024) k_lists_plan(BatchArgs A)
+{
+    __shared__ int sh[3][32];
+    __shared__ int carry[3];
+    int *q = A.work;
+    int *wsys = q + 3, *wb = wsys + A.n_slots, *wc = wb + A.n_slots + 1;
+    if (threadIdx.x < 3) carry[threadIdx.x] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int base = 0; base < A.n_slots; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        int v[3] = {0, 0, 0};
+        if (i < A.n_slots) {
+            const SysP &p = A.P[i];
+            const SysS &st = A.S[i];
+            if (p.calc_wca && st.active && st.rebuild && !(st.flags & kFlagFatal)) {
+                v[0] = 1;
+                v[1] = p.n_bead_tiles;
+                v[2] = p.n_cell_tiles;
+            }
+        }
+        int x[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            x[c] = v[c];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(0xffffffffu, x[c], o);
+                if (lane >= o) x[c] += y;
+            }
+            if (lane == 31) sh[c][wid] = x[c];
+        }
+        __syncthreads();
+        if (wid == 0) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                int y = lane < nw ? sh[c][lane] : 0;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    int z = __shfl_up_sync(0xffffffffu, y, o);
+                    if (lane >= o) y += z;
+                }
+                if (lane < nw) sh[c][lane] = y;  // inclusive prefix of warp totals
+            }
+        }
+        __syncthreads();
+        int ex[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) ex[c] = carry[c] + x[c] - v[c] + (wid > 0 ? sh[c][wid - 1] : 0);
+        if (v[0]) {
+            wsys[ex[0]] = i;
+            wb[ex[0]] = ex[1];
+            wc[ex[0]] = ex[2];
+        }
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) {
+#pragma unroll
+            for (int c = 0; c < 3; c++) carry[c] = ex[c] + v[c];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        q[0] = carry[0];
+        q[1] = carry[1];
+        q[2] = carry[2];
+        wb[carry[0]] = carry[1];
+        wc[carry[0]] = carry[2];
+    }
+}
+
 // bin every bead of a flagged system into its cell (fixed-depth slots)
 template <int D, int WHICH>
 __global__ void __launch_bounds__(512) k_bin(BatchArgs A)
 {
-    const int nt = *A.n_bead_tiles;
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const Tile tl = A.bead_tiles[t];
-        const SysP &p = A.P[tl.sys];
-        SysS &s = A.S[tl.sys];
+    const Work w = work_list(A);
+    for (int t = blockIdx.x; t < w.n_bead; t += gridDim.x) {
+        const int k = work_owner(w.bead0, w.m, t);
+        const int sys = w.sys[k];
+        const SysP &p = A.P[sys];
+        SysS &s = A.S[sys];
         if (!builds(p, s)) continue;
-        const int b = tl.begin + threadIdx.x;
+        const int b = (t - w.bead0[k]) * A.tile_beads + threadIdx.x;
         if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
         const double *X = WHICH == 0 ? p.pos : p.pos1;
         double x[3] = {0.0, 0.0, 0.0};
@@ -197,13 +316,14 @@ __global__ void __launch_bounds__(512) k_bin(BatchArgs A)
 // binning), sort the slot contents by bead id
 __global__ void __launch_bounds__(512) k_sort(BatchArgs A)
 {
-    const int nt = *A.n_cell_tiles;
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const Tile tl = A.cell_tiles[t];
-        const SysP &p = A.P[tl.sys];
-        SysS &s = A.S[tl.sys];
+    const Work w = work_list(A);
+    for (int t = blockIdx.x; t < w.n_cell; t += gridDim.x) {
+        const int k = work_owner(w.cell0, w.m, t);
+        const int sys = w.sys[k];
+        const SysP &p = A.P[sys];
+        SysS &s = A.S[sys];
         if (!builds(p, s)) continue;
-        const int c = tl.begin + threadIdx.x;
+        const int c = (t - w.cell0[k]) * A.tile_cells + threadIdx.x;
         if (c >= p.n_cells || threadIdx.x >= A.tile_cells) continue;
         const int64_t gc = p.cell_off + c;
         int n = A.cnt[gc];
@@ -254,14 +374,16 @@ __global__ void __launch_bounds__(512) k_sort(BatchArgs A)
 template <int D, int WHICH>
 __global__ void __launch_bounds__(512) k_build(BatchArgs A)
 {
-    const int nt = *A.n_bead_tiles;
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const Tile tl = A.bead_tiles[t];
-        const SysP &p = A.P[tl.sys];
-        SysS &s = A.S[tl.sys];
+    const Work w = work_list(A);
+    for (int t = blockIdx.x; t < w.n_bead; t += gridDim.x) {
+        const int k = work_owner(w.bead0, w.m, t);
+        const int sys = w.sys[k];
+        const SysP &p = A.P[sys];
+        SysS &s = A.S[sys];
         if (!builds(p, s)) continue;
-        if (tl.begin == 0 && threadIdx.x == 0) s.list_builds += 1;  // one thread per system and build
-        const int b = tl.begin + threadIdx.x;
+        const int begin = (t - w.bead0[k]) * A.tile_beads;
+        if (begin == 0 && threadIdx.x == 0) s.list_builds += 1;  // one thread per system and build
+        const int b = begin + threadIdx.x;
         if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
         const int n = p.n, nc = p.nc;
         const double *X = WHICH == 0 ? p.pos : p.pos1;
@@ -346,7 +468,7 @@ __global__ void __launch_bounds__(512) k_build(BatchArgs A)
 // min-image separation of the FP64 positions, rounded to FT, then the rule
 // in FT; writes the pair force of every bead to fp[bead]
 template <int D, typename FT, int WHICH>
-__global__ void __launch_bounds__(512) k_pair(BatchArgs A)
+__global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_pair(BatchArgs A)
 {
     const int nt = *A.n_bead_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
@@ -370,8 +492,10 @@ __global__ void __launch_bounds__(512) k_pair(BatchArgs A)
         const FT rc2 = (FT)p.rc2, p0 = (FT)p.p0, p1 = (FT)p.p1, shift = (FT)p.shift;
         FT F[3] = {FT(0), FT(0), FT(0)};
         bool bad = false;
+        int j_next = cnt > 0 ? nb[0] : 0;
         for (int k = 0; k < cnt; k++) {
-            const int j = nb[(size_t)k * stride];
+            const int j = j_next;  // the next index is loaded ahead of this pair's positions
+            if (k + 1 < cnt) j_next = nb[(size_t)(k + 1) * stride];
             if ((unsigned)j >= (unsigned)n) {
                 bad = true;
                 continue;
@@ -411,6 +535,8 @@ __device__ __forceinline__ void noise_trans(const SysP &p, const SysS &s, int b,
         const double *q = s.noise + ((size_t)s.steps_done * p.n + b) * 2 * D;
 #pragma unroll
         for (int i = 0; i < D; i++) xi[i] = (FT)q[i];
+    } else if constexpr (sizeof(FT) == 4) {
+        philox_normals_f<D>(p.seed, (uint32_t)b, s.step, false, xi);
     } else {
         double z[D];
         philox_normals<D>(p.seed, (uint32_t)b, s.step, false, z);
@@ -426,6 +552,8 @@ __device__ __forceinline__ void noise_rot(const SysP &p, const SysS &s, int b, F
         const double *q = s.noise + ((size_t)s.steps_done * p.n + b) * 2 * D + D;
 #pragma unroll
         for (int i = 0; i < D; i++) xi[i] = (FT)q[i];
+    } else if constexpr (sizeof(FT) == 4) {
+        philox_normals_f<D>(p.seed, (uint32_t)b, s.step, true, xi);
     } else {
         double z[D];
         philox_normals<D>(p.seed, (uint32_t)b, s.step, true, z);
@@ -455,7 +583,7 @@ __device__ __forceinline__ double srk_update(double x, double dt_eff, double s2,
 // stage and update kernels
 // ------------------------------------------------------------------------
 template <int D, typename FT, int STAGE>
-__global__ void __launch_bounds__(512) k_stage(BatchArgs A)
+__global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long sh_bits[16];
@@ -688,7 +816,7 @@ __global__ void __launch_bounds__(512) k_stage(BatchArgs A)
 }
 
 template <int D, typename FT>
-__global__ void __launch_bounds__(512) k_update(BatchArgs A)
+__global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A)
 {
     const int nt = *A.n_bead_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
@@ -867,6 +995,7 @@ KernelSet kernel_set(int dim, int precision)
     k.sys_dt = (void *)k_sys_dt;
     k.sys_end = (void *)k_sys_end;
     k.sys_mark = (void *)k_sys_mark;
+    k.lists_plan = (void *)k_lists_plan;
     return k;
 }
 

@@ -20,6 +20,13 @@ from ._lib import Call, Config, GcrError, Status, SystemBuffers, SystemDesc, che
 PRECISIONS = {"fp64": _lib.GCR_FP64, "mixed": _lib.GCR_MIXED}
 
 
+def default_skin(r_cut):
+    """Verlet skin for a pair cutoff: 0.2 r_cut + 0.1, within [0.2, 1].  A
+    wider skin means rarer list builds but longer lists; measured on B200 the
+    best was 0.3 for r_cut = 1 (WCA sweep) and 0.5 for r_cut = 2.23 (LJ)."""
+    return min(1.0, max(0.2, 0.2 * float(r_cut) + 0.1))
+
+
 @dataclass
 class SystemParams:
     """One system's parameters, packed the way the reference packs them.
@@ -45,7 +52,7 @@ class SystemParams:
     seed: int = 0
     step: int = 0
     cell_factor: float = 1.0
-    skin: float = 0.3            # Verlet skin of the neighbour list (length units of the box)
+    skin: float | None = None    # Verlet skin of the neighbour list; None: default_skin(r_cut)
 
     def desc(self, n_beads, n_chains):
         d = SystemDesc()
@@ -62,7 +69,7 @@ class SystemParams:
         d.dtmax, d.max_dist_per_step, d.rk_cheat = float(self.dtmax), float(self.max_dist_per_step), \
             float(self.rk_cheat)
         d.seed, d.step, d.cell_factor = int(self.seed) & (2 ** 64 - 1), int(self.step), float(self.cell_factor)
-        d.skin = float(self.skin)
+        d.skin = float(self.skin if self.skin is not None else default_skin(self.wca_params[3]))
         return d
 
 

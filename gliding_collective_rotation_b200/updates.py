@@ -106,7 +106,7 @@ class _GpuPop:
 
 def _key(pop, dim, precision, params, depth, ldepth):
     return (pop.total_pop, len(pop.rest_lengths), dim, precision, float(params.L), float(params.wca_params[3]),
-            float(params.cell_factor), float(params.skin), depth, ldepth, bool(params.calc_wca))
+            float(params.cell_factor), float(params.skin if params.skin is not None else -1.0), depth, ldepth, bool(params.calc_wca))
 
 
 def _gpu_state(pop, sim, dim, precision, params):
@@ -166,7 +166,7 @@ def SRK2_force_calc(pops, status, sim):
         calc_springs=calc_springs, calc_wca=calc_wca, self_propel=self_propel, dtmax=float(status.dtmax),
         max_dist_per_step=float(cfg.max_dist_per_step), rk_cheat=float(cfg.RK_cheat_factor), seed=seed,
         step=int(status.stepnum), cell_factor=float(sim.get('gpu_cell_factor', 1.0)),
-        skin=float(sim.get('gpu_skin', 0.3)))
+        skin=sim.get('gpu_skin', None))
     g = _gpu_state(pop, sim, dim, precision, params)
     st, eng = g.state, g.engine
 

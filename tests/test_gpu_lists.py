@@ -21,7 +21,7 @@ pytestmark = pytest.mark.gpu
 
 from gliding_collective_rotation_b200 import workloads as W  # noqa: E402
 from gliding_collective_rotation_b200.batch import Batch  # noqa: E402
-from gliding_collective_rotation_b200.engine import SystemParams  # noqa: E402
+from gliding_collective_rotation_b200.engine import SystemParams, default_skin  # noqa: E402
 from tests.golden_io import load, min_image  # noqa: E402
 
 
@@ -61,7 +61,7 @@ def _check_lists(b, spec):
     counts, part, xb = counts.cpu().numpy(), part.cpu().numpy(), xb.cpu().numpy()
     assert total == counts.sum() and counts.max() <= eng.cfg.list_depth
     p = spec.params
-    rl = p.wca_params[3] + p.skin
+    rl = p.wca_params[3] + (p.skin if p.skin is not None else default_skin(p.wca_params[3]))
     want, edge = _brute_force(xb, np.asarray(spec.chain_id), p.L, rl, p.n_nearby)
     for i in range(len(xb)):
         got = part[i, :counts[i]].tolist()
