@@ -484,7 +484,7 @@ def main():
     ap.add_argument("--steps-per-graph", type=int, default=10)
     ap.add_argument("--ctas-per-sm", type=int, default=0,
                     help="CTAs per SM of the tile kernels (0: from occupancy, <0: one CTA per tile)")
-    ap.add_argument("--block-beads", type=int, default=256)
+    ap.add_argument("--block-beads", type=int, default=128)
     ap.add_argument("--skin", type=float, default=-1.0,
                     help="Verlet skin of the neighbour lists (<0: 0.2 r_cut + 0.1, within [0.2, 1])")
     ap.add_argument("--list-depth", type=int, default=0, help="neighbour slots per bead (0: default)")

@@ -85,7 +85,7 @@ class Batch:
     """Systems of one dimension and precision resident in one context."""
 
     def __init__(self, specs, precision="mixed", device=None, steps_per_graph=10, cell_depth=None,
-                 block_beads=256, block_cells=256, stream=None, ctas_per_sm=0, list_depth=None):
+                 block_beads=128, block_cells=256, stream=None, ctas_per_sm=0, list_depth=None):
         if not specs:
             raise ValueError("empty batch")
         dims = {s.dim for s in specs}
