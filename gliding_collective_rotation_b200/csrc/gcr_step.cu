@@ -73,6 +73,18 @@ size_t stage_smem_bytes(int TB)
            (size_t)(TB + 2) * 2 * D * sizeof(FT) + (size_t)(TB + 4) + 16;
 }
 
+// 1/sqrt(x): FP64 exactly as written in the reference; FP32 (mixed path) by
+// the hardware reciprocal square root (at most 2 ulp), accurate enough for
+// forces that are FP32 anyway
+template <typename FT>
+__device__ __forceinline__ FT inv_sqrt(FT x)
+{
+    if constexpr (sizeof(FT) == 4)
+        return rsqrtf(x);
+    else
+        return 1.0 / sqrt(x);
+}
+
 // bend at a bead with forward tangent ti (its own bond) and backward tangent
 // tj (the previous bond); false when the tangents are aligned
 template <int D, typename FT>
@@ -88,7 +100,7 @@ __device__ __forceinline__ bool bend(const FT *ti, const FT *tj, FT theta0, FT k
         FT sg = (FT)((cr > FT(0)) - (cr < FT(0)));
         phi += theta0 * sg;
     }
-    phi *= kappa / sqrt(FT(1) - c * c);
+    phi *= kappa * inv_sqrt<FT>(FT(1) - c * c);
 #pragma unroll
     for (int i = 0; i < D; i++) {
         fwd[i] = phi * (c * tj[i] - ti[i]);
@@ -123,7 +135,7 @@ __device__ __forceinline__ FT wca_coeff(FT ds, FT p0, FT p1)
             return (float)c;
         }
         // ds**-4 (p0 - p1 ds**-3) from one correctly rounded reciprocal
-        float inv = __frcp_rn(ds);
+        float inv = __fdividef(1.0f, ds);  // at most 2 ulp
         float i2 = inv * inv;
         return (i2 * i2) * (p0 - p1 * (i2 * inv));
     } else {
@@ -634,7 +646,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                     }
                     if (r2 != FT(0)) {
                         const FT a = (FT)__ldg(p.rest + __ldg(p.chain + base + k));
-                        FT inv = FT(1) / sqrt(r2);
+                        FT inv = inv_sqrt<FT>(r2);
                         f = kspring * (a * inv - FT(1));
 #pragma unroll
                         for (int i = 0; i < D; i++) tt[i] = d[i] * inv;
@@ -723,7 +735,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
 #pragma unroll
                         for (int i = 0; i < D; i++) c += ti[i] * tj[i];
                         if (FT(-1) < c && c < FT(1)) {
-                            FT coeff = FT(1) / sqrt(FT(2) * (FT(1) + c));
+                            FT coeff = inv_sqrt<FT>(FT(2) * (FT(1) + c));
 #pragma unroll
                             for (int i = 0; i < D; i++) tg[i] = coeff * (ti[i] + tj[i]);
                         } else {
