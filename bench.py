@@ -473,7 +473,7 @@ def run_serve(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="gcr", choices=["gcr", "reference"])
     ap.add_argument("--workload", default="sweep", choices=["sweep", "large", "config1", "config5", "serve"])
