@@ -441,6 +441,67 @@ def run_gpu(args):
 # serving: a Poisson trace through the continuous-batching server
 # --------------------------------------------------------------------------
 
+# --------------------------------------------------------------------------
+# precision: the mixed path against the FP64 path of the same kernels
+# --------------------------------------------------------------------------
+
+def run_precision_report(args):
+    """Both precisions from one relaxed FP64 state, same Philox seeds and
+    the same dt rule: the relative force error after one step and the
+    position divergence over `--precision-report` steps."""
+    import torch
+    from gliding_collective_rotation_b200.batch import Batch
+
+    torch.cuda.set_device(0)
+    specs, desc = make_workload(args.workload, scale=args.scale, systems=args.systems)
+    dim = specs[0].dim
+    base = Batch(specs, precision="fp64")
+    relax_steps = base.relax(max_steps=args.relax_steps, adaptive_after=True)
+    sts = base.statuses()
+    dt0 = [s["dt"] for s in sts]
+    for sp, st, status in zip(specs, base.states, sts):
+        # the relaxed state and the step counter (Philox key) both runs start from
+        sp.pos = st.pos.cpu().numpy().copy()
+        sp.tangent = st.tangent.cpu().numpy().copy()
+        sp.params.step = status["step"]
+    # cells and lists as deep as the relaxed run needed, with a margin
+    depths = dict(cell_depth=min(128, 2 * base.cell_depth), list_depth=min(1024, 2 * base.list_depth))
+    base.close()
+    runs = {prec: Batch(specs, precision=prec, **depths) for prec in ("fp64", "mixed")}
+    L = np.array([sp.params.L for sp in specs])
+    report = {"checkpoints": []}
+    done = 0
+    marks = sorted({1, *[m for m in (10, 100, 1000, 5000, args.precision_report) if m <= args.precision_report]})
+    for m in marks:
+        for prec, b in runs.items():
+            b.engine.call_begin_many([st.slot for st in b.states], m - done, dt0 if done == 0 else 0.0)
+            b.run(m - done)
+            b.engine.synchronize()
+        done = m
+        err, rel_f = 0.0, None
+        num = den = 0.0
+        for i, (s64, s32) in enumerate(zip(runs["fp64"].states, runs["mixed"].states)):
+            d = (s32.pos - s64.pos).cpu().numpy()
+            d -= L[i] * np.round(d / L[i])
+            err = max(err, float(np.abs(d).max()) / L[i])
+            if m == 1:
+                f64 = s64.forces.cpu().numpy()
+                f32 = s32.forces.double().cpu().numpy()
+                num += float(((f32 - f64) ** 2).sum())
+                den += float((f64 ** 2).sum())
+        row = {"steps": m, "max_pos_err_over_L": err}
+        if m == 1:
+            row["force_rel_l2_err"] = (num / den) ** 0.5 if den > 0 else 0.0
+        flags = sorted({s["flags"] for b in runs.values() for s in b.statuses()})
+        row["flags"] = flags
+        report["checkpoints"].append(row)
+    for b in runs.values():
+        b.close()
+    line = {"metric": "mixed vs FP64 error", "workload": desc, "dim": dim, "relax_steps": relax_steps,
+            "dt_rule": "adaptive (SRK.py:323-353), dtmax = configured dt", **report}
+    print(json.dumps(line), flush=True)
+
+
 def run_serve(args):
     import torch
     from gliding_collective_rotation_b200 import serve as S
@@ -497,6 +558,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--cpu-systems", type=int, default=4)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--precision-report", type=int, default=0,
+                    help="report mixed vs FP64 error over this many steps instead of timing")
     ap.add_argument("--requests", type=int, default=64, help="serve: requests in the trace")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate per second")
     ap.add_argument("--max-beads", type=float, default=2e5, help="serve: largest request")
@@ -509,6 +572,9 @@ def main():
     args = ap.parse_args()
     if args.workload == "serve" and args.impl == "gcr":
         run_serve(args)
+        return
+    if args.precision_report > 0 and args.impl == "gcr":
+        run_precision_report(args)
         return
     if args.warmup < 3:
         args.warmup = 3
