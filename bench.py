@@ -468,28 +468,41 @@ def run_precision_report(args):
     depths = dict(cell_depth=min(128, 2 * base.cell_depth), list_depth=min(1024, 2 * base.list_depth))
     base.close()
     runs = {prec: Batch(specs, precision=prec, **depths) for prec in ("fp64", "mixed")}
+    # control: FP64 again with every position moved by about one ulp; its
+    # divergence is the growth of any perturbation in these systems
+    ctl = Batch(specs, precision="fp64", **depths)
+    rng = np.random.default_rng(1)
+    for st, sp in zip(ctl.states, specs):
+        ulp = np.spacing(sp.params.L)
+        st.pos.add_(torch.from_numpy(rng.choice([-ulp, ulp], size=tuple(st.pos.shape))).to(st.pos.device))
+        st.pos.remainder_(sp.params.L)
+    runs["fp64_ulp"] = ctl
     L = np.array([sp.params.L for sp in specs])
     report = {"checkpoints": []}
     done = 0
     marks = sorted({1, *[m for m in (10, 100, 1000, 5000, args.precision_report) if m <= args.precision_report]})
+    for b in runs.values():
+        b._carry_dt = list(dt0)  # the first call starts from the relaxed run's dt
     for m in marks:
         for prec, b in runs.items():
-            b.engine.call_begin_many([st.slot for st in b.states], m - done, dt0 if done == 0 else 0.0)
-            b.run(m - done)
+            b.run_checked(m - done)  # regrows cells or lists if the run needs them
             b.engine.synchronize()
         done = m
-        err, rel_f = 0.0, None
+        err, err_ctl = 0.0, 0.0
         num = den = 0.0
-        for i, (s64, s32) in enumerate(zip(runs["fp64"].states, runs["mixed"].states)):
+        for i, (s64, s32, sc) in enumerate(zip(runs["fp64"].states, runs["mixed"].states, runs["fp64_ulp"].states)):
             d = (s32.pos - s64.pos).cpu().numpy()
             d -= L[i] * np.round(d / L[i])
             err = max(err, float(np.abs(d).max()) / L[i])
+            d = (sc.pos - s64.pos).cpu().numpy()
+            d -= L[i] * np.round(d / L[i])
+            err_ctl = max(err_ctl, float(np.abs(d).max()) / L[i])
             if m == 1:
                 f64 = s64.forces.cpu().numpy()
                 f32 = s32.forces.double().cpu().numpy()
                 num += float(((f32 - f64) ** 2).sum())
                 den += float((f64 ** 2).sum())
-        row = {"steps": m, "max_pos_err_over_L": err}
+        row = {"steps": m, "max_pos_err_over_L": err, "fp64_ulp_control_over_L": err_ctl}
         if m == 1:
             row["force_rel_l2_err"] = (num / den) ** 0.5 if den > 0 else 0.0
         flags = sorted({s["flags"] for b in runs.values() for s in b.statuses()})

