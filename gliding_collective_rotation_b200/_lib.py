@@ -81,6 +81,9 @@ SIGNATURES = {
     "gcr_reference_lists": (C.c_int, [C.c_void_p, C.c_int32, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
                                       C.c_int64, C.c_void_p, C.c_int64, C.c_int32]),
     "gcr_cell_assignment": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.POINTER(C.c_int32)]),
+    "gcr_chain_frames": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p]),
+    "gcr_pair_correlation": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_double, C.POINTER(C.c_double),
+                                       C.c_int32, C.POINTER(C.c_int32)]),
     "gcr_neighbour_list": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p,
                                      C.POINTER(C.c_int64)]),
     "gcr_philox_noise": (C.c_int, [C.c_int32, C.c_uint64, C.c_int64, C.c_int64, C.c_int32, C.c_int32,

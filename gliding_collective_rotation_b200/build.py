@@ -17,7 +17,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgcr.so")
-SOURCES = ["gcr_step.cu", "gcr_lists.cu", "gcr_abi.cu", "gcr_noalloc.cu"]
+SOURCES = ["gcr_step.cu", "gcr_lists.cu", "gcr_abi.cu", "gcr_noalloc.cu", "gcr_observables.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibility=hidden",
          "--expt-relaxed-constexpr"]

@@ -878,6 +878,75 @@ int gcr_neighbour_list(gcr_ctx *c, int32_t slot, int32_t *counts, int32_t *partn
     return GCR_OK;
 }
 
+int gcr_chain_frames(gcr_ctx *c, int32_t slot, double *com, double *phi)
+{
+    if (!valid_slot(c, slot)) return fail(GCR_ERR_BAD_ARG, "invalid slot");
+    const Slot &sl = c->slots[slot];
+    GCR_CUDA(launch_chain_frames(c->cfg.dim, c->cfg.precision, c->hP[slot], c->chain_starts + sl.chain_off, com, phi,
+                                 c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    return GCR_OK;
+}
+
+int gcr_pair_correlation(gcr_ctx *c, int32_t slot, int32_t kind, double binsize, double *out, int32_t max_rows,
+                         int32_t *n_rows)
+{
+    if (!valid_slot(c, slot) || !out || !n_rows) return fail(GCR_ERR_BAD_ARG, "invalid slot or output");
+    if (c->cfg.dim != 2) return fail(GCR_ERR_BAD_ARG, "the pair correlations are defined for 2D systems");
+    if (kind < 0 || kind > 2) return fail(GCR_ERR_BAD_ARG, "kind must be 0 (g(r)), 1 (Cvv) or 2 (Cnn)");
+    if (!(binsize > 0.0) || !std::isfinite(binsize)) return fail(GCR_ERR_BAD_ARG, "binsize must be positive");
+    const SysP &p = c->hP[slot];
+    // bins of np.arange(0, int(L/2) * sqrt(2), binsize)
+    const double stop = (double)(int64_t)(p.L / 2.0) * std::sqrt(2.0);
+    const int64_t n_bins = (int64_t)std::ceil(stop / binsize);
+    if (n_bins < 1 || n_bins > 12000) return fail(GCR_ERR_BAD_ARG, "binsize gives more than 12000 bins");
+    const int nc = p.n_chains;
+    if (kind != 0 && (int64_t)nc * (nc - 1) > ((int64_t)1 << 31))
+        return fail(GCR_ERR_BAD_ARG, "Cvv / Cnn are limited to about 46000 chains (fixed-point sums)");
+    double *com = nullptr, *phi = nullptr;
+    unsigned long long *hist = nullptr;
+    // analysis call, not the step: its scratch is allocated here and freed below
+    cudaError_t e = cudaMalloc(&com, sizeof(double) * 2 * (size_t)nc);
+    if (e == cudaSuccess) e = cudaMalloc(&phi, sizeof(double) * 2 * (size_t)nc);
+    if (e == cudaSuccess) e = cudaMalloc(&hist, sizeof(unsigned long long) * 2 * (size_t)n_bins);
+    if (e == cudaSuccess) e = cudaMemsetAsync(hist, 0, sizeof(unsigned long long) * 2 * (size_t)n_bins, c->stream);
+    if (e == cudaSuccess)
+        e = launch_chain_frames(2, c->cfg.precision, p, c->chain_starts + c->slots[slot].chain_off, com, phi, c->stream);
+    if (e == cudaSuccess)
+        e = launch_pair_corr(com, phi, nc, p.L, binsize, (int)n_bins, kind, hist, hist + n_bins, c->sm_count, c->stream);
+    std::vector<unsigned long long> h((size_t)(2 * n_bins));
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h.data(), hist, sizeof(unsigned long long) * 2 * (size_t)n_bins, cudaMemcpyDeviceToHost,
+                            c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(com);
+    cudaFree(phi);
+    cudaFree(hist);
+    if (e != cudaSuccess) return fail(GCR_ERR_CUDA, std::string("pair correlation: ") + cudaGetErrorString(e));
+    // normalisation of correlation_func (analysis.py:229-237), rows with r < L/2
+    double total = 0.0;
+    for (int64_t b = 0; b < n_bins; b++) total += (double)h[b];
+    const double density = total / (p.L * p.L);
+    int32_t rows = 0;
+    for (int64_t b = 0; b < n_bins; b++) {
+        const double r = (double)b * binsize;
+        if (!(r < p.L / 2.0)) continue;
+        if (rows >= max_rows) return fail(GCR_ERR_CAPACITY, "out has fewer rows than the correlation");
+        double v;
+        if (kind == 0) {
+            v = (double)h[b] / (density * 2.0 * M_PI * binsize * (r + binsize / 2.0));
+        } else {
+            const double sum = (double)(long long)h[n_bins + b] / 4294967296.0;
+            v = sum / (double)std::max<unsigned long long>(h[b], 1ull);
+        }
+        out[2 * rows] = r;
+        out[2 * rows + 1] = v;
+        rows++;
+    }
+    *n_rows = rows;
+    return GCR_OK;
+}
+
 int gcr_philox_noise(int32_t dim, uint64_t seed, int64_t step, int64_t n, int32_t do_trans, int32_t do_rot,
                      double *out, void *cuda_stream)
 {

@@ -71,6 +71,12 @@ cudaError_t launch_cell_assignment(int dim, const SysP &p, int32_t *cell_of_bead
 cudaError_t launch_export_list(const int *nbr, const int *ncount, int64_t stride, int list_depth, int n,
                                int32_t *counts, int32_t *partners, int partners_depth, unsigned long long *total,
                                cudaStream_t st);
+// gcr_observables.cu
+cudaError_t launch_chain_frames(int dim, int precision, const SysP &p, const int32_t *chain_start, double *com,
+                                double *phi, cudaStream_t st);
+cudaError_t launch_pair_corr(const double *com, const double *phi, int n_chains, double L, double binsize, int n_bins,
+                             int kind, unsigned long long *counts, unsigned long long *sums, int sm_count,
+                             cudaStream_t st);
 cudaError_t launch_philox_noise(int dim, uint64_t seed, int64_t step, int64_t n, int do_trans,
                                 int do_rot, double *out, cudaStream_t st);
 

@@ -196,6 +196,21 @@ GCR_API int gcr_reference_lists(gcr_ctx *ctx, int32_t slot, int64_t n_grid, int6
 /* The GPU cell table of one system after binning its current positions:
  * cell index per bead (int32 [n], device) and the grid side (host). */
 GCR_API int gcr_cell_assignment(gcr_ctx *ctx, int32_t slot, int32_t *cell_of_bead, int32_t *n_cells_side);
+/* Per-chain frames of a resident system: com[n_chains][dim] (device, or
+ * NULL) the chain centre exactly as analysis.chain_COM computes it
+ * (analysis.py:288-292: the head plus the summed separations head - x_i,
+ * wrapped); phi[n_chains][2] (device, or NULL) the mean chain angle of
+ * output_methods.calc_avg_phi_chain (output_methods.py:492-510) with n-fold
+ * symmetry 1 and 2 (azimuth of the tangents' x, y components). */
+GCR_API int gcr_chain_frames(gcr_ctx *ctx, int32_t slot, double *com, double *phi);
+/* Pair correlation over chain centres, analysis.correlation_func
+ * (analysis.py:203-241) with the pair function of g_of_r (kind 0, norm
+ * 'all'), Cvv (1) or Cnn (2, norm 'bin'), analysis.py:243-275: bins of
+ * `binsize` over [0, int(L/2) sqrt(2)) (at most 12000 bins), rows (r, value)
+ * with r < L/2 written to out[max_rows][2] (host); *n_rows their number.
+ * 2D systems. */
+GCR_API int gcr_pair_correlation(gcr_ctx *ctx, int32_t slot, int32_t kind, double binsize, double *out,
+                                 int32_t max_rows, int32_t *n_rows);
 /* The neighbour list of a resident system as of its last build (no
  * counterpart in the reference, whose nbor_list gcr_reference_lists gives):
  * counts[n] (device, or NULL) partners per bead; partners[n][partners_depth]
