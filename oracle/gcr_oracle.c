@@ -12,6 +12,7 @@
  *   inbounds_diff              forces.py:44-55
  *   central_pair_force         forces.py:57-145 (WCA rule, no active sliding)
  *   self_propel                forces.py:206-224
+ *   project_updates_for_rigid_rod  updates.py:347-499
  *   calc_chain_spring_forces   forces.py:285-403 (Hookean branch)
  *   update_grid_list_mini      updates.py:502-522
  *   update_grid_list           updates.py:525-583 (overwrite / append modes)
@@ -265,7 +266,7 @@ typedef struct {
     double wca[4];          /* populations.py:48-58 */
     double active[3];       /* populations.py:355-358 */
     double D, Dr, radius;
-    double rigid_rod;       /* must be 0: rigid-rod projection is not restated */
+    double rigid_rod;       /* rigid_rod_projection_factor (populations.py:325-329) */
     int64_t n_nearby;
     int64_t longest_chain_length;
     double grid_factor;
@@ -765,6 +766,121 @@ GCRO_EXPORT int gcro_chunk_chain(int64_t n_threads, int64_t total, const int64_t
 /* SRK.SRK_jit (SRK.py:13-484), SRK2, one population                   */
 /* ------------------------------------------------------------------ */
 
+/* updates.project_updates_for_rigid_rod (updates.py:347-499) on one
+ * thread's chunk of n beads (chains are contiguous, sorted bead ranges, as
+ * the reference's phonebook lists them): each chain's update (forces over
+ * radius plus noise) is blended with the translation and rotation a rigid
+ * rod of the chain's rest length would see, and the chain's current
+ * deviation from that rod is removed.  rtn = (prev + update) mod L.  The
+ * arithmetic follows the reference expression by expression, including its
+ * 2D per-component torque and its 3D rotation term, which carries no
+ * distance factor.  A one-bead chain in 3D (moment of inertia 0) gets no
+ * rotation term; the reference divides by zero there. */
+static void project_rigid(double *rtn, const double *prev, const double *F, const double *noise, int64_t n,
+                          const int64_t *chain_id, const double *rest_lengths, double pf, double L, double dt,
+                          double D, double radius, int dim, double *upd, double *ool, double *dist)
+{
+    const double half = 0.5 * L;
+    const double dt_over_r = dt / radius;
+    const double s2 = sqrt(2.0 * D * dt);
+    int64_t b0 = 0;
+    while (b0 < n) {
+        int64_t b1 = b0 + 1;
+        while (b1 < n && chain_id[b1] == chain_id[b0]) b1++;
+        const int64_t len = b1 - b0;
+        const double rest = rest_lengths[chain_id[b0]];
+        const double half_clm1 = (double)(len - 1) / 2.0;
+        double inertia = 0.0;
+        for (int64_t k = 0; k < len; k++) dist[k] = rest * ((double)k - half_clm1);
+        for (int64_t k = 0; k < len; k++)
+            for (int i = 0; i < dim; i++) inertia += dist[k] * dist[k];
+        for (int64_t k = 0; k < len; k++)
+            for (int i = 0; i < dim; i++) {
+                double u = dt_over_r * F[(b0 + k) * dim + i];
+                if (s2 != 0.0) u += s2 * noise[(b0 + k) * 2 * dim + i];
+                upd[k * dim + i] = u;
+            }
+        double mean[3] = {0.0, 0.0, 0.0}, com[3] = {0.0, 0.0, 0.0}, rh[3] = {0.0, 0.0, 0.0};
+        for (int64_t k = 0; k < len; k++)
+            for (int i = 0; i < dim; i++) mean[i] += upd[k * dim + i];
+        for (int i = 0; i < dim; i++) mean[i] /= (double)len;
+        double r_mag = 0.0;
+        for (int64_t k = 0; k < len; k++)
+            for (int i = 0; i < dim; i++) {
+                double sep = prev[(b0 + k) * dim + i] - prev[b0 * dim + i];
+                if (sep < -half)
+                    sep += L;
+                else if (sep > half)
+                    sep -= L;
+                com[i] += sep;
+                if (k == len - 1) {
+                    rh[i] = sep;
+                    r_mag += sep * sep;
+                }
+            }
+        for (int i = 0; i < dim; i++) com[i] = py_mod(prev[b0 * dim + i] + com[i] / (double)len, L);
+        if (r_mag > 0) {
+            r_mag = sqrt(r_mag);
+            for (int i = 0; i < dim; i++) rh[i] /= r_mag;
+        }
+        for (int64_t k = 0; k < len; k++)
+            for (int i = 0; i < dim; i++) {
+                double sep = prev[(b0 + k) * dim + i] - (com[i] + rh[i] * dist[k]);
+                if (sep < -half)
+                    sep += L;
+                else if (sep >= half)
+                    sep -= L;
+                ool[k * dim + i] = sep;
+            }
+        const double keep = 1. - pf;
+        if (dim == 2) {
+            double tq[2] = {0.0, 0.0};
+            for (int64_t k = 0; k < len; k++)
+                for (int i = 0; i < 2; i++) tq[i] += (double)(2 * i - 1) * rh[1 - i] * upd[k * 2 + i] * dist[k];
+            if (inertia != 0)
+                for (int i = 0; i < 2; i++) tq[i] /= inertia;
+            for (int64_t k = 0; k < len; k++)
+                for (int i = 0; i < 2; i++) {
+                    double u = upd[k * 2 + i] * keep;
+                    u += pf * (-ool[k * 2 + i] + mean[i] + (tq[i] * dist[k] * (double)(2 * i - 1) * rh[1 - i]));
+                    rtn[(b0 + k) * 2 + i] = py_mod(prev[(b0 + k) * 2 + i] + u, L);
+                }
+        } else {
+            double tq[3] = {0.0, 0.0, 0.0};
+            for (int64_t k = 0; k < len; k++) {
+                const double *u = upd + k * 3;
+                tq[0] += rh[1] * u[2] - rh[2] * u[1];
+                tq[1] += rh[2] * u[0] - rh[0] * u[2];
+                tq[2] += rh[0] * u[1] - rh[1] * u[0];
+            }
+            for (int i = 0; i < 3; i++) tq[i] = r_mag * tq[i];
+            const double q = inertia != 0 ? r_mag / inertia : 0.0;
+            double rot[3];
+            rot[0] = q * (tq[1] * rh[2] - tq[2] * rh[1]);
+            rot[1] = q * (tq[2] * rh[0] - tq[0] * rh[2]);
+            rot[2] = q * (tq[0] * rh[1] - tq[1] * rh[0]);
+            for (int64_t k = 0; k < len; k++)
+                for (int i = 0; i < 3; i++) {
+                    double u = upd[k * 3 + i] * keep;
+                    u += pf * (-ool[k * 3 + i] + mean[i] + rot[i]);
+                    rtn[(b0 + k) * 3 + i] = py_mod(prev[(b0 + k) * 3 + i] + u, L);
+                }
+        }
+        b0 = b1;
+    }
+}
+
+/* the projection on its own, for the golden vectors of its direct calls */
+GCRO_EXPORT void gcro_project_rigid(double *rtn, const double *prev, const double *F, const double *noise, int64_t n,
+                                    const int64_t *chain_id, const double *rest_lengths, double pf, double L,
+                                    double dt, double D, double radius, int dim)
+{
+    double *scratch = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1) * 7);
+    project_rigid(rtn, prev, F, noise, n, chain_id, rest_lengths, pf, L, dt, D, radius, dim, scratch,
+                  scratch + 3 * (n > 0 ? n : 1), scratch + 6 * (n > 0 ? n : 1));
+    free(scratch);
+}
+
 static double draw_normal(gcro_state *st, int tid)
 {
     return gcro_mt_normal(&st->mt[tid]);
@@ -776,7 +892,8 @@ GCRO_EXPORT int gcro_srk2_run(const gcro_params *p, gcro_state *st, gcro_result 
     const int64_t N = p->n_beads;
     const double L = p->L;
     int T = p->n_threads > 0 ? p->n_threads : 1;
-    if (p->rigid_rod != 0.0 && p->longest_chain_length > 2) return -1;
+    /* SRK.py:364: the projection replaces the plain update */
+    const int rigid = p->rigid_rod != 0.0 && p->longest_chain_length > 2;
 
     /* chunk boundaries: chain-aligned (updates.py:192-199, 323-344) */
     int64_t *bounds = (int64_t *)malloc(sizeof(int64_t) * (T + 1));
@@ -826,6 +943,7 @@ GCRO_EXPORT int gcro_srk2_run(const gcro_params *p, gcro_state *st, gcro_result 
         double dt = p->dt;
         double dt_for_update = dt;
         int64_t steps_until = p->steps_until_update;
+        double *rscratch = rigid ? (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1) * 7) : NULL;
         shared[t][4] = 0;
 
         while ((shared[t][2] < (double)p->max_steps || p->max_steps < 0) &&
@@ -913,7 +1031,12 @@ GCRO_EXPORT int gcro_srk2_run(const gcro_params *p, gcro_state *st, gcro_result 
                 }
                 double dt_eff = dt_for_update * pref;
                 double s2 = sqrt(2.0 * dt_for_update * p->D);
-                if (n > 0) {
+                if (n > 0 && rigid) {
+                    /* read at check_force_at_pos: pos in the predictor, pos1
+                     * in the corrector (SRK.py:174-186, 365-371) */
+                    project_rigid(W, X, F, noise, n, st->chain_id + s0, st->rest_lengths, p->rigid_rod, L, dt_eff,
+                                  p->D, p->radius, dim, rscratch, rscratch + 3 * n, rscratch + 6 * n);
+                } else if (n > 0) {
                     dt_eff /= p->radius;
                     for (int64_t b = 0; b < n; b++)
                         for (int i = 0; i < dim; i++) {
@@ -971,6 +1094,7 @@ GCRO_EXPORT int gcro_srk2_run(const gcro_params *p, gcro_state *st, gcro_result 
             }
             (void)inject_step;
         }
+        free(rscratch);
     }
     out->dt = shared[0][0];
     out->dt_used_total = shared[0][1];

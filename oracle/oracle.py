@@ -116,6 +116,9 @@ def lib():
         L.gcro_chunk_chain.restype = C.c_int
         L.gcro_chunk_chain.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]
         L.gcro_order_params.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
+        L.gcro_project_rigid.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
+                                         C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+                                         C.c_int]
         assert L.gcro_sizeof_params() == C.sizeof(Params)
         assert L.gcro_sizeof_state() == C.sizeof(State)
         assert L.gcro_sizeof_mt() == C.sizeof(MT)
@@ -193,6 +196,20 @@ def self_propel(forces, tangent, active_params):
                            _p(np.ascontiguousarray(active_params, dtype=np.float64)), dim)
 
 
+def project_rigid(prev, forces, noise, chain_id, rest_lengths, factor, L, dt, D, radius):
+    """updates.project_updates_for_rigid_rod (updates.py:347-499) on one
+    chunk: the projected positions.  ``noise`` is the [N, 2*dim] noise_vec."""
+    prev = np.ascontiguousarray(prev, dtype=np.float64)
+    forces = np.ascontiguousarray(forces, dtype=np.float64)
+    noise = np.ascontiguousarray(noise, dtype=np.float64)
+    chain_id = np.ascontiguousarray(chain_id, dtype=np.int64)
+    rest_lengths = np.ascontiguousarray(rest_lengths, dtype=np.float64)
+    out = np.zeros_like(prev)
+    lib().gcro_project_rigid(_p(out), _p(prev), _p(forces), _p(noise), len(prev), _p(chain_id), _p(rest_lengths),
+                             float(factor), float(L), float(dt), float(D), float(radius), prev.shape[1])
+    return out
+
+
 def chunk_chain(n_threads, chain_id):
     split = np.zeros(max(n_threads - 1, 0), dtype=np.int64)
     k = lib().gcro_chunk_chain(n_threads, len(chain_id), _p(chain_id), _p(split))
@@ -224,7 +241,7 @@ class OracleSystem:
     def __init__(self, pos, tangent, chain_id, rest_lengths, L, spring_params, wca_params,
                  active_params, D, Dr, radius, n_nearby, n_grid, grid_factor=2.0,
                  calc_springs=True, calc_wca=True, self_propel=True, grid_depth=None,
-                 nbor_depth=8):
+                 nbor_depth=8, rigid_rod=0.0):
         self.pos = np.ascontiguousarray(pos, dtype=np.float64).copy()
         self.N, self.dim = self.pos.shape
         self.pos1 = np.zeros_like(self.pos)
@@ -245,6 +262,7 @@ class OracleSystem:
         self.calc_springs = bool(calc_springs) and np.max(np.bincount(self.chain_id)) > 1
         self.calc_wca, self.do_self_propel = bool(calc_wca), bool(self_propel)
         self.longest_chain_length = int(np.max(np.bincount(self.chain_id)))
+        self.rigid_rod = float(rigid_rod)
         nz = 1 if self.dim == 2 else self.n_grid
         if grid_depth is None:
             grid_depth = max(1, int(8 * self.N / self.n_grid ** self.dim))
@@ -317,7 +335,7 @@ class OracleSystem:
             p.wca[i] = self.WCA_params[i]
         for i in range(3):
             p.active[i] = self.active[i]
-        p.D, p.Dr, p.radius, p.rigid_rod = self.D, self.Dr, self.radius, 0.0
+        p.D, p.Dr, p.radius, p.rigid_rod = self.D, self.Dr, self.radius, self.rigid_rod
         p.n_nearby, p.longest_chain_length = self.n_nearby, self.longest_chain_length
         p.grid_factor = self.grid_factor
         p.dt = dt
