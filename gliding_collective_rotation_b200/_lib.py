@@ -39,7 +39,7 @@ class SystemDesc(C.Structure):
                 ("self_propel", C.c_int32), ("n_nearby", C.c_int32), ("D", C.c_double), ("Dr", C.c_double),
                 ("radius", C.c_double), ("dtmax", C.c_double), ("max_dist_per_step", C.c_double),
                 ("rk_cheat", C.c_double), ("seed", C.c_uint64), ("step", C.c_int64),
-                ("cell_factor", C.c_double), ("skin", C.c_double)]
+                ("cell_factor", C.c_double), ("skin", C.c_double), ("rigid_rod", C.c_double)]
 
 
 class SystemBuffers(C.Structure):

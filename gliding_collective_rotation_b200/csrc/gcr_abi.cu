@@ -84,7 +84,10 @@ struct Slot {
     gcr_system_desc desc{};
     gcr_system_buffers buf{};
     int64_t bead_off = 0, cell_off = 0, chain_off = 0;
-    int64_t n_cells = 0;
+    int64_t n_cells = 0;        // cells of the current grid
+    int64_t n_cells_alloc = 0;  // cells reserved at admission
+    int64_t nc = 1;             // current GPU cells per side
+    int64_t longest = 0;        // beads of the longest chain
 };
 
 int ilog2(int v)
@@ -138,6 +141,7 @@ struct gcr_ctx {
     int grid_update = 1, grid_sys = 1, grid_pair = 1, grid_bin = 1, grid_sort = 1, grid_build = 1;
     int grid_stage0 = 1, grid_stage1 = 1;
     cudaGraphExec_t graph = nullptr;
+    bool graph_rigid = false;  // the graph holds the rigid-rod projection kernels
     bool tiles_dirty = true;
 };
 
@@ -196,6 +200,7 @@ int validate_desc(const gcr_config &cfg, const gcr_system_desc *d, int64_t *nc_o
     if (d->spring_params[3] != 0.0) return fail(GCR_ERR_BAD_ARG, "FENE springs are not supported");
     if (d->active_params[1] > 0.0) return fail(GCR_ERR_BAD_ARG, "active sliding is not supported");
     if (!(d->skin >= 0.0) || !std::isfinite(d->skin)) return fail(GCR_ERR_BAD_ARG, "skin must be >= 0");
+    if (!std::isfinite(d->rigid_rod)) return fail(GCR_ERR_BAD_ARG, "rigid_rod must be finite");
     int64_t nc = 1;
     double skin = d->skin;
     if (d->calc_wca) {
@@ -275,7 +280,17 @@ void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, double skin, SysP &
     p.dtmax = d.dtmax;
     p.mdps = d.max_dist_per_step;
     p.rk = d.rk_cheat;
+    // SRK.py:364: the projection acts only when some chain has more than 2 beads
+    p.rigid = (d.rigid_rod != 0.0 && sl.longest > 2) ? d.rigid_rod : 0.0;
     p.seed = d.seed;
+}
+
+// some resident system uses the rigid-rod projection
+bool any_rigid(const gcr_ctx *c)
+{
+    for (size_t s = 0; s < c->slots.size(); s++)
+        if (c->slots[s].used && c->hP[s].rigid != 0.0) return true;
+    return false;
 }
 
 int launch(gcr_ctx *c, void *fn, int grid, int block, size_t smem = 0)
@@ -312,11 +327,13 @@ int enqueue_step(gcr_ctx *c)
     if ((rc = enqueue_lists(c, 0))) return rc;
     if ((rc = launch(c, c->ks.pair0, c->grid_pair, bb))) return rc;
     if ((rc = launch(c, c->ks.stage0, c->grid_stage0, bb, c->stage_smem))) return rc;
+    if (c->graph_rigid && (rc = launch(c, c->ks.rigid0, c->grid_update, bb))) return rc;
     if ((rc = enqueue_lists(c, 1))) return rc;
     if ((rc = launch(c, c->ks.pair1, c->grid_pair, bb))) return rc;
     if ((rc = launch(c, c->ks.stage1, c->grid_stage1, bb, c->stage_smem))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_dt))) return rc;
     if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
+    if (c->graph_rigid && (rc = launch(c, c->ks.rigid1, c->grid_update, bb))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_end))) return rc;
     return GCR_OK;
 }
@@ -330,7 +347,15 @@ int enqueue_run_start(gcr_ctx *c)
 
 int build_graph(gcr_ctx *c)
 {
+    // the projection kernels are in the graph only while some system uses it
+    const bool rigid = any_rigid(c);
+    if (c->graph && rigid != c->graph_rigid) {
+        GCR_CUDA(cudaStreamSynchronize(c->stream));
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+    }
     if (c->graph) return GCR_OK;
+    c->graph_rigid = rigid;
     cudaGraph_t g = nullptr;
     GCR_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = GCR_OK;
@@ -442,7 +467,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     e = e ? e : cudaMalloc(&c->xi, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
     e = e ? e : cudaMalloc(&c->fp, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
     e = e ? e : cudaMalloc(&c->chain_starts, sizeof(int32_t) * (cfg.bead_capacity + S));
-    e = e ? e : cudaMalloc(&c->d_err, sizeof(int));
+    e = e ? e : cudaMalloc(&c->d_err, 2 * sizeof(int));
     e = e ? e : cudaMalloc(&c->d_out, sizeof(double) * 8);
     if (e != cudaSuccess)
         return cleanup(fail(e == cudaErrorMemoryAllocation ? GCR_ERR_OOM : GCR_ERR_CUDA,
@@ -558,6 +583,8 @@ int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers 
     sl.cell_off = coff;
     sl.chain_off = choff;
     sl.n_cells = n_cells;
+    sl.n_cells_alloc = n_cells;
+    sl.nc = nc;
     fill_sysp(c, sl, nc, skin, c->hP[slot]);
     SysS &s = c->hS[slot];
     std::memset(&s, 0, sizeof(s));
@@ -571,20 +598,23 @@ int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers 
     void *targs[] = {(void *)&buf->chain_id, &n, nullptr};
     uint8_t *tp = c->topo + boff;
     targs[2] = &tp;
-    GCR_CUDA(cudaMemsetAsync(c->d_err, 0, sizeof(int), c->stream));
+    GCR_CUDA(cudaMemsetAsync(c->d_err, 0, 2 * sizeof(int), c->stream));
     GCR_CUDA(cudaLaunchKernel(c->ks.topo, dim3((n + 255) / 256), dim3(256), targs, 0, c->stream));
     GCR_CUDA(launch_chain_starts(buf->chain_id, n, (int)desc->n_chains, c->chain_starts + choff, c->d_err,
                                  c->stream));
-    int err = 0;
-    GCR_CUDA(cudaMemcpyAsync(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    int err[2] = {0, 0};
+    GCR_CUDA(cudaMemcpyAsync(err, c->d_err, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     GCR_CUDA(cudaStreamSynchronize(c->stream));
-    if (err) {
+    if (err[0]) {
         c->beads.release(boff, desc->n_beads);
         if (n_cells) c->cells.release(coff, n_cells);
         c->chains.release(choff, desc->n_chains + 1);
         sl = Slot();
-        return fail(GCR_ERR_BAD_ARG, "chain ids must be non-decreasing and in [0, n_chains)");
+        return fail(GCR_ERR_BAD_ARG, "chain ids must run 0, 1, ..., n_chains - 1 in order (contiguous chains)");
     }
+    sl.longest = err[1];
+    fill_sysp(c, sl, nc, skin, c->hP[slot]);
+    GCR_CUDA(cudaMemcpyAsync(c->dP + slot, &c->hP[slot], sizeof(SysP), cudaMemcpyHostToDevice, c->stream));
     rc = rebuild_tiles(c);
     if (rc) return rc;
     *slot_out = slot;
@@ -598,7 +628,7 @@ int gcr_evict(gcr_ctx *c, int32_t slot)
     // make sure no queued work still uses the slot's scratch
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     c->beads.release(sl.bead_off, sl.desc.n_beads);
-    if (sl.n_cells) c->cells.release(sl.cell_off, sl.n_cells);
+    if (sl.n_cells_alloc) c->cells.release(sl.cell_off, sl.n_cells_alloc);
     c->chains.release(sl.chain_off, sl.desc.n_chains + 1);
     sl = Slot();
     SysS &s = c->hS[slot];
@@ -617,13 +647,24 @@ int gcr_update_desc(gcr_ctx *c, int32_t slot, const gcr_system_desc *desc)
     double skin = 0.0;
     int rc = validate_desc(c->cfg, desc, &nc, &skin);
     if (rc) return rc;
+    // the current grid stays while its cells cover the list radius (every
+    // run starts with a list build, so a grid change between calls is safe)
+    if (desc->calc_wca && sl.desc.calc_wca && desc->L == sl.desc.L && sl.nc >= 3 &&
+        desc->L / (double)sl.nc >= desc->wca_params[3] + skin)
+        nc = sl.nc;
     int64_t n_cells = 0;
     if (desc->calc_wca) {
         n_cells = 1;
         for (int i = 0; i < c->cfg.dim; i++) n_cells *= nc;
     }
-    if (n_cells != sl.n_cells) return fail(GCR_ERR_BAD_ARG, "the GPU cell grid of a resident system cannot change");
+    if (n_cells > sl.n_cells_alloc)
+        return fail(GCR_ERR_CAPACITY, "the new GPU cell grid needs more cells than were reserved at admission");
+    // in-flight work reads the descriptor table
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    if (n_cells != sl.n_cells) c->tiles_dirty = true;
     sl.desc = *desc;
+    sl.n_cells = n_cells;
+    sl.nc = nc;
     fill_sysp(c, sl, nc, skin, c->hP[slot]);
     GCR_CUDA(cudaMemcpyAsync(c->dP + slot, &c->hP[slot], sizeof(SysP), cudaMemcpyHostToDevice, c->stream));
     GCR_CUDA(cudaStreamSynchronize(c->stream));
@@ -735,6 +776,7 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
     std::vector<cudaEvent_t> ev((size_t)n_steps * (G + 1), nullptr);
     for (auto &e : ev) GCR_CUDA(cudaEventCreate(&e));
     const int bb = c->cfg.block_beads;
+    const bool rigid = any_rigid(c);
     for (int s = 0; s < n_steps && rc == GCR_OK; s++) {
         cudaEvent_t *e = ev.data() + (size_t)s * (G + 1);
         GCR_CUDA(cudaEventRecord(e[0], c->stream));
@@ -743,6 +785,7 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
         if (!rc) rc = launch(c, c->ks.pair0, c->grid_pair, bb);
         GCR_CUDA(cudaEventRecord(e[2], c->stream));
         if (!rc) rc = launch(c, c->ks.stage0, c->grid_stage0, bb, c->stage_smem);
+        if (!rc && rigid) rc = launch(c, c->ks.rigid0, c->grid_update, bb);
         GCR_CUDA(cudaEventRecord(e[3], c->stream));
         if (!rc) rc = enqueue_lists(c, 1);
         GCR_CUDA(cudaEventRecord(e[4], c->stream));
@@ -752,6 +795,7 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
         if (!rc) rc = launch_sys(c, c->ks.sys_dt);
         GCR_CUDA(cudaEventRecord(e[6], c->stream));
         if (!rc) rc = launch(c, c->ks.update, c->grid_update, bb);
+        if (!rc && rigid) rc = launch(c, c->ks.rigid1, c->grid_update, bb);
         if (!rc) rc = launch_sys(c, c->ks.sys_end);
         GCR_CUDA(cudaEventRecord(e[7], c->stream));
     }

@@ -73,6 +73,7 @@ struct SysP {
     // noise / SRK
     double D, Dr, radius, sqrt2D;
     double dtmax, mdps, rk;
+    double rigid;  // rigid-rod projection factor (0: off, or no chain longer than 2 beads)
     uint64_t seed;
 };
 

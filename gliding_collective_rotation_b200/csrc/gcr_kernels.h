@@ -46,6 +46,8 @@ struct KernelSet {
     void *stage0;
     void *stage1;
     void *update;
+    void *rigid0;   // rigid-rod projection: predictor (pos -> pos1) and corrector (pos1 -> pos)
+    void *rigid1;
     void *topo;
     void *sys_dt;
     void *sys_end;
@@ -65,6 +67,7 @@ cudaError_t launch_reference_lists(int dim, const SysP &p, int64_t n_grid, int64
                                    int64_t *nbor_list, int64_t nbor_depth1, int *d_err, cudaStream_t st);
 cudaError_t launch_order_params(int dim, int precision, const SysP &p, const int32_t *chain_start,
                                 double *d_out, cudaStream_t st);
+// chain_start[n_chains + 1]; d_err[0] |= 4 on bad chain ids, d_err[1] = longest chain
 cudaError_t launch_chain_starts(const int32_t *chain, int n, int n_chains, int32_t *chain_start, int *d_err,
                                 cudaStream_t st);
 cudaError_t launch_cell_assignment(int dim, const SysP &p, int32_t *cell_of_bead, cudaStream_t st);

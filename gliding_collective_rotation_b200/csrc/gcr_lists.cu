@@ -278,25 +278,35 @@ cudaError_t launch_order_params(int dim, int precision, const SysP &p, const int
     return cudaGetLastError();
 }
 
-// chain start offsets; flags chain ids that are out of range or not
-// non-decreasing (chains must be contiguous bead ranges)
+// chain start offsets; flags chain ids that do not run 0, 1, ..., n_chains-1
+// in order (chains must be contiguous, non-empty bead ranges)
 __global__ void k_chain_starts(const int32_t *__restrict__ chain, int n, int n_chains, int32_t *cs, int *err)
 {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b == 0) cs[n_chains] = n;
     if (b >= n) return;
     int c = chain[b];
-    if (c < 0 || c >= n_chains || (b > 0 && chain[b - 1] > c)) {
+    const int step = b > 0 ? c - chain[b - 1] : c;
+    if (c < 0 || c >= n_chains || step < 0 || step > 1 || (b == n - 1 && c != n_chains - 1)) {
         atomicOr(err, 4);
         return;
     }
-    if (b == 0 || chain[b - 1] != c) cs[c] = b;
+    if (b == 0 || step == 1) cs[c] = b;
+}
+
+// beads of the longest chain (err[1])
+__global__ void k_chain_longest(const int32_t *__restrict__ cs, int n_chains, const int *err, int *longest)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_chains || *err) return;
+    atomicMax(longest, cs[c + 1] - cs[c]);
 }
 
 cudaError_t launch_chain_starts(const int32_t *chain, int n, int n_chains, int32_t *chain_start, int *d_err,
                                 cudaStream_t st)
 {
     k_chain_starts<<<(n + 255) / 256, 256, 0, st>>>(chain, n, n_chains, chain_start, d_err);
+    k_chain_longest<<<(n_chains + 255) / 256, 256, 0, st>>>(chain_start, n_chains, d_err, d_err + 1);
     return cudaGetLastError();
 }
 

@@ -810,21 +810,24 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                     for (int i = 0; i < D; i++) xs[i] = xi[i];
                 }
                 // predictor: pos1 = (pos + dt/r F0 + sqrt(2 D dt) xi) mod L
-                const double dt = s.dt;
-                const double dt_eff = dt * 1.0 / p.radius;
-                const double s2 = sqrt(2.0 * dt * p.D);
-                double x1[3] = {0.0, 0.0, 0.0};
-                bool finite = true;
+                // (with the rigid-rod projection on, k_rigid writes pos1)
+                if (p.rigid == 0.0) {
+                    const double dt = s.dt;
+                    const double dt_eff = dt * 1.0 / p.radius;
+                    const double s2 = sqrt(2.0 * dt * p.D);
+                    double x1[3] = {0.0, 0.0, 0.0};
+                    bool finite = true;
 #pragma unroll
-                for (int i = 0; i < D; i++) {
-                    x1[i] = srk_update<FT>(xb[i], dt_eff, s2, F[i], xi[i], p.L);
-                    finite &= isfinite(x1[i]);
-                    p.pos1[(size_t)b * D + i] = x1[i];
+                    for (int i = 0; i < D; i++) {
+                        x1[i] = srk_update<FT>(xb[i], dt_eff, s2, F[i], xi[i], p.L);
+                        finite &= isfinite(x1[i]);
+                        p.pos1[(size_t)b * D + i] = x1[i];
+                    }
+                    if (!finite)
+                        atomicOr(&s.flags, kFlagNonFinite);
+                    else if (p.calc_wca && left_skin<D>(p, A, b, x1))
+                        s.rebuild = 1;  // the list of pos no longer covers pos1
                 }
-                if (!finite)
-                    atomicOr(&s.flags, kFlagNonFinite);
-                else if (p.calc_wca && left_skin<D>(p, A, b, x1))
-                    s.rebuild = 1;  // the list of pos no longer covers pos1
             } else {
                 // |F0+F1|^2 in FP64 for the dt rule (SRK.py:328)
                 double acc = 0.0;
@@ -875,13 +878,16 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A
         }
         double x[3] = {0.0, 0.0, 0.0};
         bool finite = true;
+        const bool plain = p.rigid == 0.0;  // else k_rigid writes pos
+        if (plain) {
 #pragma unroll
-        for (int i = 0; i < D; i++) {
-            x[i] = srk_update<FT>(p.pos[(size_t)b * D + i], dt_eff, s2, frc[(size_t)b * D + i], xi[i], p.L);
-            finite &= isfinite(x[i]);
-            p.pos[(size_t)b * D + i] = x[i];
+            for (int i = 0; i < D; i++) {
+                x[i] = srk_update<FT>(p.pos[(size_t)b * D + i], dt_eff, s2, frc[(size_t)b * D + i], xi[i], p.L);
+                finite &= isfinite(x[i]);
+                p.pos[(size_t)b * D + i] = x[i];
+            }
+            if (!finite) atomicOr(&s.flags, kFlagNonFinite);
         }
-        if (!finite) atomicOr(&s.flags, kFlagNonFinite);
         if (p.Dr > 0.0 && !p.get_orient) {
             // rotational diffusion, SRK.py:399-423 (note the factor pi)
             FT xr[3] = {FT(0), FT(0), FT(0)};
@@ -907,7 +913,155 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A
 #pragma unroll
             for (int i = 0; i < D; i++) tan[(size_t)b * D + i] = tb[i] / mag;
         }
-        if (finite && p.calc_wca && left_skin<D>(p, A, b, x)) s.rebuild = 1;  // rebuild before the next step
+        if (plain && finite && p.calc_wca && left_skin<D>(p, A, b, x)) s.rebuild = 1;  // rebuild before the next step
+    }
+}
+
+// ------------------------------------------------------------------------
+// rigid-rod projection, updates.project_updates_for_rigid_rod
+// (updates.py:347-499), in place of the plain update when the factor is on
+// (SRK.py:364-371).  One thread per chain (the thread of its head bead),
+// three passes over the chain's beads; all arithmetic in FP64.
+//   STAGE 0 (predictor): pos  -> pos1, dt_eff = dt
+//   STAGE 1 (corrector): pos1 -> pos,  dt_eff = dt_used / 2, forces F0 + F1
+// The projection reads the positions the forces were taken at (pos, then
+// pos1: check_force_at_pos), as the reference does.  Per chain:
+//   u_b      = dt_eff / r F_b + sqrt(2 D dt_eff) xi_b
+//   d_b      = a (b - (n-1)/2), I = dim sum_b d_b^2
+//   c        = head + mean_b wrap(x_b - head), mod L; r_hat = wrap(x_last - head) / |.|
+//   o_b      = wrap(x_b - (c + r_hat d_b))                  (deviation from the rod)
+//   2D: tau_i = sum_b (2i-1) r_hat_{1-i} u_{b,i} d_b / I,
+//       u_b,i <- (1-f) u_b,i + f (-o_b,i + mean u_i + tau_i d_b (2i-1) r_hat_{1-i})
+//   3D: tau = |r| sum_b r_hat x u_b,
+//       u_b <- (1-f) u_b + f (-o_b + mean u + (|r| / I) tau x r_hat)
+//   x_b <- (x_b + u_b) mod L
+// (the 2D torque per component and the 3D rotation term without a distance
+// factor are the reference's expressions as written).  A one-bead chain in
+// 3D (I = 0) gets no rotation term; the reference divides by zero there.
+// ------------------------------------------------------------------------
+__device__ __forceinline__ double wrap_open(double sep, double half, double L)
+{
+    if (sep < -half)
+        sep += L;
+    else if (sep > half)
+        sep -= L;
+    return sep;
+}
+
+template <int D, typename FT, int STAGE>
+__global__ void __launch_bounds__(512) k_rigid(BatchArgs A)
+{
+    const int nt = *A.n_bead_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.bead_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        SysS &s = A.S[tl.sys];
+        // no barriers in this kernel: a per-thread decision is safe
+        if (p.rigid == 0.0) continue;
+        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal)) continue;
+        const int b0 = tl.begin + threadIdx.x;
+        if (b0 >= p.n || threadIdx.x >= A.tile_beads) continue;
+        if (A.topo[p.bead_off + b0] & kHasPrev) continue;  // not a chain's head bead
+        const int c = p.chain[b0];
+        const int len = p.chain_start[c + 1] - b0;
+        const double *prev = STAGE == 0 ? p.pos : p.pos1;
+        double *rtn = STAGE == 0 ? p.pos1 : p.pos;
+        const double dt = STAGE == 0 ? s.dt * 1.0 : s.dt_used * 0.5;
+        const FT *frc = reinterpret_cast<const FT *>(p.frc);
+        const FT *xs = reinterpret_cast<const FT *>(A.xi) + (size_t)p.bead_off * D;
+        const double L = p.L, half = 0.5 * L, f = p.rigid;
+        const double dt_over_r = dt / p.radius;
+        const double s2 = sqrt(2.0 * p.D * dt);
+        const double rest = p.rest[c];
+        const double half_clm1 = (double)(len - 1) / 2.0;
+        auto upd = [&](int b, int i) {
+            double u = dt_over_r * (double)frc[(size_t)b * D + i];
+            if (s2 != 0.0) u += s2 * (double)xs[(size_t)b * D + i];
+            return u;
+        };
+        const double *x0 = prev + (size_t)b0 * D;
+        // pass 1: moment of inertia, mean update, centre, end-to-end vector
+        double inertia = 0.0, r_mag = 0.0, mean[D], com[D], rh[D];
+#pragma unroll
+        for (int i = 0; i < D; i++) mean[i] = com[i] = rh[i] = 0.0;
+        for (int k = 0; k < len; k++) {
+            const int b = b0 + k;
+            const double dk = rest * ((double)k - half_clm1);
+#pragma unroll
+            for (int i = 0; i < D; i++) {
+                inertia += dk * dk;
+                mean[i] += upd(b, i);
+                const double sep = wrap_open(prev[(size_t)b * D + i] - x0[i], half, L);
+                com[i] += sep;
+                if (k == len - 1) {
+                    rh[i] = sep;
+                    r_mag += sep * sep;
+                }
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < D; i++) {
+            mean[i] /= (double)len;
+            com[i] = py_mod(x0[i] + com[i] / (double)len, L);
+        }
+        if (r_mag > 0.0) {
+            r_mag = sqrt(r_mag);
+#pragma unroll
+            for (int i = 0; i < D; i++) rh[i] /= r_mag;
+        }
+        // pass 2: torque
+        double tq[3] = {0.0, 0.0, 0.0}, rot[3] = {0.0, 0.0, 0.0};
+        if constexpr (D == 2) {
+            for (int k = 0; k < len; k++) {
+                const double dk = rest * ((double)k - half_clm1);
+#pragma unroll
+                for (int i = 0; i < 2; i++) tq[i] += (double)(2 * i - 1) * rh[1 - i] * upd(b0 + k, i) * dk;
+            }
+            if (inertia != 0.0) {
+                tq[0] /= inertia;
+                tq[1] /= inertia;
+            }
+        } else {
+            for (int k = 0; k < len; k++) {
+                const double u0 = upd(b0 + k, 0), u1 = upd(b0 + k, 1), u2 = upd(b0 + k, 2);
+                tq[0] += rh[1] * u2 - rh[2] * u1;
+                tq[1] += rh[2] * u0 - rh[0] * u2;
+                tq[2] += rh[0] * u1 - rh[1] * u0;
+            }
+#pragma unroll
+            for (int i = 0; i < 3; i++) tq[i] = r_mag * tq[i];
+            const double q = inertia != 0.0 ? r_mag / inertia : 0.0;
+            rot[0] = q * (tq[1] * rh[2] - tq[2] * rh[1]);
+            rot[1] = q * (tq[2] * rh[0] - tq[0] * rh[2]);
+            rot[2] = q * (tq[0] * rh[1] - tq[1] * rh[0]);
+        }
+        // pass 3: projected updates and the new positions
+        const double keep = 1. - f;
+        bool finite = true, moved = false;
+        for (int k = 0; k < len; k++) {
+            const int b = b0 + k;
+            const double dk = rest * ((double)k - half_clm1);
+            double x[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int i = 0; i < D; i++) {
+                double o = prev[(size_t)b * D + i] - (com[i] + rh[i] * dk);
+                if (o < -half)
+                    o += L;
+                else if (o >= half)
+                    o -= L;
+                double u = upd(b, i) * keep;
+                if constexpr (D == 2)
+                    u += f * (-o + mean[i] + (tq[i] * dk * (double)(2 * i - 1) * rh[1 - i]));
+                else
+                    u += f * (-o + mean[i] + rot[i]);
+                x[i] = py_mod(prev[(size_t)b * D + i] + u, L);
+                finite &= isfinite(x[i]);
+                rtn[(size_t)b * D + i] = x[i];
+            }
+            if (finite && p.calc_wca && left_skin<D>(p, A, b, x)) moved = true;
+        }
+        if (!finite) atomicOr(&s.flags, kFlagNonFinite);
+        if (moved) s.rebuild = 1;  // the list no longer covers the new positions
     }
 }
 
@@ -990,6 +1144,8 @@ struct StepKernels {
     static void *stage0() { return (void *)k_stage<D, FT, 0>; }
     static void *stage1() { return (void *)k_stage<D, FT, 1>; }
     static void *update() { return (void *)k_update<D, FT>; }
+    static void *rigid0() { return (void *)k_rigid<D, FT, 0>; }
+    static void *rigid1() { return (void *)k_rigid<D, FT, 1>; }
 };
 
 KernelSet kernel_set(int dim, int precision)
@@ -1004,7 +1160,9 @@ KernelSet kernel_set(int dim, int precision)
     k.pair1 = StepKernels<D_, FT_>::pair1();    \
     k.stage0 = StepKernels<D_, FT_>::stage0();  \
     k.stage1 = StepKernels<D_, FT_>::stage1();  \
-    k.update = StepKernels<D_, FT_>::update();
+    k.update = StepKernels<D_, FT_>::update();  \
+    k.rigid0 = StepKernels<D_, FT_>::rigid0();  \
+    k.rigid1 = StepKernels<D_, FT_>::rigid1();
     if (dim == 2 && precision == 0) {
         GCR_FILL(2, double)
     } else if (dim == 2) {

@@ -53,6 +53,7 @@ class SystemParams:
     step: int = 0
     cell_factor: float = 1.0
     skin: float | None = None    # Verlet skin of the neighbour list; None: default_skin(r_cut)
+    rigid_rod: float = 0.0       # rigid_rod_projection_factor (updates.py:347-499); 0: off
 
     def desc(self, n_beads, n_chains):
         d = SystemDesc()
@@ -70,6 +71,7 @@ class SystemParams:
             float(self.rk_cheat)
         d.seed, d.step, d.cell_factor = int(self.seed) & (2 ** 64 - 1), int(self.step), float(self.cell_factor)
         d.skin = float(self.skin if self.skin is not None else default_skin(self.wca_params[3]))
+        d.rigid_rod = float(self.rigid_rod)
         return d
 
 

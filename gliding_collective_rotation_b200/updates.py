@@ -18,8 +18,17 @@ Same signature, inputs, outputs and bookkeeping as the reference's
 
 The bead state stays on the device between calls; each call uploads the
 host arrays (the caller may have changed them) and downloads the result.
-Features outside the GPU path (walls, motors, rigid rods, FENE, active
-sliding, E-field, SRK4, several populations) raise ``NotImplementedError``.
+The rigid-rod projection (updates.project_updates_for_rigid_rod,
+updates.py:347-499) runs on the device whenever the population's
+``rigid_rod_projection_factor`` is on and a chain has more than 2 beads, so
+the reference's init-grow protocol (control.early_time_procedures,
+control.py:153-219), which changes the radius, WCA parameters, spring
+constants, rest lengths and projection factor between calls, runs through
+this step unchanged; while a population grows the step computes in FP64
+whatever ``gpu_precision`` says (radii down to 1e-8 put the WCA prefactors
+below the FP32 range).  Features outside the GPU path (walls, motors, FENE,
+active sliding, E-field, SRK4, several populations) raise
+``NotImplementedError``.
 
 ``install(updates_module, config_module)`` rebinds a reference checkout's
 ``updates.SRK2_force_calc`` to this function and makes it read that
@@ -33,7 +42,7 @@ import numpy as np
 import torch
 
 from . import config as _default_config
-from ._lib import FLAG_CELL_OVERFLOW, FLAG_LIST_OVERFLOW
+from ._lib import FLAG_CELL_OVERFLOW, FLAG_LIST_OVERFLOW, GcrError
 from .batch import MAX_DEPTH, MAX_LIST_DEPTH, cell_scale, default_depth, default_list_depth
 from .engine import Engine, SystemParams, SystemState, default_config, footprint
 
@@ -105,8 +114,10 @@ class _GpuPop:
 
 
 def _key(pop, dim, precision, params, depth, ldepth):
-    return (pop.total_pop, len(pop.rest_lengths), dim, precision, float(params.L), float(params.wca_params[3]),
-            float(params.cell_factor), float(params.skin if params.skin is not None else -1.0), depth, ldepth, bool(params.calc_wca))
+    # the pair cutoff and skin may change from call to call (init-grow): the
+    # context re-derives its cell grid within the cells it reserved
+    return (pop.total_pop, len(pop.rest_lengths), dim, precision, float(params.L), float(params.cell_factor), depth,
+            ldepth, bool(params.calc_wca))
 
 
 def _gpu_state(pop, sim, dim, precision, params):
@@ -143,10 +154,10 @@ def SRK2_force_calc(pops, status, sim):
     if extra:
         raise NotImplementedError(f"forces not on the GPU step: {sorted(extra)}")
     longest = int(pop.longest_chain_length)
-    if getattr(pop, "rigid_rod_projection_factor", 0) != 0 and longest > 2:
-        raise NotImplementedError("rigid-rod projection is not part of the GPU step")
     dim = int(cfg.dim)
     precision = sim.get('gpu_precision', 'fp64')
+    if getattr(pop, "b_init_growing", False):
+        precision = 'fp64'
     calc_springs = "springs" in forces and longest > 1
     spring = forces.get("springs", np.zeros(6))
     if calc_springs and spring[3] != 0:
@@ -166,7 +177,7 @@ def SRK2_force_calc(pops, status, sim):
         calc_springs=calc_springs, calc_wca=calc_wca, self_propel=self_propel, dtmax=float(status.dtmax),
         max_dist_per_step=float(cfg.max_dist_per_step), rk_cheat=float(cfg.RK_cheat_factor), seed=seed,
         step=int(status.stepnum), cell_factor=float(sim.get('gpu_cell_factor', 1.0)),
-        skin=sim.get('gpu_skin', None))
+        skin=sim.get('gpu_skin', None), rigid_rod=float(getattr(pop, "rigid_rod_projection_factor", 0.0)))
     g = _gpu_state(pop, sim, dim, precision, params)
     st, eng = g.state, g.engine
 
@@ -177,7 +188,14 @@ def SRK2_force_calc(pops, status, sim):
     st.tangent.copy_(g.h_tan, non_blocking=True)
     st.rest_lengths.copy_(torch.from_numpy(np.asarray(pop.rest_lengths, dtype=np.float64)))
     st.params = params
-    eng.update_params(st)
+    try:
+        eng.update_params(st)
+    except GcrError as e:
+        if e.code != -6:
+            raise
+        # the new cell grid needs more cells than the context reserved
+        g.make_engine(params, g.engine.cfg.cell_depth, g.engine.cfg.list_depth)
+        eng = g.engine
 
     noise = None
     n_noise = 0

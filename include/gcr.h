@@ -24,6 +24,8 @@
  *                                SRK2_force_calc time_vals / pop_consts updates.py:138-162
  *   gcr_reference_lists       <- updates.update_grid_list_mini updates.py:502-522 and
  *                                updates.update_nbor_list   updates.py:586-669
+ *   gcr_system_desc.rigid_rod <- updates.project_updates_for_rigid_rod updates.py:347-499
+ *                                (applied as SRK.py:364-378 applies it)
  *   gcr_order_params          <- output_methods.calc_avg_phi_chain output_methods.py:492-510,
  *                                analysis.polar_orderparameter analysis.py:315-328,
  *                                analysis.nematic_orderparameter analysis.py:294-313
@@ -100,6 +102,10 @@ typedef struct {
     double skin;                /* Verlet skin (>= 0): the neighbour list holds the pairs within
                                    r_cut + skin and is rebuilt once a bead has moved skin / 2;
                                    reduced to L/3 - r_cut when the box is too small for it */
+    double rigid_rod;           /* rigid_rod_projection_factor (populations.py:325-329): each chain's
+                                   update is blended with that of a rigid rod of its rest length;
+                                   0 = off; applied only when the longest chain has more than 2 beads
+                                   (SRK.py:364) */
 } gcr_system_desc;
 
 /* Caller-owned device buffers of one system (bound, not copied). */
@@ -148,7 +154,10 @@ GCR_API int gcr_version(void);
 GCR_API int gcr_admit(gcr_ctx *ctx, const gcr_system_desc *desc, const gcr_system_buffers *buf,
               int32_t *slot_out);
 GCR_API int gcr_evict(gcr_ctx *ctx, int32_t slot);
-/* Replace the parameters of a resident system (same bead and chain counts). */
+/* Replace the parameters of a resident system (same bead and chain counts).
+ * A changed pair cutoff or skin keeps the GPU cell grid while its cells still
+ * cover r_cut + skin, else re-derives it within the cells reserved at
+ * admission (GCR_ERR_CAPACITY beyond them: evict and re-admit). */
 GCR_API int gcr_update_desc(gcr_ctx *ctx, int32_t slot, const gcr_system_desc *desc);
 /* Arm a resident system for the next gcr_run (one SRK2_force_calc call). */
 GCR_API int gcr_call_begin(gcr_ctx *ctx, int32_t slot, const gcr_call *call);

@@ -100,6 +100,21 @@ CASES = {
                  repel_d_max=1., WCA_epsilon=1., LJ_cutoff_factor=1., v0=1., v_tan_angle=0.1,
                  T=0.01, dim=2, seed=9, dtmax=4e-3),
         dt=None, fixed_dt=False, calls=[50, 50, 50, 50, 50], noise_seed=41, save_every=0.05),
+    # rigid rods (kappa < 0: projection factor 1, populations.py:325-329)
+    # with translational noise, 2D, through the reference's own init-grow
+    "rigid2d": dict(
+        sim=dict(Lx=30., n_chains=40, chain_length=8, a=0.5, k=100., kappa=-1., repel_d_max=1.,
+                 WCA_epsilon=1., LJ_cutoff_factor=1., v0=1., v_tan_angle=0., T=0.05, dim=2, seed=17,
+                 dtmax=1e-3),
+        dt=None, fixed_dt=False, calls=[1, 19, 80], noise_seed=61, save_every=None),
+    # rigid rods in 3D, chains laid straight and relaxed by the reference's
+    # own adaptive steps (with the projection on)
+    "rigid3d": dict(
+        sim=dict(Lx=16., n_chains=40, chain_length=6, a=0.5, k=100., kappa=-1., repel_d_max=1.,
+                 WCA_epsilon=1., LJ_cutoff_factor=1., v0=1., v_tan_angle=0., T=0.05, dim=3, seed=19,
+                 dtmax=5e-4, t_init_grow=0., a_init_factor=1.0),
+        dt=None, fixed_dt=False, calls=[1, 19, 80], noise_seed=71, save_every=None,
+        init_grow=False, relax_steps=200),
     # the paper's chiral run settings (Chiral_parameters_script.sh:3-17) on a
     # small box: chain length 30, kappa 100, v_tan_angle 0.1, WCA_epsilon 1e-8,
     # WCA_shift 0.1, bead_density 0.3, adaptive dt.
@@ -177,9 +192,10 @@ def run_case(name, spec, mods):
         control.sim_loop(pops, sim, status)        # init-grow until t > 0
         control.early_time_procedures(pops, status, sim)  # ends init-grow
     else:
-        # The reference's 3D init-grow divides by zero inside its rigid-rod
-        # projection; instead chains are laid straight (a_init_factor = 1)
-        # and relaxed by the reference's own adaptive-dt steps.
+        # Chains laid straight (a_init_factor = 1) and relaxed by the
+        # reference's own adaptive-dt steps, without init-grow.  (The
+        # reference's 3D projection divides by zero only for a one-bead
+        # chain; these cases have none.)
         status.next_output_step = status.stepnum + spec["relax_steps"]
         updates.SRK2_force_calc(pops, status, sim)
     grow_s = time.time() - t0
@@ -198,6 +214,7 @@ def run_case(name, spec, mods):
                 grid_factor=config.grid_factor, n_steps_update=config.n_steps_update_grid_list,
                 rk_cheat=config.RK_cheat_factor, grid_window=sim["grid_window"],
                 longest_chain_length=pop.longest_chain_length,
+                rigid_rod=float(pop.rigid_rod_projection_factor),
                 b_get_orientations=bool(pop.b_get_orientations), noise_seed=spec["noise_seed"],
                 fixed_dt=spec["fixed_dt"], save_every=spec["save_every"],
                 init_grow_steps=int(status.stepnum), init_grow_seconds=grow_s, **init_scal)
@@ -282,7 +299,12 @@ def main():
             with open(os.path.join(args.out, f"{name}.json")) as fh:
                 index[name] = json.load(fh)
             os.remove(os.path.join(args.out, f"{name}.json"))
-        with open(os.path.join(args.out, "index.json"), "w") as fh:
+        # a run over some cases keeps the index entries of the others
+        path = os.path.join(args.out, "index.json")
+        if os.path.exists(path):
+            with open(path) as fh:
+                index = {**json.load(fh), **index}
+        with open(path, "w") as fh:
             json.dump(index, fh, indent=1, sort_keys=True)
         return
 

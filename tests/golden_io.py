@@ -5,7 +5,7 @@ import os
 import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-CASES = ["config1", "chiral_lj", "rotdiff2d", "rotdiff3d", "adaptive", "paper_chiral"]
+CASES = ["config1", "chiral_lj", "rotdiff2d", "rotdiff3d", "adaptive", "paper_chiral", "rigid2d", "rigid3d"]
 STATUS_FIELDS = ["dt", "dt_used", "stepnum", "t", "update_grid_list_counter", "max_forces_strength",
                  "next_output_step", "next_save_time", "dtmax"]
 
@@ -43,4 +43,6 @@ TRAJ_TOL = {
     "rotdiff3d": [1e-11, 1e-11, 1e-11],
     "adaptive": [1e-9, 1e-9, 1e-9, 1e-9, 1e-9],
     "paper_chiral": [1e-9, 1e-6],
+    "rigid2d": [1e-9, 1e-9, 1e-9],
+    "rigid3d": [1e-9, 1e-9, 1e-9],
 }

@@ -27,8 +27,23 @@ def pop_from_arrays(pos, tangent, chain_id, rest_lengths, spring, wca, active, D
 
 
 def pop_from_golden(d, s):
-    return pop_from_arrays(d["pos0"], d["tangent0"], d["chain_id"], d["rest_lengths"], d["spring_params"],
-                           d["wca_params"], d["active_params"], s["D"], s["Dr"], s["radius"], s["n_nearby"])
+    pop = pop_from_arrays(d["pos0"], d["tangent0"], d["chain_id"], d["rest_lengths"], d["spring_params"],
+                          d["wca_params"], d["active_params"], s["D"], s["Dr"], s["radius"], s["n_nearby"])
+    pop.rigid_rod_projection_factor = float(s.get("rigid_rod", 0.0))
+    return pop
+
+
+def set_pop_params(pop, spring, wca, active, D, Dr, radius, n_nearby, rest_lengths, rigid, growing):
+    """Give a population new parameters between calls, as the reference's
+    init-grow loop does (control.early_time_procedures)."""
+    sp, wc, ac = (np.array(a, dtype=np.float64) for a in (spring, wca, active))
+    longest = pop.longest_chain_length
+    pop.self_interactions = lambda: ([["springs", sp]] if longest > 1 else []) + [["WCA", wc],
+                                                                                   ["self-propulsion", ac]]
+    pop.D, pop.Dr, pop.repel_d_max, pop.n_nearby_beads_dont_repel = float(D), float(Dr), float(radius), int(n_nearby)
+    pop.rest_lengths[:] = rest_lengths
+    pop.rigid_rod_projection_factor = float(rigid)
+    pop.b_init_growing = bool(growing)
 
 
 def set_config(s):

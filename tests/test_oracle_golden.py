@@ -17,7 +17,8 @@ def _system(d, s):
                           d["spring_params"], d["wca_params"], d["active_params"], s["D"], s["Dr"],
                           s["radius"], s["n_nearby"], s["n_grid"], s["grid_factor"],
                           grid_depth=s["grid_depth1"] - 1,
-                          nbor_depth=2 * max(s["nbor_depth1"], s["final_nbor_depth1"]))
+                          nbor_depth=2 * max(s["nbor_depth1"], s["final_nbor_depth1"]),
+                          rigid_rod=s.get("rigid_rod", 0.0))
 
 
 def test_mt_stream_matches_numba():
