@@ -6,7 +6,7 @@
  * links, loads or calls it.
  *
  * It restates, loop for loop, the reference's Numba hot path:
- *   SRK_jit                    SRK.py:13-484   (SRK2 branch only)
+ *   SRK_jit                    SRK.py:13-484   (SRK2 and SRK4 branches)
  *   thread_wait                SRK.py:487-495  (-> OpenMP barrier)
  *   WCA                        forces.py:13-15
  *   inbounds_diff              forces.py:44-55
@@ -276,6 +276,8 @@ typedef struct {
     /* Philox key and the global step index of the first step of this call */
     uint64_t seed;
     int64_t step0;
+    /* config.SRK_order: 2 (or 0) = SRK2, 4 = SRK4 */
+    int64_t srk_order;
 } gcro_params;
 
 typedef struct {
@@ -293,6 +295,8 @@ typedef struct {
     int64_t noise_inject_steps;
     /* MT19937 state per thread (n_threads entries) */
     gcro_mt *mt;
+    /* SRK4: the force of the current stage (pop.forces_aux, populations.py:149-154) */
+    double *forces_aux;
 } gcro_state;
 
 /* shared_arr row layout, SRK.py: 0 dt, 1 elapsed, 2 steps, 3 max force,
@@ -894,6 +898,9 @@ GCRO_EXPORT int gcro_srk2_run(const gcro_params *p, gcro_state *st, gcro_result 
     int T = p->n_threads > 0 ? p->n_threads : 1;
     /* SRK.py:364: the projection replaces the plain update */
     const int rigid = p->rigid_rod != 0.0 && p->longest_chain_length > 2;
+    const int srk4 = p->srk_order == 4;
+    const int n_stages = srk4 ? 4 : 2;
+    if (srk4 && !st->forces_aux) return -2;
 
     /* chunk boundaries: chain-aligned (updates.py:192-199, 323-344) */
     int64_t *bounds = (int64_t *)malloc(sizeof(int64_t) * (T + 1));
@@ -935,6 +942,7 @@ GCRO_EXPORT int gcro_srk2_run(const gcro_params *p, gcro_state *st, gcro_result 
         double *pos = st->pos + s0 * dim, *pos1 = st->pos1 + s0 * dim;
         double *noise = st->noise + s0 * 2 * dim, *tan = st->tangent + s0 * dim;
         double *F = st->forces + s0 * dim;
+        double *Fa = srk4 ? st->forces_aux + s0 * dim : NULL;
         int64_t *nb = st->nbor_list + s0 * st->nbor_depth1;
         int64_t *wib = st->where_is_bead + s0 * 3;
         int64_t gchunk = (ng + T - 1) / T;
@@ -979,22 +987,37 @@ GCRO_EXPORT int gcro_srk2_run(const gcro_params *p, gcro_state *st, gcro_result 
                     }
                 }
             }
-            for (int64_t b = 0; b < n * dim; b++) F[b] = 0.0;
+            /* SRK.py:144-160: the forces of SRK2 (both stages) or of the
+             * SRK4 stages are wiped */
+            for (int64_t b = 0; b < n * dim; b++) (srk4 ? Fa : F)[b] = 0.0;
             shared[t][5] = 0;
 
-            for (int stage = 0; stage < 2; stage++) {
+            for (int stage = 0; stage < n_stages; stage++) {
+                /* SRK.py:166-215: where forces are taken and updates written */
                 double *X = stage == 0 ? pos : pos1;
                 double *Xfull = stage == 0 ? st->pos : st->pos1;
-                double *W = stage == 0 ? pos1 : pos;
-                double pref = stage == 0 ? 1.0 : 0.5;
+                double *W = srk4 ? (stage == 3 ? pos : pos1) : (stage == 0 ? pos1 : pos);
+                double pref = srk4 ? 1.0 : (stage == 0 ? 1.0 : 0.5);
+                double rescale = stage <= 1 ? 0.5 : 1.0;
+                double *Fs = srk4 ? Fa : F;  /* write_to_forces */
+                if (srk4 && stage > 0)
+                    for (int64_t b = 0; b < n * dim; b++) Fa[b] = 0.0;
 #pragma omp barrier
                 if (p->calc_springs)
-                    spring_forces(X, tan, st->chain_id + s0, F, n, L, p->spring, st->rest_lengths, dim);
+                    spring_forces(X, tan, st->chain_id + s0, Fs, n, L, p->spring, st->rest_lengths, dim);
 #pragma omp barrier
                 if (p->calc_wca)
-                    pair_forces(s0, X, nb, st->nbor_depth1, F, n, L, Xfull, p->wca, pbc_width, dim);
-                if (p->self_propel) self_propel(F, tan, n, p->active, dim);
-                if (stage == 1) {
+                    pair_forces(s0, X, nb, st->nbor_depth1, Fs, n, L, Xfull, p->wca, pbc_width, dim);
+                if (p->self_propel) self_propel(Fs, tan, n, p->active, dim);
+                if (srk4) {
+                    /* SRK.py:296-321: weighted sum of the four stage forces */
+                    const double mult = (stage == 0 || stage == 3) ? 1. / 6. : 1. / 3.;
+                    if (stage == 0)
+                        for (int64_t b = 0; b < n * dim; b++) F[b] = Fa[b] * mult;
+                    else
+                        for (int64_t b = 0; b < n * dim; b++) F[b] += Fa[b] * mult;
+                }
+                if (stage == n_stages - 1) {
                     shared[t][3] = sqrt(2.0 * p->D);
                     if (n > 0) {
                         double m = -1.0;
@@ -1008,7 +1031,7 @@ GCRO_EXPORT int gcro_srk2_run(const gcro_params *p, gcro_state *st, gcro_result 
                     shared[t][2] += 1;
                 }
 #pragma omp barrier
-                if (stage == 1) {
+                if (stage == n_stages - 1) {
                     double mfs = shared[0][3];
                     for (int u = 1; u < T; u++)
                         if (shared[u][3] > mfs) mfs = shared[u][3];
@@ -1029,18 +1052,20 @@ GCRO_EXPORT int gcro_srk2_run(const gcro_params *p, gcro_state *st, gcro_result 
                 } else {
                     dt_for_update = dt;
                 }
-                double dt_eff = dt_for_update * pref;
+                /* SRK.py:355-362; the SRK4 real update uses the weighted sum */
+                double dt_eff = srk4 ? dt_for_update * rescale * pref : dt_for_update * pref;
                 double s2 = sqrt(2.0 * dt_for_update * p->D);
+                const double *Fu = (srk4 && stage < 3) ? Fa : F;
                 if (n > 0 && rigid) {
-                    /* read at check_force_at_pos: pos in the predictor, pos1
-                     * in the corrector (SRK.py:174-186, 365-371) */
-                    project_rigid(W, X, F, noise, n, st->chain_id + s0, st->rest_lengths, p->rigid_rod, L, dt_eff,
+                    /* read at check_force_at_pos: pos in the first stage, pos1
+                     * after it (SRK.py:166-215, 365-371) */
+                    project_rigid(W, X, Fu, noise, n, st->chain_id + s0, st->rest_lengths, p->rigid_rod, L, dt_eff,
                                   p->D, p->radius, dim, rscratch, rscratch + 3 * n, rscratch + 6 * n);
                 } else if (n > 0) {
                     dt_eff /= p->radius;
                     for (int64_t b = 0; b < n; b++)
                         for (int i = 0; i < dim; i++) {
-                            double tmp = pos[b * dim + i] + dt_eff * F[b * dim + i];
+                            double tmp = pos[b * dim + i] + dt_eff * Fu[b * dim + i];
                             if (s2 != 0.0) tmp += s2 * noise[b * 2 * dim + i];
                             W[b * dim + i] = py_mod(tmp, L);
                         }

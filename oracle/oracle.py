@@ -55,7 +55,7 @@ class Params(C.Structure):
         ("rk_cheat", C.c_double), ("max_dt_usable", C.c_double),
         ("steps_until_update", C.c_int64), ("n_steps_update", C.c_int64),
         ("max_steps", C.c_int64),
-        ("seed", C.c_uint64), ("step0", C.c_int64),
+        ("seed", C.c_uint64), ("step0", C.c_int64), ("srk_order", C.c_int64),
     ]
 
 
@@ -69,7 +69,7 @@ class State(C.Structure):
         ("grid_depth1", C.c_int64),
         ("nbor_list", C.c_void_p), ("nbor_depth1", C.c_int64),
         ("noise_inject", C.c_void_p), ("noise_inject_steps", C.c_int64),
-        ("mt", C.c_void_p),
+        ("mt", C.c_void_p), ("forces_aux", C.c_void_p),
     ]
 
 
@@ -241,7 +241,7 @@ class OracleSystem:
     def __init__(self, pos, tangent, chain_id, rest_lengths, L, spring_params, wca_params,
                  active_params, D, Dr, radius, n_nearby, n_grid, grid_factor=2.0,
                  calc_springs=True, calc_wca=True, self_propel=True, grid_depth=None,
-                 nbor_depth=8, rigid_rod=0.0):
+                 nbor_depth=8, rigid_rod=0.0, srk_order=2):
         self.pos = np.ascontiguousarray(pos, dtype=np.float64).copy()
         self.N, self.dim = self.pos.shape
         self.pos1 = np.zeros_like(self.pos)
@@ -263,6 +263,9 @@ class OracleSystem:
         self.calc_wca, self.do_self_propel = bool(calc_wca), bool(self_propel)
         self.longest_chain_length = int(np.max(np.bincount(self.chain_id)))
         self.rigid_rod = float(rigid_rod)
+        self.srk_order = int(srk_order)
+        # SRK4 keeps the force of the last stage (populations.py:149-154)
+        self.forces_aux = np.zeros_like(self.pos) if self.srk_order == 4 else None
         nz = 1 if self.dim == 2 else self.n_grid
         if grid_depth is None:
             grid_depth = max(1, int(8 * self.N / self.n_grid ** self.dim))
@@ -287,6 +290,7 @@ class OracleSystem:
         if self._inject is not None:
             st.noise_inject, st.noise_inject_steps = _p(self._inject), self._inject.shape[0]
         st.mt = C.addressof(self.mt)
+        st.forces_aux = _p(self.forces_aux)
         return st
 
     def seed_mt(self, seed, n_threads=1):
@@ -343,6 +347,7 @@ class OracleSystem:
         p.max_dist_per_step, p.rk_cheat, p.max_dt_usable = max_dist_per_step, rk_cheat, max_dt_usable
         p.steps_until_update, p.n_steps_update, p.max_steps = steps_until_update, n_steps_update, n_steps
         p.seed, p.step0 = seed, step0
+        p.srk_order = self.srk_order
         res = Result()
         st = self._state()
         rc = lib().gcro_srk2_run(C.byref(p), C.byref(st), C.byref(res))

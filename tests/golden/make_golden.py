@@ -115,6 +115,27 @@ CASES = {
                  dtmax=5e-4, t_init_grow=0., a_init_factor=1.0),
         dt=None, fixed_dt=False, calls=[1, 19, 80], noise_seed=71, save_every=None,
         init_grow=False, relax_steps=200),
+    # SRK4 (SRK.py:186-215, 296-321): 2D with chirality, grown by the
+    # reference's init-grow under SRK4
+    "srk4_2d": dict(
+        sim=dict(Lx=30., n_chains=40, chain_length=8, a=0.5, k=100., kappa=20., repel_d_max=1.,
+                 WCA_epsilon=1., LJ_cutoff_factor=1., v0=1., v_tan_angle=0.1, T=0.05, dim=2, seed=23,
+                 dtmax=1e-3, SRK_order=4),
+        dt=None, fixed_dt=False, calls=[1, 19, 80], noise_seed=81, save_every=None),
+    # SRK4 in 3D with LJ attraction and rotational diffusion
+    "srk4_3d": dict(
+        sim=dict(Lx=16., n_chains=40, chain_length=6, a=0.5, k=100., kappa=10., repel_d_max=1.,
+                 WCA_epsilon=1., LJ_cutoff_factor=2.5 / 2 ** (1 / 6), v0=1., v_tan_angle=0., T=0.05, Dr=0.1,
+                 b_use_tangent_as_propulsion_direction=False, dim=3, seed=29, dtmax=5e-4, SRK_order=4,
+                 t_init_grow=0., a_init_factor=1.0),
+        dt=None, fixed_dt=False, calls=[1, 19, 80], noise_seed=91, save_every=None,
+        init_grow=False, relax_steps=200),
+    # SRK4 with rigid rods (the projection at every stage)
+    "srk4_rigid": dict(
+        sim=dict(Lx=30., n_chains=40, chain_length=8, a=0.5, k=100., kappa=-1., repel_d_max=1.,
+                 WCA_epsilon=1., LJ_cutoff_factor=1., v0=1., v_tan_angle=0., T=0.05, dim=2, seed=31,
+                 dtmax=1e-3, SRK_order=4),
+        dt=None, fixed_dt=False, calls=[1, 19, 80], noise_seed=101, save_every=None),
     # the paper's chiral run settings (Chiral_parameters_script.sh:3-17) on a
     # small box: chain length 30, kappa 100, v_tan_angle 0.1, WCA_epsilon 1e-8,
     # WCA_shift 0.1, bead_density 0.3, adaptive dt.
@@ -214,7 +235,7 @@ def run_case(name, spec, mods):
                 grid_factor=config.grid_factor, n_steps_update=config.n_steps_update_grid_list,
                 rk_cheat=config.RK_cheat_factor, grid_window=sim["grid_window"],
                 longest_chain_length=pop.longest_chain_length,
-                rigid_rod=float(pop.rigid_rod_projection_factor),
+                rigid_rod=float(pop.rigid_rod_projection_factor), srk_order=int(config.SRK_order),
                 b_get_orientations=bool(pop.b_get_orientations), noise_seed=spec["noise_seed"],
                 fixed_dt=spec["fixed_dt"], save_every=spec["save_every"],
                 init_grow_steps=int(status.stepnum), init_grow_seconds=grow_s, **init_scal)
@@ -268,6 +289,8 @@ def run_case(name, spec, mods):
         out[f"call{ci}_pos"] = pop.pos.copy()
         out[f"call{ci}_tangent"] = pop.tangent_list.copy()
         out[f"call{ci}_forces"] = pop.forces.copy()
+        if config.SRK_order == 4:
+            out[f"call{ci}_forces_aux"] = pop.forces_aux.copy()
         if spec["save_every"] and status.t >= status.next_save_time:
             status.next_save_time += spec["save_every"]
     out["status_before"] = np.array(st_before)

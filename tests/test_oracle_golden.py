@@ -18,7 +18,7 @@ def _system(d, s):
                           s["radius"], s["n_nearby"], s["n_grid"], s["grid_factor"],
                           grid_depth=s["grid_depth1"] - 1,
                           nbor_depth=2 * max(s["nbor_depth1"], s["final_nbor_depth1"]),
-                          rigid_rod=s.get("rigid_rod", 0.0))
+                          rigid_rod=s.get("rigid_rod", 0.0), srk_order=s.get("srk_order", 2))
 
 
 def test_mt_stream_matches_numba():
@@ -95,6 +95,10 @@ def test_srk2_calls_match_reference(name):
         err = np.max(np.abs(min_image(sysm.pos - d[f"call{ci}_pos"], s["L"])))
         assert err <= tol, (name, ci, err)
         assert np.max(np.abs(sysm.tangent_list - d[f"call{ci}_tangent"])) <= 100 * tol
+        if s.get("srk_order", 2) == 4:
+            # the last stage's force (pop.forces_aux)
+            ref_a = d[f"call{ci}_forces_aux"]
+            assert np.max(np.abs(sysm.forces_aux - ref_a)) <= 1e-9 * np.max(np.abs(ref_a))
 
 
 def test_chunked_threads_match_single_thread():
