@@ -29,7 +29,7 @@ class Config(C.Structure):
     _fields_ = [("dim", C.c_int32), ("precision", C.c_int32), ("bead_capacity", C.c_int64),
                 ("system_capacity", C.c_int32), ("cell_capacity", C.c_int64), ("cell_depth", C.c_int32),
                 ("block_beads", C.c_int32), ("block_cells", C.c_int32), ("steps_per_graph", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("list_depth", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("list_depth", C.c_int32), ("srk_order", C.c_int32)]
 
 
 class SystemDesc(C.Structure):
@@ -44,7 +44,7 @@ class SystemDesc(C.Structure):
 
 class SystemBuffers(C.Structure):
     _fields_ = [("pos", C.c_void_p), ("pos1", C.c_void_p), ("tangent", C.c_void_p), ("forces", C.c_void_p),
-                ("chain_id", C.c_void_p), ("rest_lengths", C.c_void_p)]
+                ("chain_id", C.c_void_p), ("rest_lengths", C.c_void_p), ("forces_aux", C.c_void_p)]
 
 
 class Call(C.Structure):

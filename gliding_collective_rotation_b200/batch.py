@@ -48,7 +48,7 @@ def default_list_depth(dim):
     return 32 if dim == 2 else 96
 
 
-def _views(specs, precision, device):
+def _views(specs, precision, device, srk_order=2):
     ft = torch.float64 if precision == "fp64" else torch.float32
     dim = specs[0].dim
     n_tot = sum(s.n for s in specs)
@@ -61,6 +61,8 @@ def _views(specs, precision, device):
         "chain_id": torch.empty(n_tot, dtype=torch.int32, device=device),
         "rest": torch.empty(c_tot, dtype=torch.float64, device=device),
     }
+    if srk_order == 4:
+        big["forces_aux"] = torch.zeros((n_tot, dim), dtype=ft, device=device)
     h_pos = np.concatenate([s.pos for s in specs])
     h_tan = np.concatenate([s.tangent for s in specs])
     h_chain = np.concatenate([s.chain_id for s in specs]).astype(np.int32)
@@ -75,7 +77,8 @@ def _views(specs, precision, device):
         states.append(SystemState(pos=big["pos"][bo:bo + n], pos1=big["pos1"][bo:bo + n],
                                   tangent=big["tangent"][bo:bo + n], forces=big["forces"][bo:bo + n],
                                   chain_id=big["chain_id"][bo:bo + n], rest_lengths=big["rest"][co:co + nc],
-                                  params=s.params))
+                                  params=s.params,
+                                  forces_aux=big["forces_aux"][bo:bo + n] if srk_order == 4 else None))
         bo += n
         co += nc
     return big, states
@@ -85,7 +88,7 @@ class Batch:
     """Systems of one dimension and precision resident in one context."""
 
     def __init__(self, specs, precision="mixed", device=None, steps_per_graph=10, cell_depth=None,
-                 block_beads=128, block_cells=256, stream=None, ctas_per_sm=0, list_depth=None):
+                 block_beads=128, block_cells=256, stream=None, ctas_per_sm=0, list_depth=None, srk_order=2):
         if not specs:
             raise ValueError("empty batch")
         dims = {s.dim for s in specs}
@@ -102,18 +105,21 @@ class Batch:
         self._engine_kw = dict(block_beads=block_beads, block_cells=block_cells, steps_per_graph=steps_per_graph,
                                stream=stream, ctas_per_sm=ctas_per_sm)
         self.n_beads = sum(s.n for s in specs)
-        self.big, self.states = _views(specs, precision, self.device)
+        self.srk_order = srk_order
+        self.big, self.states = _views(specs, precision, self.device, srk_order)
         torch.cuda.synchronize(self.device)
         self.engine = None
         self._carry_dt = None  # dts to hand to the next call after a regrow
         self._make_engine()
 
     def _make_engine(self):
-        cfg = default_config(self.dim, self.precision, cell_depth=self.cell_depth, list_depth=self.list_depth)
+        cfg = default_config(self.dim, self.precision, cell_depth=self.cell_depth, list_depth=self.list_depth,
+                             srk_order=self.srk_order)
         cells = sum(footprint(cfg, s.params, s.n, len(s.rest_lengths))[0] for s in self.specs)
         self.engine = Engine(self.dim, self.precision, device=self.device, bead_capacity=self.n_beads,
                              system_capacity=len(self.specs), cell_capacity=max(cells, 1),
-                             cell_depth=self.cell_depth, list_depth=self.list_depth, **self._engine_kw)
+                             cell_depth=self.cell_depth, list_depth=self.list_depth, srk_order=self.srk_order,
+                             **self._engine_kw)
         for st in self.states:
             self.engine.admit(st)
 

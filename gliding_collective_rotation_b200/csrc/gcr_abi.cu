@@ -126,6 +126,8 @@ struct gcr_ctx {
     int *work = nullptr;
     void *xi = nullptr;
     void *fp = nullptr;
+    double *pos2 = nullptr;  // SRK4 scratch: second virtual update
+    void *faux = nullptr;    // SRK4 scratch: stage forces of systems without a caller buffer
     size_t stage_smem = 0;
     int32_t *chain_starts = nullptr;
     int *d_err = nullptr;
@@ -139,7 +141,7 @@ struct gcr_ctx {
     RangeAlloc beads, cells, chains;
     BatchArgs args{};
     int grid_update = 1, grid_sys = 1, grid_pair = 1, grid_bin = 1, grid_sort = 1, grid_build = 1;
-    int grid_stage0 = 1, grid_stage1 = 1;
+    int grid_stage0 = 1, grid_stage1 = 1, grid_stage4[4] = {1, 1, 1, 1};
     cudaGraphExec_t graph = nullptr;
     bool graph_rigid = false;  // the graph holds the rigid-rod projection kernels
     bool tiles_dirty = true;
@@ -239,6 +241,10 @@ void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, double skin, SysP &
     p.chain = sl.buf.chain_id;
     p.rest = sl.buf.rest_lengths;
     p.chain_start = c->chain_starts + sl.chain_off;
+    const size_t ft = c->cfg.precision == GCR_FP64 ? 8 : 4;
+    p.pos2 = c->pos2 ? c->pos2 + (size_t)sl.bead_off * c->cfg.dim : nullptr;
+    p.faux = sl.buf.forces_aux ? sl.buf.forces_aux
+                               : (c->faux ? (void *)((char *)c->faux + (size_t)sl.bead_off * c->cfg.dim * ft) : nullptr);
     p.bead_off = sl.bead_off;
     p.cell_off = sl.cell_off;
     p.n = (int32_t)d.n_beads;
@@ -314,16 +320,39 @@ int enqueue_lists(gcr_ctx *c, int which)
 {
     int rc;
     const int bb = c->cfg.block_beads, bc = c->cfg.block_cells;
+    void *bin = which == 0 ? c->ks.bin0 : (which == 1 ? c->ks.bin1 : c->ks.bin2);
+    void *build = which == 0 ? c->ks.build0 : (which == 1 ? c->ks.build1 : c->ks.build2);
     if ((rc = launch(c, c->ks.lists_plan, 1, 1024))) return rc;
-    if ((rc = launch(c, which ? c->ks.bin1 : c->ks.bin0, c->grid_bin, bb))) return rc;
+    if ((rc = launch(c, bin, c->grid_bin, bb))) return rc;
     if ((rc = launch(c, c->ks.sort, c->grid_sort, bc))) return rc;
-    return launch(c, which ? c->ks.build1 : c->ks.build0, c->grid_build, bb);
+    return launch(c, build, c->grid_build, bb);
+}
+
+// one SRK4 step (SRK.py:166-215): four force evaluations at pos, pos1, pos2,
+// pos1, each with its lists; the virtual updates alternate pos1 / pos2
+int enqueue_step4(gcr_ctx *c)
+{
+    int rc;
+    const int bb = c->cfg.block_beads;
+    static const int reads[4] = {0, 1, 2, 1};
+    for (int k = 0; k < 4; k++) {
+        if ((rc = enqueue_lists(c, reads[k]))) return rc;
+        void *pair = reads[k] == 0 ? c->ks.pair0 : (reads[k] == 1 ? c->ks.pair1 : c->ks.pair2);
+        if ((rc = launch(c, pair, c->grid_pair, bb))) return rc;
+        if ((rc = launch(c, c->ks.stage4[k], c->grid_stage4[k], bb, c->stage_smem))) return rc;
+        if (k < 3 && c->graph_rigid && (rc = launch(c, c->ks.rigid4[k], c->grid_update, bb))) return rc;
+    }
+    if ((rc = launch_sys(c, c->ks.sys_dt))) return rc;
+    if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
+    if (c->graph_rigid && (rc = launch(c, c->ks.rigid4[3], c->grid_update, bb))) return rc;
+    return launch_sys(c, c->ks.sys_end);
 }
 
 int enqueue_step(gcr_ctx *c)
 {
     int rc;
     const int bb = c->cfg.block_beads;
+    if (c->cfg.srk_order == 4) return enqueue_step4(c);
     if ((rc = enqueue_lists(c, 0))) return rc;
     if ((rc = launch(c, c->ks.pair0, c->grid_pair, bb))) return rc;
     if ((rc = launch(c, c->ks.stage0, c->grid_stage0, bb, c->stage_smem))) return rc;
@@ -402,7 +431,8 @@ int gcr_footprint(const gcr_config *cfg, const gcr_system_desc *desc, int64_t *c
     int64_t bytes = n * d * (8 + 8 + ft + ft) + n * 4 + desc->n_chains * 8     // caller-owned state
                     + n * (1 + 2 * d * ft) + 4 * (desc->n_chains + 1)          // topo, fp, xi, chain starts
                     + n * (4 * ld + 4 + 8 * d)                                 // neighbour list, xref
-                    + cells * (8 + (int64_t)cfg->cell_depth * 4);              // counts, slots
+                    + cells * (8 + (int64_t)cfg->cell_depth * 4)               // counts, slots
+                    + (cfg->srk_order == 4 ? n * d * (8 + ft) : 0);            // SRK4: pos2, stage forces
     if (cells_out) *cells_out = cells;
     if (bytes_out) *bytes_out = bytes;
     return GCR_OK;
@@ -427,6 +457,8 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
         return fail(GCR_ERR_BAD_ARG, "capacities must be positive");
     if (cfg.list_depth == 0) cfg.list_depth = cfg.dim == 2 ? 32 : 96;
     if (cfg.list_depth < 4 || cfg.list_depth > 1024) return fail(GCR_ERR_BAD_ARG, "list_depth must be in [4, 1024]");
+    if (cfg.srk_order == 0) cfg.srk_order = 2;
+    if (cfg.srk_order != 2 && cfg.srk_order != 4) return fail(GCR_ERR_BAD_ARG, "srk_order must be 2 or 4");
 
     gcr_ctx *c = new (std::nothrow) gcr_ctx();
     if (!c) return fail(GCR_ERR_OOM, "host allocation");
@@ -469,6 +501,10 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     e = e ? e : cudaMalloc(&c->chain_starts, sizeof(int32_t) * (cfg.bead_capacity + S));
     e = e ? e : cudaMalloc(&c->d_err, 2 * sizeof(int));
     e = e ? e : cudaMalloc(&c->d_out, sizeof(double) * 8);
+    if (cfg.srk_order == 4) {
+        e = e ? e : cudaMalloc(&c->pos2, sizeof(double) * (size_t)cfg.bead_capacity * cfg.dim);
+        e = e ? e : cudaMalloc(&c->faux, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
+    }
     if (e != cudaSuccess)
         return cleanup(fail(e == cudaErrorMemoryAllocation ? GCR_ERR_OOM : GCR_ERR_CUDA,
                             std::string("device allocation: ") + cudaGetErrorString(e)));
@@ -508,11 +544,16 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     a.log_depth = ilog2(cfg.cell_depth);
     a.tile_beads = cfg.block_beads;
     a.tile_cells = cfg.block_cells;
+    a.order = cfg.srk_order;
     c->stage_smem = c->ks.stage_smem(cfg.block_beads);
     if (c->stage_smem > 48 * 1024) {
         cudaFuncSetAttribute(c->ks.stage0, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->stage_smem);
         cudaFuncSetAttribute(c->ks.stage1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->stage_smem);
+        for (int k = 0; k < 4; k++)
+            cudaFuncSetAttribute(c->ks.stage4[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->stage_smem);
     }
+    for (int k = 0; k < 4; k++)
+        c->grid_stage4[k] = kernel_grid(c, c->ks.stage4[k], cfg.block_beads, c->max_bead_tiles, c->stage_smem);
     c->grid_stage0 = kernel_grid(c, c->ks.stage0, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
     c->grid_stage1 = kernel_grid(c, c->ks.stage1, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
     c->grid_update = kernel_grid(c, c->ks.update, cfg.block_beads, c->max_bead_tiles);
@@ -533,7 +574,7 @@ int gcr_destroy(gcr_ctx *c)
     if (c->graph) cudaGraphExecDestroy(c->graph);
     void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->topo, c->cnt, c->ncell,
                     c->items, c->nbr, c->ncount, c->xref, c->work, c->xi, c->fp, c->chain_starts, c->d_err,
-                    c->d_out};
+                    c->d_out, c->pos2, c->faux};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -764,6 +805,7 @@ int gcr_run(gcr_ctx *c, int64_t max_steps, int32_t sync_every)
 int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
 {
     if (!c || !ms_out || n_steps <= 0) return fail(GCR_ERR_BAD_ARG, "bad argument");
+    if (c->cfg.srk_order != 2) return fail(GCR_ERR_BAD_ARG, "per-group profiling covers SRK2 contexts");
     if (c->tiles_dirty) {
         int rc = rebuild_tiles(c);
         if (rc) return rc;

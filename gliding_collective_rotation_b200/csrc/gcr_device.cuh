@@ -48,6 +48,8 @@ struct SysP {
     const int32_t *chain;
     const double *rest;
     const int32_t *chain_start;  // first bead of each chain (+ end), library scratch
+    double *pos2;                // SRK4: positions of the second virtual update, library scratch
+    void *faux;                  // SRK4: force of the current stage (pop.forces_aux)
     // scratch placement
     int64_t bead_off;  // into topo
     int64_t cell_off;  // into cnt / items / rec

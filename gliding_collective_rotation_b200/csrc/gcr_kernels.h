@@ -33,6 +33,7 @@ struct BatchArgs {
     int log_depth;
     int tile_beads;
     int tile_cells;
+    int order;     // SRK order of the context: 2 or 4
 };
 
 struct KernelSet {
@@ -48,6 +49,12 @@ struct KernelSet {
     void *update;
     void *rigid0;   // rigid-rod projection: predictor (pos -> pos1) and corrector (pos1 -> pos)
     void *rigid1;
+    // SRK4: lists and pair forces at pos2, the four stages, their projections
+    void *bin2;
+    void *build2;
+    void *pair2;
+    void *stage4[4];
+    void *rigid4[4];
     void *topo;
     void *sys_dt;
     void *sys_end;

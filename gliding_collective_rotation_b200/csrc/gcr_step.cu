@@ -178,6 +178,26 @@ __device__ __forceinline__ FT wca_coeff(FT ds, FT p0, FT p1)
 // whatever the batch, the skin, the cell grid or the rebuild history.
 // ------------------------------------------------------------------------
 
+// Stages (SRK.py:166-215).  SRK2: 0 predictor, 1 corrector.  SRK4: 10..13,
+// the four force evaluations.  Positions are named 0 = pos, 1 = pos1,
+// 2 = pos2: the SRK4 virtual updates alternate between pos1 and pos2 so
+// that no kernel reads the positions it writes (the reference writes pos1
+// over itself between barriers); the caller's pos1 ends as the last virtual
+// update, as in the reference.
+constexpr bool srk4_stage(int S) { return S >= 10; }
+// positions the forces of a stage are taken at (check_force_at_pos)
+constexpr int stage_reads(int S) { return (S == 0 || S == 10) ? 0 : (S == 12 ? 2 : 1); }
+// positions a stage's update writes (write_to_pos): 0 for the real update
+constexpr int stage_writes(int S) { return (S == 0 || S == 10 || S == 12) ? 1 : (S == 11 ? 2 : 0); }
+// dt_rescale_factor * force_prefactor of a stage's update (SRK.py:188-192, 355-360)
+constexpr double stage_dt_factor(int S) { return S == 1 ? 0.5 : ((S == 10 || S == 11) ? 0.5 : 1.0); }
+
+template <int WHICH>
+__device__ __forceinline__ double *stage_x(const SysP &p)
+{
+    return WHICH == 0 ? p.pos : (WHICH == 1 ? p.pos1 : p.pos2);
+}
+
 // the system takes part in a list build now
 __device__ __forceinline__ bool builds(const SysP &p, const SysS &s)
 {
@@ -328,7 +348,7 @@ __global__ void __launch_bounds__(512) k_bin(BatchArgs A)
         if (!builds(p, s)) continue;
         const int b = (t - w.bead0[k]) * A.tile_beads + threadIdx.x;
         if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
-        const double *X = WHICH == 0 ? p.pos : p.pos1;
+        const double *X = stage_x<WHICH>(p);
         double x[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int i = 0; i < D; i++) x[i] = X[(size_t)b * D + i];
@@ -417,7 +437,7 @@ __global__ void __launch_bounds__(512) k_build(BatchArgs A)
         const int b = begin + threadIdx.x;
         if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
         const int n = p.n, nc = p.nc;
-        const double *X = WHICH == 0 ? p.pos : p.pos1;
+        const double *X = stage_x<WHICH>(p);
         double x[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int i = 0; i < D; i++) x[i] = X[(size_t)b * D + i];
@@ -512,7 +532,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_pair(BatchArgs A)
         const int b = tl.begin + threadIdx.x;
         if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
         const int n = p.n;
-        const double *X = WHICH == 0 ? p.pos : p.pos1;
+        const double *X = stage_x<WHICH>(p);
         double xb[3] = {0.0, 0.0, 0.0};
 #pragma unroll
         for (int i = 0; i < D; i++) xb[i] = X[(size_t)b * D + i];
@@ -636,7 +656,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
         if (!sh_run) continue;
         const int n = p.n;
         const int base = tl.begin - 2;
-        const double *__restrict__ X = STAGE == 0 ? p.pos : p.pos1;
+        const double *__restrict__ X = stage_x<stage_reads(STAGE)>(p);
         // 1. positions and topology of beads begin-2 .. begin+TB+1
         for (int k = threadIdx.x; k < TB + 4; k += TB) {
             int m = base + k;
@@ -721,7 +741,8 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
             FT F[3], tg[3];
 #pragma unroll
             for (int i = 0; i < D; i++) {
-                Fb[i] = STAGE == 0 ? BT(0) : (BT)frc[(size_t)b * D + i];
+                // the SRK2 corrector adds to F0; every other stage starts from 0
+                Fb[i] = STAGE == 1 ? (BT)frc[(size_t)b * D + i] : BT(0);
                 tg[i] = tan[(size_t)b * D + i];
             }
             bool tang_set = false;
@@ -794,49 +815,74 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                     for (int i = 0; i < D; i++) F[i] += v0 * tg[i];
                 }
             }
+            // G: the force the caller and the dt rule see -- F0 + F1 (SRK2),
+            // the weighted sum of the stage forces (SRK4, SRK.py:296-321,
+            // with the stage's own force kept in faux)
+            FT G[3];
+            if constexpr (srk4_stage(STAGE)) {
+                FT *faux = reinterpret_cast<FT *>(p.faux);
+                const FT w = (STAGE == 10 || STAGE == 13) ? FT(1. / 6.) : FT(1. / 3.);
 #pragma unroll
-            for (int i = 0; i < D; i++) frc[(size_t)b * D + i] = F[i];
+                for (int i = 0; i < D; i++) {
+                    faux[(size_t)b * D + i] = F[i];
+                    G[i] = STAGE == 10 ? F[i] * w : frc[(size_t)b * D + i] + F[i] * w;
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < D; i++) G[i] = F[i];
+            }
+#pragma unroll
+            for (int i = 0; i < D; i++) frc[(size_t)b * D + i] = G[i];
             if (tang_set) {
 #pragma unroll
                 for (int i = 0; i < D; i++) tan[(size_t)b * D + i] = tg[i];
             }
-            if (STAGE == 0) {
-                // the step's translational noise, drawn once and kept for the corrector
+            if constexpr (stage_writes(STAGE) != 0) {
+                // the step's translational noise, drawn once in the first stage
                 FT xi[3] = {FT(0), FT(0), FT(0)};
                 if (p.D > 0.0) {
-                    noise_trans<D, FT>(p, s, b, xi);
                     FT *xs = reinterpret_cast<FT *>(A.xi) + (size_t)(p.bead_off + b) * D;
+                    if constexpr (STAGE == 0 || STAGE == 10) {
+                        noise_trans<D, FT>(p, s, b, xi);
 #pragma unroll
-                    for (int i = 0; i < D; i++) xs[i] = xi[i];
+                        for (int i = 0; i < D; i++) xs[i] = xi[i];
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < D; i++) xi[i] = xs[i];
+                    }
                 }
-                // predictor: pos1 = (pos + dt/r F0 + sqrt(2 D dt) xi) mod L
-                // (with the rigid-rod projection on, k_rigid writes pos1)
+                // virtual update: (pos + dt_eff/r F + sqrt(2 D dt) xi) mod L
+                // from the step's old positions (with the rigid-rod
+                // projection on, k_rigid writes it)
                 if (p.rigid == 0.0) {
                     const double dt = s.dt;
-                    const double dt_eff = dt * 1.0 / p.radius;
+                    const double dt_eff = dt * stage_dt_factor(STAGE) / p.radius;
                     const double s2 = sqrt(2.0 * dt * p.D);
+                    double *W = stage_x<stage_writes(STAGE)>(p);
                     double x1[3] = {0.0, 0.0, 0.0};
                     bool finite = true;
 #pragma unroll
                     for (int i = 0; i < D; i++) {
-                        x1[i] = srk_update<FT>(xb[i], dt_eff, s2, F[i], xi[i], p.L);
+                        const double x0 = stage_reads(STAGE) == 0 ? xb[i] : p.pos[(size_t)b * D + i];
+                        x1[i] = srk_update<FT>(x0, dt_eff, s2, F[i], xi[i], p.L);
                         finite &= isfinite(x1[i]);
-                        p.pos1[(size_t)b * D + i] = x1[i];
+                        W[(size_t)b * D + i] = x1[i];
                     }
                     if (!finite)
                         atomicOr(&s.flags, kFlagNonFinite);
                     else if (p.calc_wca && left_skin<D>(p, A, b, x1))
-                        s.rebuild = 1;  // the list of pos no longer covers pos1
+                        s.rebuild = 1;  // the list no longer covers the new positions
                 }
-            } else {
-                // |F0+F1|^2 in FP64 for the dt rule (SRK.py:328)
+            }
+            if constexpr (STAGE == 1 || STAGE == 13) {
+                // |G|^2 in FP64 for the dt rule (SRK.py:323-330)
                 double acc = 0.0;
 #pragma unroll
-                for (int i = 0; i < D; i++) acc += (double)F[i] * (double)F[i];
+                for (int i = 0; i < D; i++) acc += (double)G[i] * (double)G[i];
                 mf2 = acc;
             }
         }
-        if (STAGE == 1) {
+        if (STAGE == 1 || STAGE == 13) {
             // warp / block max over non-negative doubles via their bit patterns
             unsigned long long bits = (unsigned long long)__double_as_longlong(mf2);
             for (int o = 16; o > 0; o >>= 1) {
@@ -868,7 +914,8 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A
         if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
         const FT *frc = reinterpret_cast<const FT *>(p.frc);
         const double dtu = s.dt_used;
-        const double dt_eff = dtu * 0.5 / p.radius;
+        // force_prefactor 0.5 of the SRK2 corrector; 1 for SRK4's weighted sum
+        const double dt_eff = dtu * (A.order == 4 ? 1.0 : 0.5) / p.radius;
         const double s2 = sqrt(2.0 * dtu * p.D);
         FT xi[3] = {FT(0), FT(0), FT(0)};
         if (p.D > 0.0) {
@@ -924,6 +971,9 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A
 // three passes over the chain's beads; all arithmetic in FP64.
 //   STAGE 0 (predictor): pos  -> pos1, dt_eff = dt
 //   STAGE 1 (corrector): pos1 -> pos,  dt_eff = dt_used / 2, forces F0 + F1
+//   SRK4 stages 10..13: the stage's positions -> its virtual update (pos1,
+//   pos2, pos1) with dt/2, dt/2, dt and the stage force, then pos with
+//   dt_used and the weighted sum
 // The projection reads the positions the forces were taken at (pos, then
 // pos1: check_force_at_pos), as the reference does.  Per chain:
 //   u_b      = dt_eff / r F_b + sqrt(2 D dt_eff) xi_b
@@ -964,10 +1014,13 @@ __global__ void __launch_bounds__(512) k_rigid(BatchArgs A)
         if (A.topo[p.bead_off + b0] & kHasPrev) continue;  // not a chain's head bead
         const int c = p.chain[b0];
         const int len = p.chain_start[c + 1] - b0;
-        const double *prev = STAGE == 0 ? p.pos : p.pos1;
-        double *rtn = STAGE == 0 ? p.pos1 : p.pos;
-        const double dt = STAGE == 0 ? s.dt * 1.0 : s.dt_used * 0.5;
-        const FT *frc = reinterpret_cast<const FT *>(p.frc);
+        const double *prev = stage_x<stage_reads(STAGE)>(p);
+        double *rtn = stage_x<stage_writes(STAGE)>(p);
+        // dt_eff of SRK.py:355-360: the step's dt in a virtual update, dt_used
+        // in the real one
+        const double dt = (stage_writes(STAGE) != 0 ? s.dt : s.dt_used) * stage_dt_factor(STAGE);
+        // write_to_forces: the stage's own force in SRK4's virtual updates
+        const FT *frc = reinterpret_cast<const FT *>(srk4_stage(STAGE) && STAGE != 13 ? p.faux : p.frc);
         const FT *xs = reinterpret_cast<const FT *>(A.xi) + (size_t)p.bead_off * D;
         const double L = p.L, half = 0.5 * L, f = p.rigid;
         const double dt_over_r = dt / p.radius;
@@ -1074,7 +1127,7 @@ __global__ void k_sys_dt(BatchArgs A, int n_slots)
     SysS &s = A.S[i];
     if (!s.active || (s.flags & kFlagFatal)) return;
     double mf2s = __longlong_as_double((long long)s.max_f2);
-    double S = p.sqrt2D + 0.5 * sqrt(mf2s) / p.radius;
+    double S = p.sqrt2D + (A.order == 4 ? 1.0 : 0.5) * sqrt(mf2s) / p.radius;
     double dt;
     if (S == 0.0)
         dt = p.dtmax;
@@ -1146,6 +1199,18 @@ struct StepKernels {
     static void *update() { return (void *)k_update<D, FT>; }
     static void *rigid0() { return (void *)k_rigid<D, FT, 0>; }
     static void *rigid1() { return (void *)k_rigid<D, FT, 1>; }
+    static void fill4(KernelSet &k)
+    {
+        k.pair2 = (void *)k_pair<D, FT, 2>;
+        k.stage4[0] = (void *)k_stage<D, FT, 10>;
+        k.stage4[1] = (void *)k_stage<D, FT, 11>;
+        k.stage4[2] = (void *)k_stage<D, FT, 12>;
+        k.stage4[3] = (void *)k_stage<D, FT, 13>;
+        k.rigid4[0] = (void *)k_rigid<D, FT, 10>;
+        k.rigid4[1] = (void *)k_rigid<D, FT, 11>;
+        k.rigid4[2] = (void *)k_rigid<D, FT, 12>;
+        k.rigid4[3] = (void *)k_rigid<D, FT, 13>;
+    }
 };
 
 KernelSet kernel_set(int dim, int precision)
@@ -1162,7 +1227,8 @@ KernelSet kernel_set(int dim, int precision)
     k.stage1 = StepKernels<D_, FT_>::stage1();  \
     k.update = StepKernels<D_, FT_>::update();  \
     k.rigid0 = StepKernels<D_, FT_>::rigid0();  \
-    k.rigid1 = StepKernels<D_, FT_>::rigid1();
+    k.rigid1 = StepKernels<D_, FT_>::rigid1();  \
+    StepKernels<D_, FT_>::fill4(k);
     if (dim == 2 && precision == 0) {
         GCR_FILL(2, double)
     } else if (dim == 2) {
@@ -1178,11 +1244,15 @@ KernelSet kernel_set(int dim, int precision)
         k.bin1 = (void *)k_bin<2, 1>;
         k.build0 = (void *)k_build<2, 0>;
         k.build1 = (void *)k_build<2, 1>;
+        k.bin2 = (void *)k_bin<2, 2>;
+        k.build2 = (void *)k_build<2, 2>;
     } else {
         k.bin0 = (void *)k_bin<3, 0>;
         k.bin1 = (void *)k_bin<3, 1>;
         k.build0 = (void *)k_build<3, 0>;
         k.build1 = (void *)k_build<3, 1>;
+        k.bin2 = (void *)k_bin<3, 2>;
+        k.build2 = (void *)k_build<3, 2>;
     }
     k.sort = (void *)k_sort;
     k.topo = (void *)k_topo;

@@ -19,21 +19,21 @@ import numpy as np
 def set_defaults():
     sim, help = {}, {}
     sim['filelabel'] = 'most_recent'
-    help['filelabel'] = 'Unique label string for each run.'
+    help['filelabel'] = 'Label that names the files of a run.'
     sim['n_threads'] = 3
     help['n_threads'] = 'Number of threads used to calculate forces (CPU path).'
     sim['dim'] = 2
-    help['dim'] = 'System dimensionality (2 or 3).'
+    help['dim'] = 'Number of spatial dimensions: 2 or 3.'
     sim['SRK_order'] = 2
-    help['SRK_order'] = 'Order of Runge-Kutta update (the GPU path implements 2).'
+    help['SRK_order'] = 'Stochastic Runge-Kutta order of the step: 2 or 4.'
     sim['Lx'] = 50.
-    help['Lx'] = 'Size of system in both x and y directions.'
+    help['Lx'] = 'Side of the periodic box (the same along every axis).'
     sim['walls'] = 'none'
     help['walls'] = 'Boundary conditions (the GPU path is periodic only).'
     sim['bead_density'] = 0.5
-    help['bead_density'] = 'Initialization: Number of beads per unit square.'
+    help['bead_density'] = 'Initial placement: beads per unit area.'
     sim['chain_length'] = 10
-    help['chain_length'] = 'Number of beads on each chain'
+    help['chain_length'] = 'Beads per chain.'
     sim['n_chains'] = -1
     help['n_chains'] = 'Initialization: Number of chains. If positive, overrides bead_density.'
     sim['t_max'] = -1
@@ -41,7 +41,7 @@ def set_defaults():
     sim['stepnum_max'] = -1
     help['stepnum_max'] = 'Stopping conditions: maximum step number. Negative for infinity.'
     sim['dtmax'] = 4.e-3
-    help['dtmax'] = 'Maximum timestep size (before multiplication by RK_cheat_factor).'
+    help['dtmax'] = 'Upper bound of the adaptive time step (RK_cheat_factor multiplies it afterwards).'
     sim['dt0'] = 0.0001 * sim['dtmax']
     help['dt0'] = 'Small timestep to use in first update only.'
     sim['RK_cheat_factor'] = 1.
@@ -73,11 +73,11 @@ def set_defaults():
     sim['a'] = 0.5
     help['a'] = 'Linear springs: rest length.'
     sim['kappa'] = 1e1
-    help['kappa'] = 'Bending springs: bending rigidity.'
+    help['kappa'] = 'Stiffness of the bending springs (negative: rigid rods).'
     sim['spontaneous_bond_angle'] = 0.0 * np.pi
     help['spontaneous_bond_angle'] = 'Bending springs: offset angle to zero of potential.'
     sim['rigid_rod_projection_factor'] = 0.
-    help['rigid_rod_projection_factor'] = 'Rigid-rod interpolation of updates (not on the GPU path).'
+    help['rigid_rod_projection_factor'] = 'Weight of the rigid-rod motion blended into each chain update (1: rigid rods).'
     sim['FENE_tolerance'] = 0.1
     help['FENE_tolerance'] = 'FENE maximum extension (not on the GPU path).'
     sim['v0'] = 1.
@@ -115,7 +115,7 @@ def set_defaults():
     sim['ticker_every'] = 1000
     help['ticker_every'] = 'Interval in steps for printing status info.'
     sim['resultspath'] = './Results/'
-    help['resultspath'] = 'Path to results folder.'
+    help['resultspath'] = 'Folder the run writes its files to.'
     sim['save_state_every'] = -1.
     help['save_state_every'] = 'Time interval between saved states; negative: never.'
     sim['plot_every'] = -1

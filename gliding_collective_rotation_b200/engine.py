@@ -87,6 +87,7 @@ class SystemState:
     params: SystemParams
     slot: int = -1
     extra: dict = field(default_factory=dict)
+    forces_aux: torch.Tensor | None = None  # SRK4: force of the last stage (pop.forces_aux)
 
     @property
     def n(self):
@@ -97,7 +98,7 @@ class SystemState:
         return self.rest_lengths.shape[0]
 
     @staticmethod
-    def from_host(pos, tangent, chain_id, rest_lengths, params, precision="fp64", device="cuda"):
+    def from_host(pos, tangent, chain_id, rest_lengths, params, precision="fp64", device="cuda", srk_order=2):
         ft = torch.float64 if precision == "fp64" else torch.float32
         pos_t = torch.as_tensor(np.ascontiguousarray(pos), dtype=torch.float64, device=device)
         chain = np.asarray(chain_id)
@@ -110,19 +111,21 @@ class SystemState:
             forces=torch.zeros(pos_t.shape, dtype=ft, device=device),
             chain_id=torch.as_tensor(chain.astype(np.int32), device=device),
             rest_lengths=torch.as_tensor(np.asarray(rest_lengths, dtype=np.float64), device=device).clone(),
-            params=params)
+            params=params,
+            forces_aux=torch.zeros(pos_t.shape, dtype=ft, device=device) if srk_order == 4 else None)
 
     def buffers(self):
         b = SystemBuffers()
         b.pos, b.pos1 = self.pos.data_ptr(), self.pos1.data_ptr()
         b.tangent, b.forces = self.tangent.data_ptr(), self.forces.data_ptr()
         b.chain_id, b.rest_lengths = self.chain_id.data_ptr(), self.rest_lengths.data_ptr()
+        b.forces_aux = self.forces_aux.data_ptr() if self.forces_aux is not None else None
         return b
 
 
 def default_config(dim, precision="fp64", bead_capacity=1 << 20, system_capacity=1,
                    cell_capacity=None, cell_depth=None, block_beads=256, block_cells=256,
-                   steps_per_graph=10, ctas_per_sm=0, list_depth=0):
+                   steps_per_graph=10, ctas_per_sm=0, list_depth=0, srk_order=2):
     cfg = Config()
     cfg.dim = dim
     cfg.precision = PRECISIONS[precision]
@@ -135,6 +138,9 @@ def default_config(dim, precision="fp64", bead_capacity=1 << 20, system_capacity
     cfg.block_beads, cfg.block_cells = int(block_beads), int(block_cells)
     cfg.steps_per_graph, cfg.ctas_per_sm = int(steps_per_graph), int(ctas_per_sm)
     cfg.list_depth = int(list_depth)
+    if srk_order not in (2, 4):
+        raise ValueError("srk_order must be 2 or 4")
+    cfg.srk_order = int(srk_order)
     return cfg
 
 
@@ -238,7 +244,12 @@ class Engine:
 
     # -- stepping ------------------------------------------------------------
     def run(self, max_steps, sync_every=0):
+        """Queue up to ``max_steps`` steps of every armed system on the
+        context stream.  Work queued afterwards on the caller's current torch
+        stream (reading the state tensors, say) is ordered after them; the
+        host does not wait."""
         check(self.lib.gcr_run(self._ctx, int(max_steps), int(sync_every)))
+        torch.cuda.current_stream(self.device).wait_stream(self.stream)
 
     def synchronize(self):
         check(self.lib.gcr_synchronize(self._ctx))

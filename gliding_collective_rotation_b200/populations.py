@@ -79,8 +79,12 @@ class Forces_Population(Population):
         self.reset_force_arrays()
 
     def reset_force_arrays(self):
+        """populations.py:149-154: SRK4 keeps the force of its last stage."""
         self.forces = np.zeros((self.total_pop, config.dim))
-        self.forces_aux = np.empty((self.total_pop, 0))
+        if config.SRK_order == 4:
+            self.forces_aux = np.empty_like(self.forces)
+        else:
+            self.forces_aux = np.empty((self.total_pop, 0))
 
     def make_empty_grid_list(self, num_pops=1):
         super().make_empty_grid_list(num_pops=num_pops)

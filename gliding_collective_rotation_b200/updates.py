@@ -26,9 +26,10 @@ control.py:153-219), which changes the radius, WCA parameters, spring
 constants, rest lengths and projection factor between calls, runs through
 this step unchanged; while a population grows the step computes in FP64
 whatever ``gpu_precision`` says (radii down to 1e-8 put the WCA prefactors
-below the FP32 range).  Features outside the GPU path (walls, motors, FENE,
-active sliding, E-field, SRK4, several populations) raise
-``NotImplementedError``.
+below the FP32 range).  ``config.SRK_order`` 4 runs the reference's SRK4
+branch (SRK.py:144-215, 296-321) and fills ``pop.forces_aux`` with the last
+stage's force.  Features outside the GPU path (walls, motors, FENE, active
+sliding, E-field, several populations) raise ``NotImplementedError``.
 
 ``install(updates_module, config_module)`` rebinds a reference checkout's
 ``updates.SRK2_force_calc`` to this function and makes it read that
@@ -83,13 +84,13 @@ _SUPPORTED = {"springs", "WCA", "self-propulsion"}
 class _GpuPop:
     """Device copy of one population and the context that steps it."""
 
-    def __init__(self, pop, sim, dim, precision, params, cell_depth, list_depth, key):
+    def __init__(self, pop, sim, dim, precision, params, cell_depth, list_depth, key, srk_order=2):
         self.key = key
-        self.dim, self.precision = dim, precision
+        self.dim, self.precision, self.srk_order = dim, precision, srk_order
         self.n, self.n_chains = pop.total_pop, len(pop.rest_lengths)
         self.spg = int(sim.get('gpu_steps_per_graph', 10))
         self.state = SystemState.from_host(pop.pos, pop.tangent_list, pop.chain_id, pop.rest_lengths, params,
-                                           precision=precision, device=torch.device("cuda"))
+                                           precision=precision, device=torch.device("cuda"), srk_order=srk_order)
         self.engine = None
         self.make_engine(params, cell_depth, list_depth)
         n = self.n
@@ -98,6 +99,7 @@ class _GpuPop:
         self.h_tan = torch.empty((n, dim), dtype=ft, pin_memory=True)
         self.h_frc = torch.empty((n, dim), dtype=ft, pin_memory=True)
         self.h_pos1 = torch.empty((n, dim), dtype=torch.float64, pin_memory=True)
+        self.h_faux = torch.empty((n, dim), dtype=ft, pin_memory=True) if srk_order == 4 else None
         self.rng = None
 
     def make_engine(self, params, cell_depth, list_depth):
@@ -105,30 +107,31 @@ class _GpuPop:
         tensors, and so the bead state, carry over."""
         if self.engine is not None:
             self.engine.close()
-        cfg = default_config(self.dim, self.precision, cell_depth=cell_depth, list_depth=list_depth)
+        cfg = default_config(self.dim, self.precision, cell_depth=cell_depth, list_depth=list_depth,
+                             srk_order=self.srk_order)
         cells = footprint(cfg, params, self.n, self.n_chains)[0]
         self.engine = Engine(self.dim, self.precision, bead_capacity=max(self.n, 1), system_capacity=1,
                              cell_capacity=max(cells, 1), cell_depth=cell_depth, list_depth=list_depth,
-                             steps_per_graph=self.spg, device=self.state.pos.device)
+                             steps_per_graph=self.spg, device=self.state.pos.device, srk_order=self.srk_order)
         self.engine.admit(self.state)
 
 
-def _key(pop, dim, precision, params, depth, ldepth):
+def _key(pop, dim, precision, params, depth, ldepth, srk_order=2):
     # the pair cutoff and skin may change from call to call (init-grow): the
     # context re-derives its cell grid within the cells it reserved
     return (pop.total_pop, len(pop.rest_lengths), dim, precision, float(params.L), float(params.cell_factor), depth,
-            ldepth, bool(params.calc_wca))
+            ldepth, bool(params.calc_wca), srk_order)
 
 
-def _gpu_state(pop, sim, dim, precision, params):
+def _gpu_state(pop, sim, dim, precision, params, srk_order=2):
     depth = getattr(pop, "_gcr_cell_depth", default_depth(dim, cell_scale(params)))
     ldepth = getattr(pop, "_gcr_list_depth", default_list_depth(dim))
     g = getattr(pop, "_gcr", None)
-    key = _key(pop, dim, precision, params, depth, ldepth)
+    key = _key(pop, dim, precision, params, depth, ldepth, srk_order)
     if g is None or g.key != key:
         if g is not None:
             g.engine.close()
-        g = _GpuPop(pop, sim, dim, precision, params, depth, ldepth, key)
+        g = _GpuPop(pop, sim, dim, precision, params, depth, ldepth, key, srk_order)
         pop._gcr = g
     return g
 
@@ -137,8 +140,9 @@ def SRK2_force_calc(pops, status, sim):
     """Stochastic Runge-Kutta 2nd-order update (Branka and Heyes, PRE 60:2381,
     1999) of one bead-spring-chain population on the GPU."""
     cfg = _config
-    if getattr(cfg, "SRK_order", 2) != 2:
-        raise NotImplementedError("the GPU step implements SRK_order = 2")
+    srk_order = int(getattr(cfg, "SRK_order", 2))
+    if srk_order not in (2, 4):
+        raise NotImplementedError("the GPU step implements SRK_order 2 and 4")
     if np.any(getattr(cfg, "walls", np.zeros(3, dtype=bool))):
         raise NotImplementedError("walls are not part of the GPU step")
     movers = [p for p in pops if not p.fixed]
@@ -178,7 +182,7 @@ def SRK2_force_calc(pops, status, sim):
         max_dist_per_step=float(cfg.max_dist_per_step), rk_cheat=float(cfg.RK_cheat_factor), seed=seed,
         step=int(status.stepnum), cell_factor=float(sim.get('gpu_cell_factor', 1.0)),
         skin=sim.get('gpu_skin', None), rigid_rod=float(getattr(pop, "rigid_rod_projection_factor", 0.0)))
-    g = _gpu_state(pop, sim, dim, precision, params)
+    g = _gpu_state(pop, sim, dim, precision, params, srk_order)
     st, eng = g.state, g.engine
 
     # upload the host state (the caller may have changed it between calls)
@@ -250,7 +254,7 @@ def SRK2_force_calc(pops, status, sim):
         pop._gcr_cell_depth, pop._gcr_list_depth = depth, ldepth
         st.params.step = int(res['step'])
         g.make_engine(st.params, depth, ldepth)
-        g.key = _key(pop, dim, precision, params, depth, ldepth)
+        g.key = _key(pop, dim, precision, params, depth, ldepth, srk_order)
         eng = g.engine
     steps_done = done
     if mode == 'mt' and steps_done < n_noise:
@@ -263,11 +267,15 @@ def SRK2_force_calc(pops, status, sim):
     g.h_pos1.copy_(st.pos1, non_blocking=True)
     g.h_tan.copy_(st.tangent, non_blocking=True)
     g.h_frc.copy_(st.forces, non_blocking=True)
+    if g.h_faux is not None:
+        g.h_faux.copy_(st.forces_aux, non_blocking=True)
     torch.cuda.synchronize(eng.device)
     pop.pos[:] = g.h_pos.numpy()
     pop.pos1[:] = g.h_pos1.numpy()
     pop.tangent_list[:] = g.h_tan.numpy()
     pop.forces[:] = g.h_frc.numpy()
+    if g.h_faux is not None and getattr(pop, "forces_aux", np.empty((0, 0))).shape == pop.forces.shape:
+        pop.forces_aux[:] = g.h_faux.numpy()
 
     # write-back, updates.py:249-256
     status.dt = dt

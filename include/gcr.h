@@ -15,7 +15,8 @@
  *
  * Reference interfaces replaced (paths inside the reference project):
  *   gcr_run / gcr_call_begin  <- updates.SRK2_force_calc   updates.py:132-267
- *                                (the SRK.SRK_jit loop      SRK.py:13-484)
+ *                                (the SRK.SRK_jit loop      SRK.py:13-484; SRK2, and SRK4
+ *                                with gcr_config.srk_order = 4)
  *   pair rule                 <- force_rules.central_pair_force_rule = forces.WCA
  *                                                           force_rules.py:3, forces.py:13-15
  *   gcr_system_desc packing   <- populations.make_WCA_params populations.py:48-58,
@@ -80,6 +81,7 @@ typedef struct {
     int32_t steps_per_graph;  /* SRK2 steps per captured CUDA graph (1..64) */
     int32_t ctas_per_sm;      /* persistent CTAs per SM (0 = from occupancy, <0 = one CTA per tile) */
     int32_t list_depth;       /* neighbour-list slots per bead, 4..1024 (0 = 32 in 2D, 96 in 3D) */
+    int32_t srk_order;        /* config.SRK_order: 2 (0 = 2) or 4 (SRK.py:144-215, 296-321) */
 } gcr_config;
 
 /* One system.  The packed arrays follow the reference's packing exactly. */
@@ -116,6 +118,8 @@ typedef struct {
     void *forces;               /* [n, dim] FP64 or FP32 (precision) */
     const int32_t *chain_id;    /* [n] chain index; chains are contiguous ranges */
     const double *rest_lengths; /* [n_chains] */
+    void *forces_aux;           /* SRK4: [n, dim] FP64 or FP32, the force of the last stage
+                                   (pop.forces_aux); NULL: library scratch.  Unused by SRK2 */
 } gcr_system_buffers;
 
 /* Limits and inputs of one SRK2_force_calc call for one system. */
@@ -185,7 +189,7 @@ GCR_API int gcr_synchronize(gcr_ctx *ctx);
  * ms_out[0..6] receive the total milliseconds of: cell list of pos (scans and
  * pack), pair forces at pos, stage 0, cell list of pos1, pair forces at
  * pos1, stage 1 with the dt rule, update with the step bookkeeping.  For
- * profiling; the results equal gcr_run's. */
+ * profiling; the results equal gcr_run's.  SRK2 contexts only. */
 GCR_API int gcr_profile_steps(gcr_ctx *ctx, int32_t n_steps, float *ms_out);
 
 /* ---- observables and exports ------------------------------------------ */

@@ -30,6 +30,8 @@ def pop_from_golden(d, s):
     pop = pop_from_arrays(d["pos0"], d["tangent0"], d["chain_id"], d["rest_lengths"], d["spring_params"],
                           d["wca_params"], d["active_params"], s["D"], s["Dr"], s["radius"], s["n_nearby"])
     pop.rigid_rod_projection_factor = float(s.get("rigid_rod", 0.0))
+    if s.get("srk_order", 2) == 4:
+        pop.forces_aux = np.zeros_like(pop.pos)
     return pop
 
 
@@ -49,7 +51,7 @@ def set_pop_params(pop, spring, wca, active, D, Dr, radius, n_nearby, rest_lengt
 def set_config(s):
     config.dim = int(s["dim"])
     config.Lx = float(s["L"])
-    config.SRK_order = 2
+    config.SRK_order = int(s.get("srk_order", 2))
     config.n_steps_update_grid_list = int(s["n_steps_update"])
     config.max_dist_per_step = float(s["max_dist_per_step"])
     config.RK_cheat_factor = float(s["rk_cheat"])

@@ -37,6 +37,12 @@ def _replay(name, precision="fp64"):
         snap = status_from_row(d["status_before"][ci])
         snap.__dict__.update(st.__dict__)
         results.append((ci, snap, pop.pos.copy(), pop.tangent_list.copy(), pop.forces.copy()))
+        if s.get("srk_order", 2) == 4:
+            # the last stage's force (pop.forces_aux), SRK4 only
+            ref_a = d[f"call{ci}_forces_aux"]
+            tol = TRAJ_TOL[name][ci]
+            if tol is not None:
+                assert np.max(np.abs(pop.forces_aux - ref_a)) <= max(1e3 * tol, 1e-6) * np.max(np.abs(ref_a))
     return d, s, results
 
 

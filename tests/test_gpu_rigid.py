@@ -198,10 +198,14 @@ def test_update_desc_regrids_within_reserved_cells():
             b.engine.update_params(b.states[0])
         b.begin(60, dt=1e-3)
         b.run(60)
+        st = b.statuses()[0]
+        assert st["steps_done"] == 60 and st["flags"] == 0, st
         out = b.states[0].pos.cpu().numpy()
         b.close()
         return out
 
     # a smaller skin keeps the grid; a larger one takes fewer, larger cells
     for start, new in ((0.3, 0.1), (0.3, 0.9)):
-        assert np.array_equal(fresh(new, start_skin=start), fresh(new))
+        a, b = fresh(new, start_skin=start), fresh(new)
+        assert np.array_equal(a, b)
+        assert np.max(np.abs(a - pos.cpu().numpy())) > 1e-6  # the steps ran
