@@ -17,6 +17,7 @@ ERRORS = {-1: "BAD_ARG", -2: "CUDA", -3: "OOM", -4: "NONFINITE", -5: "TIMEOUT", 
           -7: "STATE", -8: "OVERFLOW"}
 GCR_FP64, GCR_MIXED = 0, 1
 FLAG_CELL_OVERFLOW, FLAG_NONFINITE, FLAG_NEXT_OVERFLOW, FLAG_LIST_CORRUPT, FLAG_LIST_OVERFLOW = 1, 2, 4, 8, 16
+FLAG_SERIES_FULL = 32
 
 
 class GcrError(RuntimeError):
@@ -49,13 +50,14 @@ class SystemBuffers(C.Structure):
 
 class Call(C.Structure):
     _fields_ = [("max_steps", C.c_int64), ("max_dt_usable", C.c_double), ("dt", C.c_double),
-                ("noise", C.c_void_p), ("noise_steps", C.c_int64)]
+                ("noise", C.c_void_p), ("noise_steps", C.c_int64), ("series", C.c_void_p),
+                ("series_every", C.c_int64), ("series_phase", C.c_int64), ("series_capacity", C.c_int64)]
 
 
 class Status(C.Structure):
     _fields_ = [("dt", C.c_double), ("dt_used", C.c_double), ("max_forces_strength", C.c_double),
                 ("steps_done", C.c_int64), ("step", C.c_int64), ("flags", C.c_int32), ("active", C.c_int32),
-                ("list_builds", C.c_int64)]
+                ("list_builds", C.c_int64), ("series_rows", C.c_int64)]
 
 
 # exported symbols and their signatures (every declaration of include/gcr.h)

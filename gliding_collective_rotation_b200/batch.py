@@ -110,6 +110,7 @@ class Batch:
         torch.cuda.synchronize(self.device)
         self.engine = None
         self._carry_dt = None  # dts to hand to the next call after a regrow
+        self.series_buf = None
         self._make_engine()
 
     def _make_engine(self):
@@ -151,15 +152,31 @@ class Batch:
         self._make_engine()
 
     # -- calls -------------------------------------------------------------------
-    def begin(self, max_steps, dt=None, max_dist_per_step=None, max_dt_usable=-1.0):
+    def begin(self, max_steps, dt=None, max_dist_per_step=None, max_dt_usable=-1.0, series_every=0):
         """Arm every system for the next run (one SRK2_force_calc call each).
         Without `dt` each system keeps the dt its last step chose, as the
-        reference's status.dt carries from call to call."""
+        reference's status.dt carries from call to call.  With
+        `series_every`, the device records the order parameters of every
+        system after every `series_every` steps of the call (``series``)."""
         for st in self.states:
             if max_dist_per_step is not None and st.params.max_dist_per_step != max_dist_per_step:
                 st.params.max_dist_per_step = max_dist_per_step
                 self.engine.update_params(st)
-        self.engine.call_begin_many([st.slot for st in self.states], max_steps, self._dts(dt), max_dt_usable)
+        self.series_buf = None
+        if series_every > 0:
+            rows = int(np.max(max_steps)) // series_every + 1
+            self.series_buf = torch.zeros((len(self.states), rows, 5), dtype=torch.float64, device=self.device)
+        self.engine.call_begin_many([st.slot for st in self.states], max_steps, self._dts(dt), max_dt_usable,
+                                    series=self.series_buf, series_every=series_every)
+
+    def series(self):
+        """Rows (step, time in the call, P, S, director angle) recorded on
+        the device in the last call, per system."""
+        if self.series_buf is None:
+            return [np.zeros((0, 5)) for _ in self.states]
+        rows = [s["series_rows"] for s in self.statuses()]
+        buf = self.series_buf.cpu().numpy()
+        return [buf[i, :r].copy() for i, r in enumerate(rows)]
 
     def _dts(self, dt=None):
         """Per-system dt of the next call: `dt`, else the dts carried over a

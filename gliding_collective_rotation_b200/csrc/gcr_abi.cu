@@ -144,6 +144,8 @@ struct gcr_ctx {
     int grid_stage0 = 1, grid_stage1 = 1, grid_stage4[4] = {1, 1, 1, 1};
     cudaGraphExec_t graph = nullptr;
     bool graph_rigid = false;  // the graph holds the rigid-rod projection kernels
+    bool graph_obs = false;    // the graph holds the series kernel
+    void *observe = nullptr;   // k_observe of the context's precision
     bool tiles_dirty = true;
 };
 
@@ -299,6 +301,15 @@ bool any_rigid(const gcr_ctx *c)
     return false;
 }
 
+// some resident system's call records a series (the host mirror of the
+// state table is current after every gcr_call_begin)
+bool any_series(const gcr_ctx *c)
+{
+    for (size_t s = 0; s < c->slots.size(); s++)
+        if (c->slots[s].used && c->hS[s].series) return true;
+    return false;
+}
+
 int launch(gcr_ctx *c, void *fn, int grid, int block, size_t smem = 0)
 {
     void *a[] = {&c->args};
@@ -328,6 +339,15 @@ int enqueue_lists(gcr_ctx *c, int which)
     return launch(c, build, c->grid_build, bb);
 }
 
+// the in-graph order-parameter series: one 1024-thread CTA per slot
+int launch_observe(gcr_ctx *c)
+{
+    int dim = c->cfg.dim;
+    void *a[] = {&c->args, &dim};
+    GCR_CUDA(cudaLaunchKernel(c->observe, dim3((unsigned)c->slots.size()), dim3(1024), a, 0, c->stream));
+    return GCR_OK;
+}
+
 // one SRK4 step (SRK.py:166-215): four force evaluations at pos, pos1, pos2,
 // pos1, each with its lists; the virtual updates alternate pos1 / pos2
 int enqueue_step4(gcr_ctx *c)
@@ -345,7 +365,8 @@ int enqueue_step4(gcr_ctx *c)
     if ((rc = launch_sys(c, c->ks.sys_dt))) return rc;
     if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
     if (c->graph_rigid && (rc = launch(c, c->ks.rigid4[3], c->grid_update, bb))) return rc;
-    return launch_sys(c, c->ks.sys_end);
+    if ((rc = launch_sys(c, c->ks.sys_end))) return rc;
+    return c->graph_obs ? launch_observe(c) : GCR_OK;
 }
 
 int enqueue_step(gcr_ctx *c)
@@ -364,7 +385,7 @@ int enqueue_step(gcr_ctx *c)
     if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
     if (c->graph_rigid && (rc = launch(c, c->ks.rigid1, c->grid_update, bb))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_end))) return rc;
-    return GCR_OK;
+    return c->graph_obs ? launch_observe(c) : GCR_OK;
 }
 
 // start of a run: zero the cell counts, flag every system for a list build
@@ -376,15 +397,17 @@ int enqueue_run_start(gcr_ctx *c)
 
 int build_graph(gcr_ctx *c)
 {
-    // the projection kernels are in the graph only while some system uses it
-    const bool rigid = any_rigid(c);
-    if (c->graph && rigid != c->graph_rigid) {
+    // the projection and series kernels are in the graph only while some
+    // system uses them
+    const bool rigid = any_rigid(c), obs = any_series(c);
+    if (c->graph && (rigid != c->graph_rigid || obs != c->graph_obs)) {
         GCR_CUDA(cudaStreamSynchronize(c->stream));
         cudaGraphExecDestroy(c->graph);
         c->graph = nullptr;
     }
     if (c->graph) return GCR_OK;
     c->graph_rigid = rigid;
+    c->graph_obs = obs;
     cudaGraph_t g = nullptr;
     GCR_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = GCR_OK;
@@ -477,6 +500,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
         c->own_stream = true;
     }
     c->ks = kernel_set(cfg.dim, cfg.precision);
+    c->observe = observe_kernel(cfg.precision);
     const int64_t S = cfg.system_capacity;
     c->max_bead_tiles = cfg.bead_capacity / cfg.block_beads + S;
     c->max_cell_tiles = cfg.cell_capacity / cfg.block_cells + S;
@@ -720,6 +744,8 @@ int check_call(const gcr_call *call)
     if (call->noise && call->max_steps < 0) return fail(GCR_ERR_BAD_ARG, "injected noise needs a step limit");
     if (call->noise && call->max_steps > call->noise_steps)
         return fail(GCR_ERR_BAD_ARG, "fewer injected noise steps than the step limit");
+    if (call->series && (call->series_every <= 0 || call->series_capacity <= 0 || call->series_phase < 0))
+        return fail(GCR_ERR_BAD_ARG, "a series needs series_every > 0, series_phase >= 0, series_capacity > 0");
     return GCR_OK;
 }
 
@@ -737,6 +763,12 @@ void arm(SysS &s, const gcr_call *call)
     s.max_dt_usable = call->max_dt_usable;
     s.noise = call->noise;
     s.noise_steps = call->noise_steps;
+    s.series = call->series;
+    s.series_every = call->series ? call->series_every : 0;
+    s.series_phase = call->series ? call->series_phase : 0;
+    s.series_cap = call->series ? call->series_capacity : 0;
+    s.series_rows = 0;
+    s.series_mark = 0;
     s.flags = 0;
     s.active = ((0 < s.max_steps || s.max_steps < 0) && (0.0 < s.max_dt_usable || s.max_dt_usable < 0.0)) ? 1 : 0;
 }
@@ -887,6 +919,7 @@ int gcr_get_status(gcr_ctx *c, int32_t slot, gcr_status *out)
     out->flags = s.flags;
     out->active = s.active;
     out->list_builds = s.list_builds;
+    out->series_rows = s.series_rows;
     return GCR_OK;
 }
 

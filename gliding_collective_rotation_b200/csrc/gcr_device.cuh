@@ -36,6 +36,7 @@ constexpr int kFlagNonFinite = 2;
 constexpr int kFlagNextOverflow = 4;
 constexpr int kFlagListCorrupt = 8;  // an inconsistent cell or neighbour list was detected and not used
 constexpr int kFlagListOverflow = 16;  // more list partners of a bead than the list depth
+constexpr int kFlagSeriesFull = 32;    // the series buffer was full (not fatal)
 // a system with one of these stops: every kernel skips it until re-armed
 constexpr int kFlagFatal = kFlagCellOverflow | kFlagNonFinite | kFlagListCorrupt | kFlagListOverflow;
 
@@ -97,6 +98,12 @@ struct SysS {
     int32_t rebuild;      // the neighbour list must be rebuilt before the next pair kernel
     int32_t pad0;
     int64_t list_builds;  // neighbour-list builds since admission
+    double *series;       // order-parameter rows of the call (step, elapsed, P, S, angle) or nullptr
+    int64_t series_every;
+    int64_t series_phase;
+    int64_t series_cap;
+    int64_t series_rows;
+    int64_t series_mark;  // steps_done of the last row
 };
 
 struct Tile {

@@ -74,6 +74,8 @@ cudaError_t launch_reference_lists(int dim, const SysP &p, int64_t n_grid, int64
                                    int64_t *nbor_list, int64_t nbor_depth1, int *d_err, cudaStream_t st);
 cudaError_t launch_order_params(int dim, int precision, const SysP &p, const int32_t *chain_start,
                                 double *d_out, cudaStream_t st);
+// k_observe<FT>(BatchArgs, int dim): the in-graph order-parameter series, one 1024-thread CTA per slot
+void *observe_kernel(int precision);
 // chain_start[n_chains + 1]; d_err[0] |= 4 on bad chain ids, d_err[1] = longest chain
 cudaError_t launch_chain_starts(const int32_t *chain, int n, int n_chains, int32_t *chain_start, int *d_err,
                                 cudaStream_t st);

@@ -231,9 +231,11 @@ cudaError_t launch_reference_lists(int dim, const SysP &p, int64_t n_grid, int64
 // order parameters: one block per system, fixed reduction order
 // ---------------------------------------------------------------------------
 template <typename FT>
-__global__ void k_order(int dim, const FT *__restrict__ tan, const int32_t *__restrict__ cs, int n_chains,
-                        double *out)
+__device__ void order_params_block(int dim, const FT *__restrict__ tan, const int32_t *__restrict__ cs,
+                                   int n_chains, double *out)
 {
+    // one CTA of 1024 threads, a fixed reduction tree: the same bits from
+    // gcr_order_params and from the in-graph series
     __shared__ double sh[4][1024];
     double ex = 0.0, ey = 0.0, q11 = 0.0, q12 = 0.0;
     for (int c = threadIdx.x; c < n_chains; c += blockDim.x) {
@@ -266,6 +268,51 @@ __global__ void k_order(int dim, const FT *__restrict__ tan, const int32_t *__re
         out[1] = Sf / (double)n_chains;
         out[2] = atan((Sf - sh[2][0]) / sh[3][0]);
     }
+}
+
+template <typename FT>
+__global__ void __launch_bounds__(1024) k_order(int dim, const FT *__restrict__ tan, const int32_t *__restrict__ cs,
+                                                int n_chains, double *out)
+{
+    order_params_block<FT>(dim, tan, cs, n_chains, out);
+}
+
+// The in-graph series: one CTA per slot after each step; a system whose call
+// asked for a series and whose step count in the call, plus the call's phase,
+// has just reached a multiple of series_every appends (step, elapsed, P, S,
+// angle).  Every thread of a CTA reads the same state words (the step kernels
+// are done), so all take one branch.
+template <typename FT>
+__global__ void __launch_bounds__(1024) k_observe(BatchArgs A, int dim)
+{
+    const int i = blockIdx.x;
+    if (i >= A.n_slots) return;
+    const SysP &p = A.P[i];
+    SysS &s = A.S[i];
+    if (!s.series || s.series_every <= 0 || s.steps_done == 0 || s.steps_done == s.series_mark) return;
+    if ((s.steps_done + s.series_phase) % s.series_every != 0 || (s.flags & kFlagFatal)) return;
+    __shared__ double row[3];
+    order_params_block<FT>(dim, reinterpret_cast<const FT *>(p.tan), p.chain_start, p.n_chains, row);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        s.series_mark = s.steps_done;
+        if (s.series_rows < s.series_cap) {
+            double *r = s.series + (size_t)s.series_rows * 5;
+            r[0] = (double)s.step;
+            r[1] = s.elapsed;
+            r[2] = row[0];
+            r[3] = row[1];
+            r[4] = row[2];
+            s.series_rows += 1;
+        } else {
+            s.flags |= kFlagSeriesFull;
+        }
+    }
+}
+
+void *observe_kernel(int precision)
+{
+    return precision == 0 ? (void *)k_observe<double> : (void *)k_observe<float>;
 }
 
 cudaError_t launch_order_params(int dim, int precision, const SysP &p, const int32_t *chain_start,

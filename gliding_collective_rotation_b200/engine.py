@@ -229,16 +229,30 @@ class Engine:
         torch.cuda.current_stream(self.device).synchronize()
         check(self.lib.gcr_call_begin(self._ctx, int(slot), C.byref(c)))
 
-    def call_begin_many(self, slots, max_steps, dts, max_dt_usable=-1.0):
-        """Arm many systems with one copy of the state table each way."""
+    def call_begin_many(self, slots, max_steps, dts, max_dt_usable=-1.0, series=None, series_every=0,
+                        series_phase=0):
+        """Arm many systems with one copy of the state table each way.
+        ``series``: a float64 device tensor [len(slots), rows, 5] that
+        receives, on the device, (step, time in the call, P, S, angle) after
+        each step k of the call with (k + phase) % series_every == 0."""
         n = len(slots)
         calls = (Call * n)()
         arr = (C.c_int32 * n)(*[int(s) for s in slots])
+        if series is not None:
+            assert series.dtype == torch.float64 and series.is_cuda and series.is_contiguous()
+            assert series.shape[0] >= n and series.shape[2] == 5
+            self._series_ref = series  # keep alive while in use
         for i in range(n):
             calls[i].max_steps = int(max_steps[i] if np.ndim(max_steps) else max_steps)
             calls[i].max_dt_usable = float(max_dt_usable[i] if np.ndim(max_dt_usable) else max_dt_usable)
             calls[i].dt = float(dts[i] if np.ndim(dts) else dts)
             calls[i].noise, calls[i].noise_steps = None, 0
+            every = int(series_every[i] if np.ndim(series_every) else series_every)
+            if series is not None and every > 0:
+                calls[i].series = series[i].data_ptr()
+                calls[i].series_every = every
+                calls[i].series_phase = int(series_phase[i] if np.ndim(series_phase) else series_phase)
+                calls[i].series_capacity = series.shape[1]
         torch.cuda.current_stream(self.device).synchronize()
         check(self.lib.gcr_call_begin_batch(self._ctx, n, arr, calls))
 
@@ -273,7 +287,7 @@ class Engine:
         check(self.lib.gcr_get_status(self._ctx, int(slot), C.byref(s)))
         return {"dt": s.dt, "dt_used": s.dt_used, "max_forces_strength": s.max_forces_strength,
                 "steps_done": s.steps_done, "step": s.step, "flags": s.flags, "active": bool(s.active),
-                "list_builds": s.list_builds}
+                "list_builds": s.list_builds, "series_rows": s.series_rows}
 
     # -- observables and exports --------------------------------------------
     def order_params(self, slot):

@@ -21,9 +21,11 @@ under the adaptive rule first (until the step takes the full dt), reported
 apart from the requested steps.  Each system's dt carries from call to call,
 as the reference's ``status.dt`` does.
 
-Calls are chunked: every system is armed for at most ``chunk`` steps (and
-never past its next observation step), the graph runs, statuses come back in
-one copy, finished requests leave.  With a fixed dt a system's trajectory
+Calls are chunked: every system is armed for at most ``chunk`` steps, the
+graph runs, statuses come back in one copy, finished requests leave.  The
+order parameters are sampled on the device inside the steps' graph (the
+call's series, counted from the request's first step), so a chunk does not
+stop at observation steps and a sample costs no host round trip.  With a fixed dt a system's trajectory
 does not depend on how its steps are split into calls (the Philox noise is
 keyed by bead and step, and the pair sums are taken in a fixed order), so a
 request served in a busy mix ends bit-for-bit where it ends alone.
@@ -105,6 +107,7 @@ class Server:
         self.dim, self.precision = dim, precision
         self.device = torch.device(device or "cuda")
         self.chunk = int(chunk)
+        self._series = None  # device rows of the in-graph order-parameter series
         self.relax_max_steps = int(relax_max_steps)
         self.max_head_wait = float(max_head_wait)
         self.cell_depth = cell_depth or default_depth(dim, 1.3)  # cells of side r_cut + skin
@@ -201,20 +204,38 @@ class Server:
     def _plan(self, lv: _Live):
         if lv.relaxing:
             return min(self.chunk, self.relax_max_steps - lv.relax_steps)
-        left = lv.req.steps - lv.done
-        k = min(self.chunk, left)
-        if lv.req.obs_every > 0:
-            k = min(k, lv.req.obs_every - lv.done % lv.req.obs_every)
-        return k
+        return min(self.chunk, lv.req.steps - lv.done)
 
     def _round(self):
         slots = sorted(self.live)
         plan = [self._plan(self.live[s]) for s in slots]
         # each system's dt carries from call to call (the reference's status.dt)
         dts = [self.live[s].dt if self.live[s].dt is not None else self.live[s].req.spec.dt for s in slots]
-        self.engine.call_begin_many(slots, plan, dts)
+        # the order parameters are sampled on the device, inside the steps'
+        # graph, every obs_every steps counted from the request's start
+        every = [0 if self.live[s].relaxing else max(0, self.live[s].req.obs_every) for s in slots]
+        phase = [self.live[s].done % e if e > 0 else 0 for s, e in zip(slots, every)]
+        series = None
+        if any(every):
+            rows = max(k // e + 1 for k, e in zip(plan, every) if e > 0)
+            if self._series is None or self._series.shape[0] < len(slots) or self._series.shape[1] < rows:
+                self._series = torch.zeros((max(self.max_systems, len(slots)), max(rows, self.chunk + 1), 5),
+                                           dtype=torch.float64, device=self.device)
+            series = self._series
+        self.engine.call_begin_many(slots, plan, dts, series=series, series_every=every, series_phase=phase)
         self.engine.run(max(plan))
         statuses = {s: self.engine.status(s) for s in slots}
+        rows_host = None
+        if series is not None and any(statuses[s]["series_rows"] for s in slots):
+            rows_host = series.cpu().numpy()
+        for i, s in enumerate(slots):
+            st, lv = statuses[s], self.live[s]
+            if rows_host is None or not st["series_rows"]:
+                continue
+            # a row's global step -> steps of the request
+            start = st["step"] - st["steps_done"]
+            for r in rows_host[i, :st["series_rows"]]:
+                lv.series.append((lv.done + int(r[0]) - start, r[2], r[3], r[4]))
         finished, overflow = [], False
         for s, k in zip(slots, plan):
             lv, st = self.live[s], statuses[s]
@@ -242,8 +263,6 @@ class Server:
             if st["flags"] or n_done < k:
                 finished.append(s)  # a failed system leaves with its flags
                 continue
-            if lv.req.obs_every > 0 and lv.done % lv.req.obs_every == 0:
-                lv.series.append((lv.done, *self.engine.order_params(s)))
             if lv.done >= lv.req.steps:
                 finished.append(s)
         for s in finished:

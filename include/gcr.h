@@ -66,6 +66,7 @@ extern "C" {
 #define GCR_FLAG_NEXT_OVERFLOW 4   /* reserved (no longer raised) */
 #define GCR_FLAG_LIST_CORRUPT 8    /* an inconsistent cell or neighbour list was detected and not used */
 #define GCR_FLAG_LIST_OVERFLOW 16  /* more list partners of a bead than list_depth */
+#define GCR_FLAG_SERIES_FULL 32    /* the order-parameter series buffer was full (rows dropped; not fatal) */
 
 typedef struct gcr_ctx gcr_ctx;
 
@@ -131,6 +132,14 @@ typedef struct {
     const double *noise;        /* injected noise_vec snapshots [noise_steps][n][2*dim],
                                    device memory, or NULL for the Philox stream */
     int64_t noise_steps;
+    double *series;             /* device buffer of series_capacity rows (step, time elapsed in
+                                   the call, P, S, director angle): a row is appended on the
+                                   device after each step k of the call with
+                                   (k + series_phase) % series_every == 0, the order parameters
+                                   of gcr_order_params (global_op-chiral.py:24-30); NULL: none */
+    int64_t series_every;
+    int64_t series_phase;
+    int64_t series_capacity;
 } gcr_call;
 
 /* What SRK2_force_calc writes back (shared_arr[0], updates.py:249-256). */
@@ -143,6 +152,7 @@ typedef struct {
     int32_t flags;              /* GCR_FLAG_* */
     int32_t active;             /* still running (limits not reached) */
     int64_t list_builds;        /* neighbour-list builds since admission */
+    int64_t series_rows;        /* rows appended to the call's series */
 } gcr_status;
 
 /* ---- context ---------------------------------------------------------- */

@@ -67,3 +67,36 @@ def test_observables_after_steps_match_the_oracle():
         want = OB.correlation(want_com, L, k, 0.5, p1, p2)
         assert got.shape == want.shape and np.allclose(got, want, rtol=1e-9, atol=1e-8), kind
     b.close()
+
+
+def test_series_recorded_in_the_graph_equals_order_params():
+    """The in-graph series (gcr_call.series) holds, bit for bit, what
+    gcr_order_params returns at the same steps, and recording it does not
+    change the trajectory."""
+    import copy
+    first, base = _batch("fp64")
+    first.close()
+
+    def fresh():
+        b = Batch([copy.deepcopy(base)], "fp64")
+        b.run_checked(5)
+        return b
+
+    b = fresh()
+    step0 = b.statuses()[0]["step"]
+    b.begin(100, series_every=25)
+    b.run(100)
+    rows = b.series()[0]
+    assert rows.shape == (4, 5)
+    assert list(rows[:, 0] - step0) == [25, 50, 75, 100]
+    assert np.array_equal(rows[-1, 2:], b.engine.order_params(b.states[0].slot))
+    pos_series = b.states[0].pos.cpu().numpy()
+    b.close()
+    c = fresh()
+    c.begin(25)
+    c.run(25)
+    assert np.array_equal(rows[0, 2:], c.engine.order_params(c.states[0].slot))
+    c.begin(75)
+    c.run(75)
+    assert np.array_equal(c.states[0].pos.cpu().numpy(), pos_series)
+    c.close()

@@ -4,6 +4,7 @@ engine that advances step counters instead of beads."""
 import math
 
 import numpy as np
+import torch
 import pytest
 
 from gliding_collective_rotation_b200 import serve as S
@@ -44,10 +45,15 @@ class FakeEngine:
     def update_params(self, st):
         assert st.slot in self.sys
 
-    def call_begin_many(self, slots, max_steps, dts):
-        for s, k, dt in zip(slots, max_steps, dts):
+    def call_begin_many(self, slots, max_steps, dts, series=None, series_every=0, series_phase=0):
+        for i, (s, k, dt) in enumerate(zip(slots, max_steps, dts)):
             v = self.sys[s]
-            v.update(armed=int(k), done=0, flags=0, dt_call=dt)
+            every = int(series_every[i] if np.ndim(series_every) else series_every)
+            phase = int(series_phase[i] if np.ndim(series_phase) else series_phase)
+            # the device series: a row after each step j of the call with
+            # (j + phase) % every == 0, in row i of `series`
+            v.update(armed=int(k), done=0, flags=0, dt_call=dt, rows=0,
+                     series=(series, i, every, phase) if series is not None and every > 0 else None)
 
     def run(self, n):
         self.runs.append(n)
@@ -57,6 +63,13 @@ class FakeEngine:
                 d //= 2
                 v["flags"] = FLAG_CELL_OVERFLOW
                 self.overflow_once = None
+            if v.get("series") is not None:
+                buf, row, every, phase = v["series"]
+                for j in range(1, d + 1):
+                    if (j + phase) % every == 0 and v["rows"] < buf.shape[1]:
+                        step = v["step"] + j
+                        buf[row, v["rows"]] = torch.tensor([step, 0.0, step * 1e-3, 0.5, 0.25], dtype=torch.float64)
+                        v["rows"] += 1
             v["done"] = d
             v["step"] += d
             relaxing = math.isfinite(v["st"].params.max_dist_per_step)
@@ -71,7 +84,7 @@ class FakeEngine:
     def status(self, slot):
         v = self.sys[slot]
         return {"dt": v["dt"], "dt_used": v["dt"], "max_forces_strength": 0.0, "steps_done": v["done"],
-                "step": v["step"], "flags": v["flags"], "active": False}
+                "step": v["step"], "flags": v["flags"], "active": False, "series_rows": v.get("rows", 0)}
 
     def order_params(self, slot):
         return np.array([self.sys[slot]["step"] * 1e-3, 0.5, 0.25])
@@ -113,10 +126,10 @@ def test_every_request_runs_exactly_its_steps_with_observations():
     for r in res:
         want = reqs[r.id].steps
         assert r.steps == want and r.flags == 0 and r.relax_steps == 0
-        # an observation at every multiple of 50, none past the end
+        # an observation at every multiple of 50 of the request's steps, none
+        # past the end, although calls of 64 steps cross them
         assert list(r.series[:, 0]) == list(range(50, want + 1, 50))
-    # a chunk never crosses an observation step
-    assert max(srv.engines[0].runs) <= 64
+    assert max(srv.engines[0].runs) == 64
 
 
 def test_relaxation_comes_first_and_is_counted_apart():
