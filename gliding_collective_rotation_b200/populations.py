@@ -6,8 +6,9 @@ class names, attribute names, parameter packing (``make_WCA_params``,
 ``spring_params``, ``active_params``, ``self_interactions``) and the same
 order of numpy random draws in construction and ``random_initialization``,
 so that a seed gives the reference's initial state.  Motors, shells,
-growth/division, special interactions and the init-grow protocol are not
-mirrored.
+growth/division and special interactions are not mirrored; the init-grow
+protocol (``set_init_grow`` / ``early_time_procedures`` / ``end_init_grow``)
+is restated as a schedule in ``growth.py``.
 """
 from __future__ import annotations
 
