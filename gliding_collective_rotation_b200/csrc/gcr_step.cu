@@ -72,6 +72,7 @@ struct StageSmem {
     BT *bf;        // [TB+3]    spring magnitude k (a/|d| - 1), 0 when |d| = 0
     BT *fw;        // [TB+2][D] bend "forward" term at bead begin-1+k
     BT *bw;        // [TB+2][D] bend "backward" term
+    BT *ra;        // [TB+4]    rest length of the bead's chain
     __device__ void carve(unsigned char *base, int TB)
     {
         x = reinterpret_cast<double *>(base);
@@ -80,7 +81,8 @@ struct StageSmem {
         bf = bt + (size_t)(TB + 3) * D;
         fw = bf + (TB + 3);
         bw = fw + (size_t)(TB + 2) * D;
-        tp = reinterpret_cast<uint8_t *>(bw + (size_t)(TB + 2) * D);
+        ra = bw + (size_t)(TB + 2) * D;
+        tp = reinterpret_cast<uint8_t *>(ra + (TB + 4));
     }
 };
 
@@ -89,7 +91,7 @@ size_t stage_smem_bytes(int TB)
 {
     using BT = typename Bonded<FT>::type;
     return (size_t)(TB + 4) * D * sizeof(double) + (size_t)(TB + 3) * (2 * D + 1) * sizeof(BT) +
-           (size_t)(TB + 2) * 2 * D * sizeof(BT) + (size_t)(TB + 4) + 16;
+           (size_t)(TB + 2) * 2 * D * sizeof(BT) + (size_t)(TB + 4) * sizeof(BT) + (size_t)(TB + 4) + 16;
 }
 
 // 1/sqrt(x): FP64 exactly as written in the reference; FP32 (mixed path) by
@@ -664,11 +666,28 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
 #pragma unroll
                 for (int i = 0; i < D; i++) sm.x[k * D + i] = __ldg(X + (size_t)m * D + i);
                 sm.tp[k] = A.topo[p.bead_off + m];
+                sm.ra[k] = p.calc_springs ? (BT)__ldg(p.rest + __ldg(p.chain + m)) : BT(0);
             } else {
                 sm.tp[k] = 0;
+                sm.ra[k] = BT(0);
             }
         }
         __syncthreads();
+        // the bead's own inputs of phase 4, loaded before the barriers
+        FT pre_t[D], pre_f[D], pre_p[D];
+        {
+            const int bq = tl.begin + (int)threadIdx.x;
+            const bool ok = bq < n;
+            const FT *tq = reinterpret_cast<const FT *>(p.tan);
+            const FT *fq = reinterpret_cast<const FT *>(p.frc);
+            const FT *pq = reinterpret_cast<const FT *>(A.fp) + (size_t)(p.bead_off + (ok ? bq : 0)) * D;
+#pragma unroll
+            for (int i = 0; i < D; i++) {
+                pre_t[i] = ok ? tq[(size_t)bq * D + i] : FT(0);
+                pre_f[i] = (ok && STAGE == 1) ? fq[(size_t)bq * D + i] : FT(0);
+                pre_p[i] = (ok && p.calc_wca) ? pq[i] : FT(0);
+            }
+        }
         const bool springs = p.calc_springs, cb = p.calc_bend;
         if (springs) {
             // 2. every bond (j, j+1) of the tile once
@@ -685,7 +704,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                         r2 += d[i] * d[i];
                     }
                     if (r2 != BT(0)) {
-                        const BT a = (BT)__ldg(p.rest + __ldg(p.chain + base + k));
+                        const BT a = sm.ra[k];
                         BT inv = inv_sqrt<BT>(r2);
                         f = kspring * (a * inv - BT(1));
 #pragma unroll
@@ -742,8 +761,8 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
 #pragma unroll
             for (int i = 0; i < D; i++) {
                 // the SRK2 corrector adds to F0; every other stage starts from 0
-                Fb[i] = STAGE == 1 ? (BT)frc[(size_t)b * D + i] : BT(0);
-                tg[i] = tan[(size_t)b * D + i];
+                Fb[i] = STAGE == 1 ? (BT)pre_f[i] : BT(0);
+                tg[i] = pre_t[i];
             }
             bool tang_set = false;
             if (springs) {
@@ -798,9 +817,8 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
 #pragma unroll
             for (int i = 0; i < D; i++) F[i] = (FT)Fb[i];
             if (p.calc_wca) {
-                const FT *fp = reinterpret_cast<const FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
 #pragma unroll
-                for (int i = 0; i < D; i++) F[i] += fp[i];
+                for (int i = 0; i < D; i++) F[i] += pre_p[i];
             }
             if (p.self_propel) {
                 const FT v0 = (FT)p.v0;
