@@ -115,6 +115,13 @@ CASES = {
                  dtmax=5e-4, t_init_grow=0., a_init_factor=1.0),
         dt=None, fixed_dt=False, calls=[1, 19, 80], noise_seed=71, save_every=None,
         init_grow=False, relax_steps=200),
+    # 3D growth: config-5 physics (LJ eps 1, kappa 10, Dr 0.1, T 0.05) on a
+    # small box, grown by the reference's own init-grow (3D rigid-rod phase)
+    "grow3d": dict(
+        sim=dict(Lx=16., n_chains=60, chain_length=10, a=0.5, k=100., kappa=10., repel_d_max=1.,
+                 WCA_epsilon=1., LJ_cutoff_factor=2.5 / 2 ** (1 / 6), v0=1., v_tan_angle=0., T=0.05, Dr=0.1,
+                 b_use_tangent_as_propulsion_direction=False, dim=3, seed=37, dtmax=5e-4, dt0=5e-4),
+        dt=None, fixed_dt=False, calls=[1, 19, 80], noise_seed=111, save_every=None),
     # SRK4 (SRK.py:186-215, 296-321): 2D with chirality, grown by the
     # reference's init-grow under SRK4
     "srk4_2d": dict(

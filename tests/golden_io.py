@@ -6,7 +6,7 @@ import numpy as np
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CASES = ["config1", "chiral_lj", "rotdiff2d", "rotdiff3d", "adaptive", "paper_chiral", "rigid2d", "rigid3d",
-         "srk4_2d", "srk4_3d", "srk4_rigid"]
+         "srk4_2d", "srk4_3d", "srk4_rigid", "grow3d"]
 STATUS_FIELDS = ["dt", "dt_used", "stepnum", "t", "update_grid_list_counter", "max_forces_strength",
                  "next_output_step", "next_save_time", "dtmax"]
 
@@ -49,4 +49,5 @@ TRAJ_TOL = {
     "srk4_2d": [1e-9, 1e-9, 1e-9],
     "srk4_3d": [1e-9, 1e-9, 1e-9],
     "srk4_rigid": [1e-9, 1e-9, 1e-9],
+    "grow3d": [1e-9, 1e-9, 1e-9],
 }

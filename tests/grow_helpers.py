@@ -28,17 +28,25 @@ def grown_stats(pos, chain, L, close=0.8):
                 bond_max=float(bl.max()), n_close=n_close // 2)
 
 
-def config1_growth_case():
-    """The reference's config-1 run: its random placement (``init_pos``), its
-    physical parameters and its grown state (``pos0``)."""
-    d, s = load("config1")
+def growth_case(name="config1"):
+    """A golden run the reference grew itself: its random placement
+    (``init_pos``), its physical parameters and its grown state (``pos0``).
+    Both runs used repel_d_max 1, WCA_epsilon 1, WCA_shift 0, rest length 0.5
+    and dt0 = dtmax."""
+    d, s = load(name)
+    ov = s["sim_overrides"]
     base = SystemParams(L=s["L"], spring_params=np.array(d["spring_params"]), wca_params=np.array(d["wca_params"]),
                         active_params=np.array(d["active_params"]), D=s["D"], Dr=s["Dr"], radius=s["radius"],
                         n_nearby=s["n_nearby"], dtmax=s["dtmax"], max_dist_per_step=s["max_dist_per_step_setup"])
-    consts = GrowthConstants(repel_d_max=1.0, WCA_epsilon=1.0, WCA_shift=0.0, LJ_cutoff_factor=1.0,
-                             reference_rest_length=0.5, longest_chain_length=s["longest_chain_length"])
-    settings = GrowSettings(dt0=s["dtmax"])  # the run set dt0 = dtmax
+    consts = GrowthConstants(repel_d_max=1.0, WCA_epsilon=1.0, WCA_shift=0.0,
+                             LJ_cutoff_factor=float(ov.get("LJ_cutoff_factor", 1.0)), reference_rest_length=0.5,
+                             longest_chain_length=s["longest_chain_length"])
+    settings = GrowSettings(dt0=s["dtmax"])
     return d, s, base, consts, settings
+
+
+def config1_growth_case():
+    return growth_case("config1")
 
 
 def check_like_reference(stats, ref, steps, ref_steps, t):

@@ -5,8 +5,9 @@
   projection factor 0.025), parameters changing between calls as
   control.early_time_procedures changes them.
 * A growing population steps in FP64 whatever precision is asked for.
-* ``growth.init_grow`` grows the reference's config-1 placement into a state
-  with the statistics of the reference's own grown state.
+* ``growth.init_grow`` grows the reference's config-1 placement and a 3D
+  placement into states with the statistics of the reference's own grown
+  states.
 * Rigid rods (factor 1) with noise stay rods; a batch holding a rigid
   system steps every system as it steps alone, bit for bit, before and after
   the projection is switched off (the graph is re-captured without it).
@@ -32,7 +33,7 @@ from gliding_collective_rotation_b200.growth import init_grow  # noqa: E402
 from gliding_collective_rotation_b200.workloads import SystemSpec  # noqa: E402
 from tests.golden_io import GOLDEN, load, min_image, status_dict  # noqa: E402
 from tests.gpu_helpers import pop_from_arrays, set_pop_params, status_from_row  # noqa: E402
-from tests.grow_helpers import check_like_reference, config1_growth_case, grown_stats  # noqa: E402
+from tests.grow_helpers import check_like_reference, growth_case, grown_stats  # noqa: E402
 
 
 def _initgrow():
@@ -93,10 +94,11 @@ def test_growing_population_steps_in_fp64():
         assert sa["dt"] == sb["dt"]
 
 
-def test_init_grow_on_device_matches_reference_statistics():
-    d, s, base, consts, settings = config1_growth_case()
+@pytest.mark.parametrize("name", ["config1", "grow3d"])
+def test_init_grow_on_device_matches_reference_statistics(name):
+    d, s, base, consts, settings = growth_case(name)
     n_chains = len(d["rest_lengths"])
-    spec = SystemSpec("config1", 2, np.array(d["init_pos"]), np.array(d["init_tangent"]),
+    spec = SystemSpec(name, int(s["dim"]), np.array(d["init_pos"]), np.array(d["init_tangent"]),
                       np.array(d["chain_id"]), np.full(n_chains, 0.5), copy.deepcopy(base), base.dtmax,
                       base.max_dist_per_step)
     res = init_grow([spec], settings, constants=[consts])
