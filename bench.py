@@ -156,7 +156,9 @@ class ClockSampler:
 def cpu_sample_rate(specs, states_host, steps, threads, max_systems=4, budget_s=20.0):
     """bead-steps/s of the oracle (the reference's Numba step restated in C,
     OpenMP threads over chain-aligned chunks) on the first systems of the
-    workload, each run for `steps` steps after an untimed list build."""
+    workload, each run for `steps` steps after an untimed list build, under
+    the reference's adaptive dt rule as the GPU arm (dtmax = the system's dt,
+    max_dist_per_step of grid_list_setup; each system's dt carried)."""
     from oracle import oracle as O
     systems = []
     for spec, (pos, tan) in list(zip(specs, states_host))[:max_systems]:
@@ -166,20 +168,22 @@ def cpu_sample_rate(specs, states_host, steps, threads, max_systems=4, budget_s=
                               p.active_params, p.D, p.Dr, p.radius, p.n_nearby, ng, nbor_depth=32)
         sysm.build_lists(grid_window=1)
         sysm.seed_mt(int(p.seed), threads)
-        systems.append((spec, sysm))
+        systems.append([spec, sysm, spec.dt])
     # rounds of `steps` steps over the sample until the time budget is used
     total_bs, total_t, used = 0, 0.0, []
     rounds = 0
     while total_t < budget_s and rounds < 1000:
-        for spec, sysm in systems:
+        for entry in systems:
+            spec, sysm, dt = entry
             t0 = time.perf_counter()
-            res = sysm.run(steps, dt=spec.dt, n_threads=threads)
+            res = sysm.run(steps, dt=dt, dtmax=spec.dt, max_dist_per_step=spec.relax_mdps, n_threads=threads)
             total_t += time.perf_counter() - t0
             total_bs += spec.n * res["steps"]
+            entry[2] = res["dt"]
             if res["flag"] < 0:
                 sysm.build_lists(grid_window=1)
         rounds += 1
-    used = [f"{spec.name}({spec.n} beads)" for spec, _ in systems]
+    used = [f"{spec.name}({spec.n} beads)" for spec, _, _ in systems]
     used.append(f"{rounds} rounds of {steps} steps")
     return total_bs / total_t, used, total_t
 
@@ -399,8 +403,12 @@ def run_gpu(args):
         threads = os.cpu_count() or 1
         r, used, secs = cpu_sample_rate(specs, host_states, args.cpu_steps, threads, max_systems=args.cpu_systems,
                                         budget_s=args.cpu_budget)
+        r1, used1, secs1 = cpu_sample_rate(specs, host_states, args.cpu_steps, 1, max_systems=2,
+                                           budget_s=max(2.0, args.cpu_budget / 3))
         cpu = {"value": r, "unit": "bead-steps/s", "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_steps} steps of {', '.join(used)} ({secs:.1f} s)"}
+               "sample": f"{args.cpu_steps} steps of {', '.join(used)} ({secs:.1f} s); adaptive dt as the GPU arm",
+               "single_thread_value": r1,
+               "single_thread_sample": f"{args.cpu_steps} steps of {', '.join(used1)} ({secs1:.1f} s)"}
 
     working_set = sum(v.numel() * v.element_size() for v in big.values()) + eng.cfg.cell_capacity * (
         8 + eng.cfg.cell_depth * 4) + n_beads * (4 * list_mean + 4 + 8 * batch.dim)

@@ -27,6 +27,7 @@ pytestmark = pytest.mark.gpu
 
 from gliding_collective_rotation_b200 import config, updates  # noqa: E402
 from gliding_collective_rotation_b200 import workloads as W  # noqa: E402
+from gliding_collective_rotation_b200._lib import GcrError  # noqa: E402
 from gliding_collective_rotation_b200.batch import Batch  # noqa: E402
 from gliding_collective_rotation_b200.engine import SystemParams  # noqa: E402
 from gliding_collective_rotation_b200.growth import init_grow  # noqa: E402
@@ -206,6 +207,18 @@ def test_update_desc_regrids_within_reserved_cells():
         b.close()
         return out
 
+    # a grid finer than the one reserved at admission is refused (the caller
+    # re-admits; the drop-in does so by itself)
+    spec = copy.deepcopy(base)
+    b = Batch([spec], precision="fp64")
+    st = b.states[0]
+    st.params.wca_params = np.array(st.params.wca_params)
+    st.params.wca_params[3] = 0.3
+    st.params.skin = 0.05
+    with pytest.raises(GcrError) as err:
+        b.engine.update_params(st)
+    assert err.value.code == -6
+    b.close()
     # a smaller skin keeps the grid; a larger one takes fewer, larger cells
     for start, new in ((0.3, 0.1), (0.3, 0.9)):
         a, b = fresh(new, start_skin=start), fresh(new)
