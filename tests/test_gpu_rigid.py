@@ -207,14 +207,22 @@ def test_update_desc_regrids_within_reserved_cells():
         b.close()
         return out
 
-    # a grid finer than the one reserved at admission is refused (the caller
-    # re-admits; the drop-in does so by itself)
+    # a smaller cutoff keeps the (coarser) grid; a grid beyond the cells
+    # reserved at admission -- pair forces switched on for a system admitted
+    # without them -- is refused (the caller re-admits; the drop-in does so by
+    # itself)
     spec = copy.deepcopy(base)
     b = Batch([spec], precision="fp64")
     st = b.states[0]
     st.params.wca_params = np.array(st.params.wca_params)
     st.params.wca_params[3] = 0.3
-    st.params.skin = 0.05
+    b.engine.update_params(st)
+    b.close()
+    spec = copy.deepcopy(base)
+    spec.params.calc_wca = False
+    b = Batch([spec], precision="fp64")
+    st = b.states[0]
+    st.params.calc_wca = True
     with pytest.raises(GcrError) as err:
         b.engine.update_params(st)
     assert err.value.code == -6
