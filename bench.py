@@ -318,8 +318,13 @@ def run_gpu(args):
     builds_per_stage = bead_builds / (2.0 * args.steps * n_beads)
 
     # ---- per-kernel profile (roofline) ----------------------------------
-    batch.begin(args.profile_steps)
-    kms = eng.profile_steps(args.profile_steps) / args.profile_steps
+    # every run starts with a forced list build; the difference of an
+    # (n+1)-step and a 1-step profile is n steps in steady state
+    batch.begin(args.profile_steps + 1)
+    k_all = eng.profile_steps(args.profile_steps + 1)
+    batch.begin(1)
+    k_one = eng.profile_steps(1)
+    kms = np.maximum(k_all - k_one, 0.0) / args.profile_steps
     cfg = eng.cfg
     from gliding_collective_rotation_b200.engine import footprint
     n_cells = sum(footprint(cfg, s.params, s.n, len(s.rest_lengths))[0] for s in specs)
