@@ -61,7 +61,7 @@ def _install_shims():
 
 
 CASES = {
-    # BASELINE config 1 exactly: 2D, Lx=60, 200 x 10 beads, a=0.5, k=100,
+    # benchmark config 1 exactly: 2D, Lx=60, 200 x 10 beads, a=0.5, k=100,
     # kappa=20, WCA (cutoff 1), v0=1 tangent-locked, T=0.01, dt=1e-3 fixed.
     "config1": dict(
         sim=dict(Lx=60., n_chains=200, chain_length=10, a=0.5, k=100., kappa=20.,

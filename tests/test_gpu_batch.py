@@ -97,7 +97,7 @@ def test_batched_equals_alone_bitwise(precision):
 
 def test_mixed_precision_error_vs_fp64():
     """FP32 forces and SRK arithmetic with FP64 positions vs the FP64 run of
-    the same kernels, same Philox noise, BASELINE config 1 from the
+    the same kernels, same Philox noise, config 1 (2,000 beads, WCA) from the
     reference's relaxed state, 1,000 steps."""
     d, s = load("config1")
     prm = lambda: SystemParams(L=s["L"], spring_params=d["spring_params"], wca_params=d["wca_params"],
