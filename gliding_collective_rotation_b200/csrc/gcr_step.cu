@@ -524,8 +524,11 @@ template <int D, typename FT, int WHICH>
 __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_pair(BatchArgs A)
 {
     const int nt = *A.n_bead_tiles;
+    // the next tile's table entry is loaded while the current tile runs
+    Tile nx = (int)blockIdx.x < nt ? A.bead_tiles[blockIdx.x] : Tile{0, 0};
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const Tile tl = A.bead_tiles[t];
+        const Tile tl = nx;
+        if (t + (int)gridDim.x < nt) nx = A.bead_tiles[t + gridDim.x];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
         if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal) || !p.calc_wca) continue;
@@ -646,19 +649,23 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
     using BT = typename StageSmem<D, FT>::BT;
     sm.carve(smem_raw, TB);
     const int nt = *A.n_bead_tiles;
+    // the next tile's table entry is loaded while the current tile runs
+    Tile nx = (int)blockIdx.x < nt ? A.bead_tiles[blockIdx.x] : Tile{0, 0};
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         __syncthreads();  // the previous tile is done with shared memory
-        const Tile tl = A.bead_tiles[t];
+        const Tile tl = nx;
+        if (t + (int)gridDim.x < nt) nx = A.bead_tiles[t + gridDim.x];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
+        // the system's constants are read before the barrier, with its flags
+        const int n = p.n;
+        const int base = tl.begin - 2;
+        const double *__restrict__ X = stage_x<stage_reads(STAGE)>(p);
         // one decision per CTA: other CTAs may raise the system's flags while
         // this one runs, and every thread must reach the same barriers
         if (threadIdx.x == 0) sh_run = ld_volatile(&s.active) && !(ld_volatile(&s.flags) & kFlagFatal);
         __syncthreads();
         if (!sh_run) continue;
-        const int n = p.n;
-        const int base = tl.begin - 2;
-        const double *__restrict__ X = stage_x<stage_reads(STAGE)>(p);
         // 1. positions and topology of beads begin-2 .. begin+TB+1
         for (int k = threadIdx.x; k < TB + 4; k += TB) {
             int m = base + k;
@@ -922,8 +929,11 @@ template <int D, typename FT>
 __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A)
 {
     const int nt = *A.n_bead_tiles;
+    // the next tile's table entry is loaded while the current tile runs
+    Tile nx = (int)blockIdx.x < nt ? A.bead_tiles[blockIdx.x] : Tile{0, 0};
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const Tile tl = A.bead_tiles[t];
+        const Tile tl = nx;
+        if (t + (int)gridDim.x < nt) nx = A.bead_tiles[t + gridDim.x];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
         // no barriers in this kernel: a per-thread decision is safe
