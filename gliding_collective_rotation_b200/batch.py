@@ -111,6 +111,7 @@ class Batch:
         self.engine = None
         self._carry_dt = None  # dts to hand to the next call after a regrow
         self.series_buf = None
+        self.groups = []  # coupled populations: (member indices, fixed flags, cross WCA parameters)
         self._make_engine()
 
     def _make_engine(self):
@@ -123,6 +124,23 @@ class Batch:
                              **self._engine_kw)
         for st in self.states:
             self.engine.admit(st)
+        for g in self.groups:
+            self._couple(*g)
+
+    def couple(self, members, fixed, cross_wca):
+        """Step the systems ``members`` (indices into this batch, in the
+        reference's population order) as the populations of one box, as
+        ``updates.SRK2_force_calc`` steps a list of populations
+        (updates.py:146-247): one dt per step, joint list builds, and the WCA
+        force ``cross_wca[i][j]`` = [p0, p1, shift, r_cut] of population j on
+        population i (``interpop_forces``, updates.py:274-312).  ``fixed[i]``:
+        population i never moves (pop.fixed).  The coupling survives a regrow."""
+        g = (list(members), [bool(f) for f in fixed], np.asarray(cross_wca, dtype=np.float64))
+        self._couple(*g)
+        self.groups.append(g)
+
+    def _couple(self, members, fixed, cross_wca):
+        self.engine.couple([self.states[i].slot for i in members], fixed, cross_wca)
 
     def overflowed(self, statuses=None):
         statuses = statuses if statuses is not None else self.statuses()

@@ -88,6 +88,15 @@ struct Slot {
     int64_t n_cells_alloc = 0;  // cells reserved at admission
     int64_t nc = 1;             // current GPU cells per side
     int64_t longest = 0;        // beads of the longest chain
+    int group = -1;             // coupled group (index into gcr_ctx::groups) or -1
+};
+
+// populations coupled in one box (gcr_couple)
+struct Group {
+    int n = 0;  // 0: dissolved
+    int32_t slots[kMaxPops] = {-1, -1, -1, -1};
+    int32_t fixed[kMaxPops] = {0, 0, 0, 0};
+    double cross[kMaxPops][kMaxPops][4] = {};  // [i][j]: force on member i from member j
 };
 
 int ilog2(int v)
@@ -145,6 +154,11 @@ struct gcr_ctx {
     cudaGraphExec_t graph = nullptr;
     bool graph_rigid = false;  // the graph holds the rigid-rod projection kernels
     bool graph_obs = false;    // the graph holds the series kernel
+    bool graph_cross = false;  // the graph holds the cross-population pair kernels
+    std::vector<Group> groups;
+    int *xnbr = nullptr;       // cross lists of coupled populations
+    int *xcount = nullptr;
+    int64_t x_rows = 0;        // rows allocated (the slot stride of xnbr)
     void *observe = nullptr;   // k_observe of the context's precision
     bool tiles_dirty = true;
 };
@@ -172,7 +186,9 @@ int rebuild_tiles(gcr_ctx *c)
     for (int s = 0; s < (int)c->slots.size(); s++) {
         const Slot &sl = c->slots[s];
         if (!sl.used) continue;
-        for (int64_t b = 0; b < sl.desc.n_beads; b += tb) c->h_bead_tiles.push_back(Tile{s, (int32_t)b});
+        // a fixed population never moves: only the list kernels visit it
+        if (!c->hP[s].fixed)
+            for (int64_t b = 0; b < sl.desc.n_beads; b += tb) c->h_bead_tiles.push_back(Tile{s, (int32_t)b});
         if (sl.desc.calc_wca)
             for (int64_t q = 0; q < sl.n_cells; q += tcl) c->h_cell_tiles.push_back(Tile{s, (int32_t)q});
     }
@@ -293,6 +309,122 @@ void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, double skin, SysP &
     p.seed = d.seed;
 }
 
+// the coupling fields of every resident system from the context's groups,
+// and the cross-list rows they need; *moved: the cross-list buffer was
+// reallocated (graphs captured with the old one must go)
+int apply_groups(gcr_ctx *c, bool *moved)
+{
+    *moved = false;
+    const int dim = c->cfg.dim;
+    for (size_t s = 0; s < c->slots.size(); s++) {
+        const Slot &sl = c->slots[s];
+        if (!sl.used) continue;
+        SysP &p = c->hP[s];
+        p.fixed = 0;
+        p.grp_n = 0;
+        p.n_cross = 0;
+        p.x_off = 0;
+        for (int k = 0; k < kMaxPops; k++) p.grp[k] = -1;
+        for (int k = 0; k < kMaxPops - 1; k++) {
+            p.cross_q[k] = -1;
+            p.cross_w[k] = 1;
+            p.cross_p0[k] = p.cross_p1[k] = p.cross_shift[k] = p.cross_rc2[k] = p.cross_rl2[k] = 0.0;
+        }
+        p.pos1 = sl.buf.pos1;
+        p.pos2 = c->pos2 ? c->pos2 + (size_t)sl.bead_off * dim : nullptr;
+    }
+    int64_t rows = 0;
+    for (const Group &g : c->groups) {
+        for (int a = 0; a < g.n; a++) {
+            SysP &p = c->hP[g.slots[a]];
+            p.grp_n = g.n;
+            for (int k = 0; k < g.n; k++) p.grp[k] = g.slots[k];
+            p.fixed = g.fixed[a] ? 1 : 0;
+            if (p.fixed) {
+                // stage positions of a population that never moves
+                p.pos1 = p.pos;
+                p.pos2 = p.pos;
+                continue;
+            }
+            const double skin_a = 2.0 * std::sqrt(p.half_skin2);
+            // the other populations in the order their forces are added
+            // (pop_index_diff = 1, 2, ..., SRK.py:287-294)
+            for (int ii = 1; ii < g.n; ii++) {
+                const int b = (a + ii) % g.n;
+                const double *w = g.cross[a][b];
+                if (!(w[3] > 0.0) || (w[0] == 0.0 && w[1] == 0.0)) continue;
+                const SysP &q = c->hP[g.slots[b]];
+                const int k = p.n_cross++;
+                p.cross_q[k] = g.slots[b];
+                p.cross_p0[k] = w[0];
+                p.cross_p1[k] = w[1];
+                p.cross_shift[k] = w[2];
+                p.cross_rc2[k] = w[3] * w[3];
+                // both populations' beads stay within half their skins of the
+                // build positions, so pairs within this radius cover r_cut
+                const double rl = w[3] + 0.5 * (skin_a + 2.0 * std::sqrt(q.half_skin2));
+                p.cross_rl2[k] = rl * rl * (1.0 + 1e-6);
+                p.cross_w[k] = std::max(1, (int)std::ceil(rl * q.inv_h));
+            }
+            p.x_off = rows;
+            rows += (int64_t)p.n_cross * p.n;
+        }
+    }
+    if (rows > c->x_rows) {
+        GCR_CUDA(cudaStreamSynchronize(c->stream));
+        if (c->xnbr) cudaFree(c->xnbr);
+        if (c->xcount) cudaFree(c->xcount);
+        c->xnbr = nullptr;
+        c->xcount = nullptr;
+        c->x_rows = 0;
+        cudaError_t e = cudaMalloc(&c->xnbr, sizeof(int) * (size_t)rows * (size_t)c->cfg.list_depth);
+        if (e == cudaSuccess) e = cudaMalloc(&c->xcount, sizeof(int) * (size_t)rows);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->xcount, 0, sizeof(int) * (size_t)rows, c->stream);
+        if (e != cudaSuccess) {
+            if (c->xnbr) cudaFree(c->xnbr);
+            if (c->xcount) cudaFree(c->xcount);
+            c->xnbr = nullptr;
+            c->xcount = nullptr;
+            return fail(e == cudaErrorMemoryAllocation ? GCR_ERR_OOM : GCR_ERR_CUDA, "cross-list allocation");
+        }
+        c->x_rows = rows;
+        *moved = true;
+    }
+    c->args.xnbr = c->xnbr;
+    c->args.xcount = c->xcount;
+    c->args.xstride = c->x_rows;
+    return GCR_OK;
+}
+
+// some resident system feels another population's pair force
+bool any_cross(const gcr_ctx *c)
+{
+    for (size_t s = 0; s < c->slots.size(); s++)
+        if (c->slots[s].used && c->hP[s].n_cross > 0) return true;
+    return false;
+}
+
+// drop the captured graph (the next gcr_run captures a new one)
+int drop_graph(gcr_ctx *c)
+{
+    if (!c->graph) return GCR_OK;
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+    return GCR_OK;
+}
+
+// dissolve group g: its members step on their own again
+int dissolve(gcr_ctx *c, int g)
+{
+    if (g < 0 || g >= (int)c->groups.size()) return GCR_OK;
+    Group &gr = c->groups[g];
+    for (int k = 0; k < gr.n; k++)
+        if (gr.slots[k] >= 0 && gr.slots[k] < (int)c->slots.size()) c->slots[gr.slots[k]].group = -1;
+    gr = Group();
+    return GCR_OK;
+}
+
 // some resident system uses the rigid-rod projection
 bool any_rigid(const gcr_ctx *c)
 {
@@ -359,6 +491,7 @@ int enqueue_step4(gcr_ctx *c)
         if ((rc = enqueue_lists(c, reads[k]))) return rc;
         void *pair = reads[k] == 0 ? c->ks.pair0 : (reads[k] == 1 ? c->ks.pair1 : c->ks.pair2);
         if ((rc = launch(c, pair, c->grid_pair, bb))) return rc;
+        if (c->graph_cross && (rc = launch(c, c->ks.cross[reads[k]], c->grid_pair, bb))) return rc;
         if ((rc = launch(c, c->ks.stage4[k], c->grid_stage4[k], bb, c->stage_smem))) return rc;
         if (k < 3 && c->graph_rigid && (rc = launch(c, c->ks.rigid4[k], c->grid_update, bb))) return rc;
     }
@@ -376,10 +509,12 @@ int enqueue_step(gcr_ctx *c)
     if (c->cfg.srk_order == 4) return enqueue_step4(c);
     if ((rc = enqueue_lists(c, 0))) return rc;
     if ((rc = launch(c, c->ks.pair0, c->grid_pair, bb))) return rc;
+    if (c->graph_cross && (rc = launch(c, c->ks.cross[0], c->grid_pair, bb))) return rc;
     if ((rc = launch(c, c->ks.stage0, c->grid_stage0, bb, c->stage_smem))) return rc;
     if (c->graph_rigid && (rc = launch(c, c->ks.rigid0, c->grid_update, bb))) return rc;
     if ((rc = enqueue_lists(c, 1))) return rc;
     if ((rc = launch(c, c->ks.pair1, c->grid_pair, bb))) return rc;
+    if (c->graph_cross && (rc = launch(c, c->ks.cross[1], c->grid_pair, bb))) return rc;
     if ((rc = launch(c, c->ks.stage1, c->grid_stage1, bb, c->stage_smem))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_dt))) return rc;
     if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
@@ -399,8 +534,8 @@ int build_graph(gcr_ctx *c)
 {
     // the projection and series kernels are in the graph only while some
     // system uses them
-    const bool rigid = any_rigid(c), obs = any_series(c);
-    if (c->graph && (rigid != c->graph_rigid || obs != c->graph_obs)) {
+    const bool rigid = any_rigid(c), obs = any_series(c), cross = any_cross(c);
+    if (c->graph && (rigid != c->graph_rigid || obs != c->graph_obs || cross != c->graph_cross)) {
         GCR_CUDA(cudaStreamSynchronize(c->stream));
         cudaGraphExecDestroy(c->graph);
         c->graph = nullptr;
@@ -408,6 +543,7 @@ int build_graph(gcr_ctx *c)
     if (c->graph) return GCR_OK;
     c->graph_rigid = rigid;
     c->graph_obs = obs;
+    c->graph_cross = cross;
     cudaGraph_t g = nullptr;
     GCR_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = GCR_OK;
@@ -598,7 +734,7 @@ int gcr_destroy(gcr_ctx *c)
     if (c->graph) cudaGraphExecDestroy(c->graph);
     void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->topo, c->cnt, c->ncell,
                     c->items, c->nbr, c->ncount, c->xref, c->work, c->xi, c->fp, c->chain_starts, c->d_err,
-                    c->d_out, c->pos2, c->faux};
+                    c->d_out, c->pos2, c->faux, c->xnbr, c->xcount};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -692,6 +828,15 @@ int gcr_evict(gcr_ctx *c, int32_t slot)
     Slot &sl = c->slots[slot];
     // make sure no queued work still uses the slot's scratch
     GCR_CUDA(cudaStreamSynchronize(c->stream));
+    if (sl.group >= 0) {
+        // its coupled populations step on their own again
+        dissolve(c, sl.group);
+        int rc = drop_graph(c);
+        if (rc) return rc;
+        bool moved = false;
+        rc = apply_groups(c, &moved);
+        if (rc) return rc;
+    }
     c->beads.release(sl.bead_off, sl.desc.n_beads);
     if (sl.n_cells_alloc) c->cells.release(sl.cell_off, sl.n_cells_alloc);
     c->chains.release(sl.chain_off, sl.desc.n_chains + 1);
@@ -731,9 +876,110 @@ int gcr_update_desc(gcr_ctx *c, int32_t slot, const gcr_system_desc *desc)
     sl.n_cells = n_cells;
     sl.nc = nc;
     fill_sysp(c, sl, nc, skin, c->hP[slot]);
-    GCR_CUDA(cudaMemcpyAsync(c->dP + slot, &c->hP[slot], sizeof(SysP), cudaMemcpyHostToDevice, c->stream));
+    if (sl.group >= 0) {
+        // the partners' cross-list radii and windows follow the new skin and grid
+        bool moved = false;
+        rc = apply_groups(c, &moved);
+        if (rc) return rc;
+        if (moved && (rc = drop_graph(c))) return rc;
+        GCR_CUDA(cudaMemcpyAsync(c->dP, c->hP.data(), sizeof(SysP) * c->hP.size(), cudaMemcpyHostToDevice,
+                                 c->stream));
+    } else {
+        GCR_CUDA(cudaMemcpyAsync(c->dP + slot, &c->hP[slot], sizeof(SysP), cudaMemcpyHostToDevice, c->stream));
+    }
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     return GCR_OK;
+}
+
+int gcr_couple(gcr_ctx *c, int32_t n, const int32_t *slots, const int32_t *fixed, const double *cross_wca)
+{
+    if (!c || !slots || !fixed || !cross_wca) return fail(GCR_ERR_BAD_ARG, "null argument");
+    if (n < 2 || n > kMaxPops) return fail(GCR_ERR_BAD_ARG, "2 to 4 populations can be coupled");
+    int g_old = -2;
+    int movers = 0, first = -1;
+    for (int a = 0; a < n; a++) {
+        if (!valid_slot(c, slots[a])) return fail(GCR_ERR_BAD_ARG, "invalid slot");
+        for (int b = 0; b < a; b++)
+            if (slots[b] == slots[a]) return fail(GCR_ERR_BAD_ARG, "a slot appears twice");
+        const Slot &sl = c->slots[slots[a]];
+        if (!sl.desc.calc_wca) return fail(GCR_ERR_BAD_ARG, "every coupled population needs its WCA force");
+        if (sl.desc.L != c->slots[slots[0]].desc.L) return fail(GCR_ERR_BAD_ARG, "coupled populations share L");
+        const int g = sl.group;
+        if (g_old == -2) g_old = g;
+        if (g != g_old || (g >= 0 && c->groups[g].n != n))
+            return fail(GCR_ERR_BAD_ARG, "a slot is coupled to other populations (gcr_decouple first)");
+        if (!fixed[a]) {
+            movers++;
+            if (first < 0) {
+                first = a;
+            } else {
+                const gcr_system_desc &d0 = c->slots[slots[first]].desc;
+                if (sl.desc.dtmax != d0.dtmax || sl.desc.max_dist_per_step != d0.max_dist_per_step ||
+                    sl.desc.rk_cheat != d0.rk_cheat)
+                    return fail(GCR_ERR_BAD_ARG, "moving populations share dtmax, max_dist_per_step and rk_cheat");
+            }
+        }
+        for (int b = 0; b < n; b++)
+            for (int k = 0; k < 4; k++)
+                if (!std::isfinite(cross_wca[((size_t)a * n + b) * 4 + k]))
+                    return fail(GCR_ERR_BAD_ARG, "cross parameters must be finite");
+    }
+    if (movers == 0) return fail(GCR_ERR_BAD_ARG, "at least one coupled population must move");
+    if (g_old >= 0) {
+        // the same members again: their order must match
+        for (int a = 0; a < n; a++)
+            if (c->groups[g_old].slots[a] != slots[a])
+                return fail(GCR_ERR_BAD_ARG, "re-coupling must list the members in the same order");
+    }
+    int rc = drop_graph(c);
+    if (rc) return rc;
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    int g = g_old;
+    if (g < 0) {
+        for (int k = 0; k < (int)c->groups.size(); k++)
+            if (c->groups[k].n == 0) {
+                g = k;
+                break;
+            }
+        if (g < 0) {
+            c->groups.push_back(Group());
+            g = (int)c->groups.size() - 1;
+        }
+    }
+    Group &gr = c->groups[g];
+    gr = Group();
+    gr.n = n;
+    for (int a = 0; a < n; a++) {
+        gr.slots[a] = slots[a];
+        gr.fixed[a] = fixed[a] ? 1 : 0;
+        c->slots[slots[a]].group = g;
+        for (int b = 0; b < n; b++)
+            for (int k = 0; k < 4; k++) gr.cross[a][b][k] = a == b ? 0.0 : cross_wca[((size_t)a * n + b) * 4 + k];
+    }
+    bool moved = false;
+    rc = apply_groups(c, &moved);
+    if (rc) {
+        dissolve(c, g);
+        apply_groups(c, &moved);
+        return rc;
+    }
+    c->tiles_dirty = true;
+    return rebuild_tiles(c);
+}
+
+int gcr_decouple(gcr_ctx *c, int32_t slot)
+{
+    if (!valid_slot(c, slot)) return fail(GCR_ERR_BAD_ARG, "invalid slot");
+    const int g = c->slots[slot].group;
+    if (g < 0) return GCR_OK;
+    int rc = drop_graph(c);
+    if (rc) return rc;
+    dissolve(c, g);
+    bool moved = false;
+    rc = apply_groups(c, &moved);
+    if (rc) return rc;
+    c->tiles_dirty = true;
+    return rebuild_tiles(c);
 }
 
 namespace {
@@ -850,13 +1096,14 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
     std::vector<cudaEvent_t> ev((size_t)n_steps * (G + 1), nullptr);
     for (auto &e : ev) GCR_CUDA(cudaEventCreate(&e));
     const int bb = c->cfg.block_beads;
-    const bool rigid = any_rigid(c);
+    const bool rigid = any_rigid(c), cross = any_cross(c);
     for (int s = 0; s < n_steps && rc == GCR_OK; s++) {
         cudaEvent_t *e = ev.data() + (size_t)s * (G + 1);
         GCR_CUDA(cudaEventRecord(e[0], c->stream));
         rc = enqueue_lists(c, 0);
         GCR_CUDA(cudaEventRecord(e[1], c->stream));
         if (!rc) rc = launch(c, c->ks.pair0, c->grid_pair, bb);
+        if (!rc && cross) rc = launch(c, c->ks.cross[0], c->grid_pair, bb);
         GCR_CUDA(cudaEventRecord(e[2], c->stream));
         if (!rc) rc = launch(c, c->ks.stage0, c->grid_stage0, bb, c->stage_smem);
         if (!rc && rigid) rc = launch(c, c->ks.rigid0, c->grid_update, bb);
@@ -864,6 +1111,7 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
         if (!rc) rc = enqueue_lists(c, 1);
         GCR_CUDA(cudaEventRecord(e[4], c->stream));
         if (!rc) rc = launch(c, c->ks.pair1, c->grid_pair, bb);
+        if (!rc && cross) rc = launch(c, c->ks.cross[1], c->grid_pair, bb);
         GCR_CUDA(cudaEventRecord(e[5], c->stream));
         if (!rc) rc = launch(c, c->ks.stage1, c->grid_stage1, bb, c->stage_smem);
         if (!rc) rc = launch_sys(c, c->ks.sys_dt);

@@ -26,6 +26,8 @@
 namespace gcr {
 
 constexpr int kMaxDim = 3;
+// populations coupled in one box, at most
+constexpr int kMaxPops = 4;
 
 // topology bits of a bead (same chain as b-1, b-2, b+1, b+2)
 constexpr uint8_t kHasPrev = 1, kHasPrev2 = 2, kHasNext = 4, kHasNext2 = 8;
@@ -78,6 +80,20 @@ struct SysP {
     double dtmax, mdps, rk;
     double rigid;  // rigid-rod projection factor (0: off, or no chain longer than 2 beads)
     uint64_t seed;
+    // populations coupled in one box (updates.py:146-247, SRK.py:166-330):
+    // the members step under one dt, rebuild their lists together, and each
+    // moving member feels the others through WCA pair forces over its cross
+    // lists.  A fixed member (pop.fixed) never moves; its pos1/pos2 alias pos.
+    int32_t fixed;
+    int32_t grp_n;                // members of its group (0: not coupled)
+    int32_t grp[kMaxPops];        // member slots, in population order
+    int32_t n_cross;              // partner populations whose force it feels
+    int32_t cross_q[kMaxPops - 1];  // partner slots, in the order the reference adds them
+    int32_t cross_w[kMaxPops - 1];  // cells scanned either side in the partner's grid
+    int32_t pad1;
+    double cross_p0[kMaxPops - 1], cross_p1[kMaxPops - 1], cross_shift[kMaxPops - 1];
+    double cross_rc2[kMaxPops - 1], cross_rl2[kMaxPops - 1];
+    int64_t x_off;                // first row of its cross lists
 };
 
 struct SysS {

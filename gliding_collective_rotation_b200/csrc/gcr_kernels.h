@@ -34,6 +34,11 @@ struct BatchArgs {
     int tile_beads;
     int tile_cells;
     int order;     // SRK order of the context: 2 or 4
+    // cross lists of coupled populations: slot k of row r at xnbr[k * xstride + r]
+    // (row r = x_off + c * n + bead for cross partner c), xcount[r] partners
+    int *xnbr;
+    int *xcount;
+    int64_t xstride;
 };
 
 struct KernelSet {
@@ -60,6 +65,7 @@ struct KernelSet {
     void *sys_end;
     void *sys_mark;  // flag every resident system for a list build
     void *lists_plan;  // compact the systems that take part in a list build
+    void *cross[3];    // cross-population pair forces at pos / pos1 / pos2 (added to the pair force)
     size_t (*stage_smem)(int block_beads);  // dynamic shared memory of the stage kernels
 };
 

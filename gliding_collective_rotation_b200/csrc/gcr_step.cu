@@ -200,10 +200,12 @@ __device__ __forceinline__ double *stage_x(const SysP &p)
     return WHICH == 0 ? p.pos : (WHICH == 1 ? p.pos1 : p.pos2);
 }
 
-// the system takes part in a list build now
+// the system takes part in a list build now (a fixed member of coupled
+// populations is binned whenever k_lists_plan listed it)
 __device__ __forceinline__ bool builds(const SysP &p, const SysS &s)
 {
-    return p.calc_wca && ld_volatile(&s.active) && s.rebuild && !(ld_volatile(&s.flags) & kFlagFatal);
+    return p.calc_wca && (p.fixed || (ld_volatile(&s.active) && s.rebuild)) &&
+           !(ld_volatile(&s.flags) & kFlagFatal);
 }
 
 template <int D>
@@ -282,7 +284,27 @@ __global__ void __launch_bounds__(1024) k_lists_plan(BatchArgs A)
         if (i < A.n_slots) {
             const SysP &p = A.P[i];
             const SysS &st = A.S[i];
-            if (p.calc_wca && st.active && st.rebuild && !(st.flags & kFlagFatal)) {
+            bool part = false;
+            if (p.calc_wca && !(st.flags & kFlagFatal)) {
+                if (p.grp_n == 0) {
+                    part = st.active && st.rebuild;
+                } else {
+                    // coupled populations rebuild together: their cross lists
+                    // read one another's cells.  Only moving, running members
+                    // ask for a build (their flags are only ever set here, so
+                    // every thread of the group reaches the same answer).
+                    bool any = false;
+                    for (int k = 0; k < p.grp_n && k < kMaxPops; k++) {
+                        const int m = p.grp[k];
+                        if (m < 0 || m >= A.n_slots) continue;
+                        const SysS &sm = A.S[m];
+                        any |= !A.P[m].fixed && sm.active && sm.rebuild && !(sm.flags & kFlagFatal);
+                    }
+                    part = any && (p.fixed || st.active);
+                    if (part && !p.fixed && !st.rebuild) A.S[i].rebuild = 1;
+                }
+            }
+            if (part) {
                 v[0] = 1;
                 v[1] = p.n_bead_tiles;
                 v[2] = p.n_cell_tiles;
@@ -422,6 +444,86 @@ __global__ void __launch_bounds__(512) k_sort(BatchArgs A)
     }
 }
 
+// cross list c of bead b of a coupled population: every bead of partner
+// population q within its cross list radius, found through q's cell grid
+// (binned in the same list build), in ascending id -- the partner's own
+// nbor_list row of the reference (populations.py:156-180, updates.py:586-669
+// with pop2 another population: no chain exclusion)
+template <int D, int WHICH>
+__device__ void build_cross(const BatchArgs &A, const SysP &p, SysS &s, int c, int b, const double *x)
+{
+    const int qs = p.cross_q[c];
+    if (qs < 0 || qs >= A.n_slots) {
+        atomicOr(&s.flags, kFlagListCorrupt);
+        return;
+    }
+    const SysP &q = A.P[qs];
+    const double *XQ = stage_x<WHICH>(q);
+    const int nq = q.n, nc = q.nc, wnd = p.cross_w[c];
+    const double rl2 = p.cross_rl2[c];
+    int ci[3] = {0, 0, 0};
+#pragma unroll
+    for (int i = 0; i < D; i++) ci[i] = cell_coord(x[i], q.inv_h, nc);
+    // cells either side; a window as wide as the grid visits every cell once
+    const bool all = 2 * wnd + 1 >= nc;
+    const int lo = all ? 0 : -wnd, hi = all ? nc - 1 : wnd;
+    const int64_t row = p.x_off + (int64_t)c * p.n + b;
+    int *out = A.xnbr + row;
+    const int64_t stride = A.xstride;
+    const int cap = A.list_depth;
+    int cnt = 0;
+    bool bad = false;
+    const int zlo = (D == 3) ? lo : 0, zhi = (D == 3) ? hi : 0;
+    for (int dz = zlo; dz <= zhi; dz++) {
+        int cz = 0;
+        if (D == 3) {
+            cz = all ? dz : ci[2] + dz;
+            cz = ((cz % nc) + nc) % nc;
+        }
+        for (int dy = lo; dy <= hi; dy++) {
+            int cy = all ? dy : ci[1] + dy;
+            cy = ((cy % nc) + nc) % nc;
+            for (int dx = lo; dx <= hi; dx++) {
+                int cx = all ? dx : ci[0] + dx;
+                cx = ((cx % nc) + nc) % nc;
+                const int64_t gc = q.cell_off + ((int64_t)cz * nc + cy) * nc + cx;
+                int m = A.ncell[gc];
+                m = m < 0 ? 0 : (m < A.depth ? m : A.depth);
+                const int *it = A.items + (gc << A.log_depth);
+                for (int k = 0; k < m; k++) {
+                    const int j = it[k];
+                    if ((unsigned)j >= (unsigned)nq) {
+                        bad = true;
+                        continue;
+                    }
+                    double ds = 0.0;
+#pragma unroll
+                    for (int i = 0; i < D; i++) {
+                        double d = inbounds(XQ[(size_t)j * D + i], x[i], p.half_L, p.L);
+                        ds += d * d;
+                    }
+                    if (ds <= rl2) {
+                        if (cnt < cap) {
+                            int q2 = cnt;
+                            while (q2 > 0) {
+                                const int prev = out[(size_t)(q2 - 1) * stride];
+                                if (prev < j) break;
+                                out[(size_t)q2 * stride] = prev;
+                                q2--;
+                            }
+                            out[(size_t)q2 * stride] = j;
+                        }
+                        cnt++;
+                    }
+                }
+            }
+        }
+    }
+    A.xcount[row] = cnt < cap ? cnt : cap;
+    if (cnt > cap) atomicOr(&s.flags, kFlagListOverflow);
+    if (bad) atomicOr(&s.flags, kFlagListCorrupt);
+}
+
 // per bead of a flagged system: every non-excluded bead within r_l in the
 // 3^d cells around it, in ascending id; records the positions of the build
 template <int D, int WHICH>
@@ -433,7 +535,8 @@ __global__ void __launch_bounds__(512) k_build(BatchArgs A)
         const int sys = w.sys[k];
         const SysP &p = A.P[sys];
         SysS &s = A.S[sys];
-        if (!builds(p, s)) continue;
+        // a fixed population is only binned: it feels no force and never moves
+        if (!builds(p, s) || p.fixed) continue;
         const int begin = (t - w.bead0[k]) * A.tile_beads;
         if (begin == 0 && threadIdx.x == 0) s.list_builds += 1;  // one thread per system and build
         const int b = begin + threadIdx.x;
@@ -514,6 +617,7 @@ __global__ void __launch_bounds__(512) k_build(BatchArgs A)
         for (int i = 0; i < D; i++) r[i] = x[i];
         if (cnt > cap) atomicOr(&s.flags, kFlagListOverflow);
         if (bad) atomicOr(&s.flags, kFlagListCorrupt);
+        for (int c = 0; c < p.n_cross && c < kMaxPops - 1; c++) build_cross<D, WHICH>(A, p, s, c, b, x);
     }
 }
 
@@ -579,6 +683,82 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_pair(BatchArgs A)
         }
         if (bad) atomicOr(&s.flags, kFlagListCorrupt);
         FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
+#pragma unroll
+        for (int i = 0; i < D; i++) fp[i] = F[i];
+    }
+}
+
+// pair forces between coupled populations: the force on a bead of one
+// population from the beads of another (central_pair_force over the cross
+// nbor_list with other_pop another population, SRK.py:229-245; the pair
+// parameters of interpop_forces, updates.py:274-312; rule forces.WCA),
+// added to the bead's own pair force partner by partner, in the order the
+// reference adds the other populations' forces (SRK.py:287-294)
+template <int D, typename FT, int WHICH>
+__global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_cross(BatchArgs A)
+{
+    const int nt = *A.n_bead_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.bead_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        SysS &s = A.S[tl.sys];
+        if (p.n_cross <= 0 || !ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal)) continue;
+        const int b = tl.begin + threadIdx.x;
+        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
+        const double *X = stage_x<WHICH>(p);
+        double xb[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < D; i++) xb[i] = X[(size_t)b * D + i];
+        FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
+        FT F[3] = {FT(0), FT(0), FT(0)};
+        if (p.calc_wca) {
+#pragma unroll
+            for (int i = 0; i < D; i++) F[i] = fp[i];
+        }
+        bool bad = false;
+        for (int c = 0; c < p.n_cross && c < kMaxPops - 1; c++) {
+            const int qs = p.cross_q[c];
+            if ((unsigned)qs >= (unsigned)A.n_slots) {
+                bad = true;
+                continue;
+            }
+            const SysP &q = A.P[qs];
+            const double *XQ = stage_x<WHICH>(q);
+            const int nq = q.n;
+            const int64_t row = p.x_off + (int64_t)c * p.n + b;
+            int cnt = A.xcount[row];
+            cnt = cnt < 0 ? 0 : (cnt < A.list_depth ? cnt : A.list_depth);
+            const FT rc2 = (FT)p.cross_rc2[c], p0 = (FT)p.cross_p0[c], p1 = (FT)p.cross_p1[c];
+            const FT shift = (FT)p.cross_shift[c];
+            for (int k = 0; k < cnt; k++) {
+                const int j = A.xnbr[row + (int64_t)k * A.xstride];
+                if ((unsigned)j >= (unsigned)nq) {
+                    bad = true;
+                    continue;
+                }
+                FT sep[3];
+                FT ds = FT(0);
+#pragma unroll
+                for (int i = 0; i < D; i++) {
+                    sep[i] = (FT)inbounds(XQ[(size_t)j * D + i], xb[i], p.half_L, p.L);
+                    ds += sep[i] * sep[i];
+                }
+                if (!(FT(0) < ds && ds <= rc2)) continue;
+                if (shift != FT(0)) {
+                    FT mag = sqrt(ds);
+                    FT nm = mag + shift;
+                    nm = nm < FT(0) ? FT(0) : nm;
+                    FT rs = nm / mag;
+#pragma unroll
+                    for (int i = 0; i < D; i++) sep[i] *= rs;
+                    ds = nm * nm;
+                }
+                FT coeff = wca_coeff<FT>(ds, p0, p1);
+#pragma unroll
+                for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
+            }
+        }
+        if (bad) atomicOr(&s.flags, kFlagListCorrupt);
 #pragma unroll
         for (int i = 0; i < D; i++) fp[i] = F[i];
     }
@@ -1154,13 +1334,26 @@ __global__ void k_sys_dt(BatchArgs A, int n_slots)
     const SysP &p = A.P[i];
     SysS &s = A.S[i];
     if (!s.active || (s.flags & kFlagFatal)) return;
+    const double pref = A.order == 4 ? 1.0 : 0.5;
     double mf2s = __longlong_as_double((long long)s.max_f2);
-    double S = p.sqrt2D + (A.order == 4 ? 1.0 : 0.5) * sqrt(mf2s) / p.radius;
+    double S = p.sqrt2D + pref * sqrt(mf2s) / p.radius;
+    // coupled populations: one dt from the largest S over the moving members
+    // (the max over every thread's shared_arr[:,3], SRK.py:333-340)
+    double Sg = (p.grp_n && p.fixed) ? 0.0 : S;
+    for (int k = 0; k < p.grp_n && k < kMaxPops; k++) {
+        const int m = p.grp[k];
+        if (m < 0 || m >= n_slots || m == i) continue;
+        const SysP &pm = A.P[m];
+        const SysS &sm = A.S[m];
+        if (pm.fixed || !sm.active || (sm.flags & kFlagFatal)) continue;
+        const double Sm = pm.sqrt2D + pref * sqrt(__longlong_as_double((long long)sm.max_f2)) / pm.radius;
+        Sg = Sm > Sg ? Sm : Sg;
+    }
     double dt;
-    if (S == 0.0)
+    if (Sg == 0.0)
         dt = p.dtmax;
     else {
-        double q = p.mdps / S;
+        double q = p.mdps / Sg;
         dt = (q < p.dtmax) ? q : p.dtmax;
     }
     double dt_used = p.rk * dt;
@@ -1238,6 +1431,9 @@ struct StepKernels {
         k.rigid4[1] = (void *)k_rigid<D, FT, 11>;
         k.rigid4[2] = (void *)k_rigid<D, FT, 12>;
         k.rigid4[3] = (void *)k_rigid<D, FT, 13>;
+        k.cross[0] = (void *)k_cross<D, FT, 0>;
+        k.cross[1] = (void *)k_cross<D, FT, 1>;
+        k.cross[2] = (void *)k_cross<D, FT, 2>;
     }
 };
 

@@ -215,6 +215,20 @@ class Engine:
     def update_params(self, st: SystemState):
         check(self.lib.gcr_update_desc(self._ctx, st.slot, C.byref(st.params.desc(st.n, st.n_chains))))
 
+    def couple(self, slots, fixed, cross_wca):
+        """Step the resident systems ``slots`` as the populations of one box
+        (``gcr_couple``): one dt, joint list builds, and the WCA force
+        ``cross_wca[i][j] = [p0, p1, shift, r_cut]`` of population j on
+        population i.  ``fixed[i]``: population i never moves."""
+        n = len(slots)
+        cw = np.ascontiguousarray(np.asarray(cross_wca, dtype=np.float64).reshape(n, n, 4))
+        s_arr = (C.c_int32 * n)(*[int(s) for s in slots])
+        f_arr = (C.c_int32 * n)(*[1 if f else 0 for f in fixed])
+        check(self.lib.gcr_couple(self._ctx, n, s_arr, f_arr, cw.ctypes.data_as(C.POINTER(C.c_double))))
+
+    def decouple(self, slot):
+        check(self.lib.gcr_decouple(self._ctx, int(slot)))
+
     def call_begin(self, slot, max_steps, dt, max_dt_usable=-1.0, noise=None):
         """Arm one system for the next ``run``: the arguments of one
         ``SRK2_force_calc`` call (updates.py:138-146)."""

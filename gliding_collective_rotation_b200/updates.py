@@ -28,8 +28,12 @@ this step unchanged; while a population grows the step computes in FP64
 whatever ``gpu_precision`` says (radii down to 1e-8 put the WCA prefactors
 below the FP32 range).  ``config.SRK_order`` 4 runs the reference's SRK4
 branch (SRK.py:144-215, 296-321) and fills ``pop.forces_aux`` with the last
-stage's force.  Features outside the GPU path (walls, motors, FENE, active
-sliding, E-field, several populations) raise ``NotImplementedError``.
+stage's force.  A list of several populations (up to 4, fixed ones
+included) steps as the reference steps it (updates.py:146-247): one dt from
+the largest max-force value over the moving populations, and each moving
+population feels the others' WCA force (``interpop_forces``,
+updates.py:274-312), through ``gcr_couple``.  Features outside the GPU path
+(walls, motors, FENE, active sliding, E-field) raise ``NotImplementedError``.
 
 ``install(updates_module, config_module)`` rebinds a reference checkout's
 ``updates.SRK2_force_calc`` to this function and makes it read that
@@ -79,6 +83,52 @@ def _force_list(pop):
 
 
 _SUPPORTED = {"springs", "WCA", "self-propulsion"}
+
+
+def _pop_params(pop, status, sim, seed):
+    """The packed parameters of one population (its self_interactions, as
+    SRK.py:58-97 reads them) as a ``SystemParams``."""
+    cfg = _config
+    forces = _force_list(pop)
+    extra = set(forces) - _SUPPORTED
+    if extra:
+        raise NotImplementedError(f"forces not on the GPU step: {sorted(extra)}")
+    longest = int(pop.longest_chain_length)
+    calc_springs = "springs" in forces and longest > 1
+    spring = forces.get("springs", np.zeros(6))
+    if calc_springs and spring[3] != 0:
+        raise NotImplementedError("FENE springs are not part of the GPU step")
+    calc_wca = "WCA" in forces
+    wca = forces.get("WCA", np.zeros(4))
+    self_propel = "self-propulsion" in forces and bool(status.b_calc_active_forces)
+    active = forces.get("self-propulsion", np.zeros(3))
+    return SystemParams(
+        L=float(cfg.Lx), spring_params=spring, wca_params=wca, active_params=active, D=float(pop.D),
+        Dr=float(pop.Dr), radius=float(pop.repel_d_max), n_nearby=int(pop.n_nearby_beads_dont_repel),
+        calc_springs=calc_springs, calc_wca=calc_wca, self_propel=self_propel, dtmax=float(status.dtmax),
+        max_dist_per_step=float(cfg.max_dist_per_step), rk_cheat=float(cfg.RK_cheat_factor), seed=seed,
+        step=int(status.stepnum), cell_factor=float(sim.get('gpu_cell_factor', 1.0)),
+        skin=sim.get('gpu_skin', None), rigid_rod=float(getattr(pop, "rigid_rod_projection_factor", 0.0)))
+
+
+def _cross_wca(pop1, pop2):
+    """The WCA parameters of the force on ``pop1`` from ``pop2``:
+    interpop_forces(pop1, pop2) (updates.py:274-312) -- a special interaction
+    if ``pop1`` has one for ``pop2``, else ``pop1.interactions(pop2)`` -- with
+    the cutoff at the potential's minimum while either population grows.
+    Zeros: no pair force."""
+    if pop2.name in getattr(pop1, "special_interactions", {}):
+        forces_list = pop1.special_interactions[pop2.name]
+    else:
+        forces_list = pop1.interactions(pop2)
+    out = np.zeros(4)
+    for name, params in forces_list or []:
+        if name != "WCA":
+            raise NotImplementedError(f"force between populations not on the GPU step: {name}")
+        out = np.array(params, dtype=np.float64)[:4].copy()
+    if (getattr(pop1, "b_init_growing", False) or getattr(pop2, "b_init_growing", False)) and out[0] != 0:
+        out[3] = (out[1] / out[0]) ** (1 / 6)
+    return out
 
 
 class _GpuPop:
@@ -146,42 +196,25 @@ def SRK2_force_calc(pops, status, sim):
     if np.any(getattr(cfg, "walls", np.zeros(3, dtype=bool))):
         raise NotImplementedError("walls are not part of the GPU step")
     movers = [p for p in pops if not p.fixed]
-    if len(pops) != 1 or len(movers) != 1:
-        raise NotImplementedError("the GPU step advances exactly one population")
+    if not movers:
+        raise NotImplementedError("the GPU step needs a population that moves")
     if _pair_rule_check is not None:
         fr, fm = _pair_rule_check
         if fr.central_pair_force_rule is not fm.WCA:
             raise NotImplementedError("the GPU step implements the forces.WCA pair rule")
+    if len(pops) > 1:
+        return _srk2_populations(pops, status, sim, srk_order)
     pop = pops[0]
-    forces = _force_list(pop)
-    extra = set(forces) - _SUPPORTED
-    if extra:
-        raise NotImplementedError(f"forces not on the GPU step: {sorted(extra)}")
-    longest = int(pop.longest_chain_length)
     dim = int(cfg.dim)
     precision = sim.get('gpu_precision', 'fp64')
     if getattr(pop, "b_init_growing", False):
         precision = 'fp64'
-    calc_springs = "springs" in forces and longest > 1
-    spring = forces.get("springs", np.zeros(6))
-    if calc_springs and spring[3] != 0:
-        raise NotImplementedError("FENE springs are not part of the GPU step")
-    calc_wca = "WCA" in forces
-    wca = forces.get("WCA", np.zeros(4))
-    self_propel = "self-propulsion" in forces and bool(status.b_calc_active_forces)
-    active = forces.get("self-propulsion", np.zeros(3))
 
     # time_vals, updates.py:138-146
     max_dt_usable = (status.next_save_time - status.t) if sim.get('save_state_every', -1) > 0 else -1.0
     max_steps = status.next_output_step - status.stepnum
     seed = int(sim.get('seed', 0))
-    params = SystemParams(
-        L=float(cfg.Lx), spring_params=spring, wca_params=wca, active_params=active, D=float(pop.D),
-        Dr=float(pop.Dr), radius=float(pop.repel_d_max), n_nearby=int(pop.n_nearby_beads_dont_repel),
-        calc_springs=calc_springs, calc_wca=calc_wca, self_propel=self_propel, dtmax=float(status.dtmax),
-        max_dist_per_step=float(cfg.max_dist_per_step), rk_cheat=float(cfg.RK_cheat_factor), seed=seed,
-        step=int(status.stepnum), cell_factor=float(sim.get('gpu_cell_factor', 1.0)),
-        skin=sim.get('gpu_skin', None), rigid_rod=float(getattr(pop, "rigid_rod_projection_factor", 0.0)))
+    params = _pop_params(pop, status, sim, seed)
     g = _gpu_state(pop, sim, dim, precision, params, srk_order)
     st, eng = g.state, g.engine
 
@@ -286,4 +319,162 @@ def SRK2_force_calc(pops, status, sim):
     status.update_grid_list_counter = max(
         1, (steps_done + status.update_grid_list_counter) % cfg.n_steps_update_grid_list)
     status.gpu_flags = res['flags']
+    return None
+
+
+class _GpuGroup:
+    """Device copies of several populations in one context, coupled as one
+    box (``Engine.couple``)."""
+
+    def __init__(self, pops, sim, dim, precision, params, fixed, cell_depth, list_depth, key, srk_order):
+        self.key = key
+        self.dim, self.precision, self.srk_order = dim, precision, srk_order
+        self.fixed = list(fixed)
+        self.spg = int(sim.get('gpu_steps_per_graph', 10))
+        dev = torch.device("cuda")
+        self.states = [SystemState.from_host(p.pos, p.tangent_list, p.chain_id, p.rest_lengths, prm,
+                                             precision=precision, device=dev, srk_order=srk_order)
+                       for p, prm in zip(pops, params)]
+        ft = torch.float64 if precision == "fp64" else torch.float32
+        self.host = []
+        for p in pops:
+            n = p.total_pop
+            self.host.append(dict(pos=torch.empty((n, dim), dtype=torch.float64, pin_memory=True),
+                                  pos1=torch.empty((n, dim), dtype=torch.float64, pin_memory=True),
+                                  tan=torch.empty((n, dim), dtype=ft, pin_memory=True),
+                                  frc=torch.empty((n, dim), dtype=ft, pin_memory=True)))
+        self.engine = None
+        self.cross = None
+        self.make_engine(cell_depth, list_depth)
+
+    def make_engine(self, cell_depth, list_depth):
+        if self.engine is not None:
+            self.engine.close()
+        cfg = default_config(self.dim, self.precision, cell_depth=cell_depth, list_depth=list_depth,
+                             srk_order=self.srk_order)
+        cells = sum(footprint(cfg, st.params, st.n, st.n_chains)[0] for st in self.states)
+        self.engine = Engine(self.dim, self.precision, bead_capacity=sum(st.n for st in self.states),
+                             system_capacity=len(self.states), cell_capacity=max(cells, 1), cell_depth=cell_depth,
+                             list_depth=list_depth, steps_per_graph=self.spg, device=self.states[0].pos.device,
+                             srk_order=self.srk_order)
+        for st in self.states:
+            self.engine.admit(st)
+        if self.cross is not None:
+            self.engine.couple([st.slot for st in self.states], self.fixed, self.cross)
+
+    def set_cross(self, cross):
+        if self.cross is None or not np.array_equal(cross, self.cross):
+            self.cross = cross
+            self.engine.couple([st.slot for st in self.states], self.fixed, cross)
+
+
+def _srk2_populations(pops, status, sim, srk_order):
+    """SRK2_force_calc over several populations (updates.py:146-247): each
+    population is a system of one context; the systems step under one dt,
+    rebuild their lists together and feel each other's WCA force
+    (interpop_forces, SRK.py:229-245, 287-294).  Fixed populations
+    (pop.fixed) never move.  Philox noise with the seed ``sim['seed'] + k``
+    for population k."""
+    cfg = _config
+    dim = int(cfg.dim)
+    if sim.get('gpu_noise', 'philox') != 'philox':
+        raise NotImplementedError("several populations draw the Philox stream")
+    precision = sim.get('gpu_precision', 'fp64')
+    if any(getattr(p, "b_init_growing", False) for p in pops):
+        precision = 'fp64'
+    if len(pops) > 4:
+        raise NotImplementedError("the GPU step couples at most 4 populations")
+    seed = int(sim.get('seed', 0))
+    params = [_pop_params(p, status, sim, seed + k) for k, p in enumerate(pops)]
+    if not all(prm.calc_wca for prm in params):
+        raise NotImplementedError("every population of the GPU step has the WCA force")
+    fixed = [bool(p.fixed) for p in pops]
+    n = len(pops)
+    cross = np.zeros((n, n, 4))
+    for k, pk in enumerate(pops):
+        for q, pq in enumerate(pops):
+            if k != q and not fixed[k]:
+                cross[k, q] = _cross_wca(pk, pq)
+    max_dt_usable = (status.next_save_time - status.t) if sim.get('save_state_every', -1) > 0 else -1.0
+    max_steps = status.next_output_step - status.stepnum
+    depth = getattr(pops[0], "_gcr_cell_depth",
+                    default_depth(dim, max(cell_scale(prm) for prm in params)))
+    ldepth = getattr(pops[0], "_gcr_list_depth", default_list_depth(dim))
+    key = (tuple((p.total_pop, len(p.rest_lengths)) for p in pops), tuple(fixed), dim, precision,
+           float(cfg.Lx), depth, ldepth, srk_order)
+    g = getattr(pops[0], "_gcr_group", None)
+    if g is None or g.key != key:
+        if g is not None:
+            g.engine.close()
+        g = _GpuGroup(pops, sim, dim, precision, params, fixed, depth, ldepth, key, srk_order)
+        pops[0]._gcr_group = g
+    eng = g.engine
+    for p, st, prm, h in zip(pops, g.states, params, g.host):
+        h["pos"].numpy()[:] = p.pos
+        h["tan"].numpy()[:] = p.tangent_list
+        st.pos.copy_(h["pos"], non_blocking=True)
+        st.tangent.copy_(h["tan"], non_blocking=True)
+        st.rest_lengths.copy_(torch.from_numpy(np.asarray(p.rest_lengths, dtype=np.float64)))
+        st.params = prm
+    try:
+        for st in g.states:
+            eng.update_params(st)
+    except GcrError as e:
+        if e.code != -6:
+            raise
+        g.make_engine(eng.cfg.cell_depth, eng.cfg.list_depth)
+        eng = g.engine
+    g.set_cross(cross)
+
+    done, elapsed, dt = 0, 0.0, float(status.dt)
+    lead = fixed.index(False)  # the first moving population reports status (shared_arr[0])
+    while True:
+        left = max_steps - done if max_steps >= 0 else -1
+        lim = max_dt_usable - elapsed if max_dt_usable >= 0 else -1.0
+        eng.call_begin_many([st.slot for st in g.states], left, [dt] * n, lim)
+        if left >= 0 and max_dt_usable < 0:
+            eng.run(left, sync_every=0)
+        else:
+            eng.run(left if left >= 0 else (1 << 62), sync_every=1)
+        sts = [eng.status(st.slot) for st in g.states]
+        res = sts[lead]
+        done += int(res['steps_done'])
+        elapsed += res['dt_used']
+        dt = res['dt']
+        flags = 0
+        for r in sts:
+            flags |= r['flags']
+        grow_cells = bool(flags & FLAG_CELL_OVERFLOW) and eng.cfg.cell_depth < MAX_DEPTH
+        grow_lists = bool(flags & FLAG_LIST_OVERFLOW) and eng.cfg.list_depth < MAX_LIST_DEPTH
+        if not (grow_cells or grow_lists) or done == max_steps or (max_dt_usable >= 0 and elapsed >= max_dt_usable):
+            break
+        depth = min(MAX_DEPTH, 2 * eng.cfg.cell_depth) if grow_cells else eng.cfg.cell_depth
+        ldepth = min(MAX_LIST_DEPTH, 2 * eng.cfg.list_depth) if grow_lists else eng.cfg.list_depth
+        pops[0]._gcr_cell_depth, pops[0]._gcr_list_depth = depth, ldepth
+        for st, r in zip(g.states, sts):
+            st.params.step = int(r['step'])
+        g.make_engine(depth, ldepth)
+        g.key = key[:5] + (depth, ldepth, srk_order)
+        eng = g.engine
+    for st, h in zip(g.states, g.host):
+        h["pos"].copy_(st.pos, non_blocking=True)
+        h["pos1"].copy_(st.pos1, non_blocking=True)
+        h["tan"].copy_(st.tangent, non_blocking=True)
+        h["frc"].copy_(st.forces, non_blocking=True)
+    torch.cuda.synchronize(eng.device)
+    for p, h, fx in zip(pops, g.host, fixed):
+        if fx:
+            continue
+        p.pos[:] = h["pos"].numpy()
+        p.pos1[:] = h["pos1"].numpy()
+        p.tangent_list[:] = h["tan"].numpy()
+        p.forces[:] = h["frc"].numpy()
+    status.dt = dt
+    status.dt_used = elapsed
+    status.stepnum += done
+    status.t += status.dt_used
+    status.max_forces_strength = res['max_forces_strength']
+    status.update_grid_list_counter = max(
+        1, (done + status.update_grid_list_counter) % cfg.n_steps_update_grid_list)
+    status.gpu_flags = flags
     return None

@@ -27,6 +27,9 @@
  *                                updates.update_nbor_list   updates.py:586-669
  *   gcr_system_desc.rigid_rod <- updates.project_updates_for_rigid_rod updates.py:347-499
  *                                (applied as SRK.py:364-378 applies it)
+ *   gcr_couple                <- SRK2_force_calc over several populations updates.py:146-247,
+ *                                interpop_forces updates.py:274-312, cross-population pair
+ *                                forces SRK.py:229-245, 287-294
  *   gcr_order_params          <- output_methods.calc_avg_phi_chain output_methods.py:492-510,
  *                                analysis.polar_orderparameter analysis.py:315-328,
  *                                analysis.nematic_orderparameter analysis.py:294-313
@@ -180,6 +183,34 @@ GCR_API int gcr_call_begin_batch(gcr_ctx *ctx, int32_t n, const int32_t *slots, 
 /* Cells and bytes a system of this description would occupy. */
 GCR_API int gcr_footprint(const gcr_config *cfg, const gcr_system_desc *desc, int64_t *cells_out,
                   int64_t *bytes_out);
+
+/* ---- several populations in one box ------------------------------------ */
+#define GCR_MAX_POPULATIONS 4
+/* Couple 2..4 resident systems as the populations of one box, listed in the
+ * reference's population order (config.pop_name_list): the multi-population
+ * updates.SRK2_force_calc (updates.py:146-247) with the SRK loop's
+ * cross-population pair forces (SRK.py:229-245, 287-294).  From the next
+ * gcr_run the members
+ *   - step under one dt: the max-force rule (SRK.py:323-353) over the largest
+ *     sqrt(2D) + pref max|F|/r of the moving members, the max over every
+ *     thread's shared_arr[:,3];
+ *   - rebuild their neighbour lists together;
+ *   - each moving member i feels, after its own pair force, the WCA force of
+ *     each other member j, taken j = i+1, i+2, ... (mod n) as the reference
+ *     adds them, with parameters cross_wca[(i*n + j)*4 + 0..3] = [p0, p1,
+ *     shift, r_cut] of forces.WCA (interpop_forces, updates.py:274-312: the
+ *     mean of the two WCA parameter sets unless a special interaction says
+ *     otherwise); r_cut <= 0 or p0 = p1 = 0 means no force.
+ * fixed[i] != 0 (pop.fixed): member i never moves and feels no force, but
+ * still acts on the others.  Every member needs calc_wca and the same L; the
+ * moving members need the same dtmax, max_dist_per_step and rk_cheat, and are
+ * armed together with the same limits for each call.  Calling it again with
+ * the same members in the same order replaces fixed and cross_wca. */
+GCR_API int gcr_couple(gcr_ctx *ctx, int32_t n, const int32_t *slots, const int32_t *fixed,
+                       const double *cross_wca);
+/* Dissolve the coupled group that holds `slot` (no-op when there is none);
+ * evicting a member does the same. */
+GCR_API int gcr_decouple(gcr_ctx *ctx, int32_t slot);
 
 /* ---- stepping --------------------------------------------------------- */
 /* Advance every armed system until its limits are reached or `max_steps`

@@ -1133,6 +1133,260 @@ GCRO_EXPORT int gcro_srk2_run(const gcro_params *p, gcro_state *st, gcro_result 
 }
 
 /* ------------------------------------------------------------------ */
+/* Several populations in one box: updates.SRK2_force_calc over a list */
+/* of populations (updates.py:146-247) with the cross-population pair  */
+/* forces of the SRK loop (SRK.py:229-245, 287-294), SRK2, one thread  */
+/* per population.                                                     */
+/* ------------------------------------------------------------------ */
+
+/* forces.central_pair_force with rule forces.WCA (forces.py:13-15, 57-145)
+ * between population P (beads XP) and population Q (beads XQ), restated
+ * over all pairs: bead b of P gets the force of every bead j of Q within
+ * r_cut, in ascending j.  same != 0 (Q is P): b itself and the beads of its
+ * chain within n_nearby of it (the whole chain for n_nearby < 0) are
+ * excluded, as update_nbor_list excludes them (updates.py:586-669).  The
+ * reference walks a Verlet list built from cells: the same pairs while the
+ * list is fresh, summed in the list's order. */
+static void pair_forces_all(const double *XP, int64_t nP, const int64_t *chainP, int64_t n_nearby,
+                            const double *XQ, int64_t nQ, int same, const double *wp, double L, int dim,
+                            double *F)
+{
+    const double half_L = L / 2.0, rc_sq = wp[3] * wp[3];
+    double seps[3];
+    for (int64_t b = 0; b < nP; b++) {
+        for (int64_t j = 0; j < nQ; j++) {
+            if (same) {
+                if (j == b) continue;
+                if (chainP[j] == chainP[b]) {
+                    int64_t d = j > b ? j - b : b - j;
+                    if (n_nearby < 0 || d <= n_nearby) continue;
+                }
+            }
+            double ds = 0.0;
+            for (int i = 0; i < dim; i++) {
+                double sep = XQ[j * dim + i] - XP[b * dim + i];
+                if (sep < -half_L)
+                    sep += L;
+                else if (sep >= half_L)
+                    sep -= L;
+                seps[i] = sep;
+                ds += sep * sep;
+            }
+            if (0.0 < ds && ds <= rc_sq) {
+                if (wp[2] != 0.0) {
+                    double mag = sqrt(ds);
+                    double nm = mag + wp[2];
+                    if (nm < 0.0) nm = 0.0;
+                    double rescale = nm / mag;
+                    for (int i = 0; i < dim; i++) seps[i] *= rescale;
+                    ds = nm * nm;
+                }
+                double coeff = ipow_neg(ds, 4) * (wp[0] - wp[1] * ipow_neg(ds, 3));
+                for (int i = 0; i < dim; i++) F[b * dim + i] += seps[i] * coeff;
+            }
+        }
+    }
+}
+
+GCRO_EXPORT void gcro_pair_forces_all(const double *XP, int64_t nP, const int64_t *chainP, int64_t n_nearby,
+                                      const double *XQ, int64_t nQ, int same, const double *wp, double L, int dim,
+                                      double *F)
+{
+    pair_forces_all(XP, nP, chainP, n_nearby, XQ, nQ, same, wp, L, dim, F);
+}
+
+/* n_pops populations: ps[k] / sts[k] as gcro_srk2_run takes them (one
+ * thread each; the lists of sts[k] are not used), fixed[k] (pop.fixed: never
+ * moves, feels nothing, acts on the others), cross[(k*n + q)*4 + 0..3] the
+ * WCA parameters of the force on population k from population q
+ * (interpop_forces, updates.py:274-312; r_cut <= 0 or p0 = p1 = 0: none).
+ * The call's time values come from g (dt, dtmax, max_dist_per_step,
+ * rk_cheat, max_dt_usable, max_steps, noise_mode, step0); noise modes as
+ * gcro_srk2_run (0: sts[k]->mt[0], 1: injected, 2: Philox with ps[k]->seed).
+ * out->max_forces_strength is the first moving population's own value
+ * (shared_arr[0, 3], the thread of the first population pair). */
+GCRO_EXPORT int gcro_group_run(int n_pops, const gcro_params *const *ps, gcro_state *const *sts,
+                               const int32_t *fixed, const double *cross, const gcro_params *g, gcro_result *out)
+{
+    if (n_pops < 1 || n_pops > 8) return -1;
+    const int dim = g->dim;
+    const double L = g->L;
+    double *tmp[8], *rscr[8];
+    int64_t nmax = 1;
+    for (int k = 0; k < n_pops; k++) nmax = ps[k]->n_beads > nmax ? ps[k]->n_beads : nmax;
+    for (int k = 0; k < n_pops; k++) {
+        tmp[k] = (double *)calloc((size_t)nmax * dim, sizeof(double));
+        rscr[k] = (double *)malloc(sizeof(double) * (size_t)nmax * 7);
+    }
+    int first = -1;
+    for (int k = 0; k < n_pops; k++)
+        if (!fixed[k] && first < 0) first = k;
+    double dt = g->dt, elapsed = 0.0, mfs0 = 0.0;
+    int64_t steps = 0;
+    while ((steps < g->max_steps || g->max_steps < 0) && (elapsed < g->max_dt_usable || g->max_dt_usable < 0)) {
+        /* noise, SRK.py:134-142, and the SRK2 force wipe */
+        for (int k = 0; k < n_pops; k++) {
+            if (fixed[k]) continue;
+            const gcro_params *p = ps[k];
+            gcro_state *st = sts[k];
+            const int64_t n = p->n_beads;
+            double *noise = st->noise;
+            if (g->noise_mode == 0) {
+                if (p->D > 0)
+                    for (int64_t b = 0; b < n; b++)
+                        for (int i = 0; i < dim; i++) noise[b * 2 * dim + i] = draw_normal(st, 0);
+                if (p->Dr > 0)
+                    for (int64_t b = 0; b < n; b++)
+                        for (int i = dim; i < 2 * dim; i++) noise[b * 2 * dim + i] = draw_normal(st, 0);
+            } else if (g->noise_mode == 1) {
+                int64_t s = steps < st->noise_inject_steps ? steps : st->noise_inject_steps - 1;
+                const double *src = st->noise_inject + s * n * 2 * dim;
+                for (int64_t b = 0; b < n * 2 * dim; b++) noise[b] = src[b];
+            } else {
+                for (int64_t b = 0; b < n; b++) {
+                    double z[4];
+                    double *row = noise + b * 2 * dim;
+                    int64_t gs = g->step0 + steps;
+                    if (p->D > 0) {
+                        gcro_philox_pair(p->seed, (uint32_t)b, gs, 0u, z);
+                        if (dim == 3) gcro_philox_pair(p->seed, (uint32_t)b, gs, 1u, z + 2);
+                        for (int i = 0; i < dim; i++) row[i] = z[i];
+                    }
+                    if (p->Dr > 0) {
+                        gcro_philox_pair(p->seed, (uint32_t)b, gs, 2u, z);
+                        if (dim == 3) gcro_philox_pair(p->seed, (uint32_t)b, gs, 3u, z + 2);
+                        for (int i = 0; i < dim; i++) row[dim + i] = z[i];
+                    }
+                }
+            }
+            for (int64_t b = 0; b < n * dim; b++) st->forces[b] = 0.0;
+        }
+        double dt_for_update = dt;
+        for (int stage = 0; stage < 2; stage++) {
+            const double pref = stage == 0 ? 1.0 : 0.5;
+            /* forces taken at pos (stage 0) or pos1; a fixed population's pos1 is its pos */
+            double *X[8];
+            for (int k = 0; k < n_pops; k++) X[k] = (stage == 0 || fixed[k]) ? sts[k]->pos : sts[k]->pos1;
+            for (int k = 0; k < n_pops; k++) {
+                if (fixed[k]) continue;
+                const gcro_params *p = ps[k];
+                gcro_state *st = sts[k];
+                if (p->calc_springs)
+                    spring_forces(X[k], st->tangent, st->chain_id, st->forces, p->n_beads, L, p->spring,
+                                  st->rest_lengths, dim);
+                if (p->calc_wca)
+                    pair_forces_all(X[k], p->n_beads, st->chain_id, p->n_nearby, X[k], p->n_beads, 1, p->wca, L,
+                                    dim, st->forces);
+                if (p->self_propel) self_propel(st->forces, st->tangent, p->n_beads, p->active, dim);
+            }
+            /* the other populations' forces, added in turns (SRK.py:287-294) */
+            for (int ii = 1; ii < n_pops; ii++)
+                for (int k = 0; k < n_pops; k++) {
+                    if (fixed[k]) continue;
+                    const int q = (k + ii) % n_pops;
+                    const double *w = cross + ((size_t)k * n_pops + q) * 4;
+                    if (!(w[3] > 0.0) || (w[0] == 0.0 && w[1] == 0.0)) continue;
+                    const int64_t n = ps[k]->n_beads;
+                    memset(tmp[k], 0, sizeof(double) * (size_t)n * dim);
+                    pair_forces_all(X[k], n, sts[k]->chain_id, 0, X[q], ps[q]->n_beads, 0, w, L, dim, tmp[k]);
+                    for (int64_t b = 0; b < n * dim; b++) sts[k]->forces[b] += tmp[k][b];
+                }
+            if (stage == 1) {
+                /* SRK.py:323-353 over every moving population */
+                double Sg = 0.0;
+                for (int k = 0; k < n_pops; k++) {
+                    if (fixed[k]) continue;
+                    const gcro_params *p = ps[k];
+                    const double *F = sts[k]->forces;
+                    double S = sqrt(2.0 * p->D);
+                    if (p->n_beads > 0) {
+                        double m = -1.0;
+                        for (int64_t b = 0; b < p->n_beads; b++) {
+                            double s2 = 0.0;
+                            for (int i = 0; i < dim; i++) s2 += F[b * dim + i] * F[b * dim + i];
+                            if (s2 > m) m = s2;
+                        }
+                        S += pref * sqrt(m) / p->radius;
+                    }
+                    if (k == first) mfs0 = S;
+                    if (S > Sg) Sg = S;
+                }
+                if (Sg == 0.0)
+                    dt = g->dtmax;
+                else {
+                    double c = g->max_dist_per_step / Sg;
+                    dt = g->dtmax < c ? g->dtmax : c;
+                }
+                double dt_used = g->rk_cheat * dt;
+                if (g->max_dt_usable > 0) {
+                    double lim = g->max_dt_usable - elapsed;
+                    if (lim < dt_used) dt_used = lim;
+                }
+                elapsed += dt_used;
+                dt_for_update = dt_used;
+            }
+            for (int k = 0; k < n_pops; k++) {
+                if (fixed[k]) continue;
+                const gcro_params *p = ps[k];
+                gcro_state *st = sts[k];
+                const int64_t n = p->n_beads;
+                double *W = stage == 0 ? st->pos1 : st->pos;
+                double dt_eff = dt_for_update * pref;
+                const double s2 = sqrt(2.0 * dt_for_update * p->D);
+                const int rigid = p->rigid_rod != 0.0 && p->longest_chain_length > 2;
+                if (n > 0 && rigid) {
+                    project_rigid(W, X[k], st->forces, st->noise, n, st->chain_id, st->rest_lengths, p->rigid_rod, L,
+                                  dt_eff, p->D, p->radius, dim, rscr[k], rscr[k] + 3 * n, rscr[k] + 6 * n);
+                } else {
+                    dt_eff /= p->radius;
+                    for (int64_t b = 0; b < n; b++)
+                        for (int i = 0; i < dim; i++) {
+                            double t = st->pos[b * dim + i] + dt_eff * st->forces[b * dim + i];
+                            if (s2 != 0.0) t += s2 * st->noise[b * 2 * dim + i];
+                            W[b * dim + i] = py_mod(t, L);
+                        }
+                }
+            }
+        }
+        /* rotational diffusion, SRK.py:399-423 */
+        for (int k = 0; k < n_pops; k++) {
+            const gcro_params *p = ps[k];
+            const int b_get_orientations = p->calc_springs ? (p->spring[4] != 0.0) : 0;
+            if (fixed[k] || !(p->Dr > 0) || b_get_orientations) continue;
+            gcro_state *st = sts[k];
+            double sq = sqrt(2.0 * dt_for_update * p->Dr) * 3.141592653589793;
+            for (int64_t b = 0; b < p->n_beads; b++) {
+                double *xr = st->noise + b * 2 * dim + dim;
+                double *tb = st->tangent + b * dim;
+                double proj = 0.0;
+                for (int i = 0; i < dim; i++) proj += xr[i] * tb[i];
+                for (int i = 0; i < dim; i++) xr[i] -= proj * tb[i];
+                double mag = 0.0;
+                for (int i = 0; i < dim; i++) {
+                    double v = tb[i] + sq * xr[i];
+                    mag += v * v;
+                    tb[i] = v;
+                }
+                mag = sqrt(mag);
+                for (int i = 0; i < dim; i++) tb[i] /= mag;
+            }
+        }
+        steps++;
+    }
+    for (int k = 0; k < n_pops; k++) {
+        free(tmp[k]);
+        free(rscr[k]);
+    }
+    out->dt = dt;
+    out->dt_used_total = elapsed;
+    out->steps = (double)steps;
+    out->max_forces_strength = mfs0;
+    out->counter = 0.0;
+    out->flag = 0.0;
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
 /* Observables                                                         */
 /* ------------------------------------------------------------------ */
 

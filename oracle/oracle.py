@@ -116,6 +116,11 @@ def lib():
         L.gcro_chunk_chain.restype = C.c_int
         L.gcro_chunk_chain.argtypes = [C.c_int64, C.c_int64, C.c_void_p, C.c_void_p]
         L.gcro_order_params.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
+        L.gcro_pair_forces_all.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
+                                           C.c_int, C.c_void_p, C.c_double, C.c_int, C.c_void_p]
+        L.gcro_group_run.restype = C.c_int
+        L.gcro_group_run.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Params),
+                                     C.POINTER(Result)]
         L.gcro_project_rigid.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p,
                                          C.c_void_p, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                          C.c_int]
@@ -327,6 +332,21 @@ class OracleSystem:
             seed=0, step0=0, n_threads=1, calc_active=True):
         """Run ``SRK_jit`` for up to ``n_steps`` steps.  Returns the row
         ``shared_arr[0]`` as a dict (dt, elapsed, steps, max force, flag)."""
+        p = self._params(n_threads, noise_mode, calc_active)
+        p.dt = dt
+        p.dtmax = dt if dtmax is None else dtmax
+        p.max_dist_per_step, p.rk_cheat, p.max_dt_usable = max_dist_per_step, rk_cheat, max_dt_usable
+        p.steps_until_update, p.n_steps_update, p.max_steps = steps_until_update, n_steps_update, n_steps
+        p.seed, p.step0 = seed, step0
+        res = Result()
+        st = self._state()
+        rc = lib().gcro_srk2_run(C.byref(p), C.byref(st), C.byref(res))
+        if rc != 0:
+            raise RuntimeError(f"oracle srk2 run failed ({rc})")
+        return {"dt": res.dt, "dt_used": res.dt_used_total, "steps": int(res.steps),
+                "max_forces_strength": res.max_forces_strength, "flag": res.flag}
+
+    def _params(self, n_threads=1, noise_mode=NOISE_MT, calc_active=True):
         p = Params()
         p.dim, p.n_threads, p.L = self.dim, n_threads, self.L
         p.n_beads, p.n_chains = self.N, len(self.rest_lengths)
@@ -342,19 +362,9 @@ class OracleSystem:
         p.D, p.Dr, p.radius, p.rigid_rod = self.D, self.Dr, self.radius, self.rigid_rod
         p.n_nearby, p.longest_chain_length = self.n_nearby, self.longest_chain_length
         p.grid_factor = self.grid_factor
-        p.dt = dt
-        p.dtmax = dt if dtmax is None else dtmax
-        p.max_dist_per_step, p.rk_cheat, p.max_dt_usable = max_dist_per_step, rk_cheat, max_dt_usable
-        p.steps_until_update, p.n_steps_update, p.max_steps = steps_until_update, n_steps_update, n_steps
-        p.seed, p.step0 = seed, step0
         p.srk_order = self.srk_order
-        res = Result()
-        st = self._state()
-        rc = lib().gcro_srk2_run(C.byref(p), C.byref(st), C.byref(res))
-        if rc != 0:
-            raise RuntimeError(f"oracle srk2 run failed ({rc})")
-        return {"dt": res.dt, "dt_used": res.dt_used_total, "steps": int(res.steps),
-                "max_forces_strength": res.max_forces_strength, "flag": res.flag}
+        p.seed = getattr(self, "seed", 0)
+        return p
 
     def chain_start(self):
         cs = np.flatnonzero(np.diff(self.chain_id)) + 1
@@ -362,3 +372,66 @@ class OracleSystem:
 
     def order_params(self):
         return order_params(self.tangent_list, self.chain_start())
+
+
+# ---------------------------------------------------------------------------
+# several populations in one box
+# ---------------------------------------------------------------------------
+
+def mean_wca(wca_a, wca_b):
+    """The default cross parameters: ``0.5 * (WCA_params + other.WCA_params)``
+    (``WCA_Population.interactions``, populations.py:226-232)."""
+    return 0.5 * (np.asarray(wca_a, dtype=np.float64) + np.asarray(wca_b, dtype=np.float64))
+
+
+def cross_forces(pos_p, pos_q, wca_params, L):
+    """The WCA force on every bead of population P from the beads of
+    population Q (forces.central_pair_force over P's nbor_list of Q), over all
+    pairs within the cutoff."""
+    pos_p = np.ascontiguousarray(pos_p, dtype=np.float64)
+    pos_q = np.ascontiguousarray(pos_q, dtype=np.float64)
+    out = np.zeros_like(pos_p)
+    chain = np.zeros(len(pos_p), dtype=np.int64)
+    lib().gcro_pair_forces_all(_p(pos_p), len(pos_p), _p(chain), 0, _p(pos_q), len(pos_q), 0,
+                               _p(np.ascontiguousarray(wca_params, dtype=np.float64)), float(L), pos_p.shape[1],
+                               _p(out))
+    return out
+
+
+class OracleGroup:
+    """Populations stepped together as ``updates.SRK2_force_calc`` steps a list
+    of populations (updates.py:146-247): one dt from the largest max-force
+    value over the moving populations, and the force of every other
+    population added after a population's own forces (SRK.py:229-245,
+    287-294).  SRK2, one thread per population; pair forces over all pairs.
+
+    ``systems``: ``OracleSystem`` per population (each with a ``seed``
+    attribute for the Philox stream), ``fixed[k]``: population k never moves,
+    ``cross[k][q]``: the WCA parameters of the force on k from q."""
+
+    def __init__(self, systems, fixed, cross):
+        self.systems = list(systems)
+        n = len(self.systems)
+        self.fixed = np.asarray([1 if f else 0 for f in fixed], dtype=np.int32)
+        self.cross = np.ascontiguousarray(np.asarray(cross, dtype=np.float64).reshape(n, n, 4))
+
+    def run(self, n_steps, dt, dtmax=None, max_dist_per_step=math.inf, rk_cheat=1.0, max_dt_usable=-1.0,
+            noise_mode=NOISE_PHILOX, step0=0, calc_active=True):
+        L = lib()
+        n = len(self.systems)
+        ps = [s._params(1, noise_mode, calc_active) for s in self.systems]
+        sts = [s._state() for s in self.systems]
+        g = Params()
+        s0 = self.systems[0]
+        g.dim, g.L, g.dt = s0.dim, s0.L, dt
+        g.dtmax = dt if dtmax is None else dtmax
+        g.max_dist_per_step, g.rk_cheat, g.max_dt_usable = max_dist_per_step, rk_cheat, max_dt_usable
+        g.max_steps, g.noise_mode, g.step0 = n_steps, noise_mode, step0
+        p_arr = (C.POINTER(Params) * n)(*[C.pointer(p) for p in ps])
+        s_arr = (C.POINTER(State) * n)(*[C.pointer(st) for st in sts])
+        res = Result()
+        rc = L.gcro_group_run(n, p_arr, s_arr, _p(self.fixed), _p(self.cross), C.byref(g), C.byref(res))
+        if rc != 0:
+            raise RuntimeError(f"oracle group run failed ({rc})")
+        return {"dt": res.dt, "dt_used": res.dt_used_total, "steps": int(res.steps),
+                "max_forces_strength": res.max_forces_strength}
