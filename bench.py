@@ -2,7 +2,7 @@
 """Benchmark of the gliding-collective-rotation SRK2 step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gcr|reference]
-                    [--workload sweep|large|config1|config5] [--precision mixed|fp64]
+                    [--workload sweep|large|config1|config5|pops] [--precision mixed|fp64]
 
 Default workload: the batched sweep -- 256 independent 2D systems (chains of
 5-40 beads, 50-4000 chains per system, area fraction 0.1-0.4, chirality and
@@ -68,9 +68,20 @@ def make_workload(name, rank=0, scale=1.0, systems=256):
     elif name == "config5":
         specs = [W.config5(seed=rank, scale=scale)]
         desc = "3D precision stress: L=200, 40,000 chains x 25 beads, LJ eps 1, Dr 0.1, SRK2"
+    elif name == "pops":
+        specs, groups = W.populations(n_boxes=max(1, systems // 2), seed=rank)
+        specs = _Specs(specs)
+        specs.groups = groups
+        desc = (f"two populations per box: {len(groups)} 2D boxes L=150, 1000 chains x 10 beads (WCA, v0=1) and "
+                "3000 passive beads of diameter 0.7, one dt per box, cross WCA = mean parameters, SRK2")
     else:
         raise SystemExit(f"unknown workload {name}")
     return specs, desc
+
+
+class _Specs(list):
+    """Workload specs; ``groups``: populations coupled in one box."""
+    groups = ()
 
 
 # --------------------------------------------------------------------------
@@ -268,6 +279,9 @@ def run_gpu(args):
         sp.params.skin = args.skin if args.skin >= 0 else None
     batch = Batch(specs, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph,
                   ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads, list_depth=args.list_depth or None)
+    groups = list(getattr(specs, "groups", ()))
+    for members, fixed, cross in groups:
+        batch.couple(members, fixed, cross)
     eng = batch.engine
     n_beads = batch.n_beads
     # untimed warm-up; every step after it, timed or not, follows the
@@ -351,7 +365,7 @@ def run_gpu(args):
 
     # ---- plain path: one system per launch sequence ---------------------
     plain = None
-    if args.plain and len(specs) > 1:
+    if args.plain and len(specs) > 1 and not groups:
         pr = PlainRunner(specs, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph)
         pr.copy_state_from(batch)
         pr.begin(args.plain_steps)
@@ -403,7 +417,9 @@ def run_gpu(args):
 
     # ---- CPU baseline (rank 0, N = 1) ------------------------------------
     cpu = None
-    if world == 1 and args.cpu_baseline:
+    # (coupled populations: the CPU sampler steps single populations, so
+    # no CPU line for them)
+    if world == 1 and args.cpu_baseline and not groups:
         host_states = [(s.pos.cpu().numpy(), s.tangent.double().cpu().numpy()) for s in batch.states]
         threads = os.cpu_count() or 1
         r, used, secs = cpu_sample_rate(specs, host_states, args.cpu_steps, threads, max_systems=args.cpu_systems,
@@ -425,6 +441,7 @@ def run_gpu(args):
                    "precision": ("FP32 forces and SRK arithmetic, FP64 positions" if args.precision == "mixed"
                                  else "FP64"),
                    "parallelism": f"{world} GPU(s), independent systems per GPU",
+                   "coupled_groups": len(groups),
                    "l2": f"inputs larger than L2: working set {working_set / 1e6:.0f} MB per GPU > 126 MB",
                    "relax_steps": relax_steps, "steps_done": steps_done, "flags": flags,
                    "dt_rule": "adaptive (SRK.py:323-353): dtmax = configured dt, max_dist_per_step of "
@@ -563,7 +580,8 @@ def main():
     ap.add_argument("--steps", type=int, default=1000)
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="gcr", choices=["gcr", "reference"])
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "large", "config1", "config5", "serve"])
+    ap.add_argument("--workload", default="sweep",
+                    choices=["sweep", "large", "config1", "config5", "serve", "pops"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--systems", type=int, default=256, help="systems of the sweep workload")

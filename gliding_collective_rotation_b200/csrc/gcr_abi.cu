@@ -489,9 +489,9 @@ int enqueue_step4(gcr_ctx *c)
     static const int reads[4] = {0, 1, 2, 1};
     for (int k = 0; k < 4; k++) {
         if ((rc = enqueue_lists(c, reads[k]))) return rc;
-        void *pair = reads[k] == 0 ? c->ks.pair0 : (reads[k] == 1 ? c->ks.pair1 : c->ks.pair2);
+        void *pair = c->graph_cross ? c->ks.pair_cross[reads[k]]
+                                    : (reads[k] == 0 ? c->ks.pair0 : (reads[k] == 1 ? c->ks.pair1 : c->ks.pair2));
         if ((rc = launch(c, pair, c->grid_pair, bb))) return rc;
-        if (c->graph_cross && (rc = launch(c, c->ks.cross[reads[k]], c->grid_pair, bb))) return rc;
         if ((rc = launch(c, c->ks.stage4[k], c->grid_stage4[k], bb, c->stage_smem))) return rc;
         if (k < 3 && c->graph_rigid && (rc = launch(c, c->ks.rigid4[k], c->grid_update, bb))) return rc;
     }
@@ -508,13 +508,11 @@ int enqueue_step(gcr_ctx *c)
     const int bb = c->cfg.block_beads;
     if (c->cfg.srk_order == 4) return enqueue_step4(c);
     if ((rc = enqueue_lists(c, 0))) return rc;
-    if ((rc = launch(c, c->ks.pair0, c->grid_pair, bb))) return rc;
-    if (c->graph_cross && (rc = launch(c, c->ks.cross[0], c->grid_pair, bb))) return rc;
+    if ((rc = launch(c, c->graph_cross ? c->ks.pair_cross[0] : c->ks.pair0, c->grid_pair, bb))) return rc;
     if ((rc = launch(c, c->ks.stage0, c->grid_stage0, bb, c->stage_smem))) return rc;
     if (c->graph_rigid && (rc = launch(c, c->ks.rigid0, c->grid_update, bb))) return rc;
     if ((rc = enqueue_lists(c, 1))) return rc;
-    if ((rc = launch(c, c->ks.pair1, c->grid_pair, bb))) return rc;
-    if (c->graph_cross && (rc = launch(c, c->ks.cross[1], c->grid_pair, bb))) return rc;
+    if ((rc = launch(c, c->graph_cross ? c->ks.pair_cross[1] : c->ks.pair1, c->grid_pair, bb))) return rc;
     if ((rc = launch(c, c->ks.stage1, c->grid_stage1, bb, c->stage_smem))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_dt))) return rc;
     if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
@@ -1102,16 +1100,14 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
         GCR_CUDA(cudaEventRecord(e[0], c->stream));
         rc = enqueue_lists(c, 0);
         GCR_CUDA(cudaEventRecord(e[1], c->stream));
-        if (!rc) rc = launch(c, c->ks.pair0, c->grid_pair, bb);
-        if (!rc && cross) rc = launch(c, c->ks.cross[0], c->grid_pair, bb);
+        if (!rc) rc = launch(c, cross ? c->ks.pair_cross[0] : c->ks.pair0, c->grid_pair, bb);
         GCR_CUDA(cudaEventRecord(e[2], c->stream));
         if (!rc) rc = launch(c, c->ks.stage0, c->grid_stage0, bb, c->stage_smem);
         if (!rc && rigid) rc = launch(c, c->ks.rigid0, c->grid_update, bb);
         GCR_CUDA(cudaEventRecord(e[3], c->stream));
         if (!rc) rc = enqueue_lists(c, 1);
         GCR_CUDA(cudaEventRecord(e[4], c->stream));
-        if (!rc) rc = launch(c, c->ks.pair1, c->grid_pair, bb);
-        if (!rc && cross) rc = launch(c, c->ks.cross[1], c->grid_pair, bb);
+        if (!rc) rc = launch(c, cross ? c->ks.pair_cross[1] : c->ks.pair1, c->grid_pair, bb);
         GCR_CUDA(cudaEventRecord(e[5], c->stream));
         if (!rc) rc = launch(c, c->ks.stage1, c->grid_stage1, bb, c->stage_smem);
         if (!rc) rc = launch_sys(c, c->ks.sys_dt);

@@ -65,7 +65,7 @@ struct KernelSet {
     void *sys_end;
     void *sys_mark;  // flag every resident system for a list build
     void *lists_plan;  // compact the systems that take part in a list build
-    void *cross[3];    // cross-population pair forces at pos / pos1 / pos2 (added to the pair force)
+    void *pair_cross[3];  // pair forces at pos / pos1 / pos2 with the other populations' (coupled systems)
     size_t (*stage_smem)(int block_beads);  // dynamic shared memory of the stage kernels
 };
 

@@ -621,10 +621,66 @@ __global__ void __launch_bounds__(512) k_build(BatchArgs A)
     }
 }
 
+// pair forces between coupled populations: the force on bead b of one
+// population from the beads of each other population (central_pair_force
+// over the cross nbor_list with other_pop another population,
+// SRK.py:229-245; the pair parameters of interpop_forces,
+// updates.py:274-312; rule forces.WCA), added after the bead's own pair
+// force, partner by partner in the order the reference adds the other
+// populations' forces (SRK.py:287-294).  Only the pair kernels of a graph
+// holding coupled populations carry it.
+template <int D, typename FT, int WHICH>
+__device__ __forceinline__ void add_cross(const BatchArgs &A, const SysP &p, int b, const double *xb, FT *F,
+                                          bool &bad)
+{
+    for (int c = 0; c < p.n_cross && c < kMaxPops - 1; c++) {
+        const int qs = p.cross_q[c];
+        if ((unsigned)qs >= (unsigned)A.n_slots) {
+            bad = true;
+            continue;
+        }
+        const SysP &q = A.P[qs];
+        const double *XQ = stage_x<WHICH>(q);
+        const int nq = q.n;
+        const int64_t row = p.x_off + (int64_t)c * p.n + b;
+        int cnt = A.xcount[row];
+        cnt = cnt < 0 ? 0 : (cnt < A.list_depth ? cnt : A.list_depth);
+        const FT rc2 = (FT)p.cross_rc2[c], p0 = (FT)p.cross_p0[c], p1 = (FT)p.cross_p1[c];
+        const FT shift = (FT)p.cross_shift[c];
+        for (int k = 0; k < cnt; k++) {
+            const int j = A.xnbr[row + (int64_t)k * A.xstride];
+            if ((unsigned)j >= (unsigned)nq) {
+                bad = true;
+                continue;
+            }
+            FT sep[3];
+            FT ds = FT(0);
+#pragma unroll
+            for (int i = 0; i < D; i++) {
+                sep[i] = (FT)inbounds(XQ[(size_t)j * D + i], xb[i], p.half_L, p.L);
+                ds += sep[i] * sep[i];
+            }
+            if (!(FT(0) < ds && ds <= rc2)) continue;
+            if (shift != FT(0)) {
+                FT mag = sqrt(ds);
+                FT nm = mag + shift;
+                nm = nm < FT(0) ? FT(0) : nm;
+                FT rs = nm / mag;
+#pragma unroll
+                for (int i = 0; i < D; i++) sep[i] *= rs;
+                ds = nm * nm;
+            }
+            FT coeff = wca_coeff<FT>(ds, p0, p1);
+#pragma unroll
+            for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
+        }
+    }
+}
+
 // pair forces over the neighbour list (forces.py:57-145, rule forces.WCA):
 // min-image separation of the FP64 positions, rounded to FT, then the rule
 // in FT; writes the pair force of every bead to fp[bead]
-template <int D, typename FT, int WHICH>
+template <int D, typename FT, int WHICH, bool CROSS>
 __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_pair(BatchArgs A)
 {
     const int nt = *A.n_bead_tiles;
@@ -681,84 +737,9 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_pair(BatchArgs A)
 #pragma unroll
             for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
         }
+        if constexpr (CROSS) add_cross<D, FT, WHICH>(A, p, b, xb, F, bad);
         if (bad) atomicOr(&s.flags, kFlagListCorrupt);
         FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
-#pragma unroll
-        for (int i = 0; i < D; i++) fp[i] = F[i];
-    }
-}
-
-// pair forces between coupled populations: the force on a bead of one
-// population from the beads of another (central_pair_force over the cross
-// nbor_list with other_pop another population, SRK.py:229-245; the pair
-// parameters of interpop_forces, updates.py:274-312; rule forces.WCA),
-// added to the bead's own pair force partner by partner, in the order the
-// reference adds the other populations' forces (SRK.py:287-294)
-template <int D, typename FT, int WHICH>
-__global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_cross(BatchArgs A)
-{
-    const int nt = *A.n_bead_tiles;
-    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
-        const Tile tl = A.bead_tiles[t];
-        const SysP &p = A.P[tl.sys];
-        SysS &s = A.S[tl.sys];
-        if (p.n_cross <= 0 || !ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal)) continue;
-        const int b = tl.begin + threadIdx.x;
-        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
-        const double *X = stage_x<WHICH>(p);
-        double xb[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-        for (int i = 0; i < D; i++) xb[i] = X[(size_t)b * D + i];
-        FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
-        FT F[3] = {FT(0), FT(0), FT(0)};
-        if (p.calc_wca) {
-#pragma unroll
-            for (int i = 0; i < D; i++) F[i] = fp[i];
-        }
-        bool bad = false;
-        for (int c = 0; c < p.n_cross && c < kMaxPops - 1; c++) {
-            const int qs = p.cross_q[c];
-            if ((unsigned)qs >= (unsigned)A.n_slots) {
-                bad = true;
-                continue;
-            }
-            const SysP &q = A.P[qs];
-            const double *XQ = stage_x<WHICH>(q);
-            const int nq = q.n;
-            const int64_t row = p.x_off + (int64_t)c * p.n + b;
-            int cnt = A.xcount[row];
-            cnt = cnt < 0 ? 0 : (cnt < A.list_depth ? cnt : A.list_depth);
-            const FT rc2 = (FT)p.cross_rc2[c], p0 = (FT)p.cross_p0[c], p1 = (FT)p.cross_p1[c];
-            const FT shift = (FT)p.cross_shift[c];
-            for (int k = 0; k < cnt; k++) {
-                const int j = A.xnbr[row + (int64_t)k * A.xstride];
-                if ((unsigned)j >= (unsigned)nq) {
-                    bad = true;
-                    continue;
-                }
-                FT sep[3];
-                FT ds = FT(0);
-#pragma unroll
-                for (int i = 0; i < D; i++) {
-                    sep[i] = (FT)inbounds(XQ[(size_t)j * D + i], xb[i], p.half_L, p.L);
-                    ds += sep[i] * sep[i];
-                }
-                if (!(FT(0) < ds && ds <= rc2)) continue;
-                if (shift != FT(0)) {
-                    FT mag = sqrt(ds);
-                    FT nm = mag + shift;
-                    nm = nm < FT(0) ? FT(0) : nm;
-                    FT rs = nm / mag;
-#pragma unroll
-                    for (int i = 0; i < D; i++) sep[i] *= rs;
-                    ds = nm * nm;
-                }
-                FT coeff = wca_coeff<FT>(ds, p0, p1);
-#pragma unroll
-                for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
-            }
-        }
-        if (bad) atomicOr(&s.flags, kFlagListCorrupt);
 #pragma unroll
         for (int i = 0; i < D; i++) fp[i] = F[i];
     }
@@ -1413,8 +1394,8 @@ __global__ void k_sys_mark(BatchArgs A, int n_slots)
 // ------------------------------------------------------------------------
 template <int D, typename FT>
 struct StepKernels {
-    static void *pair0() { return (void *)k_pair<D, FT, 0>; }
-    static void *pair1() { return (void *)k_pair<D, FT, 1>; }
+    static void *pair0() { return (void *)k_pair<D, FT, 0, false>; }
+    static void *pair1() { return (void *)k_pair<D, FT, 1, false>; }
     static void *stage0() { return (void *)k_stage<D, FT, 0>; }
     static void *stage1() { return (void *)k_stage<D, FT, 1>; }
     static void *update() { return (void *)k_update<D, FT>; }
@@ -1422,7 +1403,7 @@ struct StepKernels {
     static void *rigid1() { return (void *)k_rigid<D, FT, 1>; }
     static void fill4(KernelSet &k)
     {
-        k.pair2 = (void *)k_pair<D, FT, 2>;
+        k.pair2 = (void *)k_pair<D, FT, 2, false>;
         k.stage4[0] = (void *)k_stage<D, FT, 10>;
         k.stage4[1] = (void *)k_stage<D, FT, 11>;
         k.stage4[2] = (void *)k_stage<D, FT, 12>;
@@ -1431,9 +1412,9 @@ struct StepKernels {
         k.rigid4[1] = (void *)k_rigid<D, FT, 11>;
         k.rigid4[2] = (void *)k_rigid<D, FT, 12>;
         k.rigid4[3] = (void *)k_rigid<D, FT, 13>;
-        k.cross[0] = (void *)k_cross<D, FT, 0>;
-        k.cross[1] = (void *)k_cross<D, FT, 1>;
-        k.cross[2] = (void *)k_cross<D, FT, 2>;
+        k.pair_cross[0] = (void *)k_pair<D, FT, 0, true>;
+        k.pair_cross[1] = (void *)k_pair<D, FT, 1, true>;
+        k.pair_cross[2] = (void *)k_pair<D, FT, 2, true>;
     }
 };
 

@@ -123,6 +123,39 @@ def config5(seed=0, scale=1.0):
                        Dr=0.1, tangent_locked=False, dt=5e-4)
 
 
+def populations(n_boxes=128, seed=0):
+    """Boxes of two populations each (the multi-population step,
+    updates.py:146-247): 2D, L = 150, 1000 chains x 10 beads as config 1
+    (WCA, v0 = 1 tangent-locked) and 3000 single passive beads of diameter
+    0.7; cross parameters the mean of the two WCA sets (populations.py:226-232).
+    Returns the specs (chains of box i at 2i, beads at 2i + 1) and the
+    groups ``(members, fixed, cross_wca)``."""
+    specs, groups = [], []
+    for i in range(n_boxes):
+        rs = np.random.RandomState(seed * 100003 + i)
+        chains = make_system(f"box{i}_chains", 2, 1000, 10, 150.0, seed=5000 + i, noise_seed=2 * i)
+        L = 150.0
+        nb = 3000
+        pos = rs.uniform(0.0, L, size=(nb, 2))
+        ang = rs.uniform(0.0, 2 * math.pi, size=nb)
+        tan = np.stack([np.cos(ang), np.sin(ang)], axis=1)
+        r = 0.7
+        wca = make_WCA_params(r, 1.0, 0.0, 1.0)
+        D = 0.01 / r
+        params = SystemParams(
+            L=L, spring_params=np.array([100.0, 20.0, 0.0, 0.0, 0.0, 0.1]), wca_params=wca,
+            active_params=np.array([0.0, 0.0, 0.0]), D=D, Dr=3 * D / (4 * r * r), radius=r, n_nearby=4,
+            calc_springs=False, calc_wca=True, self_propel=False, dtmax=1e-3, max_dist_per_step=math.inf,
+            rk_cheat=1.0, seed=2 * i + 1, step=0)
+        beads = SystemSpec(f"box{i}_beads", 2, pos, tan, np.arange(nb), np.full(nb, 0.5), params, 1e-3,
+                           chains.relax_mdps)
+        cross = np.zeros((2, 2, 4))
+        cross[0, 1] = cross[1, 0] = 0.5 * (chains.params.wca_params + wca)
+        specs += [chains, beads]
+        groups.append(([2 * i, 2 * i + 1], [False, False], cross))
+    return specs, groups
+
+
 def serve_trace(n_requests, rate=20.0, seed=7, min_beads=1000, max_beads=1_000_000, min_steps=1000,
                 max_steps=20000):
     """Poisson arrivals at `rate`/s of config-3-style systems with bead count
