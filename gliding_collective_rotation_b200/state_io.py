@@ -134,6 +134,21 @@ def save_batch(batch, prefix, filenumber, t=None, n_digits=8):
     return names
 
 
+def save_populations(batch, members, pop_names, prefix, filenumber, stepnum, t, n_digits=8):
+    """Write the populations of one box (systems ``members`` of a ``Batch``,
+    coupled with ``Batch.couple``) the way ``output_methods.save_state``
+    writes a list of populations (output_methods.py:420-466): one file per
+    population, ``<prefix>_<pop name>_<n>.dat``, the same file number, step
+    and time in every header; returns the file names."""
+    names = []
+    for i, name in zip(members, pop_names):
+        st = batch.states[i]
+        names.append(write_state(prefix, filenumber, stepnum, t, st.pos.cpu().numpy(),
+                                 st.tangent.double().cpu().numpy(), st.chain_id.cpu().numpy(), pop_name=name,
+                                 n_digits=n_digits))
+    return names
+
+
 def latest_state(prefix, pop_name="beads"):
     """The most recent file of a run (highest file number)."""
     d = os.path.dirname(prefix) or "."

@@ -69,6 +69,21 @@ def test_one_step_lands_on_a_reference_trial(name):
     b.close()
 
 
+def test_populations_write_one_state_file_each(tmp_path):
+    from gliding_collective_rotation_b200 import state_io
+    d, s = load("pops3_fixed_2d")
+    b = _batch(d, s, D=0.01, seeds=[1, 2, 3])
+    b.begin(3, dt=d["status_before"][0])
+    b.run(3)
+    files = state_io.save_populations(b, range(s["n_pops"]), s["names"], str(tmp_path / "run"), 7, 3, 0.003)
+    for k, fn in enumerate(files):
+        assert fn.endswith(f"run_{s['names'][k]}_00000007.dat")
+        back = state_io.read_state(fn)
+        np.testing.assert_allclose(back["pos"], b.states[k].pos.cpu().numpy(), rtol=1e-8, atol=0)
+        assert back["stepnum"] == 3
+    b.close()
+
+
 @pytest.mark.parametrize("name", CASES)
 def test_matches_the_oracle_with_noise(name):
     """T > 0 (D = 0.01 for the moving populations), the Philox stream with
