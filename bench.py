@@ -287,7 +287,27 @@ def run_gpu(args):
     # untimed warm-up; every step after it, timed or not, follows the
     # reference's default adaptive dt rule (dtmax = the configured dt)
     relax_steps = batch.relax(max_steps=args.relax_steps, adaptive_after=True)
-    # warm-up at the fixed dt (regrows the cells if a system overflowed them)
+    tuned = None
+    if args.autotune:
+        # launch shapes measured on copies of the relaxed systems (untimed);
+        # the batch is rebuilt from the same relaxed state with the best one
+        import dataclasses
+        from gliding_collective_rotation_b200 import autotune
+        relaxed = [dataclasses.replace(sp, pos=st.pos.cpu().numpy(), tangent=st.tangent.double().cpu().numpy())
+                   for sp, st in zip(specs, batch.states)]
+        tuned = autotune.tune(relaxed, precision=args.precision, device=dev, couplings=groups,
+                              refresh=args.autotune > 1)
+        batch.close()
+        tspecs, kw = autotune.apply(relaxed, tuned)
+        for sp, tsp in zip(specs, tspecs):
+            sp.pos, sp.tangent, sp.params = tsp.pos, tsp.tangent, tsp.params
+        batch = Batch(specs, precision=args.precision, device=dev, list_depth=args.list_depth or None, **kw)
+        for members, fixed, cross in groups:
+            batch.couple(members, fixed, cross)
+        batch.set_adaptive(True)
+        args.steps_per_graph, args.ctas_per_sm, args.block_beads = (kw["steps_per_graph"], kw["ctas_per_sm"],
+                                                                    kw["block_beads"])
+    # warm-up under the adaptive dt (regrows the cells if a system overflowed them)
     batch.run_checked(args.warmup)
     eng = batch.engine
     eng.synchronize()
@@ -451,7 +471,9 @@ def run_gpu(args):
                    else default_skin(specs[0].params.wca_params[3]),
                    "steps_per_graph": args.steps_per_graph, "cell_depth": batch.cell_depth,
                    "list_depth": batch.list_depth, "list_mean": list_mean,
-                   "list_builds_per_stage": builds_per_stage},
+                   "list_builds_per_stage": builds_per_stage, "block_beads": args.block_beads,
+                   "ctas_per_sm": args.ctas_per_sm,
+                   "autotune": None if tuned is None else {k: v for k, v in tuned.items() if k != "trials"}},
         "e2e": e2e, "roofline": roofline, "clocks": clk,
         "gpu_launches": 15 * args.steps + 1,
     }
@@ -594,6 +616,8 @@ def main():
                     help="Verlet skin of the neighbour lists (<0: 0.2 r_cut + 0.1, within [0.2, 1])")
     ap.add_argument("--list-depth", type=int, default=0, help="neighbour slots per bead (0: default)")
     ap.add_argument("--relax-steps", type=int, default=2000)
+    ap.add_argument("--autotune", type=int, default=0,
+                    help="1: launch shapes from the autotuner (cached per workload and device); 2: re-tune")
     ap.add_argument("--profile-steps", type=int, default=10)
     ap.add_argument("--plain", type=int, default=1)
     ap.add_argument("--plain-steps", type=int, default=50)
