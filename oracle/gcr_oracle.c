@@ -1201,7 +1201,8 @@ GCRO_EXPORT void gcro_pair_forces_all(const double *XP, int64_t nP, const int64_
  * WCA parameters of the force on population k from population q
  * (interpop_forces, updates.py:274-312; r_cut <= 0 or p0 = p1 = 0: none).
  * The call's time values come from g (dt, dtmax, max_dist_per_step,
- * rk_cheat, max_dt_usable, max_steps, noise_mode, step0); noise modes as
+ * rk_cheat, max_dt_usable, max_steps, noise_mode, step0, srk_order: 2 or 4
+ * with sts[k]->forces_aux for SRK4); noise modes as
  * gcro_srk2_run (0: sts[k]->mt[0], 1: injected, 2: Philox with ps[k]->seed).
  * out->max_forces_strength is the first moving population's own value
  * (shared_arr[0, 3], the thread of the first population pair). */
@@ -1221,6 +1222,12 @@ GCRO_EXPORT int gcro_group_run(int n_pops, const gcro_params *const *ps, gcro_st
     int first = -1;
     for (int k = 0; k < n_pops; k++)
         if (!fixed[k] && first < 0) first = k;
+    /* SRK4 (SRK.py:186-215, 296-321): four stages, each stage's force in
+     * forces_aux, their weighted sum in forces */
+    const int srk4 = g->srk_order == 4;
+    const int n_stages = srk4 ? 4 : 2;
+    for (int k = 0; k < n_pops; k++)
+        if (srk4 && !fixed[k] && !sts[k]->forces_aux) return -2;
     double dt = g->dt, elapsed = 0.0, mfs0 = 0.0;
     int64_t steps = 0;
     while ((steps < g->max_steps || g->max_steps < 0) && (elapsed < g->max_dt_usable || g->max_dt_usable < 0)) {
@@ -1259,11 +1266,16 @@ GCRO_EXPORT int gcro_group_run(int n_pops, const gcro_params *const *ps, gcro_st
                     }
                 }
             }
-            for (int64_t b = 0; b < n * dim; b++) st->forces[b] = 0.0;
+            for (int64_t b = 0; b < n * dim; b++) (srk4 ? st->forces_aux : st->forces)[b] = 0.0;
         }
         double dt_for_update = dt;
-        for (int stage = 0; stage < 2; stage++) {
-            const double pref = stage == 0 ? 1.0 : 0.5;
+        for (int stage = 0; stage < n_stages; stage++) {
+            const double pref = srk4 ? 1.0 : (stage == 0 ? 1.0 : 0.5);
+            const double rescale = stage <= 1 ? 0.5 : 1.0;
+            if (srk4 && stage > 0)
+                for (int k = 0; k < n_pops; k++)
+                    if (!fixed[k])
+                        for (int64_t b = 0; b < ps[k]->n_beads * dim; b++) sts[k]->forces_aux[b] = 0.0;
             /* forces taken at pos (stage 0) or pos1; a fixed population's pos1 is its pos */
             double *X[8];
             for (int k = 0; k < n_pops; k++) X[k] = (stage == 0 || fixed[k]) ? sts[k]->pos : sts[k]->pos1;
@@ -1271,13 +1283,14 @@ GCRO_EXPORT int gcro_group_run(int n_pops, const gcro_params *const *ps, gcro_st
                 if (fixed[k]) continue;
                 const gcro_params *p = ps[k];
                 gcro_state *st = sts[k];
+                double *Fs = srk4 ? st->forces_aux : st->forces; /* write_to_forces */
                 if (p->calc_springs)
-                    spring_forces(X[k], st->tangent, st->chain_id, st->forces, p->n_beads, L, p->spring,
-                                  st->rest_lengths, dim);
+                    spring_forces(X[k], st->tangent, st->chain_id, Fs, p->n_beads, L, p->spring, st->rest_lengths,
+                                  dim);
                 if (p->calc_wca)
                     pair_forces_all(X[k], p->n_beads, st->chain_id, p->n_nearby, X[k], p->n_beads, 1, p->wca, L,
-                                    dim, st->forces);
-                if (p->self_propel) self_propel(st->forces, st->tangent, p->n_beads, p->active, dim);
+                                    dim, Fs);
+                if (p->self_propel) self_propel(Fs, st->tangent, p->n_beads, p->active, dim);
             }
             /* the other populations' forces, added in turns (SRK.py:287-294) */
             for (int ii = 1; ii < n_pops; ii++)
@@ -1289,9 +1302,20 @@ GCRO_EXPORT int gcro_group_run(int n_pops, const gcro_params *const *ps, gcro_st
                     const int64_t n = ps[k]->n_beads;
                     memset(tmp[k], 0, sizeof(double) * (size_t)n * dim);
                     pair_forces_all(X[k], n, sts[k]->chain_id, 0, X[q], ps[q]->n_beads, 0, w, L, dim, tmp[k]);
-                    for (int64_t b = 0; b < n * dim; b++) sts[k]->forces[b] += tmp[k][b];
+                    double *Fs = srk4 ? sts[k]->forces_aux : sts[k]->forces;
+                    for (int64_t b = 0; b < n * dim; b++) Fs[b] += tmp[k][b];
                 }
-            if (stage == 1) {
+            if (srk4) {
+                /* SRK.py:296-321: weighted sum of the stage forces */
+                const double mult = (stage == 0 || stage == 3) ? 1. / 6. : 1. / 3.;
+                for (int k = 0; k < n_pops; k++) {
+                    if (fixed[k]) continue;
+                    double *F = sts[k]->forces;
+                    const double *Fa = sts[k]->forces_aux;
+                    for (int64_t b = 0; b < ps[k]->n_beads * dim; b++) F[b] = stage == 0 ? Fa[b] * mult : F[b] + Fa[b] * mult;
+                }
+            }
+            if (stage == n_stages - 1) {
                 /* SRK.py:323-353 over every moving population */
                 double Sg = 0.0;
                 for (int k = 0; k < n_pops; k++) {
@@ -1330,18 +1354,20 @@ GCRO_EXPORT int gcro_group_run(int n_pops, const gcro_params *const *ps, gcro_st
                 const gcro_params *p = ps[k];
                 gcro_state *st = sts[k];
                 const int64_t n = p->n_beads;
-                double *W = stage == 0 ? st->pos1 : st->pos;
-                double dt_eff = dt_for_update * pref;
+                double *W = srk4 ? (stage == 3 ? st->pos : st->pos1) : (stage == 0 ? st->pos1 : st->pos);
+                double dt_eff = srk4 ? dt_for_update * rescale * pref : dt_for_update * pref;
                 const double s2 = sqrt(2.0 * dt_for_update * p->D);
                 const int rigid = p->rigid_rod != 0.0 && p->longest_chain_length > 2;
+                /* SRK.py:355-362: virtual SRK4 updates use the stage force */
+                const double *Fu = (srk4 && stage < 3) ? st->forces_aux : st->forces;
                 if (n > 0 && rigid) {
-                    project_rigid(W, X[k], st->forces, st->noise, n, st->chain_id, st->rest_lengths, p->rigid_rod, L,
+                    project_rigid(W, X[k], Fu, st->noise, n, st->chain_id, st->rest_lengths, p->rigid_rod, L,
                                   dt_eff, p->D, p->radius, dim, rscr[k], rscr[k] + 3 * n, rscr[k] + 6 * n);
                 } else {
                     dt_eff /= p->radius;
                     for (int64_t b = 0; b < n; b++)
                         for (int i = 0; i < dim; i++) {
-                            double t = st->pos[b * dim + i] + dt_eff * st->forces[b * dim + i];
+                            double t = st->pos[b * dim + i] + dt_eff * Fu[b * dim + i];
                             if (s2 != 0.0) t += s2 * st->noise[b * 2 * dim + i];
                             W[b * dim + i] = py_mod(t, L);
                         }

@@ -416,7 +416,9 @@ class OracleGroup:
         self.cross = np.ascontiguousarray(np.asarray(cross, dtype=np.float64).reshape(n, n, 4))
 
     def run(self, n_steps, dt, dtmax=None, max_dist_per_step=math.inf, rk_cheat=1.0, max_dt_usable=-1.0,
-            noise_mode=NOISE_PHILOX, step0=0, calc_active=True):
+            noise_mode=NOISE_PHILOX, step0=0, calc_active=True, srk_order=2):
+        """SRK2, or the SRK4 branch with ``srk_order=4`` (every system made
+        with ``srk_order=4``, so that it has its ``forces_aux``)."""
         L = lib()
         n = len(self.systems)
         ps = [s._params(1, noise_mode, calc_active) for s in self.systems]
@@ -427,6 +429,7 @@ class OracleGroup:
         g.dtmax = dt if dtmax is None else dtmax
         g.max_dist_per_step, g.rk_cheat, g.max_dt_usable = max_dist_per_step, rk_cheat, max_dt_usable
         g.max_steps, g.noise_mode, g.step0 = n_steps, noise_mode, step0
+        g.srk_order = srk_order
         p_arr = (C.POINTER(Params) * n)(*[C.pointer(p) for p in ps])
         s_arr = (C.POINTER(State) * n)(*[C.pointer(st) for st in sts])
         res = Result()

@@ -146,14 +146,34 @@ def test_decoupled_systems_step_alone():
         x.close()
 
 
-def test_srk4_coupled_runs():
-    d, s = load("pops2_2d")
-    b = _batch(d, s, D=0.01, seeds=[3, 4], srk_order=4)
-    b.begin(10, dt=d["status_before"][0])
-    b.run(10)
-    sts = b.statuses()
-    assert all(x["flags"] == 0 and x["steps_done"] == 10 for x in sts)
-    assert sts[0]["dt"] == sts[1]["dt"]
+@pytest.mark.parametrize("name", ["pops2_2d", "pops3_fixed_2d"])
+def test_srk4_coupled_matches_the_oracle(name):
+    """The SRK4 branch (SRK.py:186-215, 296-321) with several populations:
+    the cross forces enter every stage force."""
+    d, s = load(name)
+    n, L = s["n_pops"], s["L"]
+    seeds = [31 + k for k in range(n)]
+    st0 = d["status_before"]
+    b = _batch(d, s, D=0.01, seeds=seeds, srk_order=4)
+    g = oracle_group(d, s, D=0.01, seeds=seeds, srk_order=4)
+    dt, step0 = st0[0], 0
+    for n_steps, tol in ((1, 1e-12), (9, 1e-9)):
+        b.begin(n_steps, dt=dt)
+        b.run(n_steps)
+        sts = b.statuses()
+        assert all(x["flags"] == 0 and x["steps_done"] == n_steps for x in sts)
+        res = g.run(n_steps, dt=dt, dtmax=st0[8], max_dist_per_step=s["max_dist_per_step"], rk_cheat=s["rk_cheat"],
+                    noise_mode=O.NOISE_PHILOX, step0=step0, srk_order=4)
+        step0 += n_steps
+        dt = res["dt"]
+        lead = s["fixed"].index(False)
+        assert abs(sts[lead]["dt"] - res["dt"]) <= 1e-9 * res["dt"]
+        for k in range(n):
+            err = np.max(np.abs(_min_image(b.states[k].pos.cpu().numpy() - g.systems[k].pos, L)))
+            assert err < tol, (k, n_steps, err)
+            if not s["fixed"][k]:
+                fa = b.states[k].forces_aux.cpu().numpy()
+                assert np.max(np.abs(fa - g.systems[k].forces_aux)) <= 1e-8 * max(1.0, np.max(np.abs(fa)))
     b.close()
 
 

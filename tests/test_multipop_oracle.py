@@ -111,3 +111,25 @@ def test_one_population_group_is_the_single_population_step():
     one.seed = 7
     O.OracleGroup([one], [False], np.zeros((1, 1, 4))).run(5, dt=1e-4, noise_mode=O.NOISE_PHILOX)
     assert np.max(np.abs(_min_image(one.pos - single.pos, s["L"]))) < 1e-12
+
+
+def test_one_population_group_is_the_single_population_srk4_step():
+    d, s = load("pops2_2d")
+    from tests.multipop_helpers import pop_arrays
+    a = pop_arrays(d, s, 0)
+
+    def make():
+        return O.OracleSystem(a["pos"], a["tangent"], a["chain_id"], a["rest_lengths"], s["L"], a["spring"],
+                              a["wca"], a["active"], 0.01, 0.0, a["radius"], a["n_nearby"], s["n_grid"],
+                              nbor_depth=256, srk_order=4)
+    single = make()
+    single.build_lists(grid_window=1)
+    r1 = single.run(5, dt=1e-4, dtmax=1e-3, max_dist_per_step=0.01, noise_mode=O.NOISE_PHILOX, seed=7,
+                    steps_until_update=1000)
+    one = make()
+    one.seed = 7
+    r2 = O.OracleGroup([one], [False], np.zeros((1, 1, 4))).run(5, dt=1e-4, dtmax=1e-3, max_dist_per_step=0.01,
+                                                               noise_mode=O.NOISE_PHILOX, srk_order=4)
+    assert np.max(np.abs(_min_image(one.pos - single.pos, s["L"]))) < 1e-12
+    assert np.max(np.abs(one.forces_aux - single.forces_aux)) < 1e-9
+    assert abs(r1["dt"] - r2["dt"]) <= 1e-12 * r1["dt"]
