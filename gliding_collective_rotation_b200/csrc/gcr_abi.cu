@@ -855,6 +855,15 @@ int gcr_update_desc(gcr_ctx *c, int32_t slot, const gcr_system_desc *desc)
     double skin = 0.0;
     int rc = validate_desc(c->cfg, desc, &nc, &skin);
     if (rc) return rc;
+    if (sl.group >= 0) {
+        // a coupled population keeps what gcr_couple checked: its cells
+        // (the others' cross lists read them) and the shared box
+        const Group &g = c->groups[sl.group];
+        if (!desc->calc_wca) return fail(GCR_ERR_BAD_ARG, "a coupled population keeps its WCA force");
+        for (int k = 0; k < g.n; k++)
+            if (g.slots[k] != slot && c->slots[g.slots[k]].desc.L != desc->L)
+                return fail(GCR_ERR_BAD_ARG, "coupled populations share L");
+    }
     // the current grid stays while its cells cover the list radius (every
     // run starts with a list build, so a grid change between calls is safe)
     if (desc->calc_wca && sl.desc.calc_wca && desc->L == sl.desc.L && sl.nc >= 3 &&
@@ -894,7 +903,7 @@ int gcr_couple(gcr_ctx *c, int32_t n, const int32_t *slots, const int32_t *fixed
     if (!c || !slots || !fixed || !cross_wca) return fail(GCR_ERR_BAD_ARG, "null argument");
     if (n < 2 || n > kMaxPops) return fail(GCR_ERR_BAD_ARG, "2 to 4 populations can be coupled");
     int g_old = -2;
-    int movers = 0, first = -1;
+    int movers = 0;
     for (int a = 0; a < n; a++) {
         if (!valid_slot(c, slots[a])) return fail(GCR_ERR_BAD_ARG, "invalid slot");
         for (int b = 0; b < a; b++)
@@ -906,17 +915,7 @@ int gcr_couple(gcr_ctx *c, int32_t n, const int32_t *slots, const int32_t *fixed
         if (g_old == -2) g_old = g;
         if (g != g_old || (g >= 0 && c->groups[g].n != n))
             return fail(GCR_ERR_BAD_ARG, "a slot is coupled to other populations (gcr_decouple first)");
-        if (!fixed[a]) {
-            movers++;
-            if (first < 0) {
-                first = a;
-            } else {
-                const gcr_system_desc &d0 = c->slots[slots[first]].desc;
-                if (sl.desc.dtmax != d0.dtmax || sl.desc.max_dist_per_step != d0.max_dist_per_step ||
-                    sl.desc.rk_cheat != d0.rk_cheat)
-                    return fail(GCR_ERR_BAD_ARG, "moving populations share dtmax, max_dist_per_step and rk_cheat");
-            }
-        }
+        if (!fixed[a]) movers++;
         for (int b = 0; b < n; b++)
             for (int k = 0; k < 4; k++)
                 if (!std::isfinite(cross_wca[((size_t)a * n + b) * 4 + k]))

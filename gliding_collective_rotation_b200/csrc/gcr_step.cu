@@ -1321,23 +1321,33 @@ __global__ void k_sys_dt(BatchArgs A, int n_slots)
     // coupled populations: one dt from the largest S over the moving members
     // (the max over every thread's shared_arr[:,3], SRK.py:333-340)
     double Sg = (p.grp_n && p.fixed) ? 0.0 : S;
+    // the rule's constants of a group come from its first moving member, so
+    // every member takes the same dt
+    double dtmax = p.dtmax, mdps = p.mdps, rk = p.rk;
+    bool lead = false;
     for (int k = 0; k < p.grp_n && k < kMaxPops; k++) {
         const int m = p.grp[k];
-        if (m < 0 || m >= n_slots || m == i) continue;
+        if (m < 0 || m >= n_slots) continue;
         const SysP &pm = A.P[m];
+        if (!pm.fixed && !lead) {
+            dtmax = pm.dtmax;
+            mdps = pm.mdps;
+            rk = pm.rk;
+            lead = true;
+        }
         const SysS &sm = A.S[m];
-        if (pm.fixed || !sm.active || (sm.flags & kFlagFatal)) continue;
+        if (m == i || pm.fixed || !sm.active || (sm.flags & kFlagFatal)) continue;
         const double Sm = pm.sqrt2D + pref * sqrt(__longlong_as_double((long long)sm.max_f2)) / pm.radius;
         Sg = Sm > Sg ? Sm : Sg;
     }
     double dt;
     if (Sg == 0.0)
-        dt = p.dtmax;
+        dt = dtmax;
     else {
-        double q = p.mdps / Sg;
-        dt = (q < p.dtmax) ? q : p.dtmax;
+        double q = mdps / Sg;
+        dt = (q < dtmax) ? q : dtmax;
     }
-    double dt_used = p.rk * dt;
+    double dt_used = rk * dt;
     if (s.max_dt_usable > 0.0) {
         double lim = s.max_dt_usable - s.elapsed;
         dt_used = (lim < dt_used) ? lim : dt_used;

@@ -202,8 +202,10 @@ GCR_API int gcr_footprint(const gcr_config *cfg, const gcr_system_desc *desc, in
  *     mean of the two WCA parameter sets unless a special interaction says
  *     otherwise); r_cut <= 0 or p0 = p1 = 0 means no force.
  * fixed[i] != 0 (pop.fixed): member i never moves and feels no force, but
- * still acts on the others.  Every member needs calc_wca and the same L; the
- * moving members need the same dtmax, max_dist_per_step and rk_cheat, and are
+ * still acts on the others.  Every member needs calc_wca and the same L (also
+ * through later gcr_update_desc calls); the dt rule takes dtmax,
+ * max_dist_per_step and rk_cheat from the first moving member (time_vals are
+ * one array for every population in the reference).  The moving members are
  * armed together with the same limits for each call.  Calling it again with
  * the same members in the same order replaces fixed and cross_wca. */
 GCR_API int gcr_couple(gcr_ctx *ctx, int32_t n, const int32_t *slots, const int32_t *fixed,
