@@ -90,6 +90,8 @@ SIGNATURES = {
                                      C.POINTER(C.c_int64)]),
     "gcr_philox_noise": (C.c_int, [C.c_int32, C.c_uint64, C.c_int64, C.c_int64, C.c_int32, C.c_int32,
                                    C.c_void_p, C.c_void_p]),
+    "gcr_unwrapped_positions": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
+    "gcr_reset_images": (C.c_int, [C.c_void_p, C.c_int32]),
     "gcr_couple": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                              C.POINTER(C.c_double)]),
     "gcr_decouple": (C.c_int, [C.c_void_p, C.c_int32]),

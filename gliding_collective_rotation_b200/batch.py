@@ -112,6 +112,7 @@ class Batch:
         self._carry_dt = None  # dts to hand to the next call after a regrow
         self.series_buf = None
         self.groups = []  # coupled populations: (member indices, fixed flags, cross WCA parameters)
+        self._img_carry = [None] * len(specs)  # L * images crossed before the last regrow
         self._make_engine()
 
     def _make_engine(self):
@@ -158,6 +159,10 @@ class Batch:
             flags |= s["flags"]
         # a re-admitted system starts from dtmax: its dt is handed over by the next call
         self._carry_dt = [s["dt"] for s in sts]
+        # the new context counts images from 0: keep those crossed so far
+        for i, st in enumerate(self.states):
+            img = self.engine.unwrapped(st.slot) - st.pos
+            self._img_carry[i] = img if self._img_carry[i] is None else self._img_carry[i] + img
         cell = bool(flags & FLAG_CELL_OVERFLOW)
         lst = bool(flags & FLAG_LIST_OVERFLOW) or not cell
         if (cell and self.cell_depth >= MAX_DEPTH) or (lst and self.list_depth >= MAX_LIST_DEPTH):
@@ -269,6 +274,21 @@ class Batch:
 
     def order_params(self):
         return np.array([self.engine.order_params(st.slot) for st in self.states])
+
+    def unwrapped(self):
+        """Per system, its positions plus the periodic images its beads
+        crossed since the batch was made (float64 [n, dim] on the device):
+        mean-squared displacements without host round trips."""
+        out = []
+        for st, carry in zip(self.states, self._img_carry):
+            u = self.engine.unwrapped(st.slot)
+            out.append(u if carry is None else u + carry)
+        return out
+
+    def msd(self, reference):
+        """Mean-squared displacement per system from ``reference`` (a list of
+        unwrapped positions, e.g. an earlier ``unwrapped()``), in FP64."""
+        return np.array([float(((u - r) ** 2).sum(dim=1).mean()) for u, r in zip(self.unwrapped(), reference)])
 
     def close(self):
         self.engine.close()

@@ -132,6 +132,7 @@ struct gcr_ctx {
     int *nbr = nullptr;
     int *ncount = nullptr;
     double *xref = nullptr;
+    int *img = nullptr;  // periodic images crossed per bead and axis since admission
     int *work = nullptr;
     void *xi = nullptr;
     void *fp = nullptr;
@@ -653,6 +654,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     e = e ? e : cudaMalloc(&c->nbr, sizeof(int) * (size_t)cfg.bead_capacity * (size_t)cfg.list_depth);
     e = e ? e : cudaMalloc(&c->ncount, sizeof(int) * (size_t)cfg.bead_capacity);
     e = e ? e : cudaMalloc(&c->xref, sizeof(double) * (size_t)cfg.bead_capacity * cfg.dim);
+    e = e ? e : cudaMalloc(&c->img, sizeof(int) * (size_t)cfg.bead_capacity * cfg.dim);
     e = e ? e : cudaMalloc(&c->work, sizeof(int) * (size_t)(3 + 3 * (S + 1)));
     e = e ? e : cudaMalloc(&c->xi, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
     e = e ? e : cudaMalloc(&c->fp, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
@@ -671,6 +673,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     cudaMemsetAsync(c->cnt, 0, sizeof(int) * cells_alloc, c->stream);
     cudaMemsetAsync(c->ncell, 0, sizeof(int) * cells_alloc, c->stream);
     cudaMemsetAsync(c->ncount, 0, sizeof(int) * (size_t)cfg.bead_capacity, c->stream);
+    cudaMemsetAsync(c->img, 0, sizeof(int) * (size_t)cfg.bead_capacity * cfg.dim, c->stream);
     cudaMemsetAsync(c->work, 0, sizeof(int) * (size_t)(3 + 3 * (S + 1)), c->stream);
     c->slots.assign(S, Slot());
     c->hP.assign(S, SysP());
@@ -692,6 +695,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     a.nbr = c->nbr;
     a.ncount = c->ncount;
     a.xref = c->xref;
+    a.img = c->img;
     a.xi = c->xi;
     a.fp = c->fp;
     a.work = c->work;
@@ -732,7 +736,7 @@ int gcr_destroy(gcr_ctx *c)
     if (c->graph) cudaGraphExecDestroy(c->graph);
     void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->topo, c->cnt, c->ncell,
                     c->items, c->nbr, c->ncount, c->xref, c->work, c->xi, c->fp, c->chain_starts, c->d_err,
-                    c->d_out, c->pos2, c->faux, c->xnbr, c->xcount};
+                    c->d_out, c->pos2, c->faux, c->xnbr, c->xcount, c->img};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -798,6 +802,8 @@ int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers 
     uint8_t *tp = c->topo + boff;
     targs[2] = &tp;
     GCR_CUDA(cudaMemsetAsync(c->d_err, 0, 2 * sizeof(int), c->stream));
+    // image counters start at 0: unwrapped positions are measured from admission
+    GCR_CUDA(cudaMemsetAsync(c->img + (size_t)boff * c->cfg.dim, 0, sizeof(int) * (size_t)n * c->cfg.dim, c->stream));
     GCR_CUDA(cudaLaunchKernel(c->ks.topo, dim3((n + 255) / 256), dim3(256), targs, 0, c->stream));
     GCR_CUDA(launch_chain_starts(buf->chain_id, n, (int)desc->n_chains, c->chain_starts + choff, c->d_err,
                                  c->stream));
@@ -1126,6 +1132,26 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
         }
     for (auto &e : ev) cudaEventDestroy(e);
     return rc;
+}
+
+int gcr_unwrapped_positions(gcr_ctx *c, int32_t slot, double *out)
+{
+    if (!valid_slot(c, slot) || !out) return fail(GCR_ERR_BAD_ARG, "bad argument");
+    const Slot &sl = c->slots[slot];
+    GCR_CUDA(launch_unwrap(c->cfg.dim, sl.buf.pos, c->img + (size_t)sl.bead_off * c->cfg.dim, (int)sl.desc.n_beads,
+                           sl.desc.L, out, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    return GCR_OK;
+}
+
+int gcr_reset_images(gcr_ctx *c, int32_t slot)
+{
+    if (!valid_slot(c, slot)) return fail(GCR_ERR_BAD_ARG, "invalid slot");
+    const Slot &sl = c->slots[slot];
+    GCR_CUDA(cudaMemsetAsync(c->img + (size_t)sl.bead_off * c->cfg.dim, 0,
+                             sizeof(int) * (size_t)sl.desc.n_beads * c->cfg.dim, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    return GCR_OK;
 }
 
 int gcr_synchronize(gcr_ctx *c)

@@ -261,6 +261,13 @@ __device__ __forceinline__ double inbounds(double a, double b, double half_L, do
     return o;
 }
 
+// periodic images crossed by one coordinate in a real update: a bead moves
+// far less than half a box per step, so a jump of more than L/2 is a wrap
+__device__ __forceinline__ int image_step(double x_old, double x_new, double half_L)
+{
+    return (x_new - x_old > half_L) ? -1 : ((x_old - x_new > half_L) ? 1 : 0);
+}
+
 // read of a word that other CTAs may change during the kernel
 __device__ __forceinline__ int ld_volatile(const int *p) { return *(const volatile int *)p; }
 

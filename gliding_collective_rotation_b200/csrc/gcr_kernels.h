@@ -39,6 +39,9 @@ struct BatchArgs {
     int *xnbr;
     int *xcount;
     int64_t xstride;
+    // periodic images crossed by each bead since admission, int32 [bead][dim]
+    // (the real updates count them; unwrapped = pos + L * img)
+    int *img;
 };
 
 struct KernelSet {
@@ -95,6 +98,8 @@ cudaError_t launch_chain_frames(int dim, int precision, const SysP &p, const int
 cudaError_t launch_pair_corr(const double *com, const double *phi, int n_chains, double L, double binsize, int n_bins,
                              int kind, unsigned long long *counts, unsigned long long *sums, int sm_count,
                              cudaStream_t st);
+// out[n][dim] = pos + L * img (unwrapped positions of one system)
+cudaError_t launch_unwrap(int dim, const double *pos, const int *img, int n, double L, double *out, cudaStream_t st);
 cudaError_t launch_philox_noise(int dim, uint64_t seed, int64_t step, int64_t n, int do_trans,
                                 int do_rot, double *out, cudaStream_t st);
 

@@ -372,6 +372,22 @@ cudaError_t launch_cell_assignment(int dim, const SysP &p, int32_t *cell_of_bead
     return cudaGetLastError();
 }
 
+__global__ void k_unwrap(int dim, const double *__restrict__ pos, const int *__restrict__ img, int n, double L,
+                         double *out)
+{
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (int64_t)n * dim) return;
+    out[i] = pos[i] + L * (double)img[i];
+}
+
+cudaError_t launch_unwrap(int dim, const double *pos, const int *img, int n, double L, double *out, cudaStream_t st)
+{
+    int64_t m = (int64_t)n * dim;
+    if (m <= 0) return cudaSuccess;
+    k_unwrap<<<(unsigned)((m + 255) / 256), 256, 0, st>>>(dim, pos, img, n, L, out);
+    return cudaGetLastError();
+}
+
 template <int D>
 __global__ void k_philox_noise(uint64_t seed, int64_t step, int64_t n, int do_trans, int do_rot, double *out)
 {

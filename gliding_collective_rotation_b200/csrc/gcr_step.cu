@@ -1118,9 +1118,12 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A
         if (plain) {
 #pragma unroll
             for (int i = 0; i < D; i++) {
-                x[i] = srk_update<FT>(p.pos[(size_t)b * D + i], dt_eff, s2, frc[(size_t)b * D + i], xi[i], p.L);
+                const double xo = p.pos[(size_t)b * D + i];
+                x[i] = srk_update<FT>(xo, dt_eff, s2, frc[(size_t)b * D + i], xi[i], p.L);
                 finite &= isfinite(x[i]);
                 p.pos[(size_t)b * D + i] = x[i];
+                const int di = image_step(xo, x[i], p.half_L);
+                if (di) A.img[(size_t)(p.bead_off + b) * D + i] += di;
             }
             if (!finite) atomicOr(&s.flags, kFlagNonFinite);
         }
@@ -1298,6 +1301,11 @@ __global__ void __launch_bounds__(512) k_rigid(BatchArgs A)
                     u += f * (-o + mean[i] + rot[i]);
                 x[i] = py_mod(prev[(size_t)b * D + i] + u, L);
                 finite &= isfinite(x[i]);
+                if constexpr (stage_writes(STAGE) == 0) {
+                    // the real update: count the images crossed since the old pos
+                    const int di = image_step(rtn[(size_t)b * D + i], x[i], half);
+                    if (di) A.img[(size_t)(p.bead_off + b) * D + i] += di;
+                }
                 rtn[(size_t)b * D + i] = x[i];
             }
             if (finite && p.calc_wca && left_skin<D>(p, A, b, x)) moved = true;

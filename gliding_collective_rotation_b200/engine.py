@@ -226,6 +226,18 @@ class Engine:
         f_arr = (C.c_int32 * n)(*[1 if f else 0 for f in fixed])
         check(self.lib.gcr_couple(self._ctx, n, s_arr, f_arr, cw.ctypes.data_as(C.POINTER(C.c_double))))
 
+    def unwrapped(self, slot):
+        """Positions plus the periodic images each bead crossed since
+        admission (or ``reset_images``): float64 [n, dim] on the device."""
+        st = self.systems[int(slot)]
+        out = torch.empty_like(st.pos)
+        torch.cuda.current_stream(self.device).synchronize()
+        check(self.lib.gcr_unwrapped_positions(self._ctx, int(slot), C.c_void_p(out.data_ptr())))
+        return out
+
+    def reset_images(self, slot):
+        check(self.lib.gcr_reset_images(self._ctx, int(slot)))
+
     def decouple(self, slot):
         check(self.lib.gcr_decouple(self._ctx, int(slot)))
 

@@ -275,6 +275,13 @@ GCR_API int gcr_pair_correlation(gcr_ctx *ctx, int32_t slot, int32_t kind, doubl
  * positions the list was built from; *entries (host, or NULL) the total. */
 GCR_API int gcr_neighbour_list(gcr_ctx *ctx, int32_t slot, int32_t *counts, int32_t *partners,
                                int32_t partners_depth, double *build_pos, int64_t *entries);
+/* Unwrapped positions of a resident system, out[n][dim] (device): pos + L *
+ * the periodic images each bead crossed in the real updates since its
+ * admission or the last gcr_reset_images -- the displacement record of the
+ * mean-squared displacement (no counterpart in the reference, whose
+ * analysis unwraps between saved states).  Synchronises the stream. */
+GCR_API int gcr_unwrapped_positions(gcr_ctx *ctx, int32_t slot, double *out);
+GCR_API int gcr_reset_images(gcr_ctx *ctx, int32_t slot);
 /* Standard normals of the Philox stream the step draws: [n][2*dim] noise_vec
  * layout for one step (device out). */
 GCR_API int gcr_philox_noise(int32_t dim, uint64_t seed, int64_t step, int64_t n, int32_t do_trans,
