@@ -85,7 +85,12 @@ def _views(specs, precision, device, srk_order=2):
 
 
 class Batch:
-    """Systems of one dimension and precision resident in one context."""
+    """Systems of one dimension and precision resident in one context.
+
+    Each system's parameters are its spec's own ``params`` object, shared:
+    ``relax``/``set_adaptive`` write the dt rule into it and ``regrow`` the
+    step counter, so the specs follow the batch (pass copies to keep the
+    originals)."""
 
     def __init__(self, specs, precision="mixed", device=None, steps_per_graph=10, cell_depth=None,
                  block_beads=128, block_cells=256, stream=None, ctas_per_sm=0, list_depth=None, srk_order=2):
