@@ -1333,6 +1333,7 @@ __global__ void k_sys_dt(BatchArgs A, int n_slots)
     // every member takes the same dt
     double dtmax = p.dtmax, mdps = p.mdps, rk = p.rk;
     bool lead = false;
+    int group_fatal = 0;
     for (int k = 0; k < p.grp_n && k < kMaxPops; k++) {
         const int m = p.grp[k];
         if (m < 0 || m >= n_slots) continue;
@@ -1344,9 +1345,17 @@ __global__ void k_sys_dt(BatchArgs A, int n_slots)
             lead = true;
         }
         const SysS &sm = A.S[m];
+        if (m != i) group_fatal |= sm.flags & kFlagFatal;
         if (m == i || pm.fixed || !sm.active || (sm.flags & kFlagFatal)) continue;
         const double Sm = pm.sqrt2D + pref * sqrt(__longlong_as_double((long long)sm.max_f2)) / pm.radius;
         Sg = Sm > Sg ? Sm : Sg;
+    }
+    if (group_fatal) {
+        // a population of the box stopped this step (its forces on the others
+        // are stale): the whole box stops before the real update, the step is
+        // not counted, and the host sees the same flag on every member
+        s.flags |= group_fatal;
+        return;
     }
     double dt;
     if (Sg == 0.0)

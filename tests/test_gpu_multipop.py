@@ -23,7 +23,7 @@ def _min_image(d, L):
     return d - L * np.round(d / L)
 
 
-def _batch(d, s, precision="fp64", D=None, seeds=None, srk_order=2):
+def _batch(d, s, precision="fp64", D=None, seeds=None, srk_order=2, list_depth=None):
     st0 = d["status_before"]
     specs = []
     for k in range(s["n_pops"]):
@@ -35,7 +35,7 @@ def _batch(d, s, precision="fp64", D=None, seeds=None, srk_order=2):
                               rk_cheat=s["rk_cheat"], seed=int(seeds[k]) if seeds is not None else 0)
         specs.append(SystemSpec(f"pop{k}", s["dim"], a["pos"], a["tangent"], a["chain_id"], a["rest_lengths"],
                                 params, st0[8], s["max_dist_per_step"]))
-    b = Batch(specs, precision=precision, srk_order=srk_order)
+    b = Batch(specs, precision=precision, srk_order=srk_order, list_depth=list_depth)
     b.couple(range(s["n_pops"]), s["fixed"], d["cross_wca"])
     return b
 
@@ -210,3 +210,28 @@ def test_drop_in_steps_a_list_of_populations(name):
     assert abs(st.dt - d["status_after"][best][0]) <= 1e-12 * st.dt
     assert abs(st.max_forces_strength - d["status_after"][best][5]) <= 1e-10 * st.max_forces_strength
     pops[0]._gcr_group.engine.close()
+
+
+@pytest.mark.parametrize("name", ["pops2_2d", "pops3_fixed_2d"])
+def test_a_member_overflow_stops_the_box(name):
+    """Lists too short for one population: its overflow stops every
+    population of the box before the real update, the batch regrows and
+    re-runs the step for all of them, and the result is the run with deep
+    enough lists from the start, bit for bit."""
+    d, s = load(name)
+    st0 = d["status_before"]
+    b = _batch(d, s, D=0.01, seeds=[5, 6, 7], list_depth=4)
+    b.begin(1, dt=st0[0])
+    b.run(1)
+    # the short lists overflow at the first build: no member took the step
+    assert all(x["steps_done"] == 0 and x["flags"] & 16 for x in b.statuses())
+    b.close()
+    out = []
+    for depth in (4, 128):
+        b = _batch(d, s, D=0.01, seeds=[5, 6, 7], list_depth=depth)
+        sts = b.run_checked(20)
+        assert all(x["steps_done"] == 20 and x["flags"] == 0 for x in sts)
+        out.append([st.pos.cpu().numpy() for st in b.states])
+        b.close()
+    for a, c in zip(*out):
+        np.testing.assert_array_equal(a, c)
