@@ -27,7 +27,7 @@ def pop_arrays(d, s, k):
                 n_nearby=s["n_nearby"][k], longest=s["longest"][k], fixed=s["fixed"][k])
 
 
-def oracle_group(d, s, D=None, seeds=None, srk_order=2):
+def oracle_group(d, s, D=None, seeds=None, srk_order=2, rigid=None):
     """An ``OracleGroup`` at the case's relaxed state (``D`` replaces every
     moving population's translational diffusion constant)."""
     systems = []
@@ -36,7 +36,8 @@ def oracle_group(d, s, D=None, seeds=None, srk_order=2):
         Dk = a["D"] if D is None or a["fixed"] else D
         o = O.OracleSystem(a["pos"], a["tangent"], a["chain_id"], a["rest_lengths"], s["L"], a["spring"], a["wca"],
                            a["active"], Dk, a["Dr"], a["radius"], a["n_nearby"], s["n_grid"],
-                           calc_springs=a["longest"] > 1, srk_order=srk_order)
+                           calc_springs=a["longest"] > 1, srk_order=srk_order,
+                           rigid_rod=(rigid[k] if rigid is not None else 0.0))
         o.seed = int(seeds[k]) if seeds is not None else 0
         systems.append(o)
     return O.OracleGroup(systems, s["fixed"], d["cross_wca"])

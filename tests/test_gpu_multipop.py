@@ -23,7 +23,7 @@ def _min_image(d, L):
     return d - L * np.round(d / L)
 
 
-def _batch(d, s, precision="fp64", D=None, seeds=None, srk_order=2, list_depth=None):
+def _batch(d, s, precision="fp64", D=None, seeds=None, srk_order=2, list_depth=None, rigid=None):
     st0 = d["status_before"]
     specs = []
     for k in range(s["n_pops"]):
@@ -32,7 +32,8 @@ def _batch(d, s, precision="fp64", D=None, seeds=None, srk_order=2, list_depth=N
         params = SystemParams(L=s["L"], spring_params=a["spring"], wca_params=a["wca"], active_params=a["active"],
                               D=Dk, Dr=a["Dr"], radius=a["radius"], n_nearby=a["n_nearby"],
                               calc_springs=a["longest"] > 1, dtmax=st0[8], max_dist_per_step=s["max_dist_per_step"],
-                              rk_cheat=s["rk_cheat"], seed=int(seeds[k]) if seeds is not None else 0)
+                              rk_cheat=s["rk_cheat"], seed=int(seeds[k]) if seeds is not None else 0,
+                              rigid_rod=(rigid[k] if rigid is not None else 0.0))
         specs.append(SystemSpec(f"pop{k}", s["dim"], a["pos"], a["tangent"], a["chain_id"], a["rest_lengths"],
                                 params, st0[8], s["max_dist_per_step"]))
     b = Batch(specs, precision=precision, srk_order=srk_order, list_depth=list_depth)
@@ -235,3 +236,30 @@ def test_a_member_overflow_stops_the_box(name):
         b.close()
     for a, c in zip(*out):
         np.testing.assert_array_equal(a, c)
+
+
+@pytest.mark.parametrize("srk_order", [2, 4])
+def test_rigid_rods_among_populations_match_the_oracle(srk_order):
+    """The chains blended towards rigid rods beside free beads: the
+    projection uses each stage's force, cross forces included.  Factor 0.05:
+    the relaxed chains are bent, and a larger factor snaps them onto their
+    neighbours (forces of 1e4 to 1e6, dt down to 1e-8)."""
+    d, s = load("pops2_2d")
+    n, L = s["n_pops"], s["L"]
+    rigid = [0.05, 0.0]
+    st0 = d["status_before"]
+    b = _batch(d, s, D=0.01, seeds=[41, 42], srk_order=srk_order, rigid=rigid)
+    g = oracle_group(d, s, D=0.01, seeds=[41, 42], srk_order=srk_order, rigid=rigid)
+    dt, step0 = st0[0], 0
+    for n_steps, tol in ((1, 1e-12), (9, 1e-9)):
+        b.begin(n_steps, dt=dt)
+        b.run(n_steps)
+        assert all(x["flags"] == 0 and x["steps_done"] == n_steps for x in b.statuses())
+        res = g.run(n_steps, dt=dt, dtmax=st0[8], max_dist_per_step=s["max_dist_per_step"], rk_cheat=s["rk_cheat"],
+                    noise_mode=O.NOISE_PHILOX, step0=step0, srk_order=srk_order)
+        step0 += n_steps
+        dt = res["dt"]
+        for k in range(n):
+            err = np.max(np.abs(_min_image(b.states[k].pos.cpu().numpy() - g.systems[k].pos, L)))
+            assert err < tol, (k, n_steps, err)
+    b.close()
