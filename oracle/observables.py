@@ -1,7 +1,7 @@
 """CPU restatement of the reference's observables -- test infrastructure.
 
-Only the tests (and the bench's CPU arm) use this module, as the checker of
-the GPU observables in ``gliding_collective_rotation_b200/observables.py``.
+Only the tests (and the bench's CPU arm) use this module, to check the GPU
+observables in ``gliding_collective_rotation_b200/observables.py``.
 It follows the reference definition by definition and is pinned to the
 reference's own outputs in ``tests/golden/observables.npz`` (made by
 ``tests/golden/make_observables_golden.py``).

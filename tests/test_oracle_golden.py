@@ -1,6 +1,6 @@
 """The CPU oracle against golden vectors produced by the reference itself.
 
-These pin the oracle before it is trusted as the checker of the CUDA path:
+These pin the oracle before the CUDA path is compared with it:
 RNG stream, single kernels (springs, pair forces, propulsion), cell and
 neighbour lists (exact), and whole SRK2_force_calc calls (trajectories and
 status bookkeeping) from ``tests/golden/*.npz``.
