@@ -227,6 +227,12 @@ def run_reference(args):
     if rank != 0:
         return
     specs, desc = make_workload(args.workload, systems=args.systems)
+    if getattr(specs, "groups", ()):
+        # the CPU restatement couples populations over all pairs, not over the
+        # reference's lists: its time would not be the reference's
+        print(json.dumps({"impl": "reference", "unavailable": "coupled populations: no list-based CPU "
+                          "restatement of the multi-population step to time"}), flush=True)
+        return
     threads = os.cpu_count() or 1
     # a bounded sample: the first systems, relaxed untimed with the reference's adaptive dt
     sample = specs[:args.cpu_systems]
