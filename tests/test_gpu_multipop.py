@@ -147,7 +147,7 @@ def test_decoupled_systems_step_alone():
         x.close()
 
 
-@pytest.mark.parametrize("name", ["pops2_2d", "pops3_fixed_2d"])
+@pytest.mark.parametrize("name", CASES)
 def test_srk4_coupled_matches_the_oracle(name):
     """The SRK4 branch (SRK.py:186-215, 296-321) with several populations:
     the cross forces enter every stage force."""
@@ -238,13 +238,14 @@ def test_a_member_overflow_stops_the_box(name):
         np.testing.assert_array_equal(a, c)
 
 
+@pytest.mark.parametrize("name", ["pops2_2d", "pops2_3d"])
 @pytest.mark.parametrize("srk_order", [2, 4])
-def test_rigid_rods_among_populations_match_the_oracle(srk_order):
+def test_rigid_rods_among_populations_match_the_oracle(srk_order, name):
     """The chains blended towards rigid rods beside free beads: the
     projection uses each stage's force, cross forces included.  Factor 0.05:
     the relaxed chains are bent, and a larger factor snaps them onto their
     neighbours (forces of 1e4 to 1e6, dt down to 1e-8)."""
-    d, s = load("pops2_2d")
+    d, s = load(name)
     n, L = s["n_pops"], s["L"]
     rigid = [0.05, 0.0]
     st0 = d["status_before"]
