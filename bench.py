@@ -26,9 +26,7 @@ import argparse
 import json
 import math
 import os
-import subprocess
 import sys
-import tempfile
 import time
 
 import numpy as np
@@ -84,17 +82,68 @@ class _Specs(list):
     groups = ()
 
 
+def workload_config(args, specs, desc, world):
+    """The ``config`` of the JSON line: what the workload is, the same in the
+    GPU arm and the reference arm (measured quantities go elsewhere)."""
+    n_beads = sum(s.n for s in specs)
+    dim = specs[0].dim
+    F = 8 if args.precision == "fp64" else 4
+    # bytes per bead a step touches: pos, pos1, build positions (FP64), the
+    # tangent, force, pair force and noise (FT), list count, topology, images
+    touched = 3 * dim * 8 + 4 * dim * F + 4 + 1 + 4 * dim
+    return {"workload": desc, "systems_per_gpu": len(specs), "beads_per_gpu": n_beads,
+            "coupled_groups": len(getattr(specs, "groups", ())),
+            "parallelism": f"{world} GPU(s), independent systems per GPU (no collective in the data path)",
+            "l2": f"inputs larger than L2: a step touches ~{touched * n_beads / 1e6:.0f} MB per GPU > 126 MB",
+            "dt_rule": "adaptive (SRK.py:323-353): dtmax = configured dt, max_dist_per_step of "
+                       "config.grid_list_setup"}
+
+
+def stratified(specs, m):
+    """Indices of `m` systems at the bead-count quantiles (k + 1/2) / m of
+    the workload: the CPU arms time a sample spread over the size range."""
+    order = sorted(range(len(specs)), key=lambda i: (specs[i].n, i))
+    if m >= len(order):
+        return order
+    return sorted({order[min(len(order) - 1, int((k + 0.5) * len(order) / m))] for k in range(m)})
+
+
 # --------------------------------------------------------------------------
-# algorithmic bytes per kernel launch (HBM roofline)
+# algorithmic bytes (HBM roofline)
 # --------------------------------------------------------------------------
 
+def step_bytes(dim, precision):
+    """Minimum HBM bytes per bead of one SRK2 step with one cell rebuild, by
+    phase, as the hot path's measurement contract defines them (P = 8 B per
+    FP64 position component, F = 4 B (mixed) or 8 B (FP64) per force
+    component):
+      predictor  read pos, write pos1, write F0, 4 B of metadata = 2dP + dF + 4
+      corrector  read pos and pos1, read F0, write pos and the tangent, 4 B
+                 of metadata                                     = 3dP + 2dF + 4
+      cell build read pos, 8 B of cell key and sorted index, the sorted copy
+                                                                 = 2dP + 8
+    in all 7dP + 3dF + 16: 152 B in 2D mixed, 176 B 2D FP64, 220 B 3D mixed."""
+    P = 8
+    F = 8 if precision == "fp64" else 4
+    out = {"predictor": 2 * dim * P + dim * F + 4, "corrector": 3 * dim * P + 2 * dim * F + 4,
+           "cell_build": 2 * dim * P + 8}
+    out["step"] = sum(out.values())
+    return out
+
+
+# the phase of the step each timed kernel group belongs to
+KERNEL_PHASE = {"lists_pos": "cell_build", "pair_pos": "predictor", "stage0": "predictor", "lists_pos1": "cell_build",
+                "pair_pos1": "corrector", "stage1": "corrector", "update": "corrector"}
+
+
 def algorithmic_bytes(dim, precision, n_beads, n_cells, get_orient, rot_diff, list_mean, builds_per_stage):
-    """Minimum DRAM bytes of one launch of each kernel group: every input read
-    once and every output written once.  A list build (bin + sort + build)
-    reads the positions, writes and reads one cell slot per bead, writes the
-    list and the build positions; it runs for a fraction `builds_per_stage`
-    of the beads per stage (measured), and that fraction of its bytes is
-    charged to each list launch."""
+    """This design's own byte model of one launch of each kernel group (the
+    ``model_frac`` of the line): every input the kernel reads counted once
+    and every output once.  A list build (bin + sort + build) reads the
+    positions, writes and reads one cell slot per bead, writes the list and
+    the build positions; it runs for a fraction `builds_per_stage` of the
+    beads per stage (measured), and that fraction of its bytes is charged to
+    each list launch."""
     P = 8                                   # FP64 position component
     F = 8 if precision == "fp64" else 4     # force / tangent / noise component
     tan = dim * F if get_orient else 0
@@ -116,63 +165,110 @@ KERNELS = ["lists_pos", "pair_pos", "stage0", "lists_pos1", "pair_pos1", "stage1
 # --------------------------------------------------------------------------
 
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock, its maximum and the active clock-event reasons of one GPU,
+    read through NVML (the library nvidia-smi queries) on a host thread every
+    `period` seconds between ``start`` and ``stop``: the timed region of a
+    20-step run lasts ~15 ms, far below nvidia-smi's sampling interval, so
+    the sampler runs in-process.  The main thread waits on the GPU (CUDA
+    events) while it samples."""
 
-    def __init__(self, gpu_index=0):
-        self.gpu = gpu_index
-        self.proc = None
-        self.path = None
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
+
+    def __init__(self, device_index=0, period=0.002):
+        self.device_index = device_index
+        self.period = period
+        self.samples = []
+        self.error = None
+        self._stop = None
+        self._thread = None
+        self._nvml = None
+        self._h = None
+
+    def _handle(self, nv):
+        import torch
+        props = torch.cuda.get_device_properties(self.device_index)
+        uuid = getattr(props, "uuid", None)
+        if uuid is not None:
+            try:
+                return nv.nvmlDeviceGetHandleByUUID(("GPU-" + str(uuid)).encode())
+            except Exception:
+                pass
+        bus = getattr(props, "pci_bus_id", None)
+        if bus is not None:
+            pci = f"{getattr(props, 'pci_domain_id', 0):08x}:{bus:02x}:{getattr(props, 'pci_device_id', 0):02x}.0"
+            try:
+                return nv.nvmlDeviceGetHandleByPciBusId_v2(pci.encode())
+            except Exception:
+                pass
+        return nv.nvmlDeviceGetHandleByIndex(self.device_index)
 
     def start(self):
+        import threading
         try:
-            fd, self.path = tempfile.mkstemp(suffix=".csv")
-            os.close(fd)
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except (OSError, FileNotFoundError):
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            self._nvml = nv
+            self._h = self._handle(nv)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self._h, nv.NVML_CLOCK_SM))
+        except Exception as e:  # no NVML: the line says so
+            self.error = f"NVML unavailable: {e}"
+            return
+        self._stop = threading.Event()
+
+        def loop():
+            nv, h = self._nvml, self._h
+            while not self._stop.is_set():
+                try:
+                    self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                         int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))))
+                except Exception as e:
+                    self.error = str(e)
+                    return
+                self._stop.wait(self.period)
+
+        self._thread = threading.Thread(target=loop, daemon=True)
+        self._thread.start()
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
+        if self._thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.error or "not started"]}
+        self._stop.set()
+        self._thread.join(timeout=5)
         try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        rows = []
-        with open(self.path) as fh:
-            for line in fh:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.path)
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+            self._nvml.nvmlShutdown()
+        except Exception:
+            pass
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["no samples"]}
+        nv = self._nvml
+        active = 0
+        for _, r in self.samples:
+            active |= r
+        reasons = sorted(name for name, const in self.REASONS if active & getattr(nv, const, 0))
+        sm = [s for s, _ in self.samples]
+        return {"sm_mhz": float(np.median(sm)), "sm_min_mhz": float(min(sm)), "sm_max_mhz": self.max_mhz,
+                "reasons": reasons, "samples": len(self.samples), "source": "NVML, every 2 ms in the timed region"}
 
 
 # --------------------------------------------------------------------------
 # CPU arm: the reference's algorithm (oracle) on a bounded sample
 # --------------------------------------------------------------------------
 
-def cpu_sample_rate(specs, states_host, steps, threads, max_systems=4, budget_s=20.0):
+def cpu_sample_rate(specs, states_host, steps, threads, budget_s=20.0):
     """bead-steps/s of the oracle (the reference's Numba step restated in C,
-    OpenMP threads over chain-aligned chunks) on the first systems of the
-    workload, each run for `steps` steps after an untimed list build, under
-    the reference's adaptive dt rule as the GPU arm (dtmax = the system's dt,
-    max_dist_per_step of grid_list_setup; each system's dt carried)."""
+    OpenMP threads over chain-aligned chunks) on the systems `specs` (a
+    sample of the workload) from the states `states_host`, in rounds of
+    `steps` steps per system after an untimed list build until `budget_s`
+    seconds of stepping, under the reference's adaptive dt rule as the GPU
+    arm (dtmax = the system's dt, max_dist_per_step of grid_list_setup; each
+    system's dt carried)."""
     from oracle import oracle as O
     systems = []
-    for spec, (pos, tan) in list(zip(specs, states_host))[:max_systems]:
+    for spec, (pos, tan) in zip(specs, states_host):
         p = spec.params
         ng = max(1, int(p.L / (2.0 * max(2 * spec.rest_lengths.max(), p.wca_params[3]))))
         sysm = O.OracleSystem(pos, tan, spec.chain_id, spec.rest_lengths, p.L, p.spring_params, p.wca_params,
@@ -234,24 +330,27 @@ def run_reference(args):
                           "restatement of the multi-population step to time"}), flush=True)
         return
     threads = os.cpu_count() or 1
-    # a bounded sample: the first systems, relaxed untimed with the reference's adaptive dt
-    sample = specs[:args.cpu_systems]
+    # a bounded sample spread over the size range, relaxed untimed with the
+    # reference's adaptive dt
+    sample = [specs[i] for i in stratified(specs, args.cpu_systems)]
     states = [relax_on_cpu(s) for s in sample]
     for _ in range(max(0, min(args.warmup, 1))):
-        cpu_sample_rate(sample, states, 2, threads, max_systems=1)
+        cpu_sample_rate(sample[:1], states[:1], 2, threads)
     rates = []
     for _ in range(args.steps):
-        r, used, secs = cpu_sample_rate(sample, states, args.cpu_steps, threads, max_systems=len(sample),
+        r, used, secs = cpu_sample_rate(sample, states, args.cpu_steps, threads,
                                         budget_s=args.cpu_budget / max(args.steps, 1))
         rates.append(r)
     value = float(np.median(rates))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     line = {
         "impl": "reference", "metric": "bead-steps/s", "value": value, "unit": "bead-steps/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": desc, "sample": ", ".join(used)},
+        "config": workload_config(args, specs, desc, world),
         "cpu_baseline": {"value": value, "unit": "bead-steps/s", "cores": threads, "kind": "port",
-                         "sample": f"{len(used)} systems x {args.cpu_steps} steps per timed step: {', '.join(used)}"},
+                         "sample": f"{len(sample)} systems at the bead-count quantiles of the workload, relaxed on "
+                                   f"the CPU, {args.cpu_steps}-step rounds per timed step: {', '.join(used)}"},
         "e2e": {"value": value, "unit": "bead-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -358,36 +457,48 @@ def run_gpu(args):
     builds_per_stage = bead_builds / (2.0 * args.steps * n_beads)
 
     # ---- per-kernel profile (roofline) ----------------------------------
-    # every run starts with a forced list build; the difference of an
-    # (n+1)-step and a 1-step profile is n steps in steady state
-    batch.begin(args.profile_steps + 1)
-    k_all = eng.profile_steps(args.profile_steps + 1)
-    batch.begin(1)
-    k_one = eng.profile_steps(1)
-    kms = np.maximum(k_all - k_one, 0.0) / args.profile_steps
+    # the same steps launched kernel group by kernel group with CUDA events
+    # between the groups on the context stream (steady state: the lists
+    # carry over from the timed run)
+    batch.begin(args.profile_steps)
+    kms = eng.profile_steps(args.profile_steps) / args.profile_steps
     cfg = eng.cfg
     from gliding_collective_rotation_b200.engine import footprint
     n_cells = sum(footprint(cfg, s.params, s.n, len(s.rest_lengths))[0] for s in specs)
     get_orient = bool(specs[0].params.spring_params[4])
     rot_diff = (not get_orient) and specs[0].params.Dr > 0
-    alg = algorithmic_bytes(batch.dim, args.precision, n_beads, n_cells, get_orient, rot_diff, list_mean,
-                            builds_per_stage)
+    model = algorithmic_bytes(batch.dim, args.precision, n_beads, n_cells, get_orient, rot_diff, list_mean,
+                              builds_per_stage)
+    sb = step_bytes(batch.dim, args.precision)
     dom = int(np.argmax(kms))
+    kname = KERNELS[dom]
     pk = peaks()
-    achieved = alg[KERNELS[dom]] / (kms[dom] / 1e3) / 1e9
+    # the dominant kernel against the contract's bytes of its phase of the
+    # step (beads x bytes per bead of that phase, per launch)
+    alg_bytes = sb[KERNEL_PHASE[kname]] * n_beads
+    achieved = alg_bytes / (kms[dom] / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as fh:
             tr = json.load(fh).get(args.workload, {}).get(args.precision, {})
-        if KERNELS[dom] in tr:
-            traffic = tr[KERNELS[dom]] * n_beads
-    roofline = {"bound": "hbm", "kernel": KERNELS[dom], "achieved": achieved, "peak": pk["hbm_gbs"],
+        if kname in tr:
+            v = tr[kname]
+            traffic = (v["bytes_per_bead"] if isinstance(v, dict) else float(v)) * n_beads
+    step_achieved = sb["step"] * value / world / 1e9
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": pk["hbm_gbs"],
                 "unit": "GB/s", "frac": achieved / pk["hbm_gbs"], "traffic": traffic,
-                "algorithmic_bytes": alg[KERNELS[dom]], "peak_source": pk["source"],
+                "algorithmic_bytes": alg_bytes,
+                "algorithmic_bytes_source": f"{sb[KERNEL_PHASE[kname]]} B per bead: the {KERNEL_PHASE[kname]} "
+                                            f"phase of the hot-path contract's {sb['step']} B per bead-step",
+                "peak_source": f"{pk['source']} (MEASURED_PEAKS.json hbm_gbs)" if pk["source"] == "measured"
+                else pk["source"],
                 "kernel_ms": {k: float(v) for k, v in zip(KERNELS, kms)},
-                "step_alg_bytes_per_bead": sum(alg.values()) / n_beads,
-                "step_frac": (sum(alg.values()) / (kms.sum() / 1e3) / 1e9) / pk["hbm_gbs"]}
+                "step_bytes_per_bead": sb["step"], "step_achieved": step_achieved,
+                "step_frac": step_achieved / pk["hbm_gbs"],
+                "model_bytes_per_bead": {k: float(v) / n_beads for k, v in model.items()},
+                "model_frac": (model[kname] / (kms[dom] / 1e3) / 1e9) / pk["hbm_gbs"],
+                "model_step_frac": (sum(model.values()) / (kms.sum() / 1e3) / 1e9) / pk["hbm_gbs"]}
 
     # ---- plain path: one system per launch sequence ---------------------
     plain = None
@@ -441,6 +552,11 @@ def run_gpu(args):
            "steps_per_call": spc, "calls": n_calls,
            "api": "Batch.begin/run (gcr_call_begin_batch, gcr_run) with pinned host buffers"}
 
+    # ---- the same workload in FP64, and the mixed path's error against it
+    fp64 = None
+    if args.fp64_block and args.precision == "mixed" and not groups:
+        fp64 = fp64_block(args, specs, batch, dev)
+
     # ---- CPU baseline (rank 0, N = 1) ------------------------------------
     cpu = None
     # (coupled populations: the CPU sampler steps single populations, so
@@ -448,41 +564,44 @@ def run_gpu(args):
     if world == 1 and args.cpu_baseline and not groups:
         host_states = [(s.pos.cpu().numpy(), s.tangent.double().cpu().numpy()) for s in batch.states]
         threads = os.cpu_count() or 1
-        r, used, secs = cpu_sample_rate(specs, host_states, args.cpu_steps, threads, max_systems=args.cpu_systems,
-                                        budget_s=args.cpu_budget)
-        r1, used1, secs1 = cpu_sample_rate(specs, host_states, args.cpu_steps, 1, max_systems=2,
-                                           budget_s=max(2.0, args.cpu_budget / 3))
+        idx = stratified(specs, args.cpu_systems)
+        r, used, secs = cpu_sample_rate([specs[i] for i in idx], [host_states[i] for i in idx], args.cpu_steps,
+                                        threads, budget_s=args.cpu_budget)
+        idx1 = stratified(specs, 2)
+        r1, used1, secs1 = cpu_sample_rate([specs[i] for i in idx1], [host_states[i] for i in idx1], args.cpu_steps,
+                                           1, budget_s=max(2.0, args.cpu_budget / 3))
         cpu = {"value": r, "unit": "bead-steps/s", "cores": threads, "kind": "port",
-               "sample": f"{args.cpu_steps} steps of {', '.join(used)} ({secs:.1f} s); adaptive dt as the GPU arm",
+               "sample": f"{len(idx)} systems at the bead-count quantiles of the workload from the GPU's relaxed "
+                         f"states, {args.cpu_steps}-step rounds: {', '.join(used)} ({secs:.1f} s); adaptive dt as "
+                         "the GPU arm",
                "single_thread_value": r1,
-               "single_thread_sample": f"{args.cpu_steps} steps of {', '.join(used1)} ({secs1:.1f} s)"}
+               "single_thread_sample": f"{args.cpu_steps}-step rounds of {', '.join(used1)} ({secs1:.1f} s)"}
 
-    working_set = sum(v.numel() * v.element_size() for v in big.values()) + eng.cfg.cell_capacity * (
-        8 + eng.cfg.cell_depth * 4) + n_beads * (4 * list_mean + 4 + 8 * batch.dim)
+    spg = args.steps_per_graph
     line = {
         "metric": "bead-steps/s", "value": value, "unit": "bead-steps/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
-        "config": {"workload": desc, "systems_per_gpu": len(specs), "beads_per_gpu": n_beads,
-                   "precision": ("FP32 forces and SRK arithmetic, FP64 positions" if args.precision == "mixed"
-                                 else "FP64"),
-                   "parallelism": f"{world} GPU(s), independent systems per GPU",
-                   "coupled_groups": len(groups),
-                   "l2": f"inputs larger than L2: working set {working_set / 1e6:.0f} MB per GPU > 126 MB",
-                   "relax_steps": relax_steps, "steps_done": steps_done, "flags": flags,
-                   "dt_rule": "adaptive (SRK.py:323-353): dtmax = configured dt, max_dist_per_step of "
-                              "config.grid_list_setup", "dt_mean": dt_mean,
-                   "cell_factor": args.cell_factor,
-                   "skin": specs[0].params.skin if specs[0].params.skin is not None
-                   else default_skin(specs[0].params.wca_params[3]),
-                   "steps_per_graph": args.steps_per_graph, "cell_depth": batch.cell_depth,
-                   "list_depth": batch.list_depth, "list_mean": list_mean,
-                   "list_builds_per_stage": builds_per_stage, "block_beads": args.block_beads,
-                   "ctas_per_sm": args.ctas_per_sm,
-                   "autotune": None if tuned is None else {k: v for k, v in tuned.items() if k != "trials"}},
+        "config": workload_config(args, specs, desc, world),
+        "run": {"precision": ("FP32 forces and SRK arithmetic, FP64 positions" if args.precision == "mixed"
+                              else "FP64"),
+                "relax_steps": relax_steps, "steps_done": steps_done, "flags": flags, "dt_mean": dt_mean,
+                "cell_factor": args.cell_factor,
+                "skin": specs[0].params.skin if specs[0].params.skin is not None
+                else default_skin(specs[0].params.wca_params[3]),
+                "steps_per_graph": spg, "cell_depth": batch.cell_depth,
+                "list_depth": batch.list_depth, "list_mean": list_mean,
+                "list_builds_per_stage": builds_per_stage, "block_beads": args.block_beads,
+                "ctas_per_sm": args.ctas_per_sm,
+                "autotune": None if tuned is None else {k: v for k, v in tuned.items() if k != "trials"}},
         "e2e": e2e, "roofline": roofline, "clocks": clk,
-        "gpu_launches": 15 * args.steps + 1,
+        # the run-start check, then 15 kernels per step (two list builds of
+        # four, two pair, two stage, dt rule, update, bookkeeping) in graphs
+        # of steps_per_graph steps
+        "gpu_launches": 1 + 15 * spg * math.ceil(args.steps / spg),
     }
+    if fp64 is not None:
+        line["fp64"] = fp64
     if plain is not None:
         line["plain"] = plain
         line["batched_over_plain"] = value / world / plain["value"]
@@ -496,39 +615,39 @@ def run_gpu(args):
 
 
 # --------------------------------------------------------------------------
-# serving: a Poisson trace through the continuous-batching server
-# --------------------------------------------------------------------------
-
-# --------------------------------------------------------------------------
 # precision: the mixed path against the FP64 path of the same kernels
 # --------------------------------------------------------------------------
 
-def run_precision_report(args):
-    """Both precisions from one relaxed FP64 state, same Philox seeds and
-    the same dt rule: the relative force error after one step and the
-    position divergence over `--precision-report` steps."""
+def specs_at(specs, positions, tangents, steps):
+    """Copies of `specs` that start from the given device state and step
+    counters (the Philox key), with parameter objects of their own."""
+    import copy
+    import dataclasses
+    out = []
+    for sp, p, t, k in zip(specs, positions, tangents, steps):
+        prm = copy.copy(sp.params)
+        prm.step = int(k)
+        out.append(dataclasses.replace(sp, pos=p.cpu().numpy().copy(), tangent=t.double().cpu().numpy().copy(),
+                                       params=prm))
+    return out
+
+
+def compare_precisions(specs, dt0, marks, depths):
+    """The mixed path and the FP64 path of the same kernels from one state
+    (`specs`, as ``specs_at`` makes them), same Philox seeds and the same
+    adaptive dt rule, with an FP64 control whose positions start one ulp
+    away (its divergence is the growth of any perturbation in these chaotic
+    systems): per checkpoint in `marks`, the largest position difference
+    over L of any system against FP64, that of the control, and after the
+    first step the relative L2 error of the forces (F0 + F1)."""
     import torch
     from gliding_collective_rotation_b200.batch import Batch
 
-    torch.cuda.set_device(0)
-    specs, desc = make_workload(args.workload, scale=args.scale, systems=args.systems)
-    dim = specs[0].dim
-    base = Batch(specs, precision="fp64")
-    relax_steps = base.relax(max_steps=args.relax_steps, adaptive_after=True)
-    sts = base.statuses()
-    dt0 = [s["dt"] for s in sts]
-    for sp, st, status in zip(specs, base.states, sts):
-        # the relaxed state and the step counter (Philox key) both runs start from
-        sp.pos = st.pos.cpu().numpy().copy()
-        sp.tangent = st.tangent.cpu().numpy().copy()
-        sp.params.step = status["step"]
-    # cells and lists as deep as the relaxed run needed, with a margin
-    depths = dict(cell_depth=min(128, 2 * base.cell_depth), list_depth=min(1024, 2 * base.list_depth))
-    base.close()
     runs = {prec: Batch(specs, precision=prec, **depths) for prec in ("fp64", "mixed")}
-    # control: FP64 again with every position moved by about one ulp; its
-    # divergence is the growth of any perturbation in these systems
+    for b in runs.values():
+        b.set_adaptive(True)
     ctl = Batch(specs, precision="fp64", **depths)
+    ctl.set_adaptive(True)
     rng = np.random.default_rng(1)
     for st, sp in zip(ctl.states, specs):
         ulp = np.spacing(sp.params.L)
@@ -536,13 +655,12 @@ def run_precision_report(args):
         st.pos.remainder_(sp.params.L)
     runs["fp64_ulp"] = ctl
     L = np.array([sp.params.L for sp in specs])
-    report = {"checkpoints": []}
+    rows = []
     done = 0
-    marks = sorted({1, *[m for m in (10, 100, 1000, 5000, args.precision_report) if m <= args.precision_report]})
     for b in runs.values():
-        b._carry_dt = list(dt0)  # the first call starts from the relaxed run's dt
-    for m in marks:
-        for prec, b in runs.items():
+        b._carry_dt = list(dt0)  # the first call starts from the common state's dt
+    for m in sorted(set(marks) | {1}):
+        for b in runs.values():
             b.run_checked(m - done)  # regrows cells or lists if the run needs them
             b.engine.synchronize()
         done = m
@@ -563,14 +681,84 @@ def run_precision_report(args):
         row = {"steps": m, "max_pos_err_over_L": err, "fp64_ulp_control_over_L": err_ctl}
         if m == 1:
             row["force_rel_l2_err"] = (num / den) ** 0.5 if den > 0 else 0.0
-        flags = sorted({s["flags"] for b in runs.values() for s in b.statuses()})
-        row["flags"] = flags
-        report["checkpoints"].append(row)
+        row["flags"] = sorted({s["flags"] for b in runs.values() for s in b.statuses()})
+        rows.append(row)
     for b in runs.values():
         b.close()
+    return rows
+
+
+def fp64_block(args, specs, batch, dev):
+    """The workload's FP64 throughput and the mixed path's error against
+    FP64, both from the mixed run's state after its timed steps: an FP64
+    batch of the same systems is warmed up and timed over `--steps` steps as
+    the line's own value is, then ``compare_precisions`` runs to
+    `--fp64-steps` steps."""
+    import torch
+    from gliding_collective_rotation_b200.batch import Batch
+
+    sts = batch.statuses()
+    start = ([s.pos for s in batch.states], [s.tangent for s in batch.states], [s["step"] for s in sts])
+    state = specs_at(specs, *start)
+    dt0 = [s["dt"] for s in sts]
+    depths = dict(cell_depth=min(128, 2 * batch.cell_depth), list_depth=min(1024, 2 * batch.list_depth))
+    b = Batch(specs_at(specs, *start), precision="fp64", device=dev, steps_per_graph=args.steps_per_graph,
+              ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads, **depths)
+    b.set_adaptive(True)
+    b._carry_dt = list(dt0)
+    b.run_checked(args.warmup)
+    b.begin(args.steps)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(b.engine.stream)
+    b.run(args.steps)
+    e1.record(b.engine.stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    flags = sorted({s["flags"] for s in b.statuses()})
+    b.close()
+    marks = [m for m in (10, 100, 1000, 5000) if m <= args.fp64_steps]
+    rows = compare_precisions(state, dt0, marks, depths)
+    by = {r["steps"]: r for r in rows}
+    return {"value": b.n_beads * args.steps / (ms / 1e3), "unit": "bead-steps/s", "ms_per_step": ms / args.steps,
+            "steps": args.steps, "flags": flags,
+            "force_rel_l2_err_1step": by[1]["force_rel_l2_err"],
+            "max_pos_err_over_L": {str(m): by[m]["max_pos_err_over_L"] for m in marks},
+            "fp64_ulp_control_over_L": {str(m): by[m]["fp64_ulp_control_over_L"] for m in marks},
+            "error_run_flags": sorted({f for r in rows for f in r["flags"]}),
+            "from": "the mixed run's state after its timed steps; same Philox seeds, same adaptive dt rule; the "
+                    "control is FP64 with every position moved by one ulp"}
+
+
+def run_precision_report(args):
+    """Both precisions from one relaxed FP64 state, same Philox seeds and
+    the same dt rule: the relative force error after one step and the
+    position divergence over `--precision-report` steps."""
+    import torch
+    from gliding_collective_rotation_b200.batch import Batch
+
+    torch.cuda.set_device(0)
+    specs, desc = make_workload(args.workload, scale=args.scale, systems=args.systems)
+    dim = specs[0].dim
+    base = Batch(specs, precision="fp64")
+    relax_steps = base.relax(max_steps=args.relax_steps, adaptive_after=True)
+    sts = base.statuses()
+    dt0 = [s["dt"] for s in sts]
+    state = specs_at(specs, [s.pos for s in base.states], [s.tangent for s in base.states], [s["step"] for s in sts])
+    # cells and lists as deep as the relaxed run needed, with a margin
+    depths = dict(cell_depth=min(128, 2 * base.cell_depth), list_depth=min(1024, 2 * base.list_depth))
+    base.close()
+    marks = [m for m in (10, 100, 1000, 5000, args.precision_report) if m <= args.precision_report]
+    rows = compare_precisions(state, dt0, marks, depths)
     line = {"metric": "mixed vs FP64 error", "workload": desc, "dim": dim, "relax_steps": relax_steps,
-            "dt_rule": "adaptive (SRK.py:323-353), dtmax = configured dt", **report}
+            "dt_rule": "adaptive (SRK.py:323-353), dtmax = configured dt", "checkpoints": rows}
     print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------
+# serving: a Poisson trace through the continuous-batching server
+# --------------------------------------------------------------------------
 
 
 def run_serve(args):
@@ -583,12 +771,24 @@ def run_serve(args):
                        max_steps=args.max_steps)
     reqs = [S.request_from_trace(e, obs_every=args.obs_every) for e in tr]
     srv = S.Server(2, args.precision, hbm_budget=int(args.hbm_budget_gb * (1 << 30)), chunk=args.chunk)
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(0, period=0.05)
     clocks.start()
     res = srv.serve(reqs, timeout=args.serve_timeout)
     clk = clocks.stop()
+    st = dict(srv.stats)
+    rejected = list(srv.rejected)
     srv.close()
     s = S.summarize(res)
+    dev = max(st["device_s"], 1e-12)
+    # where the makespan went: the rounds' graphs on the device, the host
+    # work of the rounds around them, and waiting with nothing resident
+    gap = {"makespan_s": s["makespan_s"], "device_busy_s": st["device_s"],
+           "round_host_s": st["round_wall_s"] - st["device_s"], "idle_s": st["idle_s"],
+           "other_host_s": s["makespan_s"] - st["round_wall_s"] - st["idle_s"],
+           "rounds": st["rounds"], "regrows": st["regrows"],
+           "device_bead_steps_per_s": st["bead_steps_done"] / dev,
+           "mean_resident_beads": st["resident_bead_s"] / dev,
+           "armed_step_fraction": st["bead_steps_done"] / max(st["bead_steps_armed_max"], 1)}
     line = {
         "metric": "bead-steps/s", "value": s["bead_steps_per_s"], "unit": "bead-steps/s", "n_gpus": 1,
         "steps": None, "warmup": 0, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
@@ -596,8 +796,8 @@ def run_serve(args):
         "config": {"workload": f"served trace: {args.requests} requests, Poisson {args.rate}/s, beads log-uniform "
                                f"[1e3, {args.max_beads:.0e}], steps uniform [{args.min_steps}, {args.max_steps}], "
                                f"adaptive dt (dtmax 1e-3), P/S/angle every {args.obs_every} steps",
-                   "chunk": args.chunk, "hbm_budget_gb": args.hbm_budget_gb, **s},
-        "clocks": clk,
+                   "chunk": args.chunk, "hbm_budget_gb": args.hbm_budget_gb},
+        "serve": {**s, "rejected": len(rejected)}, "gap": gap, "clocks": clk,
     }
     print(json.dumps(line), flush=True)
 
@@ -630,19 +830,23 @@ def main():
     ap.add_argument("--e2e-steps-per-call", type=int, default=100)
     ap.add_argument("--cpu-baseline", type=int, default=1)
     ap.add_argument("--cpu-steps", type=int, default=20)
-    ap.add_argument("--cpu-systems", type=int, default=4)
+    ap.add_argument("--cpu-systems", type=int, default=8, help="systems of the CPU sample (size quantiles)")
     ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--fp64-block", type=int, default=1,
+                    help="1: add the FP64 throughput and the mixed path's error against FP64 to the line")
+    ap.add_argument("--fp64-steps", type=int, default=1000, help="steps of the mixed-vs-FP64 comparison")
     ap.add_argument("--precision-report", type=int, default=0,
                     help="report mixed vs FP64 error over this many steps instead of timing")
-    ap.add_argument("--requests", type=int, default=64, help="serve: requests in the trace")
+    # serving (--workload serve): the defaults are the serving configuration
+    ap.add_argument("--requests", type=int, default=200, help="serve: requests in the trace")
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate per second")
-    ap.add_argument("--max-beads", type=float, default=2e5, help="serve: largest request")
+    ap.add_argument("--max-beads", type=float, default=1e6, help="serve: largest request (log-uniform from 1e3)")
     ap.add_argument("--min-steps", type=int, default=1000)
-    ap.add_argument("--max-steps", type=int, default=5000)
+    ap.add_argument("--max-steps", type=int, default=20000)
     ap.add_argument("--obs-every", type=int, default=100)
     ap.add_argument("--chunk", type=int, default=200)
-    ap.add_argument("--hbm-budget-gb", type=float, default=16.0)
-    ap.add_argument("--serve-timeout", type=float, default=600.0)
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
+    ap.add_argument("--serve-timeout", type=float, default=900.0)
     args = ap.parse_args()
     if args.workload == "serve" and args.impl == "gcr":
         run_serve(args)

@@ -76,6 +76,7 @@ SIGNATURES = {
                                 C.POINTER(C.c_int64)]),
     "gcr_run": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32]),
     "gcr_get_status": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Status)]),
+    "gcr_get_statuses": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(Status)]),
     "gcr_count_active": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "gcr_synchronize": (C.c_int, [C.c_void_p]),
     "gcr_profile_steps": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_float)]),

@@ -252,7 +252,7 @@ class Batch:
         return done
 
     def statuses(self):
-        return [self.engine.status(st.slot) for st in self.states]
+        return self.engine.statuses([st.slot for st in self.states])
 
     def run_checked(self, steps, max_regrow=6):
         """Run `steps` steps of every system; after a cell or list overflow

@@ -522,11 +522,27 @@ int enqueue_step(gcr_ctx *c)
     return c->graph_obs ? launch_observe(c) : GCR_OK;
 }
 
-// start of a run: zero the cell counts, flag every system for a list build
+// start of a run: flag the armed systems whose neighbour lists no longer
+// cover their positions (the host may have moved beads between calls); the
+// others keep their lists
 int enqueue_run_start(gcr_ctx *c)
 {
-    GCR_CUDA(cudaMemsetAsync(c->cnt, 0, sizeof(int) * std::max<int64_t>(c->cfg.cell_capacity, 1), c->stream));
-    return launch_sys(c, c->ks.sys_mark);
+    return launch(c, c->ks.run_check, c->grid_update, c->cfg.block_beads);
+}
+
+// a list build of `slot` before its next pair forces, from zeroed cell
+// counts: admission, a new descriptor (grid, cutoff, skin, exclusions), a
+// coupling change, and re-arming after a stop (a build that overflowed its
+// cells leaves their counts set)
+int mark_rebuild(gcr_ctx *c, int slot)
+{
+    const Slot &sl = c->slots[slot];
+    if (sl.n_cells_alloc > 0)
+        GCR_CUDA(cudaMemsetAsync(c->cnt + sl.cell_off, 0, sizeof(int) * (size_t)sl.n_cells_alloc, c->stream));
+    int n = (int)c->slots.size();
+    void *a[] = {&c->args, &n, &slot};
+    GCR_CUDA(cudaLaunchKernel(c->ks.sys_mark, dim3(c->grid_sys), dim3(128), a, 0, c->stream));
+    return GCR_OK;
 }
 
 int build_graph(gcr_ctx *c)
@@ -820,6 +836,9 @@ int gcr_admit(gcr_ctx *c, const gcr_system_desc *desc, const gcr_system_buffers 
     sl.longest = err[1];
     fill_sysp(c, sl, nc, skin, c->hP[slot]);
     GCR_CUDA(cudaMemcpyAsync(c->dP + slot, &c->hP[slot], sizeof(SysP), cudaMemcpyHostToDevice, c->stream));
+    // its first stage builds the lists, from zeroed counts in its cells
+    rc = mark_rebuild(c, slot);
+    if (rc) return rc;
     rc = rebuild_tiles(c);
     if (rc) return rc;
     *slot_out = slot;
@@ -834,12 +853,15 @@ int gcr_evict(gcr_ctx *c, int32_t slot)
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     if (sl.group >= 0) {
         // its coupled populations step on their own again
+        const Group members = c->groups[sl.group];
         dissolve(c, sl.group);
         int rc = drop_graph(c);
         if (rc) return rc;
         bool moved = false;
         rc = apply_groups(c, &moved);
         if (rc) return rc;
+        for (int k = 0; k < members.n; k++)
+            if (members.slots[k] != slot && (rc = mark_rebuild(c, members.slots[k]))) return rc;
     }
     c->beads.release(sl.bead_off, sl.desc.n_beads);
     if (sl.n_cells_alloc) c->cells.release(sl.cell_off, sl.n_cells_alloc);
@@ -870,8 +892,9 @@ int gcr_update_desc(gcr_ctx *c, int32_t slot, const gcr_system_desc *desc)
             if (g.slots[k] != slot && c->slots[g.slots[k]].desc.L != desc->L)
                 return fail(GCR_ERR_BAD_ARG, "coupled populations share L");
     }
-    // the current grid stays while its cells cover the list radius (every
-    // run starts with a list build, so a grid change between calls is safe)
+    // the current grid stays while its cells cover the list radius (a new
+    // descriptor marks the system for a list build, so a grid change between
+    // calls is safe)
     if (desc->calc_wca && sl.desc.calc_wca && desc->L == sl.desc.L && sl.nc >= 3 &&
         desc->L / (double)sl.nc >= desc->wca_params[3] + skin)
         nc = sl.nc;
@@ -899,6 +922,15 @@ int gcr_update_desc(gcr_ctx *c, int32_t slot, const gcr_system_desc *desc)
                                  c->stream));
     } else {
         GCR_CUDA(cudaMemcpyAsync(c->dP + slot, &c->hP[slot], sizeof(SysP), cudaMemcpyHostToDevice, c->stream));
+    }
+    // the lists follow the new cutoff, skin, exclusions and grid (coupled:
+    // the partners' cross lists too)
+    if (sl.group >= 0) {
+        const Group &g = c->groups[sl.group];
+        for (int k = 0; k < g.n; k++)
+            if ((rc = mark_rebuild(c, g.slots[k]))) return rc;
+    } else if ((rc = mark_rebuild(c, slot))) {
+        return rc;
     }
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     return GCR_OK;
@@ -967,6 +999,8 @@ int gcr_couple(gcr_ctx *c, int32_t n, const int32_t *slots, const int32_t *fixed
         return rc;
     }
     c->tiles_dirty = true;
+    for (int a = 0; a < n; a++)
+        if ((rc = mark_rebuild(c, slots[a]))) return rc;
     return rebuild_tiles(c);
 }
 
@@ -977,11 +1011,14 @@ int gcr_decouple(gcr_ctx *c, int32_t slot)
     if (g < 0) return GCR_OK;
     int rc = drop_graph(c);
     if (rc) return rc;
+    const Group members = c->groups[g];
     dissolve(c, g);
     bool moved = false;
     rc = apply_groups(c, &moved);
     if (rc) return rc;
     c->tiles_dirty = true;
+    for (int k = 0; k < members.n; k++)
+        if ((rc = mark_rebuild(c, members.slots[k]))) return rc;
     return rebuild_tiles(c);
 }
 
@@ -998,8 +1035,11 @@ int check_call(const gcr_call *call)
     return GCR_OK;
 }
 
-void arm(SysS &s, const gcr_call *call)
+// arm one system for a call; true when its last call ended in a stop (a
+// fatal flag), after which its lists are rebuilt from zeroed cell counts
+bool arm(SysS &s, const gcr_call *call)
 {
+    const bool stopped = (s.flags & kFlagFatal) != 0;
     // dt <= 0: the system keeps the dt its last step chose (status.dt of the
     // reference, which carries from call to call)
     if (call->dt > 0.0) s.dt = call->dt;
@@ -1020,6 +1060,7 @@ void arm(SysS &s, const gcr_call *call)
     s.series_mark = 0;
     s.flags = 0;
     s.active = ((0 < s.max_steps || s.max_steps < 0) && (0.0 < s.max_dt_usable || s.max_dt_usable < 0.0)) ? 1 : 0;
+    return stopped;
 }
 }  // namespace
 
@@ -1035,8 +1076,14 @@ int gcr_call_begin_batch(gcr_ctx *c, int32_t n, const int32_t *slots, const gcr_
     // the device table holds the step counters: fetch it, arm, write it back
     GCR_CUDA(cudaMemcpyAsync(c->hS.data(), c->dS, sizeof(SysS) * S, cudaMemcpyDeviceToHost, c->stream));
     GCR_CUDA(cudaStreamSynchronize(c->stream));
-    for (int i = 0; i < n; i++) arm(c->hS[slots[i]], calls + i);
+    std::vector<int> stopped;
+    for (int i = 0; i < n; i++)
+        if (arm(c->hS[slots[i]], calls + i)) stopped.push_back(slots[i]);
     GCR_CUDA(cudaMemcpyAsync(c->dS, c->hS.data(), sizeof(SysS) * S, cudaMemcpyHostToDevice, c->stream));
+    for (int sl : stopped) {
+        int rc = mark_rebuild(c, sl);
+        if (rc) return rc;
+    }
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     return GCR_OK;
 }
@@ -1050,8 +1097,9 @@ int gcr_call_begin(gcr_ctx *c, int32_t slot, const gcr_call *call)
     // the device copy holds the current step counter: fetch it first
     GCR_CUDA(cudaMemcpyAsync(&s, c->dS + slot, sizeof(SysS), cudaMemcpyDeviceToHost, c->stream));
     GCR_CUDA(cudaStreamSynchronize(c->stream));
-    arm(s, call);
+    const bool stopped = arm(s, call);
     GCR_CUDA(cudaMemcpyAsync(c->dS + slot, &s, sizeof(SysS), cudaMemcpyHostToDevice, c->stream));
+    if (stopped && (rc = mark_rebuild(c, slot))) return rc;
     GCR_CUDA(cudaStreamSynchronize(c->stream));
     return GCR_OK;
 }
@@ -1174,12 +1222,9 @@ int gcr_count_active(gcr_ctx *c, int32_t *n_out)
     return GCR_OK;
 }
 
-int gcr_get_status(gcr_ctx *c, int32_t slot, gcr_status *out)
+namespace {
+void fill_status(const SysS &s, gcr_status *out)
 {
-    if (!valid_slot(c, slot) || !out) return fail(GCR_ERR_BAD_ARG, "invalid slot or output");
-    SysS &s = c->hS[slot];
-    GCR_CUDA(cudaMemcpyAsync(&s, c->dS + slot, sizeof(SysS), cudaMemcpyDeviceToHost, c->stream));
-    GCR_CUDA(cudaStreamSynchronize(c->stream));
     out->dt = s.dt;
     out->dt_used = s.elapsed;
     out->max_forces_strength = s.mfs;
@@ -1189,6 +1234,28 @@ int gcr_get_status(gcr_ctx *c, int32_t slot, gcr_status *out)
     out->active = s.active;
     out->list_builds = s.list_builds;
     out->series_rows = s.series_rows;
+}
+}  // namespace
+
+int gcr_get_statuses(gcr_ctx *c, int32_t n, const int32_t *slots, gcr_status *out)
+{
+    if (!c || n < 0 || (n > 0 && (!slots || !out))) return fail(GCR_ERR_BAD_ARG, "bad argument");
+    for (int i = 0; i < n; i++)
+        if (!valid_slot(c, slots[i])) return fail(GCR_ERR_BAD_ARG, "invalid slot");
+    const int S = (int)c->slots.size();
+    GCR_CUDA(cudaMemcpyAsync(c->hS.data(), c->dS, sizeof(SysS) * S, cudaMemcpyDeviceToHost, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < n; i++) fill_status(c->hS[slots[i]], out + i);
+    return GCR_OK;
+}
+
+int gcr_get_status(gcr_ctx *c, int32_t slot, gcr_status *out)
+{
+    if (!valid_slot(c, slot) || !out) return fail(GCR_ERR_BAD_ARG, "invalid slot or output");
+    SysS &s = c->hS[slot];
+    GCR_CUDA(cudaMemcpyAsync(&s, c->dS + slot, sizeof(SysS), cudaMemcpyDeviceToHost, c->stream));
+    GCR_CUDA(cudaStreamSynchronize(c->stream));
+    fill_status(s, out);
     return GCR_OK;
 }
 

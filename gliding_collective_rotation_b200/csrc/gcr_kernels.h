@@ -66,7 +66,8 @@ struct KernelSet {
     void *topo;
     void *sys_dt;
     void *sys_end;
-    void *sys_mark;  // flag every resident system for a list build
+    void *sys_mark;  // flag one resident system (or all) for a list build
+    void *run_check;  // run start: flag the armed systems whose lists no longer cover their positions
     void *lists_plan;  // compact the systems that take part in a list build
     void *pair_cross[3];  // pair forces at pos / pos1 / pos2 with the other populations' (coupled systems)
     size_t (*stage_smem)(int block_beads);  // dynamic shared memory of the stage kernels

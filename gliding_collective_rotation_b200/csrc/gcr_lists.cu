@@ -326,14 +326,17 @@ cudaError_t launch_order_params(int dim, int precision, const SysP &p, const int
 }
 
 // chain start offsets; flags chain ids that do not run 0, 1, ..., n_chains-1
-// in order (chains must be contiguous, non-empty bead ranges)
+// in order (chains must be contiguous, non-empty bead ranges): the first
+// bead is in chain 0, each next bead in the same chain or the next one, the
+// last bead in chain n_chains-1 -- so every chain id owns a bead range and
+// every start offset is written
 __global__ void k_chain_starts(const int32_t *__restrict__ chain, int n, int n_chains, int32_t *cs, int *err)
 {
     int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b == 0) cs[n_chains] = n;
     if (b >= n) return;
     int c = chain[b];
-    const int step = b > 0 ? c - chain[b - 1] : c;
+    const int step = b > 0 ? c - chain[b - 1] : (c == 0 ? 0 : -1);
     if (c < 0 || c >= n_chains || step < 0 || step > 1 || (b == n - 1 && c != n_chains - 1)) {
         atomicOr(err, 4);
         return;

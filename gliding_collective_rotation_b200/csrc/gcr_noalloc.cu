@@ -4,23 +4,25 @@
 // gcr_order_params_noalloc computes what gcr_order_params computes (the
 // per-chain angle and the polar / nematic order parameters), but for caller
 // owned device arrays and without a context, so it never calls cudaMalloc or
-// cudaFree.  It is meant for callers that must not allocate device memory:
-// an analysis hook that runs while steps are queued on the GPU (cudaFree
-// synchronises the whole device, and a cudaMalloc inside a stream capture
-// in the global capture mode is an error), or a host application that hands
-// out all device memory from its own pool under a fixed budget.
+// cudaFree.  It is meant for callers that cannot allocate device memory: an
+// analysis hook that samples a system while other work is queued on the
+// device (cudaFree waits for the whole device, stalling that work), or a host
+// application that hands out all device memory from its own pool under a
+// fixed budget and leaves none to a library.  The call waits for its own
+// stream before it returns, with the results on the host.
 //
-// Its scratch (chain start offsets, the three results and an error word)
+// Its scratch (chain start offsets, the three results and two error words)
 // lives in the file-scope array below, sized for at most
 // GCR_NOALLOC_MAX_CHAINS chains: about 1 MiB that every GPU which loads
 // the library holds until the process exits.  In host code the array's name
 // only stands for the device object; its device address is looked up with
 // cudaGetSymbolAddress once per device, with that device current, by the
-// first call made on that device.  Make that first call before any stream
-// capture.  All calls share the one array and it keeps the last call's
-// contents: each call clears the words that must start at zero, and calls
-// that overlap on the GPU (different streams, or different host threads on
-// one device) race on it.
+// first call made on that device, and kept for the life of the process (a
+// cudaDeviceReset after that first call leaves the kept address stale and is
+// not supported).  All calls share the one array and it keeps the last
+// call's contents: each call clears the words that must start at zero, and
+// calls that overlap on the GPU (different streams, or different host
+// threads on one device) race on it.
 #include <cstring>
 #include <mutex>
 
@@ -53,23 +55,6 @@ int noalloc_fail(int code, const char *msg)
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 namespace {
-
-// chain ids must be 0, 1, ..., n_chains-1 in non-decreasing runs, so that
-// every chain owns a non-empty bead range
-__global__ void k_noalloc_check_chains(const int32_t *__restrict__ chain, int n, int n_chains, int *err)
-{
-    int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b >= n) return;
-    int c = chain[b];
-    bool ok = (c >= 0 && c < n_chains);
-    if (b == 0) ok = ok && c == 0;
-    if (b == n - 1) ok = ok && c == n_chains - 1;
-    if (b > 0) {
-        int d = c - chain[b - 1];
-        ok = ok && (d == 0 || d == 1);
-    }
-    if (!ok) atomicOr(err, 8);
-}
 
 // device address of the scratch on the current device (set-up once per device)
 int scratch_on_current_device(unsigned char **out)
@@ -111,12 +96,13 @@ int gcr_order_params_noalloc(int32_t dim, int32_t precision, const void *tangent
     int *d_err = reinterpret_cast<int *>(base + kErrOff);
     cudaStream_t st = static_cast<cudaStream_t>(cuda_stream);
     const int n = (int)n_beads, nch = (int)n_chains;
-    // the error word and the results start at zero; the starts of this call
-    // are all written by launch_chain_starts once the chain ids are valid
-    if (cudaMemsetAsync(d_err, 0, sizeof(int), st) != cudaSuccess ||
+    // the error words (bad chain ids, longest chain) and the results start at
+    // zero; launch_chain_starts checks the chain ids (first bead in chain 0,
+    // steps of 0 or 1, last bead in chain n_chains-1) and, when they pass,
+    // has written every start offset of this call
+    if (cudaMemsetAsync(d_err, 0, 2 * sizeof(int), st) != cudaSuccess ||
         cudaMemsetAsync(d_out, 0, 4 * sizeof(double), st) != cudaSuccess)
         return noalloc_fail(GCR_ERR_CUDA, "clearing the scratch failed");
-    k_noalloc_check_chains<<<(n + 255) / 256, 256, 0, st>>>(chain_id, n, nch, d_err);
     if (gcr::launch_chain_starts(chain_id, n, nch, starts, d_err, st) != cudaSuccess)
         return noalloc_fail(GCR_ERR_CUDA, "chain start kernel failed to launch");
     int err = 0;

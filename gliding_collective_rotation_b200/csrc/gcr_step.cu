@@ -1407,13 +1407,43 @@ __global__ void k_topo(const int32_t *__restrict__ chain, int n, uint8_t *topo)
 }
 
 
-// flag every resident system for a list build (the start of a run: the host
-// may have changed positions since the last list)
-__global__ void k_sys_mark(BatchArgs A, int n_slots)
+// flag system `slot` for a list build (every resident system when slot < 0):
+// admission, a new descriptor, a coupling change
+__global__ void k_sys_mark(BatchArgs A, int n_slots, int slot)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_slots) return;
+    if (i >= n_slots || (slot >= 0 && i != slot)) return;
     A.S[i].rebuild = 1;
+}
+
+// start of a run: the host may have written positions since the last list
+// build, so every armed system is tested against its list as the step
+// kernels test it -- a bead farther than skin/2 from where the list was built
+// flags a rebuild, and otherwise the list still holds every pair within
+// r_cut.  Coupled populations are flagged outright: their fixed members have
+// no bead tiles to test.
+template <int D>
+__global__ void __launch_bounds__(512) k_run_check(BatchArgs A)
+{
+    const int nt = *A.n_bead_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.bead_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        SysS &s = A.S[tl.sys];
+        // no barriers in this kernel: a per-thread decision is safe
+        if (!p.calc_wca || !ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal)) continue;
+        if (ld_volatile(&s.rebuild)) continue;
+        const int b = tl.begin + threadIdx.x;
+        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
+        if (p.grp_n > 0) {
+            s.rebuild = 1;
+            continue;
+        }
+        double x[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < D; i++) x[i] = p.pos[(size_t)b * D + i];
+        if (left_skin<D>(p, A, b, x)) s.rebuild = 1;
+    }
 }
 
 // ------------------------------------------------------------------------
@@ -1478,6 +1508,7 @@ KernelSet kernel_set(int dim, int precision)
         k.build1 = (void *)k_build<2, 1>;
         k.bin2 = (void *)k_bin<2, 2>;
         k.build2 = (void *)k_build<2, 2>;
+        k.run_check = (void *)k_run_check<2>;
     } else {
         k.bin0 = (void *)k_bin<3, 0>;
         k.bin1 = (void *)k_bin<3, 1>;
@@ -1485,6 +1516,7 @@ KernelSet kernel_set(int dim, int precision)
         k.build1 = (void *)k_build<3, 1>;
         k.bin2 = (void *)k_bin<3, 2>;
         k.build2 = (void *)k_build<3, 2>;
+        k.run_check = (void *)k_run_check<3>;
     }
     k.sort = (void *)k_sort;
     k.topo = (void *)k_topo;

@@ -39,7 +39,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from ._lib import FLAG_CELL_OVERFLOW, FLAG_LIST_OVERFLOW
+from ._lib import FLAG_CELL_OVERFLOW, FLAG_LIST_OVERFLOW, GcrError
 from .batch import MAX_DEPTH, MAX_LIST_DEPTH, OVERFLOW, default_depth, default_list_depth
 from .engine import Engine, SystemState
 from .workloads import SystemSpec, make_system
@@ -90,6 +90,48 @@ class _Live:
     series: list = field(default_factory=list)
 
 
+def check_request(req, dim, bead_capacity):
+    """Why ``req`` cannot be served (a short reason), or None.  A request
+    must ask for at least one step, hold at least one bead, have arrays of
+    matching shapes with finite values, chain ids 0, 1, ..., n_chains - 1 in
+    contiguous increasing ranges (the layout the step kernels index by), a
+    positive box side and rest lengths, and fit an empty context."""
+    sp = getattr(req, "spec", None)
+    if sp is None:
+        return "no system"
+    steps = req.steps
+    if not isinstance(steps, (int, np.integer)) or steps < 1:
+        return f"steps must be a positive integer (got {steps!r})"
+    if not isinstance(req.obs_every, (int, np.integer)) or req.obs_every < 0:
+        return f"obs_every must be a non-negative integer (got {req.obs_every!r})"
+    if sp.dim != dim:
+        return f"dimension {sp.dim} in a {dim}D server"
+    pos, tan = np.asarray(sp.pos), np.asarray(sp.tangent)
+    chain, rest = np.asarray(sp.chain_id), np.asarray(sp.rest_lengths)
+    n = pos.shape[0] if pos.ndim == 2 else -1
+    if n < 1 or pos.shape[1] != dim:
+        return f"positions must be [n >= 1, {dim}] (got {pos.shape})"
+    if tan.shape != pos.shape or chain.shape != (n,):
+        return "tangent [n, dim] and chain_id [n] must match the positions"
+    if rest.ndim != 1 or rest.shape[0] < 1:
+        return "rest_lengths must be [n_chains >= 1]"
+    if not np.issubdtype(chain.dtype, np.integer):
+        return "chain ids must be integers"
+    steps_c = np.diff(chain)
+    if chain[0] != 0 or np.any((steps_c != 0) & (steps_c != 1)) or chain[-1] != rest.shape[0] - 1:
+        return "chain ids must run 0, 1, ..., n_chains - 1 in contiguous increasing ranges"
+    L = float(sp.params.L)
+    if not (math.isfinite(L) and L > 0):
+        return f"box side must be positive and finite (got {L})"
+    if not (np.all(np.isfinite(pos)) and np.all(np.isfinite(tan)) and np.all(np.isfinite(rest))):
+        return "non-finite positions, tangents or rest lengths"
+    if np.any(rest <= 0):
+        return "rest lengths must be positive"
+    if n > bead_capacity:
+        return f"{n} beads exceed the context ({bead_capacity})"
+    return None
+
+
 def request_from_trace(entry, relax=False, obs_every=0, adaptive=True):
     """A ``Request`` from one entry of ``workloads.serve_trace``."""
     spec = make_system(f"req{entry['id']}", 2, entry["n_chains"], entry["chain_length"], entry["L"],
@@ -121,7 +163,14 @@ class Server:
         self.live: dict[int, _Live] = {}
         self.queue: list[Request] = []
         self.results: list[Result] = []
+        self.rejected: list[tuple[int, str]] = []  # (request id, reason)
         self.t0 = None
+        # where the time of a served trace goes: device time of the rounds'
+        # graphs (CUDA events on the context stream), wall time of the rounds
+        # (arming, statuses, series, finished requests, regrows around them),
+        # and time with nothing resident waiting for arrivals
+        self.stats = {"rounds": 0, "device_s": 0.0, "round_wall_s": 0.0, "idle_s": 0.0, "regrows": 0,
+                      "resident_bead_s": 0.0, "bead_steps_done": 0, "bead_steps_armed_max": 0}
 
     # -- memory ----------------------------------------------------------------
     def _per_bead_bytes(self):
@@ -148,18 +197,38 @@ class Server:
 
     # -- admission -------------------------------------------------------------
     def _admit_one(self, req: Request):
+        """Admit the queued request ``req``: True when it left the queue
+        (admitted, or rejected), False when the context has no room yet."""
+        why = check_request(req, self.dim, self.bead_capacity)
+        if why is not None:
+            self._reject(req, why)
+            return True
         sp = req.spec
         p = sp.params
         if req.relax or req.adaptive:
             p.max_dist_per_step = sp.relax_mdps
         st = SystemState.from_host(sp.pos, sp.tangent, sp.chain_id, sp.rest_lengths, p, precision=self.precision,
                                    device=self.device)
-        slot = self.engine.try_admit(st)
+        try:
+            slot = self.engine.try_admit(st)
+        except GcrError as e:
+            if e.code != -1:  # GCR_ERR_BAD_ARG: the library refused the system itself
+                raise
+            del st
+            self._reject(req, str(e))
+            return True
         if slot is None:
             del st
             return False
+        self.queue.remove(req)
         self.live[slot] = _Live(req, st, self.now(), relaxing=req.relax)
         return True
+
+    def _reject(self, req, reason):
+        """A request that cannot be served leaves the queue with its reason;
+        the resident requests are not touched."""
+        self.queue.remove(req)
+        self.rejected.append((req.id, reason))
 
     def _admit(self):
         now = self.now()
@@ -168,13 +237,11 @@ class Server:
             return
         blocked = None  # the first arrived request that did not fit
         for r in arrived:
-            if len(self.live) >= self.max_systems:
+            if len(self.live) >= self.max_systems and check_request(r, self.dim, self.bead_capacity) is None:
                 break
             if blocked is not None and now - blocked.arrival > self.max_head_wait:
                 break  # no backfill past a head that has waited too long
-            if self._admit_one(r):
-                self.queue.remove(r)
-            elif blocked is None:
+            if not self._admit_one(r) and blocked is None:
                 blocked = r
 
     # -- overflow --------------------------------------------------------------
@@ -222,9 +289,24 @@ class Server:
                 self._series = torch.zeros((max(self.max_systems, len(slots)), max(rows, self.chunk + 1), 5),
                                            dtype=torch.float64, device=self.device)
             series = self._series
+        t_round = time.perf_counter()
         self.engine.call_begin_many(slots, plan, dts, series=series, series_every=every, series_phase=phase)
+        ev = None
+        if self.device.type == "cuda":
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record(self.engine.stream)
         self.engine.run(max(plan))
-        statuses = {s: self.engine.status(s) for s in slots}
+        if ev is not None:
+            ev[1].record(self.engine.stream)
+        statuses = dict(zip(slots, self.engine.statuses(slots)))
+        st_ = self.stats
+        st_["rounds"] += 1
+        if ev is not None:
+            dev_s = ev[0].elapsed_time(ev[1]) / 1e3
+            st_["device_s"] += dev_s
+            st_["resident_bead_s"] += dev_s * sum(self.live[s].state.n for s in slots)
+        st_["bead_steps_done"] += sum(self.live[s].state.n * statuses[s]["steps_done"] for s in slots)
+        st_["bead_steps_armed_max"] += sum(self.live[s].state.n for s in slots) * max(plan)
         rows_host = None
         if series is not None and any(statuses[s]["series_rows"] for s in slots):
             rows_host = series.cpu().numpy()
@@ -269,6 +351,8 @@ class Server:
             self._finish(s, statuses[s]["flags"])
         if overflow:
             self._regrow({s: statuses[s] for s in self.live})
+            st_["regrows"] += 1
+        st_["round_wall_s"] += time.perf_counter() - t_round
 
     def _finish(self, slot, flags):
         lv = self.live.pop(slot)
@@ -283,10 +367,10 @@ class Server:
     # -- driver ----------------------------------------------------------------
     def serve(self, requests, timeout=None):
         """Serve ``requests`` (arrival times in seconds from the start) until
-        all are done; returns the results in completion order."""
-        for r in requests:
-            if not self.fits_ever(r):
-                raise ValueError(f"request {r.id}: {r.spec.n} beads exceed the context ({self.bead_capacity})")
+        all are done; returns the results in completion order.  A request that
+        cannot be served (``check_request``) is rejected when it arrives and
+        listed in ``rejected`` as (id, reason); the others run as if it had
+        never come."""
         self.queue = sorted(requests, key=lambda r: (r.arrival, r.id))
         self.t0 = time.perf_counter()
         while self.queue or self.live:
@@ -298,6 +382,7 @@ class Server:
                     wait = self.queue[0].arrival - self.now()
                     if wait > 0:
                         time.sleep(min(wait, 0.05))
+                        self.stats["idle_s"] += min(wait, 0.05)
                     elif not self._admit_one_blocking():
                         raise RuntimeError("a request does not fit an empty context")
                 continue
@@ -305,11 +390,7 @@ class Server:
         return self.results
 
     def _admit_one_blocking(self):
-        head = self.queue[0]
-        if self._admit_one(head):
-            self.queue.remove(head)
-            return True
-        return False
+        return self._admit_one(self.queue[0])
 
     def close(self):
         self.engine.close()

@@ -224,6 +224,11 @@ GCR_API int gcr_decouple(gcr_ctx *ctx, int32_t slot);
 GCR_API int gcr_run(gcr_ctx *ctx, int64_t max_steps, int32_t sync_every);
 /* Copy the status of a system to the host (synchronises the stream). */
 GCR_API int gcr_get_status(gcr_ctx *ctx, int32_t slot, gcr_status *out);
+/* The statuses of `n` resident systems `slots` at once, out[n] (host): one
+ * copy of the state table (synchronises the stream).  Like gcr_get_status,
+ * the write-back of updates.SRK2_force_calc (updates.py:249-256), for many
+ * systems at the end of a serving round. */
+GCR_API int gcr_get_statuses(gcr_ctx *ctx, int32_t n, const int32_t *slots, gcr_status *out);
 /* Number of armed systems still running (synchronises the stream). */
 GCR_API int gcr_count_active(gcr_ctx *ctx, int32_t *n_out);
 GCR_API int gcr_synchronize(gcr_ctx *ctx);
@@ -292,16 +297,19 @@ GCR_API int gcr_philox_noise(int32_t dim, uint64_t seed, int64_t step, int64_t n
  * (what gcr_order_params computes) from caller-owned device arrays --
  * tangents [n_beads][2] (FP64 for GCR_FP64, FP32 for GCR_MIXED) and chain
  * ids [n_beads] running 0..n_chains-1 in contiguous ranges -- without a
- * context and without allocating device memory: for callers that must not
- * call cudaMalloc/cudaFree (an analysis hook running while steps are queued,
- * since cudaFree synchronises the device; code inside a global-mode stream
- * capture; an application that owns all device memory through its own
- * pool).  Its scratch is a static device array of about 1 MiB held by every
- * GPU that loads the library, sized for at most GCR_NOALLOC_MAX_CHAINS
- * chains; more chains return GCR_ERR_CAPACITY.  The first call on a device
- * looks up that array's device address (cudaGetSymbolAddress) and must come
- * before any stream capture.  Calls that overlap on the GPU race on the
- * shared scratch.  Synchronises `cuda_stream`; out = [P, S, director]. */
+ * context and without allocating device memory: for callers that cannot
+ * call cudaMalloc/cudaFree (an analysis hook sampling a system while other
+ * work is queued on the device, since cudaFree waits for the whole device;
+ * an application that hands out all device memory from its own pool).  Its
+ * scratch is a static device array of about 1 MiB held by every GPU that
+ * loads the library until the process exits, sized for at most
+ * GCR_NOALLOC_MAX_CHAINS chains; more chains return GCR_ERR_CAPACITY.  The
+ * first call on a device, with that device current, looks up that array's
+ * device address (cudaGetSymbolAddress) and keeps it for the life of the
+ * process (a cudaDeviceReset after that call is not supported).  Chain ids
+ * that do not run 0..n_chains-1 as described return GCR_ERR_BAD_ARG.  Calls
+ * that overlap on the GPU race on the shared scratch.  The call waits for
+ * `cuda_stream` before it returns; out = [P, S, director] (host). */
 #define GCR_NOALLOC_MAX_CHAINS 262144
 GCR_API int gcr_order_params_noalloc(int32_t dim, int32_t precision, const void *tangent,
                                      const int32_t *chain_id, int64_t n_beads, int64_t n_chains,

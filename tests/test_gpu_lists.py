@@ -99,7 +99,8 @@ def test_skin_does_not_change_the_trajectory(precision):
     out = {}
     for skin in (0.0, 0.3, 0.8):
         b = Batch([_config1_spec(skin)], precision=precision)
-        # two calls: a run start forces a build, which must not matter either
+        # two calls: the second starts from the lists the first left, which
+        # must not matter either
         b.begin(120)
         b.run(120)
         b.begin(80)

@@ -63,6 +63,42 @@ def test_served_in_a_mix_equals_alone():
             assert np.allclose(r.series[-1, 1:], op, rtol=0, atol=1e-12)
 
 
+def test_corrupt_requests_leave_the_mix_untouched():
+    """Requests with zero beads, negative steps, chain ids out of order or a
+    NaN position arrive while three valid ones are resident: each is
+    rejected with its reason, and the valid ones end bit for bit where they
+    end alone."""
+    specs = _relaxed(3)
+    steps = [400, 300, 350]
+    good = [S.Request(i, copy.deepcopy(sp), steps[i], 0.0, 0, relax=False) for i, sp in enumerate(specs)]
+    bad = []
+    for k, fault in enumerate(["zero_beads", "negative_steps", "chain_order", "nan_pos"]):
+        sp = copy.deepcopy(specs[k % 3])
+        n_steps = 50
+        if fault == "zero_beads":
+            sp.pos, sp.tangent, sp.chain_id = sp.pos[:0], sp.tangent[:0], sp.chain_id[:0]
+        elif fault == "negative_steps":
+            n_steps = -1
+        elif fault == "chain_order":
+            sp.chain_id = sp.chain_id[::-1].copy()
+        else:
+            sp.pos = sp.pos.copy()
+            sp.pos[0, 0] = np.nan
+        # they arrive once the valid requests are on the device
+        bad.append(S.Request(10 + k, sp, n_steps, 0.02 * (k + 1), 0, relax=False))
+    srv = S.Server(2, "mixed", hbm_budget=1 << 30, chunk=25)
+    res = {r.id: r for r in srv.serve(good + bad, timeout=300)}
+    rejected = dict(srv.rejected)
+    srv.close()
+    assert sorted(res) == [0, 1, 2]
+    assert sorted(rejected) == [10, 11, 12, 13]
+    for i, sp in enumerate(specs):
+        r = res[i]
+        assert r.flags == 0 and r.steps == steps[i]
+        pos, _ = _alone(sp, steps[i])
+        assert np.array_equal(r.pos, pos), i
+
+
 def test_fresh_requests_relax_then_run():
     tr = W.serve_trace(3, rate=1000.0, max_beads=4000, min_steps=50, max_steps=120, seed=3)
     reqs = [S.request_from_trace(e, relax=True, obs_every=25) for e in tr]

@@ -86,6 +86,9 @@ class FakeEngine:
         return {"dt": v["dt"], "dt_used": v["dt"], "max_forces_strength": 0.0, "steps_done": v["done"],
                 "step": v["step"], "flags": v["flags"], "active": False, "series_rows": v.get("rows", 0)}
 
+    def statuses(self, slots):
+        return [self.status(s) for s in slots]
+
     def order_params(self, slot):
         return np.array([self.sys[slot]["step"] * 1e-3, 0.5, 0.25])
 
@@ -193,3 +196,57 @@ def test_request_from_trace_shapes():
     for e, r in zip(tr, reqs):
         assert r.spec.n == e["n_chains"] * e["chain_length"] and r.steps == e["steps"]
         assert r.arrival == e["arrival"] and r.spec.params.seed == e["seed"]
+
+
+def _corrupt_requests(first_id, arrival):
+    """Requests the server must refuse, one fault each."""
+    bad = []
+    for k, fault in enumerate(["zero_beads", "negative_steps", "zero_steps", "chain_order", "chain_gap", "nan_pos",
+                               "dim3", "huge"]):
+        spec = W.make_system(f"bad{k}", 2, 20, 10, 40.0, seed=100 + k)
+        steps = 50
+        if fault == "zero_beads":
+            spec.pos, spec.tangent, spec.chain_id = spec.pos[:0], spec.tangent[:0], spec.chain_id[:0]
+        elif fault == "negative_steps":
+            steps = -5
+        elif fault == "zero_steps":
+            steps = 0
+        elif fault == "chain_order":
+            spec.chain_id = spec.chain_id[::-1].copy()
+        elif fault == "chain_gap":
+            spec.chain_id = np.where(spec.chain_id >= 5, spec.chain_id + 1, spec.chain_id)
+        elif fault == "nan_pos":
+            spec.pos = spec.pos.copy()
+            spec.pos[3, 1] = np.nan
+        elif fault == "dim3":
+            spec = W.make_system(f"bad{k}", 3, 20, 10, 40.0, seed=100 + k)
+        elif fault == "huge":
+            spec = W.make_system(f"bad{k}", 2, 2000, 10, 400.0, seed=100 + k)
+        bad.append((fault, S.Request(first_id + k, spec, steps, arrival, 0, False, True)))
+    return bad
+
+
+def test_corrupt_requests_are_rejected_and_the_rest_run():
+    srv = FakeServer(hbm_budget=1 << 20, chunk=40)
+    srv.bead_capacity = 5000
+    srv.engine = srv._make_engine()
+    good = _requests(3, [120, 80, 100])
+    bad = _corrupt_requests(10, arrival=0.0)
+    res = srv.serve(good + [r for _, r in bad], timeout=30)
+    assert sorted(r.id for r in res) == [0, 1, 2]
+    assert all(r.steps == q.steps and r.flags == 0 for r, q in zip(sorted(res, key=lambda r: r.id), good))
+    rejected = dict(srv.rejected)
+    assert sorted(rejected) == [r.id for _, r in bad]
+    reasons = {fault: rejected[r.id] for fault, r in bad}
+    assert "n >= 1" in reasons["zero_beads"]
+    assert "positive integer" in reasons["negative_steps"] and "positive integer" in reasons["zero_steps"]
+    assert "chain ids" in reasons["chain_order"] and "chain ids" in reasons["chain_gap"]
+    assert "non-finite" in reasons["nan_pos"]
+    assert "dimension" in reasons["dim3"]
+    assert "exceed" in reasons["huge"]
+
+
+def test_check_request_accepts_the_trace():
+    tr = W.serve_trace(5, max_beads=5000)
+    for e in tr:
+        assert S.check_request(S.request_from_trace(e), 2, 10_000) is None
