@@ -7,7 +7,7 @@ the continuous-batching request loop on top of it.
 """
 from . import _lib  # noqa: F401
 
-__all__ = ["engine", "updates", "populations", "config", "defaults"]
+__all__ = ["engine", "updates", "config", "defaults", "batch", "serve"]
 __version__ = "0.1.0"
 
 

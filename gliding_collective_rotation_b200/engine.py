@@ -20,6 +20,17 @@ from ._lib import Call, Config, GcrError, Status, SystemBuffers, SystemDesc, che
 PRECISIONS = {"fp64": _lib.GCR_FP64, "mixed": _lib.GCR_MIXED}
 
 
+def wca_params(radius, epsilon, shift, cutoff_factor):
+    """The packed pair parameters the step reads, in the reference's layout
+    (the array populations.make_WCA_params returns, populations.py:48-58):
+    [12 eps r^6, 12 eps r^12, shift, cutoff], the cutoff being
+    cutoff_factor * r - shift, for the rule coeff = ds^-4 (p0 - p1 ds^-3)
+    of forces.WCA."""
+    r6 = float(radius) ** 6
+    p0 = 12.0 * r6 * float(epsilon)
+    return np.array([p0, p0 * r6, float(shift), float(cutoff_factor) * float(radius) - float(shift)])
+
+
 def default_skin(r_cut):
     """Verlet skin for a pair cutoff: 0.2 r_cut + 0.1, within [0.2, 1].  A
     wider skin means rarer list builds but longer lists; measured on B200 the
@@ -308,12 +319,24 @@ class Engine:
         check(self.lib.gcr_count_active(self._ctx, C.byref(n)))
         return n.value
 
-    def status(self, slot):
-        s = Status()
-        check(self.lib.gcr_get_status(self._ctx, int(slot), C.byref(s)))
+    @staticmethod
+    def _status_dict(s):
         return {"dt": s.dt, "dt_used": s.dt_used, "max_forces_strength": s.max_forces_strength,
                 "steps_done": s.steps_done, "step": s.step, "flags": s.flags, "active": bool(s.active),
                 "list_builds": s.list_builds, "series_rows": s.series_rows}
+
+    def status(self, slot):
+        s = Status()
+        check(self.lib.gcr_get_status(self._ctx, int(slot), C.byref(s)))
+        return self._status_dict(s)
+
+    def statuses(self, slots):
+        """The statuses of many systems with one copy of the state table."""
+        n = len(slots)
+        out = (Status * max(n, 1))()
+        arr = (C.c_int32 * max(n, 1))(*[int(s) for s in slots])
+        check(self.lib.gcr_get_statuses(self._ctx, n, arr, out))
+        return [self._status_dict(out[i]) for i in range(n)]
 
     # -- observables and exports --------------------------------------------
     def order_params(self, slot):

@@ -17,7 +17,8 @@ reference's:
   - progress < 1: full radius, kappa = 10, projection factor
     max(0.025, the population's own factor);
   - rest lengths a * a_init_factor ** (1 - progress ** 0.1);
-  - WCA parameters from make_WCA_params at the current radius, with the
+  - WCA parameters packed at the current radius (``engine.wca_params``,
+    the layout of the reference's make_WCA_params), with the
     pair cutoff at the potential minimum while growing
     (updates.interpop_forces, updates.py:304-310);
 * once t > 0, ``end_init_grow`` (populations.py:137-140, 238-240, 297-299,
@@ -39,7 +40,7 @@ import numpy as np
 import torch
 
 from .batch import Batch
-from .populations import make_WCA_params
+from .engine import wca_params
 
 
 @dataclass
@@ -67,7 +68,7 @@ class GrowthConstants:
     def from_spec(cls, spec, WCA_epsilon=None, LJ_cutoff_factor=None):
         """Read the constants off a spec's packed parameters; give
         ``WCA_epsilon`` and ``LJ_cutoff_factor`` to avoid the round trip
-        through make_WCA_params."""
+        through ``wca_params``."""
         p = spec.params
         r = float(p.radius)
         shift = float(p.wca_params[2])
@@ -111,7 +112,7 @@ def grow_params(base, c, t, t_start, settings):
             rigid = 0.0
             kappa = float(base.spring_params[1])
             k = float(base.spring_params[0])
-    wca = make_WCA_params(radius, c.WCA_epsilon, 0.0, c.LJ_cutoff_factor)
+    wca = wca_params(radius, c.WCA_epsilon, 0.0, c.LJ_cutoff_factor)
     if wca[0] != 0:
         # repulsive only while growing: cutoff at the potential minimum
         wca[3] = (wca[1] / wca[0]) ** (1 / 6)

@@ -14,8 +14,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from .engine import SystemParams
-from .populations import make_WCA_params
+from .engine import SystemParams, wca_params
 
 LJ_CUTOFF = 2.5 / 2 ** (1 / 6)  # 2.5 sigma in units of r_WCA = 2^(1/6) sigma
 
@@ -72,7 +71,7 @@ def make_system(name, dim, n_chains, chain_length, L, seed, *, a=0.5, k=100.0, k
     if Dr is None:
         Dr = 3 * D / (4 * radius ** 2)
     get_orient = tangent_locked and chain_length > 1
-    wca = make_WCA_params(radius, eps, 0.0, cutoff)
+    wca = wca_params(radius, eps, 0.0, cutoff)
     params = SystemParams(
         L=L, spring_params=np.array([k, kappa, 0.0, 0.0, float(get_orient), 0.1]), wca_params=wca,
         active_params=np.array([v0, 0.0, v_tan_angle]), D=D, Dr=Dr, radius=radius, n_nearby=4,
@@ -140,7 +139,7 @@ def populations(n_boxes=128, seed=0):
         ang = rs.uniform(0.0, 2 * math.pi, size=nb)
         tan = np.stack([np.cos(ang), np.sin(ang)], axis=1)
         r = 0.7
-        wca = make_WCA_params(r, 1.0, 0.0, 1.0)
+        wca = wca_params(r, 1.0, 0.0, 1.0)
         D = 0.01 / r
         params = SystemParams(
             L=L, spring_params=np.array([100.0, 20.0, 0.0, 0.0, 0.0, 0.1]), wca_params=wca,

@@ -26,7 +26,7 @@ pytestmark = pytest.mark.gpu
 
 from gliding_collective_rotation_b200.batch import Batch  # noqa: E402
 from gliding_collective_rotation_b200.engine import SystemParams  # noqa: E402
-from gliding_collective_rotation_b200.populations import make_WCA_params  # noqa: E402
+from gliding_collective_rotation_b200.engine import wca_params as make_WCA_params  # noqa: E402
 from gliding_collective_rotation_b200.workloads import SystemSpec  # noqa: E402
 from oracle import oracle as O  # noqa: E402
 from tests.golden_io import min_image  # noqa: E402

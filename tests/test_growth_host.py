@@ -8,7 +8,7 @@ import pytest
 
 from gliding_collective_rotation_b200.engine import SystemParams
 from gliding_collective_rotation_b200.growth import GrowSettings, GrowthConstants, grow_params
-from gliding_collective_rotation_b200.populations import make_WCA_params
+from gliding_collective_rotation_b200.engine import wca_params as make_WCA_params
 from tests.golden_io import GOLDEN, status_dict
 
 

@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from gliding_collective_rotation_b200 import updates
-from gliding_collective_rotation_b200.populations import make_WCA_params
+from gliding_collective_rotation_b200.engine import wca_params as make_WCA_params
 
 
 def _pop(name, wca, growing=False, special=None, extra=()):
