@@ -202,6 +202,8 @@ def SRK2_force_calc(pops, status, sim):
         fr, fm = _pair_rule_check
         if fr.central_pair_force_rule is not fm.WCA:
             raise NotImplementedError("the GPU step implements the forces.WCA pair rule")
+    if not torch.cuda.is_available():
+        raise GcrError(-2, "no CUDA device: the gcr hot path runs on the GPU only")
     if len(pops) > 1:
         return _srk2_populations(pops, status, sim, srk_order)
     pop = pops[0]
