@@ -10,7 +10,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libgcr.so")
+# the in-tree build; GCR_LIBRARY names another build of the same sources (a
+# different revision to compare against, say)
+LIB_PATH = os.environ.get("GCR_LIBRARY") or os.path.join(HERE, "libgcr.so")
 
 GCR_OK = 0
 ERRORS = {-1: "BAD_ARG", -2: "CUDA", -3: "OOM", -4: "NONFINITE", -5: "TIMEOUT", -6: "CAPACITY",
@@ -30,7 +32,8 @@ class Config(C.Structure):
     _fields_ = [("dim", C.c_int32), ("precision", C.c_int32), ("bead_capacity", C.c_int64),
                 ("system_capacity", C.c_int32), ("cell_capacity", C.c_int64), ("cell_depth", C.c_int32),
                 ("block_beads", C.c_int32), ("block_cells", C.c_int32), ("steps_per_graph", C.c_int32),
-                ("ctas_per_sm", C.c_int32), ("list_depth", C.c_int32), ("srk_order", C.c_int32)]
+                ("ctas_per_sm", C.c_int32), ("list_depth", C.c_int32), ("srk_order", C.c_int32),
+                ("fuse_pair", C.c_int32)]
 
 
 class SystemDesc(C.Structure):

@@ -42,6 +42,12 @@ struct BatchArgs {
     // periodic images crossed by each bead since admission, int32 [bead][dim]
     // (the real updates count them; unwrapped = pos + L * img)
     int *img;
+    // rest length of each bead's chain in the bonded arithmetic's type BT
+    // [bead] (8 bytes a bead allocated, enough for either type):
+    // rest_lengths[chain_id[b]], written for every armed system at the start
+    // of each run (the host may change rest lengths between calls), so that
+    // the stage kernels stage it with the positions
+    void *restb;
 };
 
 struct KernelSet {
@@ -54,6 +60,8 @@ struct KernelSet {
     void *pair1;
     void *stage0;
     void *stage1;
+    void *stage0f;  // stages 0 and 1 that sum the pair forces themselves (no k_pair launch)
+    void *stage1f;
     void *update;
     void *rigid0;   // rigid-rod projection: predictor (pos -> pos1) and corrector (pos1 -> pos)
     void *rigid1;
@@ -70,7 +78,9 @@ struct KernelSet {
     void *run_check;  // run start: flag the armed systems whose lists no longer cover their positions
     void *lists_plan;  // compact the systems that take part in a list build
     void *pair_cross[3];  // pair forces at pos / pos1 / pos2 with the other populations' (coupled systems)
-    size_t (*stage_smem)(int block_beads);  // dynamic shared memory of the stage kernels
+    size_t (*stage_smem)(int block_beads);   // dynamic shared memory of the stage kernels
+    size_t (*update_smem)(int block_beads);  // dynamic shared memory of the update kernel
+    size_t (*pair_smem)(int block_beads);    // dynamic shared memory of the pair kernels
 };
 
 KernelSet kernel_set(int dim, int precision);

@@ -86,6 +86,9 @@ typedef struct {
     int32_t ctas_per_sm;      /* persistent CTAs per SM (0 = from occupancy, <0 = one CTA per tile) */
     int32_t list_depth;       /* neighbour-list slots per bead, 4..1024 (0 = 32 in 2D, 96 in 3D) */
     int32_t srk_order;        /* config.SRK_order: 2 (0 = 2) or 4 (SRK.py:144-215, 296-321) */
+    int32_t fuse_pair;        /* 1: the stage kernels sum the pair forces themselves instead of a
+                                 separate pair launch per stage (SRK2 while no system is coupled to
+                                 another population; same results bit for bit); 0: separate */
 } gcr_config;
 
 /* One system.  The packed arrays follow the reference's packing exactly. */

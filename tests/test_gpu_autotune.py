@@ -34,14 +34,18 @@ def test_tune_measures_and_caches(tmp_path, monkeypatch):
     assert again == res
 
 
-def test_every_shape_gives_the_same_trajectory():
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_every_shape_gives_the_same_trajectory(precision):
+    """Tile size, persistent grid, graph length, skin and whether the stage
+    kernels sum the pair forces themselves change no bit of a trajectory."""
     specs = _specs(4)
     out = []
-    for res in ({"block_beads": 128, "ctas_per_sm": 0, "steps_per_graph": 10, "skin_scale": 1.0},
-                {"block_beads": 64, "ctas_per_sm": 2, "steps_per_graph": 5, "skin_scale": 1.5},
-                {"block_beads": 256, "ctas_per_sm": 4, "steps_per_graph": 20, "skin_scale": 0.67}):
+    for res in ({"block_beads": 128, "ctas_per_sm": 0, "steps_per_graph": 10, "skin_scale": 1.0, "fuse_pair": 0},
+                {"block_beads": 64, "ctas_per_sm": 2, "steps_per_graph": 5, "skin_scale": 1.5, "fuse_pair": 1},
+                {"block_beads": 256, "ctas_per_sm": 4, "steps_per_graph": 20, "skin_scale": 0.67, "fuse_pair": 0},
+                {"block_beads": 128, "ctas_per_sm": 0, "steps_per_graph": 10, "skin_scale": 1.0, "fuse_pair": 1}):
         sp, kw = autotune.apply(specs, res)
-        b = Batch(sp, precision="fp64", **kw)
+        b = Batch(sp, precision=precision, **kw)
         b.set_adaptive(True)
         b.begin(60)
         b.run(60)

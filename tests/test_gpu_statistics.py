@@ -113,7 +113,7 @@ def test_long_run_statistics_match_the_oracle():
 # the config-2 and config-5 physics, and the mixed path
 # ---------------------------------------------------------------------------
 #
-# Twelve independent Philox seeds on each side from the reference's relaxed
+# 24 independent Philox seeds on each side from the reference's relaxed
 # state of each fixture, run to the same physical time T in 20 chunks of
 # T/20 (the call's time limit, max_dt_usable, as the reference's save times
 # cut its calls, SRK.py:128-130), the GPU in the given precision, the oracle
@@ -131,7 +131,7 @@ def test_long_run_statistics_match_the_oracle():
 # by a chi-square over its bins (sum of squared z-scores below the 99.9%
 # point of chi2 with as many degrees of freedom as bins).
 
-N_SEEDS = 12
+N_SEEDS = 24
 GR_EDGES = np.linspace(0.0, 3.0, 16)
 STAT_CASES = {  # fixture: (physical time, chunks)
     "chiral_lj": (1.0, 20),
@@ -210,7 +210,9 @@ def _stats_gpu(name, precision):
                            rk_cheat=s["rk_cheat"], seed=2000 + k)
         specs.append(W.SystemSpec(f"{name}_{k}", dim, d["pos0"], d["tangent0"], d["chain_id"], d["rest_lengths"],
                                   prm, s["dtmax"], mdps))
-    b = Batch(specs, precision=precision)
+    # lists deep enough for the LJ clusters (calls are armed directly here,
+    # without the regrow that Batch.run_checked does after an overflow)
+    b = Batch(specs, precision=precision, list_depth=256, cell_depth=64)
     chain = np.asarray(d["chain_id"])
     cs = _chain_starts(chain)
     pos0 = [st.pos.cpu().numpy().copy() for st in b.states]

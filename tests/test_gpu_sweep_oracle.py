@@ -73,6 +73,7 @@ def test_sweep_systems_match_the_oracle():
         oracles.append(o)
     until = [N_UPDATE] * len(sel)
     done = 0
+    report, bad = [], []
     for n_steps, tol in ((1, 1e-12), (9, 1e-11), (40, 1e-10), (150, 1e-9)):
         b.begin(n_steps)
         b.run(n_steps)
@@ -83,10 +84,16 @@ def test_sweep_systems_match_the_oracle():
             res = o.run(n_steps, dt=dts[j], dtmax=sp.dt, max_dist_per_step=sp.relax_mdps,
                         noise_mode=O.NOISE_PHILOX, seed=p.seed, step0=step0[j] + done, steps_until_update=until[j])
             assert res["steps"] == n_steps
-            assert abs(res["dt"] - sts[j]["dt"]) <= 1e-9 * res["dt"], (sp.name, res["dt"], sts[j]["dt"])
+            # the dt rule on the same forces: equal to rounding after the first
+            # step; later the trajectories' own (tiny) differences feed it
+            dt_tol = 1e-12 if done == 0 else 1e-6
+            dt_err = abs(res["dt"] - sts[j]["dt"]) / res["dt"]
             dts[j] = res["dt"]
             until[j] = _countdown(until[j], n_steps)
             err = np.max(np.abs(min_image(st.pos.cpu().numpy() - o.pos, p.L))) / p.L
-            assert err < tol, (sp.name, sp.n, done + n_steps, err)
+            report.append((sp.name, sp.n, done + n_steps, err, dt_err))
+            if err >= tol or dt_err > dt_tol:
+                bad.append(report[-1])
         done += n_steps
     b.close()
+    assert not bad, (bad, report)
