@@ -133,15 +133,12 @@ struct gcr_ctx {
     int *ncount = nullptr;
     double *xref = nullptr;
     int *img = nullptr;  // periodic images crossed per bead and axis since admission
-    void *restb = nullptr;  // rest length of each bead's chain (refreshed at every run start)
     int *work = nullptr;
     void *xi = nullptr;
     void *fp = nullptr;
     double *pos2 = nullptr;  // SRK4 scratch: second virtual update
     void *faux = nullptr;    // SRK4 scratch: stage forces of systems without a caller buffer
     size_t stage_smem = 0;
-    size_t update_smem = 0;
-    size_t pair_smem = 0;
     int32_t *chain_starts = nullptr;
     int *d_err = nullptr;
     double *d_out = nullptr;
@@ -496,31 +493,32 @@ int enqueue_step4(gcr_ctx *c)
         if ((rc = enqueue_lists(c, reads[k]))) return rc;
         void *pair = c->graph_cross ? c->ks.pair_cross[reads[k]]
                                     : (reads[k] == 0 ? c->ks.pair0 : (reads[k] == 1 ? c->ks.pair1 : c->ks.pair2));
-        if ((rc = launch(c, pair, c->grid_pair, bb, c->pair_smem))) return rc;
+        if ((rc = launch(c, pair, c->grid_pair, bb))) return rc;
         if ((rc = launch(c, c->ks.stage4[k], c->grid_stage4[k], bb, c->stage_smem))) return rc;
         if (k < 3 && c->graph_rigid && (rc = launch(c, c->ks.rigid4[k], c->grid_update, bb))) return rc;
     }
     if ((rc = launch_sys(c, c->ks.sys_dt))) return rc;
-    if ((rc = launch(c, c->ks.update, c->grid_update, bb, c->update_smem))) return rc;
+    if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
     if (c->graph_rigid && (rc = launch(c, c->ks.rigid4[3], c->grid_update, bb))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_end))) return rc;
     return c->graph_obs ? launch_observe(c) : GCR_OK;
 }
 
-// the stage kernels sum the pair forces themselves (SRK2, no coupled system)
-bool fused_pair(const gcr_ctx *c) { return c->cfg.fuse_pair && c->cfg.srk_order == 2 && !c->graph_cross; }
+// the SRK2 stage kernels sum the pair forces themselves (gcr_config.fuse_pair;
+// not with coupled populations, whose cross forces only k_pair adds)
+bool fused_pair(const gcr_ctx *c, bool cross) { return c->cfg.fuse_pair && c->cfg.srk_order == 2 && !cross; }
 
 // SRK2 stage s (0 predictor, 1 corrector): the pair forces, then the stage
-int enqueue_pair(gcr_ctx *c, int s)
+int enqueue_pair(gcr_ctx *c, int s, bool cross)
 {
-    if (fused_pair(c)) return GCR_OK;
-    void *pair = c->graph_cross ? c->ks.pair_cross[s] : (s == 0 ? c->ks.pair0 : c->ks.pair1);
-    return launch(c, pair, c->grid_pair, c->cfg.block_beads, c->pair_smem);
+    if (fused_pair(c, cross)) return GCR_OK;
+    void *pair = cross ? c->ks.pair_cross[s] : (s == 0 ? c->ks.pair0 : c->ks.pair1);
+    return launch(c, pair, c->grid_pair, c->cfg.block_beads);
 }
 
-int enqueue_stage(gcr_ctx *c, int s)
+int enqueue_stage(gcr_ctx *c, int s, bool cross)
 {
-    const bool f = fused_pair(c);
+    const bool f = fused_pair(c, cross);
     void *stage = s == 0 ? (f ? c->ks.stage0f : c->ks.stage0) : (f ? c->ks.stage1f : c->ks.stage1);
     const int grid = s == 0 ? (f ? c->grid_stage0f : c->grid_stage0) : (f ? c->grid_stage1f : c->grid_stage1);
     return launch(c, stage, grid, c->cfg.block_beads, c->stage_smem);
@@ -532,14 +530,14 @@ int enqueue_step(gcr_ctx *c)
     const int bb = c->cfg.block_beads;
     if (c->cfg.srk_order == 4) return enqueue_step4(c);
     if ((rc = enqueue_lists(c, 0))) return rc;
-    if ((rc = enqueue_pair(c, 0))) return rc;
-    if ((rc = enqueue_stage(c, 0))) return rc;
+    if ((rc = enqueue_pair(c, 0, c->graph_cross))) return rc;
+    if ((rc = enqueue_stage(c, 0, c->graph_cross))) return rc;
     if (c->graph_rigid && (rc = launch(c, c->ks.rigid0, c->grid_update, bb))) return rc;
     if ((rc = enqueue_lists(c, 1))) return rc;
-    if ((rc = enqueue_pair(c, 1))) return rc;
-    if ((rc = enqueue_stage(c, 1))) return rc;
+    if ((rc = enqueue_pair(c, 1, c->graph_cross))) return rc;
+    if ((rc = enqueue_stage(c, 1, c->graph_cross))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_dt))) return rc;
-    if ((rc = launch(c, c->ks.update, c->grid_update, bb, c->update_smem))) return rc;
+    if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
     if (c->graph_rigid && (rc = launch(c, c->ks.rigid1, c->grid_update, bb))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_end))) return rc;
     return c->graph_obs ? launch_observe(c) : GCR_OK;
@@ -626,7 +624,7 @@ int gcr_footprint(const gcr_config *cfg, const gcr_system_desc *desc, int64_t *c
     const int64_t ft = cfg->precision == GCR_FP64 ? 8 : 4;
     const int64_t ld = cfg->list_depth > 0 ? cfg->list_depth : (cfg->dim == 2 ? 32 : 96);
     int64_t bytes = n * d * (8 + 8 + ft + ft) + n * 4 + desc->n_chains * 8     // caller-owned state
-                    + n * (1 + 2 * d * ft + 8) + 4 * (desc->n_chains + 1)      // topo, fp, xi, rest, chain starts
+                    + n * (1 + 2 * d * ft) + 4 * (desc->n_chains + 1)          // topo, fp, xi, chain starts
                     + n * (4 * ld + 4 + 8 * d)                                 // neighbour list, xref
                     + cells * (8 + (int64_t)cfg->cell_depth * 4)               // counts, slots
                     + (cfg->srk_order == 4 ? n * d * (8 + ft) : 0);            // SRK4: pos2, stage forces
@@ -695,7 +693,6 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     e = e ? e : cudaMalloc(&c->ncount, sizeof(int) * (size_t)cfg.bead_capacity);
     e = e ? e : cudaMalloc(&c->xref, sizeof(double) * (size_t)cfg.bead_capacity * cfg.dim);
     e = e ? e : cudaMalloc(&c->img, sizeof(int) * (size_t)cfg.bead_capacity * cfg.dim);
-    e = e ? e : cudaMalloc(&c->restb, sizeof(double) * (size_t)cfg.bead_capacity);
     e = e ? e : cudaMalloc(&c->work, sizeof(int) * (size_t)(3 + 3 * (S + 1)));
     e = e ? e : cudaMalloc(&c->xi, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
     e = e ? e : cudaMalloc(&c->fp, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
@@ -739,7 +736,6 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     a.img = c->img;
     a.xi = c->xi;
     a.fp = c->fp;
-    a.restb = c->restb;
     a.work = c->work;
     a.n_slots = (int)S;
     a.list_stride = cfg.bead_capacity;
@@ -764,12 +760,8 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     c->grid_stage1 = kernel_grid(c, c->ks.stage1, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
     c->grid_stage0f = kernel_grid(c, c->ks.stage0f, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
     c->grid_stage1f = kernel_grid(c, c->ks.stage1f, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
-    c->update_smem = c->ks.update_smem(cfg.block_beads);
-    if (c->update_smem > 48 * 1024)
-        cudaFuncSetAttribute(c->ks.update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->update_smem);
-    c->grid_update = kernel_grid(c, c->ks.update, cfg.block_beads, c->max_bead_tiles, c->update_smem);
-    c->pair_smem = c->ks.pair_smem(cfg.block_beads);
-    c->grid_pair = kernel_grid(c, c->ks.pair0, cfg.block_beads, c->max_bead_tiles, c->pair_smem);
+    c->grid_update = kernel_grid(c, c->ks.update, cfg.block_beads, c->max_bead_tiles);
+    c->grid_pair = kernel_grid(c, c->ks.pair0, cfg.block_beads, c->max_bead_tiles);
     c->grid_bin = kernel_grid(c, c->ks.bin0, cfg.block_beads, c->max_bead_tiles);
     c->grid_sort = kernel_grid(c, c->ks.sort, cfg.block_cells, c->max_cell_tiles);
     c->grid_build = kernel_grid(c, c->ks.build0, cfg.block_beads, c->max_bead_tiles);
@@ -786,7 +778,7 @@ int gcr_destroy(gcr_ctx *c)
     if (c->graph) cudaGraphExecDestroy(c->graph);
     void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->topo, c->cnt, c->ncell,
                     c->items, c->nbr, c->ncount, c->xref, c->work, c->xi, c->fp, c->chain_starts, c->d_err,
-                    c->d_out, c->pos2, c->faux, c->xnbr, c->xcount, c->img, c->restb};
+                    c->d_out, c->pos2, c->faux, c->xnbr, c->xcount, c->img};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -1182,32 +1174,24 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
     for (auto &e : ev) GCR_CUDA(cudaEventCreate(&e));
     const int bb = c->cfg.block_beads;
     const bool rigid = any_rigid(c), cross = any_cross(c);
-    // with fused stages the pair groups are empty and the stages carry them
-    const bool fused = c->cfg.fuse_pair && !cross;
     for (int s = 0; s < n_steps && rc == GCR_OK; s++) {
         cudaEvent_t *e = ev.data() + (size_t)s * (G + 1);
         GCR_CUDA(cudaEventRecord(e[0], c->stream));
         rc = enqueue_lists(c, 0);
         GCR_CUDA(cudaEventRecord(e[1], c->stream));
-        if (!rc && !fused)
-            rc = launch(c, cross ? c->ks.pair_cross[0] : c->ks.pair0, c->grid_pair, bb, c->pair_smem);
+        if (!rc) rc = enqueue_pair(c, 0, cross);  // nothing with fused stages
         GCR_CUDA(cudaEventRecord(e[2], c->stream));
-        if (!rc)
-            rc = launch(c, fused ? c->ks.stage0f : c->ks.stage0, fused ? c->grid_stage0f : c->grid_stage0, bb,
-                        c->stage_smem);
+        if (!rc) rc = enqueue_stage(c, 0, cross);
         if (!rc && rigid) rc = launch(c, c->ks.rigid0, c->grid_update, bb);
         GCR_CUDA(cudaEventRecord(e[3], c->stream));
         if (!rc) rc = enqueue_lists(c, 1);
         GCR_CUDA(cudaEventRecord(e[4], c->stream));
-        if (!rc && !fused)
-            rc = launch(c, cross ? c->ks.pair_cross[1] : c->ks.pair1, c->grid_pair, bb, c->pair_smem);
+        if (!rc) rc = enqueue_pair(c, 1, cross);
         GCR_CUDA(cudaEventRecord(e[5], c->stream));
-        if (!rc)
-            rc = launch(c, fused ? c->ks.stage1f : c->ks.stage1, fused ? c->grid_stage1f : c->grid_stage1, bb,
-                        c->stage_smem);
+        if (!rc) rc = enqueue_stage(c, 1, cross);
         if (!rc) rc = launch_sys(c, c->ks.sys_dt);
         GCR_CUDA(cudaEventRecord(e[6], c->stream));
-        if (!rc) rc = launch(c, c->ks.update, c->grid_update, bb, c->update_smem);
+        if (!rc) rc = launch(c, c->ks.update, c->grid_update, bb);
         if (!rc && rigid) rc = launch(c, c->ks.rigid1, c->grid_update, bb);
         if (!rc) rc = launch_sys(c, c->ks.sys_end);
         GCR_CUDA(cudaEventRecord(e[7], c->stream));

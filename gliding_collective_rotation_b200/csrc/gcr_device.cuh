@@ -271,27 +271,6 @@ __device__ __forceinline__ int image_step(double x_old, double x_new, double hal
 // read of a word that other CTAs may change during the kernel
 __device__ __forceinline__ int ld_volatile(const int *p) { return *(const volatile int *)p; }
 
-// Asynchronous copy of one 4- or 8-byte element from global to shared memory
-// (cp.async): both addresses aligned to the element.  A thread's copies are
-// grouped by cp_async_commit, waited for by cp_async_wait<N> (all but the N
-// most recent groups complete), and made visible to the CTA by the barrier
-// that follows the wait.
-template <int BYTES>
-__device__ __forceinline__ void cp_async(void *smem, const void *gmem)
-{
-    static_assert(BYTES == 4 || BYTES == 8, "4- or 8-byte elements");
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(s), "l"(gmem), "n"(BYTES) : "memory");
-}
-
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-
-template <int N>
-__device__ __forceinline__ void cp_async_wait()
-{
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
 // GPU cell coordinate of a position (clamped; non-finite -> 0)
 __device__ __forceinline__ int cell_coord(double x, double inv_h, int nc)
 {

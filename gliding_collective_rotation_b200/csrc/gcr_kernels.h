@@ -42,12 +42,6 @@ struct BatchArgs {
     // periodic images crossed by each bead since admission, int32 [bead][dim]
     // (the real updates count them; unwrapped = pos + L * img)
     int *img;
-    // rest length of each bead's chain in the bonded arithmetic's type BT
-    // [bead] (8 bytes a bead allocated, enough for either type):
-    // rest_lengths[chain_id[b]], written for every armed system at the start
-    // of each run (the host may change rest lengths between calls), so that
-    // the stage kernels stage it with the positions
-    void *restb;
 };
 
 struct KernelSet {
@@ -78,9 +72,7 @@ struct KernelSet {
     void *run_check;  // run start: flag the armed systems whose lists no longer cover their positions
     void *lists_plan;  // compact the systems that take part in a list build
     void *pair_cross[3];  // pair forces at pos / pos1 / pos2 with the other populations' (coupled systems)
-    size_t (*stage_smem)(int block_beads);   // dynamic shared memory of the stage kernels
-    size_t (*update_smem)(int block_beads);  // dynamic shared memory of the update kernel
-    size_t (*pair_smem)(int block_beads);    // dynamic shared memory of the pair kernels
+    size_t (*stage_smem)(int block_beads);  // dynamic shared memory of the stage kernels
 };
 
 KernelSet kernel_set(int dim, int precision);

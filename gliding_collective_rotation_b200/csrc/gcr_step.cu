@@ -62,76 +62,36 @@ struct Bonded {
     using type = typename std::conditional<GCR_BONDED_FP64 || sizeof(FT) == 8, double, FT>::type;
 };
 
-// list entries a bead's pair walk finds staged in shared memory before its
-// first gather (the pair kernel, and the stage kernels that sum pair forces
-// themselves); at most the smallest list depth (4)
-constexpr int kPairSlots = 4;
-
-// Shared memory of a stage kernel.  The inputs of a tile are double-buffered
-// and staged one tile ahead with cp.async, into the buffer the previous tile
-// no longer reads, so that their latency overlaps the current tile's
-// arithmetic; the per-tile work arrays are single.  Index k <-> bead
-// begin-2+k (a halo of two beads either side), own index j <-> bead begin+j.
 template <int D, typename FT>
 struct StageSmem {
     using BT = typename Bonded<FT>::type;
-    // inputs, buffer 0; buffer 1 lies `step` bytes further (see in())
-    double *x;      // [TB+4][D] positions the stage's forces are taken at
-    int *ch;        // [TB+4]    chain id (-1 outside the system)
-    BT *ra;         // [TB+4]    rest length of the bead's chain
-    double *xr;     // [TB][D]   own position at the last list build (skin test)
-    FT *tin;        // [TB][D]   own tangent
-    FT *pin;        // [TB][D]   own pair force
-    FT *fin;        // [TB][D]   own force so far (SRK2 corrector: F0; SRK4: the weighted sum)
-    int *lc;        // [TB]      own list count (stages that sum the pair forces)
-    int *li;        // [kPairSlots][TB] own first list entries (slot-major)
-    size_t step;    // bytes from buffer 0 to buffer 1
-    BT *bd;         // [TB+3][D] bond vector d_j = min_image(x_j - x_{j+1}), k <-> bond begin-2+k
-    BT *bt;         // [TB+3][D] unit tangent of the bond (d itself when |d| = 0)
-    BT *bf;         // [TB+3]    spring magnitude k (a/|d| - 1), 0 when |d| = 0
-    BT *fw;         // [TB+2][D] bend "forward" term at bead begin-1+k
-    BT *bw;         // [TB+2][D] bend "backward" term
-    // an input array in buffer b
-    template <typename T>
-    __device__ __forceinline__ T *in(T *a, int b) const
+    double *x;     // [TB+4][D] positions, index k <-> bead begin-2+k
+    uint8_t *tp;   // [TB+4]    topology bits
+    BT *bd;        // [TB+3][D] bond vector d_j = min_image(x_j - x_{j+1}), k <-> bond begin-2+k
+    BT *bt;        // [TB+3][D] unit tangent of the bond (d itself when |d| = 0)
+    BT *bf;        // [TB+3]    spring magnitude k (a/|d| - 1), 0 when |d| = 0
+    BT *fw;        // [TB+2][D] bend "forward" term at bead begin-1+k
+    BT *bw;        // [TB+2][D] bend "backward" term
+    BT *ra;        // [TB+4]    rest length of the bead's chain
+    __device__ void carve(unsigned char *base, int TB)
     {
-        return reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(a) + (size_t)b * step);
-    }
-    // lays the arrays out from `base` (16-byte aligned pieces; no pointers
-    // are formed for a null base); returns the bytes used
-    __host__ __device__ size_t carve(unsigned char *base, int TB)
-    {
-        size_t off = 0;
-        auto take = [&](size_t bytes) {
-            unsigned char *r = base ? base + off : nullptr;
-            off += (bytes + 15) / 16 * 16;
-            return r;
-        };
-        x = reinterpret_cast<double *>(take((size_t)(TB + 4) * D * sizeof(double)));
-        xr = reinterpret_cast<double *>(take((size_t)TB * D * sizeof(double)));
-        ch = reinterpret_cast<int *>(take((size_t)(TB + 4) * sizeof(int)));
-        ra = reinterpret_cast<BT *>(take((size_t)(TB + 4) * sizeof(BT)));
-        tin = reinterpret_cast<FT *>(take((size_t)TB * D * sizeof(FT)));
-        pin = reinterpret_cast<FT *>(take((size_t)TB * D * sizeof(FT)));
-        fin = reinterpret_cast<FT *>(take((size_t)TB * D * sizeof(FT)));
-        lc = reinterpret_cast<int *>(take((size_t)TB * sizeof(int)));
-        li = reinterpret_cast<int *>(take((size_t)kPairSlots * TB * sizeof(int)));
-        step = off;
-        take(step);  // buffer 1
-        bd = reinterpret_cast<BT *>(take((size_t)(TB + 3) * D * sizeof(BT)));
-        bt = reinterpret_cast<BT *>(take((size_t)(TB + 3) * D * sizeof(BT)));
-        bf = reinterpret_cast<BT *>(take((size_t)(TB + 3) * sizeof(BT)));
-        fw = reinterpret_cast<BT *>(take((size_t)(TB + 2) * D * sizeof(BT)));
-        bw = reinterpret_cast<BT *>(take((size_t)(TB + 2) * D * sizeof(BT)));
-        return off;
+        x = reinterpret_cast<double *>(base);
+        bd = reinterpret_cast<BT *>(x + (size_t)(TB + 4) * D);
+        bt = bd + (size_t)(TB + 3) * D;
+        bf = bt + (size_t)(TB + 3) * D;
+        fw = bf + (TB + 3);
+        bw = fw + (size_t)(TB + 2) * D;
+        ra = bw + (size_t)(TB + 2) * D;
+        tp = reinterpret_cast<uint8_t *>(ra + (TB + 4));
     }
 };
 
 template <int D, typename FT>
 size_t stage_smem_bytes(int TB)
 {
-    StageSmem<D, FT> sm;
-    return sm.carve(nullptr, TB);
+    using BT = typename Bonded<FT>::type;
+    return (size_t)(TB + 4) * D * sizeof(double) + (size_t)(TB + 3) * (2 * D + 1) * sizeof(BT) +
+           (size_t)(TB + 2) * 2 * D * sizeof(BT) + (size_t)(TB + 4) * sizeof(BT) + (size_t)(TB + 4) + 16;
 }
 
 // 1/sqrt(x): FP64 exactly as written in the reference; FP32 (mixed path) by
@@ -171,7 +131,7 @@ __device__ __forceinline__ bool bend(const FT *ti, const FT *tj, FT theta0, FT k
 }
 
 // CTAs of 512 threads per SM that the bead kernels are compiled for: the 2D
-// mixed-precision kernels fit in 42 registers a thread with 3 (12 CTAs of 128
+// mixed-precision kernels fit in 42 registers a thread with 3 (6 CTAs of 256
 // per SM), 64 with 2; the FP64 and 3D kernels keep the registers they need
 #ifndef GCR_MIXED2D_MIN_BLOCKS
 #define GCR_MIXED2D_MIN_BLOCKS 3
@@ -244,9 +204,9 @@ __device__ __forceinline__ double *stage_x(const SysP &p)
     return WHICH == 0 ? p.pos : (WHICH == 1 ? p.pos1 : p.pos2);
 }
 
-// a system of the build's work list (k_lists_plan listed it) still takes part:
-// a bin that overflowed its cells stops it (a fixed member of coupled
-// populations is binned whenever its group is listed)
+// a system that k_lists_plan listed still takes part in the build (its flags
+// may have turned fatal since; a fixed member of coupled populations is
+// binned whenever it was listed)
 __device__ __forceinline__ bool builds(const SysP &p, const SysS &s)
 {
     return p.calc_wca && (p.fixed || ld_volatile(&s.active)) && !(ld_volatile(&s.flags) & kFlagFatal);
@@ -258,19 +218,6 @@ __device__ __forceinline__ void cell_of(const SysP &p, const double *x, int *ci)
     ci[0] = ci[1] = ci[2] = 0;
 #pragma unroll
     for (int i = 0; i < D; i++) ci[i] = cell_coord(x[i], p.inv_h, p.nc);
-}
-
-// a bead at x is farther than skin/2 from r, where the list was built
-template <int D>
-__device__ __forceinline__ bool left_skin_of(const SysP &p, const double *r, const double *x)
-{
-    double dd = 0.0;
-#pragma unroll
-    for (int i = 0; i < D; i++) {
-        double d = inbounds(x[i], r[i], p.half_L, p.L);
-        dd += d * d;
-    }
-    return !(dd <= p.half_skin2);
 }
 
 // a bead moved farther than skin/2 from where the list was built
@@ -348,8 +295,8 @@ __global__ void __launch_bounds__(1024) k_lists_plan(BatchArgs A)
                 } else {
                     // coupled populations rebuild together: their cross lists
                     // read one another's cells.  Only moving, running members
-                    // ask for a build, and every thread of the group reads
-                    // the same flags (they are cleared after the scan).
+                    // ask for a build (no flag changes during the scan, so
+                    // every thread of the group reaches the same answer).
                     bool any = false;
                     for (int k = 0; k < p.grp_n && k < kMaxPops; k++) {
                         const int m = p.grp[k];
@@ -737,87 +684,24 @@ __device__ __forceinline__ void add_cross(const BatchArgs &A, const SysP &p, int
     }
 }
 
-// pair forces over the neighbour list (forces.py:57-145, rule forces.WCA):
-// min-image separation of the FP64 positions, rounded to FT, then the rule
-// in FT; writes the pair force of every bead to fp[bead]
-// Shared memory of the pair kernel: each thread's own position, list count
-// and first kPairSlots list entries, double-buffered and copied one tile ahead
-// (cp.async), so that a tile's first partner gathers depend on one load only.
-template <int D>
-struct PairSmem {
-    double *x;    // [TB][D] own position
-    int *cnt;     // [TB]    list count
-    int *idx;     // [kPairSlots][TB] first list entries (slot-major)
-    size_t step;  // bytes from buffer 0 to buffer 1
-    template <typename T>
-    __device__ __forceinline__ T *in(T *a, int b) const
-    {
-        return reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(a) + (size_t)b * step);
-    }
-    __host__ __device__ size_t carve(unsigned char *base, int TB)
-    {
-        size_t off = 0;
-        auto take = [&](size_t bytes) {
-            unsigned char *r = base ? base + off : nullptr;
-            off += (bytes + 15) / 16 * 16;
-            return r;
-        };
-        x = reinterpret_cast<double *>(take((size_t)TB * D * sizeof(double)));
-        cnt = reinterpret_cast<int *>(take((size_t)TB * sizeof(int)));
-        idx = reinterpret_cast<int *>(take((size_t)kPairSlots * TB * sizeof(int)));
-        step = off;
-        take(step);
-        return off;
-    }
-};
-
-template <int D>
-size_t pair_smem_bytes(int TB)
-{
-    PairSmem<D> sm;
-    return sm.carve(nullptr, TB);
-}
-
-// issue the copies of each thread's inputs of tile `tl` into buffer `b`
-template <int D, int WHICH>
-__device__ __forceinline__ void pair_prefetch(const BatchArgs &A, PairSmem<D> &sm, const Tile &tl, int b)
-{
-    const SysP &p = A.P[tl.sys];
-    const int j = threadIdx.x, m = tl.begin + j, TB = blockDim.x;
-    if (j >= A.tile_beads || m >= p.n || !p.calc_wca) return;
-    const double *X = stage_x<WHICH>(p);
-    double *x = sm.in(sm.x, b) + j * D;
-#pragma unroll
-    for (int i = 0; i < D; i++) cp_async<8>(x + i, X + (size_t)m * D + i);
-    cp_async<4>(sm.in(sm.cnt, b) + j, A.ncount + p.bead_off + m);
-    // the first slots whatever the count (the list depth is at least
-    // kPairSlots; slots past the count are never read)
-    int *idx = sm.in(sm.idx, b);
-#pragma unroll
-    for (int k = 0; k < kPairSlots; k++)
-        cp_async<4>(idx + k * TB + j, A.nbr + (size_t)k * A.list_stride + p.bead_off + m);
-}
-
-// The pair force on bead b at positions X (its own xb) summed over its
-// neighbour list in list order (ascending id): the min-image separation of
-// the FP64 positions rounded to FT, then the rule forces.WCA in FT
-// (forces.py:57-145, 13-15) for the partners within r_cut.  `cnt` is the
-// list count; `first` holds the first kPairSlots entries (`ts` apart), the
-// others are read from the list.  An entry outside the system sets `bad`
-// and is not used.
+// pair force on bead b over its neighbour list (forces.py:57-145, rule
+// forces.WCA): min-image separation of the FP64 positions X, rounded to FT,
+// then the rule in FT, added to F partner by partner in ascending id.  An
+// entry outside the system sets `bad` and is not used.
 template <int D, typename FT>
-__device__ __forceinline__ void list_pair_force(const BatchArgs &A, const SysP &p, const double *X, const double *xb,
-                                                int b, int cnt, const int *first, int ts, FT *F, bool &bad)
+__device__ __forceinline__ void list_pair_force(const BatchArgs &A, const SysP &p, const double *X,
+                                                const double *xb, int b, FT *F, bool &bad)
 {
     const int n = p.n;
+    int cnt = A.ncount[p.bead_off + b];
     cnt = cnt < 0 ? 0 : (cnt < A.list_depth ? cnt : A.list_depth);
     const int *nb = A.nbr + p.bead_off + b;
     const int64_t stride = A.list_stride;
     const FT rc2 = (FT)p.rc2, p0 = (FT)p.p0, p1 = (FT)p.p1, shift = (FT)p.shift;
-    int j_next = cnt > 0 ? first[0] : 0;
+    int j_next = cnt > 0 ? nb[0] : 0;
     for (int k = 0; k < cnt; k++) {
         const int j = j_next;  // the next index is loaded ahead of this pair's positions
-        if (k + 1 < cnt) j_next = k + 1 < kPairSlots ? first[(k + 1) * ts] : nb[(size_t)(k + 1) * stride];
+        if (k + 1 < cnt) j_next = nb[(size_t)(k + 1) * stride];
         if ((unsigned)j >= (unsigned)n) {
             bad = true;
             continue;
@@ -845,72 +729,35 @@ __device__ __forceinline__ void list_pair_force(const BatchArgs &A, const SysP &
     }
 }
 
+// pair forces of every bead (the list walk above, then the coupled
+// populations' cross lists); writes them to fp[bead]
 template <int D, typename FT, int WHICH, bool CROSS>
 __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_pair(BatchArgs A)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ int sh_run;
-    PairSmem<D> sm;
-    const int TB = blockDim.x;
-    sm.carve(smem_raw, TB);
     const int nt = *A.n_bead_tiles;
-    const int g = gridDim.x;
-    // software pipeline over the tiles: a tile's inputs are copied during the
-    // previous one; the table entries and the run flags run one tile ahead
-    Tile nxt = (int)blockIdx.x < nt ? A.bead_tiles[blockIdx.x] : Tile{0, 0};
-    Tile after = (int)blockIdx.x + g < nt ? A.bead_tiles[blockIdx.x + g] : Tile{0, 0};
-    int run_next = 0;  // thread 0: the next tile's system runs (its flags as of one tile earlier)
-    if ((int)blockIdx.x < nt) {
-        pair_prefetch<D, WHICH>(A, sm, nxt, 0);
-        if (threadIdx.x == 0) {
-            const SysS &s0 = A.S[nxt.sys];
-            run_next = ld_volatile(&s0.active) && !(ld_volatile(&s0.flags) & kFlagFatal) && A.P[nxt.sys].calc_wca;
-        }
-    }
-    cp_async_commit();
-    int buf = 1;
-    for (int t = blockIdx.x; t < nt; t += g) {
-        buf ^= 1;  // the buffer holding this tile's inputs
-        const Tile tl = nxt;
-        nxt = after;
-        if (t + 2 * g < nt) after = A.bead_tiles[t + 2 * g];
-        __syncthreads();  // the previous tile is done with its buffer
-        const bool more = t + g < nt;
-        if (more) pair_prefetch<D, WHICH>(A, sm, nxt, buf ^ 1);
-        cp_async_commit();
-        // one decision per CTA, taken by thread 0 (every thread reaches the
-        // same barriers); a flag another CTA raises meanwhile only costs the
-        // work of one more tile of a system that stopped
-        if (threadIdx.x == 0) {
-            sh_run = run_next;
-            if (more) {
-                const SysS &sn = A.S[nxt.sys];
-                run_next = ld_volatile(&sn.active) && !(ld_volatile(&sn.flags) & kFlagFatal) && A.P[nxt.sys].calc_wca;
-            }
-        }
-        cp_async_wait<1>();  // this thread's copies of this tile have landed
-        __syncthreads();     // ... and every other thread's
-        if (!sh_run) continue;
+    // the next tile's table entry is loaded while the current tile runs
+    Tile nx = (int)blockIdx.x < nt ? A.bead_tiles[blockIdx.x] : Tile{0, 0};
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = nx;
+        if (t + (int)gridDim.x < nt) nx = A.bead_tiles[t + gridDim.x];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
-        const int jt = threadIdx.x;
-        const int b = tl.begin + jt;
-        if (b >= p.n || jt >= A.tile_beads) continue;
+        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal) || !p.calc_wca) continue;
+        const int b = tl.begin + threadIdx.x;
+        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
         const double *X = stage_x<WHICH>(p);
         double xb[3] = {0.0, 0.0, 0.0};
-        const double *xo = sm.in(sm.x, buf) + jt * D;
 #pragma unroll
-        for (int i = 0; i < D; i++) xb[i] = xo[i];
+        for (int i = 0; i < D; i++) xb[i] = X[(size_t)b * D + i];
         FT F[3] = {FT(0), FT(0), FT(0)};
         bool bad = false;
-        list_pair_force<D, FT>(A, p, X, xb, b, sm.in(sm.cnt, buf)[jt], sm.in(sm.idx, buf) + jt, TB, F, bad);
+        list_pair_force<D, FT>(A, p, X, xb, b, F, bad);
         if constexpr (CROSS) add_cross<D, FT, WHICH>(A, p, b, xb, F, bad);
         if (bad) atomicOr(&s.flags, kFlagListCorrupt);
         FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
 #pragma unroll
         for (int i = 0; i < D; i++) fp[i] = F[i];
     }
-    cp_async_wait<0>();  // no copy is left in flight when the CTA exits
 }
 
 template <int D, typename FT>
@@ -965,97 +812,12 @@ __device__ __forceinline__ double srk_update(double x, double dt_eff, double s2,
 
 
 // ------------------------------------------------------------------------
-// stage and update kernels
+// stage and update kernels.  FUSED: the stage walks the bead's neighbour
+// list itself (list_pair_force, the same sum in the same order as k_pair)
+// instead of reading fp, which saves the pair kernel's launch, its second
+// read of the positions and the fp round trip (SRK2 without coupled
+// populations only; chosen per context by gcr_config.fuse_pair).
 // ------------------------------------------------------------------------
-// the stage reads the force accumulated so far: the SRK2 corrector adds to
-// F0, SRK4 stages after the first add to the weighted sum
-constexpr bool stage_reads_force(int S) { return S == 1 || (srk4_stage(S) && S != 10); }
-
-// Issue the copies of tile `tl`'s inputs into buffer `b` (every thread of the
-// CTA): the positions, chain ids and rest lengths of beads begin-2 ..
-// begin+TB+1, and each thread's own tangent, pair force, force so far and
-// build position (FUSED: its list count and first list entries instead of a
-// pair force).  Beads outside the system get neutral values.
-template <int D, typename FT, int STAGE, bool FUSED>
-__device__ __forceinline__ void stage_prefetch(const BatchArgs &A, StageSmem<D, FT> &sm, const Tile &tl, int b,
-                                               int TB)
-{
-    using BT = typename StageSmem<D, FT>::BT;
-    const SysP &p = A.P[tl.sys];
-    const int n = p.n, base = tl.begin - 2;
-    const double *X = stage_x<stage_reads(STAGE)>(p);
-    const BT *RB = reinterpret_cast<const BT *>(A.restb) + p.bead_off;
-    double *xs = sm.in(sm.x, b);
-    int *chs = sm.in(sm.ch, b);
-    BT *ras = sm.in(sm.ra, b);
-    for (int k = threadIdx.x; k < TB + 4; k += TB) {
-        const int m = base + k;
-        if (m >= 0 && m < n) {
-#pragma unroll
-            for (int i = 0; i < D; i++) cp_async<8>(xs + k * D + i, X + (size_t)m * D + i);
-            cp_async<4>(chs + k, p.chain + m);
-            cp_async<sizeof(BT)>(ras + k, RB + m);
-        } else {
-#pragma unroll
-            for (int i = 0; i < D; i++) xs[k * D + i] = 0.0;
-            chs[k] = -1;
-            ras[k] = BT(0);
-        }
-    }
-    const int j = threadIdx.x, m = tl.begin + j;
-    if (j < TB && m < n) {
-        const FT *T = reinterpret_cast<const FT *>(p.tan) + (size_t)m * D;
-        FT *tin = sm.in(sm.tin, b) + j * D;
-#pragma unroll
-        for (int i = 0; i < D; i++) cp_async<sizeof(FT)>(tin + i, T + i);
-        if (p.calc_wca) {
-            if constexpr (FUSED) {
-                // the list depth is at least kPairSlots; slots past the count are never read
-                cp_async<4>(sm.in(sm.lc, b) + j, A.ncount + p.bead_off + m);
-                int *li = sm.in(sm.li, b);
-#pragma unroll
-                for (int k = 0; k < kPairSlots; k++)
-                    cp_async<4>(li + k * TB + j, A.nbr + (size_t)k * A.list_stride + p.bead_off + m);
-            } else {
-                const FT *P = reinterpret_cast<const FT *>(A.fp) + (size_t)(p.bead_off + m) * D;
-                FT *pin = sm.in(sm.pin, b) + j * D;
-#pragma unroll
-                for (int i = 0; i < D; i++) cp_async<sizeof(FT)>(pin + i, P + i);
-            }
-        }
-        if constexpr (stage_reads_force(STAGE)) {
-            const FT *F = reinterpret_cast<const FT *>(p.frc) + (size_t)m * D;
-            FT *fin = sm.in(sm.fin, b) + j * D;
-#pragma unroll
-            for (int i = 0; i < D; i++) cp_async<sizeof(FT)>(fin + i, F + i);
-        }
-        if constexpr (stage_writes(STAGE) != 0) {
-            if (p.calc_wca && p.rigid == 0.0) {
-                const double *R = A.xref + (size_t)(p.bead_off + m) * D;
-                double *xr = sm.in(sm.xr, b) + j * D;
-#pragma unroll
-                for (int i = 0; i < D; i++) cp_async<8>(xr + i, R + i);
-            }
-        }
-    }
-}
-
-// same-chain neighbours of staged bead k from the staged chain ids (the bits
-// k_topo writes; a bead outside the system, chain id -1, has none): ch[k+1]
-// for staged_next, ch[k-2 .. k+2] for staged_topo, which the callers keep
-// inside the window
-__device__ __forceinline__ bool staged_next(const int *ch, int k) { return ch[k] >= 0 && ch[k + 1] == ch[k]; }
-__device__ __forceinline__ uint8_t staged_topo(const int *ch, int k)
-{
-    const int c = ch[k];
-    if (c < 0) return 0;
-    return (uint8_t)((ch[k - 1] == c ? kHasPrev : 0) | (ch[k - 2] == c ? kHasPrev2 : 0) |
-                     (ch[k + 1] == c ? kHasNext : 0) | (ch[k + 2] == c ? kHasNext2 : 0));
-}
-
-// FUSED: the stage sums the pair forces itself over the bead's list (the
-// arithmetic of k_pair, which then is not launched), SRK2 without coupled
-// populations
 template <int D, typename FT, int STAGE, bool FUSED = false>
 __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
 {
@@ -1067,61 +829,50 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
     using BT = typename StageSmem<D, FT>::BT;
     sm.carve(smem_raw, TB);
     const int nt = *A.n_bead_tiles;
-    const int g = gridDim.x;
-    // software pipeline over the tiles: tile t's inputs were copied during
-    // tile t - gridDim.x; the table entries and run flags run one tile ahead
-    Tile nxt = (int)blockIdx.x < nt ? A.bead_tiles[blockIdx.x] : Tile{0, 0};
-    Tile after = (int)blockIdx.x + g < nt ? A.bead_tiles[blockIdx.x + g] : Tile{0, 0};
-    int run_next = 0;  // thread 0: the next tile's system runs (its flags as of one tile earlier)
-    if ((int)blockIdx.x < nt) {
-        stage_prefetch<D, FT, STAGE, FUSED>(A, sm, nxt, 0, TB);
-        if (threadIdx.x == 0) {
-            const SysS &s0 = A.S[nxt.sys];
-            run_next = ld_volatile(&s0.active) && !(ld_volatile(&s0.flags) & kFlagFatal);
-        }
-    }
-    cp_async_commit();
-    int buf = 1;
-    for (int t = blockIdx.x; t < nt; t += g) {
-        buf ^= 1;  // the buffer holding this tile's inputs
-        const Tile tl = nxt;
-        nxt = after;
-        if (t + 2 * g < nt) after = A.bead_tiles[t + 2 * g];
-        __syncthreads();  // the previous tile is done with its buffer and the work arrays
-        const bool more = t + g < nt;
-        if (more) stage_prefetch<D, FT, STAGE, FUSED>(A, sm, nxt, buf ^ 1, TB);
-        cp_async_commit();
-        // one decision per CTA, taken by thread 0 (every thread must reach the
-        // same barriers); a flag another CTA raises meanwhile only costs the
-        // work of one more tile of a system that stopped
-        if (threadIdx.x == 0) {
-            sh_run = run_next;
-            if (more) {
-                const SysS &sn = A.S[nxt.sys];
-                run_next = ld_volatile(&sn.active) && !(ld_volatile(&sn.flags) & kFlagFatal);
-            }
-        }
-        cp_async_wait<1>();  // this thread's copies of this tile have landed
-        __syncthreads();     // ... and every other thread's
-        if (!sh_run) continue;
+    // the next tile's table entry is loaded while the current tile runs
+    Tile nx = (int)blockIdx.x < nt ? A.bead_tiles[blockIdx.x] : Tile{0, 0};
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        __syncthreads();  // the previous tile is done with shared memory
+        const Tile tl = nx;
+        if (t + (int)gridDim.x < nt) nx = A.bead_tiles[t + gridDim.x];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
+        // the system's constants are read before the barrier, with its flags
         const int n = p.n;
-        const double *const xs = sm.in(sm.x, buf);
-        const int *const chs = sm.in(sm.ch, buf);
-        const BT *const ras = sm.in(sm.ra, buf);
-        // the bead's own inputs
+        const int base = tl.begin - 2;
+        const double *__restrict__ X = stage_x<stage_reads(STAGE)>(p);
+        // one decision per CTA: other CTAs may raise the system's flags while
+        // this one runs, and every thread must reach the same barriers
+        if (threadIdx.x == 0) sh_run = ld_volatile(&s.active) && !(ld_volatile(&s.flags) & kFlagFatal);
+        __syncthreads();
+        if (!sh_run) continue;
+        // 1. positions and topology of beads begin-2 .. begin+TB+1
+        for (int k = threadIdx.x; k < TB + 4; k += TB) {
+            int m = base + k;
+            if (m >= 0 && m < n) {
+#pragma unroll
+                for (int i = 0; i < D; i++) sm.x[k * D + i] = __ldg(X + (size_t)m * D + i);
+                sm.tp[k] = A.topo[p.bead_off + m];
+                sm.ra[k] = p.calc_springs ? (BT)__ldg(p.rest + __ldg(p.chain + m)) : BT(0);
+            } else {
+                sm.tp[k] = 0;
+                sm.ra[k] = BT(0);
+            }
+        }
+        __syncthreads();
+        // the bead's own inputs of phase 4, loaded before the barriers
         FT pre_t[D], pre_f[D], pre_p[D];
         {
-            const int j = threadIdx.x;
-            const bool ok = tl.begin + j < n;
-            const FT *tin = sm.in(sm.tin, buf) + j * D, *fin = sm.in(sm.fin, buf) + j * D;
-            const FT *pin = sm.in(sm.pin, buf) + j * D;
+            const int bq = tl.begin + (int)threadIdx.x;
+            const bool ok = bq < n;
+            const FT *tq = reinterpret_cast<const FT *>(p.tan);
+            const FT *fq = reinterpret_cast<const FT *>(p.frc);
+            const FT *pq = reinterpret_cast<const FT *>(A.fp) + (size_t)(p.bead_off + (ok ? bq : 0)) * D;
 #pragma unroll
             for (int i = 0; i < D; i++) {
-                pre_t[i] = ok ? tin[i] : FT(0);
-                pre_f[i] = (ok && stage_reads_force(STAGE)) ? fin[i] : FT(0);
-                pre_p[i] = (ok && p.calc_wca && !FUSED) ? pin[i] : FT(0);
+                pre_t[i] = ok ? tq[(size_t)bq * D + i] : FT(0);
+                pre_f[i] = (ok && STAGE == 1) ? fq[(size_t)bq * D + i] : FT(0);
+                pre_p[i] = (!FUSED && ok && p.calc_wca) ? pq[i] : FT(0);
             }
         }
         const bool springs = p.calc_springs, cb = p.calc_bend;
@@ -1132,15 +883,15 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                 BT d[D], tt[D], f = BT(0);
 #pragma unroll
                 for (int i = 0; i < D; i++) d[i] = tt[i] = BT(0);
-                if (staged_next(chs, k)) {
+                if (sm.tp[k] & kHasNext) {
                     BT r2 = BT(0);
 #pragma unroll
                     for (int i = 0; i < D; i++) {
-                        d[i] = (BT)inbounds(xs[k * D + i], xs[(k + 1) * D + i], p.half_L, p.L);
+                        d[i] = (BT)inbounds(sm.x[k * D + i], sm.x[(k + 1) * D + i], p.half_L, p.L);
                         r2 += d[i] * d[i];
                     }
                     if (r2 != BT(0)) {
-                        const BT a = ras[k];
+                        const BT a = sm.ra[k];
                         BT inv = inv_sqrt<BT>(r2);
                         f = kspring * (a * inv - BT(1));
 #pragma unroll
@@ -1165,9 +916,8 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                     BT fw[D], bw[D];
 #pragma unroll
                     for (int i = 0; i < D; i++) fw[i] = bw[i] = BT(0);
-                    // bead k+1 has a same-chain bead either side
-                    const int c1 = chs[k + 1];
-                    if (c1 >= 0 && chs[k] == c1 && chs[k + 2] == c1) {
+                    const uint8_t tp = sm.tp[k + 1];
+                    if ((tp & kHasPrev) && (tp & kHasNext)) {
                         if (!bend<D, BT>(sm.bt + (k + 1) * D, sm.bt + k * D, theta0, kappa, fw, bw)) {
 #pragma unroll
                             for (int i = 0; i < D; i++) fw[i] = bw[i] = BT(0);
@@ -1191,7 +941,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
             FT *tan = reinterpret_cast<FT *>(p.tan);
             double xb[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-            for (int i = 0; i < D; i++) xb[i] = xs[(tid + 2) * D + i];
+            for (int i = 0; i < D; i++) xb[i] = sm.x[(tid + 2) * D + i];
             // F0 (stage 1) and the bonded terms summed in BT, then FT
             BT Fb[3];
             FT F[3], tg[3];
@@ -1203,7 +953,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
             }
             bool tang_set = false;
             if (springs) {
-                const uint8_t tp = staged_topo(chs, tid + 2);
+                const uint8_t tp = sm.tp[tid + 2];
                 const bool prev = tp & kHasPrev, next = tp & kHasNext;
                 if (prev) {
                     const BT f = sm.bf[tid + 1];
@@ -1255,14 +1005,16 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
             for (int i = 0; i < D; i++) F[i] = (FT)Fb[i];
             if (p.calc_wca) {
                 if constexpr (FUSED) {
-                    // the pair force k_pair would have written to fp[b]
+                    FT Fp[3] = {FT(0), FT(0), FT(0)};
                     bool bad = false;
-                    list_pair_force<D, FT>(A, p, stage_x<stage_reads(STAGE)>(p), xb, b, sm.in(sm.lc, buf)[tid],
-                                           sm.in(sm.li, buf) + tid, TB, pre_p, bad);
+                    list_pair_force<D, FT>(A, p, X, xb, b, Fp, bad);
                     if (bad) atomicOr(&s.flags, kFlagListCorrupt);
-                }
 #pragma unroll
-                for (int i = 0; i < D; i++) F[i] += pre_p[i];
+                    for (int i = 0; i < D; i++) F[i] += Fp[i];
+                } else {
+#pragma unroll
+                    for (int i = 0; i < D; i++) F[i] += pre_p[i];
+                }
             }
             if (p.self_propel) {
                 const FT v0 = (FT)p.v0;
@@ -1287,7 +1039,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
 #pragma unroll
                 for (int i = 0; i < D; i++) {
                     faux[(size_t)b * D + i] = F[i];
-                    G[i] = STAGE == 10 ? F[i] * w : pre_f[i] + F[i] * w;
+                    G[i] = STAGE == 10 ? F[i] * w : frc[(size_t)b * D + i] + F[i] * w;
                 }
             } else {
 #pragma unroll
@@ -1303,14 +1055,14 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                 // the step's translational noise, drawn once in the first stage
                 FT xi[3] = {FT(0), FT(0), FT(0)};
                 if (p.D > 0.0) {
-                    FT *xn = reinterpret_cast<FT *>(A.xi) + (size_t)(p.bead_off + b) * D;
+                    FT *xs = reinterpret_cast<FT *>(A.xi) + (size_t)(p.bead_off + b) * D;
                     if constexpr (STAGE == 0 || STAGE == 10) {
                         noise_trans<D, FT>(p, s, b, xi);
 #pragma unroll
-                        for (int i = 0; i < D; i++) xn[i] = xi[i];
+                        for (int i = 0; i < D; i++) xs[i] = xi[i];
                     } else {
 #pragma unroll
-                        for (int i = 0; i < D; i++) xi[i] = xn[i];
+                        for (int i = 0; i < D; i++) xi[i] = xs[i];
                     }
                 }
                 // virtual update: (pos + dt_eff/r F + sqrt(2 D dt) xi) mod L
@@ -1332,7 +1084,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                     }
                     if (!finite)
                         atomicOr(&s.flags, kFlagNonFinite);
-                    else if (p.calc_wca && left_skin_of<D>(p, sm.in(sm.xr, buf) + tid * D, x1))
+                    else if (p.calc_wca && left_skin<D>(p, A, b, x1))
                         s.rebuild = 1;  // the list no longer covers the new positions
                 }
             }
@@ -1360,147 +1112,42 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
             }
         }
     }
-    cp_async_wait<0>();  // no copy is left in flight when the CTA exits
-}
-
-// Shared memory of the update kernel: each thread's own inputs, double-
-// buffered and copied one tile ahead (cp.async), as in the stage kernels.
-template <int D, typename FT>
-struct UpdateSmem {
-    double *x;   // [TB][D] positions
-    double *xr;  // [TB][D] positions at the last list build (skin test)
-    FT *f;       // [TB][D] F0 + F1 (SRK2) or the weighted sum (SRK4)
-    FT *xi;      // [TB][D] the step's translational noise
-    size_t step; // bytes from buffer 0 to buffer 1
-    template <typename T>
-    __device__ __forceinline__ T *in(T *a, int b) const
-    {
-        return reinterpret_cast<T *>(reinterpret_cast<unsigned char *>(a) + (size_t)b * step);
-    }
-    __host__ __device__ size_t carve(unsigned char *base, int TB)
-    {
-        size_t off = 0;
-        auto take = [&](size_t bytes) {
-            unsigned char *r = base ? base + off : nullptr;
-            off += (bytes + 15) / 16 * 16;
-            return r;
-        };
-        x = reinterpret_cast<double *>(take((size_t)TB * D * sizeof(double)));
-        xr = reinterpret_cast<double *>(take((size_t)TB * D * sizeof(double)));
-        f = reinterpret_cast<FT *>(take((size_t)TB * D * sizeof(FT)));
-        xi = reinterpret_cast<FT *>(take((size_t)TB * D * sizeof(FT)));
-        step = off;
-        take(step);
-        return off;
-    }
-};
-
-template <int D, typename FT>
-size_t update_smem_bytes(int TB)
-{
-    UpdateSmem<D, FT> sm;
-    return sm.carve(nullptr, TB);
-}
-
-// issue the copies of each thread's inputs of tile `tl` into buffer `b`
-template <int D, typename FT>
-__device__ __forceinline__ void update_prefetch(const BatchArgs &A, UpdateSmem<D, FT> &sm, const Tile &tl, int b)
-{
-    const SysP &p = A.P[tl.sys];
-    const int j = threadIdx.x, m = tl.begin + j;
-    if (j >= A.tile_beads || m >= p.n) return;
-    if (p.rigid == 0.0) {
-        double *x = sm.in(sm.x, b) + j * D;
-        const FT *F = reinterpret_cast<const FT *>(p.frc) + (size_t)m * D;
-        FT *f = sm.in(sm.f, b) + j * D;
-#pragma unroll
-        for (int i = 0; i < D; i++) {
-            cp_async<8>(x + i, p.pos + (size_t)m * D + i);
-            cp_async<sizeof(FT)>(f + i, F + i);
-        }
-        if (p.calc_wca) {
-            double *xr = sm.in(sm.xr, b) + j * D;
-            const double *R = A.xref + (size_t)(p.bead_off + m) * D;
-#pragma unroll
-            for (int i = 0; i < D; i++) cp_async<8>(xr + i, R + i);
-        }
-    }
-    if (p.D > 0.0) {
-        FT *xi = sm.in(sm.xi, b) + j * D;
-        const FT *X = reinterpret_cast<const FT *>(A.xi) + (size_t)(p.bead_off + m) * D;
-#pragma unroll
-        for (int i = 0; i < D; i++) cp_async<sizeof(FT)>(xi + i, X + i);
-    }
 }
 
 template <int D, typename FT>
 __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ int sh_run;
-    UpdateSmem<D, FT> sm;
-    sm.carve(smem_raw, blockDim.x);
     const int nt = *A.n_bead_tiles;
-    const int g = gridDim.x;
-    // software pipeline over the tiles, as in k_stage: a tile's inputs are
-    // copied during the previous one; table entries and run flags run ahead
-    Tile nxt = (int)blockIdx.x < nt ? A.bead_tiles[blockIdx.x] : Tile{0, 0};
-    Tile after = (int)blockIdx.x + g < nt ? A.bead_tiles[blockIdx.x + g] : Tile{0, 0};
-    int run_next = 0;
-    if ((int)blockIdx.x < nt) {
-        update_prefetch<D, FT>(A, sm, nxt, 0);
-        if (threadIdx.x == 0) {
-            const SysS &s0 = A.S[nxt.sys];
-            run_next = ld_volatile(&s0.active) && !(ld_volatile(&s0.flags) & kFlagFatal);
-        }
-    }
-    cp_async_commit();
-    int buf = 1;
-    for (int t = blockIdx.x; t < nt; t += g) {
-        buf ^= 1;
-        const Tile tl = nxt;
-        nxt = after;
-        if (t + 2 * g < nt) after = A.bead_tiles[t + 2 * g];
-        __syncthreads();  // the previous tile is done with its buffer
-        const bool more = t + g < nt;
-        if (more) update_prefetch<D, FT>(A, sm, nxt, buf ^ 1);
-        cp_async_commit();
-        if (threadIdx.x == 0) {
-            sh_run = run_next;
-            if (more) {
-                const SysS &sn = A.S[nxt.sys];
-                run_next = ld_volatile(&sn.active) && !(ld_volatile(&sn.flags) & kFlagFatal);
-            }
-        }
-        cp_async_wait<1>();
-        __syncthreads();
-        if (!sh_run) continue;
+    // the next tile's table entry is loaded while the current tile runs
+    Tile nx = (int)blockIdx.x < nt ? A.bead_tiles[blockIdx.x] : Tile{0, 0};
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = nx;
+        if (t + (int)gridDim.x < nt) nx = A.bead_tiles[t + gridDim.x];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
-        const int j = threadIdx.x;
-        const int b = tl.begin + j;
-        // a thread past its system's beads goes to the next tile's barrier
-        if (b >= p.n || j >= A.tile_beads) continue;
+        // no barriers in this kernel: a per-thread decision is safe
+        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal)) continue;
+        const int b = tl.begin + threadIdx.x;
+        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
+        const FT *frc = reinterpret_cast<const FT *>(p.frc);
         const double dtu = s.dt_used;
         // force_prefactor 0.5 of the SRK2 corrector; 1 for SRK4's weighted sum
         const double dt_eff = dtu * (A.order == 4 ? 1.0 : 0.5) / p.radius;
         const double s2 = sqrt(2.0 * dtu * p.D);
         FT xi[3] = {FT(0), FT(0), FT(0)};
         if (p.D > 0.0) {
-            const FT *xs = sm.in(sm.xi, buf) + j * D;
+            const FT *xs = reinterpret_cast<const FT *>(A.xi) + (size_t)(p.bead_off + b) * D;
 #pragma unroll
             for (int i = 0; i < D; i++) xi[i] = xs[i];
         }
         double x[3] = {0.0, 0.0, 0.0};
         bool finite = true;
         const bool plain = p.rigid == 0.0;  // else k_rigid writes pos
-        const double *xo_s = sm.in(sm.x, buf) + j * D;
-        const FT *f_s = sm.in(sm.f, buf) + j * D;
         if (plain) {
 #pragma unroll
             for (int i = 0; i < D; i++) {
-                const double xo = xo_s[i];
-                x[i] = srk_update<FT>(xo, dt_eff, s2, f_s[i], xi[i], p.L);
+                const double xo = p.pos[(size_t)b * D + i];
+                x[i] = srk_update<FT>(xo, dt_eff, s2, frc[(size_t)b * D + i], xi[i], p.L);
                 finite &= isfinite(x[i]);
                 p.pos[(size_t)b * D + i] = x[i];
                 const int di = image_step(xo, x[i], p.half_L);
@@ -1533,10 +1180,8 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A
 #pragma unroll
             for (int i = 0; i < D; i++) tan[(size_t)b * D + i] = tb[i] / mag;
         }
-        // rebuild before the next step
-        if (plain && finite && p.calc_wca && left_skin_of<D>(p, sm.in(sm.xr, buf) + j * D, x)) s.rebuild = 1;
+        if (plain && finite && p.calc_wca && left_skin<D>(p, A, b, x)) s.rebuild = 1;  // rebuild before the next step
     }
-    cp_async_wait<0>();  // no copy is left in flight when the CTA exits
 }
 
 // ------------------------------------------------------------------------
@@ -1804,26 +1449,20 @@ __global__ void k_sys_mark(BatchArgs A, int n_slots, int slot)
 // kernels test it -- a bead farther than skin/2 from where the list was built
 // flags a rebuild, and otherwise the list still holds every pair within
 // r_cut.  Coupled populations are flagged outright: their fixed members have
-// no bead tiles to test.  The host may also have changed rest lengths: each
-// bead's is copied from its chain's (A.restb, which the stage kernels stage
-// with the positions).
-template <int D, typename FT>
+// no bead tiles to test.
+template <int D>
 __global__ void __launch_bounds__(512) k_run_check(BatchArgs A)
 {
-    using BT = typename Bonded<FT>::type;
     const int nt = *A.n_bead_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const Tile tl = A.bead_tiles[t];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
         // no barriers in this kernel: a per-thread decision is safe
-        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal)) continue;
+        if (!p.calc_wca || !ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal)) continue;
+        if (ld_volatile(&s.rebuild)) continue;
         const int b = tl.begin + threadIdx.x;
         if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
-        int ch = p.chain[b];
-        ch = ch < 0 ? 0 : (ch >= p.n_chains ? p.n_chains - 1 : ch);
-        reinterpret_cast<BT *>(A.restb)[p.bead_off + b] = (BT)p.rest[ch];
-        if (!p.calc_wca || ld_volatile(&s.rebuild)) continue;
         if (p.grp_n > 0) {
             s.rebuild = 1;
             continue;
@@ -1869,26 +1508,20 @@ struct StepKernels {
 KernelSet kernel_set(int dim, int precision)
 {
     KernelSet k{};
-    if (dim == 2) {
+    if (dim == 2)
         k.stage_smem = precision == 0 ? stage_smem_bytes<2, double> : stage_smem_bytes<2, float>;
-        k.update_smem = precision == 0 ? update_smem_bytes<2, double> : update_smem_bytes<2, float>;
-        k.pair_smem = pair_smem_bytes<2>;
-    } else {
+    else
         k.stage_smem = precision == 0 ? stage_smem_bytes<3, double> : stage_smem_bytes<3, float>;
-        k.update_smem = precision == 0 ? update_smem_bytes<3, double> : update_smem_bytes<3, float>;
-        k.pair_smem = pair_smem_bytes<3>;
-    }
-#define GCR_FILL(D_, FT_)                        \
-    k.pair0 = StepKernels<D_, FT_>::pair0();     \
-    k.pair1 = StepKernels<D_, FT_>::pair1();     \
-    k.stage0 = StepKernels<D_, FT_>::stage0();   \
-    k.stage1 = StepKernels<D_, FT_>::stage1();   \
+#define GCR_FILL(D_, FT_)                       \
+    k.pair0 = StepKernels<D_, FT_>::pair0();    \
+    k.pair1 = StepKernels<D_, FT_>::pair1();    \
+    k.stage0 = StepKernels<D_, FT_>::stage0();  \
+    k.stage1 = StepKernels<D_, FT_>::stage1();  \
     k.stage0f = StepKernels<D_, FT_>::stage0f(); \
     k.stage1f = StepKernels<D_, FT_>::stage1f(); \
-    k.update = StepKernels<D_, FT_>::update();   \
-    k.rigid0 = StepKernels<D_, FT_>::rigid0();   \
-    k.rigid1 = StepKernels<D_, FT_>::rigid1();   \
-    k.run_check = (void *)k_run_check<D_, FT_>; \
+    k.update = StepKernels<D_, FT_>::update();  \
+    k.rigid0 = StepKernels<D_, FT_>::rigid0();  \
+    k.rigid1 = StepKernels<D_, FT_>::rigid1();  \
     StepKernels<D_, FT_>::fill4(k);
     if (dim == 2 && precision == 0) {
         GCR_FILL(2, double)
@@ -1907,6 +1540,7 @@ KernelSet kernel_set(int dim, int precision)
         k.build1 = (void *)k_build<2, 1>;
         k.bin2 = (void *)k_bin<2, 2>;
         k.build2 = (void *)k_build<2, 2>;
+        k.run_check = (void *)k_run_check<2>;
     } else {
         k.bin0 = (void *)k_bin<3, 0>;
         k.bin1 = (void *)k_bin<3, 1>;
@@ -1914,6 +1548,7 @@ KernelSet kernel_set(int dim, int precision)
         k.build1 = (void *)k_build<3, 1>;
         k.bin2 = (void *)k_bin<3, 2>;
         k.build2 = (void *)k_build<3, 2>;
+        k.run_check = (void *)k_run_check<3>;
     }
     k.sort = (void *)k_sort;
     k.topo = (void *)k_topo;

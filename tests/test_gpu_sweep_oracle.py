@@ -7,9 +7,20 @@ smallest and largest bending constant and chirality -- are relaxed together
 on the device in FP64 and then advanced in one batch with the Philox stream;
 the oracle (the reference's step restated in C, same Philox stream, the
 reference's 40-step Verlet lists and its own summation order) advances each
-from the same state under the reference's adaptive dt rule.  Positions
-agree within 1e-12 of the box after one step and 1e-9 after 200; the dt
-each step took agrees within 1e-9 relative.
+from the same state under the reference's adaptive dt rule.
+
+These dense systems are chaotic right after relaxation: two FP64 runs of the
+oracle itself, one started from positions one ulp away, drift apart by about
+a decade every 10-20 steps (1e-16 of the box after one step, 1e-10 after 50,
+order one after a few hundred).  Rounding differences between any two
+correct FP64 implementations grow the same way, so past the first steps the
+bound is that control, not a fixed number: at every checkpoint where the
+one-ulp control is still below 1e-6 of the box (the linear regime), the GPU
+must be within 1e-13 of the box or 100 times the control's own divergence,
+and its dt within 1e-12 relative or 100 times the control's dt difference.
+Past the linear regime no trajectory comparison means anything (the
+statistics tests cover that regime); every system is required to stay in
+the linear regime for at least its first two checkpoints (1 and 10 steps).
 """
 import math
 
@@ -51,6 +62,17 @@ def _countdown(until, n):
     return N_UPDATE - (n - until) % N_UPDATE
 
 
+def _one_ulp(pos):
+    """Positions one ulp toward zero (a position of exactly 0 is kept)."""
+    return np.where(pos > 0, np.nextafter(pos, -np.inf), pos)
+
+
+LINEAR = 1e-6   # control divergence (fraction of the box) up to which the trajectories are compared
+FLOOR = 1e-13   # absolute floor of the position bound (fraction of the box)
+DT_FLOOR = 1e-12
+FACTOR = 100.0
+
+
 def test_sweep_systems_match_the_oracle():
     specs = W.config3(n_systems=256, param_seed=12345)
     idx = pick_systems(specs)
@@ -60,40 +82,53 @@ def test_sweep_systems_match_the_oracle():
     b.relax(max_steps=2000, adaptive_after=True)
     sts = b.statuses()
     assert not any(s["flags"] for s in sts)
-    oracles, dts, step0 = [], [s["dt"] for s in sts], [s["step"] for s in sts]
+    oracles, controls = [], []
+    step0 = [s["step"] for s in sts]
+    dts = [s["dt"] for s in sts]
+    dts_c = list(dts)
     for st, sp in zip(b.states, sel):
         p = sp.params
         a = float(sp.rest_lengths.max())
         rc = float(p.wca_params[3])
         ng = max(1, int(p.L / (2.0 * max(2 * a, rc))))
-        o = O.OracleSystem(st.pos.cpu().numpy(), st.tangent.cpu().numpy(), sp.chain_id, sp.rest_lengths, p.L,
-                           p.spring_params, p.wca_params, p.active_params, p.D, p.Dr, p.radius, p.n_nearby, ng,
-                           nbor_depth=64)
-        o.build_lists(grid_window=max(1, math.ceil(max(2 * a, rc) / (p.L / ng))))
-        oracles.append(o)
+        window = max(1, math.ceil(max(2 * a, rc) / (p.L / ng)))
+        pos = st.pos.cpu().numpy()
+        for start, out in ((pos, oracles), (_one_ulp(pos), controls)):
+            o = O.OracleSystem(start, st.tangent.cpu().numpy(), sp.chain_id, sp.rest_lengths, p.L,
+                               p.spring_params, p.wca_params, p.active_params, p.D, p.Dr, p.radius, p.n_nearby,
+                               ng, nbor_depth=64)
+            o.build_lists(grid_window=window)
+            out.append(o)
     until = [N_UPDATE] * len(sel)
     done = 0
     report, bad = [], []
-    for n_steps, tol in ((1, 1e-12), (9, 1e-11), (40, 1e-10), (150, 1e-9)):
+    compared = {sp.name: [] for sp in sel}
+    for n_steps in (1, 9, 40, 150):
         b.begin(n_steps)
         b.run(n_steps)
         sts = b.statuses()
-        for j, (st, sp, o) in enumerate(zip(b.states, sel, oracles)):
+        for j, (st, sp, o, oc) in enumerate(zip(b.states, sel, oracles, controls)):
             p = sp.params
             assert sts[j]["steps_done"] == n_steps and sts[j]["flags"] == 0, (sp.name, sts[j])
-            res = o.run(n_steps, dt=dts[j], dtmax=sp.dt, max_dist_per_step=sp.relax_mdps,
-                        noise_mode=O.NOISE_PHILOX, seed=p.seed, step0=step0[j] + done, steps_until_update=until[j])
-            assert res["steps"] == n_steps
-            # the dt rule on the same forces: equal to rounding after the first
-            # step; later the trajectories' own (tiny) differences feed it
-            dt_tol = 1e-12 if done == 0 else 1e-6
+            kw = dict(dtmax=sp.dt, max_dist_per_step=sp.relax_mdps, noise_mode=O.NOISE_PHILOX, seed=p.seed,
+                      step0=step0[j] + done, steps_until_update=until[j])
+            res = o.run(n_steps, dt=dts[j], **kw)
+            res_c = oc.run(n_steps, dt=dts_c[j], **kw)
+            assert res["steps"] == n_steps and res_c["steps"] == n_steps
             dt_err = abs(res["dt"] - sts[j]["dt"]) / res["dt"]
-            dts[j] = res["dt"]
+            dt_ctrl = abs(res["dt"] - res_c["dt"]) / res["dt"]
+            dts[j], dts_c[j] = res["dt"], res_c["dt"]
             until[j] = _countdown(until[j], n_steps)
             err = np.max(np.abs(min_image(st.pos.cpu().numpy() - o.pos, p.L))) / p.L
-            report.append((sp.name, sp.n, done + n_steps, err, dt_err))
-            if err >= tol or dt_err > dt_tol:
-                bad.append(report[-1])
+            ctrl = np.max(np.abs(min_image(oc.pos - o.pos, p.L))) / p.L
+            row = (sp.name, sp.n, done + n_steps, float(err), float(ctrl), float(dt_err), float(dt_ctrl))
+            report.append(row)
+            if ctrl < LINEAR:
+                compared[sp.name].append(done + n_steps)
+                if err > max(FLOOR, FACTOR * ctrl) or dt_err > max(DT_FLOOR, FACTOR * dt_ctrl):
+                    bad.append(row)
         done += n_steps
     b.close()
     assert not bad, (bad, report)
+    short = {k: v for k, v in compared.items() if v[:2] != [1, 10]}
+    assert not short, ("left the linear regime within 10 steps", short, report)
