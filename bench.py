@@ -384,7 +384,7 @@ def run_gpu(args):
         sp.params.skin = args.skin if args.skin >= 0 else None
     batch = Batch(specs, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph,
                   ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads, list_depth=args.list_depth or None,
-                  fuse_pair=args.fuse_pair)
+                  pair_mode=args.pair_mode)
     groups = list(getattr(specs, "groups", ()))
     for members, fixed, cross in groups:
         batch.couple(members, fixed, cross)
@@ -413,7 +413,7 @@ def run_gpu(args):
         batch.set_adaptive(True)
         args.steps_per_graph, args.ctas_per_sm, args.block_beads = (kw["steps_per_graph"], kw["ctas_per_sm"],
                                                                     kw["block_beads"])
-        args.fuse_pair = kw["fuse_pair"]
+        args.pair_mode = kw["pair_mode"]
     # warm-up under the adaptive dt (regrows the cells if a system overflowed them)
     batch.run_checked(args.warmup)
     eng = batch.engine
@@ -594,13 +594,13 @@ def run_gpu(args):
                 "steps_per_graph": spg, "cell_depth": batch.cell_depth,
                 "list_depth": batch.list_depth, "list_mean": list_mean,
                 "list_builds_per_stage": builds_per_stage, "block_beads": args.block_beads,
-                "ctas_per_sm": args.ctas_per_sm, "fuse_pair": args.fuse_pair,
+                "ctas_per_sm": args.ctas_per_sm, "pair_mode": args.pair_mode,
                 "autotune": None if tuned is None else {k: v for k, v in tuned.items() if k != "trials"}},
         "e2e": e2e, "roofline": roofline, "clocks": clk,
         # the run-start check, then 15 kernels per step (two list builds of
         # four, two pair, two stage, dt rule, update, bookkeeping; 13 when
         # the stages sum the pair forces) in graphs of steps_per_graph steps
-        "gpu_launches": 1 + (13 if args.fuse_pair and not groups else 15) * spg * math.ceil(args.steps / spg),
+        "gpu_launches": 1 + (13 if args.pair_mode == 1 and not groups else 15) * spg * math.ceil(args.steps / spg),
     }
     if fp64 is not None:
         line["fp64"] = fp64
@@ -705,7 +705,7 @@ def fp64_block(args, specs, batch, dev):
     dt0 = [s["dt"] for s in sts]
     depths = dict(cell_depth=min(128, 2 * batch.cell_depth), list_depth=min(1024, 2 * batch.list_depth))
     b = Batch(specs_at(specs, *start), precision="fp64", device=dev, steps_per_graph=args.steps_per_graph,
-              ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads, fuse_pair=args.fuse_pair, **depths)
+              ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads, pair_mode=args.pair_mode, **depths)
     b.set_adaptive(True)
     b._carry_dt = list(dt0)
     b.run_checked(args.warmup)
@@ -820,8 +820,9 @@ def main():
     ap.add_argument("--ctas-per-sm", type=int, default=0,
                     help="CTAs per SM of the tile kernels (0: from occupancy, <0: one CTA per tile)")
     ap.add_argument("--block-beads", type=int, default=128)
-    ap.add_argument("--fuse-pair", type=int, default=0,
-                    help="1: the stage kernels sum the pair forces themselves (no separate pair launch)")
+    ap.add_argument("--pair-mode", type=int, default=0, choices=[0, 1, 2],
+                    help="pair forces: 0 list kernel, 1 list walk inside the stage kernels (no pair launch), "
+                         "2 cell-staged kernel")
     ap.add_argument("--skin", type=float, default=-1.0,
                     help="Verlet skin of the neighbour lists (<0: 0.2 r_cut + 0.1, within [0.2, 1])")
     ap.add_argument("--list-depth", type=int, default=0, help="neighbour slots per bead (0: default)")

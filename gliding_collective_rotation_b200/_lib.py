@@ -33,7 +33,7 @@ class Config(C.Structure):
                 ("system_capacity", C.c_int32), ("cell_capacity", C.c_int64), ("cell_depth", C.c_int32),
                 ("block_beads", C.c_int32), ("block_cells", C.c_int32), ("steps_per_graph", C.c_int32),
                 ("ctas_per_sm", C.c_int32), ("list_depth", C.c_int32), ("srk_order", C.c_int32),
-                ("fuse_pair", C.c_int32)]
+                ("pair_mode", C.c_int32)]
 
 
 class SystemDesc(C.Structure):

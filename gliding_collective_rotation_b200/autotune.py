@@ -33,9 +33,9 @@ SPACE = {
     "ctas_per_sm": (0, 2, 4, 8),       # persistent CTAs per SM (0: as many as fit)
     "steps_per_graph": (5, 10, 20),    # steps per captured CUDA graph
     "skin_scale": (0.67, 1.0, 1.5),    # Verlet skin relative to engine.default_skin(r_cut)
-    "fuse_pair": (0, 1),               # 1: the stage kernels sum the pair forces (no pair launch)
+    "pair_mode": (0, 1, 2),            # pair forces: list kernel, list walk in the stages, cell-staged kernel
 }
-DEFAULT = {"block_beads": 128, "ctas_per_sm": 0, "steps_per_graph": 10, "skin_scale": 1.0, "fuse_pair": 0}
+DEFAULT = {"block_beads": 128, "ctas_per_sm": 0, "steps_per_graph": 10, "skin_scale": 1.0, "pair_mode": 0}
 CACHE = os.path.join(os.path.expanduser("~"), ".cache", "gcr_autotune.json")
 
 
@@ -103,7 +103,7 @@ def measure_shape(specs, shape, precision="mixed", steps=40, warmup=10, device=N
     try:
         b = Batch(sp, precision=precision, device=device, steps_per_graph=shape["steps_per_graph"],
                   block_beads=shape["block_beads"], ctas_per_sm=shape["ctas_per_sm"], srk_order=srk_order,
-                  fuse_pair=shape.get("fuse_pair", 0))
+                  pair_mode=shape.get("pair_mode", 0))
     except (GcrError, RuntimeError, ValueError):
         return math.inf
     try:
@@ -163,5 +163,5 @@ def apply(specs, result):
     """The specs with the tuned skin, and the Batch keyword arguments of the
     tuned shape."""
     kw = {"block_beads": result["block_beads"], "ctas_per_sm": result["ctas_per_sm"],
-          "steps_per_graph": result["steps_per_graph"], "fuse_pair": result.get("fuse_pair", 0)}
+          "steps_per_graph": result["steps_per_graph"], "pair_mode": result.get("pair_mode", 0)}
     return _with_skin(specs, result.get("skin_scale", 1.0)), kw

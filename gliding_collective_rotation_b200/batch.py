@@ -94,7 +94,7 @@ class Batch:
 
     def __init__(self, specs, precision="mixed", device=None, steps_per_graph=10, cell_depth=None,
                  block_beads=128, block_cells=256, stream=None, ctas_per_sm=0, list_depth=None, srk_order=2,
-                 fuse_pair=0):
+                 pair_mode=0):
         if not specs:
             raise ValueError("empty batch")
         dims = {s.dim for s in specs}
@@ -109,7 +109,7 @@ class Batch:
         self.cell_depth = cell_depth
         self.list_depth = list_depth or default_list_depth(self.dim)
         self._engine_kw = dict(block_beads=block_beads, block_cells=block_cells, steps_per_graph=steps_per_graph,
-                               stream=stream, ctas_per_sm=ctas_per_sm, fuse_pair=fuse_pair)
+                               stream=stream, ctas_per_sm=ctas_per_sm, pair_mode=pair_mode)
         self.n_beads = sum(s.n for s in specs)
         self.srk_order = srk_order
         self.big, self.states = _views(specs, precision, self.device, srk_order)

@@ -124,6 +124,7 @@ struct gcr_ctx {
     SysS *dS = nullptr;
     Tile *d_bead_tiles = nullptr;
     Tile *d_cell_tiles = nullptr;
+    int *d_row_prefix = nullptr;  // row tiles of the cell-staged pair kernel per slot, prefix [S + 1]
     int *d_ntiles = nullptr;  // [0] bead tiles, [1] cell tiles
     uint8_t *topo = nullptr;
     int *cnt = nullptr;
@@ -139,6 +140,7 @@ struct gcr_ctx {
     double *pos2 = nullptr;  // SRK4 scratch: second virtual update
     void *faux = nullptr;    // SRK4 scratch: stage forces of systems without a caller buffer
     size_t stage_smem = 0;
+    size_t pair_cells_smem = 0;
     int32_t *chain_starts = nullptr;
     int *d_err = nullptr;
     double *d_out = nullptr;
@@ -148,11 +150,12 @@ struct gcr_ctx {
     std::vector<SysP> hP;
     std::vector<SysS> hS;
     std::vector<Tile> h_bead_tiles, h_cell_tiles;
+    std::vector<int> h_row_prefix;
     RangeAlloc beads, cells, chains;
     BatchArgs args{};
     int grid_update = 1, grid_sys = 1, grid_pair = 1, grid_bin = 1, grid_sort = 1, grid_build = 1;
     int grid_stage0 = 1, grid_stage1 = 1, grid_stage4[4] = {1, 1, 1, 1};
-    int grid_stage0f = 1, grid_stage1f = 1;
+    int grid_stage0f = 1, grid_stage1f = 1, grid_pair_cells = 1;
     cudaGraphExec_t graph = nullptr;
     bool graph_rigid = false;  // the graph holds the rigid-rod projection kernels
     bool graph_obs = false;    // the graph holds the series kernel
@@ -184,6 +187,8 @@ int rebuild_tiles(gcr_ctx *c)
 {
     c->h_bead_tiles.clear();
     c->h_cell_tiles.clear();
+    c->h_row_prefix.assign(c->slots.size() + 1, 0);
+    int64_t rows = 0;
     const int tb = c->cfg.block_beads, tcl = c->cfg.block_cells;
     for (int s = 0; s < (int)c->slots.size(); s++) {
         const Slot &sl = c->slots[s];
@@ -194,6 +199,12 @@ int rebuild_tiles(gcr_ctx *c)
         if (sl.desc.calc_wca)
             for (int64_t q = 0; q < sl.n_cells; q += tcl) c->h_cell_tiles.push_back(Tile{s, (int32_t)q});
     }
+    for (int s = 0; s < (int)c->slots.size(); s++) {
+        c->h_row_prefix[s] = (int)rows;
+        if (c->slots[s].used) rows += c->hP[s].n_row_tiles;
+    }
+    if (rows > INT32_MAX / 2) return fail(GCR_ERR_CAPACITY, "too many row tiles");
+    c->h_row_prefix[c->slots.size()] = (int)rows;
     GCR_CUDA(cudaMemcpyAsync(c->dP, c->hP.data(), sizeof(SysP) * c->hP.size(), cudaMemcpyHostToDevice,
                              c->stream));
     if ((int64_t)c->h_bead_tiles.size() > c->max_bead_tiles || (int64_t)c->h_cell_tiles.size() > c->max_cell_tiles)
@@ -203,6 +214,8 @@ int rebuild_tiles(gcr_ctx *c)
                                         cudaMemcpyHostToDevice, c->stream));
     if (nt[1]) GCR_CUDA(cudaMemcpyAsync(c->d_cell_tiles, c->h_cell_tiles.data(), nt[1] * sizeof(Tile),
                                         cudaMemcpyHostToDevice, c->stream));
+    GCR_CUDA(cudaMemcpyAsync(c->d_row_prefix, c->h_row_prefix.data(), c->h_row_prefix.size() * sizeof(int),
+                             cudaMemcpyHostToDevice, c->stream));
     GCR_CUDA(cudaMemcpyAsync(c->d_ntiles, nt, sizeof(nt), cudaMemcpyHostToDevice, c->stream));
     // the host arrays must outlive the asynchronous copies
     GCR_CUDA(cudaStreamSynchronize(c->stream));
@@ -250,6 +263,24 @@ int validate_desc(const gcr_config &cfg, const gcr_system_desc *d, int64_t *nc_o
     return GCR_OK;
 }
 
+// row tiles of the cell-staged pair kernel: segments of T cells of each
+// row of the GPU grid, T chosen so that a segment holds about one CTA's
+// worth (block_beads) of beads at the system's mean cell occupancy
+void row_tiling(const gcr_ctx *c, const gcr_system_desc &d, int64_t nc, SysP &p)
+{
+    p.row_cells = 0;
+    p.n_row_tiles = 0;
+    if (!d.calc_wca || p.fixed || nc < 3) return;
+    int64_t cells = 1, rows = 1;
+    for (int i = 0; i < c->cfg.dim; i++) cells *= nc;
+    for (int i = 1; i < c->cfg.dim; i++) rows *= nc;
+    const double per_cell = (double)d.n_beads / (double)cells;
+    int64_t T = (int64_t)std::floor((double)c->cfg.block_beads / std::max(per_cell, 1e-3));
+    T = std::max<int64_t>(1, std::min<int64_t>(T, c->ks.max_row_cells));
+    p.row_cells = (int32_t)T;
+    p.n_row_tiles = (int32_t)(rows * ((nc + T - 1) / T));
+}
+
 void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, double skin, SysP &p)
 {
     const gcr_system_desc &d = sl.desc;
@@ -273,6 +304,7 @@ void fill_sysp(const gcr_ctx *c, const Slot &sl, int64_t nc, double skin, SysP &
     p.n_cells = (int32_t)sl.n_cells;
     p.n_bead_tiles = (int32_t)((d.n_beads + c->cfg.block_beads - 1) / c->cfg.block_beads);
     p.n_cell_tiles = (int32_t)((sl.n_cells + c->cfg.block_cells - 1) / c->cfg.block_cells);
+    row_tiling(c, d, nc, p);
     p.L = d.L;
     p.half_L = d.L / 2.0;
     p.h = d.L / (double)nc;
@@ -504,14 +536,17 @@ int enqueue_step4(gcr_ctx *c)
     return c->graph_obs ? launch_observe(c) : GCR_OK;
 }
 
-// the SRK2 stage kernels sum the pair forces themselves (gcr_config.fuse_pair;
-// not with coupled populations, whose cross forces only k_pair adds)
-bool fused_pair(const gcr_ctx *c, bool cross) { return c->cfg.fuse_pair && c->cfg.srk_order == 2 && !cross; }
+// pair_mode of an SRK2 graph: 1 and 2 only without coupled populations,
+// whose cross forces only k_pair adds
+int pair_mode(const gcr_ctx *c, bool cross) { return (c->cfg.srk_order == 2 && !cross) ? c->cfg.pair_mode : 0; }
+bool fused_pair(const gcr_ctx *c, bool cross) { return pair_mode(c, cross) == 1; }
 
 // SRK2 stage s (0 predictor, 1 corrector): the pair forces, then the stage
 int enqueue_pair(gcr_ctx *c, int s, bool cross)
 {
-    if (fused_pair(c, cross)) return GCR_OK;
+    const int mode = pair_mode(c, cross);
+    if (mode == 1) return GCR_OK;
+    if (mode == 2) return launch(c, c->ks.pair_cells[s], c->grid_pair_cells, c->cfg.block_beads, c->pair_cells_smem);
     void *pair = cross ? c->ks.pair_cross[s] : (s == 0 ? c->ks.pair0 : c->ks.pair1);
     return launch(c, pair, c->grid_pair, c->cfg.block_beads);
 }
@@ -653,7 +688,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     if (cfg.list_depth == 0) cfg.list_depth = cfg.dim == 2 ? 32 : 96;
     if (cfg.list_depth < 4 || cfg.list_depth > 1024) return fail(GCR_ERR_BAD_ARG, "list_depth must be in [4, 1024]");
     if (cfg.srk_order == 0) cfg.srk_order = 2;
-    if (cfg.fuse_pair != 0 && cfg.fuse_pair != 1) return fail(GCR_ERR_BAD_ARG, "fuse_pair must be 0 or 1");
+    if (cfg.pair_mode < 0 || cfg.pair_mode > 2) return fail(GCR_ERR_BAD_ARG, "pair_mode must be 0, 1 or 2");
     if (cfg.srk_order != 2 && cfg.srk_order != 4) return fail(GCR_ERR_BAD_ARG, "srk_order must be 2 or 4");
 
     gcr_ctx *c = new (std::nothrow) gcr_ctx();
@@ -685,6 +720,8 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     e = e ? e : cudaMalloc(&c->d_bead_tiles, sizeof(Tile) * c->max_bead_tiles);
     e = e ? e : cudaMalloc(&c->d_cell_tiles, sizeof(Tile) * c->max_cell_tiles);
     e = e ? e : cudaMalloc(&c->d_ntiles, sizeof(int) * 2);
+    e = e ? e : cudaMalloc(&c->d_row_prefix, sizeof(int) * (size_t)(S + 1));
+    e = e ? e : cudaMemsetAsync(c->d_row_prefix, 0, sizeof(int) * (size_t)(S + 1), c->stream);
     e = e ? e : cudaMalloc(&c->topo, (size_t)cfg.bead_capacity);
     e = e ? e : cudaMalloc(&c->cnt, sizeof(int) * cells_alloc);
     e = e ? e : cudaMalloc(&c->ncell, sizeof(int) * cells_alloc);
@@ -734,6 +771,11 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     a.ncount = c->ncount;
     a.xref = c->xref;
     a.img = c->img;
+    a.row_prefix = c->d_row_prefix;
+    // staging capacity of the cell-staged pair kernel: twice the beads of a
+    // row tile and its neighbour rows at the mean occupancy (the row tiling
+    // aims at block_beads beads per row); a denser tile reads global memory
+    a.cell_stage_cap = 2 * c->ks.pair_cells_rows * cfg.block_beads;
     a.xi = c->xi;
     a.fp = c->fp;
     a.work = c->work;
@@ -760,6 +802,16 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     c->grid_stage1 = kernel_grid(c, c->ks.stage1, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
     c->grid_stage0f = kernel_grid(c, c->ks.stage0f, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
     c->grid_stage1f = kernel_grid(c, c->ks.stage1f, cfg.block_beads, c->max_bead_tiles, c->stage_smem);
+    c->pair_cells_smem = c->ks.pair_cells_smem(a.cell_stage_cap);
+    if (c->pair_cells_smem > 48 * 1024)
+        for (int k = 0; k < 2; k++)
+            cudaFuncSetAttribute(c->ks.pair_cells[k], cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)c->pair_cells_smem);
+    // row tiles: at most cells/3 rows, plus cells/T <= 2 beads/block_beads (or cells/128) segments
+    c->grid_pair_cells = kernel_grid(c, c->ks.pair_cells[0], cfg.block_beads,
+                                     cfg.cell_capacity / 3 + cfg.cell_capacity / 128 +
+                                         2 * cfg.bead_capacity / cfg.block_beads + S,
+                                     c->pair_cells_smem);
     c->grid_update = kernel_grid(c, c->ks.update, cfg.block_beads, c->max_bead_tiles);
     c->grid_pair = kernel_grid(c, c->ks.pair0, cfg.block_beads, c->max_bead_tiles);
     c->grid_bin = kernel_grid(c, c->ks.bin0, cfg.block_beads, c->max_bead_tiles);
@@ -776,7 +828,8 @@ int gcr_destroy(gcr_ctx *c)
     if (!c) return GCR_OK;
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
-    void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->topo, c->cnt, c->ncell,
+    void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->d_row_prefix, c->topo, c->cnt,
+                    c->ncell,
                     c->items, c->nbr, c->ncount, c->xref, c->work, c->xi, c->fp, c->chain_starts, c->d_err,
                     c->d_out, c->pos2, c->faux, c->xnbr, c->xcount, c->img};
     for (void *p : ptrs)

@@ -73,7 +73,7 @@ struct SysP {
     int32_t n_nearby;
     int32_t self_propel;
     int32_t rotate_prop;  // 2D and v_tan_angle != 0
-    int32_t pad0;
+    int32_t row_cells;    // cells of a row tile of the cell-staged pair kernel
     double v0, cos_a, sin_a;
     // noise / SRK
     double D, Dr, radius, sqrt2D;
@@ -90,7 +90,7 @@ struct SysP {
     int32_t n_cross;              // partner populations whose force it feels
     int32_t cross_q[kMaxPops - 1];  // partner slots, in the order the reference adds them
     int32_t cross_w[kMaxPops - 1];  // cells scanned either side in the partner's grid
-    int32_t pad1;
+    int32_t n_row_tiles;          // row tiles of the cell-staged pair kernel (0: no pair forces)
     double cross_p0[kMaxPops - 1], cross_p1[kMaxPops - 1], cross_shift[kMaxPops - 1];
     double cross_rc2[kMaxPops - 1], cross_rl2[kMaxPops - 1];
     int64_t x_off;                // first row of its cross lists

@@ -42,6 +42,11 @@ struct BatchArgs {
     // periodic images crossed by each bead since admission, int32 [bead][dim]
     // (the real updates count them; unwrapped = pos + L * img)
     int *img;
+    // row tiles of the cell-staged pair kernel: slot k owns tiles
+    // row_prefix[k] .. row_prefix[k+1]-1 (row_prefix[n_slots] = all tiles);
+    // tile r of a system is segment r % segments of row r / segments
+    const int *row_prefix;
+    int cell_stage_cap;  // beads a CTA of the cell-staged pair kernel copies into shared memory
 };
 
 struct KernelSet {
@@ -72,6 +77,10 @@ struct KernelSet {
     void *run_check;  // run start: flag the armed systems whose lists no longer cover their positions
     void *lists_plan;  // compact the systems that take part in a list build
     void *pair_cross[3];  // pair forces at pos / pos1 / pos2 with the other populations' (coupled systems)
+    void *pair_cells[2];  // cell-staged pair forces at pos / pos1 (pair_mode 2)
+    size_t (*pair_cells_smem)(int cap);  // their dynamic shared memory for `cap` staged beads
+    int pair_cells_rows;  // cell rows a row tile stages (3 in 2D, 9 in 3D)
+    int max_row_cells;    // cells of a row tile, at most
     size_t (*stage_smem)(int block_beads);  // dynamic shared memory of the stage kernels
 };
 

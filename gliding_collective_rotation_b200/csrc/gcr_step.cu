@@ -684,10 +684,37 @@ __device__ __forceinline__ void add_cross(const BatchArgs &A, const SysP &p, int
     }
 }
 
-// pair force on bead b over its neighbour list (forces.py:57-145, rule
-// forces.WCA): min-image separation of the FP64 positions X, rounded to FT,
-// then the rule in FT, added to F partner by partner in ascending id.  An
-// entry outside the system sets `bad` and is not used.
+// one pair of the rule forces.WCA (forces.py:57-145): min-image separation
+// of the FP64 positions xj - xb, rounded to FT, then the rule in FT, added to
+// F when 0 < r^2 <= r_cut^2 (with the optional shift rescale, 123-131)
+template <int D, typename FT>
+__device__ __forceinline__ void pair_term(const SysP &p, const double *xj, const double *xb, FT rc2, FT p0, FT p1,
+                                          FT shift, FT *F)
+{
+    FT sep[3];
+    FT ds = FT(0);
+#pragma unroll
+    for (int i = 0; i < D; i++) {
+        sep[i] = (FT)inbounds(xj[i], xb[i], p.half_L, p.L);
+        ds += sep[i] * sep[i];
+    }
+    if (!(FT(0) < ds && ds <= rc2)) return;
+    if (shift != FT(0)) {
+        FT mag = sqrt(ds);
+        FT nm = mag + shift;
+        nm = nm < FT(0) ? FT(0) : nm;
+        FT rs = nm / mag;
+#pragma unroll
+        for (int i = 0; i < D; i++) sep[i] *= rs;
+        ds = nm * nm;
+    }
+    FT coeff = wca_coeff<FT>(ds, p0, p1);
+#pragma unroll
+    for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
+}
+
+// pair force on bead b over its neighbour list, partner by partner in
+// ascending id.  An entry outside the system sets `bad` and is not used.
 template <int D, typename FT>
 __device__ __forceinline__ void list_pair_force(const BatchArgs &A, const SysP &p, const double *X,
                                                 const double *xb, int b, FT *F, bool &bad)
@@ -706,26 +733,7 @@ __device__ __forceinline__ void list_pair_force(const BatchArgs &A, const SysP &
             bad = true;
             continue;
         }
-        FT sep[3];
-        FT ds = FT(0);
-#pragma unroll
-        for (int i = 0; i < D; i++) {
-            sep[i] = (FT)inbounds(X[(size_t)j * D + i], xb[i], p.half_L, p.L);
-            ds += sep[i] * sep[i];
-        }
-        if (!(FT(0) < ds && ds <= rc2)) continue;
-        if (shift != FT(0)) {
-            FT mag = sqrt(ds);
-            FT nm = mag + shift;
-            nm = nm < FT(0) ? FT(0) : nm;
-            FT rs = nm / mag;
-#pragma unroll
-            for (int i = 0; i < D; i++) sep[i] *= rs;
-            ds = nm * nm;
-        }
-        FT coeff = wca_coeff<FT>(ds, p0, p1);
-#pragma unroll
-        for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
+        pair_term<D, FT>(p, X + (size_t)j * D, xb, rc2, p0, p1, shift, F);
     }
 }
 
@@ -758,6 +766,214 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_pair(BatchArgs A)
 #pragma unroll
         for (int i = 0; i < D; i++) fp[i] = F[i];
     }
+}
+
+// ------------------------------------------------------------------------
+// cell-staged pair forces (gcr_config.pair_mode = 2: SRK2 without coupled
+// populations).  Instead of each bead gathering its list partners, a CTA
+// takes a row tile -- the cells x0 .. x0+w-1 of one row (y, z) of a
+// system's GPU grid -- and copies the beads of those cells and of their
+// neighbour cells (3 rows in 2D, 9 in 3D; columns x0-1 .. x0+w) into shared
+// memory, bead ids and FP64 positions, compacted by a block-wide scan of the
+// cell counts.  Each bead of the tile then walks the beads of its 3^d
+// neighbour cells there.  The cells are those of the last list build: a
+// cell is at least r_cut + skin wide and no bead has moved skin/2 since, so
+// every pair within r_cut is among them (the argument that makes the lists
+// complete).  The pair sum runs cell by cell -- rows (dz, dy) ascending, then
+// the three columns, each cell in ascending id -- so it has the list walk's
+// pairs in another order: the forces differ from the list path's in FP
+// rounding only.  A tile with more beads than the staging capacity reads
+// the same beads from global memory in the same order.
+// ------------------------------------------------------------------------
+constexpr int kMaxRowCells = 128;
+
+// exclusive prefix sum of a[0..n) in shared memory, in place; returns the
+// total.  Every thread of the CTA calls it (blockDim.x a multiple of 32).
+__device__ int block_exclusive_scan(int *a, int n, int *warp_sums)
+{
+    const int per = (n + (int)blockDim.x - 1) / (int)blockDim.x;
+    const int lo = threadIdx.x * per, hi = min(n, lo + per);
+    int sum = 0;
+    for (int k = lo; k < hi; k++) sum += a[k];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    int x = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        int y = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int z = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += z;
+        }
+        if (lane < nw) warp_sums[lane] = y;  // inclusive prefix of the warp totals
+    }
+    __syncthreads();
+    int run = x - sum + (wid > 0 ? warp_sums[wid - 1] : 0);
+    const int total = warp_sums[nw - 1];
+    for (int k = lo; k < hi; k++) {
+        const int v = a[k];
+        a[k] = run;
+        run += v;
+    }
+    __syncthreads();
+    return total;
+}
+
+// largest q in [0, n) with off[q] <= k (off non-decreasing, off[0] <= k)
+__device__ __forceinline__ int cell_of_slot(const int *off, int n, int k)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= k)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int D, typename FT, int WHICH>
+__global__ void __launch_bounds__(512) k_pair_cells(BatchArgs A)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int R = D == 3 ? 9 : 3;  // rows of a tile with its neighbour rows
+    __shared__ int off[R * (kMaxRowCells + 2) + 1];
+    __shared__ int warp_sums[32];
+    __shared__ int sh_run;
+    const int cap = A.cell_stage_cap;
+    double *xs = reinterpret_cast<double *>(smem_raw);            // [cap][D]
+    int *ids = reinterpret_cast<int *>(xs + (size_t)cap * D);      // [cap]
+    const int nt = A.row_prefix[A.n_slots];
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const int sys = work_owner(A.row_prefix, A.n_slots, t);
+        const Tile tl{sys, t - A.row_prefix[sys]};
+        const SysP &p = A.P[tl.sys];
+        SysS &s = A.S[tl.sys];
+        __syncthreads();  // the previous tile is done with shared memory
+        // one decision per CTA (every thread must reach the same barriers)
+        if (threadIdx.x == 0)
+            sh_run = ld_volatile(&s.active) && !(ld_volatile(&s.flags) & kFlagFatal) && p.calc_wca;
+        __syncthreads();
+        if (!sh_run) continue;
+        const int nc = p.nc;
+        const int T = max(1, min(p.row_cells, kMaxRowCells));
+        const int segs = (nc + T - 1) / T;
+        const int row = tl.begin / segs;
+        const int x0 = (tl.begin - row * segs) * T;
+        const int w = min(T, nc - x0), W = w + 2;
+        const int ry = row % nc, rz = (D == 3) ? row / nc : 0;
+        // staged cell q = r W + c: row r = 3 (dz + 1) + (dy + 1), column x0 - 1 + c
+        auto cell_at = [&](int q) -> int64_t {
+            const int r = q / W, c = q - r * W;
+            int cx = x0 - 1 + c;
+            cx = cx < 0 ? cx + nc : (cx >= nc ? cx - nc : cx);
+            int cy = ry + (r % 3) - 1;
+            cy = cy < 0 ? cy + nc : (cy >= nc ? cy - nc : cy);
+            int cz = 0;
+            if (D == 3) {
+                cz = rz + r / 3 - 1;
+                cz = cz < 0 ? cz + nc : (cz >= nc ? cz - nc : cz);
+            }
+            return p.cell_off + ((int64_t)cz * nc + cy) * nc + cx;
+        };
+        const int nq = R * W;
+        for (int q = threadIdx.x; q < nq; q += blockDim.x) {
+            const int m = A.ncell[cell_at(q)];
+            off[q] = m < 0 ? 0 : (m < A.depth ? m : A.depth);
+        }
+        __syncthreads();
+        const int total = block_exclusive_scan(off, nq, warp_sums);
+        if (threadIdx.x == 0) off[nq] = total;
+        __syncthreads();
+        const bool staged = total <= cap;
+        const double *__restrict__ X = stage_x<WHICH>(p);
+        const int n = p.n;
+        bool bad = false;
+        if (staged) {
+            for (int k = threadIdx.x; k < total; k += blockDim.x) {
+                const int q = cell_of_slot(off, nq, k);
+                const int j = A.items[(cell_at(q) << A.log_depth) + (k - off[q])];
+                const bool ok = (unsigned)j < (unsigned)n;
+                bad |= !ok;
+                ids[k] = ok ? j : -1;
+#pragma unroll
+                for (int i = 0; i < D; i++) xs[(size_t)k * D + i] = ok ? X[(size_t)j * D + i] : 0.0;
+            }
+            __syncthreads();
+        }
+        // the tile's own beads: centre row (dz = dy = 0), columns 1 .. w
+        const int rmid = (R - 1) / 2;
+        const int i_lo = off[rmid * W + 1], i_hi = off[rmid * W + 1 + w];
+        const FT rc2 = (FT)p.rc2, p0 = (FT)p.p0, p1 = (FT)p.p1, shift = (FT)p.shift;
+        for (int k = i_lo + threadIdx.x; k < i_hi; k += blockDim.x) {
+            const int q = cell_of_slot(off, nq, k);
+            const int c = q - rmid * W;  // column of the bead's cell in the tile, 1 .. w
+            int b;
+            double xb[3] = {0.0, 0.0, 0.0};
+            if (staged) {
+                b = ids[k];
+            } else {
+                b = A.items[(cell_at(q) << A.log_depth) + (k - off[q])];
+            }
+            if ((unsigned)b >= (unsigned)n) {
+                bad = true;
+                continue;
+            }
+#pragma unroll
+            for (int i = 0; i < D; i++) xb[i] = staged ? xs[(size_t)k * D + i] : X[(size_t)b * D + i];
+            // excluded partners, as the list build excludes them
+            int ch = p.chain[b];
+            ch = ch < 0 ? 0 : (ch >= p.n_chains ? p.n_chains - 1 : ch);
+            const int c_lo = p.chain_start[ch], c_hi = p.chain_start[ch + 1] - 1;
+            const int nn = p.n_nearby;
+            const int ex_lo = nn < 0 ? c_lo : max(c_lo, b - nn);
+            const int ex_hi = nn < 0 ? c_hi : min(c_hi, b + nn);
+            FT F[3] = {FT(0), FT(0), FT(0)};
+            for (int r = 0; r < R; r++) {
+                const int q0 = r * W + c - 1;
+                if (staged) {
+                    const int k_hi = off[q0 + 3];
+                    for (int kk = off[q0]; kk < k_hi; kk++) {
+                        const int j = ids[kk];
+                        if (j < 0 || (j >= ex_lo && j <= ex_hi)) continue;
+                        pair_term<D, FT>(p, xs + (size_t)kk * D, xb, rc2, p0, p1, shift, F);
+                    }
+                } else {
+                    for (int cc = 0; cc < 3; cc++) {
+                        const int *it = A.items + (cell_at(q0 + cc) << A.log_depth);
+                        const int m = off[q0 + cc + 1] - off[q0 + cc];
+                        for (int kk = 0; kk < m; kk++) {
+                            const int j = it[kk];
+                            if ((unsigned)j >= (unsigned)n) {
+                                bad = true;
+                                continue;
+                            }
+                            if (j >= ex_lo && j <= ex_hi) continue;
+                            pair_term<D, FT>(p, X + (size_t)j * D, xb, rc2, p0, p1, shift, F);
+                        }
+                    }
+                }
+            }
+            FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
+#pragma unroll
+            for (int i = 0; i < D; i++) fp[i] = F[i];
+        }
+        if (bad) atomicOr(&s.flags, kFlagListCorrupt);
+    }
+}
+
+// dynamic shared memory of k_pair_cells for `cap` staged beads
+template <int D>
+size_t pair_cells_smem_bytes(int cap)
+{
+    return (size_t)cap * (D * sizeof(double) + sizeof(int));
 }
 
 template <int D, typename FT>
@@ -1485,6 +1701,8 @@ struct StepKernels {
     static void *stage1() { return (void *)k_stage<D, FT, 1>; }
     static void *stage0f() { return (void *)k_stage<D, FT, 0, true>; }
     static void *stage1f() { return (void *)k_stage<D, FT, 1, true>; }
+    static void *pair_cells0() { return (void *)k_pair_cells<D, FT, 0>; }
+    static void *pair_cells1() { return (void *)k_pair_cells<D, FT, 1>; }
     static void *update() { return (void *)k_update<D, FT>; }
     static void *rigid0() { return (void *)k_rigid<D, FT, 0>; }
     static void *rigid1() { return (void *)k_rigid<D, FT, 1>; }
@@ -1512,6 +1730,9 @@ KernelSet kernel_set(int dim, int precision)
         k.stage_smem = precision == 0 ? stage_smem_bytes<2, double> : stage_smem_bytes<2, float>;
     else
         k.stage_smem = precision == 0 ? stage_smem_bytes<3, double> : stage_smem_bytes<3, float>;
+    k.pair_cells_smem = dim == 2 ? pair_cells_smem_bytes<2> : pair_cells_smem_bytes<3>;
+    k.pair_cells_rows = dim == 2 ? 3 : 9;
+    k.max_row_cells = kMaxRowCells;
 #define GCR_FILL(D_, FT_)                       \
     k.pair0 = StepKernels<D_, FT_>::pair0();    \
     k.pair1 = StepKernels<D_, FT_>::pair1();    \
@@ -1519,6 +1740,8 @@ KernelSet kernel_set(int dim, int precision)
     k.stage1 = StepKernels<D_, FT_>::stage1();  \
     k.stage0f = StepKernels<D_, FT_>::stage0f(); \
     k.stage1f = StepKernels<D_, FT_>::stage1f(); \
+    k.pair_cells[0] = StepKernels<D_, FT_>::pair_cells0(); \
+    k.pair_cells[1] = StepKernels<D_, FT_>::pair_cells1(); \
     k.update = StepKernels<D_, FT_>::update();  \
     k.rigid0 = StepKernels<D_, FT_>::rigid0();  \
     k.rigid1 = StepKernels<D_, FT_>::rigid1();  \

@@ -136,7 +136,7 @@ class SystemState:
 
 def default_config(dim, precision="fp64", bead_capacity=1 << 20, system_capacity=1,
                    cell_capacity=None, cell_depth=None, block_beads=256, block_cells=256,
-                   steps_per_graph=10, ctas_per_sm=0, list_depth=0, srk_order=2, fuse_pair=0):
+                   steps_per_graph=10, ctas_per_sm=0, list_depth=0, srk_order=2, pair_mode=0):
     cfg = Config()
     cfg.dim = dim
     cfg.precision = PRECISIONS[precision]
@@ -152,8 +152,11 @@ def default_config(dim, precision="fp64", bead_capacity=1 << 20, system_capacity
     if srk_order not in (2, 4):
         raise ValueError("srk_order must be 2 or 4")
     cfg.srk_order = int(srk_order)
-    # the stage kernels sum the pair forces themselves (same bits; chosen by measurement)
-    cfg.fuse_pair = 1 if fuse_pair else 0
+    # pair forces: 0 list kernel, 1 list walk inside the stage kernels (same
+    # bits), 2 cell-staged kernel (same pairs, another summation order)
+    if pair_mode not in (0, 1, 2):
+        raise ValueError("pair_mode must be 0, 1 or 2")
+    cfg.pair_mode = int(pair_mode)
     return cfg
 
 

@@ -86,9 +86,14 @@ typedef struct {
     int32_t ctas_per_sm;      /* persistent CTAs per SM (0 = from occupancy, <0 = one CTA per tile) */
     int32_t list_depth;       /* neighbour-list slots per bead, 4..1024 (0 = 32 in 2D, 96 in 3D) */
     int32_t srk_order;        /* config.SRK_order: 2 (0 = 2) or 4 (SRK.py:144-215, 296-321) */
-    int32_t fuse_pair;        /* 1: the stage kernels sum the pair forces themselves instead of a
-                                 separate pair launch per stage (SRK2 while no system is coupled to
-                                 another population; same results bit for bit); 0: separate */
+    int32_t pair_mode;        /* pair forces of SRK2 contexts while no system is coupled to another
+                                 population (SRK4 and coupled systems always use 0):
+                                 0: a pair kernel walks each bead's neighbour list;
+                                 1: the stage kernels walk the lists themselves (no pair launch;
+                                    the same bits as 0);
+                                 2: a cell-staged pair kernel: each CTA copies a row of cells and
+                                    its neighbour cells into shared memory and sums over them (the
+                                    same pairs as 0, summed cell by cell: FP rounding differs) */
 } gcr_config;
 
 /* One system.  The packed arrays follow the reference's packing exactly. */

@@ -31,6 +31,11 @@ import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB_PATH = os.path.join(_HERE, "libgcr_oracle.so")
+# the same restatement compiled with FMA contraction (a * b + c fused, as
+# nvcc does by default): a second valid FP64 evaluation of every step whose
+# divergence from the first measures how sensitive a trajectory is to
+# rounding (tests only; it needs a CPU with FMA and AVX2)
+_FMA_LIB_PATH = os.path.join(_HERE, "libgcr_oracle_fma.so")
 
 NOISE_MT, NOISE_INJECT, NOISE_PHILOX = 0, 1, 2
 
@@ -79,7 +84,17 @@ class Result(C.Structure):
                 ("flag", C.c_double)]
 
 
-_lib = None
+_libs = {}
+
+
+def fma_available():
+    """The host CPU runs the contracted build (x86-64-v3: FMA and AVX2)."""
+    try:
+        with open("/proc/cpuinfo") as fh:
+            flags = next((ln.split(":", 1)[1].split() for ln in fh if ln.startswith("flags")), [])
+    except OSError:
+        return False
+    return "fma" in flags and "avx2" in flags
 
 
 def build():
@@ -87,12 +102,16 @@ def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(_LIB_PATH):
+def lib(variant=""):
+    """The oracle library: ``""`` the reference's arithmetic (no
+    contraction), ``"fma"`` the contracted control build."""
+    if variant not in _libs:
+        path = {"": _LIB_PATH, "fma": _FMA_LIB_PATH}[variant]
+        if variant == "fma" and not fma_available():
+            raise RuntimeError("the contracted oracle needs a CPU with FMA and AVX2")
+        if not os.path.exists(path):
             build()
-        L = C.CDLL(_LIB_PATH)
+        L = C.CDLL(path)
         L.gcro_srk2_run.restype = C.c_int
         L.gcro_srk2_run.argtypes = [C.POINTER(Params), C.POINTER(State), C.POINTER(Result)]
         L.gcro_mt_seed.argtypes = [C.POINTER(MT), C.c_uint32]
@@ -127,8 +146,8 @@ def lib():
         assert L.gcro_sizeof_params() == C.sizeof(Params)
         assert L.gcro_sizeof_state() == C.sizeof(State)
         assert L.gcro_sizeof_mt() == C.sizeof(MT)
-        _lib = L
-    return _lib
+        _libs[variant] = L
+    return _libs[variant]
 
 
 def _p(a):
@@ -246,7 +265,8 @@ class OracleSystem:
     def __init__(self, pos, tangent, chain_id, rest_lengths, L, spring_params, wca_params,
                  active_params, D, Dr, radius, n_nearby, n_grid, grid_factor=2.0,
                  calc_springs=True, calc_wca=True, self_propel=True, grid_depth=None,
-                 nbor_depth=8, rigid_rod=0.0, srk_order=2):
+                 nbor_depth=8, rigid_rod=0.0, srk_order=2, variant=""):
+        self.variant = variant  # oracle library: "" or "fma" (see lib())
         self.pos = np.ascontiguousarray(pos, dtype=np.float64).copy()
         self.N, self.dim = self.pos.shape
         self.pos1 = np.zeros_like(self.pos)
@@ -301,7 +321,7 @@ class OracleSystem:
     def seed_mt(self, seed, n_threads=1):
         """Seed the per-thread MT19937 streams (thread t gets seed + t)."""
         for t in range(min(n_threads, 64)):
-            lib().gcro_mt_seed(C.byref(self.mt[t]), (seed + t) & 0xFFFFFFFF)
+            lib(self.variant).gcro_mt_seed(C.byref(self.mt[t]), (seed + t) & 0xFFFFFFFF)
 
     def set_injected_noise(self, snapshots):
         self._inject = np.ascontiguousarray(snapshots, dtype=np.float64)
@@ -309,7 +329,7 @@ class OracleSystem:
     # -- list construction -------------------------------------------------
     def build_lists(self, grid_window=None):
         """Initial lists as ``configure_start`` builds them (control.py:116-150)."""
-        L = lib()
+        L = lib(self.variant)
         while True:
             st = self._state()
             if L.gcro_update_grid_list(C.byref(st), _p(self.pos), self.N, self.L, self.dim, 0, 1, 0):
@@ -340,7 +360,7 @@ class OracleSystem:
         p.seed, p.step0 = seed, step0
         res = Result()
         st = self._state()
-        rc = lib().gcro_srk2_run(C.byref(p), C.byref(st), C.byref(res))
+        rc = lib(self.variant).gcro_srk2_run(C.byref(p), C.byref(st), C.byref(res))
         if rc != 0:
             raise RuntimeError(f"oracle srk2 run failed ({rc})")
         return {"dt": res.dt, "dt_used": res.dt_used_total, "steps": int(res.steps),

@@ -18,7 +18,7 @@ def _fake(best):
 
 
 def test_search_finds_the_minimum_of_a_separable_cost():
-    best = {"block_beads": 256, "ctas_per_sm": 4, "steps_per_graph": 20, "skin_scale": 0.67, "fuse_pair": 1}
+    best = {"block_beads": 256, "ctas_per_sm": 4, "steps_per_graph": 20, "skin_scale": 0.67, "pair_mode": 1}
     shape, ms, trials = autotune.search(_fake(best))
     assert shape == best and ms == 1.0
     # coordinate descent: far fewer runs than the full grid
@@ -51,9 +51,9 @@ def test_signature_separates_workloads():
 
 def test_apply_scales_the_skin_and_keeps_the_physics():
     specs = config3(n_systems=3, param_seed=2)
-    res = {"block_beads": 64, "ctas_per_sm": 2, "steps_per_graph": 5, "skin_scale": 1.5, "fuse_pair": 1}
+    res = {"block_beads": 64, "ctas_per_sm": 2, "steps_per_graph": 5, "skin_scale": 1.5, "pair_mode": 1}
     out, kw = autotune.apply(specs, res)
-    assert kw == {"block_beads": 64, "ctas_per_sm": 2, "steps_per_graph": 5, "fuse_pair": 1}
+    assert kw == {"block_beads": 64, "ctas_per_sm": 2, "steps_per_graph": 5, "pair_mode": 1}
     from gliding_collective_rotation_b200.engine import default_skin
     for s, o in zip(specs, out):
         assert o.params.skin == default_skin(s.params.wca_params[3]) * 1.5

@@ -40,10 +40,10 @@ def test_every_shape_gives_the_same_trajectory(precision):
     kernels sum the pair forces themselves change no bit of a trajectory."""
     specs = _specs(4)
     out = []
-    for res in ({"block_beads": 128, "ctas_per_sm": 0, "steps_per_graph": 10, "skin_scale": 1.0, "fuse_pair": 0},
-                {"block_beads": 64, "ctas_per_sm": 2, "steps_per_graph": 5, "skin_scale": 1.5, "fuse_pair": 1},
-                {"block_beads": 256, "ctas_per_sm": 4, "steps_per_graph": 20, "skin_scale": 0.67, "fuse_pair": 0},
-                {"block_beads": 128, "ctas_per_sm": 0, "steps_per_graph": 10, "skin_scale": 1.0, "fuse_pair": 1}):
+    for res in ({"block_beads": 128, "ctas_per_sm": 0, "steps_per_graph": 10, "skin_scale": 1.0, "pair_mode": 0},
+                {"block_beads": 64, "ctas_per_sm": 2, "steps_per_graph": 5, "skin_scale": 1.5, "pair_mode": 1},
+                {"block_beads": 256, "ctas_per_sm": 4, "steps_per_graph": 20, "skin_scale": 0.67, "pair_mode": 0},
+                {"block_beads": 128, "ctas_per_sm": 0, "steps_per_graph": 10, "skin_scale": 1.0, "pair_mode": 1}):
         sp, kw = autotune.apply(specs, res)
         b = Batch(sp, precision=precision, **kw)
         b.set_adaptive(True)

@@ -9,18 +9,22 @@ the oracle (the reference's step restated in C, same Philox stream, the
 reference's 40-step Verlet lists and its own summation order) advances each
 from the same state under the reference's adaptive dt rule.
 
-These dense systems are chaotic right after relaxation: two FP64 runs of the
-oracle itself, one started from positions one ulp away, drift apart by about
-a decade every 10-20 steps (1e-16 of the box after one step, 1e-10 after 50,
-order one after a few hundred).  Rounding differences between any two
-correct FP64 implementations grow the same way, so past the first steps the
-bound is that control, not a fixed number: at every checkpoint where the
-one-ulp control is still below 1e-6 of the box (the linear regime), the GPU
-must be within 1e-13 of the box or 100 times the control's own divergence,
-and its dt within 1e-12 relative or 100 times the control's dt difference.
-Past the linear regime no trajectory comparison means anything (the
-statistics tests cover that regime); every system is required to stay in
-the linear regime for at least its first two checkpoints (1 and 10 steps).
+These dense systems are chaotic right after relaxation, and the reference's
+bend force acos(c)/sqrt(1 - c^2) of nearly straight chains turns last-bit
+differences of c into relative differences of ~1e-8 in the force.  Two
+valid FP64 evaluations of the same step therefore drift apart: the oracle
+compiled with FMA contraction (as nvcc contracts) against the oracle
+without it, from the same state, differ by ~1e-16 of the box after one
+step, ~1e-9 after 50 and ~1e-3 after 200 (measured on a 924-bead sweep
+system).  So past the first step the bound is that control, not a fixed
+number: at every checkpoint where the contracted oracle is still within
+1e-6 of the box of the plain one (the linear regime), the GPU must be within
+1e-13 of the box or 100 times the control's divergence, and its dt within
+1e-12 relative after the first step (1e-9 later) or 100 times the control's
+dt difference.  Past the linear regime no trajectory comparison means
+anything (the statistics tests cover that regime); every system must stay
+in the linear regime for at least its first two checkpoints (1 and 10
+steps).
 """
 import math
 
@@ -62,17 +66,12 @@ def _countdown(until, n):
     return N_UPDATE - (n - until) % N_UPDATE
 
 
-def _one_ulp(pos):
-    """Positions one ulp toward zero (a position of exactly 0 is kept)."""
-    return np.where(pos > 0, np.nextafter(pos, -np.inf), pos)
-
-
 LINEAR = 1e-6   # control divergence (fraction of the box) up to which the trajectories are compared
 FLOOR = 1e-13   # absolute floor of the position bound (fraction of the box)
-DT_FLOOR = 1e-12
 FACTOR = 100.0
 
 
+@pytest.mark.skipif(not O.fma_available(), reason="the contracted oracle needs FMA and AVX2 on the host")
 def test_sweep_systems_match_the_oracle():
     specs = W.config3(n_systems=256, param_seed=12345)
     idx = pick_systems(specs)
@@ -93,10 +92,10 @@ def test_sweep_systems_match_the_oracle():
         ng = max(1, int(p.L / (2.0 * max(2 * a, rc))))
         window = max(1, math.ceil(max(2 * a, rc) / (p.L / ng)))
         pos = st.pos.cpu().numpy()
-        for start, out in ((pos, oracles), (_one_ulp(pos), controls)):
-            o = O.OracleSystem(start, st.tangent.cpu().numpy(), sp.chain_id, sp.rest_lengths, p.L,
+        for variant, out in (("", oracles), ("fma", controls)):
+            o = O.OracleSystem(pos, st.tangent.cpu().numpy(), sp.chain_id, sp.rest_lengths, p.L,
                                p.spring_params, p.wca_params, p.active_params, p.D, p.Dr, p.radius, p.n_nearby,
-                               ng, nbor_depth=64)
+                               ng, nbor_depth=64, variant=variant)
             o.build_lists(grid_window=window)
             out.append(o)
     until = [N_UPDATE] * len(sel)
@@ -125,10 +124,14 @@ def test_sweep_systems_match_the_oracle():
             report.append(row)
             if ctrl < LINEAR:
                 compared[sp.name].append(done + n_steps)
-                if err > max(FLOOR, FACTOR * ctrl) or dt_err > max(DT_FLOOR, FACTOR * dt_ctrl):
+                dt_floor = 1e-12 if done == 0 else 1e-9
+                if err > max(FLOOR, FACTOR * ctrl) or dt_err > max(dt_floor, FACTOR * dt_ctrl):
                     bad.append(row)
         done += n_steps
     b.close()
-    assert not bad, (bad, report)
+    print("system beads steps err/L control/L dt_err dt_control")
+    for row in report:
+        print("%s %d %d %.3e %.3e %.3e %.3e" % row)
+    assert not bad, bad
     short = {k: v for k, v in compared.items() if v[:2] != [1, 10]}
     assert not short, ("left the linear regime within 10 steps", short, report)
