@@ -49,7 +49,7 @@ CASES = {
 
 
 def _relaxed(specs):
-    b = Batch(specs, precision="fp64")
+    b = Batch(specs, precision="fp64", cell_depth=64, list_depth=256)
     b.relax(max_steps=600, adaptive_after=True)
     out = [dataclasses.replace(sp, pos=st.pos.cpu().numpy(), tangent=st.tangent.cpu().numpy())
            for sp, st in zip(specs, b.states)]
@@ -58,8 +58,9 @@ def _relaxed(specs):
 
 
 def _run(specs, precision, steps, **kw):
+    # lists and cells deep enough for the LJ clusters (no regrow inside the comparison)
     b = Batch([dataclasses.replace(s, params=dataclasses.replace(s.params)) for s in specs],
-              precision=precision, **kw)
+              precision=precision, cell_depth=64, list_depth=256, **kw)
     b.set_adaptive(True)
     b.begin(steps)
     b.run(steps)
