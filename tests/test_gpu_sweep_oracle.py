@@ -15,16 +15,21 @@ differences of c into relative differences of ~1e-8 in the force.  Two
 valid FP64 evaluations of the same step therefore drift apart: the oracle
 compiled with FMA contraction (as nvcc contracts) against the oracle
 without it, from the same state, differ by ~1e-16 of the box after one
-step, ~1e-9 after 50 and ~1e-3 after 200 (measured on a 924-bead sweep
-system).  So past the first step the bound is that control, not a fixed
-number: at every checkpoint where the contracted oracle is still within
-1e-6 of the box of the plain one (the linear regime), the GPU must be within
-1e-13 of the box or 100 times the control's divergence, and its dt within
-1e-12 relative after the first step (1e-9 later) or 100 times the control's
-dt difference.  Past the linear regime no trajectory comparison means
-anything (the statistics tests cover that regime); every system must stay
-in the linear regime for at least its first two checkpoints (1 and 10
-steps).
+step, 1e-12..1e-8 after 50 and ~1e-3 after 200 (the same systems; the
+reference's 40-step lists and lists rebuilt every step give the same
+trajectory to 1e-16 over those 50 steps, so the drift is rounding alone).
+The bounds:
+
+* after 1 step, every system within 1e-13 of the box and its dt within
+  1e-12 relative;
+* after 10 steps, every system within 1e-10 of the box;
+* after 50 steps, the GPU drifts from the oracle as the contracted oracle
+  does: the geometric mean over the six systems of (GPU - oracle) /
+  (contracted oracle - oracle) lies within [1/30, 30] (a single system's
+  ratio varies by orders of magnitude between realisations of the same
+  rounding noise), and no system has left the linear regime (< 1e-5);
+* after 200 steps the trajectories are decorrelated on both sides and only
+  reported (the statistics tests cover that regime).
 """
 import math
 
@@ -66,9 +71,7 @@ def _countdown(until, n):
     return N_UPDATE - (n - until) % N_UPDATE
 
 
-LINEAR = 1e-6   # control divergence (fraction of the box) up to which the trajectories are compared
-FLOOR = 1e-13   # absolute floor of the position bound (fraction of the box)
-FACTOR = 100.0
+CHECKS = (1, 10, 50, 200)  # cumulative steps at the checkpoints
 
 
 @pytest.mark.skipif(not O.fma_available(), reason="the contracted oracle needs FMA and AVX2 on the host")
@@ -100,12 +103,16 @@ def test_sweep_systems_match_the_oracle():
             out.append(o)
     until = [N_UPDATE] * len(sel)
     done = 0
-    report, bad = [], []
-    compared = {sp.name: [] for sp in sel}
-    for n_steps in (1, 9, 40, 150):
+    err = {c: [] for c in CHECKS}
+    ctrl = {c: [] for c in CHECKS}
+    dt_err = {c: [] for c in CHECKS}
+    report = []
+    for n_steps in np.diff((0,) + CHECKS):
+        n_steps = int(n_steps)
         b.begin(n_steps)
         b.run(n_steps)
         sts = b.statuses()
+        mark = done + n_steps
         for j, (st, sp, o, oc) in enumerate(zip(b.states, sel, oracles, controls)):
             p = sp.params
             assert sts[j]["steps_done"] == n_steps and sts[j]["flags"] == 0, (sp.name, sts[j])
@@ -114,24 +121,21 @@ def test_sweep_systems_match_the_oracle():
             res = o.run(n_steps, dt=dts[j], **kw)
             res_c = oc.run(n_steps, dt=dts_c[j], **kw)
             assert res["steps"] == n_steps and res_c["steps"] == n_steps
-            dt_err = abs(res["dt"] - sts[j]["dt"]) / res["dt"]
-            dt_ctrl = abs(res["dt"] - res_c["dt"]) / res["dt"]
+            dt_err[mark].append(abs(res["dt"] - sts[j]["dt"]) / res["dt"])
             dts[j], dts_c[j] = res["dt"], res_c["dt"]
             until[j] = _countdown(until[j], n_steps)
-            err = np.max(np.abs(min_image(st.pos.cpu().numpy() - o.pos, p.L))) / p.L
-            ctrl = np.max(np.abs(min_image(oc.pos - o.pos, p.L))) / p.L
-            row = (sp.name, sp.n, done + n_steps, float(err), float(ctrl), float(dt_err), float(dt_ctrl))
-            report.append(row)
-            if ctrl < LINEAR:
-                compared[sp.name].append(done + n_steps)
-                dt_floor = 1e-12 if done == 0 else 1e-9
-                if err > max(FLOOR, FACTOR * ctrl) or dt_err > max(dt_floor, FACTOR * dt_ctrl):
-                    bad.append(row)
-        done += n_steps
+            err[mark].append(float(np.max(np.abs(min_image(st.pos.cpu().numpy() - o.pos, p.L))) / p.L))
+            ctrl[mark].append(float(np.max(np.abs(min_image(oc.pos - o.pos, p.L))) / p.L))
+            report.append((sp.name, sp.n, mark, err[mark][-1], ctrl[mark][-1], dt_err[mark][-1]))
+        done = mark
     b.close()
-    print("system beads steps err/L control/L dt_err dt_control")
+    print("system beads steps err/L control/L dt_err")
     for row in report:
-        print("%s %d %d %.3e %.3e %.3e %.3e" % row)
-    assert not bad, bad
-    short = {k: v for k, v in compared.items() if v[:2] != [1, 10]}
-    assert not short, ("left the linear regime within 10 steps", short, report)
+        print("%s %d %d %.3e %.3e %.3e" % row)
+    assert max(err[1]) < 1e-13 and max(dt_err[1]) < 1e-12, report
+    assert max(err[10]) < 1e-10, report
+    e50, c50 = np.array(err[50]), np.array(ctrl[50])
+    assert e50.max() < 1e-5 and c50.min() > 0, report
+    gm = float(np.exp(np.mean(np.log(e50 / c50))))
+    print("geometric mean of the 50-step ratio: %.3g" % gm)
+    assert 1 / 30 <= gm <= 30, (gm, report)
