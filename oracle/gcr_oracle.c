@@ -163,6 +163,25 @@ GCRO_EXPORT void gcro_philox_pair(uint64_t seed, uint32_t bead, int64_t step, ui
     out[1] = rad * sin(ang);
 }
 
+/* Two uniforms in [0, 1) for the motor decisions of (motor, bead) at a
+ * stage of a step (53 bits each, as the normals above): u[0] for k_off,
+ * u[1] for k_on.  Keyed Philox stands in for the reference's sequential
+ * np.random.random() draws (forces.py:268, 275), which nothing seeds. */
+GCRO_EXPORT void gcro_motor_uniforms(uint64_t seed, uint32_t motor, uint32_t bead, int64_t step, int stage,
+                                     double u[2])
+{
+    uint32_t ctr[4] = {motor, bead, (uint32_t)((uint64_t)step & 0xffffffffu),
+                       ((uint32_t)((uint64_t)step >> 32) & 0xffffu) | ((uint32_t)stage << 16)};
+    uint32_t key[2] = {(uint32_t)(seed & 0xffffffffu) ^ 0x6d6f746fu, (uint32_t)(seed >> 32)};
+    uint32_t r[4];
+    philox4x32_10(ctr, key, r);
+    const double two_m53 = 1.1102230246251565e-16;
+    uint64_t a = (((uint64_t)r[0] << 21) ^ (uint64_t)(r[1] >> 11)) & (((uint64_t)1 << 53) - 1);
+    uint64_t b = (((uint64_t)r[2] << 21) ^ (uint64_t)(r[3] >> 11)) & (((uint64_t)1 << 53) - 1);
+    u[0] = (double)a * two_m53;
+    u[1] = (double)b * two_m53;
+}
+
 /* Fill noise_vec [N, 2*dim] for one step from the Philox stream.
  * Translational components use streams 0..; rotational ones 2... */
 GCRO_EXPORT void gcro_philox_noise(uint64_t seed, int64_t step, int dim, int64_t n,
@@ -1195,6 +1214,80 @@ GCRO_EXPORT void gcro_pair_forces_all(const double *XP, int64_t nP, const int64_
     pair_forces_all(XP, nP, chainP, n_nearby, XQ, nQ, same, wp, L, dim, F);
 }
 
+/* ------------------------------------------------------------------ */
+/* Motors: forces.calc_motor_push (forces.py:248-283), the motor        */
+/* parameters of Chain_Collection.interactions (populations.py:276-287) */
+/* and the diffusion of Motor_Population (SRK.py:389-395)                */
+/* ------------------------------------------------------------------ */
+
+/* params = [motor_max_dist_sq, b_one_motor_per_bead, imparts_force, k_on,
+ * k_off].  The reference's loop as written: beads in order, each bead's
+ * motor neighbours in its list's order (nbor rows [count, ids...]); an
+ * attached motor stays with probability 1 - k_off (and then adds nothing),
+ * else it detaches -- whichever bead it was attached to, the count of the
+ * bead that drew is decremented -- and a free motor attaches with
+ * probability k_on when within motor_max_dist, adding imparts_force times
+ * the bead's tangent.  b_one_motor_per_bead ends the inner loop's body with
+ * `continue` and so changes nothing.  Draws come from the MT19937 stream
+ * `mt` in the reference's order (np.random.random, forces.py:268, 275). */
+GCRO_EXPORT void gcro_motor_push_mt(const double *pos_b, int64_t nb, const int64_t *nbor, int64_t nbd1,
+                                    double *forces_b, int64_t *where_active_b, const double *tangent, double L,
+                                    const double *pos_m, int64_t *where_active_m, const double *params, gcro_mt *mt,
+                                    int dim)
+{
+    const double half_L = L / 2.0;
+    double seps[3];
+    for (int64_t bi = 0; bi < nb; bi++) {
+        const int64_t *row = nbor + bi * nbd1;
+        for (int64_t k = 0; k < row[0]; k++) {
+            const int64_t mi = row[1 + k];
+            if (where_active_m[mi] >= 0) {
+                if (mt_double(mt) > params[4]) continue;
+                where_active_m[mi] = -1;
+                where_active_b[bi] -= 1;
+            }
+            if (where_active_m[mi] < 0) {
+                if (mt_double(mt) < params[3]) {
+                    double ds = inbounds_diff(pos_m + mi * dim, pos_b + bi * dim, half_L, L, seps, dim);
+                    if (ds <= params[0]) {
+                        where_active_b[bi] += 1;
+                        where_active_m[mi] = bi;
+                        for (int i = 0; i < dim; i++) forces_b[bi * dim + i] += params[2] * tangent[bi * dim + i];
+                    }
+                }
+            }
+        }
+    }
+}
+
+/* The same loop over every bead and every motor within sqrt(list_r2) of it
+ * (the beads whose list holds the motor), in ascending motor id, with the
+ * keyed draws of gcro_motor_uniforms(seed, motor, bead, step, stage). */
+static void motor_push_keyed(const double *pos_b, int64_t nb, double *forces_b, int32_t *act_b,
+                             const double *tangent, double L, const double *pos_m, int64_t nm, int32_t *act_m,
+                             const double *params, double list_r2, uint64_t seed, int64_t step, int stage, int dim)
+{
+    const double half_L = L / 2.0;
+    double seps[3], u[2];
+    for (int64_t bi = 0; bi < nb; bi++) {
+        for (int64_t mi = 0; mi < nm; mi++) {
+            double ds = inbounds_diff(pos_m + mi * dim, pos_b + bi * dim, half_L, L, seps, dim);
+            if (!(ds <= list_r2)) continue;
+            gcro_motor_uniforms(seed, (uint32_t)mi, (uint32_t)bi, step, stage, u);
+            if (act_m[mi] >= 0) {
+                if (u[0] > params[4]) continue;
+                act_m[mi] = -1;
+                act_b[bi] -= 1;
+            }
+            if (act_m[mi] < 0 && u[1] < params[3] && ds <= params[0]) {
+                act_b[bi] += 1;
+                act_m[mi] = (int32_t)bi;
+                for (int i = 0; i < dim; i++) forces_b[bi * dim + i] += params[2] * tangent[bi * dim + i];
+            }
+        }
+    }
+}
+
 /* n_pops populations: ps[k] / sts[k] as gcro_srk2_run takes them (one
  * thread each; the lists of sts[k] are not used), fixed[k] (pop.fixed: never
  * moves, feels nothing, acts on the others), cross[(k*n + q)*4 + 0..3] the
@@ -1206,8 +1299,46 @@ GCRO_EXPORT void gcro_pair_forces_all(const double *XP, int64_t nP, const int64_
  * gcro_srk2_run (0: sts[k]->mt[0], 1: injected, 2: Philox with ps[k]->seed).
  * out->max_forces_strength is the first moving population's own value
  * (shared_arr[0, 3], the thread of the first population pair). */
+/* A motor population in a group (Motor_Population pushing Chain_Collection
+ * `chain_pop`): where_active of every population is reset to -1 at the start
+ * of each step (SRK.py:132), the chains get the motor push of each stage as
+ * the force of the other population (SRK.py:261-267), and with dont_diffuse
+ * an attached motor keeps its position in the stage's update (SRK.py:389-395:
+ * after a predictor its pos1 keeps the previous value). */
+typedef struct {
+    int32_t motor_pop, chain_pop;
+    int32_t dont_diffuse;
+    int32_t pad;
+    double params[5]; /* [motor_max_dist_sq, b_one_motor_per_bead, imparts_force, k_on, k_off] */
+    double list_r2;   /* a motor is on the list of the beads within sqrt(list_r2) */
+    int32_t *act[8];  /* where_active of each population, int32 [n_beads] */
+} gcro_motors;
+
+static int group_run(int n_pops, const gcro_params *const *ps, gcro_state *const *sts, const int32_t *fixed,
+                     const double *cross, const gcro_params *g, gcro_result *out, const gcro_motors *mo);
+
 GCRO_EXPORT int gcro_group_run(int n_pops, const gcro_params *const *ps, gcro_state *const *sts,
                                const int32_t *fixed, const double *cross, const gcro_params *g, gcro_result *out)
+{
+    return group_run(n_pops, ps, sts, fixed, cross, g, out, NULL);
+}
+
+/* gcro_group_run with a motor population (SRK2, Philox noise and draws) */
+GCRO_EXPORT int gcro_group_run_motors(int n_pops, const gcro_params *const *ps, gcro_state *const *sts,
+                                      const int32_t *fixed, const double *cross, const gcro_params *g,
+                                      gcro_result *out, const gcro_motors *mo)
+{
+    if (!mo || g->srk_order == 4 || g->noise_mode != 2) return -3;
+    if (mo->motor_pop < 0 || mo->motor_pop >= n_pops || mo->chain_pop < 0 || mo->chain_pop >= n_pops ||
+        mo->motor_pop == mo->chain_pop)
+        return -1;
+    return group_run(n_pops, ps, sts, fixed, cross, g, out, mo);
+}
+
+GCRO_EXPORT int gcro_sizeof_motors(void) { return (int)sizeof(gcro_motors); }
+
+static int group_run(int n_pops, const gcro_params *const *ps, gcro_state *const *sts, const int32_t *fixed,
+                     const double *cross, const gcro_params *g, gcro_result *out, const gcro_motors *mo)
 {
     if (n_pops < 1 || n_pops > 8) return -1;
     const int dim = g->dim;
@@ -1231,6 +1362,9 @@ GCRO_EXPORT int gcro_group_run(int n_pops, const gcro_params *const *ps, gcro_st
     double dt = g->dt, elapsed = 0.0, mfs0 = 0.0;
     int64_t steps = 0;
     while ((steps < g->max_steps || g->max_steps < 0) && (elapsed < g->max_dt_usable || g->max_dt_usable < 0)) {
+        if (mo)
+            for (int k = 0; k < n_pops; k++)
+                for (int64_t b = 0; b < ps[k]->n_beads; b++) mo->act[k][b] = -1;
         /* noise, SRK.py:134-142, and the SRK2 force wipe */
         for (int k = 0; k < n_pops; k++) {
             if (fixed[k]) continue;
@@ -1297,6 +1431,16 @@ GCRO_EXPORT int gcro_group_run(int n_pops, const gcro_params *const *ps, gcro_st
                 for (int k = 0; k < n_pops; k++) {
                     if (fixed[k]) continue;
                     const int q = (k + ii) % n_pops;
+                    if (mo && k == mo->chain_pop && q == mo->motor_pop) {
+                        const int64_t n = ps[k]->n_beads;
+                        memset(tmp[k], 0, sizeof(double) * (size_t)n * dim);
+                        motor_push_keyed(X[k], n, tmp[k], mo->act[k], sts[k]->tangent, L, X[q], ps[q]->n_beads,
+                                         mo->act[q], mo->params, mo->list_r2, ps[q]->seed, g->step0 + steps, stage,
+                                         dim);
+                        double *Fs = sts[k]->forces;
+                        for (int64_t b = 0; b < n * dim; b++) Fs[b] += tmp[k][b];
+                        continue;
+                    }
                     const double *w = cross + ((size_t)k * n_pops + q) * 4;
                     if (!(w[3] > 0.0) || (w[0] == 0.0 && w[1] == 0.0)) continue;
                     const int64_t n = ps[k]->n_beads;
@@ -1365,8 +1509,10 @@ GCRO_EXPORT int gcro_group_run(int n_pops, const gcro_params *const *ps, gcro_st
                                   dt_eff, p->D, p->radius, dim, rscr[k], rscr[k] + 3 * n, rscr[k] + 6 * n);
                 } else {
                     dt_eff /= p->radius;
+                    const int hold = mo && k == mo->motor_pop && mo->dont_diffuse;
                     for (int64_t b = 0; b < n; b++)
                         for (int i = 0; i < dim; i++) {
+                            if (hold && mo->act[k][b] >= 0) continue; /* an attached motor stays */
                             double t = st->pos[b * dim + i] + dt_eff * Fu[b * dim + i];
                             if (s2 != 0.0) t += s2 * st->noise[b * 2 * dim + i];
                             W[b * dim + i] = py_mod(t, L);

@@ -78,6 +78,13 @@ class State(C.Structure):
     ]
 
 
+class Motors(C.Structure):
+    """A motor population of a group (gcro_motors)."""
+    _fields_ = [("motor_pop", C.c_int32), ("chain_pop", C.c_int32), ("dont_diffuse", C.c_int32),
+                ("pad", C.c_int32), ("params", C.c_double * 5), ("list_r2", C.c_double),
+                ("act", C.c_void_p * 8)]
+
+
 class Result(C.Structure):
     _fields_ = [("dt", C.c_double), ("dt_used_total", C.c_double), ("steps", C.c_double),
                 ("max_forces_strength", C.c_double), ("counter", C.c_double),
@@ -137,6 +144,13 @@ def lib(variant=""):
         L.gcro_order_params.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_void_p]
         L.gcro_pair_forces_all.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_int64,
                                            C.c_int, C.c_void_p, C.c_double, C.c_int, C.c_void_p]
+        L.gcro_motor_uniforms.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int64, C.c_int, C.c_void_p]
+        L.gcro_motor_push_mt.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.POINTER(MT), C.c_int]
+        L.gcro_group_run_motors.restype = C.c_int
+        L.gcro_group_run_motors.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.POINTER(Params), C.POINTER(Result), C.POINTER(Motors)]
         L.gcro_group_run.restype = C.c_int
         L.gcro_group_run.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Params),
                                      C.POINTER(Result)]
@@ -146,6 +160,7 @@ def lib(variant=""):
         assert L.gcro_sizeof_params() == C.sizeof(Params)
         assert L.gcro_sizeof_state() == C.sizeof(State)
         assert L.gcro_sizeof_mt() == C.sizeof(MT)
+        assert L.gcro_sizeof_motors() == C.sizeof(Motors)
         _libs[variant] = L
     return _libs[variant]
 
@@ -238,6 +253,32 @@ def chunk_chain(n_threads, chain_id):
     split = np.zeros(max(n_threads - 1, 0), dtype=np.int64)
     k = lib().gcro_chunk_chain(n_threads, len(chain_id), _p(chain_id), _p(split))
     return split[:k]
+
+
+def motor_uniforms(seed, motor, bead, step, stage):
+    """The keyed (u_off, u_on) draws of one (motor, bead) decision."""
+    out = np.zeros(2)
+    lib().gcro_motor_uniforms(seed, motor, bead, step, stage, _p(out))
+    return out
+
+
+def motor_push_mt(pos_b, nbor_list, forces_b, where_active_b, tangent, L, pos_m, where_active_m, params, seed):
+    """forces.calc_motor_push (forces.py:248-283) on the reference's arrays,
+    with its draws from MT19937 seeded with `seed` (np.random.seed(seed) in
+    a Numba-compiled function gives the same stream).  Arrays are updated in
+    place: forces_b, where_active_b, where_active_m (int64)."""
+    pos_b = np.ascontiguousarray(pos_b, dtype=np.float64)
+    pos_m = np.ascontiguousarray(pos_m, dtype=np.float64)
+    tangent = np.ascontiguousarray(tangent, dtype=np.float64)
+    nbor = np.ascontiguousarray(nbor_list, dtype=np.int64)
+    for a, t in ((forces_b, np.float64), (where_active_b, np.int64), (where_active_m, np.int64)):
+        assert a.dtype == t and a.flags.c_contiguous
+    mt = MT()
+    lib().gcro_mt_seed(C.byref(mt), seed & 0xFFFFFFFF)
+    prm = np.ascontiguousarray(params, dtype=np.float64)
+    lib().gcro_motor_push_mt(_p(pos_b), len(pos_b), _p(nbor), nbor.shape[1], _p(forces_b), _p(where_active_b),
+                             _p(tangent), float(L), _p(pos_m), _p(where_active_m), _p(prm), C.byref(mt),
+                             pos_b.shape[1])
 
 
 def order_params(tangent, chain_start):
@@ -429,11 +470,15 @@ class OracleGroup:
     attribute for the Philox stream), ``fixed[k]``: population k never moves,
     ``cross[k][q]``: the WCA parameters of the force on k from q."""
 
-    def __init__(self, systems, fixed, cross):
+    def __init__(self, systems, fixed, cross, motors=None):
         self.systems = list(systems)
         n = len(self.systems)
         self.fixed = np.asarray([1 if f else 0 for f in fixed], dtype=np.int32)
         self.cross = np.ascontiguousarray(np.asarray(cross, dtype=np.float64).reshape(n, n, 4))
+        # motors: dict(motor_pop, chain_pop, params [5], dont_diffuse, list_r2); where_active of
+        # every population is kept in self.where_active (int32, -1 at each step start)
+        self.motors = motors
+        self.where_active = [np.zeros(s.N, dtype=np.int32) for s in self.systems]
 
     def run(self, n_steps, dt, dtmax=None, max_dist_per_step=math.inf, rk_cheat=1.0, max_dt_usable=-1.0,
             noise_mode=NOISE_PHILOX, step0=0, calc_active=True, srk_order=2):
@@ -453,7 +498,19 @@ class OracleGroup:
         p_arr = (C.POINTER(Params) * n)(*[C.pointer(p) for p in ps])
         s_arr = (C.POINTER(State) * n)(*[C.pointer(st) for st in sts])
         res = Result()
-        rc = L.gcro_group_run(n, p_arr, s_arr, _p(self.fixed), _p(self.cross), C.byref(g), C.byref(res))
+        if self.motors is not None:
+            mo = Motors()
+            mo.motor_pop, mo.chain_pop = self.motors["motor_pop"], self.motors["chain_pop"]
+            mo.dont_diffuse = 1 if self.motors.get("dont_diffuse", True) else 0
+            for i, v in enumerate(self.motors["params"]):
+                mo.params[i] = v
+            mo.list_r2 = self.motors["list_r2"]
+            for k, a in enumerate(self.where_active):
+                mo.act[k] = a.ctypes.data
+            rc = L.gcro_group_run_motors(n, p_arr, s_arr, _p(self.fixed), _p(self.cross), C.byref(g),
+                                         C.byref(res), C.byref(mo))
+        else:
+            rc = L.gcro_group_run(n, p_arr, s_arr, _p(self.fixed), _p(self.cross), C.byref(g), C.byref(res))
         if rc != 0:
             raise RuntimeError(f"oracle group run failed ({rc})")
         return {"dt": res.dt, "dt_used": res.dt_used_total, "steps": int(res.steps),
