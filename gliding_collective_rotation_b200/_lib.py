@@ -99,6 +99,8 @@ SIGNATURES = {
     "gcr_couple": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                              C.POINTER(C.c_double)]),
     "gcr_decouple": (C.c_int, [C.c_void_p, C.c_int32]),
+    "gcr_set_motors": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.POINTER(C.c_double), C.c_int32]),
+    "gcr_where_active": (C.c_int, [C.c_void_p, C.c_int32, C.c_void_p]),
     "gcr_order_params_noalloc": (C.c_int, [C.c_int32, C.c_int32, C.c_void_p, C.c_void_p, C.c_int64, C.c_int64,
                                            C.POINTER(C.c_double), C.c_void_p]),
 }

@@ -118,6 +118,7 @@ class Batch:
         self._carry_dt = None  # dts to hand to the next call after a regrow
         self.series_buf = None
         self.groups = []  # coupled populations: (member indices, fixed flags, cross WCA parameters)
+        self.motors = []  # motor populations: (motor index, chain index, params, hold)
         self._img_carry = [None] * len(specs)  # L * images crossed before the last regrow
         self._make_engine()
 
@@ -133,6 +134,27 @@ class Batch:
             self.engine.admit(st)
         for g in self.groups:
             self._couple(*g)
+        for m in self.motors:
+            self._set_motors(*m)
+
+    def set_motors(self, motor, chains, params, hold=True):
+        """System ``motor`` (single beads, coupled with ``chains`` by
+        ``couple`` whose cross r_cut of motor from chains is the list radius)
+        is a motor population pushing the beads of system ``chains``
+        (forces.calc_motor_push, forces.py:248-283): params =
+        [motor_max_dist_sq, b_one_motor_per_bead, imparts_force, k_on,
+        k_off]; ``hold``: b_motors_dont_diffuse_while_pushing.  Survives a
+        regrow."""
+        m = (int(motor), int(chains), np.asarray(params, dtype=np.float64), bool(hold))
+        self._set_motors(*m)
+        self.motors.append(m)
+
+    def _set_motors(self, motor, chains, params, hold):
+        self.engine.set_motors(self.states[motor].slot, self.states[chains].slot, params, hold)
+
+    def where_active(self, i):
+        """pop.where_active of system i after the last step (int32 numpy)."""
+        return self.engine.where_active(self.states[i].slot).cpu().numpy()
 
     def couple(self, members, fixed, cross_wca):
         """Step the systems ``members`` (indices into this batch, in the

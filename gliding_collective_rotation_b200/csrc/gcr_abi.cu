@@ -89,6 +89,10 @@ struct Slot {
     int64_t nc = 1;             // current GPU cells per side
     int64_t longest = 0;        // beads of the longest chain
     int group = -1;             // coupled group (index into gcr_ctx::groups) or -1
+    // a motor population (gcr_set_motors): the chains it pushes and how
+    int motor_chain = -1;
+    double mparams[5] = {0, 0, 0, 0, 0};
+    int motor_hold = 1;
 };
 
 // populations coupled in one box (gcr_couple)
@@ -160,6 +164,10 @@ struct gcr_ctx {
     bool graph_rigid = false;  // the graph holds the rigid-rod projection kernels
     bool graph_obs = false;    // the graph holds the series kernel
     bool graph_cross = false;  // the graph holds the cross-population pair kernels
+    bool graph_motor = false;  // the graph holds the motor kernels
+    int *act = nullptr;        // motors: where_active per bead, pushes and changes per stage (lazy)
+    int *mpush = nullptr;
+    int *mdelta = nullptr;
     std::vector<Group> groups;
     int *xnbr = nullptr;       // cross lists of coupled populations
     int *xcount = nullptr;
@@ -366,6 +374,12 @@ int apply_groups(gcr_ctx *c, bool *moved)
         }
         p.pos1 = sl.buf.pos1;
         p.pos2 = c->pos2 ? c->pos2 + (size_t)sl.bead_off * dim : nullptr;
+        p.motor = 0;
+        p.motor_k = -1;
+        p.motor_hold = 0;
+        p.pushed = 0;
+        p.push_force = 0.0;
+        for (int k = 0; k < 5; k++) p.mparams[k] = 0.0;
     }
     int64_t rows = 0;
     for (const Group &g : c->groups) {
@@ -383,12 +397,25 @@ int apply_groups(gcr_ctx *c, bool *moved)
             const double skin_a = 2.0 * std::sqrt(p.half_skin2);
             // the other populations in the order their forces are added
             // (pop_index_diff = 1, 2, ..., SRK.py:287-294)
+            // a motor population's cross list to the chains it pushes holds
+            // its candidate beads (radius w[3]), not a force
+            const Slot &sa = c->slots[g.slots[a]];
             for (int ii = 1; ii < g.n; ii++) {
                 const int b = (a + ii) % g.n;
                 const double *w = g.cross[a][b];
-                if (!(w[3] > 0.0) || (w[0] == 0.0 && w[1] == 0.0)) continue;
+                const bool pushes = sa.motor_chain >= 0 && sa.motor_chain == g.slots[b] && !g.fixed[b];
+                if (!(w[3] > 0.0) || (!pushes && w[0] == 0.0 && w[1] == 0.0)) continue;
                 const SysP &q = c->hP[g.slots[b]];
                 const int k = p.n_cross++;
+                if (pushes) {
+                    SysP &ch = c->hP[g.slots[b]];
+                    p.motor = 1;
+                    p.motor_k = k;
+                    p.motor_hold = sa.motor_hold;
+                    for (int e = 0; e < 5; e++) p.mparams[e] = sa.mparams[e];
+                    ch.pushed = 1;
+                    ch.push_force = sa.mparams[2];
+                }
                 p.cross_q[k] = g.slots[b];
                 p.cross_p0[k] = w[0];
                 p.cross_p1[k] = w[1];
@@ -428,6 +455,14 @@ int apply_groups(gcr_ctx *c, bool *moved)
     c->args.xcount = c->xcount;
     c->args.xstride = c->x_rows;
     return GCR_OK;
+}
+
+// some resident system is a motor population pushing chains
+bool any_motor(const gcr_ctx *c)
+{
+    for (size_t s = 0; s < c->slots.size(); s++)
+        if (c->slots[s].used && c->hP[s].motor) return true;
+    return false;
 }
 
 // some resident system feels another population's pair force
@@ -566,10 +601,12 @@ int enqueue_step(gcr_ctx *c)
     if (c->cfg.srk_order == 4) return enqueue_step4(c);
     if ((rc = enqueue_lists(c, 0))) return rc;
     if ((rc = enqueue_pair(c, 0, c->graph_cross))) return rc;
+    if (c->graph_motor && (rc = launch(c, c->ks.motor[0], c->grid_update, bb))) return rc;
     if ((rc = enqueue_stage(c, 0, c->graph_cross))) return rc;
     if (c->graph_rigid && (rc = launch(c, c->ks.rigid0, c->grid_update, bb))) return rc;
     if ((rc = enqueue_lists(c, 1))) return rc;
     if ((rc = enqueue_pair(c, 1, c->graph_cross))) return rc;
+    if (c->graph_motor && (rc = launch(c, c->ks.motor[1], c->grid_update, bb))) return rc;
     if ((rc = enqueue_stage(c, 1, c->graph_cross))) return rc;
     if ((rc = launch_sys(c, c->ks.sys_dt))) return rc;
     if ((rc = launch(c, c->ks.update, c->grid_update, bb))) return rc;
@@ -605,8 +642,9 @@ int build_graph(gcr_ctx *c)
 {
     // the projection and series kernels are in the graph only while some
     // system uses them
-    const bool rigid = any_rigid(c), obs = any_series(c), cross = any_cross(c);
-    if (c->graph && (rigid != c->graph_rigid || obs != c->graph_obs || cross != c->graph_cross)) {
+    const bool rigid = any_rigid(c), obs = any_series(c), cross = any_cross(c), motor = any_motor(c);
+    if (c->graph && (rigid != c->graph_rigid || obs != c->graph_obs || cross != c->graph_cross ||
+                     motor != c->graph_motor)) {
         GCR_CUDA(cudaStreamSynchronize(c->stream));
         cudaGraphExecDestroy(c->graph);
         c->graph = nullptr;
@@ -615,6 +653,7 @@ int build_graph(gcr_ctx *c)
     c->graph_rigid = rigid;
     c->graph_obs = obs;
     c->graph_cross = cross;
+    c->graph_motor = motor;
     cudaGraph_t g = nullptr;
     GCR_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int rc = GCR_OK;
@@ -831,7 +870,7 @@ int gcr_destroy(gcr_ctx *c)
     void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->d_row_prefix, c->topo, c->cnt,
                     c->ncell,
                     c->items, c->nbr, c->ncount, c->xref, c->work, c->xi, c->fp, c->chain_starts, c->d_err,
-                    c->d_out, c->pos2, c->faux, c->xnbr, c->xcount, c->img};
+                    c->d_out, c->pos2, c->faux, c->xnbr, c->xcount, c->img, c->act, c->mpush, c->mdelta};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -946,6 +985,8 @@ int gcr_evict(gcr_ctx *c, int32_t slot)
     if (sl.n_cells_alloc) c->cells.release(sl.cell_off, sl.n_cells_alloc);
     c->chains.release(sl.chain_off, sl.desc.n_chains + 1);
     sl = Slot();
+    for (Slot &o : c->slots)
+        if (o.motor_chain == slot) o.motor_chain = -1;
     SysS &s = c->hS[slot];
     std::memset(&s, 0, sizeof(s));
     GCR_CUDA(cudaMemcpyAsync(c->dS + slot, &s, sizeof(SysS), cudaMemcpyHostToDevice, c->stream));
@@ -1101,6 +1142,70 @@ int gcr_decouple(gcr_ctx *c, int32_t slot)
     return rebuild_tiles(c);
 }
 
+int gcr_set_motors(gcr_ctx *c, int32_t motor_slot, int32_t chain_slot, const double *params, int32_t hold)
+{
+    if (!valid_slot(c, motor_slot)) return fail(GCR_ERR_BAD_ARG, "invalid motor slot");
+    if (c->cfg.srk_order != 2) return fail(GCR_ERR_BAD_ARG, "motors are stepped by SRK2 contexts");
+    Slot &ms = c->slots[motor_slot];
+    if (chain_slot >= 0) {
+        if (!valid_slot(c, chain_slot) || chain_slot == motor_slot)
+            return fail(GCR_ERR_BAD_ARG, "invalid chain slot");
+        if (!params) return fail(GCR_ERR_BAD_ARG, "null params");
+        for (int k = 0; k < 5; k++)
+            if (!std::isfinite(params[k])) return fail(GCR_ERR_BAD_ARG, "motor parameters must be finite");
+        if (!(params[0] >= 0.0)) return fail(GCR_ERR_BAD_ARG, "motor_max_dist_sq must be >= 0");
+        if (ms.desc.calc_springs || ms.desc.self_propel || ms.desc.n_chains != ms.desc.n_beads)
+            return fail(GCR_ERR_BAD_ARG, "motors are single beads without springs or propulsion");
+        for (const Slot &o : c->slots)
+            if (&o != &ms && o.used && o.motor_chain == chain_slot)
+                return fail(GCR_ERR_BAD_ARG, "the chains are pushed by another motor population");
+    }
+    int rc = drop_graph(c);
+    if (rc) return rc;
+    if (chain_slot >= 0 && !c->act) {
+        const size_t n = (size_t)c->cfg.bead_capacity;
+        cudaError_t e = cudaMalloc(&c->act, sizeof(int) * n);
+        e = e ? e : cudaMalloc(&c->mpush, sizeof(int) * n);
+        e = e ? e : cudaMalloc(&c->mdelta, sizeof(int) * n);
+        e = e ? e : cudaMemsetAsync(c->act, 0xff, sizeof(int) * n, c->stream);  // -1
+        e = e ? e : cudaMemsetAsync(c->mpush, 0, sizeof(int) * n, c->stream);
+        e = e ? e : cudaMemsetAsync(c->mdelta, 0, sizeof(int) * n, c->stream);
+        if (e != cudaSuccess) {
+            for (int **q : {&c->act, &c->mpush, &c->mdelta}) {
+                if (*q) cudaFree(*q);
+                *q = nullptr;
+            }
+            return fail(e == cudaErrorMemoryAllocation ? GCR_ERR_OOM : GCR_ERR_CUDA, "motor arrays");
+        }
+        c->args.act = c->act;
+        c->args.mpush = c->mpush;
+        c->args.mdelta = c->mdelta;
+    }
+    const int old_chain = ms.motor_chain;
+    ms.motor_chain = chain_slot;
+    if (chain_slot >= 0) {
+        for (int k = 0; k < 5; k++) ms.mparams[k] = params[k];
+        ms.motor_hold = hold ? 1 : 0;
+    }
+    bool moved = false;
+    if ((rc = apply_groups(c, &moved))) return rc;
+    c->tiles_dirty = true;
+    for (int32_t s : {motor_slot, chain_slot, (int32_t)old_chain})
+        if (s >= 0 && valid_slot(c, s) && (rc = mark_rebuild(c, s))) return rc;
+    return rebuild_tiles(c);
+}
+
+int gcr_where_active(gcr_ctx *c, int32_t slot, int32_t *dst)
+{
+    if (!valid_slot(c, slot)) return fail(GCR_ERR_BAD_ARG, "invalid slot");
+    if (!dst) return fail(GCR_ERR_BAD_ARG, "null destination");
+    if (!c->act) return fail(GCR_ERR_BAD_ARG, "no motor population was set");
+    const Slot &sl = c->slots[slot];
+    GCR_CUDA(cudaMemcpyAsync(dst, c->act + sl.bead_off, sizeof(int) * (size_t)sl.desc.n_beads,
+                             cudaMemcpyDeviceToDevice, c->stream));
+    return GCR_OK;
+}
+
 namespace {
 int check_call(const gcr_call *call)
 {
@@ -1233,6 +1338,7 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
         rc = enqueue_lists(c, 0);
         GCR_CUDA(cudaEventRecord(e[1], c->stream));
         if (!rc) rc = enqueue_pair(c, 0, cross);  // nothing with fused stages
+        if (!rc && any_motor(c)) rc = launch(c, c->ks.motor[0], c->grid_update, bb);
         GCR_CUDA(cudaEventRecord(e[2], c->stream));
         if (!rc) rc = enqueue_stage(c, 0, cross);
         if (!rc && rigid) rc = launch(c, c->ks.rigid0, c->grid_update, bb);
@@ -1240,6 +1346,7 @@ int gcr_profile_steps(gcr_ctx *c, int32_t n_steps, float *ms_out)
         if (!rc) rc = enqueue_lists(c, 1);
         GCR_CUDA(cudaEventRecord(e[4], c->stream));
         if (!rc) rc = enqueue_pair(c, 1, cross);
+        if (!rc && any_motor(c)) rc = launch(c, c->ks.motor[1], c->grid_update, bb);
         GCR_CUDA(cudaEventRecord(e[5], c->stream));
         if (!rc) rc = enqueue_stage(c, 1, cross);
         if (!rc) rc = launch_sys(c, c->ks.sys_dt);

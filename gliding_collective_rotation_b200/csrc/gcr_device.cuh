@@ -94,6 +94,15 @@ struct SysP {
     double cross_p0[kMaxPops - 1], cross_p1[kMaxPops - 1], cross_shift[kMaxPops - 1];
     double cross_rc2[kMaxPops - 1], cross_rl2[kMaxPops - 1];
     int64_t x_off;                // first row of its cross lists
+    // motors (Motor_Population, populations.py:617-661; forces.calc_motor_push,
+    // forces.py:248-283): a motor population pushes the beads of the chain
+    // population on its cross list motor_k; the chains add the pushes
+    int32_t motor;       // 1: this system is a motor population
+    int32_t motor_k;     // its cross-list index of the chains it pushes
+    int32_t motor_hold;  // b_motors_dont_diffuse_while_pushing: an attached motor keeps its position
+    int32_t pushed;      // 1: chains pushed by a motor population
+    double mparams[5];   // motors: [motor_max_dist_sq, b_one_motor_per_bead, imparts_force, k_on, k_off]
+    double push_force;   // chains: the pushing motors' imparts_force
 };
 
 struct SysS {
@@ -143,6 +152,23 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1
         k1 += 0xBB67AE85u;
     }
     return c;
+}
+
+// two uniforms in [0, 1) for the motor decisions of (motor, bead) at a
+// stage of a step: u0 against k_off, u1 against k_on (53 bits each); the
+// keyed stand-in for the reference's sequential np.random.random() draws
+// (forces.py:268, 275)
+__device__ __forceinline__ void motor_uniforms(uint64_t seed, uint32_t motor, uint32_t bead, int64_t step,
+                                               int stage, double &u0, double &u1)
+{
+    uint4 r = philox4x32_10(make_uint4(motor, bead, (uint32_t)((uint64_t)step & 0xffffffffu),
+                                       ((uint32_t)((uint64_t)step >> 32) & 0xffffu) | ((uint32_t)stage << 16)),
+                            (uint32_t)(seed & 0xffffffffu) ^ 0x6d6f746fu, (uint32_t)(seed >> 32));
+    const double two_m53 = 1.1102230246251565e-16;
+    uint64_t a = (((uint64_t)r.x << 21) ^ (uint64_t)(r.y >> 11)) & ((1ull << 53) - 1);
+    uint64_t b = (((uint64_t)r.z << 21) ^ (uint64_t)(r.w >> 11)) & ((1ull << 53) - 1);
+    u0 = (double)a * two_m53;
+    u1 = (double)b * two_m53;
 }
 
 __device__ __forceinline__ void normal_pair(uint64_t seed, uint32_t bead, int64_t step,

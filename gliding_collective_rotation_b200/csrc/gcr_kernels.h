@@ -47,6 +47,13 @@ struct BatchArgs {
     // tile r of a system is segment r % segments of row r / segments
     const int *row_prefix;
     int cell_stage_cap;  // beads a CTA of the cell-staged pair kernel copies into shared memory
+    // motors (allocated with the first motor population): where_active of every
+    // bead (chains: motors attached, -1 + count; motors: the bead it pushes or
+    // -1), and per chain bead the pushes and the where_active change of the
+    // current stage (written by k_motor, consumed and zeroed by k_stage)
+    int *act;
+    int *mpush;
+    int *mdelta;
 };
 
 struct KernelSet {
@@ -78,6 +85,7 @@ struct KernelSet {
     void *lists_plan;  // compact the systems that take part in a list build
     void *pair_cross[3];  // pair forces at pos / pos1 / pos2 with the other populations' (coupled systems)
     void *pair_cells[2];  // cell-staged pair forces at pos / pos1 (pair_mode 2)
+    void *motor[2];       // motor decisions of stage 0 / 1 (graphs with a motor population)
     size_t (*pair_cells_smem)(int cap);  // their dynamic shared memory for `cap` staged beads
     int pair_cells_rows;  // cell rows a row tile stages (3 in 2D, 9 in 3D)
     int max_row_cells;    // cells of a row tile, at most

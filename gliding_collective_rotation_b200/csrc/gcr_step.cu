@@ -760,7 +760,9 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_pair(BatchArgs A)
         FT F[3] = {FT(0), FT(0), FT(0)};
         bool bad = false;
         list_pair_force<D, FT>(A, p, X, xb, b, F, bad);
-        if constexpr (CROSS) add_cross<D, FT, WHICH>(A, p, b, xb, F, bad);
+        // a motor's cross list is its candidate beads, not a force
+        if constexpr (CROSS)
+            if (!p.motor) add_cross<D, FT, WHICH>(A, p, b, xb, F, bad);
         if (bad) atomicOr(&s.flags, kFlagListCorrupt);
         FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
 #pragma unroll
@@ -1245,6 +1247,30 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                     for (int i = 0; i < D; i++) F[i] += v0 * tg[i];
                 }
             }
+            if constexpr (!srk4_stage(STAGE)) {
+                if (p.pushed) {
+                    // the motor pushes of this stage (k_motor), added after
+                    // the chains' own forces as the other population's
+                    // force (SRK.py:261-267, 287-294); where_active counts
+                    // the attached motors from -1 at each step (SRK.py:132)
+                    int *mp = A.mpush + p.bead_off + b, *md = A.mdelta + p.bead_off + b;
+                    const int npush = *mp, dl = *md;
+                    *mp = 0;
+                    *md = 0;
+                    int *ab = A.act + p.bead_off + b;
+                    *ab = (STAGE == 0 ? -1 : *ab) + dl;
+                    if (npush > 0) {
+                        const FT f = (FT)p.push_force;
+                        FT M[3] = {FT(0), FT(0), FT(0)};
+                        for (int k = 0; k < npush; k++) {
+#pragma unroll
+                            for (int i = 0; i < D; i++) M[i] += f * tg[i];
+                        }
+#pragma unroll
+                        for (int i = 0; i < D; i++) F[i] += M[i];
+                    }
+                }
+            }
             // G: the force the caller and the dt rule see -- F0 + F1 (SRK2),
             // the weighted sum of the stage forces (SRK4, SRK.py:296-321,
             // with the stage's own force kept in faux)
@@ -1291,8 +1317,15 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                     double *W = stage_x<stage_writes(STAGE)>(p);
                     double x1[3] = {0.0, 0.0, 0.0};
                     bool finite = true;
+                    // an attached motor writes no virtual position: its pos1
+                    // keeps the previous value (SRK.py:389-395)
+                    const bool hold = p.motor && p.motor_hold && A.act[p.bead_off + b] >= 0;
 #pragma unroll
                     for (int i = 0; i < D; i++) {
+                        if (hold) {
+                            x1[i] = W[(size_t)b * D + i];
+                            continue;
+                        }
                         const double x0 = stage_reads(STAGE) == 0 ? xb[i] : p.pos[(size_t)b * D + i];
                         x1[i] = srk_update<FT>(x0, dt_eff, s2, F[i], xi[i], p.L);
                         finite &= isfinite(x1[i]);
@@ -1359,10 +1392,16 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A
         double x[3] = {0.0, 0.0, 0.0};
         bool finite = true;
         const bool plain = p.rigid == 0.0;  // else k_rigid writes pos
+        // an attached motor keeps its position (SRK.py:389-395)
+        const bool hold = p.motor && p.motor_hold && A.act[p.bead_off + b] >= 0;
         if (plain) {
 #pragma unroll
             for (int i = 0; i < D; i++) {
                 const double xo = p.pos[(size_t)b * D + i];
+                if (hold) {
+                    x[i] = xo;
+                    continue;
+                }
                 x[i] = srk_update<FT>(xo, dt_eff, s2, frc[(size_t)b * D + i], xi[i], p.L);
                 finite &= isfinite(x[i]);
                 p.pos[(size_t)b * D + i] = x[i];
@@ -1691,6 +1730,88 @@ __global__ void __launch_bounds__(512) k_run_check(BatchArgs A)
 }
 
 // ------------------------------------------------------------------------
+// motor decisions of one SRK2 stage (forces.calc_motor_push,
+// forces.py:248-283), one thread per motor.  The reference loops over the
+// chain beads in order and, for each, over the motors on its list; a motor's
+// fate depends only on the beads that reach it, in bead order, so each
+// thread replays its motor's sequence: over its candidate beads (the chain
+// beads within the list radius, cross_rc2, at the stage's positions, in
+// ascending id) an attached motor stays with probability 1 - k_off, else
+// detaches (the drawing bead's where_active drops by one), and a free motor
+// attaches with probability k_on when within motor_max_dist (that bead's
+// where_active rises by one and it gets one push).  The chain beads' pushes
+// and where_active changes are summed with integer atomics, so the result
+// does not depend on the order of the motors' threads; the stage kernel
+// turns them into forces.  Draws: motor_uniforms(seed, motor, bead, step,
+// stage).  Distances in FP64 without contraction, as the reference computes
+// them (forces.inbounds_diff, forces.py:44-55).
+// ------------------------------------------------------------------------
+template <int D, int WHICH>
+__global__ void __launch_bounds__(512) k_motor(BatchArgs A)
+{
+    const int nt = *A.n_bead_tiles;
+    for (int t = blockIdx.x; t < nt; t += gridDim.x) {
+        const Tile tl = A.bead_tiles[t];
+        const SysP &p = A.P[tl.sys];
+        if (!p.motor) continue;
+        SysS &s = A.S[tl.sys];
+        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal)) continue;
+        const int m = tl.begin + threadIdx.x;
+        if (m >= p.n || threadIdx.x >= A.tile_beads) continue;
+        int *act_m = A.act + p.bead_off + m;
+        // where_active is wiped at the start of each step (SRK.py:132)
+        int am = WHICH == 0 ? -1 : *act_m;
+        const int k = p.motor_k;
+        const int qs = (k >= 0 && k < p.n_cross && k < kMaxPops - 1) ? p.cross_q[k] : -1;
+        if ((unsigned)qs >= (unsigned)A.n_slots) {
+            *act_m = am;
+            atomicOr(&s.flags, kFlagListCorrupt);
+            continue;
+        }
+        const SysP &q = A.P[qs];
+        const double *XM = stage_x<WHICH>(p);
+        const double *XQ = stage_x<WHICH>(q);
+        double xm[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int i = 0; i < D; i++) xm[i] = XM[(size_t)m * D + i];
+        const int64_t row = p.x_off + (int64_t)k * p.n + m;
+        int cnt = A.xcount[row];
+        cnt = cnt < 0 ? 0 : (cnt < A.list_depth ? cnt : A.list_depth);
+        const double r2 = p.cross_rc2[k], dmax2 = p.mparams[0], k_on = p.mparams[3], k_off = p.mparams[4];
+        const int64_t step = s.step;
+        bool bad = false;
+        for (int e = 0; e < cnt; e++) {
+            const int j = A.xnbr[row + (int64_t)e * A.xstride];
+            if ((unsigned)j >= (unsigned)q.n) {
+                bad = true;
+                continue;
+            }
+            double ds = 0.0;
+#pragma unroll
+            for (int i = 0; i < D; i++) {
+                const double d = inbounds(xm[i], XQ[(size_t)j * D + i], p.half_L, p.L);
+                ds = __dadd_rn(ds, __dmul_rn(d, d));
+            }
+            if (!(ds <= r2)) continue;
+            double u_off, u_on;
+            motor_uniforms(p.seed, (uint32_t)m, (uint32_t)j, step, WHICH, u_off, u_on);
+            if (am >= 0) {
+                if (u_off > k_off) continue;
+                am = -1;
+                atomicAdd(A.mdelta + q.bead_off + j, -1);
+            }
+            if (am < 0 && u_on < k_on && ds <= dmax2) {
+                atomicAdd(A.mdelta + q.bead_off + j, 1);
+                atomicAdd(A.mpush + q.bead_off + j, 1);
+                am = j;
+            }
+        }
+        *act_m = am;
+        if (bad) atomicOr(&s.flags, kFlagListCorrupt);
+    }
+}
+
+// ------------------------------------------------------------------------
 // launchers
 // ------------------------------------------------------------------------
 template <int D, typename FT>
@@ -1764,6 +1885,8 @@ KernelSet kernel_set(int dim, int precision)
         k.bin2 = (void *)k_bin<2, 2>;
         k.build2 = (void *)k_build<2, 2>;
         k.run_check = (void *)k_run_check<2>;
+        k.motor[0] = (void *)k_motor<2, 0>;
+        k.motor[1] = (void *)k_motor<2, 1>;
     } else {
         k.bin0 = (void *)k_bin<3, 0>;
         k.bin1 = (void *)k_bin<3, 1>;
@@ -1772,6 +1895,8 @@ KernelSet kernel_set(int dim, int precision)
         k.bin2 = (void *)k_bin<3, 2>;
         k.build2 = (void *)k_build<3, 2>;
         k.run_check = (void *)k_run_check<3>;
+        k.motor[0] = (void *)k_motor<3, 0>;
+        k.motor[1] = (void *)k_motor<3, 1>;
     }
     k.sort = (void *)k_sort;
     k.topo = (void *)k_topo;

@@ -242,6 +242,30 @@ class Engine:
         f_arr = (C.c_int32 * n)(*[1 if f else 0 for f in fixed])
         check(self.lib.gcr_couple(self._ctx, n, s_arr, f_arr, cw.ctypes.data_as(C.POINTER(C.c_double))))
 
+    def set_motors(self, motor_slot, chain_slot, params, hold=True):
+        """``motor_slot`` (single beads, coupled with ``chain_slot`` by
+        ``couple`` with the list radius as the cross r_cut of motor from
+        chains) pushes the chains' beads (``gcr_set_motors``): params =
+        [motor_max_dist_sq, b_one_motor_per_bead, imparts_force, k_on,
+        k_off] (populations.py:276-287); ``hold``:
+        b_motors_dont_diffuse_while_pushing.  ``chain_slot=-1`` undoes it."""
+        prm = np.ascontiguousarray(np.asarray(params if params is not None else np.zeros(5), dtype=np.float64))
+        if prm.shape != (5,):
+            raise ValueError("motor params are [max_dist_sq, one_per_bead, force, k_on, k_off]")
+        check(self.lib.gcr_set_motors(self._ctx, int(motor_slot), int(chain_slot),
+                                      prm.ctypes.data_as(C.POINTER(C.c_double)), 1 if hold else 0))
+
+    def where_active(self, slot):
+        """pop.where_active of a resident system after the last step: int32
+        [n] on the device (chains: motors attached minus one; motors: the
+        bead pushed or -1)."""
+        st = self.systems[int(slot)]
+        out = torch.empty(st.n, dtype=torch.int32, device=st.pos.device)
+        torch.cuda.current_stream(self.device).synchronize()
+        check(self.lib.gcr_where_active(self._ctx, int(slot), C.c_void_p(out.data_ptr())))
+        self.synchronize()
+        return out
+
     def unwrapped(self, slot):
         """Positions plus the periodic images each bead crossed since
         admission (or ``reset_images``): float64 [n, dim] on the device."""

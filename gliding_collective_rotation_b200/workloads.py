@@ -155,6 +155,64 @@ def populations(n_boxes=128, seed=0):
     return specs, groups
 
 
+def motor_params(a=0.5, force=1.0, k_on=0.9, k_off=0.2, one_per_bead=False):
+    """The motor_push parameters of Chain_Collection.interactions
+    (populations.py:276-287) with the reference's defaults: motor_max_dist =
+    a / 2 (squared), imparts_force = v0 (config.py:95-98), k_on 0.9, k_off 0.2
+    (defaults.py:185-201)."""
+    return np.array([(a / 2) ** 2, float(one_per_bead), force, k_on, k_off])
+
+
+def motor_list_radius(L, biggest_interaction, max_dist_sq, grid_factor=2.0, n_grid_min=1):
+    """The list radius of the reference's chain-motor lists: grid_window *
+    Lx / n_grid with n_grid of config.grid_list_setup (config.py:147-193) and
+    the chain-motor thread's grid_window = max(1, ceil(grid_factor *
+    nbor_length_scale / grid_spacing)), whose length scale is the squared
+    motor_max_dist (SRK.py:84-87, 99-101); the list holds the motors within
+    that radius (updates.py:603-604)."""
+    n_grid = max(n_grid_min, int(L / (grid_factor * biggest_interaction)))
+    h = L / n_grid
+    window = max(1, int(math.ceil(grid_factor * max_dist_sq / h)))
+    return window * h
+
+
+def motors(n_boxes=16, seed=0, n_chains=200, chain_length=10, L=60.0, motor_density=0.5, D_motors=0.1,
+           k_on=0.9, k_off=0.2, hold=True):
+    """Boxes of chains pushed by motors (Motor_Population,
+    populations.py:617-661; BDsim.py:24-25): config-1 chains whose
+    propulsion v0 = 1 is handed to the motors (config.py:95-98: chains keep v0
+    = 0), and round(L^2 motor_density) motors of diffusion D_motors
+    (defaults.py:179-201).  Returns specs (chains of box i at 2i, motors at
+    2i + 1), the groups ``(members, fixed, cross_wca)`` and the motor settings
+    ``(motor index, chain index, params, hold)``; the motors' cross r_cut is
+    the reference's chain-motor list radius."""
+    specs, groups, mots = [], [], []
+    a = 0.5
+    prm = motor_params(a, 1.0, k_on, k_off)
+    for i in range(n_boxes):
+        rs = np.random.RandomState(seed * 100019 + i)
+        chains = make_system(f"box{i}_chains", 2, n_chains, chain_length, L, seed=7000 + i, v0=0.0,
+                             noise_seed=2 * i)
+        nm = int(round(L * L * motor_density))
+        pos = rs.uniform(0.0, L, size=(nm, 2))
+        tan = np.tile([1.0, 0.0], (nm, 1))
+        # biggest interaction distance: 2 a (springs), r_cut (WCA), motor_max_dist
+        r_list = motor_list_radius(L, max(2 * a, float(chains.params.wca_params[3]), a / 2), prm[0])
+        params = SystemParams(
+            L=L, spring_params=np.array([0.0, 0.0, 0.0, 0.0, 0.0, 0.1]), wca_params=np.array([0.0, 0.0, 0.0, r_list]),
+            active_params=np.array([0.0, 0.0, 0.0]), D=D_motors, Dr=0.0, radius=1.0, n_nearby=0,
+            calc_springs=False, calc_wca=True, self_propel=False, dtmax=chains.params.dtmax,
+            max_dist_per_step=math.inf, rk_cheat=1.0, seed=2 * i + 1, step=0)
+        mot = SystemSpec(f"box{i}_motors", 2, pos, tan, np.arange(nm), np.full(nm, a), params, chains.dt,
+                         chains.relax_mdps)
+        cross = np.zeros((2, 2, 4))
+        cross[1, 0] = [0.0, 0.0, 0.0, r_list]
+        specs += [chains, mot]
+        groups.append(([2 * i, 2 * i + 1], [False, False], cross))
+        mots.append((2 * i + 1, 2 * i, prm, hold))
+    return specs, groups, mots
+
+
 def serve_trace(n_requests, rate=20.0, seed=7, min_beads=1000, max_beads=1_000_000, min_steps=1000,
                 max_steps=20000):
     """Poisson arrivals at `rate`/s of config-3-style systems with bead count

@@ -221,6 +221,30 @@ GCR_API int gcr_couple(gcr_ctx *ctx, int32_t n, const int32_t *slots, const int3
 /* Dissolve the coupled group that holds `slot` (no-op when there is none);
  * evicting a member does the same. */
 GCR_API int gcr_decouple(gcr_ctx *ctx, int32_t slot);
+/* Motors (Motor_Population, populations.py:617-661; forces.calc_motor_push,
+ * forces.py:248-283; its diffusion, SRK.py:389-395).  `motor_slot` holds the
+ * motors as single beads (chains of 1, springs and propulsion off, calc_wca
+ * with p0 = p1 = 0 so that they are binned, D = D_motors); it pushes the
+ * beads of `chain_slot`, a moving member of the same coupled group whose
+ * cross entry (motor from chains) in gcr_couple has r_cut = the list radius
+ * of the reference's chain-motor lists (grid_window * Lx / n_grid) and p0 =
+ * p1 = 0.  params = [motor_max_dist_sq, b_one_motor_per_bead, imparts_force,
+ * k_on, k_off] as Chain_Collection.interactions packs them
+ * (populations.py:276-287); hold = b_motors_dont_diffuse_while_pushing.
+ * Each SRK2 stage a motor walks the chain beads within the list radius in
+ * ascending id, detaches with probability k_off, attaches with probability
+ * k_on when within motor_max_dist and then pushes that bead once by
+ * imparts_force along its tangent; where_active is -1 at the start of each
+ * step.  Draws are keyed Philox (seed of the motor system) instead of the
+ * reference's unseeded sequential np.random.random().  SRK2 contexts only;
+ * chain_slot = -1 turns the slot back into a plain population. */
+GCR_API int gcr_set_motors(gcr_ctx *ctx, int32_t motor_slot, int32_t chain_slot, const double *params,
+                           int32_t hold);
+/* where_active of a resident system (pop.where_active: chains, the motors
+ * attached minus one; motors, the bead pushed or -1) as int32 [n_beads] into
+ * device memory `dst` on the context stream; GCR_ERR_BAD_ARG before any
+ * motor population was set. */
+GCR_API int gcr_where_active(gcr_ctx *ctx, int32_t slot, int32_t *dst);
 
 /* ---- stepping --------------------------------------------------------- */
 /* Advance every armed system until its limits are reached or `max_steps`
