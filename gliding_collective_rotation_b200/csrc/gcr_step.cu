@@ -222,6 +222,18 @@ __device__ __forceinline__ void cell_of(const SysP &p, const double *x, int *ci)
 
 // a bead moved farther than skin/2 from where the list was built
 template <int D>
+__device__ __forceinline__ bool left_skin_of(const SysP &p, const double *r, const double *x)
+{
+    double dd = 0.0;
+#pragma unroll
+    for (int i = 0; i < D; i++) {
+        double d = inbounds(x[i], r[i], p.half_L, p.L);
+        dd += d * d;
+    }
+    return !(dd <= p.half_skin2);
+}
+
+template <int D>
 __device__ __forceinline__ bool left_skin(const SysP &p, const BatchArgs &A, int b, const double *x)
 {
     const double *r = A.xref + (size_t)(p.bead_off + b) * D;
@@ -1363,8 +1375,18 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
     }
 }
 
+// the update kernel holds all its inputs in registers at once
+#ifndef GCR_UPDATE_MIN_BLOCKS
+#define GCR_UPDATE_MIN_BLOCKS 3
+#endif
 template <int D, typename FT>
-__global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A)
+constexpr int update_min_blocks()
+{
+    return (D == 2 && sizeof(FT) == 4) ? GCR_UPDATE_MIN_BLOCKS : 1;
+}
+
+template <int D, typename FT>
+__global__ void __launch_bounds__(512, update_min_blocks<D, FT>()) k_update(BatchArgs A)
 {
     const int nt = *A.n_bead_tiles;
     // the next tile's table entry is loaded while the current tile runs
@@ -1383,26 +1405,42 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A
         // force_prefactor 0.5 of the SRK2 corrector; 1 for SRK4's weighted sum
         const double dt_eff = dtu * (A.order == 4 ? 1.0 : 0.5) / p.radius;
         const double s2 = sqrt(2.0 * dtu * p.D);
-        FT xi[3] = {FT(0), FT(0), FT(0)};
+        const bool plain = p.rigid == 0.0;  // else k_rigid writes pos
+        // every input is loaded before the first store: a store to pos may
+        // alias them for the compiler, which would order each later load
+        // behind it
+        FT xi[3] = {FT(0), FT(0), FT(0)}, fo[3] = {FT(0), FT(0), FT(0)};
+        double xold[3] = {0.0, 0.0, 0.0}, xr[3] = {0.0, 0.0, 0.0};
         if (p.D > 0.0) {
             const FT *xs = reinterpret_cast<const FT *>(A.xi) + (size_t)(p.bead_off + b) * D;
 #pragma unroll
             for (int i = 0; i < D; i++) xi[i] = xs[i];
         }
+        if (plain) {
+#pragma unroll
+            for (int i = 0; i < D; i++) {
+                xold[i] = p.pos[(size_t)b * D + i];
+                fo[i] = frc[(size_t)b * D + i];
+            }
+            if (p.calc_wca) {
+                const double *r = A.xref + (size_t)(p.bead_off + b) * D;
+#pragma unroll
+                for (int i = 0; i < D; i++) xr[i] = r[i];
+            }
+        }
         double x[3] = {0.0, 0.0, 0.0};
         bool finite = true;
-        const bool plain = p.rigid == 0.0;  // else k_rigid writes pos
         // an attached motor keeps its position (SRK.py:389-395)
         const bool hold = p.motor && p.motor_hold && A.act[p.bead_off + b] >= 0;
         if (plain) {
 #pragma unroll
             for (int i = 0; i < D; i++) {
-                const double xo = p.pos[(size_t)b * D + i];
+                const double xo = xold[i];
                 if (hold) {
                     x[i] = xo;
                     continue;
                 }
-                x[i] = srk_update<FT>(xo, dt_eff, s2, frc[(size_t)b * D + i], xi[i], p.L);
+                x[i] = srk_update<FT>(xo, dt_eff, s2, fo[i], xi[i], p.L);
                 finite &= isfinite(x[i]);
                 p.pos[(size_t)b * D + i] = x[i];
                 const int di = image_step(xo, x[i], p.half_L);
@@ -1435,7 +1473,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_update(BatchArgs A
 #pragma unroll
             for (int i = 0; i < D; i++) tan[(size_t)b * D + i] = tb[i] / mag;
         }
-        if (plain && finite && p.calc_wca && left_skin<D>(p, A, b, x)) s.rebuild = 1;  // rebuild before the next step
+        if (plain && finite && p.calc_wca && left_skin_of<D>(p, xr, x)) s.rebuild = 1;  // rebuild before the next step
     }
 }
 

@@ -32,8 +32,11 @@ stage's force.  A list of several populations (up to 4, fixed ones
 included) steps as the reference steps it (updates.py:146-247): one dt from
 the largest max-force value over the moving populations, and each moving
 population feels the others' WCA force (``interpop_forces``,
-updates.py:274-312), through ``gcr_couple``.  Features outside the GPU path
-(walls, motors, FENE, active sliding, E-field) raise ``NotImplementedError``.
+updates.py:274-312), through ``gcr_couple``.  A Motor_Population in the
+list pushes the chains it interacts with (``motor_push``,
+forces.py:248-283, through ``gcr_set_motors``; SRK2) and ``where_active``
+of every population is written back.  Features outside the GPU path (walls,
+FENE, active sliding, E-field) raise ``NotImplementedError``.
 
 ``install(updates_module, config_module)`` rebinds a reference checkout's
 ``updates.SRK2_force_calc`` to this function and makes it read that
@@ -85,9 +88,57 @@ def _force_list(pop):
 _SUPPORTED = {"springs", "WCA", "self-propulsion"}
 
 
+def _is_motors(pop):
+    """A Motor_Population (populations.py:617-661): single beads that only
+    diffuse and push the chains near them."""
+    return type(pop).__name__ == "Motor_Population" or hasattr(pop, "motor_max_dist_sq")
+
+
+def _pop_arrays(pop, dim):
+    """Positions, tangents, chain ids and rest lengths of a population; a
+    motor population has no chains or tangents: one chain per motor."""
+    if _is_motors(pop):
+        n = pop.total_pop
+        return pop.pos, np.tile(np.eye(dim)[0], (n, 1)), np.arange(n), np.ones(n)
+    return pop.pos, pop.tangent_list, pop.chain_id, pop.rest_lengths
+
+
+def _motor_list_radius(cfg, params):
+    """The radius of the reference's chain-motor lists: grid_window * Lx /
+    n_grid (updates.py:603-604), grid_window of the chain-motor thread from
+    its length scale, the squared motor_max_dist (SRK.py:84-87, 99-101)."""
+    L = float(cfg.Lx)
+    n_grid = int(getattr(cfg, "n_grid", 0) or 0)
+    grid_factor = float(getattr(cfg, "grid_factor", 2.0))
+    if n_grid <= 0:
+        raise NotImplementedError("motors need config.n_grid (config.grid_list_setup)")
+    h = L / n_grid
+    return max(1, int(np.ceil(grid_factor * float(params[0]) / h))) * h
+
+
+def _motor_params(pop, status, sim, seed):
+    """A motor population as a system: single beads with D = D_motors and
+    no force of their own (their diffusion, SRK.py:389-395), binned with a
+    zero-strength WCA of cutoff the chain-motor list radius.  A motor
+    population with D = 0 (pop.fixed) steps with D = 0: it keeps its place."""
+    cfg = _config
+    names = [f[0] for f in pop.self_interactions()]
+    if set(names) - {"diffuse"}:
+        raise NotImplementedError(f"forces not on the GPU step: {sorted(set(names) - {'diffuse'})}")
+    r_list = _motor_list_radius(cfg, [float(pop.motor_max_dist_sq)])
+    return SystemParams(
+        L=float(cfg.Lx), spring_params=np.zeros(6), wca_params=np.array([0.0, 0.0, 0.0, r_list]),
+        active_params=np.zeros(3), D=float(pop.D), Dr=0.0, radius=1.0, n_nearby=0, calc_springs=False,
+        calc_wca=True, self_propel=False, dtmax=float(status.dtmax), max_dist_per_step=float(cfg.max_dist_per_step),
+        rk_cheat=float(cfg.RK_cheat_factor), seed=seed, step=int(status.stepnum),
+        cell_factor=float(sim.get('gpu_cell_factor', 1.0)), skin=sim.get('gpu_skin', None))
+
+
 def _pop_params(pop, status, sim, seed):
     """The packed parameters of one population (its self_interactions, as
     SRK.py:58-97 reads them) as a ``SystemParams``."""
+    if _is_motors(pop):
+        return _motor_params(pop, status, sim, seed)
     cfg = _config
     forces = _force_list(pop)
     extra = set(forces) - _SUPPORTED
@@ -123,6 +174,8 @@ def _cross_wca(pop1, pop2):
         forces_list = pop1.interactions(pop2)
     out = np.zeros(4)
     for name, params in forces_list or []:
+        if name == "motor_push":
+            continue  # the motors' push: gcr_set_motors, not a pair force
         if name != "WCA":
             raise NotImplementedError(f"force between populations not on the GPU step: {name}")
         out = np.array(params, dtype=np.float64)[:4].copy()
@@ -334,8 +387,8 @@ class _GpuGroup:
         self.fixed = list(fixed)
         self.spg = int(sim.get('gpu_steps_per_graph', 10))
         dev = torch.device("cuda")
-        self.states = [SystemState.from_host(p.pos, p.tangent_list, p.chain_id, p.rest_lengths, prm,
-                                             precision=precision, device=dev, srk_order=srk_order)
+        self.states = [SystemState.from_host(*_pop_arrays(p, dim), prm, precision=precision, device=dev,
+                                             srk_order=srk_order)
                        for p, prm in zip(pops, params)]
         ft = torch.float64 if precision == "fp64" else torch.float32
         self.host = []
@@ -347,6 +400,7 @@ class _GpuGroup:
                                   frc=torch.empty((n, dim), dtype=ft, pin_memory=True)))
         self.engine = None
         self.cross = None
+        self.motors = []
         self.make_engine(cell_depth, list_depth)
 
     def make_engine(self, cell_depth, list_depth):
@@ -363,6 +417,19 @@ class _GpuGroup:
             self.engine.admit(st)
         if self.cross is not None:
             self.engine.couple([st.slot for st in self.states], self.fixed, self.cross)
+        for motor, chains, prm, hold in self.motors:
+            self.engine.set_motors(self.states[motor].slot, self.states[chains].slot, prm, hold)
+
+    def set_motors(self, motors):
+        """Motor populations: (motor index, chain index, params, hold)."""
+        same = len(motors) == len(self.motors) and all(
+            a[:2] == b[:2] and np.array_equal(a[2], b[2]) and a[3] == b[3] for a, b in zip(motors, self.motors))
+        if not same:
+            for motor, _, _, _ in self.motors:
+                self.engine.set_motors(self.states[motor].slot, -1, None)
+            self.motors = list(motors)
+            for motor, chains, prm, hold in self.motors:
+                self.engine.set_motors(self.states[motor].slot, self.states[chains].slot, prm, hold)
 
     def set_cross(self, cross):
         if self.cross is None or not np.array_equal(cross, self.cross):
@@ -390,20 +457,41 @@ def _srk2_populations(pops, status, sim, srk_order):
     params = [_pop_params(p, status, sim, seed + k) for k, p in enumerate(pops)]
     if not all(prm.calc_wca for prm in params):
         raise NotImplementedError("every population of the GPU step has the WCA force")
-    fixed = [bool(p.fixed) for p in pops]
+    # motors step even when they do not diffuse (D = 0 moves them by nothing)
+    fixed = [bool(p.fixed) and not _is_motors(p) for p in pops]
     n = len(pops)
     cross = np.zeros((n, n, 4))
     for k, pk in enumerate(pops):
         for q, pq in enumerate(pops):
             if k != q and not fixed[k]:
                 cross[k, q] = _cross_wca(pk, pq)
+    # motor pushes (Chain_Collection.interactions, populations.py:276-287),
+    # gated like every active force (SRK.py:84-87); the motors' cross entry
+    # carries the chain-motor list radius
+    motors = []
+    for k, pk in enumerate(pops):
+        for q, pq in enumerate(pops):
+            if k == q or not _is_motors(pq) or _is_motors(pk):
+                continue
+            for name, prm in pk.interactions(pq) or []:
+                if name != "motor_push":
+                    continue
+                prm = np.array(prm, dtype=np.float64)[:5].copy()
+                if not status.b_calc_active_forces:
+                    prm[3] = 0.0  # no motor attaches while active forces are off
+                if any(m[0] == q for m in motors):
+                    raise NotImplementedError("a motor population pushes one chain population on the GPU step")
+                motors.append((q, k, prm, bool(getattr(pq, "b_motors_dont_diffuse_while_pushing", True))))
+                cross[q, k] = [0.0, 0.0, 0.0, params[q].wca_params[3]]
     max_dt_usable = (status.next_save_time - status.t) if sim.get('save_state_every', -1) > 0 else -1.0
     max_steps = status.next_output_step - status.stepnum
     depth = getattr(pops[0], "_gcr_cell_depth",
                     default_depth(dim, max(cell_scale(prm) for prm in params)))
     ldepth = getattr(pops[0], "_gcr_list_depth", default_list_depth(dim))
-    key = (tuple((p.total_pop, len(p.rest_lengths)) for p in pops), tuple(fixed), dim, precision,
+    key = (tuple((p.total_pop, len(_pop_arrays(p, dim)[3])) for p in pops), tuple(fixed), dim, precision,
            float(cfg.Lx), depth, ldepth, srk_order)
+    if motors and srk_order != 2:
+        raise NotImplementedError("motors are stepped by the SRK2 branch on the GPU")
     g = getattr(pops[0], "_gcr_group", None)
     if g is None or g.key != key:
         if g is not None:
@@ -413,10 +501,11 @@ def _srk2_populations(pops, status, sim, srk_order):
     eng = g.engine
     for p, st, prm, h in zip(pops, g.states, params, g.host):
         h["pos"].numpy()[:] = p.pos
-        h["tan"].numpy()[:] = p.tangent_list
         st.pos.copy_(h["pos"], non_blocking=True)
-        st.tangent.copy_(h["tan"], non_blocking=True)
-        st.rest_lengths.copy_(torch.from_numpy(np.asarray(p.rest_lengths, dtype=np.float64)))
+        if not _is_motors(p):
+            h["tan"].numpy()[:] = p.tangent_list
+            st.tangent.copy_(h["tan"], non_blocking=True)
+            st.rest_lengths.copy_(torch.from_numpy(np.asarray(p.rest_lengths, dtype=np.float64)))
         st.params = prm
     try:
         for st in g.states:
@@ -427,6 +516,7 @@ def _srk2_populations(pops, status, sim, srk_order):
         g.make_engine(eng.cfg.cell_depth, eng.cfg.list_depth)
         eng = g.engine
     g.set_cross(cross)
+    g.set_motors(motors)
 
     done, elapsed, dt = 0, 0.0, float(status.dt)
     lead = fixed.index(False)  # the first moving population reports status (shared_arr[0])
@@ -469,8 +559,13 @@ def _srk2_populations(pops, status, sim, srk_order):
             continue
         p.pos[:] = h["pos"].numpy()
         p.pos1[:] = h["pos1"].numpy()
+        if _is_motors(p):
+            continue
         p.tangent_list[:] = h["tan"].numpy()
         p.forces[:] = h["frc"].numpy()
+    if g.motors:
+        for p, st in zip(pops, g.states):
+            p.where_active[:] = eng.where_active(st.slot).cpu().numpy()
     status.dt = dt
     status.dt_used = elapsed
     status.stepnum += done

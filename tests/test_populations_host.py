@@ -47,7 +47,38 @@ def test_no_interaction_gives_zeros():
 
 
 def test_other_forces_between_populations_are_refused():
-    a = _pop("chains", make_WCA_params(1.0, 1.0, 0.0, 1.0), extra=[["motor_push", np.zeros(5)]])
-    b = _pop("motors", make_WCA_params(1.0, 1.0, 0.0, 1.0))
-    with pytest.raises(NotImplementedError, match="motor_push"):
+    a = _pop("chains", make_WCA_params(1.0, 1.0, 0.0, 1.0), extra=[["quadrupole_quadrupole", np.zeros(2)]])
+    b = _pop("shells", make_WCA_params(1.0, 1.0, 0.0, 1.0))
+    with pytest.raises(NotImplementedError, match="quadrupole_quadrupole"):
         updates._cross_wca(a, b)
+
+
+def test_motor_push_is_no_pair_force():
+    a = SimpleNamespace(name="chains", special_interactions={}, b_init_growing=False,
+                        interactions=lambda other: [["motor_push", np.array([0.0625, 0, 1.0, 0.9, 0.2])]])
+    b = SimpleNamespace(name="motors", special_interactions={}, b_init_growing=False, interactions=lambda o: [])
+    np.testing.assert_array_equal(updates._cross_wca(a, b), np.zeros(4))
+
+
+def test_motor_population_as_a_system(monkeypatch):
+    """A Motor_Population maps to single diffusing beads with a zero-strength
+    WCA whose cutoff is the chain-motor list radius: grid_window * Lx /
+    n_grid with grid_window from the squared motor_max_dist (SRK.py:84-101)."""
+    cfg = SimpleNamespace(Lx=60.0, n_grid=30, grid_factor=2.0, max_dist_per_step=0.0125, RK_cheat_factor=1.0,
+                          dim=2)
+    monkeypatch.setattr(updates, "_config", cfg)
+    mot = SimpleNamespace(name="motors", total_pop=5, pos=np.zeros((5, 2)), D=0.1, Dr=0.3, fixed=False,
+                          motor_max_dist_sq=0.0625, special_interactions={}, b_init_growing=False,
+                          self_interactions=lambda: [["diffuse", np.array([1.0])]], where_active=np.zeros(5))
+    status = SimpleNamespace(dtmax=1e-3, stepnum=7, b_calc_active_forces=True)
+    prm = updates._pop_params(mot, status, {}, 3)
+    assert updates._is_motors(mot)
+    assert prm.wca_params.tolist() == [0.0, 0.0, 0.0, 2.0]
+    assert prm.D == 0.1 and prm.Dr == 0.0 and not prm.calc_springs and not prm.self_propel and prm.calc_wca
+    pos, tan, chain, rest = updates._pop_arrays(mot, 2)
+    assert chain.tolist() == [0, 1, 2, 3, 4] and tan.shape == (5, 2) and rest.shape == (5,)
+    # a wide motor reach widens the window: ceil(2 * 9 / 2) cells of 2
+    assert updates._motor_list_radius(cfg, [9.0]) == 18.0
+    # the list radius agrees with the workload's own derivation
+    from gliding_collective_rotation_b200.workloads import motor_list_radius
+    assert motor_list_radius(60.0, 1.0, 0.0625) == updates._motor_list_radius(cfg, [0.0625])
