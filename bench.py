@@ -2,7 +2,7 @@
 """Benchmark of the gliding-collective-rotation SRK2 step on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gcr|reference]
-                    [--workload sweep|large|config1|config5|pops] [--precision mixed|fp64]
+                    [--workload sweep|large|config1|config5|pops|motors] [--precision mixed|fp64]
 
 Default workload: the batched sweep -- 256 independent 2D systems (chains of
 5-40 beads, 50-4000 chains per system, area fraction 0.1-0.4, chirality and
@@ -72,14 +72,22 @@ def make_workload(name, rank=0, scale=1.0, systems=256):
         specs.groups = groups
         desc = (f"two populations per box: {len(groups)} 2D boxes L=150, 1000 chains x 10 beads (WCA, v0=1) and "
                 "3000 passive beads of diameter 0.7, one dt per box, cross WCA = mean parameters, SRK2")
+    elif name == "motors":
+        specs, groups, motors = W.motors(n_boxes=max(1, systems // 2), seed=rank, n_chains=1000, L=150.0)
+        specs = _Specs(specs)
+        specs.groups, specs.motors = groups, motors
+        desc = (f"chains pushed by motors: {len(groups)} 2D boxes L=150, 1000 chains x 10 beads (v0 handed to the "
+                "motors), 11,250 motors (density 0.5, D 0.1, k_on 0.9, k_off 0.2, reach a/2), SRK2")
     else:
         raise SystemExit(f"unknown workload {name}")
     return specs, desc
 
 
 class _Specs(list):
-    """Workload specs; ``groups``: populations coupled in one box."""
+    """Workload specs; ``groups``: populations coupled in one box; ``motors``:
+    motor populations (motor index, chain index, params, hold)."""
     groups = ()
+    motors = ()
 
 
 def workload_config(args, specs, desc, world):
@@ -388,6 +396,8 @@ def run_gpu(args):
     groups = list(getattr(specs, "groups", ()))
     for members, fixed, cross in groups:
         batch.couple(members, fixed, cross)
+    for m in getattr(specs, "motors", ()):
+        batch.set_motors(*m)
     eng = batch.engine
     n_beads = batch.n_beads
     # untimed warm-up; every step after it, timed or not, follows the
@@ -410,6 +420,8 @@ def run_gpu(args):
         batch = Batch(specs, precision=args.precision, device=dev, list_depth=args.list_depth or None, **kw)
         for members, fixed, cross in groups:
             batch.couple(members, fixed, cross)
+        for m in getattr(specs, "motors", ()):
+            batch.set_motors(*m)
         batch.set_adaptive(True)
         args.steps_per_graph, args.ctas_per_sm, args.block_beads = (kw["steps_per_graph"], kw["ctas_per_sm"],
                                                                     kw["block_beads"])
@@ -811,7 +823,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="gcr", choices=["gcr", "reference"])
     ap.add_argument("--workload", default="sweep",
-                    choices=["sweep", "large", "config1", "config5", "serve", "pops"])
+                    choices=["sweep", "large", "config1", "config5", "serve", "pops", "motors"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--systems", type=int, default=256, help="systems of the sweep workload")

@@ -30,6 +30,10 @@
  *   gcr_couple                <- SRK2_force_calc over several populations updates.py:146-247,
  *                                interpop_forces updates.py:274-312, cross-population pair
  *                                forces SRK.py:229-245, 287-294
+ *   gcr_set_motors            <- forces.calc_motor_push forces.py:248-283 with the motor_push
+ *                                parameters of Chain_Collection.interactions populations.py:276-287,
+ *                                Motor_Population diffusion SRK.py:389-395
+ *   gcr_where_active          <- pop.where_active (SRK.py:132, forces.py:267-279)
  *   gcr_order_params          <- output_methods.calc_avg_phi_chain output_methods.py:492-510,
  *                                analysis.polar_orderparameter analysis.py:315-328,
  *                                analysis.nematic_orderparameter analysis.py:294-313

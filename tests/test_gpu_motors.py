@@ -137,3 +137,57 @@ def test_set_motors_refuses_what_it_cannot_step():
     with pytest.raises(GcrError):
         b.engine.where_active(b.states[0].slot)
     b.close()
+
+
+def _fake_pops(specs, mots):
+    """The reference's population objects as the drop-in reads them: the
+    chains (Chain_Collection with motor_push toward the motors,
+    populations.py:276-287) and a Motor_Population."""
+    from types import SimpleNamespace
+    from tests.gpu_helpers import pop_from_arrays
+    ch, mo = specs
+    p = ch.params
+    chains = pop_from_arrays(ch.pos.copy(), ch.tangent.copy(), ch.chain_id, ch.rest_lengths, p.spring_params,
+                             p.wca_params, p.active_params, p.D, p.Dr, p.radius, p.n_nearby)
+    chains.name = "chains"
+    chains.where_active = np.zeros(ch.n, dtype=np.int64)
+    prm = mots[0][2]
+    motors = SimpleNamespace(
+        name="motors", total_pop=mo.n, pos=mo.pos.copy(), pos1=np.zeros_like(mo.pos), D=mo.params.D, Dr=0.0,
+        fixed=False, motor_max_dist_sq=float(prm[0]), b_motors_dont_diffuse_while_pushing=bool(mots[0][3]),
+        special_interactions={}, b_init_growing=False, n_nearby_beads_dont_repel=0,
+        where_active=np.zeros(mo.n, dtype=np.int64), interactions=lambda other: [],
+        self_interactions=lambda: [["diffuse", np.array([1.0])]])
+    chains.interactions = lambda other: [["motor_push", prm]] if other is motors else []
+    return chains, motors
+
+
+def test_drop_in_steps_chains_and_motors_as_the_batch_does(monkeypatch):
+    """updates.SRK2_force_calc over [chains, motors] (seeds sim['seed'] + k)
+    equals the Batch path with the same systems bit for bit, and writes
+    where_active back into both populations."""
+    from types import SimpleNamespace
+    from gliding_collective_rotation_b200 import config, updates
+    specs, groups, mots = _box()
+    ch = specs[0]
+    L = ch.params.L
+    for k, v in dict(dim=2, Lx=L, SRK_order=2, max_dist_per_step=ch.relax_mdps, RK_cheat_factor=1.0,
+                     n_steps_update_grid_list=40, grid_factor=2.0, n_grid=int(L / 2.0)).items():
+        monkeypatch.setattr(config, k, v)
+    monkeypatch.setattr(updates, "_config", config)
+    chains, motors = _fake_pops(specs, mots)
+    status = SimpleNamespace(dt=ch.dt, dtmax=ch.dt, stepnum=0, t=0.0, next_output_step=20, next_save_time=1e9,
+                             update_grid_list_counter=1, b_calc_active_forces=True, max_forces_strength=0.0)
+    sim = dict(seed=0, gpu_precision="fp64", save_state_every=-1)
+    updates.SRK2_force_calc([chains, motors], status, sim)
+    assert status.stepnum == 20
+    b = _batch(specs, groups, mots)
+    b.set_adaptive(True)
+    b.begin(20, dt=ch.dt)
+    b.run(20)
+    np.testing.assert_array_equal(chains.pos, b.states[0].pos.cpu().numpy())
+    np.testing.assert_array_equal(motors.pos, b.states[1].pos.cpu().numpy())
+    np.testing.assert_array_equal(chains.where_active, b.where_active(0))
+    np.testing.assert_array_equal(motors.where_active, b.where_active(1))
+    assert (motors.where_active >= 0).any()
+    b.close()
