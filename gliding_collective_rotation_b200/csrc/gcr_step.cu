@@ -1048,6 +1048,9 @@ __device__ __forceinline__ double srk_update(double x, double dt_eff, double s2,
 // read of the positions and the fp round trip (SRK2 without coupled
 // populations only; chosen per context by gcr_config.fuse_pair).
 // ------------------------------------------------------------------------
+#ifndef GCR_STAGE_XREF_EARLY
+#define GCR_STAGE_XREF_EARLY 1
+#endif
 template <int D, typename FT, int STAGE, bool FUSED = false>
 __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
 {
@@ -1090,8 +1093,11 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
             }
         }
         __syncthreads();
-        // the bead's own inputs of phase 4, loaded before the barriers
+        // the bead's own inputs of phase 4, loaded before the barriers (the
+        // build positions of a virtual update's skin test too: loaded after
+        // the pos1 stores, they would wait behind them)
         FT pre_t[D], pre_f[D], pre_p[D];
+        double pre_r[D];
         {
             const int bq = tl.begin + (int)threadIdx.x;
             const bool ok = bq < n;
@@ -1103,6 +1109,11 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                 pre_t[i] = ok ? tq[(size_t)bq * D + i] : FT(0);
                 pre_f[i] = (ok && STAGE == 1) ? fq[(size_t)bq * D + i] : FT(0);
                 pre_p[i] = (!FUSED && ok && p.calc_wca) ? pq[i] : FT(0);
+            }
+            if constexpr (stage_writes(STAGE) != 0 && GCR_STAGE_XREF_EARLY) {
+                const double *rq = A.xref + (size_t)(p.bead_off + (ok ? bq : 0)) * D;
+#pragma unroll
+                for (int i = 0; i < D; i++) pre_r[i] = (ok && p.calc_wca) ? rq[i] : 0.0;
             }
         }
         const bool springs = p.calc_springs, cb = p.calc_bend;
@@ -1345,7 +1356,8 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                     }
                     if (!finite)
                         atomicOr(&s.flags, kFlagNonFinite);
-                    else if (p.calc_wca && left_skin<D>(p, A, b, x1))
+                    else if (p.calc_wca && (GCR_STAGE_XREF_EARLY ? left_skin_of<D>(p, pre_r, x1)
+                                                                 : left_skin<D>(p, A, b, x1)))
                         s.rebuild = 1;  // the list no longer covers the new positions
                 }
             }
