@@ -117,7 +117,9 @@ class SystemState:
             raise ValueError("chains must be contiguous, increasing ranges of beads")
         return SystemState(
             pos=pos_t.clone(),
-            pos1=torch.zeros_like(pos_t),
+            # pos1 starts at pos: a motor that is attached in its first
+            # predictor keeps its previous pos1 (SRK.py:389-395)
+            pos1=pos_t.clone(),
             tangent=torch.as_tensor(np.ascontiguousarray(tangent), dtype=ft, device=device).clone(),
             forces=torch.zeros(pos_t.shape, dtype=ft, device=device),
             chain_id=torch.as_tensor(chain.astype(np.int32), device=device),
