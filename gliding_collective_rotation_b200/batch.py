@@ -194,7 +194,10 @@ class Batch:
         cell = bool(flags & FLAG_CELL_OVERFLOW)
         lst = bool(flags & FLAG_LIST_OVERFLOW) or not cell
         if (cell and self.cell_depth >= MAX_DEPTH) or (lst and self.list_depth >= MAX_LIST_DEPTH):
-            raise RuntimeError("GPU cell or list depth limit reached")
+            bad = [(x.name if hasattr(x, "name") else i, s["flags"]) for i, (x, s) in enumerate(zip(self.specs, sts))
+                   if s["flags"]]
+            raise RuntimeError(f"GPU cell or list depth limit reached (cell depth {self.cell_depth}, list depth "
+                               f"{self.list_depth}; flags {bad[:8]})")
         self.engine.close()
         if cell:
             self.cell_depth *= 2

@@ -176,6 +176,9 @@ def test_drop_in_steps_chains_and_motors_as_the_batch_does(monkeypatch):
         monkeypatch.setattr(config, k, v)
     monkeypatch.setattr(updates, "_config", config)
     chains, motors = _fake_pops(specs, mots)
+    # the batch's depths: no regrow inside the call (a regrow repeats the
+    # interrupted step, whose predictor may have moved a motor's pos1)
+    chains._gcr_cell_depth, chains._gcr_list_depth = 32, 128
     status = SimpleNamespace(dt=ch.dt, dtmax=ch.dt, stepnum=0, t=0.0, next_output_step=20, next_save_time=1e9,
                              update_grid_list_counter=1, b_calc_active_forces=True, max_forces_strength=0.0)
     sim = dict(seed=0, gpu_precision="fp64", save_state_every=-1)
