@@ -68,6 +68,9 @@ def _views(specs, precision, device, srk_order=2):
     h_chain = np.concatenate([s.chain_id for s in specs]).astype(np.int32)
     h_rest = np.concatenate([s.rest_lengths for s in specs])
     big["pos"].copy_(torch.from_numpy(h_pos))
+    # pos1 starts at pos: a motor attached in its first predictor keeps its
+    # previous pos1 (SRK.py:389-395)
+    big["pos1"].copy_(big["pos"])
     big["tangent"].copy_(torch.from_numpy(h_tan))
     big["chain_id"].copy_(torch.from_numpy(h_chain))
     big["rest"].copy_(torch.from_numpy(h_rest))

@@ -145,7 +145,6 @@ struct gcr_ctx {
     void *faux = nullptr;    // SRK4 scratch: stage forces of systems without a caller buffer
     size_t stage_smem = 0;
     size_t pair_cells_smem = 0;
-    size_t build_smem = 0;  // the list builds' shared-memory lists (list_depth <= 64), else 0
     int32_t *chain_starts = nullptr;
     int *d_err = nullptr;
     double *d_out = nullptr;
@@ -538,7 +537,7 @@ int enqueue_lists(gcr_ctx *c, int which)
     if ((rc = launch(c, c->ks.lists_plan, 1, 1024))) return rc;
     if ((rc = launch(c, bin, c->grid_bin, bb))) return rc;
     if ((rc = launch(c, c->ks.sort, c->grid_sort, bc))) return rc;
-    return launch(c, build, c->grid_build, bb, c->build_smem);
+    return launch(c, build, c->grid_build, bb);
 }
 
 // the in-graph order-parameter series: one 1024-thread CTA per slot
@@ -856,12 +855,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     c->grid_pair = kernel_grid(c, c->ks.pair0, cfg.block_beads, c->max_bead_tiles);
     c->grid_bin = kernel_grid(c, c->ks.bin0, cfg.block_beads, c->max_bead_tiles);
     c->grid_sort = kernel_grid(c, c->ks.sort, cfg.block_cells, c->max_cell_tiles);
-    // k_build keeps a thread's list in shared memory while it sorts it
-    c->build_smem = cfg.list_depth <= 64 ? (size_t)cfg.block_beads * cfg.list_depth * sizeof(int) : 0;
-    if (c->build_smem > 48 * 1024)
-        for (void *fn : {c->ks.build0, c->ks.build1, c->ks.build2})
-            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)c->build_smem);
-    c->grid_build = kernel_grid(c, c->ks.build0, cfg.block_beads, c->max_bead_tiles, c->build_smem);
+    c->grid_build = kernel_grid(c, c->ks.build0, cfg.block_beads, c->max_bead_tiles);
     c->grid_sys = (int)((S + 127) / 128);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return cleanup(fail(GCR_ERR_CUDA, "initialisation"));
     *out = c;

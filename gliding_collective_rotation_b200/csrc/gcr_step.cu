@@ -543,24 +543,12 @@ __device__ void build_cross(const BatchArgs &A, const SysP &p, SysS &s, int c, i
     if (bad) atomicOr(&s.flags, kFlagListCorrupt);
 }
 
-// list slots a thread keeps in shared memory while it builds its bead's
-// list (deeper lists are built in place in global memory)
-constexpr int kBuildSmemDepth = 64;
-
 // per bead of a flagged system: every non-excluded bead within r_l in the
-// 3^d cells around it, in ascending id; records the positions of the build.
-// The counts of the 3^d cells are loaded together before the walk, and
-// with list_depth <= kBuildSmemDepth the sorted insertion shifts entries in
-// shared memory (slot-major, one column per thread: no bank conflicts)
-// instead of global memory; the finished list is written once.
+// 3^d cells around it, in ascending id; records the positions of the build
 template <int D, int WHICH>
 __global__ void __launch_bounds__(512) k_build(BatchArgs A)
 {
-    extern __shared__ int build_smem[];
-    constexpr int NC = D == 3 ? 27 : 9;
     const Work w = work_list(A);
-    const bool in_smem = A.list_depth <= kBuildSmemDepth;
-    const int TB = blockDim.x;
     for (int t = blockIdx.x; t < w.n_bead; t += gridDim.x) {
         const int k = work_owner(w.bead0, w.m, t);
         const int sys = w.sys[k];
@@ -587,69 +575,62 @@ __global__ void __launch_bounds__(512) k_build(BatchArgs A)
         const int nn = p.n_nearby;
         const int ex_lo = nn < 0 ? c_lo : max(c_lo, b - nn);
         const int ex_hi = nn < 0 ? c_hi : min(c_hi, b + nn);
-        // the neighbour cells (dz, dy, dx ascending; index within the
-        // system's grid, which has fewer than 2^30 cells) and their counts
-        int lcs[NC];
-        int ms[NC];
-#pragma unroll
-        for (int c = 0; c < NC; c++) {
-            const int dx = c % 3 - 1, dy = (c / 3) % 3 - 1, dz = D == 3 ? c / 9 - 1 : 0;
-            int cx = ci[0] + dx, cy = ci[1] + dy, cz = D == 3 ? ci[2] + dz : 0;
-            cx = cx < 0 ? cx + nc : (cx >= nc ? cx - nc : cx);
-            cy = cy < 0 ? cy + nc : (cy >= nc ? cy - nc : cy);
-            cz = cz < 0 ? cz + nc : (cz >= nc ? cz - nc : cz);
-            lcs[c] = (cz * nc + cy) * nc + cx;
-        }
-#pragma unroll
-        for (int c = 0; c < NC; c++) {
-            const int m = A.ncell[p.cell_off + lcs[c]];
-            ms[c] = m < 0 ? 0 : (m < A.depth ? m : A.depth);
-        }
-        int *gout = A.nbr + p.bead_off + b;
-        const int64_t gstride = A.list_stride;
-        int *out = in_smem ? build_smem + threadIdx.x : gout;
-        const int64_t stride = in_smem ? TB : gstride;
+        int *out = A.nbr + p.bead_off + b;
+        const int64_t stride = A.list_stride;
         const int cap = A.list_depth;
         int cnt = 0;
         bool bad = false;
-        for (int c = 0; c < NC; c++) {
-            const int m = ms[c];
-            const int *it = A.items + ((p.cell_off + lcs[c]) << A.log_depth);
-            for (int q = 0; q < m; q++) {
-                const int j = it[q];
-                if ((unsigned)j >= (unsigned)n) {
-                    bad = true;  // never index outside the system
-                    continue;
-                }
-                if (j >= ex_lo && j <= ex_hi) continue;  // b itself is in this range
-                double ds = 0.0;
-#pragma unroll
-                for (int i = 0; i < D; i++) {
-                    double d = inbounds(X[(size_t)j * D + i], x[i], p.half_L, p.L);
-                    ds += d * d;
-                }
-                if (ds <= p.rl2) {
-                    if (cnt < cap) {
-                        // insert in ascending bead id: the pair sum then
-                        // depends on the positions only, not on when or on
-                        // which cell grid the list was built
-                        int q2 = cnt;
-                        while (q2 > 0) {
-                            const int prev = out[(size_t)(q2 - 1) * stride];
-                            if (prev < j) break;
-                            out[(size_t)q2 * stride] = prev;
-                            q2--;
+        const int zlo = (D == 3) ? -1 : 0, zhi = (D == 3) ? 1 : 0;
+        for (int dz = zlo; dz <= zhi; dz++) {
+            int cz = 0;
+            if (D == 3) {
+                cz = ci[2] + dz;
+                cz = cz < 0 ? cz + nc : (cz >= nc ? cz - nc : cz);
+            }
+            for (int dy = -1; dy <= 1; dy++) {
+                int cy = ci[1] + dy;
+                cy = cy < 0 ? cy + nc : (cy >= nc ? cy - nc : cy);
+                for (int dx = -1; dx <= 1; dx++) {
+                    int cx = ci[0] + dx;
+                    cx = cx < 0 ? cx + nc : (cx >= nc ? cx - nc : cx);
+                    const int64_t gc = p.cell_off + ((int64_t)cz * nc + cy) * nc + cx;
+                    int m = A.ncell[gc];
+                    m = m < 0 ? 0 : (m < A.depth ? m : A.depth);
+                    const int *it = A.items + (gc << A.log_depth);
+                    for (int q = 0; q < m; q++) {
+                        const int j = it[q];
+                        if ((unsigned)j >= (unsigned)n) {
+                            bad = true;  // never index outside the system
+                            continue;
                         }
-                        out[(size_t)q2 * stride] = j;
+                        if (j >= ex_lo && j <= ex_hi) continue;  // b itself is in this range
+                        double ds = 0.0;
+#pragma unroll
+                        for (int i = 0; i < D; i++) {
+                            double d = inbounds(X[(size_t)j * D + i], x[i], p.half_L, p.L);
+                            ds += d * d;
+                        }
+                        if (ds <= p.rl2) {
+                            if (cnt < cap) {
+                                // insert in ascending bead id: the pair sum then
+                                // depends on the positions only, not on when
+                                // or on which cell grid the list was built
+                                int q2 = cnt;
+                                while (q2 > 0) {
+                                    const int prev = out[(size_t)(q2 - 1) * stride];
+                                    if (prev < j) break;
+                                    out[(size_t)q2 * stride] = prev;
+                                    q2--;
+                                }
+                                out[(size_t)q2 * stride] = j;
+                            }
+                            cnt++;
+                        }
                     }
-                    cnt++;
                 }
             }
         }
-        const int kept = cnt < cap ? cnt : cap;
-        if (in_smem)
-            for (int e = 0; e < kept; e++) gout[(size_t)e * gstride] = out[(size_t)e * stride];
-        A.ncount[p.bead_off + b] = kept;
+        A.ncount[p.bead_off + b] = cnt < cap ? cnt : cap;
         double *r = A.xref + (size_t)(p.bead_off + b) * D;
 #pragma unroll
         for (int i = 0; i < D; i++) r[i] = x[i];
