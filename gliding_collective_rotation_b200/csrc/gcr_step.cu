@@ -580,7 +580,8 @@ __global__ void __launch_bounds__(512) k_build(BatchArgs A)
         const int cap = A.list_depth;
         int cnt = 0;
         bool bad = false;
-        const int zlo = (D == 3) ? -1 : 0, zhi = (D == 3) ? 1 : 0;
+        // a motor needs only its cross list (the chain beads it may push)
+        const int zlo = (D == 3) ? -1 : 0, zhi = p.motor ? zlo - 1 : ((D == 3) ? 1 : 0);
         for (int dz = zlo; dz <= zhi; dz++) {
             int cz = 0;
             if (D == 3) {
@@ -771,7 +772,9 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_pair(BatchArgs A)
         for (int i = 0; i < D; i++) xb[i] = X[(size_t)b * D + i];
         FT F[3] = {FT(0), FT(0), FT(0)};
         bool bad = false;
-        list_pair_force<D, FT>(A, p, X, xb, b, F, bad);
+        // motors have no pair force of their own (their zero-strength WCA
+        // only bins them) and no list of one another
+        if (!p.motor) list_pair_force<D, FT>(A, p, X, xb, b, F, bad);
         // a motor's cross list is its candidate beads, not a force
         if constexpr (CROSS)
             if (!p.motor) add_cross<D, FT, WHICH>(A, p, b, xb, F, bad);
