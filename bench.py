@@ -611,8 +611,10 @@ def run_gpu(args):
         "e2e": e2e, "roofline": roofline, "clocks": clk,
         # the run-start check, then 15 kernels per step (two list builds of
         # four, two pair, two stage, dt rule, update, bookkeeping; 13 when
-        # the stages sum the pair forces) in graphs of steps_per_graph steps
-        "gpu_launches": 1 + (13 if args.pair_mode == 1 and not groups else 15) * spg * math.ceil(args.steps / spg),
+        # the stages sum the pair forces; two motor-decision kernels more
+        # with motor populations) in graphs of steps_per_graph steps
+        "gpu_launches": 1 + ((13 if args.pair_mode == 1 and not groups else 15)
+                             + (2 if getattr(specs, "motors", ()) else 0)) * spg * math.ceil(args.steps / spg),
     }
     if fp64 is not None:
         line["fp64"] = fp64
