@@ -107,10 +107,42 @@ __device__ __forceinline__ FT inv_sqrt(FT x)
 }
 
 // bend at a bead with forward tangent ti (its own bond) and backward tangent
-// tj (the previous bond); false when the tangents are aligned
+// tj (the previous bond); false when the tangents are aligned.  In FP64 the
+// reference's formula as written; in FP32 the same function from the chord
+// dv = tj - ti: 1 - c = |dv|^2 / 2, acos(c) = 2 asin(|dv| / 2),
+// sqrt(1 - c^2) = sqrt((1 - c)(1 + c)), c tj - ti = dv - (1 - c) tj and
+// tj - c ti = dv + (1 - c) ti.  The dot product c of two nearly aligned
+// FP32 unit vectors cancels: near c = 1 its ulp (6e-8) is a relative error
+// of ~1e-3..1 in 1 - c and so in the bend force of a chain straight to a few
+// 1e-4 rad (measured: 2-4% force errors at such beads); the chord keeps
+// FP32's relative precision at every angle.
 template <int D, typename FT>
 __device__ __forceinline__ bool bend(const FT *ti, const FT *tj, FT theta0, FT kappa, FT *fwd, FT *bwd)
 {
+    if constexpr (sizeof(FT) == 4) {
+        FT dv[D];
+        FT ch2 = FT(0);
+#pragma unroll
+        for (int i = 0; i < D; i++) {
+            dv[i] = tj[i] - ti[i];
+            ch2 += dv[i] * dv[i];
+        }
+        const FT omc = FT(0.5) * ch2;  // 1 - c
+        if (!(omc > FT(0) && omc < FT(2))) return false;
+        FT phi = FT(2) * asinf(FT(0.5) * sqrtf(ch2));
+        if (theta0 != FT(0)) {
+            FT cr = -ti[0] * tj[1] + ti[1] * tj[0];
+            FT sg = (FT)((cr > FT(0)) - (cr < FT(0)));
+            phi += theta0 * sg;
+        }
+        phi *= kappa * inv_sqrt<FT>(omc * (FT(2) - omc));
+#pragma unroll
+        for (int i = 0; i < D; i++) {
+            fwd[i] = phi * (dv[i] - omc * tj[i]);
+            bwd[i] = phi * (dv[i] + omc * ti[i]);
+        }
+        return true;
+    }
     FT c = FT(0);
 #pragma unroll
     for (int i = 0; i < D; i++) c += ti[i] * tj[i];
@@ -1224,11 +1256,26 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                 if (p.get_orient && (prev || next)) {
                     const BT *ti = sm.bt + (tid + 2) * D, *tj = sm.bt + (tid + 1) * D;
                     if (prev && next) {
-                        BT c = BT(0);
+                        // (ti + tj) / sqrt(2 (1 + c)); aligned tangents give ti.  In
+                        // FP32 1 + c = 2 - |tj - ti|^2 / 2 and the aligned test
+                        // from the chord, as in bend()
+                        bool interior;
+                        BT coeff;
+                        if constexpr (sizeof(BT) == 4) {
+                            BT ch2 = BT(0);
 #pragma unroll
-                        for (int i = 0; i < D; i++) c += ti[i] * tj[i];
-                        if (BT(-1) < c && c < BT(1)) {
-                            BT coeff = inv_sqrt<BT>(BT(2) * (BT(1) + c));
+                            for (int i = 0; i < D; i++) ch2 += (tj[i] - ti[i]) * (tj[i] - ti[i]);
+                            const BT omc = BT(0.5) * ch2;
+                            interior = omc > BT(0) && omc < BT(2);
+                            coeff = inv_sqrt<BT>(BT(2) * (BT(2) - omc));
+                        } else {
+                            BT c = BT(0);
+#pragma unroll
+                            for (int i = 0; i < D; i++) c += ti[i] * tj[i];
+                            interior = BT(-1) < c && c < BT(1);
+                            coeff = inv_sqrt<BT>(BT(2) * (BT(1) + c));
+                        }
+                        if (interior) {
 #pragma unroll
                             for (int i = 0; i < D; i++) tg[i] = (FT)(coeff * (ti[i] + tj[i]));
                         } else {
