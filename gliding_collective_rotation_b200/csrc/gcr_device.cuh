@@ -191,8 +191,13 @@ __device__ __forceinline__ void normal_pair(uint64_t seed, uint32_t bead, int64_
 
 // The same Philox block turned into two FP32 deviates (mixed precision):
 // 24-bit uniforms from the top bits of the words the FP64 pair uses, and the
-// Box-Muller transform in FP32.  Normals agree with the FP64 pair to about
-// 1e-6 relative; the largest |z| is sqrt(2 ln 2^24) = 5.77.
+// Box-Muller transform in FP32 from the same 53-bit u1 as the FP64 pair:
+// r.x * 2^-32 + ((r.y >> 11) + 1) * 2^-53 summed in FP32 keeps 2^-24 of
+// relative precision at every magnitude, so the normals agree with the FP64
+// pair to about 1e-6 relative also in the far tail (the largest |z| is
+// sqrt(2 ln 2^53) = 8.57 on both sides).  A u1 of 24 bits alone would cut the
+// tail at 5.77 and give tail draws (one bead in ~1e6 per step) a visibly
+// different displacement from the FP64 path's.
 __device__ __forceinline__ void normal_pair_f(uint64_t seed, uint32_t bead, int64_t step, uint32_t stream,
                                               float &z0, float &z1)
 {
@@ -200,7 +205,9 @@ __device__ __forceinline__ void normal_pair_f(uint64_t seed, uint32_t bead, int6
                                        (uint32_t)((uint64_t)step >> 32), stream),
                             (uint32_t)(seed & 0xffffffffu), (uint32_t)(seed >> 32));
     const float two_m24 = 5.9604644775390625e-08f;
-    float u1 = ((float)(r.x >> 8) + 1.0f) * two_m24;
+    const float two_m32 = 2.3283064365386963e-10f, two_m53 = 1.1102230246251565e-16f;
+    // (float)r.x may round up to 2^32: u1 <= 1 keeps the log finite
+    float u1 = fminf((float)r.x * two_m32 + (float)((r.y >> 11) + 1u) * two_m53, 1.0f);
     float u2 = (float)(r.z >> 8) * two_m24;
     float rad = sqrtf(-2.0f * logf(u1));
     float s, c;
