@@ -48,12 +48,11 @@ namespace gcr {
 // which is the order in which the reference's sequential loop adds them.
 // ------------------------------------------------------------------------
 // Arithmetic type of the bonded terms on the mixed path: FP32 by default, as
-// every force; FP64 with -DGCR_BONDED_FP64=1.  A spring near its rest length,
-// k (a/|d| - 1), and the bend of a nearly straight chain, acos(c)/sqrt(1-c^2),
-// cancel in FP32: measured on B200 on the 500k-bead LJ system, the relative
-// L2 force error against FP64 is 1.2e-4 with FP32 bonded terms and 3.2e-6
-// with FP64 ones, for 8-11% more time per step; the position divergence
-// after 100-1000 steps is the same either way (chaotic growth).
+// every force; FP64 with -DGCR_BONDED_FP64=1 (8-11% more time per step).  In
+// FP32 the bend is taken from the chord of the two tangents (bend()), which
+// keeps the relative L2 force error against FP64 at 3.9e-6 on the 500k-bead
+// LJ system (3.2e-6 with FP64 bonded terms; 1.2e-4 with the FP32 dot
+// product, which cancels near c = 1).
 #ifndef GCR_BONDED_FP64
 #define GCR_BONDED_FP64 0
 #endif
