@@ -1082,9 +1082,6 @@ __device__ __forceinline__ double srk_update(double x, double dt_eff, double s2,
 // read of the positions and the fp round trip (SRK2 without coupled
 // populations only; chosen per context by gcr_config.fuse_pair).
 // ------------------------------------------------------------------------
-#ifndef GCR_STAGE_XREF_EARLY
-#define GCR_STAGE_XREF_EARLY 1
-#endif
 template <int D, typename FT, int STAGE, bool FUSED = false>
 __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
 {
@@ -1144,7 +1141,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                 pre_f[i] = (ok && STAGE == 1) ? fq[(size_t)bq * D + i] : FT(0);
                 pre_p[i] = (!FUSED && ok && p.calc_wca) ? pq[i] : FT(0);
             }
-            if constexpr (stage_writes(STAGE) != 0 && GCR_STAGE_XREF_EARLY) {
+            if constexpr (stage_writes(STAGE) != 0) {
                 const double *rq = A.xref + (size_t)(p.bead_off + (ok ? bq : 0)) * D;
 #pragma unroll
                 for (int i = 0; i < D; i++) pre_r[i] = (ok && p.calc_wca) ? rq[i] : 0.0;
@@ -1405,8 +1402,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
                     }
                     if (!finite)
                         atomicOr(&s.flags, kFlagNonFinite);
-                    else if (p.calc_wca && (GCR_STAGE_XREF_EARLY ? left_skin_of<D>(p, pre_r, x1)
-                                                                 : left_skin<D>(p, A, b, x1)))
+                    else if (p.calc_wca && left_skin_of<D>(p, pre_r, x1))
                         s.rebuild = 1;  // the list no longer covers the new positions
                 }
             }
