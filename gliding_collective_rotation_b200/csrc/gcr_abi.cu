@@ -138,6 +138,7 @@ struct gcr_ctx {
     int *ncount = nullptr;
     double *xref = nullptr;
     int *img = nullptr;  // periodic images crossed per bead and axis since admission
+    double *restb = nullptr;  // rest length of each bead's chain (refreshed at every run start)
     int *work = nullptr;
     void *xi = nullptr;
     void *fp = nullptr;
@@ -698,7 +699,7 @@ int gcr_footprint(const gcr_config *cfg, const gcr_system_desc *desc, int64_t *c
     const int64_t ft = cfg->precision == GCR_FP64 ? 8 : 4;
     const int64_t ld = cfg->list_depth > 0 ? cfg->list_depth : (cfg->dim == 2 ? 32 : 96);
     int64_t bytes = n * d * (8 + 8 + ft + ft) + n * 4 + desc->n_chains * 8     // caller-owned state
-                    + n * (1 + 2 * d * ft) + 4 * (desc->n_chains + 1)          // topo, fp, xi, chain starts
+                    + n * (1 + 2 * d * ft + 8) + 4 * (desc->n_chains + 1)      // topo, fp, xi, rest, chain starts
                     + n * (4 * ld + 4 + 8 * d)                                 // neighbour list, xref
                     + cells * (8 + (int64_t)cfg->cell_depth * 4)               // counts, slots
                     + (cfg->srk_order == 4 ? n * d * (8 + ft) : 0);            // SRK4: pos2, stage forces
@@ -769,6 +770,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     e = e ? e : cudaMalloc(&c->ncount, sizeof(int) * (size_t)cfg.bead_capacity);
     e = e ? e : cudaMalloc(&c->xref, sizeof(double) * (size_t)cfg.bead_capacity * cfg.dim);
     e = e ? e : cudaMalloc(&c->img, sizeof(int) * (size_t)cfg.bead_capacity * cfg.dim);
+    e = e ? e : cudaMalloc(&c->restb, sizeof(double) * (size_t)cfg.bead_capacity);
     e = e ? e : cudaMalloc(&c->work, sizeof(int) * (size_t)(3 + 3 * (S + 1)));
     e = e ? e : cudaMalloc(&c->xi, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
     e = e ? e : cudaMalloc(&c->fp, (size_t)cfg.bead_capacity * cfg.dim * (cfg.precision == GCR_FP64 ? 8 : 4));
@@ -810,6 +812,7 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     a.ncount = c->ncount;
     a.xref = c->xref;
     a.img = c->img;
+    a.restb = c->restb;
     a.row_prefix = c->d_row_prefix;
     // staging capacity of the cell-staged pair kernel: twice the beads of a
     // row tile and its neighbour rows at the mean occupancy (the row tiling
@@ -870,7 +873,7 @@ int gcr_destroy(gcr_ctx *c)
     void *ptrs[] = {c->dP, c->dS, c->d_bead_tiles, c->d_cell_tiles, c->d_ntiles, c->d_row_prefix, c->topo, c->cnt,
                     c->ncell,
                     c->items, c->nbr, c->ncount, c->xref, c->work, c->xi, c->fp, c->chain_starts, c->d_err,
-                    c->d_out, c->pos2, c->faux, c->xnbr, c->xcount, c->img, c->act, c->mpush, c->mdelta};
+                    c->d_out, c->pos2, c->faux, c->xnbr, c->xcount, c->img, c->act, c->mpush, c->mdelta, c->restb};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);

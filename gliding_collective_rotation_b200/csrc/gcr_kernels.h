@@ -54,6 +54,11 @@ struct BatchArgs {
     int *act;
     int *mpush;
     int *mdelta;
+    // rest length of each bead's chain, FP64 [bead]: rest_lengths[chain_id],
+    // written for every armed system at each run start (the host may change
+    // rest lengths between calls), so that the stage kernels stage it with
+    // one load instead of the chain-id load and the dependent gather
+    double *restb;
 };
 
 struct KernelSet {

@@ -1117,7 +1117,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
 #pragma unroll
                 for (int i = 0; i < D; i++) sm.x[k * D + i] = __ldg(X + (size_t)m * D + i);
                 sm.tp[k] = A.topo[p.bead_off + m];
-                sm.ra[k] = p.calc_springs ? (BT)__ldg(p.rest + __ldg(p.chain + m)) : BT(0);
+                sm.ra[k] = p.calc_springs ? (BT)A.restb[p.bead_off + m] : BT(0);
             } else {
                 sm.tp[k] = 0;
                 sm.ra[k] = BT(0);
@@ -1794,7 +1794,8 @@ __global__ void k_sys_mark(BatchArgs A, int n_slots, int slot)
     A.S[i].rebuild = 1;
 }
 
-// start of a run: the host may have written positions since the last list
+// start of a run: the rest length of every armed bead's chain into restb;
+// the host may have written positions since the last list
 // build, so every armed system is tested against its list as the step
 // kernels test it -- a bead farther than skin/2 from where the list was built
 // flags a rebuild, and otherwise the list still holds every pair within
@@ -1809,10 +1810,15 @@ __global__ void __launch_bounds__(512) k_run_check(BatchArgs A)
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
         // no barriers in this kernel: a per-thread decision is safe
-        if (!p.calc_wca || !ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal)) continue;
-        if (ld_volatile(&s.rebuild)) continue;
+        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal)) continue;
         const int b = tl.begin + threadIdx.x;
         if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
+        if (p.calc_springs) {
+            int ch = p.chain[b];
+            ch = ch < 0 ? 0 : (ch >= p.n_chains ? p.n_chains - 1 : ch);
+            A.restb[p.bead_off + b] = p.rest[ch];
+        }
+        if (!p.calc_wca || ld_volatile(&s.rebuild)) continue;
         if (p.grp_n > 0) {
             s.rebuild = 1;
             continue;

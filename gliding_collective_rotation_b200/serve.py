@@ -175,8 +175,8 @@ class Server:
     # -- memory ----------------------------------------------------------------
     def _per_bead_bytes(self):
         ft = 4 if self.precision == "mixed" else 8
-        # fp, xi, topo, list, xref
-        scratch = 2 * self.dim * ft + 1 + 4 * self.list_depth + 4 + 8 * self.dim
+        # fp, xi, topo, list, xref, rest length
+        scratch = 2 * self.dim * ft + 1 + 4 * self.list_depth + 4 + 8 * self.dim + 8
         per_cell = 4 * (self.cell_depth + 2)               # slots, count, count at the build
         return _STATE_BYTES[self.precision] + scratch + self.cells_per_bead * per_cell
 
