@@ -373,6 +373,10 @@ def run_gpu(args):
     import torch.distributed as dist
     from gliding_collective_rotation_b200.batch import Batch, PlainRunner
     from gliding_collective_rotation_b200.engine import default_skin
+    from gliding_collective_rotation_b200._lib import (FLAG_CELL_OVERFLOW, FLAG_LIST_CORRUPT, FLAG_LIST_OVERFLOW,
+                                                       FLAG_NONFINITE)
+    FLAG_FATAL = FLAG_CELL_OVERFLOW | FLAG_NONFINITE | FLAG_LIST_CORRUPT | FLAG_LIST_OVERFLOW
+    regrows = 0
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -435,32 +439,50 @@ def run_gpu(args):
         if world > 1:
             dist.barrier()
 
+    def any_rank(flag):
+        if world > 1:
+            t = torch.tensor([int(flag)], device=dev, dtype=torch.int64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            flag = bool(t.item())
+        return bool(flag)
+
     # ---- device-timed batched steps -------------------------------------
-    builds0 = [s["list_builds"] for s in batch.statuses()]
-    batch.begin(args.steps)
-    clocks = ClockSampler(local)
-    barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.nvtx.range_push("timed")
-    ev0.record(eng.stream)
-    batch.run(args.steps)
-    ev1.record(eng.stream)
-    torch.cuda.nvtx.range_pop()
-    ev1.synchronize()
-    clk = clocks.stop()
-    torch.cuda.synchronize()
-    barrier()
-    ms = ev0.elapsed_time(ev1)
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    st = batch.statuses()
+    # a system whose cells or lists overflow inside the timed steps stops
+    # there: the depths are doubled and the steps timed again, so that the
+    # number reported is of args.steps steps of every system
+    for attempt in range(4):
+        builds0 = [s["list_builds"] for s in batch.statuses()]
+        batch.begin(args.steps)
+        clocks = ClockSampler(local)
+        barrier()
+        torch.cuda.synchronize()
+        clocks.start()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.nvtx.range_push("timed")
+        ev0.record(eng.stream)
+        batch.run(args.steps)
+        ev1.record(eng.stream)
+        torch.cuda.nvtx.range_pop()
+        ev1.synchronize()
+        clk = clocks.stop()
+        torch.cuda.synchronize()
+        barrier()
+        ms = ev0.elapsed_time(ev1)
+        if world > 1:
+            t = torch.tensor([ms], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        st = batch.statuses()
+        if not any_rank(batch.overflowed(st)) or attempt == 3:
+            break
+        batch.regrow()
+        eng = batch.engine
+        regrows += 1
     steps_done = min(s["steps_done"] for s in st)
     flags = sorted({s["flags"] for s in st})
+    if steps_done < args.steps or any(f & FLAG_FATAL for f in flags):
+        raise SystemExit(f"timed run incomplete: {steps_done} of {args.steps} steps, flags {flags}")
     value = world * n_beads * args.steps / (ms / 1e3)
     # the dt the adaptive rule took: bead-weighted mean over the timed steps
     dt_mean = sum(s["dt_used"] * x.n for s, x in zip(st, batch.states)) / (args.steps * n_beads)
@@ -535,28 +557,39 @@ def run_gpu(args):
         pr.close()
 
     # ---- end to end through the public API with host buffers ------------
-    big = batch.big
-    h_pos = torch.empty(big["pos"].shape, dtype=big["pos"].dtype, pin_memory=True)
-    h_tan = torch.empty(big["tangent"].shape, dtype=big["tangent"].dtype, pin_memory=True)
-    h_pos.copy_(big["pos"])
-    h_tan.copy_(big["tangent"])
-    torch.cuda.synchronize()
+    # (timed again after a regrow, as above)
     spc = args.e2e_steps_per_call
     n_calls = max(1, args.steps // spc)
-    e2e_bytes_in = h_pos.numel() * h_pos.element_size() + h_tan.numel() * h_tan.element_size()
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(n_calls):
-        big["pos"].copy_(h_pos, non_blocking=True)
-        big["tangent"].copy_(h_tan, non_blocking=True)
-        batch.begin(spc)
-        batch.run(spc)
-        eng.synchronize()
-        h_pos.copy_(big["pos"], non_blocking=True)
-        h_tan.copy_(big["tangent"], non_blocking=True)
+    for attempt in range(4):
+        big = batch.big
+        h_pos = torch.empty(big["pos"].shape, dtype=big["pos"].dtype, pin_memory=True)
+        h_tan = torch.empty(big["tangent"].shape, dtype=big["tangent"].dtype, pin_memory=True)
+        h_pos.copy_(big["pos"])
+        h_tan.copy_(big["tangent"])
         torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
+        e2e_bytes_in = h_pos.numel() * h_pos.element_size() + h_tan.numel() * h_tan.element_size()
+        short = False
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n_calls):
+            big["pos"].copy_(h_pos, non_blocking=True)
+            big["tangent"].copy_(h_tan, non_blocking=True)
+            batch.begin(spc)
+            batch.run(spc)
+            batch.engine.synchronize()
+            h_pos.copy_(big["pos"], non_blocking=True)
+            h_tan.copy_(big["tangent"], non_blocking=True)
+            torch.cuda.synchronize()
+            short = short or min(s["steps_done"] for s in batch.statuses()) < spc
+        e2e_s = time.perf_counter() - t0
+        if not any_rank(short) or attempt == 3:
+            break
+        batch.regrow()
+        regrows += 1
+    if short:
+        raise SystemExit("end-to-end run incomplete after regrows")
+    eng = batch.engine
     if world > 1:
         t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -600,7 +633,7 @@ def run_gpu(args):
         "run": {"precision": ("FP32 forces and SRK arithmetic, FP64 positions" if args.precision == "mixed"
                               else "FP64"),
                 "relax_steps": relax_steps, "steps_done": steps_done, "flags": flags, "dt_mean": dt_mean,
-                "cell_factor": args.cell_factor,
+                "regrows_in_timing": regrows, "cell_factor": args.cell_factor,
                 "skin": specs[0].params.skin if specs[0].params.skin is not None
                 else default_skin(specs[0].params.wca_params[3]),
                 "steps_per_graph": spg, "cell_depth": batch.cell_depth,

@@ -146,6 +146,7 @@ struct gcr_ctx {
     void *faux = nullptr;    // SRK4 scratch: stage forces of systems without a caller buffer
     size_t stage_smem = 0;
     size_t pair_cells_smem = 0;
+    size_t pair_smem = 0;
     int32_t *chain_starts = nullptr;
     int *d_err = nullptr;
     double *d_out = nullptr;
@@ -561,7 +562,7 @@ int enqueue_step4(gcr_ctx *c)
         if ((rc = enqueue_lists(c, reads[k]))) return rc;
         void *pair = c->graph_cross ? c->ks.pair_cross[reads[k]]
                                     : (reads[k] == 0 ? c->ks.pair0 : (reads[k] == 1 ? c->ks.pair1 : c->ks.pair2));
-        if ((rc = launch(c, pair, c->grid_pair, bb))) return rc;
+        if ((rc = launch(c, pair, c->grid_pair, bb, c->pair_smem))) return rc;
         if ((rc = launch(c, c->ks.stage4[k], c->grid_stage4[k], bb, c->stage_smem))) return rc;
         if (k < 3 && c->graph_rigid && (rc = launch(c, c->ks.rigid4[k], c->grid_update, bb))) return rc;
     }
@@ -584,7 +585,7 @@ int enqueue_pair(gcr_ctx *c, int s, bool cross)
     if (mode == 1) return GCR_OK;
     if (mode == 2) return launch(c, c->ks.pair_cells[s], c->grid_pair_cells, c->cfg.block_beads, c->pair_cells_smem);
     void *pair = cross ? c->ks.pair_cross[s] : (s == 0 ? c->ks.pair0 : c->ks.pair1);
-    return launch(c, pair, c->grid_pair, c->cfg.block_beads);
+    return launch(c, pair, c->grid_pair, c->cfg.block_beads, c->pair_smem);
 }
 
 int enqueue_stage(gcr_ctx *c, int s, bool cross)
@@ -855,7 +856,8 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
                                          2 * cfg.bead_capacity / cfg.block_beads + S,
                                      c->pair_cells_smem);
     c->grid_update = kernel_grid(c, c->ks.update, cfg.block_beads, c->max_bead_tiles);
-    c->grid_pair = kernel_grid(c, c->ks.pair0, cfg.block_beads, c->max_bead_tiles);
+    c->pair_smem = c->ks.pair_smem(cfg.block_beads);
+    c->grid_pair = kernel_grid(c, c->ks.pair0, cfg.block_beads, c->max_bead_tiles, c->pair_smem);
     c->grid_bin = kernel_grid(c, c->ks.bin0, cfg.block_beads, c->max_bead_tiles);
     c->grid_sort = kernel_grid(c, c->ks.sort, cfg.block_cells, c->max_cell_tiles);
     c->grid_build = kernel_grid(c, c->ks.build0, cfg.block_beads, c->max_bead_tiles);

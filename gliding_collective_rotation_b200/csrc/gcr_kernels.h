@@ -95,6 +95,7 @@ struct KernelSet {
     int pair_cells_rows;  // cell rows a row tile stages (3 in 2D, 9 in 3D)
     int max_row_cells;    // cells of a row tile, at most
     size_t (*stage_smem)(int block_beads);  // dynamic shared memory of the stage kernels
+    size_t (*pair_smem)(int block_beads);   // dynamic shared memory of the pair kernels
 };
 
 KernelSet kernel_set(int dim, int precision);

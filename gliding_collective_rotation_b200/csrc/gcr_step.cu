@@ -732,17 +732,16 @@ __device__ __forceinline__ void add_cross(const BatchArgs &A, const SysP &p, int
 // of the FP64 positions xj - xb, rounded to FT, then the rule in FT, added to
 // F when 0 < r^2 <= r_cut^2 (with the optional shift rescale, 123-131)
 template <int D, typename FT>
-__device__ __forceinline__ void pair_term(const SysP &p, const double *xj, const double *xb, FT rc2, FT p0, FT p1,
-                                          FT shift, FT *F)
+__device__ __forceinline__ bool pair_coeff(const SysP &p, const double *xj, const double *xb, FT rc2, FT p0, FT p1,
+                                           FT shift, FT *sep, FT &coeff)
 {
-    FT sep[3];
     FT ds = FT(0);
 #pragma unroll
     for (int i = 0; i < D; i++) {
         sep[i] = (FT)inbounds(xj[i], xb[i], p.half_L, p.L);
         ds += sep[i] * sep[i];
     }
-    if (!(FT(0) < ds && ds <= rc2)) return;
+    if (!(FT(0) < ds && ds <= rc2)) return false;
     if (shift != FT(0)) {
         FT mag = sqrt(ds);
         FT nm = mag + shift;
@@ -752,7 +751,16 @@ __device__ __forceinline__ void pair_term(const SysP &p, const double *xj, const
         for (int i = 0; i < D; i++) sep[i] *= rs;
         ds = nm * nm;
     }
-    FT coeff = wca_coeff<FT>(ds, p0, p1);
+    coeff = wca_coeff<FT>(ds, p0, p1);
+    return true;
+}
+
+template <int D, typename FT>
+__device__ __forceinline__ void pair_term(const SysP &p, const double *xj, const double *xb, FT rc2, FT p0, FT p1,
+                                          FT shift, FT *F)
+{
+    FT sep[3], coeff;
+    if (!pair_coeff<D, FT>(p, xj, xb, rc2, p0, p1, shift, sep, coeff)) return;
 #pragma unroll
     for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
 }
@@ -781,11 +789,147 @@ __device__ __forceinline__ void list_pair_force(const BatchArgs &A, const SysP &
     }
 }
 
+// The same list walk for the 32 beads of a warp.  When the warp's pairs fill
+// more than one round of the flattened walk below, the list rows that keep at
+// least kRowBusy lanes busy (row k: the lanes whose count exceeds k) are
+// walked bead by bead, as above (a walked row costs half the instructions of
+// a flattened one, but its gathers wait on one another: for short lists one
+// flattened round is faster).  The rest -- the tails of the longer lists --
+// is flattened: those (bead, list entry) pairs are numbered bead by bead (a
+// warp scan of the remaining counts) and each lane evaluates pairs q = lane,
+// lane + 32, ..., kPairChunk of them in flight at a time, every lane busy
+// whatever the spread of the list lengths.  A lane finds the owner of its pair
+// by a binary search over the warp's exclusive prefix (owner = last lane whose
+// prefix <= q).  The pair terms (separation and coefficient, zero outside the
+// cutoff) go to the warp's shared buffer and each owner then adds its own in
+// ascending list order after its walked rows, F += sep * coeff as the serial
+// walk does: the same sums, bit for bit.  A flattened pair costs about two
+// walked rows' instructions (search, shuffles, hand-back), hence kRowBusy 16.
+#ifndef GCR_PAIR_CHUNK
+#define GCR_PAIR_CHUNK 2
+#endif
+#ifndef GCR_PAIR_ROW_BUSY
+#define GCR_PAIR_ROW_BUSY 16
+#endif
+#ifndef GCR_PAIR3D_MIN_BLOCKS
+#define GCR_PAIR3D_MIN_BLOCKS 2
+#endif
+constexpr int kPairChunk = GCR_PAIR_CHUNK;
+constexpr int kRowBusy = GCR_PAIR_ROW_BUSY;
+
+template <int D, typename FT>
+size_t pair_smem_bytes(int TB)
+{
+    return (size_t)(TB / 32) * (D + 1) * 32 * kPairChunk * sizeof(FT);
+}
+
+template <int D, typename FT>
+__device__ __forceinline__ void warp_list_pair_force(const BatchArgs &A, const SysP &p, const double *X,
+                                                     const double *xb, int b, int cnt, FT *F, bool &bad, FT *buf)
+{
+    constexpr unsigned kAll = 0xffffffffu;
+    constexpr int C = kPairChunk, Q = 32 * C;
+    const int lane = threadIdx.x & 31;
+    cnt = cnt < 0 ? 0 : (cnt < A.list_depth ? cnt : A.list_depth);
+    const int n = p.n;
+    const int64_t stride = A.list_stride;
+    const FT rc2 = (FT)p.rc2, p0 = (FT)p.p0, p1 = (FT)p.p1, shift = (FT)p.shift;
+    // the busy rows, walked bead by bead
+    int rows = 0;
+    if (__reduce_add_sync(kAll, (unsigned)cnt) > (unsigned)Q)
+        while (rows < A.list_depth && __popc(__ballot_sync(kAll, cnt > rows)) >= kRowBusy) rows++;
+    {
+        const int m = cnt < rows ? cnt : rows;
+        const int *nb = A.nbr + p.bead_off + b;
+        int j_next = m > 0 ? nb[0] : 0;
+        for (int k = 0; k < m; k++) {
+            const int j = j_next;
+            if (k + 1 < m) j_next = nb[(size_t)(k + 1) * stride];
+            if ((unsigned)j >= (unsigned)n) {
+                bad = true;
+                continue;
+            }
+            pair_term<D, FT>(p, X + (size_t)j * D, xb, rc2, p0, p1, shift, F);
+        }
+    }
+    // the tails, flattened
+    cnt = cnt > rows ? cnt - rows : 0;
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(kAll, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const int excl = incl - cnt;
+    const int total = __shfl_sync(kAll, incl, 31);
+    const int *nb0 = A.nbr + p.bead_off + (b - lane) + (size_t)rows * stride;
+    for (int base = 0; base < total; base += Q) {
+        int own[C], j[C];
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const int q = base + 32 * c + lane;
+            int lo = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1)
+                if (__shfl_sync(kAll, excl, lo + step) <= q) lo += step;
+            own[c] = lo;
+            const int k = q - __shfl_sync(kAll, excl, lo);
+            j[c] = q < total ? nb0[lo + (size_t)k * stride] : 0;
+        }
+        double xj[C][3];
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const bool ok = base + 32 * c + lane < total && (unsigned)j[c] < (unsigned)n;
+#pragma unroll
+            for (int i = 0; i < D; i++) xj[c][i] = ok ? X[(size_t)j[c] * D + i] : 0.0;
+        }
+#pragma unroll
+        for (int c = 0; c < C; c++) {
+            const int q = base + 32 * c + lane;
+            double xo[3];
+#pragma unroll
+            for (int i = 0; i < D; i++) xo[i] = __shfl_sync(kAll, xb[i], own[c]);
+            FT sep[3] = {FT(0), FT(0), FT(0)}, coeff = FT(0);
+            if (q < total) {
+                if ((unsigned)j[c] >= (unsigned)n) {
+                    bad = true;
+                } else if (!pair_coeff<D, FT>(p, xj[c], xo, rc2, p0, p1, shift, sep, coeff)) {
+#pragma unroll
+                    for (int i = 0; i < D; i++) sep[i] = FT(0);
+                    coeff = FT(0);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < D; i++) buf[i * Q + 32 * c + lane] = sep[i];
+            buf[D * Q + 32 * c + lane] = coeff;
+        }
+        __syncwarp();
+        const int q0 = excl > base ? excl : base, q1 = incl < base + Q ? incl : base + Q;
+        for (int q = q0; q < q1; q++) {
+            const FT cf = buf[D * Q + q - base];
+#pragma unroll
+            for (int i = 0; i < D; i++) F[i] += buf[i * Q + q - base] * cf;
+        }
+        __syncwarp();
+    }
+}
+
+// resident CTAs of 512 threads the pair kernel is compiled for: the 3D mixed
+// kernel is held to 64 registers (1024 threads per SM; unbounded it takes 96
+// and four fewer 128-bead CTAs fit)
+template <int D, typename FT>
+constexpr int pair_min_blocks()
+{
+    return (D == 3 && sizeof(FT) == 4) ? GCR_PAIR3D_MIN_BLOCKS : min_blocks<D, FT>();
+}
+
 // pair forces of every bead (the list walk above, then the coupled
 // populations' cross lists); writes them to fp[bead]
 template <int D, typename FT, int WHICH, bool CROSS>
-__global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_pair(BatchArgs A)
+__global__ void __launch_bounds__(512, pair_min_blocks<D, FT>()) k_pair(BatchArgs A)
 {
+    extern __shared__ __align__(16) unsigned char pair_smem[];
+    FT *wbuf = reinterpret_cast<FT *>(pair_smem) + (size_t)(threadIdx.x >> 5) * (D + 1) * 32 * kPairChunk;
     const int nt = *A.n_bead_tiles;
     // the next tile's table entry is loaded while the current tile runs
     Tile nx = (int)blockIdx.x < nt ? A.bead_tiles[blockIdx.x] : Tile{0, 0};
@@ -794,22 +938,31 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_pair(BatchArgs A)
         if (t + (int)gridDim.x < nt) nx = A.bead_tiles[t + gridDim.x];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
-        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal) || !p.calc_wca) continue;
         const int b = tl.begin + threadIdx.x;
-        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
+        const bool valid = b < p.n && threadIdx.x < A.tile_beads;
+        // the bead's own position and list count are loaded (from a valid
+        // bead of the tile, whatever the lane) together with the system's
+        // state; plain loads: only the per-system kernel between steps
+        // changes `active`, and a fatal flag raised meanwhile costs one
+        // wasted tile at most
+        const int bc = valid ? b : tl.begin;
         const double *X = stage_x<WHICH>(p);
         double xb[3] = {0.0, 0.0, 0.0};
 #pragma unroll
-        for (int i = 0; i < D; i++) xb[i] = X[(size_t)b * D + i];
+        for (int i = 0; i < D; i++) xb[i] = X[(size_t)bc * D + i];
+        const int cnt = A.ncount[p.bead_off + bc];
+        // block-uniform: every lane of a warp reaches the warp-wide walk
+        if (!s.active || (s.flags & kFlagFatal) || !p.calc_wca) continue;
         FT F[3] = {FT(0), FT(0), FT(0)};
         bool bad = false;
         // motors have no pair force of their own (their zero-strength WCA
         // only bins them) and no list of one another
-        if (!p.motor) list_pair_force<D, FT>(A, p, X, xb, b, F, bad);
+        warp_list_pair_force<D, FT>(A, p, X, xb, b, valid && !p.motor ? cnt : 0, F, bad, wbuf);
         // a motor's cross list is its candidate beads, not a force
         if constexpr (CROSS)
-            if (!p.motor) add_cross<D, FT, WHICH>(A, p, b, xb, F, bad);
+            if (valid && !p.motor) add_cross<D, FT, WHICH>(A, p, b, xb, F, bad);
         if (bad) atomicOr(&s.flags, kFlagListCorrupt);
+        if (!valid) continue;
         FT *fp = reinterpret_cast<FT *>(A.fp) + (size_t)(p.bead_off + b) * D;
 #pragma unroll
         for (int i = 0; i < D; i++) fp[i] = F[i];
@@ -1952,6 +2105,10 @@ KernelSet kernel_set(int dim, int precision)
         k.stage_smem = precision == 0 ? stage_smem_bytes<2, double> : stage_smem_bytes<2, float>;
     else
         k.stage_smem = precision == 0 ? stage_smem_bytes<3, double> : stage_smem_bytes<3, float>;
+    if (dim == 2)
+        k.pair_smem = precision == 0 ? pair_smem_bytes<2, double> : pair_smem_bytes<2, float>;
+    else
+        k.pair_smem = precision == 0 ? pair_smem_bytes<3, double> : pair_smem_bytes<3, float>;
     k.pair_cells_smem = dim == 2 ? pair_cells_smem_bytes<2> : pair_cells_smem_bytes<3>;
     k.pair_cells_rows = dim == 2 ? 3 : 9;
     k.max_row_cells = kMaxRowCells;
