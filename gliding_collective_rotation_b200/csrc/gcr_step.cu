@@ -1606,38 +1606,42 @@ __global__ void __launch_bounds__(512, update_min_blocks<D, FT>()) k_update(Batc
         if (t + (int)gridDim.x < nt) nx = A.bead_tiles[t + gridDim.x];
         const SysP &p = A.P[tl.sys];
         SysS &s = A.S[tl.sys];
-        // no barriers in this kernel: a per-thread decision is safe
-        if (!ld_volatile(&s.active) || (ld_volatile(&s.flags) & kFlagFatal)) continue;
         const int b = tl.begin + threadIdx.x;
-        if (b >= p.n || threadIdx.x >= A.tile_beads) continue;
+        const bool valid = b < p.n && threadIdx.x < A.tile_beads;
         const FT *frc = reinterpret_cast<const FT *>(p.frc);
-        const double dtu = s.dt_used;
-        // force_prefactor 0.5 of the SRK2 corrector; 1 for SRK4's weighted sum
-        const double dt_eff = dtu * (A.order == 4 ? 1.0 : 0.5) / p.radius;
-        const double s2 = sqrt(2.0 * dtu * p.D);
         const bool plain = p.rigid == 0.0;  // else k_rigid writes pos
         // every input is loaded before the first store: a store to pos may
         // alias them for the compiler, which would order each later load
-        // behind it
+        // behind it.  They go out (from a valid bead of the tile, whatever
+        // the thread) together with the system's state: plain loads, as a
+        // fatal flag raised meanwhile by another thread costs at most the
+        // update of a system that is stopping anyway
+        const int bc = valid ? b : tl.begin;
         FT xi[3] = {FT(0), FT(0), FT(0)}, fo[3] = {FT(0), FT(0), FT(0)};
         double xold[3] = {0.0, 0.0, 0.0}, xr[3] = {0.0, 0.0, 0.0};
         if (p.D > 0.0) {
-            const FT *xs = reinterpret_cast<const FT *>(A.xi) + (size_t)(p.bead_off + b) * D;
+            const FT *xs = reinterpret_cast<const FT *>(A.xi) + (size_t)(p.bead_off + bc) * D;
 #pragma unroll
             for (int i = 0; i < D; i++) xi[i] = xs[i];
         }
         if (plain) {
 #pragma unroll
             for (int i = 0; i < D; i++) {
-                xold[i] = p.pos[(size_t)b * D + i];
-                fo[i] = frc[(size_t)b * D + i];
+                xold[i] = p.pos[(size_t)bc * D + i];
+                fo[i] = frc[(size_t)bc * D + i];
             }
             if (p.calc_wca) {
-                const double *r = A.xref + (size_t)(p.bead_off + b) * D;
+                const double *r = A.xref + (size_t)(p.bead_off + bc) * D;
 #pragma unroll
                 for (int i = 0; i < D; i++) xr[i] = r[i];
             }
         }
+        // no barriers in this kernel: a per-thread decision is safe
+        if (!s.active || (s.flags & kFlagFatal) || !valid) continue;
+        const double dtu = s.dt_used;
+        // force_prefactor 0.5 of the SRK2 corrector; 1 for SRK4's weighted sum
+        const double dt_eff = dtu * (A.order == 4 ? 1.0 : 0.5) / p.radius;
+        const double s2 = sqrt(2.0 * dtu * p.D);
         double x[3] = {0.0, 0.0, 0.0};
         bool finite = true;
         // an attached motor keeps its position (SRK.py:389-395)
