@@ -492,15 +492,15 @@ def run_gpu(args):
     bead_builds = sum((s["list_builds"] - b0) * x.n for s, b0, x in zip(st, builds0, batch.states))
     builds_per_stage = bead_builds / (2.0 * args.steps * n_beads)
 
-    # ---- the same steps over two contexts -------------------------------
+    # ---- the same steps over several contexts ---------------------------
     # workloads of several independent systems: the line's value is the
-    # device time of both contexts' steps (the one-context figure above is
+    # device time of all the contexts' steps (the one-context figure above is
     # kept beside it, and is what the per-kernel profile below explains)
-    two = (args.contexts == 2 and len(specs) >= 2 and not groups and not getattr(specs, "motors", ()))
+    split = (args.contexts >= 2 and len(specs) >= 2 and not groups and not getattr(specs, "motors", ()))
     tc = None
     one_context = {"value": value, "ms_per_step": ms / args.steps}
-    if two:
-        tc = TwoContexts(args, specs, batch, dev)
+    if split:
+        tc = SplitContexts(args, specs, batch, dev, k=args.contexts)
         clocks = ClockSampler(local)
         clocks.start()
         ms2, st2 = tc.timed(args.steps, barrier, any_rank)
@@ -512,7 +512,7 @@ def run_gpu(args):
         done2 = min(s["steps_done"] for s in st2)
         flags2 = sorted({s["flags"] for s in st2})
         if done2 < args.steps or any(f & FLAG_FATAL for f in flags2):
-            raise SystemExit(f"two-context timed run incomplete: {done2} of {args.steps} steps, flags {flags2}")
+            raise SystemExit(f"split-context timed run incomplete: {done2} of {args.steps} steps, flags {flags2}")
         regrows += tc.regrows
         ms, clk = ms2, clk2
         value = world * n_beads * args.steps / (ms / 1e3)
@@ -585,7 +585,7 @@ def run_gpu(args):
     # (timed again after a regrow, as above)
     spc = args.e2e_steps_per_call
     n_calls = max(1, args.steps // spc)
-    for attempt in range(0 if two else 4):
+    for attempt in range(0 if split else 4):
         big = batch.big
         h_pos = torch.empty(big["pos"].shape, dtype=big["pos"].dtype, pin_memory=True)
         h_tan = torch.empty(big["tangent"].shape, dtype=big["tangent"].dtype, pin_memory=True)
@@ -612,7 +612,7 @@ def run_gpu(args):
             break
         batch.regrow()
         regrows += 1
-    if two:
+    if split:
         e2e_s, e2e_bytes_in, short = tc.e2e(spc, n_calls, barrier)
         short = any_rank(short)
         tc.close()
@@ -627,9 +627,9 @@ def run_gpu(args):
            "h2d_bytes_per_step": e2e_bytes_in / spc, "d2h_bytes_per_step": e2e_bytes_in / spc,
            "steps_per_call": spc, "calls": n_calls,
            "api": "Batch.begin/run (gcr_call_begin_batch, gcr_run) with pinned host buffers"
-           + ("; two Batch contexts, half of the systems each, on their own streams: one half's copies "
-              "run while the other half steps" if two else ""),
-           "contexts": 2 if two else 1}
+           + (f"; {len(tc.parts)} Batch contexts, a share of the systems each, on their own streams: one "
+              "context's copies run while the others step" if split else ""),
+           "contexts": len(tc.parts) if split else 1}
 
     # ---- the same workload in FP64, and the mixed path's error against it
     fp64 = None
@@ -672,17 +672,17 @@ def run_gpu(args):
                 "list_depth": batch.list_depth, "list_mean": list_mean,
                 "list_builds_per_stage": builds_per_stage, "block_beads": args.block_beads,
                 "ctas_per_sm": args.ctas_per_sm, "pair_mode": args.pair_mode,
-                "contexts": 2 if two else 1,
+                "contexts": len(tc.parts) if split else 1,
                 "autotune": None if tuned is None else {k: v for k, v in tuned.items() if k != "trials"}},
         "one_context": dict(one_context, note="the same steps in one context, device-timed; the per-kernel "
-                            "profile of `roofline` is of this context") if two else None,
+                            "profile of `roofline` is of this context") if split else None,
         "e2e": e2e, "roofline": roofline, "clocks": clk,
         # the run-start check, then 15 kernels per step (two list builds of
         # four, two pair, two stage, dt rule, update, bookkeeping; 13 when
         # the stages sum the pair forces; two motor-decision kernels more
         # with motor populations) in graphs of steps_per_graph steps
-        # (per context: two contexts launch both sequences)
-        "gpu_launches": (2 if two else 1) * (1 + ((13 if args.pair_mode == 1 and not groups else 15)
+        # (per context: each context launches the whole sequence)
+        "gpu_launches": (len(tc.parts) if split else 1) * (1 + ((13 if args.pair_mode == 1 and not groups else 15)
                                                   + (2 if getattr(specs, "motors", ()) else 0))
                                              * spg * math.ceil(args.steps / spg)),
     }
@@ -704,24 +704,29 @@ def run_gpu(args):
 # precision: the mixed path against the FP64 path of the same kernels
 # --------------------------------------------------------------------------
 
-class TwoContexts:
-    """The workload's systems split, by beads, over two Batch contexts, each
+class SplitContexts:
+    """The workload's systems split, by beads, over `k` Batch contexts, each
     on its own stream, started from the batch's current positions and
     tangents and warmed up untimed (their lists are built at the first
-    call).  Queued in turn, one context's kernels fill the other's tails and
+    call).  Queued in turn, one context's kernels fill the others' tails and
     idle SMs (the list kernels of a few flagged systems, the ends of the
-    persistent grids), and one context's host copies run while the other
-    steps."""
+    persistent grids), and one context's host copies run while the others
+    step."""
 
-    def __init__(self, args, specs, batch, dev):
+    def __init__(self, args, specs, batch, dev, k=2):
         import torch
         from gliding_collective_rotation_b200.batch import Batch
         self.args = args
         cum = np.cumsum([sp.n for sp in specs])
-        h = int(np.searchsorted(cum, cum[-1] / 2.0)) + 1
-        h = min(max(h, 1), len(specs) - 1)
-        self.halves = []
-        for part, states in ((specs[:h], batch.states[:h]), (specs[h:], batch.states[h:])):
+        k = max(2, min(k, len(specs)))
+        cuts = [0]
+        for q in range(1, k):
+            c = int(np.searchsorted(cum, cum[-1] * q / k)) + 1
+            cuts.append(min(max(c, cuts[-1] + 1), len(specs) - (k - q)))
+        cuts.append(len(specs))
+        self.parts = []
+        for a, b in zip(cuts[:-1], cuts[1:]):
+            part, states = specs[a:b], batch.states[a:b]
             hb = Batch(part, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph,
                        ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads, list_depth=batch.list_depth,
                        cell_depth=batch.cell_depth, pair_mode=args.pair_mode)
@@ -731,43 +736,46 @@ class TwoContexts:
             torch.cuda.synchronize()
             hb.set_adaptive(True)
             hb.run_checked(max(args.warmup, 1))
-            self.halves.append(hb)
+            self.parts.append(hb)
         self.regrows = 0
 
     def statuses(self):
-        return [st for hb in self.halves for st in hb.statuses()]
+        return [st for hb in self.parts for st in hb.statuses()]
 
     def timed(self, steps, barrier, any_rank):
-        """Device milliseconds of `steps` steps of both contexts (CUDA events
-        around both streams) and their statuses; after an overflow inside
+        """Device milliseconds of `steps` steps of every context (CUDA events
+        around all the streams) and their statuses; after an overflow inside
         the steps the overflowed context is regrown and the steps timed
         again (at most three times)."""
         import torch
         for attempt in range(4):
-            for hb in self.halves:
+            for hb in self.parts:
                 hb.begin(steps)
             torch.cuda.synchronize()
-            s0, s1 = self.halves[0].engine.stream, self.halves[1].engine.stream
-            ev0, ev1, evb = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-                             torch.cuda.Event())
+            streams = [hb.engine.stream for hb in self.parts]
+            s0 = streams[0]
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             barrier()
-            torch.cuda.nvtx.range_push("timed_two_contexts")
+            torch.cuda.nvtx.range_push("timed_contexts")
             ev0.record(s0)
-            s1.wait_event(ev0)
-            for hb in self.halves:
+            for st in streams[1:]:
+                st.wait_event(ev0)
+            for hb in self.parts:
                 hb.run(steps)
-            evb.record(s1)
-            s0.wait_event(evb)
+            for st in streams[1:]:
+                evb = torch.cuda.Event()
+                evb.record(st)
+                s0.wait_event(evb)
             ev1.record(s0)
             torch.cuda.nvtx.range_pop()
             ev1.synchronize()
             torch.cuda.synchronize()
             barrier()
             ms = ev0.elapsed_time(ev1)
-            over = [hb.overflowed() for hb in self.halves]
+            over = [hb.overflowed() for hb in self.parts]
             if not any_rank(any(over)) or attempt == 3:
                 return ms, self.statuses()
-            for hb, o in zip(self.halves, over):
+            for hb, o in zip(self.parts, over):
                 if o:
                     hb.regrow()
             self.regrows += 1
@@ -778,7 +786,7 @@ class TwoContexts:
         call; whether a call fell short."""
         import torch
         hosts = []
-        for hb in self.halves:
+        for hb in self.parts:
             hp = torch.empty(hb.big["pos"].shape, dtype=hb.big["pos"].dtype, pin_memory=True)
             ht = torch.empty(hb.big["tangent"].shape, dtype=hb.big["tangent"].dtype, pin_memory=True)
             hp.copy_(hb.big["pos"])
@@ -791,7 +799,7 @@ class TwoContexts:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for call in range(n_calls):
-            for hb, (hp, ht) in zip(self.halves, hosts):
+            for hb, (hp, ht) in zip(self.parts, hosts):
                 with torch.cuda.stream(hb.engine.stream):
                     hb.big["pos"].copy_(hp, non_blocking=True)
                     hb.big["tangent"].copy_(ht, non_blocking=True)
@@ -804,7 +812,7 @@ class TwoContexts:
                     hb.run(spc)
                     hp.copy_(hb.big["pos"], non_blocking=True)
                     ht.copy_(hb.big["tangent"], non_blocking=True)
-        for hb in self.halves:
+        for hb in self.parts:
             hb.engine.stream.synchronize()
         torch.cuda.synchronize()
         secs = time.perf_counter() - t0
@@ -812,7 +820,7 @@ class TwoContexts:
         return secs, nbytes, short
 
     def close(self):
-        for hb in self.halves:
+        for hb in self.parts:
             hb.close()
 
 
@@ -1030,9 +1038,9 @@ def main():
     ap.add_argument("--plain", type=int, default=1)
     ap.add_argument("--plain-steps", type=int, default=50)
     ap.add_argument("--e2e-steps-per-call", type=int, default=100)
-    ap.add_argument("--contexts", type=int, default=2, choices=[1, 2],
-                    help="2: the timed and end-to-end steps of a workload of several independent systems run "
-                         "over two contexts on their own streams (half of the systems each, by beads); 1: one")
+    ap.add_argument("--contexts", type=int, default=4, choices=range(1, 9),
+                    help="k > 1: the timed and end-to-end steps of a workload of several independent systems run "
+                         "over k contexts on their own streams (a share of the systems each, by beads); 1: one")
     ap.add_argument("--cpu-baseline", type=int, default=1)
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--cpu-systems", type=int, default=8, help="systems of the CPU sample (size quantiles)")
