@@ -61,6 +61,12 @@ struct Bonded {
     using type = typename std::conditional<GCR_BONDED_FP64 || sizeof(FT) == 8, double, FT>::type;
 };
 
+// list pairs a lane of the warp-wide list walk evaluates per round
+#ifndef GCR_PAIR_CHUNK
+#define GCR_PAIR_CHUNK 2
+#endif
+constexpr int kPairChunk = GCR_PAIR_CHUNK;
+
 template <int D, typename FT>
 struct StageSmem {
     using BT = typename Bonded<FT>::type;
@@ -72,6 +78,7 @@ struct StageSmem {
     BT *fw;        // [TB+2][D] bend "forward" term at bead begin-1+k
     BT *bw;        // [TB+2][D] bend "backward" term
     BT *ra;        // [TB+4]    rest length of the bead's chain
+    FT *pb;        // [TB/32][D+1][32 kPairChunk] the warps' buffers of the list walk (fused pair forces)
     __device__ void carve(unsigned char *base, int TB)
     {
         x = reinterpret_cast<double *>(base);
@@ -82,15 +89,20 @@ struct StageSmem {
         bw = fw + (size_t)(TB + 2) * D;
         ra = bw + (size_t)(TB + 2) * D;
         tp = reinterpret_cast<uint8_t *>(ra + (TB + 4));
+        pb = reinterpret_cast<FT *>(base + ((stage_base_bytes(TB) + 15) & ~(size_t)15));
+    }
+    static __host__ __device__ size_t stage_base_bytes(int TB)
+    {
+        return (size_t)(TB + 4) * D * sizeof(double) + (size_t)(TB + 3) * (2 * D + 1) * sizeof(BT) +
+               (size_t)(TB + 2) * 2 * D * sizeof(BT) + (size_t)(TB + 4) * sizeof(BT) + (size_t)(TB + 4);
     }
 };
 
 template <int D, typename FT>
 size_t stage_smem_bytes(int TB)
 {
-    using BT = typename Bonded<FT>::type;
-    return (size_t)(TB + 4) * D * sizeof(double) + (size_t)(TB + 3) * (2 * D + 1) * sizeof(BT) +
-           (size_t)(TB + 2) * 2 * D * sizeof(BT) + (size_t)(TB + 4) * sizeof(BT) + (size_t)(TB + 4) + 16;
+    return ((StageSmem<D, FT>::stage_base_bytes(TB) + 15) & ~(size_t)15) +
+           (size_t)(TB / 32) * (D + 1) * 32 * kPairChunk * sizeof(FT);
 }
 
 // 1/sqrt(x): FP64 exactly as written in the reference; FP32 (mixed path) by
@@ -765,34 +777,12 @@ __device__ __forceinline__ void pair_term(const SysP &p, const double *xj, const
     for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
 }
 
-// pair force on bead b over its neighbour list, partner by partner in
-// ascending id.  An entry outside the system sets `bad` and is not used.
-template <int D, typename FT>
-__device__ __forceinline__ void list_pair_force(const BatchArgs &A, const SysP &p, const double *X,
-                                                const double *xb, int b, FT *F, bool &bad)
-{
-    const int n = p.n;
-    int cnt = A.ncount[p.bead_off + b];
-    cnt = cnt < 0 ? 0 : (cnt < A.list_depth ? cnt : A.list_depth);
-    const int *nb = A.nbr + p.bead_off + b;
-    const int64_t stride = A.list_stride;
-    const FT rc2 = (FT)p.rc2, p0 = (FT)p.p0, p1 = (FT)p.p1, shift = (FT)p.shift;
-    int j_next = cnt > 0 ? nb[0] : 0;
-    for (int k = 0; k < cnt; k++) {
-        const int j = j_next;  // the next index is loaded ahead of this pair's positions
-        if (k + 1 < cnt) j_next = nb[(size_t)(k + 1) * stride];
-        if ((unsigned)j >= (unsigned)n) {
-            bad = true;
-            continue;
-        }
-        pair_term<D, FT>(p, X + (size_t)j * D, xb, rc2, p0, p1, shift, F);
-    }
-}
-
-// The same list walk for the 32 beads of a warp.  When the warp's pairs fill
+// The pair forces of the 32 beads of a warp over their neighbour lists, each
+// bead's partners in ascending id (an entry outside the system sets `bad`
+// and is not used).  When the warp's pairs fill
 // more than one round of the flattened walk below, the list rows that keep at
 // least kRowBusy lanes busy (row k: the lanes whose count exceeds k) are
-// walked bead by bead, as above (a walked row costs half the instructions of
+// walked bead by bead, one lane per bead (a walked row costs half the instructions of
 // a flattened one, but its gathers wait on one another: for short lists one
 // flattened round is faster).  The rest -- the tails of the longer lists --
 // is flattened: those (bead, list entry) pairs are numbered bead by bead (a
@@ -805,16 +795,12 @@ __device__ __forceinline__ void list_pair_force(const BatchArgs &A, const SysP &
 // ascending list order after its walked rows, F += sep * coeff as the serial
 // walk does: the same sums, bit for bit.  A flattened pair costs about two
 // walked rows' instructions (search, shuffles, hand-back), hence kRowBusy 16.
-#ifndef GCR_PAIR_CHUNK
-#define GCR_PAIR_CHUNK 2
-#endif
 #ifndef GCR_PAIR_ROW_BUSY
 #define GCR_PAIR_ROW_BUSY 16
 #endif
 #ifndef GCR_PAIR3D_MIN_BLOCKS
 #define GCR_PAIR3D_MIN_BLOCKS 2
 #endif
-constexpr int kPairChunk = GCR_PAIR_CHUNK;
 constexpr int kRowBusy = GCR_PAIR_ROW_BUSY;
 
 template <int D, typename FT>
@@ -1229,11 +1215,11 @@ __device__ __forceinline__ double srk_update(double x, double dt_eff, double s2,
 
 
 // ------------------------------------------------------------------------
-// stage and update kernels.  FUSED: the stage walks the bead's neighbour
-// list itself (list_pair_force, the same sum in the same order as k_pair)
-// instead of reading fp, which saves the pair kernel's launch, its second
-// read of the positions and the fp round trip (SRK2 without coupled
-// populations only; chosen per context by gcr_config.fuse_pair).
+// stage and update kernels.  FUSED: the stage walks its beads' neighbour
+// lists itself (warp_list_pair_force, the same sums as k_pair) instead of
+// reading fp, which saves the pair kernel's launch, its second read of the
+// positions and the fp round trip (SRK2 without coupled populations only;
+// gcr_config.pair_mode 1).
 // ------------------------------------------------------------------------
 template <int D, typename FT, int STAGE, bool FUSED = false>
 __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
@@ -1282,6 +1268,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
         // the pos1 stores, they would wait behind them)
         FT pre_t[D], pre_f[D], pre_p[D];
         double pre_r[D];
+        int pre_cnt = 0;  // list count of the fused pair walk
         {
             const int bq = tl.begin + (int)threadIdx.x;
             const bool ok = bq < n;
@@ -1299,6 +1286,7 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
 #pragma unroll
                 for (int i = 0; i < D; i++) pre_r[i] = (ok && p.calc_wca) ? rq[i] : 0.0;
             }
+            if constexpr (FUSED) pre_cnt = (ok && p.calc_wca && !p.motor) ? A.ncount[p.bead_off + bq] : 0;
         }
         const bool springs = p.calc_springs, cb = p.calc_bend;
         if (springs) {
@@ -1360,6 +1348,20 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
         // 4. per bead: gather bonded terms, pair forces, propulsion, update
         const int tid = threadIdx.x;
         const int b = tl.begin + tid;
+        // fused pair forces: the warp-wide list walk of k_pair, which every
+        // lane of the warp joins (a lane past the system with no list)
+        FT Fp[3] = {FT(0), FT(0), FT(0)};
+        if constexpr (FUSED) {
+            if (p.calc_wca) {
+                bool bad = false;
+                double xq[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                for (int i = 0; i < D; i++) xq[i] = sm.x[(tid + 2) * D + i];
+                warp_list_pair_force<D, FT>(A, p, X, xq, b, pre_cnt, Fp, bad,
+                                            sm.pb + (size_t)(tid >> 5) * (D + 1) * 32 * kPairChunk);
+                if (bad) atomicOr(&s.flags, kFlagListCorrupt);
+            }
+        }
         double mf2 = 0.0;
         if (b < n) {
             FT *frc = reinterpret_cast<FT *>(p.frc);
@@ -1445,10 +1447,6 @@ __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
             for (int i = 0; i < D; i++) F[i] = (FT)Fb[i];
             if (p.calc_wca) {
                 if constexpr (FUSED) {
-                    FT Fp[3] = {FT(0), FT(0), FT(0)};
-                    bool bad = false;
-                    list_pair_force<D, FT>(A, p, X, xb, b, Fp, bad);
-                    if (bad) atomicOr(&s.flags, kFlagListCorrupt);
 #pragma unroll
                     for (int i = 0; i < D; i++) F[i] += Fp[i];
                 } else {
