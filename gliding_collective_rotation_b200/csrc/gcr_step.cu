@@ -753,8 +753,9 @@ __device__ __forceinline__ bool pair_coeff(const SysP &p, const double *xj, cons
         sep[i] = (FT)inbounds(xj[i], xb[i], p.half_L, p.L);
         ds += sep[i] * sep[i];
     }
-    if (!(FT(0) < ds && ds <= rc2)) return false;
+    const bool in = FT(0) < ds && ds <= rc2;
     if (shift != FT(0)) {
+        if (!in) return false;
         FT mag = sqrt(ds);
         FT nm = mag + shift;
         nm = nm < FT(0) ? FT(0) : nm;
@@ -763,8 +764,10 @@ __device__ __forceinline__ bool pair_coeff(const SysP &p, const double *xj, cons
         for (int i = 0; i < D; i++) sep[i] *= rs;
         ds = nm * nm;
     }
-    coeff = wca_coeff<FT>(ds, p0, p1);
-    return true;
+    // without a shift, branch-free: a pair outside the cutoff takes the
+    // (finite) coefficient at r_c, which the caller does not use
+    coeff = wca_coeff<FT>(in ? ds : rc2, p0, p1);
+    return in;
 }
 
 template <int D, typename FT>
@@ -772,7 +775,10 @@ __device__ __forceinline__ void pair_term(const SysP &p, const double *xj, const
                                           FT shift, FT *F)
 {
     FT sep[3], coeff;
-    if (!pair_coeff<D, FT>(p, xj, xb, rc2, p0, p1, shift, sep, coeff)) return;
+    const bool in = pair_coeff<D, FT>(p, xj, xb, rc2, p0, p1, shift, sep, coeff);
+    // a pair outside the cutoff adds sep * 0: F unchanged, bit for bit (F
+    // starts at +0 and a sum never turns it into -0)
+    coeff = in ? coeff : FT(0);
 #pragma unroll
     for (int i = 0; i < D; i++) F[i] += sep[i] * coeff;
 }
