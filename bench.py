@@ -704,6 +704,21 @@ def run_gpu(args):
 # precision: the mixed path against the FP64 path of the same kernels
 # --------------------------------------------------------------------------
 
+def split_by_beads(sizes, k):
+    """Cut a list of system sizes into min(k, len) contiguous, non-empty runs
+    of about equal beads: the boundaries [0, c1, ..., len].  Run q ends at
+    the first system whose running bead count reaches q/k of the total."""
+    n = len(sizes)
+    k = max(1, min(int(k), n))
+    cum = np.cumsum(sizes)
+    cuts = [0]
+    for q in range(1, k):
+        c = int(np.searchsorted(cum, cum[-1] * q / k)) + 1
+        cuts.append(min(max(c, cuts[-1] + 1), n - (k - q)))
+    cuts.append(n)
+    return cuts
+
+
 class SplitContexts:
     """The workload's systems split, by beads, over `k` Batch contexts, each
     on its own stream, started from the batch's current positions and
@@ -717,13 +732,7 @@ class SplitContexts:
         import torch
         from gliding_collective_rotation_b200.batch import Batch
         self.args = args
-        cum = np.cumsum([sp.n for sp in specs])
-        k = max(2, min(k, len(specs)))
-        cuts = [0]
-        for q in range(1, k):
-            c = int(np.searchsorted(cum, cum[-1] * q / k)) + 1
-            cuts.append(min(max(c, cuts[-1] + 1), len(specs) - (k - q)))
-        cuts.append(len(specs))
+        cuts = split_by_beads([sp.n for sp in specs], max(2, k))
         self.parts = []
         for a, b in zip(cuts[:-1], cuts[1:]):
             part, states = specs[a:b], batch.states[a:b]
