@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <new>
@@ -175,6 +176,7 @@ struct gcr_ctx {
     int *xcount = nullptr;
     int64_t x_rows = 0;        // rows allocated (the slot stride of xnbr)
     void *observe = nullptr;   // k_observe of the context's precision
+    bool pdl = true;           // programmatic dependent launch of the step kernels
     bool tiles_dirty = true;
 };
 
@@ -513,19 +515,37 @@ bool any_series(const gcr_ctx *c)
     return false;
 }
 
+// a step kernel, with programmatic dependent launch: it may be scheduled
+// while the previous kernel on the stream drains, and waits for it in its
+// first statement (pdl_wait), so only the launch latency overlaps.  Off with
+// GCR_PDL=0 in the environment.
+int launch_args(gcr_ctx *c, void *fn, int grid, int block, size_t smem, void **a)
+{
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(grid);
+    lc.blockDim = dim3(block);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = c->pdl ? 1 : 0;
+    lc.attrs = at;
+    lc.numAttrs = 1;
+    GCR_CUDA(cudaLaunchKernelExC(&lc, fn, a));
+    return GCR_OK;
+}
+
 int launch(gcr_ctx *c, void *fn, int grid, int block, size_t smem = 0)
 {
     void *a[] = {&c->args};
-    GCR_CUDA(cudaLaunchKernel(fn, dim3(grid), dim3(block), a, smem, c->stream));
-    return GCR_OK;
+    return launch_args(c, fn, grid, block, smem, a);
 }
 
 int launch_sys(gcr_ctx *c, void *fn)
 {
     int n = (int)c->slots.size();
     void *a[] = {&c->args, &n};
-    GCR_CUDA(cudaLaunchKernel(fn, dim3(c->grid_sys), dim3(128), a, 0, c->stream));
-    return GCR_OK;
+    return launch_args(c, fn, c->grid_sys, 128, 0, a);
 }
 
 // one stage's neighbour lists (flagged systems only): plan, bin, per-cell
@@ -547,8 +567,7 @@ int launch_observe(gcr_ctx *c)
 {
     int dim = c->cfg.dim;
     void *a[] = {&c->args, &dim};
-    GCR_CUDA(cudaLaunchKernel(c->observe, dim3((unsigned)c->slots.size()), dim3(1024), a, 0, c->stream));
-    return GCR_OK;
+    return launch_args(c, c->observe, (int)c->slots.size(), 1024, 0, a);
 }
 
 // one SRK4 step (SRK.py:166-215): four force evaluations at pos, pos1, pos2,
@@ -750,6 +769,10 @@ int gcr_create(const gcr_config *cfg_in, void *cuda_stream, gcr_ctx **out)
     }
     c->ks = kernel_set(cfg.dim, cfg.precision);
     c->observe = observe_kernel(cfg.precision);
+    {
+        const char *e = std::getenv("GCR_PDL");
+        c->pdl = !(e && e[0] == '0');
+    }
     const int64_t S = cfg.system_capacity;
     c->max_bead_tiles = cfg.bead_capacity / cfg.block_beads + S;
     c->max_cell_tiles = cfg.cell_capacity / cfg.block_cells + S;

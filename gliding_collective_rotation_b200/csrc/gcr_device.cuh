@@ -33,6 +33,13 @@ constexpr int kMaxPops = 4;
 constexpr uint8_t kHasPrev = 1, kHasPrev2 = 2, kHasNext = 4, kHasNext2 = 8;
 
 // device status flags (mirror GCR_FLAG_* in gcr.h)
+// The step graph launches its kernels with programmatic dependent launch: a
+// kernel may be scheduled while the one before it on the stream drains.
+// Every such kernel calls this first, before touching memory: it returns
+// once the previous kernel has completed and its writes are visible (at
+// once when the launch was an ordinary one).
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 constexpr int kFlagCellOverflow = 1;
 constexpr int kFlagNonFinite = 2;
 constexpr int kFlagNextOverflow = 4;

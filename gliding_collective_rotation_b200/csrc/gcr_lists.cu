@@ -285,6 +285,7 @@ __global__ void __launch_bounds__(1024) k_order(int dim, const FT *__restrict__ 
 template <typename FT>
 __global__ void __launch_bounds__(1024) k_observe(BatchArgs A, int dim)
 {
+    pdl_wait();
     const int i = blockIdx.x;
     if (i >= A.n_slots) return;
     const SysP &p = A.P[i];

@@ -330,6 +330,7 @@ __device__ __forceinline__ int work_owner(const int *pre, int m, int i)
 // one CTA: compact the systems that take part in a list build now
 __global__ void __launch_bounds__(1024) k_lists_plan(BatchArgs A)
 {
+    pdl_wait();
     __shared__ int sh[3][32];
     __shared__ int carry[3];
     int *q = A.work;
@@ -425,6 +426,7 @@ __global__ void __launch_bounds__(1024) k_lists_plan(BatchArgs A)
 template <int D, int WHICH>
 __global__ void __launch_bounds__(512) k_bin(BatchArgs A)
 {
+    pdl_wait();
     const Work w = work_list(A);
     for (int t = blockIdx.x; t < w.n_bead; t += gridDim.x) {
         const int k = work_owner(w.bead0, w.m, t);
@@ -453,6 +455,7 @@ __global__ void __launch_bounds__(512) k_bin(BatchArgs A)
 // binning), sort the slot contents by bead id
 __global__ void __launch_bounds__(512) k_sort(BatchArgs A)
 {
+    pdl_wait();
     const Work w = work_list(A);
     for (int t = blockIdx.x; t < w.n_cell; t += gridDim.x) {
         const int k = work_owner(w.cell0, w.m, t);
@@ -591,6 +594,7 @@ __device__ void build_cross(const BatchArgs &A, const SysP &p, SysS &s, int c, i
 template <int D, int WHICH>
 __global__ void __launch_bounds__(512) k_build(BatchArgs A)
 {
+    pdl_wait();
     const Work w = work_list(A);
     for (int t = blockIdx.x; t < w.n_bead; t += gridDim.x) {
         const int k = work_owner(w.bead0, w.m, t);
@@ -920,6 +924,7 @@ constexpr int pair_min_blocks()
 template <int D, typename FT, int WHICH, bool CROSS>
 __global__ void __launch_bounds__(512, pair_min_blocks<D, FT>()) k_pair(BatchArgs A)
 {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char pair_smem[];
     FT *wbuf = reinterpret_cast<FT *>(pair_smem) + (size_t)(threadIdx.x >> 5) * (D + 1) * 32 * kPairChunk;
     const int nt = *A.n_bead_tiles;
@@ -1035,6 +1040,7 @@ __device__ __forceinline__ int cell_of_slot(const int *off, int n, int k)
 template <int D, typename FT, int WHICH>
 __global__ void __launch_bounds__(512) k_pair_cells(BatchArgs A)
 {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int R = D == 3 ? 9 : 3;  // rows of a tile with its neighbour rows
     __shared__ int off[R * (kMaxRowCells + 2) + 1];
@@ -1230,6 +1236,7 @@ __device__ __forceinline__ double srk_update(double x, double dt_eff, double s2,
 template <int D, typename FT, int STAGE, bool FUSED = false>
 __global__ void __launch_bounds__(512, min_blocks<D, FT>()) k_stage(BatchArgs A)
 {
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ unsigned long long sh_bits[16];
     __shared__ int sh_run;
@@ -1602,6 +1609,7 @@ constexpr int update_min_blocks()
 template <int D, typename FT>
 __global__ void __launch_bounds__(512, update_min_blocks<D, FT>()) k_update(BatchArgs A)
 {
+    pdl_wait();
     const int nt = *A.n_bead_tiles;
     // the next tile's table entry is loaded while the current tile runs
     Tile nx = (int)blockIdx.x < nt ? A.bead_tiles[blockIdx.x] : Tile{0, 0};
@@ -1732,6 +1740,7 @@ __device__ __forceinline__ double wrap_open(double sep, double half, double L)
 template <int D, typename FT, int STAGE>
 __global__ void __launch_bounds__(512) k_rigid(BatchArgs A)
 {
+    pdl_wait();
     const int nt = *A.n_bead_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const Tile tl = A.bead_tiles[t];
@@ -1857,6 +1866,7 @@ __global__ void __launch_bounds__(512) k_rigid(BatchArgs A)
 // per-system dt rule after stage 1 (SRK.py:323-353): one thread per slot
 __global__ void k_sys_dt(BatchArgs A, int n_slots)
 {
+    pdl_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_slots) return;
     const SysP &p = A.P[i];
@@ -1917,6 +1927,7 @@ __global__ void k_sys_dt(BatchArgs A, int n_slots)
 // 128-130): one thread per slot; a step aborted by a fatal flag is not counted
 __global__ void k_sys_end(BatchArgs A, int n_slots)
 {
+    pdl_wait();
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_slots) return;
     SysS &s = A.S[i];
@@ -1965,6 +1976,7 @@ __global__ void k_sys_mark(BatchArgs A, int n_slots, int slot)
 template <int D>
 __global__ void __launch_bounds__(512) k_run_check(BatchArgs A)
 {
+    pdl_wait();
     const int nt = *A.n_bead_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const Tile tl = A.bead_tiles[t];
@@ -2011,6 +2023,7 @@ __global__ void __launch_bounds__(512) k_run_check(BatchArgs A)
 template <int D, int WHICH>
 __global__ void __launch_bounds__(512) k_motor(BatchArgs A)
 {
+    pdl_wait();
     const int nt = *A.n_bead_tiles;
     for (int t = blockIdx.x; t < nt; t += gridDim.x) {
         const Tile tl = A.bead_tiles[t];
