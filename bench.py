@@ -493,14 +493,15 @@ def run_gpu(args):
     builds_per_stage = bead_builds / (2.0 * args.steps * n_beads)
 
     # ---- the same steps over several contexts ---------------------------
-    # workloads of several independent systems: the line's value is the
+    # workloads of several independent systems or boxes: the line's value is the
     # device time of all the contexts' steps (the one-context figure above is
     # kept beside it, and is what the per-kernel profile below explains)
-    split = (args.contexts >= 2 and len(specs) >= 2 and not groups and not getattr(specs, "motors", ()))
+    split = args.contexts >= 2 and len(context_parts([sp.n for sp in specs], args.contexts, groups)) >= 2
     tc = None
     one_context = {"value": value, "ms_per_step": ms / args.steps}
     if split:
-        tc = SplitContexts(args, specs, batch, dev, k=args.contexts)
+        tc = SplitContexts(args, specs, batch, dev, k=args.contexts, groups=groups,
+                           motors=getattr(specs, "motors", ()))
         clocks = ClockSampler(local)
         clocks.start()
         ms2, st2 = tc.timed(args.steps, barrier, any_rank)
@@ -719,6 +720,17 @@ def split_by_beads(sizes, k):
     return cuts
 
 
+def context_parts(sizes, k, groups=()):
+    """The systems of each context, as index lists: contiguous runs of about
+    equal beads (``split_by_beads``), or, with coupled populations, whole
+    boxes (a coupled group stays together) balanced by beads."""
+    if not groups:
+        cuts = split_by_beads(sizes, k)
+        return [list(range(a, b)) for a, b in zip(cuts[:-1], cuts[1:])]
+    from gliding_collective_rotation_b200 import sharding
+    return [p for p in sharding.partition_units(list(sizes), groups, k) if p]
+
+
 class SplitContexts:
     """The workload's systems split, by beads, over `k` Batch contexts, each
     on its own stream, started from the batch's current positions and
@@ -728,17 +740,25 @@ class SplitContexts:
     persistent grids), and one context's host copies run while the others
     step."""
 
-    def __init__(self, args, specs, batch, dev, k=2):
+    def __init__(self, args, specs, batch, dev, k=2, groups=(), motors=()):
         import torch
         from gliding_collective_rotation_b200.batch import Batch
         self.args = args
-        cuts = split_by_beads([sp.n for sp in specs], max(2, k))
+        index_parts = context_parts([sp.n for sp in specs], max(2, k), groups)
         self.parts = []
-        for a, b in zip(cuts[:-1], cuts[1:]):
-            part, states = specs[a:b], batch.states[a:b]
+        for idx in index_parts:
+            part, states = [specs[i] for i in idx], [batch.states[i] for i in idx]
             hb = Batch(part, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph,
                        ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads, list_depth=batch.list_depth,
                        cell_depth=batch.cell_depth, pair_mode=args.pair_mode)
+            # the populations of a box, and its motors, stay in one context
+            at = {g: j for j, g in enumerate(idx)}
+            for members, fixed, cross in groups:
+                if members[0] in at:
+                    hb.couple([at[m] for m in members], fixed, cross)
+            for m, c, prm, hold in motors:
+                if m in at:
+                    hb.set_motors(at[m], at[c], prm, hold)
             for dst, src in zip(hb.states, states):
                 dst.pos.copy_(src.pos)
                 dst.tangent.copy_(src.tangent)
