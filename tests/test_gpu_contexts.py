@@ -59,3 +59,21 @@ def test_systems_split_over_contexts_step_as_in_one():
     whole.close()
     for b in parts:
         b.close()
+
+
+def test_programmatic_launch_changes_no_bit(monkeypatch):
+    """The step kernels launched with and without programmatic dependent
+    launch (GCR_PDL, read when a context is created) end on the same bits."""
+    specs = _relaxed(4)
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("GCR_PDL", flag)
+        b = Batch(copy.deepcopy(specs), "mixed")
+        b.set_adaptive(True)
+        b.begin(60)
+        b.run(60)
+        assert all(s["flags"] == 0 and s["steps_done"] == 60 for s in b.statuses())
+        out.append([st.pos.cpu().numpy() for st in b.states])
+        b.close()
+    for a, c in zip(*out):
+        np.testing.assert_array_equal(a, c)
