@@ -674,6 +674,7 @@ def run_gpu(args):
                 "list_builds_per_stage": builds_per_stage, "block_beads": args.block_beads,
                 "ctas_per_sm": args.ctas_per_sm, "pair_mode": args.pair_mode,
                 "contexts": len(tc.parts) if split else 1,
+                "split_ctas_per_sm": (args.ctas_per_sm or args.split_ctas_per_sm) if split else None,
                 "autotune": None if tuned is None else {k: v for k, v in tuned.items() if k != "trials"}},
         "one_context": dict(one_context, note="the same steps in one context, device-timed; the per-kernel "
                             "profile of `roofline` is of this context") if split else None,
@@ -748,8 +749,11 @@ class SplitContexts:
         self.parts = []
         for idx in index_parts:
             part, states = [specs[i] for i in idx], [batch.states[i] for i in idx]
+            # persistent grids of at most split_ctas_per_sm CTAs per SM: the
+            # contexts' grids then share the SMs instead of each filling them
+            cps = args.ctas_per_sm if args.ctas_per_sm else args.split_ctas_per_sm
             hb = Batch(part, precision=args.precision, device=dev, steps_per_graph=args.steps_per_graph,
-                       ctas_per_sm=args.ctas_per_sm, block_beads=args.block_beads, list_depth=batch.list_depth,
+                       ctas_per_sm=cps, block_beads=args.block_beads, list_depth=batch.list_depth,
                        cell_depth=batch.cell_depth, pair_mode=args.pair_mode)
             # the populations of a box, and its motors, stay in one context
             at = {g: j for j, g in enumerate(idx)}
@@ -1067,6 +1071,9 @@ def main():
     ap.add_argument("--plain", type=int, default=1)
     ap.add_argument("--plain-steps", type=int, default=50)
     ap.add_argument("--e2e-steps-per-call", type=int, default=100)
+    ap.add_argument("--split-ctas-per-sm", type=int, default=6,
+                    help="persistent CTAs per SM of each context when the systems are split over several "
+                         "(0: as many as fit); --ctas-per-sm, when given, sets both")
     ap.add_argument("--contexts", type=int, default=4, choices=range(1, 9),
                     help="k > 1: the timed and end-to-end steps of a workload of several independent systems run "
                          "over k contexts on their own streams (a share of the systems each, by beads); 1: one")
